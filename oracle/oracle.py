@@ -1,0 +1,387 @@
+"""ctypes bindings for the CPU oracles -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's ``cpu_baseline`` /
+``--impl reference`` legs import this module.  It exposes
+
+* :class:`Oracle` -- our C restatement (``oracle/liboracle.so``, built from
+  ``dcrf_oracle.c``; rebuilt with gcc on first use if missing), and
+* :class:`Reference` -- the unmodified densecrf_ho compiled from its own sources
+  (``oracle/_ref/libdcrf_ref.so``, built here by ``oracle/Makefile``; absent on
+  machines without the reference tree, in which case :func:`reference_available`
+  is False).
+
+Both take and return numpy arrays in the reference's memory order:
+``[N][L]`` float32 for label matrices, ``[N][d]`` for features.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libdcrf_ref.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i16p = np.ctypeslib.ndpointer(np.int16, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+
+LP_DEFAULTS = dict(prox_reg_const=1e-2, dual_gap_tol=1e3, prox_energy_tol=1e3, prox_max_iter=10,
+                   fw_max_iter=10, qp_max_iter=1000, qp_tol=1e3, qp_const=1e-16, best_int=1,
+                   accel_prox=1, work_set_size=10, approx_fw_iter=10,
+                   less_confident_percent=0.0, confidence_tol=0.95)
+"""``LP_inf_params()`` defaults (src/densecrf.cpp:287-302)."""
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def _build_oracle():
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+
+
+class _OrcLP(C.Structure):
+    _fields_ = [("prox_reg_const", C.c_float), ("dual_gap_tol", C.c_float),
+                ("prox_energy_tol", C.c_float), ("prox_max_iter", C.c_int),
+                ("fw_max_iter", C.c_int), ("qp_max_iter", C.c_int), ("qp_tol", C.c_float),
+                ("qp_const", C.c_float), ("best_int", C.c_int), ("accel_prox", C.c_int),
+                ("work_set_size", C.c_int), ("approx_fw_iter", C.c_int),
+                ("less_confident_percent", C.c_float), ("confidence_tol", C.c_float)]
+
+
+_olib = None
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        src = os.path.join(HERE, "dcrf_oracle.c")
+        if (not os.path.exists(ORACLE_SO)) or os.path.getmtime(ORACLE_SO) < os.path.getmtime(src):
+            _build_oracle()
+        L = C.CDLL(ORACLE_SO)
+        vp = C.c_void_p
+        L.orc_lattice_new.restype = vp
+        L.orc_lattice_new.argtypes = [_f32p, C.c_int, C.c_int]
+        L.orc_lattice_free.argtypes = [vp]
+        L.orc_lattice_M.argtypes = [vp]
+        L.orc_lattice_export.argtypes = [vp, _i32p, _i32p, _f32p, _i16p, _i32p]
+        L.orc_lattice_compute.argtypes = [vp, _f32p, _f32p, C.c_int, C.c_int]
+        L.orc_lattice_compute_f64.argtypes = [vp, _f64p, _f64p, C.c_int, C.c_int]
+        L.orc_lattice_compute_ord.argtypes = [vp, _f32p, _f32p, C.c_int]
+        L.orc_model_new.restype = vp
+        L.orc_model_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
+        L.orc_model_free.argtypes = [vp]
+        L.orc_model_add_features.argtypes = [vp, _f32p, C.c_int, C.c_float]
+        L.orc_model_add_gaussian.argtypes = [vp, C.c_float, C.c_float, C.c_float]
+        L.orc_model_add_bilateral.argtypes = [vp] + [C.c_float] * 5 + [_u8p, C.c_float]
+        L.orc_model_set_cliques.argtypes = [vp, C.c_int, _i32p, _i32p, _f32p, _f32p]
+        L.orc_model_lattice_M.argtypes = [vp, C.c_int]
+        L.orc_unary_init.argtypes = [vp, _f32p]
+        L.orc_apply.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
+        L.orc_apply_ord.argtypes = [vp, C.c_int, _f32p, _f32p]
+        L.orc_qp.argtypes = [vp, _f32p, _f32p, C.c_int, C.c_void_p]
+        L.orc_lp.argtypes = [vp, _f32p, _f32p, C.POINTER(_OrcLP), C.POINTER(C.c_int)]
+        L.orc_current_map.argtypes = [vp, _f32p, _i16p]
+        for fn in ("orc_energy_true", "orc_energy_ho"):
+            getattr(L, fn).restype = C.c_double
+            getattr(L, fn).argtypes = [vp, _i16p]
+        for fn in ("orc_energy_lp", "orc_lr_qp_value"):
+            getattr(L, fn).restype = C.c_double
+            getattr(L, fn).argtypes = [vp, _f32p]
+        L.orc_last_error.restype = C.c_char_p
+        _olib = L
+    return _olib
+
+
+_rlib = None
+
+
+def reference_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref_lib():
+    global _rlib
+    if _rlib is None:
+        if not reference_available():
+            raise FileNotFoundError(f"{REF_SO} not built (make -C oracle ref)")
+        L = C.CDLL(REF_SO)
+        vp = C.c_void_p
+        L.refl_new.restype = vp
+        L.refl_new.argtypes = [_f32p, C.c_int, C.c_int]
+        L.refl_free.argtypes = [vp]
+        L.refl_M.argtypes = [vp]
+        L.refl_export.argtypes = [vp, _i32p, _i32p, _f32p, _i32p]
+        L.refl_compute.argtypes = [vp, _f32p, _f32p, C.c_int, C.c_int]
+        L.refl_compute_ord.argtypes = [vp, _f32p, _f32p, C.c_int]
+        L.refm_new.restype = vp
+        L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
+        L.refm_free.argtypes = [vp]
+        L.refm_add_gaussian.argtypes = [vp, C.c_float, C.c_float, C.c_float]
+        L.refm_add_bilateral.argtypes = [vp] + [C.c_float] * 5 + [_u8p, C.c_float]
+        L.refm_add_features.argtypes = [vp, _f32p, C.c_int, C.c_float]
+        L.refm_add_superpixel.argtypes = [vp, _u8p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.refm_num_cliques.argtypes = [vp]
+        L.refm_clique_total.argtypes = [vp]
+        L.refm_get_cliques.argtypes = [vp, _i32p, _i32p, _f32p, _f32p]
+        L.refm_set_cliques.argtypes = [vp, C.c_int, _i32p, _i32p, _f32p, _f32p]
+        L.refm_unary_init.argtypes = [vp, _f32p]
+        L.refm_apply.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
+        L.refm_apply_ord.argtypes = [vp, C.c_int, _f32p, _f32p]
+        L.refm_qp.argtypes = [vp, _f32p, _f32p]
+        L.refm_qp_fixed.argtypes = [vp, _f32p, _f32p, C.c_int, C.c_void_p]
+        L.refm_lp.argtypes = ([vp, _f32p, _f32p] + [C.c_float] * 3 + [C.c_int] * 3 +
+                              [C.c_float] * 2 + [C.c_int] * 4 + [C.c_float] * 2)
+        L.refm_current_map.argtypes = [vp, _f32p, _i16p]
+        for fn in ("refm_energy_true", "refm_energy_ho"):
+            getattr(L, fn).restype = C.c_double
+            getattr(L, fn).argtypes = [vp, _i16p]
+        for fn in ("refm_energy_lp", "refm_lr_qp_value"):
+            getattr(L, fn).restype = C.c_double
+            getattr(L, fn).argtypes = [vp, _f32p]
+        L.ref_last_error.restype = C.c_char_p
+        _rlib = L
+    return _rlib
+
+
+class _Lattice:
+    def __init__(self, lib, pfx, f):
+        f = _c(f, np.float32)
+        self.N, self.d = f.shape
+        self._lib, self._p = lib, pfx
+        self._h = getattr(lib, pfx + "_new")(f, self.d, self.N)
+
+    def __del__(self):
+        try:
+            getattr(self._lib, self._p + "_free")(self._h)
+        except Exception:
+            pass
+
+    @property
+    def M(self):
+        return getattr(self._lib, self._p + "_M")(self._h)
+
+    def compute(self, x, reverse=False):
+        x = _c(x, np.float32)
+        out = np.empty_like(x)
+        getattr(self._lib, self._p + "_compute")(self._h, out, x, x.shape[1], int(reverse))
+        return out
+
+    def compute_ord(self, x):
+        x = _c(x, np.float32)
+        out = np.empty_like(x)
+        getattr(self._lib, self._p + "_compute_ord")(self._h, out, x, x.shape[1])
+        return out
+
+
+class OracleLattice(_Lattice):
+    """Restated ``Permutohedral`` (init / compute / compute_upper_minus_lower_ord)."""
+
+    def __init__(self, f):
+        super().__init__(oracle_lib(), "orc_lattice", f)
+
+    def export(self):
+        d1, N, M = self.d + 1, self.N, self.M
+        off = np.empty(N * d1, np.int32)
+        rk = np.empty(N * d1, np.int32)
+        by = np.empty(N * d1, np.float32)
+        keys = np.empty(max(M * self.d, 1), np.int16)
+        nbr = np.empty(max(2 * d1 * M, 1), np.int32)
+        self._lib.orc_lattice_export(self._h, off, rk, by, keys, nbr)
+        return dict(offset=off, rank=rk, bary=by, keys=keys[:M * self.d],
+                    nbr=nbr[:2 * d1 * M], M=M)
+
+    def compute_f64(self, x, reverse=False):
+        x = _c(x, np.float64)
+        out = np.empty_like(x)
+        self._lib.orc_lattice_compute_f64(self._h, out, x, x.shape[1], int(reverse))
+        return out
+
+
+class ReferenceLattice(_Lattice):
+    """The reference's own ``Permutohedral``."""
+
+    def __init__(self, f):
+        super().__init__(ref_lib(), "refl", f)
+
+    def export(self):
+        d1, N, M = self.d + 1, self.N, self.M
+        off = np.empty(N * d1, np.int32)
+        rk = np.empty(N * d1, np.int32)
+        by = np.empty(N * d1, np.float32)
+        nbr = np.empty(max(2 * d1 * M, 1), np.int32)
+        self._lib.refl_export(self._h, off, rk, by, nbr)
+        return dict(offset=off, rank=rk, bary=by, nbr=nbr[:2 * d1 * M], M=M)
+
+
+class _Model:
+    pfx = ""
+
+    def __init__(self, lib, W, H, L, unary):
+        self._lib, self.W, self.H, self.L, self.N = lib, W, H, L, W * H
+        self._h = getattr(lib, self.pfx + "_new")(W, H, L, _c(unary, np.float32))
+        self.nterms = 0
+
+    def _fn(self, name):
+        return getattr(self._lib, self.pfx + "_" + name)
+
+    def __del__(self):
+        try:
+            self._fn("free")(self._h)
+        except Exception:
+            pass
+
+    def add_gaussian(self, sx, sy, w):
+        self._fn("add_gaussian")(self._h, sx, sy, w)
+        self.nterms += 1
+
+    def add_bilateral(self, sx, sy, sr, sg, sb, rgb, w):
+        self._fn("add_bilateral")(self._h, sx, sy, sr, sg, sb, _c(rgb, np.uint8), w)
+        self.nterms += 1
+
+    def add_features(self, f, w):
+        f = _c(f, np.float32)
+        self._fn("add_features")(self._h, f, f.shape[1], w)
+        self.nterms += 1
+
+    def set_cliques(self, offsets, idx, expw, constants):
+        offsets = _c(offsets, np.int32)
+        self._fn("set_cliques")(self._h, len(offsets) - 1, offsets, _c(idx, np.int32),
+                                _c(expw, np.float32), _c(constants, np.float32))
+
+    def _new(self):
+        return np.empty((self.N, self.L), np.float32)
+
+    def unary_init(self):
+        q = self._new()
+        self._fn("unary_init")(self._h, q)
+        return q
+
+    def apply(self, k, x, nonorm=False):
+        out = self._new()
+        self._fn("apply")(self._h, k, int(nonorm), out, _c(x, np.float32))
+        return out
+
+    def current_map(self, Q):
+        lab = np.empty(self.N, np.int16)
+        self._fn("current_map")(self._h, _c(Q, np.float32), lab)
+        return lab
+
+    def energy_true(self, lab):
+        return self._fn("energy_true")(self._h, _c(lab, np.int16))
+
+    def energy_ho(self, lab):
+        return self._fn("energy_ho")(self._h, _c(lab, np.int16))
+
+    def energy_lp(self, Q):
+        return self._fn("energy_lp")(self._h, _c(Q, np.float32))
+
+    def lr_qp_value(self, Q):
+        return self._fn("lr_qp_value")(self._h, _c(Q, np.float32))
+
+
+class OracleModel(_Model):
+    """Restated ``DenseCRF2D`` with Potts terms."""
+    pfx = "orc_model"
+
+    def __init__(self, W, H, L, unary):
+        super().__init__(oracle_lib(), W, H, L, unary)
+
+    def _fn(self, name):
+        lib = self._lib
+        return getattr(lib, "orc_model_" + name) if hasattr(lib, "orc_model_" + name) \
+            else getattr(lib, "orc_" + name)
+
+    def lattice_M(self, k):
+        return self._lib.orc_model_lattice_M(self._h, k)
+
+    def apply_ord(self, k, x):
+        out = self._new()
+        if self._lib.orc_apply_ord(self._h, k, out, _c(x, np.float32)) != 0:
+            raise RuntimeError(self._lib.orc_last_error().decode())
+        return out
+
+    def qp(self, init, fixed_iters=0):
+        out = self._new()
+        en = np.zeros(max(fixed_iters, 1) + 4096, np.float64)
+        it = self._lib.orc_qp(self._h, _c(init, np.float32), out, fixed_iters,
+                              en.ctypes.data_as(C.c_void_p))
+        return out, it, en[:it]
+
+    def lp(self, init, **params):
+        p = dict(LP_DEFAULTS)
+        p.update(params)
+        s = _OrcLP(**p)
+        out = self._new()
+        nit = C.c_int(0)
+        if self._lib.orc_lp(self._h, _c(init, np.float32), out, C.byref(s), C.byref(nit)) != 0:
+            raise RuntimeError(self._lib.orc_last_error().decode())
+        return out, nit.value
+
+
+class ReferenceModel(_Model):
+    """The reference's own ``DenseCRF2D`` (Potts terms)."""
+    pfx = "refm"
+
+    def __init__(self, W, H, L, unary):
+        super().__init__(ref_lib(), W, H, L, unary)
+
+    def add_superpixel(self, rgb, spatial, rng, min_region, constant, normaliser):
+        buf = _c(rgb, np.uint8).copy()
+        return self._lib.refm_add_superpixel(self._h, buf, spatial, rng, min_region, constant,
+                                             normaliser)
+
+    def get_cliques(self):
+        R = self._lib.refm_num_cliques(self._h)
+        T = self._lib.refm_clique_total(self._h)
+        off = np.empty(R + 1, np.int32)
+        idx = np.empty(max(T, 1), np.int32)
+        ex = np.empty(max(R, 1), np.float32)
+        cs = np.empty(max(R, 1), np.float32)
+        self._lib.refm_get_cliques(self._h, off, idx, ex, cs)
+        return off, idx[:T], ex[:R], cs[:R]
+
+    def apply_ord(self, k, x):
+        out = self._new()
+        if self._lib.refm_apply_ord(self._h, k, out, _c(x, np.float32)) != 0:
+            raise RuntimeError(self._lib.ref_last_error().decode())
+        return out
+
+    def qp(self, init, fixed_iters=0):
+        out = self._new()
+        if fixed_iters <= 0:
+            self._lib.refm_qp(self._h, _c(init, np.float32), out)
+            return out, None, None
+        en = np.zeros(fixed_iters, np.float64)
+        it = self._lib.refm_qp_fixed(self._h, _c(init, np.float32), out, fixed_iters,
+                                     en.ctypes.data_as(C.c_void_p))
+        return out, it, en[:it]
+
+    def lp(self, init, **params):
+        p = dict(LP_DEFAULTS)
+        p.update(params)
+        out = self._new()
+        rc = self._lib.refm_lp(self._h, _c(init, np.float32), out, p["prox_reg_const"],
+                               p["dual_gap_tol"], p["prox_energy_tol"], p["prox_max_iter"],
+                               p["fw_max_iter"], p["qp_max_iter"], p["qp_tol"], p["qp_const"],
+                               p["best_int"], p["accel_prox"], p["work_set_size"],
+                               p["approx_fw_iter"], p["less_confident_percent"],
+                               p["confidence_tol"])
+        if rc != 0:
+            raise RuntimeError(self._lib.ref_last_error().decode())
+        return out, None
+
+
+def build_model(cls, img, gaussian=(3.0, 3.0), bilateral=(50.0, 15.0, 5.0)):
+    """Gaussian + bilateral Potts model of ``src/example_inference.cpp:39-42``."""
+    m = cls(img["W"], img["H"], img["L"], img["unary"])
+    m.add_gaussian(gaussian[0], gaussian[0], gaussian[1])
+    s, c, w = bilateral
+    m.add_bilateral(s, s, c, c, c, img["rgb"], w)
+    return m

@@ -1,0 +1,311 @@
+// Test-infrastructure C driver over the UNMODIFIED densecrf_ho reference.
+//
+// This file is linked against the reference's own sources (compiled in place
+// by oracle/Makefile into oracle/_ref/libdcrf_ref.so).  It exists so that the
+// test suite, the golden-fixture generator and bench.py's CPU baseline can call
+// the reference from Python through ctypes.  Nothing in the product links it.
+//
+// Reference classes are reached through small subclasses that expose their
+// protected members (Permutohedral::offset_ etc., DenseCRF::pairwise_ etc.);
+// no reference code is modified or copied.
+//
+// Layouts: every matrix crosses this boundary as the reference's Eigen
+// column-major L x N storage, i.e. a flat float array indexed [pixel*L + label].
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
+#include <limits>
+
+#include "densecrf.h"
+#include "eigen_utils.hpp"
+#include "permutohedral.h"
+#include "qp.hpp"
+
+namespace {
+
+struct LatticeProbe : public Permutohedral {
+    int N() const { return N_; }
+    int M() const { return M_; }
+    int d() const { return d_; }
+    const std::vector<int>& offsets() const { return offset_; }
+    const std::vector<int>& ranks() const { return rank_; }
+    const std::vector<float>& barys() const { return barycentric_; }
+    void neighbours(int* out) const {
+        for (size_t i = 0; i < blur_neighbors_.size(); i++) {
+            out[2 * i] = blur_neighbors_[i].n1;
+            out[2 * i + 1] = blur_neighbors_[i].n2;
+        }
+    }
+};
+
+// Exposes DenseCRF's protected state so cliques can be injected directly and
+// so a fixed-iteration QP can be run from the reference's own building blocks.
+struct RefModel : public DenseCRF2D {
+    RefModel(int W, int H, int L) : DenseCRF2D(W, H, L) {}
+    int N() const { return N_; }
+    int L() const { return M_; }
+    int R() const { return R_; }
+    PairwisePotential* pw(int k) const { return pairwise_[k]; }
+    PairwisePotential* pw_nonorm(int k) const { return no_norm_pairwise_[k]; }
+    int num_pairwise() const { return (int)pairwise_.size(); }
+
+    void set_cliques(int R, const int* offsets, const int* idx, const float* expw,
+                     const float* constants) {
+        super_pixel_container_.clear();
+        constants_.clear();
+        exp_of_superpixels_.resize(R);
+        mean_of_superpixels_ = VectorXf::Zero(R);
+        for (int r = 0; r < R; r++) {
+            std::vector<double> px;
+            for (int p = offsets[r]; p < offsets[r + 1]; p++) px.push_back((double)idx[p]);
+            super_pixel_container_.push_back(px);
+            exp_of_superpixels_[r] = expw[r];
+            constants_.push_back(constants[r]);
+        }
+        R_ = R;
+    }
+    int clique_total() const {
+        int t = 0;
+        for (auto& c : super_pixel_container_) t += (int)c.size();
+        return t;
+    }
+    void get_cliques(int* offsets, int* idx, float* expw, float* constants) const {
+        int t = 0;
+        for (int r = 0; r < R_; r++) {
+            offsets[r] = t;
+            for (double p : super_pixel_container_[r]) idx[t++] = (int)p;
+            expw[r] = exp_of_superpixels_[r];
+            constants[r] = constants_[r];
+        }
+        offsets[R_] = t;
+    }
+
+    // The QP loop of DenseCRF::qp_inference_super_pixels_non_convex
+    // (src/densecrf.cpp:353-441) with its energy-decrease stop rule replaced by
+    // a fixed iteration count; every operation is the reference's own
+    // (PairwisePotential::apply, descent_direction, dotProduct,
+    // multiplySuperPixels).  Returns the number of iterations run.
+    int qp_fixed(const MatrixXf& init, MatrixXf& Qout, int iters, double* energies) {
+        MatrixXf Q(M_, N_), unary(M_, N_), tmp(M_, N_), grad_y(M_, N_), cond_grad_y(M_, N_),
+            grad_z(M_, R_), cond_grad_z(M_, R_), sx_z(M_, R_), sx_y(M_, N_), psisx(M_, N_),
+            z_labels(M_, R_);
+        MatrixP temp_dot(M_, N_);
+        MatrixXf constant = exp_of_superpixels_.replicate(1, grad_z.rows()).transpose();
+        grad_z.fill(0);
+        cond_grad_z.fill(0);
+        z_labels.fill(1);
+        double optimal_step_size = 0;
+        unary.fill(0);
+        if (unary_) unary = unary_->get();
+        Q = init;
+        grad_z = (MatrixXf::Ones(M_, R_) + multiplySuperPixels((Q - MatrixXf::Ones(M_, N_))));
+        grad_z = grad_z.cwiseProduct(constant);
+        descent_direction_z(cond_grad_z, grad_z);
+        grad_y = unary;
+        for (unsigned int i = 0; i < pairwise_.size(); i++) {
+            pairwise_[i]->apply(tmp, Q);
+            grad_y += 2 * tmp;
+        }
+        grad_y += multiplySuperPixels((z_labels - MatrixXf::Ones(M_, R_)).cwiseProduct(constant));
+        double energy = compute_LR_QP_value(Q, 0 * MatrixXf::Ones(M_, N_));
+        energy += (z_labels.cwiseProduct(constant).sum() +
+                   multiplySuperPixels((MatrixXf::Ones(M_, R_) - z_labels).cwiseProduct(constant),
+                                       (Q - MatrixXf::Ones(M_, N_))));
+        int it = 0;
+        for (; it < iters; it++) {
+            descent_direction(cond_grad_y, grad_y);
+            descent_direction_z(cond_grad_z, grad_z);
+            sx_y = cond_grad_y - Q;
+            sx_z = cond_grad_z - z_labels;
+            psisx.fill(0);
+            for (unsigned int i = 0; i < pairwise_.size(); i++) {
+                pairwise_[i]->apply(tmp, sx_y);
+                psisx += tmp;
+            }
+            double a = multiplySuperPixels(sx_z.cwiseProduct(constant), (Q - MatrixXf::Ones(M_, N_)));
+            double b = multiplySuperPixels((cond_grad_z - MatrixXf::Ones(M_, R_)).cwiseProduct(constant), sx_y);
+            double num = dotProduct(unary, sx_y, temp_dot) + 2 * dotProduct(Q, psisx, temp_dot) + a + b + sx_z.sum();
+            double denom = dotProduct(sx_y, psisx, temp_dot) + multiplySuperPixels(sx_z.cwiseProduct(constant), sx_y);
+            optimal_step_size = -num / (2 * denom);
+            if (denom == 0 || num == 0) break;
+            if (denom < 0) optimal_step_size = 1;
+            Q += optimal_step_size * sx_y;
+            z_labels += optimal_step_size * sx_z;
+            grad_y += 2 * optimal_step_size * psisx +
+                      optimal_step_size * multiplySuperPixels((z_labels - MatrixXf::Ones(M_, R_)).cwiseProduct(constant));
+            grad_z = MatrixXf::Ones(M_, R_).cwiseProduct(constant) +
+                     (multiplySuperPixels(Q - MatrixXf::Ones(M_, N_))).cwiseProduct(constant);
+            energy = dotProduct(Q, grad_y + unary, temp_dot);
+            energy += (z_labels.cwiseProduct(constant).sum() +
+                       multiplySuperPixels((MatrixXf::Ones(M_, R_) - z_labels).cwiseProduct(constant),
+                                           (Q - MatrixXf::Ones(M_, N_))));
+            if (energies) energies[it] = energy;
+        }
+        z_labels_ = z_labels;
+        Qout = Q;
+        return it;
+    }
+};
+
+thread_local char g_err[512] = {0};
+
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_err; }
+
+// ---------------------------------------------------------------- lattice --
+void* refl_new(const float* f, int d, int N) {
+    MatrixXf F = Map<const MatrixXf>(f, d, N);
+    LatticeProbe* p = new LatticeProbe();
+    p->init(F);
+    return p;
+}
+void refl_free(void* h) { delete (LatticeProbe*)h; }
+int refl_M(void* h) { return ((LatticeProbe*)h)->M(); }
+// offsets/ranks/barys: (d+1)*N entries of the first N pixels (pixel-major).
+// nbr: (d+1)*M pairs (n1, n2), axis-major, raw reference ids (-1 = absent).
+void refl_export(void* h, int* offset, int* rank, float* bary, int* nbr) {
+    LatticeProbe* p = (LatticeProbe*)h;
+    size_t E = (size_t)(p->d() + 1) * p->N();
+    if (offset) std::memcpy(offset, p->offsets().data(), E * sizeof(int));
+    if (rank) std::memcpy(rank, p->ranks().data(), E * sizeof(int));
+    if (bary) std::memcpy(bary, p->barys().data(), E * sizeof(float));
+    if (nbr) p->neighbours(nbr);
+}
+void refl_compute(void* h, float* out, const float* in, int L, int reverse) {
+    LatticeProbe* p = (LatticeProbe*)h;
+    MatrixXf I = Map<const MatrixXf>(in, L, p->N());
+    MatrixXf O;
+    p->compute(O, I, reverse != 0);
+    std::memcpy(out, O.data(), sizeof(float) * (size_t)L * p->N());
+}
+void refl_compute_ord(void* h, float* out, const float* in, int L) {
+    LatticeProbe* p = (LatticeProbe*)h;
+    MatrixXf I = Map<const MatrixXf>(in, L, p->N());
+    MatrixXf O = MatrixXf::Zero(L, p->N());
+    p->compute_upper_minus_lower_ord(O, I);
+    std::memcpy(out, O.data(), sizeof(float) * (size_t)L * p->N());
+}
+
+// ------------------------------------------------------------------ model --
+void* refm_new(int W, int H, int L, const float* unary) {
+    RefModel* m = new RefModel(W, H, L);
+    MatrixXf U = Map<const MatrixXf>(unary, L, W * H);
+    m->setUnaryEnergy(U);
+    return m;
+}
+void refm_free(void* h) { delete (RefModel*)h; }
+void refm_add_gaussian(void* h, float sx, float sy, float w) {
+    ((RefModel*)h)->addPairwiseGaussian(sx, sy, new PottsCompatibility(w));
+}
+void refm_add_bilateral(void* h, float sx, float sy, float sr, float sg, float sb,
+                        const unsigned char* rgb, float w) {
+    ((RefModel*)h)->addPairwiseBilateral(sx, sy, sr, sg, sb, rgb, new PottsCompatibility(w));
+}
+void refm_add_features(void* h, const float* f, int d, float w) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf F = Map<const MatrixXf>(f, d, m->N());
+    m->addPairwiseEnergy(F, new PottsCompatibility(w));
+}
+int refm_add_superpixel(void* h, unsigned char* rgb, int sr, int rr, int minreg, float c, float nrm) {
+    RefModel* m = (RefModel*)h;
+    int before = m->R();
+    m->addSuperPixel(rgb, sr, rr, minreg, c, nrm);
+    return m->R() - before;
+}
+int refm_num_cliques(void* h) { return ((RefModel*)h)->R(); }
+int refm_clique_total(void* h) { return ((RefModel*)h)->clique_total(); }
+void refm_get_cliques(void* h, int* offsets, int* idx, float* expw, float* constants) {
+    ((RefModel*)h)->get_cliques(offsets, idx, expw, constants);
+}
+void refm_set_cliques(void* h, int R, const int* offsets, const int* idx, const float* expw,
+                      const float* constants) {
+    ((RefModel*)h)->set_cliques(R, offsets, idx, expw, constants);
+}
+void refm_unary_init(void* h, float* Q) {
+    MatrixXf q = ((RefModel*)h)->unary_init();
+    std::memcpy(Q, q.data(), sizeof(float) * q.size());
+}
+void refm_apply(void* h, int k, int nonorm, float* out, const float* in) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(in, m->L(), m->N());
+    MatrixXf O;
+    (nonorm ? m->pw_nonorm(k) : m->pw(k))->apply(O, I);
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+}
+int refm_apply_ord(void* h, int k, float* out, const float* in) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(in, m->L(), m->N());
+    MatrixXf O(m->L(), m->N());
+    try {
+        m->pw(k)->apply_upper_minus_lower_ord(O, I);
+    } catch (std::exception& e) {
+        std::snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return -1;
+    }
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+    return 0;
+}
+void refm_qp(void* h, const float* init, float* out) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(init, m->L(), m->N());
+    MatrixXf O = m->qp_inference_super_pixels_non_convex(I);
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+}
+int refm_qp_fixed(void* h, const float* init, float* out, int iters, double* energies) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(init, m->L(), m->N());
+    MatrixXf O;
+    int it = m->qp_fixed(I, O, iters, energies);
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+    return it;
+}
+int refm_lp(void* h, const float* init, float* out, float prox_reg_const, float dual_gap_tol,
+            float prox_energy_tol, int prox_max_iter, int fw_max_iter, int qp_max_iter,
+            float qp_tol, float qp_const, int best_int, int accel_prox, int work_set_size,
+            int approx_fw_iter, float less_confident_percent, float confidence_tol) {
+    RefModel* m = (RefModel*)h;
+    LP_inf_params p(prox_reg_const, dual_gap_tol, prox_energy_tol, prox_max_iter, fw_max_iter,
+                    qp_max_iter, qp_tol, qp_const, best_int != 0, accel_prox != 0, work_set_size,
+                    approx_fw_iter, less_confident_percent, confidence_tol);
+    MatrixXf I = Map<const MatrixXf>(init, m->L(), m->N());
+    try {
+        MatrixXf O = m->lp_inference_prox_super_pixels(I, p);
+        std::memcpy(out, O.data(), sizeof(float) * O.size());
+    } catch (std::exception& e) {
+        std::snprintf(g_err, sizeof(g_err), "%s", e.what());
+        return -1;
+    }
+    return 0;
+}
+void refm_current_map(void* h, const float* Q, short* labels) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(Q, m->L(), m->N());
+    VectorXs l = m->currentMap(I);
+    std::memcpy(labels, l.data(), sizeof(short) * l.size());
+}
+double refm_energy_true(void* h, const short* labels) {
+    RefModel* m = (RefModel*)h;
+    VectorXs l = Map<const VectorXs>(labels, m->N());
+    return m->assignment_energy_true(l);
+}
+double refm_energy_ho(void* h, const short* labels) {
+    RefModel* m = (RefModel*)h;
+    VectorXs l = Map<const VectorXs>(labels, m->N());
+    return m->assignment_energy_higher_order(l);
+}
+double refm_energy_lp(void* h, const float* Q) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(Q, m->L(), m->N());
+    return m->compute_energy_LP_higher_order(I);
+}
+double refm_lr_qp_value(void* h, const float* Q) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(Q, m->L(), m->N());
+    return m->compute_LR_QP_value(I, MatrixXf::Zero(m->L(), m->N()));
+}
+
+}  // extern "C"
