@@ -1,0 +1,229 @@
+"""densecrf_ho_b200 -- B200-native dense-CRF inference, a drop-in for the hot
+path of densecrf_ho.
+
+The product is the C ABI ``libdcrf_cuda.so`` (``include/dcrf.h``) and the C++
+shim with the reference's class API (``densecrf_ho_b200/cpp``).  This module is
+a thin ctypes mirror of the same classes, used by the test-suite, the
+benchmark and Python callers:
+
+* :class:`Permutohedral` -- ``init`` / ``compute`` /
+  ``compute_upper_minus_lower_ord`` (include/permutohedral.h:50-88);
+* :class:`DenseCRF2D` -- ``setUnaryEnergy``, ``addPairwiseGaussian``,
+  ``addPairwiseBilateral``, ``addPairwiseEnergy``, cliques, ``unary_init``,
+  ``qp_inference_super_pixels_non_convex``, ``lp_inference_prox_super_pixels``,
+  ``currentMap`` and the energies (include/densecrf.h:73-194).
+
+Arrays use the reference's memory order: label matrices ``[N, L]`` float32
+(Eigen column-major L x N), features ``[N, d]``.  There is no CPU fallback:
+without the CUDA library or a GPU every call raises :class:`DCRFError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import DCRFError, LPParams, SolveStats, lib, check
+
+__all__ = ["Permutohedral", "DenseCRF2D", "LPParams", "SolveStats", "DCRFError", "lib"]
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None and a.shape != shape:
+        a = a.reshape(shape)
+    return a
+
+
+class Permutohedral:
+    """Device permutohedral lattice (class Permutohedral)."""
+
+    def __init__(self):
+        self._h = C.c_void_p()
+        check(lib().dcrf_lattice_create(C.byref(self._h)))
+        self.N = self.d = self.M = 0
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().dcrf_lattice_destroy(h)
+            except Exception:
+                pass
+
+    def init(self, features):
+        f = _f32(features)
+        N, d = f.shape
+        check(lib().dcrf_lattice_init(self._h, f.ctypes.data_as(C.c_void_p), d, N))
+        M = C.c_int()
+        check(lib().dcrf_lattice_info(self._h, C.byref(M), None, None))
+        self.N, self.d, self.M = N, d, M.value
+        return self
+
+    def compute(self, inp, reverse=False):
+        x = _f32(inp)
+        if x.ndim == 1:
+            x = x.reshape(-1, 1)
+        out = np.empty_like(x)
+        check(lib().dcrf_lattice_compute(self._h, out.ctypes.data_as(C.c_void_p),
+                                         x.ctypes.data_as(C.c_void_p), x.shape[1], int(reverse)))
+        return out
+
+    def compute_upper_minus_lower_ord(self, Q):
+        x = _f32(Q)
+        out = np.empty_like(x)
+        check(lib().dcrf_lattice_compute_ord(self._h, out.ctypes.data_as(C.c_void_p),
+                                             x.ctypes.data_as(C.c_void_p), x.shape[1]))
+        return out
+
+    def export(self):
+        d1, N, M, d = self.d + 1, self.N, self.M, self.d
+        off = np.empty(N * d1, np.int32)
+        rk = np.empty(N * d1, np.int32)
+        by = np.empty(N * d1, np.float32)
+        keys = np.empty(max(M * d, 1), np.int16)
+        nbr = np.empty(max(2 * d1 * M, 1), np.int32)
+        check(lib().dcrf_lattice_export(self._h, off.ctypes.data_as(C.c_void_p),
+                                        rk.ctypes.data_as(C.c_void_p), by.ctypes.data_as(C.c_void_p),
+                                        keys.ctypes.data_as(C.c_void_p), nbr.ctypes.data_as(C.c_void_p)))
+        return dict(offset=off, rank=rk, bary=by, keys=keys[:M * d], nbr=nbr[:2 * d1 * M], M=M)
+
+
+class DenseCRF2D:
+    """Device dense CRF over a W x H grid with L labels (class DenseCRF2D)."""
+
+    def __init__(self, W, H, L):
+        self.W, self.H, self.L, self.N = W, H, L, W * H
+        self._h = C.c_void_p()
+        check(lib().dcrf_model_create(C.byref(self._h), W, H, L))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().dcrf_model_destroy(h)
+            except Exception:
+                pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _mat(self, a):
+        return _f32(a, (self.N, self.L))
+
+    def _new(self):
+        return np.empty((self.N, self.L), np.float32)
+
+    # -- set-up ---------------------------------------------------------
+    def setUnaryEnergy(self, unary):
+        u = self._mat(unary)
+        check(lib().dcrf_model_set_unary(self._h, u.ctypes.data_as(C.c_void_p)))
+
+    def addPairwiseGaussian(self, sx, sy, w):
+        check(lib().dcrf_model_add_gaussian(self._h, C.c_float(sx), C.c_float(sy), C.c_float(w)))
+
+    def addPairwiseBilateral(self, sx, sy, sr, sg, sb, rgb, w):
+        im = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1)
+        if im.size != 3 * self.N:
+            raise DCRFError(1, "rgb must hold W*H*3 bytes")
+        check(lib().dcrf_model_add_bilateral(self._h, *(C.c_float(v) for v in (sx, sy, sr, sg, sb)),
+                                             im.ctypes.data_as(C.c_void_p), C.c_float(w)))
+
+    def addPairwiseEnergy(self, features, w):
+        f = _f32(features)
+        check(lib().dcrf_model_add_pairwise(self._h, f.ctypes.data_as(C.c_void_p), f.shape[1],
+                                            C.c_float(w)))
+
+    def setCliques(self, offsets, idx, exp_weight, constants):
+        offsets = np.ascontiguousarray(offsets, np.int32)
+        idx = np.ascontiguousarray(idx, np.int32)
+        ew = np.ascontiguousarray(exp_weight, np.float32)
+        cs = np.ascontiguousarray(constants, np.float32)
+        R = len(offsets) - 1
+        check(lib().dcrf_model_set_cliques(self._h, R, offsets.ctypes.data_as(C.c_void_p),
+                                           idx.ctypes.data_as(C.c_void_p) if idx.size else None,
+                                           ew.ctypes.data_as(C.c_void_p), cs.ctypes.data_as(C.c_void_p)))
+
+    def info(self):
+        n, N, L = C.c_int(), C.c_int(), C.c_int()
+        check(lib().dcrf_model_info(self._h, C.byref(n), C.byref(N), C.byref(L)))
+        return n.value
+
+    def lattice_size(self, k):
+        M = C.c_int()
+        check(lib().dcrf_model_lattice_size(self._h, k, C.byref(M)))
+        return M.value
+
+    # -- inference ------------------------------------------------------
+    def unary_init(self):
+        q = self._new()
+        check(lib().dcrf_model_unary_init(self._h, q.ctypes.data_as(C.c_void_p)))
+        return q
+
+    def pairwise_apply(self, k, Q, nonorm=False):
+        x = self._mat(Q)
+        out = self._new()
+        check(lib().dcrf_model_pairwise_apply(self._h, k, int(nonorm), out.ctypes.data_as(C.c_void_p),
+                                              x.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def pairwise_apply_upper_minus_lower_ord(self, k, Q):
+        x = self._mat(Q)
+        out = self._new()
+        check(lib().dcrf_model_pairwise_apply_ord(self._h, k, out.ctypes.data_as(C.c_void_p),
+                                                  x.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def qp_inference_super_pixels_non_convex(self, init, max_iter=0, stats=False):
+        x = self._mat(init)
+        out = self._new()
+        p = C.c_int(max_iter)
+        st = SolveStats()
+        check(lib().dcrf_model_qp(self._h, x.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p),
+                                  C.byref(p), C.byref(st)))
+        return (out, st) if stats else out
+
+    def lp_inference_prox_super_pixels(self, init, params=None, stats=False, **kw):
+        x = self._mat(init)
+        out = self._new()
+        p = params if params is not None else LPParams.default()
+        for k, v in kw.items():
+            setattr(p, k, v)
+        st = SolveStats()
+        check(lib().dcrf_model_lp(self._h, x.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p),
+                                  C.byref(p), C.byref(st)))
+        return (out, st) if stats else out
+
+    def currentMap(self, Q):
+        x = self._mat(Q)
+        lab = np.empty(self.N, np.int16)
+        check(lib().dcrf_model_current_map(self._h, x.ctypes.data_as(C.c_void_p),
+                                           lab.ctypes.data_as(C.c_void_p)))
+        return lab
+
+    def _energy_l(self, fn, labels):
+        lab = np.ascontiguousarray(labels, np.int16)
+        e = C.c_double()
+        check(fn(self._h, lab.ctypes.data_as(C.c_void_p), C.byref(e)))
+        return e.value
+
+    def assignment_energy_true(self, labels):
+        return self._energy_l(lib().dcrf_model_energy_true, labels)
+
+    def assignment_energy_higher_order(self, labels):
+        return self._energy_l(lib().dcrf_model_energy_ho, labels)
+
+    def compute_energy_LP_higher_order(self, Q):
+        x = self._mat(Q)
+        e = C.c_double()
+        check(lib().dcrf_model_energy_lp(self._h, x.ctypes.data_as(C.c_void_p), C.byref(e)))
+        return e.value
+
+    def compute_LR_QP_value(self, Q):
+        x = self._mat(Q)
+        e = C.c_double()
+        check(lib().dcrf_model_lr_qp_value(self._h, x.ctypes.data_as(C.c_void_p), C.byref(e)))
+        return e.value

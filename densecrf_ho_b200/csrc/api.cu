@@ -1,0 +1,568 @@
+// extern "C" boundary of libdcrf_cuda.so (declared in include/dcrf.h).
+// Converts exceptions to dcrf_status codes; host-pointer entry points stage
+// through device buffers owned by the handle and synchronise before return.
+#include <cstring>
+#include <string>
+
+#include "model.cuh"
+
+using dcrf::DevBuf;
+using dcrf::Error;
+
+struct dcrf_lattice_s {
+    dcrf::Lattice lat;
+    cudaStream_t stream = nullptr;
+    DevBuf<float> feat, in, out;
+};
+
+struct dcrf_model_s {
+    dcrf::Model* m = nullptr;
+    DevBuf<float> io0, io1, feat;
+    DevBuf<uint8_t> img;
+    DevBuf<int16_t> lab;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+dcrf_status guard(F&& f) {
+    try {
+        f();
+        return DCRF_OK;
+    } catch (const Error& e) {
+        g_err = e.what();
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        g_err = "host allocation failed";
+        return DCRF_E_NOMEM;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return DCRF_E_CUDA;
+    }
+}
+
+void check_device() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        throw Error(DCRF_E_CUDA, std::string("no usable CUDA device: ") + cudaGetErrorString(e));
+}
+
+template <typename T>
+T* upload(DevBuf<T>& b, const T* h, size_t n, cudaStream_t st) {
+    T* d = b.ensure(n);
+    DCRF_CUDA(cudaMemcpyAsync(d, h, sizeof(T) * n, cudaMemcpyHostToDevice, st));
+    return d;
+}
+
+template <typename T>
+void download(T* h, const T* d, size_t n, cudaStream_t st) {
+    DCRF_CUDA(cudaMemcpyAsync(h, d, sizeof(T) * n, cudaMemcpyDeviceToHost, st));
+    DCRF_CUDA(cudaStreamSynchronize(st));
+}
+
+void need(const void* p, const char* what) {
+    if (!p) throw Error(DCRF_E_ARG, std::string(what) + " is NULL");
+}
+
+dcrf::Model& M(dcrf_model h) {
+    if (!h || !h->m) throw Error(DCRF_E_ARG, "invalid model handle");
+    return *h->m;
+}
+
+void check_term(dcrf::Model& m, int k) {
+    if (k < 0 || k >= (int)m.terms.size()) throw Error(DCRF_E_ARG, "pairwise term index out of range");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dcrf_last_error(void) { return g_err.c_str(); }
+const char* dcrf_version(void) { return "dcrf-b200 0.1 (sm_100a)"; }
+
+void dcrf_lp_params_default(dcrf_lp_params* p) {
+    if (!p) return;
+    p->prox_reg_const = 1e-2f;
+    p->dual_gap_tol = 1e3f;
+    p->prox_energy_tol = 1e3f;
+    p->prox_max_iter = 10;
+    p->fw_max_iter = 10;
+    p->qp_max_iter = 1000;
+    p->qp_tol = 1e3f;
+    p->qp_const = 1e-16f;
+    p->best_int = 1;
+    p->accel_prox = 1;
+    p->work_set_size = 10;
+    p->approx_fw_iter = 10;
+    p->less_confident_percent = 0.0f;
+    p->confidence_tol = 0.95f;
+}
+
+// ------------------------------------------------------------- lattice --
+dcrf_status dcrf_lattice_create(dcrf_lattice* out) {
+    return guard([&] {
+        need(out, "out");
+        check_device();
+        auto* h = new dcrf_lattice_s();
+        cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            delete h;
+            throw Error(DCRF_E_CUDA, cudaGetErrorString(e));
+        }
+        h->lat.stream = h->stream;
+        *out = h;
+    });
+}
+
+dcrf_status dcrf_lattice_destroy(dcrf_lattice h) {
+    return guard([&] {
+        if (!h) return;
+        cudaStreamSynchronize(h->stream);
+        cudaStream_t st = h->stream;
+        delete h;
+        cudaStreamDestroy(st);
+    });
+}
+
+dcrf_status dcrf_lattice_init_dev(dcrf_lattice h, const float* d_features, int d, int N) {
+    return guard([&] {
+        need(h, "lattice");
+        need(d_features, "features");
+        h->lat.build(d_features, d, N);
+    });
+}
+
+dcrf_status dcrf_lattice_init(dcrf_lattice h, const float* features, int d, int N) {
+    return guard([&] {
+        need(h, "lattice");
+        need(features, "features");
+        if (d < 1 || N < 1) throw Error(DCRF_E_ARG, "invalid feature shape");
+        const float* df = upload(h->feat, features, (size_t)d * N, h->stream);
+        h->lat.build(df, d, N);
+        DCRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
+dcrf_status dcrf_lattice_info(dcrf_lattice h, int* M, int* N, int* d) {
+    return guard([&] {
+        need(h, "lattice");
+        if (M) *M = h->lat.M;
+        if (N) *N = h->lat.N;
+        if (d) *d = h->lat.d;
+    });
+}
+
+dcrf_status dcrf_lattice_compute_dev(dcrf_lattice h, float* d_out, const float* d_in, int L, int reverse) {
+    return guard([&] {
+        need(h, "lattice");
+        need(d_out, "out");
+        need(d_in, "in");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        dcrf::SliceEpilogue ep;
+        h->lat.compute(d_out, d_in, L, reverse != 0, ep);
+    });
+}
+
+dcrf_status dcrf_lattice_compute(dcrf_lattice h, float* out, const float* in, int L, int reverse) {
+    return guard([&] {
+        need(h, "lattice");
+        need(out, "out");
+        need(in, "in");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        if (L < 1) throw Error(DCRF_E_ARG, "L must be >= 1");
+        const size_t n = (size_t)L * h->lat.N;
+        float* di = upload(h->in, in, n, h->stream);
+        float* dout = h->out.ensure(n);
+        dcrf::SliceEpilogue ep;
+        h->lat.compute(dout, di, L, reverse != 0, ep);
+        download(out, dout, n, h->stream);
+    });
+}
+
+dcrf_status dcrf_lattice_compute_ord_dev(dcrf_lattice h, float* d_out, const float* d_Q, int L) {
+    return guard([&] {
+        need(h, "lattice");
+        need(d_out, "out");
+        need(d_Q, "Q");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        dcrf::SliceEpilogue ep;
+        h->lat.compute_ord(d_out, d_Q, L, ep);
+    });
+}
+
+dcrf_status dcrf_lattice_compute_ord(dcrf_lattice h, float* out, const float* Q, int L) {
+    return guard([&] {
+        need(h, "lattice");
+        need(out, "out");
+        need(Q, "Q");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        if (L < 1) throw Error(DCRF_E_ARG, "L must be >= 1");
+        const size_t n = (size_t)L * h->lat.N;
+        for (size_t i = 0; i < n; i++)  // the reference asserts 0 <= Q <= 1 here
+            if (!(Q[i] >= 0.0f && Q[i] <= 1.0f)) throw Error(DCRF_E_RANGE, "Value out of bounds");
+        float* dq = upload(h->in, Q, n, h->stream);
+        float* dout = h->out.ensure(n);
+        dcrf::SliceEpilogue ep;
+        h->lat.compute_ord(dout, dq, L, ep);
+        download(out, dout, n, h->stream);
+    });
+}
+
+dcrf_status dcrf_lattice_export(dcrf_lattice h, int32_t* offset, int32_t* rank, float* bary, int16_t* keys,
+                                int32_t* nbr) {
+    return guard([&] {
+        need(h, "lattice");
+        dcrf::Lattice& L = h->lat;
+        if (L.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        const size_t E = (size_t)L.N * (L.d + 1);
+        cudaStream_t st = h->stream;
+        if (offset) download(offset, L.offset.get(), E, st);
+        if (rank) download(rank, L.rank.get(), E, st);
+        if (bary) download(bary, L.bary.get(), E, st);
+        if (keys && L.M) download(keys, L.vkeys.get(), (size_t)L.M * L.d, st);
+        if (nbr && L.M) {
+            const size_t n = (size_t)(L.d + 1) * L.M;
+            download(reinterpret_cast<int2*>(nbr), L.nbr.get(), n, st);
+            for (size_t i = 0; i < 2 * n; i++) nbr[i] -= 1;  // stored shifted by one
+        }
+    });
+}
+
+dcrf_status dcrf_lattice_stream(dcrf_lattice h, void** stream) {
+    return guard([&] {
+        need(h, "lattice");
+        need(stream, "stream");
+        *stream = (void*)h->stream;
+    });
+}
+
+// --------------------------------------------------------------- model --
+dcrf_status dcrf_model_create(dcrf_model* out, int W, int H, int L) {
+    return guard([&] {
+        need(out, "out");
+        if (W < 1 || H < 1 || L < 1 || L > 64 || (long long)W * H * L >= (1LL << 31))
+            throw Error(DCRF_E_ARG, "invalid model size (W, H >= 1; 1 <= L <= 64; W*H*L < 2^31)");
+        check_device();
+        auto* h = new dcrf_model_s();
+        try {
+            h->m = new dcrf::Model(W, H, L);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+dcrf_status dcrf_model_destroy(dcrf_model h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->m;
+        delete h;
+    });
+}
+
+dcrf_status dcrf_model_set_unary_dev(dcrf_model h, const float* d_unary) {
+    return guard([&] {
+        auto& m = M(h);
+        need(d_unary, "unary");
+        float* u = m.unary.ensure((size_t)m.N * m.L);
+        DCRF_CUDA(cudaMemcpyAsync(u, d_unary, sizeof(float) * m.N * m.L, cudaMemcpyDeviceToDevice, m.stream));
+        m.has_unary = true;
+    });
+}
+
+dcrf_status dcrf_model_set_unary(dcrf_model h, const float* unary) {
+    return guard([&] {
+        auto& m = M(h);
+        need(unary, "unary");
+        upload(m.unary, unary, (size_t)m.N * m.L, m.stream);
+        m.has_unary = true;
+        m.sync();
+    });
+}
+
+dcrf_status dcrf_model_add_pairwise(dcrf_model h, const float* features, int d, float w_potts) {
+    return guard([&] {
+        auto& m = M(h);
+        need(features, "features");
+        if (d < 1 || d > 16) throw Error(DCRF_E_ARG, "feature dimension must be in [1, 16]");
+        const float* df = upload(h->feat, features, (size_t)d * m.N, m.stream);
+        m.add_term(df, d, w_potts);
+        m.sync();
+    });
+}
+
+dcrf_status dcrf_model_add_gaussian(dcrf_model h, float sx, float sy, float w_potts) {
+    return guard([&] {
+        auto& m = M(h);
+        std::vector<float> f((size_t)2 * m.N);
+        for (int j = 0; j < m.H; j++)
+            for (int i = 0; i < m.W; i++) {
+                f[2 * ((size_t)j * m.W + i)] = i / sx;
+                f[2 * ((size_t)j * m.W + i) + 1] = j / sy;
+            }
+        const float* df = upload(h->feat, f.data(), f.size(), m.stream);
+        m.add_term(df, 2, w_potts);
+        m.sync();
+    });
+}
+
+dcrf_status dcrf_model_add_bilateral(dcrf_model h, float sx, float sy, float sr, float sg, float sb,
+                                     const uint8_t* rgb, float w_potts) {
+    return guard([&] {
+        auto& m = M(h);
+        need(rgb, "rgb");
+        std::vector<float> f((size_t)5 * m.N);
+        for (int j = 0; j < m.H; j++)
+            for (int i = 0; i < m.W; i++) {
+                const size_t p = (size_t)j * m.W + i;
+                f[5 * p] = i / sx;
+                f[5 * p + 1] = j / sy;
+                f[5 * p + 2] = rgb[3 * p] / sr;
+                f[5 * p + 3] = rgb[3 * p + 1] / sg;
+                f[5 * p + 4] = rgb[3 * p + 2] / sb;
+            }
+        const float* df = upload(h->feat, f.data(), f.size(), m.stream);
+        m.add_term(df, 5, w_potts);
+        m.sync();
+    });
+}
+
+dcrf_status dcrf_model_set_cliques(dcrf_model h, int R, const int32_t* offsets, const int32_t* idx,
+                                   const float* exp_weight, const float* constants) {
+    return guard([&] {
+        auto& m = M(h);
+        if (R < 0) throw Error(DCRF_E_ARG, "R must be >= 0");
+        if (R > 0) {
+            need(offsets, "offsets");
+            need(exp_weight, "exp_weight");
+            need(constants, "constants");
+            if (offsets[0] != 0) throw Error(DCRF_E_ARG, "offsets[0] must be 0");
+            for (int r = 0; r < R; r++) {
+                const int sz = offsets[r + 1] - offsets[r];
+                if (sz < 1) throw Error(DCRF_E_ARG, "every clique needs at least one pixel");
+                if (sz > m.N) throw Error(DCRF_E_ARG, "clique larger than the image");
+            }
+            if (offsets[R] > 0) need(idx, "idx");
+            for (int p = 0; p < offsets[R]; p++)
+                if (idx[p] < 0 || idx[p] >= m.N) throw Error(DCRF_E_ARG, "clique pixel index out of range");
+        }
+        static const int zero = 0;
+        m.set_cliques(R, R > 0 ? offsets : &zero, idx, exp_weight, constants);
+    });
+}
+
+dcrf_status dcrf_model_unary_init(dcrf_model h, float* Q) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        const size_t n = (size_t)m.N * m.L;
+        float* d = h->io0.ensure(n);
+        m.unary_init(d);
+        download(Q, d, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply_dev(dcrf_model h, int k, int nonorm, float* d_out, const float* d_in) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(d_out, "out");
+        need(d_in, "in");
+        m.apply(k, nonorm != 0, d_out, d_in);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply(dcrf_model h, int k, int nonorm, float* out, const float* in) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(out, "out");
+        need(in, "in");
+        const size_t n = (size_t)m.N * m.L;
+        float* di = upload(h->io0, in, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        m.apply(k, nonorm != 0, dout, di);
+        download(out, dout, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply_ord(dcrf_model h, int k, float* out, const float* Q) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(out, "out");
+        need(Q, "Q");
+        const size_t n = (size_t)m.N * m.L;
+        float* dq = upload(h->io0, Q, n, m.stream);
+        m.check_unit_range(dq);
+        float* dout = h->io1.ensure(n);
+        m.apply_ord(k, dout, dq);
+        download(out, dout, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_qp_dev(dcrf_model h, const float* d_init, float* d_out, const dcrf_qp_params* params,
+                              dcrf_solve_stats* stats) {
+    return guard([&] {
+        auto& m = M(h);
+        need(d_init, "init");
+        need(d_out, "out");
+        const int max_iter = params ? params->max_iter : 0;
+        if (max_iter < 0) throw Error(DCRF_E_ARG, "max_iter must be >= 0");
+        double e = 0.0;
+        int it = m.qp(d_init, d_out, max_iter, &e);
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->iterations = it;
+            stats->energy = e;
+        }
+    });
+}
+
+dcrf_status dcrf_model_qp(dcrf_model h, const float* init, float* out, const dcrf_qp_params* params,
+                          dcrf_solve_stats* stats) {
+    return guard([&] {
+        auto& m = M(h);
+        need(init, "init");
+        need(out, "out");
+        const size_t n = (size_t)m.N * m.L;
+        float* di = upload(h->io0, init, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        const int max_iter = params ? params->max_iter : 0;
+        if (max_iter < 0) throw Error(DCRF_E_ARG, "max_iter must be >= 0");
+        double e = 0.0;
+        int it = m.qp(di, dout, max_iter, &e);
+        download(out, dout, n, m.stream);
+        if (stats) {
+            std::memset(stats, 0, sizeof(*stats));
+            stats->iterations = it;
+            stats->energy = e;
+        }
+    });
+}
+
+static void check_lp_params(const dcrf_lp_params& p) {
+    if (p.prox_max_iter < 1 || p.fw_max_iter < 1 || p.qp_max_iter < 1)
+        throw Error(DCRF_E_ARG, "LP iteration counts must be >= 1");
+}
+
+dcrf_status dcrf_model_lp_dev(dcrf_model h, const float* d_init, float* d_out, const dcrf_lp_params* params,
+                              dcrf_solve_stats* stats) {
+    return guard([&] {
+        auto& m = M(h);
+        need(d_init, "init");
+        need(d_out, "out");
+        dcrf_lp_params p;
+        if (params) p = *params;
+        else dcrf_lp_params_default(&p);
+        check_lp_params(p);
+        dcrf_solve_stats s{};
+        m.lp(d_init, d_out, p, &s);
+        if (stats) *stats = s;
+    });
+}
+
+dcrf_status dcrf_model_lp(dcrf_model h, const float* init, float* out, const dcrf_lp_params* params,
+                          dcrf_solve_stats* stats) {
+    return guard([&] {
+        auto& m = M(h);
+        need(init, "init");
+        need(out, "out");
+        dcrf_lp_params p;
+        if (params) p = *params;
+        else dcrf_lp_params_default(&p);
+        check_lp_params(p);
+        const size_t n = (size_t)m.N * m.L;
+        float* di = upload(h->io0, init, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        dcrf_solve_stats s{};
+        m.lp(di, dout, p, &s);
+        download(out, dout, n, m.stream);
+        if (stats) *stats = s;
+    });
+}
+
+dcrf_status dcrf_model_current_map(dcrf_model h, const float* Q, int16_t* labels) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        need(labels, "labels");
+        float* dq = upload(h->io0, Q, (size_t)m.N * m.L, m.stream);
+        int16_t* dl = h->lab.ensure(m.N);
+        m.current_map(dq, dl);
+        download(labels, dl, m.N, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_energy_true(dcrf_model h, const int16_t* labels, double* energy) {
+    return guard([&] {
+        auto& m = M(h);
+        need(labels, "labels");
+        need(energy, "energy");
+        int16_t* dl = upload(h->lab, labels, m.N, m.stream);
+        *energy = m.energy_true(dl, false);
+    });
+}
+
+dcrf_status dcrf_model_energy_ho(dcrf_model h, const int16_t* labels, double* energy) {
+    return guard([&] {
+        auto& m = M(h);
+        need(labels, "labels");
+        need(energy, "energy");
+        int16_t* dl = upload(h->lab, labels, m.N, m.stream);
+        *energy = m.energy_true(dl, true);
+    });
+}
+
+dcrf_status dcrf_model_energy_lp(dcrf_model h, const float* Q, double* energy) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        need(energy, "energy");
+        float* dq = upload(h->io0, Q, (size_t)m.N * m.L, m.stream);
+        *energy = m.energy_lp(dq);
+    });
+}
+
+dcrf_status dcrf_model_lr_qp_value(dcrf_model h, const float* Q, double* energy) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        need(energy, "energy");
+        float* dq = upload(h->io0, Q, (size_t)m.N * m.L, m.stream);
+        *energy = m.lr_qp_value(dq);
+    });
+}
+
+dcrf_status dcrf_model_info(dcrf_model h, int* n_terms, int* N, int* L) {
+    return guard([&] {
+        auto& m = M(h);
+        if (n_terms) *n_terms = (int)m.terms.size();
+        if (N) *N = m.N;
+        if (L) *L = m.L;
+    });
+}
+
+dcrf_status dcrf_model_lattice_size(dcrf_model h, int k, int* Mv) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(Mv, "M");
+        *Mv = m.terms[k]->lat->M;
+    });
+}
+
+dcrf_status dcrf_model_stream(dcrf_model h, void** stream) {
+    return guard([&] {
+        auto& m = M(h);
+        need(stream, "stream");
+        *stream = (void*)m.stream;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+// Shared helpers of libdcrf_cuda: status plumbing, device buffers, and the
+// exact-rounding arithmetic the reference's SSE2 build performs.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+#include "dcrf.h"
+
+namespace dcrf {
+
+// Thrown inside the library, converted to a dcrf_status at the C boundary.
+struct Error : public std::runtime_error {
+    dcrf_status code;
+    Error(dcrf_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define DCRF_CUDA(call)                                                              \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess)                                                       \
+            throw ::dcrf::Error(e_ == cudaErrorMemoryAllocation ? DCRF_E_NOMEM       \
+                                                                : DCRF_E_CUDA,       \
+                                std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define DCRF_LAUNCH_CHECK() DCRF_CUDA(cudaGetLastError())
+
+inline void require(bool ok, dcrf_status code, const std::string& msg) {
+    if (!ok) throw Error(code, msg);
+}
+
+// Owning device allocation; grows, never shrinks.
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    T* ensure(size_t count) {
+        if (count > n) {
+            release();
+            DCRF_CUDA(cudaMalloc(&p, (count ? count : 1) * sizeof(T)));
+            n = count;
+        }
+        return p;
+    }
+    T* get() const { return p; }
+};
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Number of SMs of the current device (cached per process; one device per
+// process is the supported deployment).
+int sm_count();
+
+// ------------------------------------------------------------------------
+// Exact float arithmetic.  The reference is compiled for x86-64 SSE2, which
+// has no fused multiply-add; every product and sum is rounded separately to
+// nearest-even.  These wrappers keep nvcc from contracting them (the library
+// is additionally built with -fmad=false).
+// ------------------------------------------------------------------------
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+
+}  // namespace dcrf

@@ -1,0 +1,616 @@
+// Permutohedral lattice construction and filtering on sm_100a.
+//
+// Construction reproduces Permutohedral::init's SSE path
+// (src/permutohedral.cpp:152-333) bit for bit:
+//   K1 elevate   one thread per pixel: elevation, rounding to the nearest
+//                0-coloured vertex (round-to-nearest-even, as _mm_cvtps_epi32
+//                does), rank, barycentric weights and the d+1 vertex keys;
+//                the pixel count is padded to a multiple of 4 with zero
+//                features, like the reference's last SSE block.
+//   K2 insert    open-addressing hash insert of every (pixel, remainder)
+//                entry; each slot ends up holding the SMALLEST entry index
+//                with its key (atomicMin), i.e. the key's first occurrence.
+//   K3 compact   vertex id = rank of the first occurrence among all first
+//                occurrences (flag + exclusive scan) -- exactly the
+//                insertion order HashTable::find produces (:100-128).
+//   K4 neighbours  per (axis, vertex) lookup of key -1/+d and key +1/-d
+//                (:316-330).
+//   K5 splat lists  stable radix sort of entries by vertex id.
+// Filtering reproduces sseCompute (L > 2) / seqCompute (L <= 2)
+// (src/permutohedral.cpp:998-1058 / 488-540) and the 10-bin ordered filter
+// (:548-701) with the same per-element operation order, so results are
+// identical to the reference, with no float atomics.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "lattice.cuh"
+
+namespace dcrf {
+
+namespace {
+
+constexpr int kEmpty = -1;
+constexpr int kRes = 10;       // RESOLUTION (include/permutohedral.h:41)
+constexpr int kOrdW = 2 * kRes;  // lower + upper bins per (vertex, label)
+
+template <int KW>
+struct Key {
+    int4 w[KW];
+};
+
+template <int KW>
+__device__ __forceinline__ Key<KW> load_key(const int4* __restrict__ k, long e) {
+    Key<KW> r;
+#pragma unroll
+    for (int i = 0; i < KW; i++) r.w[i] = __ldg(k + e * KW + i);
+    return r;
+}
+
+template <int KW>
+__device__ __forceinline__ bool key_eq(const Key<KW>& a, const Key<KW>& b) {
+    bool eq = true;
+#pragma unroll
+    for (int i = 0; i < KW; i++)
+        eq &= (a.w[i].x == b.w[i].x) & (a.w[i].y == b.w[i].y) & (a.w[i].z == b.w[i].z) &
+              (a.w[i].w == b.w[i].w);
+    return eq;
+}
+
+__device__ __forceinline__ uint32_t mix32(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+template <int KW>
+__device__ __forceinline__ uint32_t key_hash(const Key<KW>& k) {
+    uint32_t h = 0x9e3779b9u;
+#pragma unroll
+    for (int i = 0; i < KW; i++) {
+        h = mix32(h ^ (uint32_t)k.w[i].x);
+        h = mix32(h ^ (uint32_t)k.w[i].y);
+        h = mix32(h ^ (uint32_t)k.w[i].z);
+        h = mix32(h ^ (uint32_t)k.w[i].w);
+    }
+    return h;
+}
+
+template <int KW>
+__device__ __forceinline__ void key_set(Key<KW>& k, int c, int16_t v) {
+    int* words = reinterpret_cast<int*>(k.w);
+    int wi = c >> 1;
+    uint32_t u = (uint32_t)words[wi];
+    if (c & 1) u = (u & 0x0000ffffu) | ((uint32_t)(uint16_t)v << 16);
+    else u = (u & 0xffff0000u) | (uint32_t)(uint16_t)v;
+    words[wi] = (int)u;
+}
+
+template <int KW>
+__device__ __forceinline__ int16_t key_get(const Key<KW>& k, int c) {
+    const int* words = reinterpret_cast<const int*>(k.w);
+    uint32_t u = (uint32_t)words[c >> 1];
+    return (int16_t)(uint16_t)((c & 1) ? (u >> 16) : (u & 0xffffu));
+}
+
+template <int KW>
+__device__ __forceinline__ void key_zero(Key<KW>& k) {
+#pragma unroll
+    for (int i = 0; i < KW; i++) k.w[i] = make_int4(0, 0, 0, 0);
+}
+
+// _mm_cvtps_epi32 (round to nearest even; out-of-range -> INT_MIN) and back.
+__device__ __forceinline__ float cvt_rne(float v) {
+    if (!(fabsf(v) < 2147483648.0f)) return -2147483648.0f;
+    return (float)__float2int_rn(v);
+}
+
+// K1: one thread per (padded) pixel.
+template <int DM>
+__global__ void elevate_kernel(const float* __restrict__ feat, int N, int Np, int d,
+                               const float* __restrict__ scale, int4* __restrict__ ekeys,
+                               int* __restrict__ rank_out, float* __restrict__ bary_out) {
+    constexpr int KW = (DM + 7) / 8;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= Np) return;
+    const int d1 = d + 1;
+    const float invdp1 = 1.0f / (float)d1, dp1 = (float)d1;
+    float f[DM], el[DM + 1], rem0[DM + 1], rk[DM + 1], b[DM + 2];
+    for (int j = 0; j < d; j++) f[j] = k < N ? feat[(long)k * d + j] : 0.0f;
+    // Elevation (:213-219): sm accumulates from the last coordinate down.
+    float sm = 0.0f;
+    for (int j = d; j > 0; j--) {
+        float cf = fmul(f[j - 1], scale[j - 1]);
+        el[j] = fsub(sm, fmul((float)j, cf));
+        sm = fadd(sm, cf);
+    }
+    el[0] = sm;
+    // Closest 0-coloured simplex (:222-232).
+    float sum = 0.0f;
+    for (int i = 0; i <= d; i++) {
+        float v = cvt_rne(fmul(invdp1, el[i]));
+        rem0[i] = fmul(v, dp1);
+        sum = fadd(sum, v);
+    }
+    // Rank (:235-245).
+    for (int i = 0; i <= d; i++) rk[i] = 0.0f;
+    for (int i = 0; i < d; i++) {
+        float di = fsub(el[i], rem0[i]);
+        for (int j = i + 1; j <= d; j++) {
+            float dj = fsub(el[j], rem0[j]);
+            float c = (di < dj) ? 1.0f : 0.0f;
+            rk[i] = fadd(rk[i], c);
+            rk[j] = fadd(rk[j], fsub(1.0f, c));
+        }
+    }
+    // Back onto the plane (:248-254).
+    for (int i = 0; i <= d; i++) {
+        rk[i] = fadd(rk[i], sum);
+        float add = rk[i] < 0.0f ? dp1 : 0.0f;
+        float sub = rk[i] >= dp1 ? dp1 : 0.0f;
+        float t = fsub(add, sub);
+        rk[i] = fadd(rk[i], t);
+        rem0[i] = fadd(rem0[i], t);
+    }
+    // Barycentric coordinates (:257-275).
+    for (int i = 0; i < d + 2; i++) b[i] = 0.0f;
+    for (int i = 0; i <= d; i++) {
+        float v = fmul(fsub(el[i], rem0[i]), invdp1);
+        int p = (int)fsub((float)d, rk[i]);
+        p = min(max(p, 0), d);  // in range for finite features; guards NaN input
+        b[p] = fadd(b[p], v);
+        b[p + 1] = fsub(b[p + 1], v);
+    }
+    b[0] = fadd(b[0], fadd(1.0f, b[d + 1]));
+    // Keys of the d+1 vertices (:280-287); canonical simplex (:183-188).
+    for (int r = 0; r <= d; r++) {
+        Key<KW> key;
+        key_zero(key);
+        for (int i = 0; i < d; i++) {
+            int ri = (int)rk[i];
+            int canon = (ri <= d - r) ? r : r - d1;
+            key_set(key, i, (int16_t)(int)fadd(rem0[i], (float)canon));
+        }
+        long e = (long)k * d1 + r;
+#pragma unroll
+        for (int w = 0; w < KW; w++) ekeys[e * KW + w] = key.w[w];
+        if (k < N) {
+            rank_out[e] = (int)rk[r];
+            bary_out[e] = b[r];
+        }
+    }
+}
+
+// K2: insert every entry; slots keep the smallest entry index of their key.
+template <int KW>
+__global__ void insert_kernel(const int4* __restrict__ ekeys, int E, int* table, unsigned mask,
+                              int* __restrict__ entry_slot) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const Key<KW> key = load_key<KW>(ekeys, e);
+    unsigned h = key_hash(key) & mask;
+    for (unsigned probe = 0; probe <= mask; probe++) {  // bounded: table is never full
+        int cur = *(volatile int*)(table + h);
+        if (cur == kEmpty) {
+            int old = atomicCAS(table + h, kEmpty, e);
+            if (old == kEmpty) {
+                entry_slot[e] = (int)h;
+                return;
+            }
+            cur = old;
+        }
+        if (key_eq(load_key<KW>(ekeys, cur), key)) {
+            atomicMin(table + h, e);
+            entry_slot[e] = (int)h;
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+}
+
+__global__ void first_flag_kernel(int E, const int* __restrict__ entry_slot,
+                                  const int* __restrict__ table, int* __restrict__ flag) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    flag[e] = table[entry_slot[e]] == e ? 1 : 0;
+}
+
+// K3: vertex ids and vertex keys.
+template <int KW>
+__global__ void finalize_kernel(int E, int Ereal, int d, const int* __restrict__ entry_slot,
+                                const int* __restrict__ table, const int* __restrict__ first_rank,
+                                const int4* __restrict__ ekeys, int* __restrict__ offset,
+                                int16_t* __restrict__ vkeys, int* __restrict__ slot_vid) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    const int s = entry_slot[e];
+    const int f = table[s];
+    const int vid = first_rank[f];
+    if (e < Ereal) offset[e] = vid;
+    if (f == e) {
+        slot_vid[s] = vid;
+        const Key<KW> key = load_key<KW>(ekeys, e);
+        for (int c = 0; c < d; c++) vkeys[(long)vid * d + c] = key_get(key, c);
+    }
+}
+
+template <int KW>
+__device__ __forceinline__ int lookup(const Key<KW>& key, const int* __restrict__ table,
+                                      unsigned mask, const int4* __restrict__ ekeys,
+                                      const int* __restrict__ slot_vid) {
+    unsigned h = key_hash(key) & mask;
+    for (unsigned probe = 0; probe <= mask; probe++) {
+        int cur = table[h];
+        if (cur == kEmpty) return -1;
+        if (key_eq(load_key<KW>(ekeys, cur), key)) return slot_vid[h];
+        h = (h + 1) & mask;
+    }
+    return -1;
+}
+
+// K4: blur neighbours, stored shifted by one (0 = absent).
+template <int KW>
+__global__ void neighbor_kernel(int M, int d, const int16_t* __restrict__ vkeys,
+                                const int* __restrict__ table, unsigned mask,
+                                const int4* __restrict__ ekeys, const int* __restrict__ slot_vid,
+                                int2* __restrict__ nbr) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)(d + 1) * M) return;
+    const int j = (int)(t / M), v = (int)(t - (long)j * M);
+    Key<KW> n1, n2;
+    key_zero(n1);
+    key_zero(n2);
+    for (int c = 0; c < d; c++) {
+        int kc = vkeys[(long)v * d + c];
+        int a = c == j ? kc + d : kc - 1;
+        int bb = c == j ? kc - d : kc + 1;
+        key_set(n1, c, (int16_t)a);
+        key_set(n2, c, (int16_t)bb);
+    }
+    int i1 = lookup(n1, table, mask, ekeys, slot_vid);
+    int i2 = lookup(n2, table, mask, ekeys, slot_vid);
+    nbr[t] = make_int2(i1 + 1, i2 + 1);
+}
+
+__global__ void count_kernel(int E, const int* __restrict__ offset, int* __restrict__ counts) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < E) atomicAdd(counts + offset[e], 1);
+}
+
+__global__ void iota_copy_kernel(int E, const int* __restrict__ offset, int* __restrict__ keys,
+                                 int* __restrict__ vals) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    keys[e] = offset[e];
+    vals[e] = e;
+}
+
+__global__ void seg_fill_kernel(int E, int d1, const int* __restrict__ sorted_entries,
+                                const float* __restrict__ bary, int* __restrict__ seg_pix,
+                                float* __restrict__ seg_w) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= E) return;
+    const int e = sorted_entries[s];
+    seg_pix[s] = e / d1;
+    seg_w[s] = bary[e];
+}
+
+// ------------------------------------------------------------- filter --
+
+// Splat as a gather: value(v, k) = sum over v's entries, in entry order, of
+// w * in[p][k] (times the symmetric normalisation when pre_norm is given,
+// which DenseKernel::filter applies before the lattice, src/pairwise.cpp:61).
+template <bool PRE_NORM>
+__global__ void splat_kernel(int M, int L, const int* __restrict__ seg_start,
+                             const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                             const float* __restrict__ in, const float* __restrict__ norm,
+                             float* __restrict__ vals) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * L) return;
+    const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    float acc = 0.0f;
+    for (int s = s0; s < s1; s++) {
+        const int p = seg_pix[s];
+        float x = in[(long)p * L + k];
+        if (PRE_NORM) x = fmul(x, norm[p]);
+        acc = fadd(acc, fmul(seg_w[s], x));
+    }
+    vals[(long)(v + 1) * L + k] = acc;
+}
+
+// One blur pass along one lattice axis: new = old + 1/2 (n1 + n2).  seqCompute
+// evaluates it in double (0.5 is a double literal there, :518).
+template <bool SEQ>
+__global__ void blur_kernel(int M, int L, const int2* __restrict__ nbr,
+                            const float* __restrict__ src, float* __restrict__ dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * L) return;
+    const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    const int2 nb = nbr[v];
+    const float a = src[(long)(v + 1) * L + k];
+    const float s = fadd(src[(long)nb.x * L + k], src[(long)nb.y * L + k]);
+    float r;
+    if (SEQ) r = (float)dadd((double)a, dmul(0.5, (double)s));
+    else r = fadd(a, fmul(0.5f, s));
+    dst[(long)(v + 1) * L + k] = r;
+}
+
+__device__ __forceinline__ float apply_epilogue(float v, long t, int i, const SliceEpilogue& ep) {
+    if (ep.potts) {
+        if (ep.norm) v = fmul(v, ep.norm[i]);
+        v = fmul(ep.scale, v);
+    }
+    if (ep.base) v = fadd(ep.base[t], fmul(ep.coef, v));
+    else if (ep.zero_base) v = fadd(0.0f, fmul(ep.coef, v));
+    return v;
+}
+
+// Slice: out(i, k) = sum_j (bary_ij * alpha) * value(o_ij, k) (sseCompute,
+// :1046-1051) or sum_j (bary_ij * value) * alpha (seqCompute, :529-534).
+template <bool SEQ>
+__global__ void slice_kernel(int N, int L, int d, const int* __restrict__ offset,
+                             const float* __restrict__ bary, const float* __restrict__ vals,
+                             float alpha, float* out, SliceEpilogue ep) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)N * L) return;
+    const int i = (int)(t / L), k = (int)(t - (long)i * L);
+    const int d1 = d + 1;
+    float acc = 0.0f;
+    for (int j = 0; j <= d; j++) {
+        const int o = offset[(long)i * d1 + j];
+        const float w = bary[(long)i * d1 + j];
+        const float v = vals[(long)(o + 1) * L + k];
+        if (SEQ) acc = fadd(acc, fmul(fmul(w, v), alpha));
+        else acc = fadd(acc, fmul(fmul(w, alpha), v));
+    }
+    out[t] = apply_epilogue(acc, t, i, ep);
+}
+
+// addSplitArray / sliceSplitArray bins (:548-589): the lower pass rounds
+// q*10 in float, the upper pass (q - 1e-9)*10 in double.
+// For q in [0, 1] these are the reference's indices; other values (which the
+// reference rejects with an assert) are clamped to a valid bin so no access
+// can leave the bin array.
+__device__ __forceinline__ int bin_lower(float q) {
+    int c = (int)floorf(fmul(q, (float)kRes));
+    c = c < kRes - 1 ? c : kRes - 1;
+    return c > 0 ? c : 0;
+}
+__device__ __forceinline__ int bin_upper(float q) {
+    int c = (int)floor(dmul(__dsub_rn((double)q, 1e-9), (double)kRes));
+    c = c > 0 ? c : 0;
+    return c < kRes - 1 ? c : kRes - 1;
+}
+
+// Ordered splat, both passes at once: bins [0,10) lower, [10,20) upper.
+__global__ void ord_splat_kernel(int M, int L, const int* __restrict__ seg_start,
+                                 const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                                 const float* __restrict__ Q, float* __restrict__ vals) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * L) return;
+    const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    float lo[kRes], up[kRes];
+#pragma unroll
+    for (int b = 0; b < kRes; b++) lo[b] = up[b] = 0.0f;
+    for (int s = s0; s < s1; s++) {
+        const int p = seg_pix[s];
+        const float w = seg_w[s];
+        const float q = Q[(long)p * L + k];
+        const int cl = bin_lower(q), cu = bin_upper(q);
+#pragma unroll
+        for (int b = 0; b < kRes; b++) {
+            if (b <= cl) lo[b] = fadd(lo[b], w);
+            if (b >= cu) up[b] = fadd(up[b], w);
+        }
+    }
+    float4* dst = reinterpret_cast<float4*>(vals + ((long)(v + 1) * L + k) * kOrdW);
+    dst[0] = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    dst[1] = make_float4(lo[4], lo[5], lo[6], lo[7]);
+    dst[2] = make_float4(lo[8], lo[9], up[0], up[1]);
+    dst[3] = make_float4(up[2], up[3], up[4], up[5]);
+    dst[4] = make_float4(up[6], up[7], up[8], up[9]);
+}
+
+// Ordered blur: every bin independently, weightedAddSplitArray (:570-578).
+__global__ void ord_blur_kernel(int M, int row4, const int2* __restrict__ nbr,
+                                const float4* __restrict__ src, float4* __restrict__ dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * row4) return;
+    const int v = (int)(t / row4), c = (int)(t - (long)v * row4);
+    const int2 nb = nbr[v];
+    const float4 a = src[(long)(v + 1) * row4 + c];
+    const float4 p = src[(long)nb.x * row4 + c];
+    const float4 q = src[(long)nb.y * row4 + c];
+    float4 r;
+    r.x = fadd(a.x, fmul(0.5f, fadd(p.x, q.x)));
+    r.y = fadd(a.y, fmul(0.5f, fadd(p.y, q.y)));
+    r.z = fadd(a.z, fmul(0.5f, fadd(p.z, q.z)));
+    r.w = fadd(a.w, fmul(0.5f, fadd(p.w, q.w)));
+    dst[(long)(v + 1) * row4 + c] = r;
+}
+
+// Ordered slice: lower pass with weight -w*alpha, then upper with w*alpha
+// (:639-650, :687-696), accumulated into one value.
+__global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ offset,
+                                 const float* __restrict__ bary, const float* __restrict__ vals,
+                                 const float* __restrict__ Q, float alpha, float* out,
+                                 SliceEpilogue ep) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)N * L) return;
+    const int i = (int)(t / L), k = (int)(t - (long)i * L);
+    const int d1 = d + 1;
+    const float q = Q[t];
+    const int cl = bin_lower(q), cu = bin_upper(q);
+    float acc = 0.0f;
+    for (int j = 0; j <= d; j++) {
+        const int o = offset[(long)i * d1 + j];
+        const float w = bary[(long)i * d1 + j];
+        acc = fadd(acc, fmul(vals[((long)(o + 1) * L + k) * kOrdW + cl], fmul(-w, alpha)));
+    }
+    for (int j = 0; j <= d; j++) {
+        const int o = offset[(long)i * d1 + j];
+        const float w = bary[(long)i * d1 + j];
+        acc = fadd(acc, fmul(vals[((long)(o + 1) * L + k) * kOrdW + kRes + cu], fmul(w, alpha)));
+    }
+    out[t] = apply_epilogue(acc, t, i, ep);
+}
+
+int bits_for(int n) {  // bits needed to hold values 0..n-1
+    int b = 0;
+    while ((1LL << b) < (long long)n) b++;
+    return b;
+}
+
+constexpr int kTB = 256;
+
+template <int DM>
+void build_impl(Lattice& L, const float* d_features) {
+    constexpr int KW = (DM + 7) / 8;
+    cudaStream_t st = L.stream;
+    const int N = L.N, d = L.d, d1 = d + 1;
+    const int Np = (N + 3) & ~3;
+    const long E = (long)Np * d1, Ereal = (long)N * d1;
+    require(E < (1L << 30), DCRF_E_ARG, "lattice too large (N*(d+1) >= 2^30)");
+
+    // scale_factor (:190-194): computed in double, rounded to float.
+    std::vector<float> scale(d);
+    const float inv_std_dev = (float)(std::sqrt(2.0 / 3.0) * (d + 1));
+    for (int i = 0; i < d; i++) scale[i] = (float)(1.0 / std::sqrt((double)((i + 2) * (i + 1))) * inv_std_dev);
+    float* dscale = L.fscale.ensure(d);
+    DCRF_CUDA(cudaMemcpyAsync(dscale, scale.data(), sizeof(float) * d, cudaMemcpyHostToDevice, st));
+
+    int4* ekeys = L.ekeys.ensure((size_t)E * KW);
+    int* rank = L.rank.ensure(Ereal);
+    float* bary = L.bary.ensure(Ereal);
+    elevate_kernel<DM><<<ceil_div(Np, kTB), kTB, 0, st>>>(d_features, N, Np, d, dscale, ekeys, rank, bary);
+    DCRF_LAUNCH_CHECK();
+
+    unsigned cap = 1;
+    while ((long)cap < 2 * E) cap <<= 1;
+    int* table = L.table.ensure(cap);
+    DCRF_CUDA(cudaMemsetAsync(table, 0xff, sizeof(int) * cap, st));
+    int* eslot = L.entry_slot.ensure(E);
+    insert_kernel<KW><<<ceil_div(E, kTB), kTB, 0, st>>>(ekeys, (int)E, table, cap - 1, eslot);
+    int* flags = L.flags.ensure(E);
+    first_flag_kernel<<<ceil_div(E, kTB), kTB, 0, st>>>((int)E, eslot, table, flags);
+    DCRF_LAUNCH_CHECK();
+    int* dtotal = L.total.ensure(1);
+    exclusive_scan(flags, flags, (int)E, dtotal, L.scan, st);
+    int M = 0;
+    DCRF_CUDA(cudaMemcpyAsync(&M, dtotal, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCRF_CUDA(cudaStreamSynchronize(st));
+    L.M = M;
+
+    int* offset = L.offset.ensure(Ereal);
+    int16_t* vkeys = L.vkeys.ensure((size_t)M * d);
+    int* slot_vid = L.slot_vid.ensure(cap);
+    finalize_kernel<KW><<<ceil_div(E, kTB), kTB, 0, st>>>((int)E, (int)Ereal, d, eslot, table, flags,
+                                                         ekeys, offset, vkeys, slot_vid);
+    int2* nbr = L.nbr.ensure((size_t)d1 * M);
+    neighbor_kernel<KW><<<ceil_div((long)d1 * M, kTB), kTB, 0, st>>>(M, d, vkeys, table, cap - 1,
+                                                                     ekeys, slot_vid, nbr);
+    DCRF_LAUNCH_CHECK();
+
+    // Splat lists: per-vertex counts -> starts; stable sort of entries by vertex.
+    int* counts = L.counts.ensure((size_t)M + 1);
+    DCRF_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)M + 1), st));
+    count_kernel<<<ceil_div(Ereal, kTB), kTB, 0, st>>>((int)Ereal, offset, counts);
+    int* seg_start = L.seg_start.ensure((size_t)M + 1);
+    exclusive_scan(counts, seg_start, M + 1, nullptr, L.scan, st);
+    int* skeys = L.sort_keys.ensure(Ereal);
+    int* svals = L.sort_vals.ensure(Ereal);
+    iota_copy_kernel<<<ceil_div(Ereal, kTB), kTB, 0, st>>>((int)Ereal, offset, skeys, svals);
+    DCRF_LAUNCH_CHECK();
+    radix_sort_pairs(skeys, svals, (int)Ereal, bits_for(M), L.sort, st);
+    int* seg_pix = L.seg_pix.ensure(Ereal);
+    float* seg_w = L.seg_w.ensure(Ereal);
+    seg_fill_kernel<<<ceil_div(Ereal, kTB), kTB, 0, st>>>((int)Ereal, d1, svals, bary, seg_pix, seg_w);
+    DCRF_LAUNCH_CHECK();
+    L.va_floats = 0;
+}
+
+}  // namespace
+
+void Lattice::build(const float* d_features, int d_, int N_) {
+    require(N_ > 0, DCRF_E_ARG, "lattice: N must be positive");
+    require(d_ >= 1 && d_ <= 16, DCRF_E_ARG, "lattice: feature dimension must be in [1, 16]");
+    N = N_;
+    d = d_;
+    if (d <= 2) build_impl<2>(*this, d_features);
+    else if (d <= 5) build_impl<5>(*this, d_features);
+    else if (d <= 8) build_impl<8>(*this, d_features);
+    else build_impl<16>(*this, d_features);
+}
+
+void Lattice::ensure_values(size_t row_width) {
+    size_t need = (size_t)(M + 1) * row_width;
+    if (need > va_floats) {
+        va.ensure(need);
+        vb.ensure(need);
+        va_floats = need;
+    }
+    // Row 0 is the zero row that absent neighbours read.
+    DCRF_CUDA(cudaMemsetAsync(va.get(), 0, sizeof(float) * row_width, stream));
+    DCRF_CUDA(cudaMemsetAsync(vb.get(), 0, sizeof(float) * row_width, stream));
+}
+
+void Lattice::compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,
+                      const float* pre_norm) {
+    require(L >= 1, DCRF_E_ARG, "compute: L must be >= 1");
+    ensure_values((size_t)L);
+    cudaStream_t st = stream;
+    const long ML = (long)M * L, NL = (long)N * L;
+    float *src = va.get(), *dst = vb.get();
+    if (pre_norm)
+        splat_kernel<true><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, seg_start.get(), seg_pix.get(),
+                                                              seg_w.get(), in, pre_norm, src);
+    else
+        splat_kernel<false><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, seg_start.get(), seg_pix.get(),
+                                                               seg_w.get(), in, nullptr, src);
+    const bool seq = L <= 2;
+    for (int jj = 0; jj <= d; jj++) {
+        const int j = reverse ? d - jj : jj;
+        if (seq)
+            blur_kernel<true><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, nbr.get() + (long)j * M, src, dst);
+        else
+            blur_kernel<false><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, nbr.get() + (long)j * M, src, dst);
+        std::swap(src, dst);
+    }
+    const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
+    if (seq)
+        slice_kernel<true><<<ceil_div(NL, kTB), kTB, 0, st>>>(N, L, d, offset.get(), bary.get(), src,
+                                                              alpha, out, ep);
+    else
+        slice_kernel<false><<<ceil_div(NL, kTB), kTB, 0, st>>>(N, L, d, offset.get(), bary.get(), src,
+                                                               alpha, out, ep);
+    DCRF_LAUNCH_CHECK();
+}
+
+void Lattice::compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep) {
+    require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
+    const size_t row = (size_t)L * kOrdW;
+    ensure_values(row);
+    cudaStream_t st = stream;
+    const long ML = (long)M * L, NL = (long)N * L;
+    float *src = va.get(), *dst = vb.get();
+    ord_splat_kernel<<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, seg_start.get(), seg_pix.get(),
+                                                        seg_w.get(), Q, src);
+    const int row4 = (int)(row / 4);
+    for (int j = 0; j <= d; j++) {
+        ord_blur_kernel<<<ceil_div((long)M * row4, kTB), kTB, 0, st>>>(
+            M, row4, nbr.get() + (long)j * M, reinterpret_cast<const float4*>(src),
+            reinterpret_cast<float4*>(dst));
+        std::swap(src, dst);
+    }
+    const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
+    ord_slice_kernel<<<ceil_div(NL, kTB), kTB, 0, st>>>(N, L, d, offset.get(), bary.get(), src, Q,
+                                                        alpha, out, ep);
+    DCRF_LAUNCH_CHECK();
+}
+
+}  // namespace dcrf

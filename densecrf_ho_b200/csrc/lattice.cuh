@@ -1,0 +1,61 @@
+// Device-resident permutohedral lattice: construction and filtering.
+//
+// Layout in HBM (all arrays are owned by the Lattice):
+//   offset[N*(d+1)], bary[N*(d+1)], rank[N*(d+1)]  pixel-major, as the
+//       reference's offset_ / barycentric_ / rank_ (src/permutohedral.cpp:166-170)
+//   vkeys[M*d]      int16 key of each vertex, vertex ids = first-occurrence order
+//   nbr[(d+1)*M]    int2 (n1+1, n2+1): blur neighbours of each vertex per axis,
+//                   shifted by one so that row 0 of a value buffer is the zero
+//                   row standing in for "absent" (src/permutohedral.cpp:490-516)
+//   seg_start[M+1], seg_pix[E], seg_w[E]   splat lists: for each vertex the
+//                   (pixel, weight) pairs that touch it, in increasing
+//                   (pixel, remainder) order, E = N*(d+1).  Splatting then
+//                   gathers in exactly the order in which the reference's
+//                   scatter accumulates, without float atomics.
+//   value buffers   [(M+1)][L] floats (ordered filter: [(M+1)][L][20]).
+#pragma once
+#include "common.cuh"
+#include "primitives.cuh"
+
+namespace dcrf {
+
+// What the slice kernel does with the filtered value v of (pixel i, label k).
+struct SliceEpilogue {
+    const float* norm = nullptr;  // multiply by norm[i] (symmetric normalisation)
+    float scale = 1.0f;           // then by this (Potts: -w); exactly 1 = skip
+    bool potts = false;           // apply norm / scale at all
+    const float* base = nullptr;  // then out = base[...] + coef * v
+    float coef = 1.0f;
+    bool zero_base = false;       // out = 0.0f + coef * v  (Eigen fill(0); +=)
+};
+
+struct Lattice {
+    int N = 0, d = 0, M = 0;
+    cudaStream_t stream = nullptr;  // borrowed
+
+    DevBuf<int> offset, rank, seg_start, seg_pix;
+    DevBuf<float> bary, seg_w;
+    DevBuf<int16_t> vkeys;
+    DevBuf<int2> nbr;
+    DevBuf<float> va, vb;    // filter value buffers
+    size_t va_floats = 0;    // rows (M+1) * width currently zero-headed
+
+    // build scratch
+    DevBuf<int4> ekeys;
+    DevBuf<int> table, entry_slot, flags, slot_vid, sort_keys, sort_vals, counts, total;
+    DevBuf<float> fscale;
+    ScanScratch scan;
+    SortScratch sort;
+
+    // features: device [N][d]
+    void build(const float* d_features, int d_, int N_);
+    // out/in: device [N][L]; out may alias in.
+    void compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,
+                 const float* pre_norm = nullptr);
+    // Ordered (upper minus lower, 10-bin) filter of Q in [0,1]; out = epilogue(v).
+    void compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep);
+
+    void ensure_values(size_t row_width);
+};
+
+}  // namespace dcrf

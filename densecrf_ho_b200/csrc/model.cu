@@ -1,0 +1,254 @@
+// DenseCRF2D on the device: model set-up, pairwise application, energies.
+//
+// Per-pixel arithmetic follows the reference's operation order (Eigen 3.2
+// expression evaluation, SSE2, no FMA) so per-pixel results are identical;
+// global FP64 sums are deterministic fixed-order trees whose order differs
+// from Eigen's sequential packet sums (differences are O(1e-16) relative).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "reduce.cuh"
+#include "model_kernels.cuh"
+
+namespace dcrf {
+
+int sm_count() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 148;
+    }
+    return n;
+}
+
+namespace {
+
+__global__ void gaussian_features_kernel(int W, int H, float sx, float sy, float* f) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= W * H) return;
+    const int j = p / W, i = p - j * W;
+    f[2 * (long)p] = (float)i / sx;
+    f[2 * (long)p + 1] = (float)j / sy;
+}
+
+__global__ void bilateral_features_kernel(int W, int H, float sx, float sy, float sr, float sg,
+                                          float sb, const uint8_t* __restrict__ im, float* f) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= W * H) return;
+    const int j = p / W, i = p - j * W;
+    f[5 * (long)p] = (float)i / sx;
+    f[5 * (long)p + 1] = (float)j / sy;
+    f[5 * (long)p + 2] = (float)im[3 * (long)p] / sr;
+    f[5 * (long)p + 3] = (float)im[3 * (long)p + 1] / sg;
+    f[5 * (long)p + 4] = (float)im[3 * (long)p + 2] / sb;
+}
+
+__global__ void fill_kernel(long n, float v, float* x) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) x[t] = v;
+}
+
+// norm = 1 / sqrt(K 1 + 1e-20), in double like src/pairwise.cpp:50.
+__global__ void norm_kernel(int N, float* x) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) x[i] = (float)(1.0 / sqrt(dadd((double)x[i], 1e-20)));
+}
+
+}  // namespace
+
+Model::Model(int W_, int H_, int L_) : W(W_), H(H_), N(W_ * H_), L(L_) {
+    DCRF_CUDA(cudaGetDevice(&device));
+    DCRF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    DCRF_CUDA(cudaMallocHost(&h_scal, sizeof(SolverScalars)));
+    scal.ensure(1);
+    partials.ensure((size_t)kRedBlocks * 16);
+}
+
+Model::~Model() {
+    if (stream) cudaStreamSynchronize(stream);
+    terms.clear();
+    if (h_scal) cudaFreeHost(h_scal);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+void Model::fetch_scalars() {
+    DCRF_CUDA(cudaMemcpyAsync(h_scal, scal.get(), sizeof(SolverScalars), cudaMemcpyDeviceToHost, stream));
+    sync();
+}
+
+void Model::add_term(const float* d_features, int d, float w) {
+    auto t = std::make_unique<Term>();
+    t->lat = std::make_unique<Lattice>();
+    t->lat->stream = stream;
+    t->lat->build(d_features, d, N);
+    t->w = w;
+    t->d = d;
+    float* nrm = t->norm.ensure(N);
+    fill_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, 1.0f, nrm);
+    SliceEpilogue ep;  // plain output
+    t->lat->compute(nrm, nrm, 1, false, ep);
+    norm_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, nrm);
+    DCRF_LAUNCH_CHECK();
+    terms.push_back(std::move(t));
+}
+
+void Model::set_cliques(int R_, const int* off, const int* idx, const float* expw, const float* cst) {
+    R = R_;
+    h_cl_off.assign(off, off + R + 1);
+    clique_total = off[R];
+    h_cl_idx.assign(idx, idx + clique_total);
+    h_cl_exp.assign(expw, expw + R);
+    h_cl_const.assign(cst, cst + R);
+    clique_max = 0;
+    for (int r = 0; r < R; r++) clique_max = std::max(clique_max, off[r + 1] - off[r]);
+    // by-size order used by the prefix-chain clique kernels
+    std::vector<int> order(R), sorted_sizes(R);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b2) { return off[a + 1] - off[a] < off[b2 + 1] - off[b2]; });
+    std::vector<int> packed(2 * (size_t)R + 1 + (size_t)(R + 1));
+    // layout: [R+1 offsets][R order][R sorted sizes]
+    std::memcpy(packed.data(), off, sizeof(int) * (R + 1));
+    for (int r = 0; r < R; r++) {
+        packed[R + 1 + r] = order[r];
+        packed[2 * R + 1 + r] = off[order[r] + 1] - off[order[r]];
+    }
+    int* doff = cl_off.ensure(packed.size());
+    DCRF_CUDA(cudaMemcpyAsync(doff, packed.data(), sizeof(int) * packed.size(), cudaMemcpyHostToDevice, stream));
+    int* didx = cl_idx.ensure(std::max(clique_total, 1));
+    if (clique_total)
+        DCRF_CUDA(cudaMemcpyAsync(didx, idx, sizeof(int) * clique_total, cudaMemcpyHostToDevice, stream));
+    float* de = cl_exp.ensure(std::max(R, 1));
+    float* dc = cl_const.ensure(std::max(R, 1));
+    if (R) {
+        DCRF_CUDA(cudaMemcpyAsync(de, expw, sizeof(float) * R, cudaMemcpyHostToDevice, stream));
+        DCRF_CUDA(cudaMemcpyAsync(dc, cst, sizeof(float) * R, cudaMemcpyHostToDevice, stream));
+    }
+    sync();  // host vectors above are the caller's; finish the copies
+}
+
+void Model::apply(int k, bool nonorm, float* out, const float* in, const float* base, float coef,
+                  bool zero_base) {
+    Term& t = *terms[k];
+    SliceEpilogue ep;
+    ep.potts = true;
+    ep.norm = nonorm ? nullptr : t.norm.get();
+    ep.scale = -t.w;
+    ep.base = base;
+    ep.coef = coef;
+    ep.zero_base = zero_base;
+    t.lat->compute(out, in, L, false, ep, nonorm ? nullptr : t.norm.get());
+}
+
+void Model::apply_ord(int k, float* out, const float* rq, const float* base, bool zero_base) {
+    Term& t = *terms[k];
+    SliceEpilogue ep;
+    ep.potts = true;
+    ep.scale = -t.w;
+    ep.base = base;
+    ep.zero_base = zero_base;
+    t.lat->compute_ord(out, rq, L, ep);
+}
+
+void Model::check_unit_range(const float* Q) {
+    minmax_partial_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, partials.get());
+    minmax_finish_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, scal.get());
+    DCRF_LAUNCH_CHECK();
+    fetch_scalars();
+    if (h_scal->qmax > 1.0f || h_scal->qmin < 0.0f) throw Error(DCRF_E_RANGE, "Value out of bounds");
+}
+
+void Model::rescale(float* out, const float* Q) {
+    minmax_partial_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, partials.get());
+    minmax_finish_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, scal.get());
+    rescale_kernel<<<ceil_div((long)N * L, 256), 256, 0, stream>>>((long)N * L, Q, scal.get(), out);
+    DCRF_LAUNCH_CHECK();
+}
+
+void Model::unary_init(float* Q) {
+    require(has_unary, DCRF_E_STATE, "unary_init: no unary energy set");
+    with_lc(L, [&](auto lc) {
+        constexpr int LC = decltype(lc)::value;
+        unary_init_kernel<LC><<<ceil_div(N, 128), 128, 0, stream>>>(N, L, unary.get(), Q);
+    });
+    DCRF_LAUNCH_CHECK();
+}
+
+void Model::current_map(const float* Q, int16_t* lab) {
+    with_lc(L, [&](auto lc) {
+        constexpr int LC = decltype(lc)::value;
+        current_map_kernel<LC><<<ceil_div(N, 128), 128, 0, stream>>>(N, L, Q, lab);
+    });
+    DCRF_LAUNCH_CHECK();
+}
+
+// assignment_energy_true / assignment_energy_higher_order
+// (src/densecrf.cpp:873-885, 844-870, 887-927).
+double Model::energy_true(const int16_t* d_lab, bool ho) {
+    require(has_unary, DCRF_E_STATE, "energy: no unary energy set");
+    float* qc = buf(10);
+    float* o = buf(11);
+    float* pw = b[12].ensure(N);
+    onehot_complement_kernel<<<ceil_div((long)N * L, 256), 256, 0, stream>>>(N, L, d_lab, qc);
+    for (size_t k = 0; k < terms.size(); k++) {
+        apply((int)k, true, o, qc);
+        pairwise_pick_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, L, d_lab, o, pw, k == 0);
+    }
+    if (terms.empty()) fill_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, 0.0f, pw);
+    energy_sum_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, d_lab, unary.get(), pw, partials.get());
+    finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 0, scal.get());
+    if (ho && R > 0) {
+        int* flags = ipart.ensure(std::max(R, 1));
+        clique_label_change_kernel<<<R, 256, 0, stream>>>(cl_off.get(), cl_idx.get(), d_lab, flags);
+        energy_ho_finish_kernel<<<1, 1, 0, stream>>>(R, flags, cl_exp.get(), scal.get());
+    }
+    DCRF_LAUNCH_CHECK();
+    fetch_scalars();
+    return h_scal->sums[0];
+}
+
+// compute_energy_LP_higher_order (src/densecrf.cpp:982-1037).
+double Model::energy_lp(const float* Q) {
+    require(has_unary, DCRF_E_STATE, "energy: no unary energy set");
+    float* rq = buf(10);
+    float* o = buf(11);
+    rescale(rq, Q);
+    dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, unary.get(), Q, partials.get());
+    finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 0, scal.get());
+    for (size_t k = 0; k < terms.size(); k++) {
+        apply_ord((int)k, o, rq);
+        dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, o, partials.get());
+        finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
+    }
+    if (R > 0) {
+        float* diffs = b[13].ensure(std::max(R, 1));
+        clique_maxdiff_kernel<<<R, 256, 0, stream>>>(cl_off.get(), cl_idx.get(), L, Q, diffs);
+    }
+    energy_lp_finish_kernel<<<1, 1, 0, stream>>>((int)terms.size(), R, b[13].get(), cl_exp.get(), scal.get());
+    DCRF_LAUNCH_CHECK();
+    fetch_scalars();
+    return h_scal->energy;
+}
+
+// compute_LR_QP_value(Q, 0) (src/densecrf.cpp:940-957).
+double Model::lr_qp_value(const float* Q) {
+    require(has_unary, DCRF_E_STATE, "energy: no unary energy set");
+    float* o = buf(11);
+    dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, unary.get(), Q, partials.get());
+    finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 0, scal.get());
+    for (size_t k = 0; k < terms.size(); k++) {
+        apply((int)k, false, o, Q);
+        dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, o, partials.get());
+        finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
+    }
+    lr_finish_kernel<<<1, 1, 0, stream>>>((int)terms.size(), scal.get());
+    DCRF_LAUNCH_CHECK();
+    fetch_scalars();
+    return h_scal->energy;
+}
+
+}  // namespace dcrf

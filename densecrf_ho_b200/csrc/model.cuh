@@ -1,0 +1,92 @@
+// DenseCRF2D state on the device: unaries, Potts pairwise terms (each with
+// its lattice and symmetric normalisation), superpixel cliques, and the
+// solver work buffers.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "lattice.cuh"
+
+namespace dcrf {
+
+struct Term {
+    std::unique_ptr<Lattice> lat;
+    DevBuf<float> norm;  // 1/sqrt(K 1 + 1e-20) (src/pairwise.cpp:46-50)
+    float w = 0.0f;      // Potts weight
+    int d = 0;
+};
+
+// Fixed-size deterministic FP64 reduction: every reduction kernel runs this
+// many blocks and writes one partial per block; a one-warp kernel sums the
+// partials in a fixed order.
+constexpr int kRedBlocks = 296;
+constexpr int kRedThreads = 256;
+
+// Device-side scalars of the solvers (one struct, updated by 1-thread kernels).
+struct SolverScalars {
+    double sums[16];     // finalised reductions
+    double energy, old_energy;
+    float fstep, f2step;  // QP step as float and 2*step as float
+    float delta;          // LP Frank-Wolfe step
+    float qp_value;       // LP gamma objective (previous iterate)
+    float qmin, qmax;     // rescale bounds
+    int stop;             // loop-exit flag (QP: stop rule / zero step; LP: gamma converged)
+    int zero_step;        // QP: num == 0 or denom == 0
+    int steps;
+    int err;              // DCRF_E_* raised by a device check
+};
+
+struct Model {
+    int W = 0, H = 0, N = 0, L = 0, device = 0;
+    cudaStream_t stream = nullptr;
+    bool has_unary = false;
+    DevBuf<float> unary;
+    std::vector<std::unique_ptr<Term>> terms;
+
+    // cliques (super_pixel_container_, exp_of_superpixels_, constants_)
+    int R = 0, clique_total = 0, clique_max = 0;
+    std::vector<int> h_cl_off, h_cl_idx;
+    std::vector<float> h_cl_exp, h_cl_const;
+    DevBuf<int> cl_off, cl_idx;
+    DevBuf<float> cl_exp, cl_const;
+
+    // work buffers
+    DevBuf<float> b[16];
+    DevBuf<double> partials;
+    DevBuf<SolverScalars> scal;
+    DevBuf<int16_t> labels;
+    DevBuf<int> ipart;
+    SolverScalars* h_scal = nullptr;  // pinned mirror
+
+    Model(int W_, int H_, int L_);
+    ~Model();
+
+    float* buf(int i) { return b[i].ensure((size_t)N * L); }
+    void add_term(const float* d_features, int d, float w);
+    void set_cliques(int R, const int* off, const int* idx, const float* expw, const float* cst);
+
+    // PairwisePotential::apply / no_norm_pairwise_ apply, with epilogue
+    // out = base + coef * (-w K~ in)  (see SliceEpilogue).
+    void apply(int k, bool nonorm, float* out, const float* in, const float* base = nullptr,
+               float coef = 1.0f, bool zero_base = false);
+    void apply_ord(int k, float* out, const float* rq, const float* base = nullptr,
+                   bool zero_base = false);
+    // Checks Q in [0,1] like apply_upper_minus_lower_ord (throws DCRF_E_RANGE).
+    void check_unit_range(const float* Q);
+
+    void unary_init(float* Q);
+    void current_map(const float* Q, int16_t* lab);
+    double energy_true(const int16_t* d_lab, bool ho);
+    double energy_lp(const float* Q);
+    double lr_qp_value(const float* Q);
+    void rescale(float* out, const float* Q);  // rescale (src/eigen_utils.cpp:120-141)
+
+    int qp(const float* init, float* out, int max_iter, double* energy);
+    int lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve_stats* stats);
+
+    void sync() { DCRF_CUDA(cudaStreamSynchronize(stream)); }
+    void fetch_scalars();  // D2H of the scalars (synchronises)
+};
+
+}  // namespace dcrf

@@ -1,0 +1,271 @@
+// Per-pixel and reduction kernels shared by model.cu and solvers.cu.
+#pragma once
+#include <type_traits>
+
+#include "reduce.cuh"
+
+namespace dcrf {
+
+constexpr int kLMax = 64;  // largest label count of the run-time-L kernels
+
+// Runs f(std::integral_constant<int, LC>) with LC = L for the label counts
+// that have a fully unrolled register instantiation, else LC = 0 (run-time L).
+template <typename F>
+void with_lc(int L, F&& f) {
+    require(L >= 1 && L <= kLMax, DCRF_E_ARG, "label count must be in [1, 64]");
+    if (L == 21) f(std::integral_constant<int, 21>{});
+    else f(std::integral_constant<int, 0>{});
+}
+
+template <int LC>
+struct PixVec {
+    static constexpr int S = LC > 0 ? LC : kLMax;
+};
+
+namespace {
+
+// One warp per value: sums nblk partials in a fixed order.
+__global__ void finalize_sums_kernel(const double* __restrict__ partials, int nblk, int nv, int dst,
+                                     SolverScalars* sc) {
+    const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (j >= nv) return;
+    double s = 0.0;
+    for (int b = lane; b < nblk; b += 32) s += partials[(long)j * nblk + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
+    if (lane == 0) sc->sums[dst + j] = s;
+}
+
+__global__ void dot_kernel(long n, const float* __restrict__ a, const float* __restrict__ b,
+                           double* __restrict__ partials) {
+    double v[1] = {0.0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+        v[0] += (double)a[t] * (double)b[t];
+    block_sum_store<1>(v, partials);
+}
+
+// min / max of x (exact, so order-free): per-block partials stored as
+// doubles, then minmax_finish_kernel combines them into sc->qmin / sc->qmax.
+__global__ void minmax_partial_kernel(long n, const float* __restrict__ x, double* __restrict__ partials) {
+    __shared__ float smin[kRedThreads / 32], smax[kRedThreads / 32];
+    float mn = INFINITY, mx = -INFINITY;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const float v = x[t];
+        mn = fminf(mn, v);
+        mx = fmaxf(mx, v);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) {
+        smin[w] = mn;
+        smax[w] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < kRedThreads / 32; i++) {
+            mn = fminf(mn, smin[i]);
+            mx = fmaxf(mx, smax[i]);
+        }
+        partials[blockIdx.x] = mn;
+        partials[gridDim.x + blockIdx.x] = mx;
+    }
+}
+
+__global__ void minmax_finish_kernel(const double* __restrict__ partials, int nblk, SolverScalars* sc) {
+    const int lane = threadIdx.x;
+    float mn = INFINITY, mx = -INFINITY;
+    for (int b = lane; b < nblk; b += 32) {
+        mn = fminf(mn, (float)partials[b]);
+        mx = fmaxf(mx, (float)partials[nblk + b]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+    }
+    if (lane == 0) {
+        sc->qmin = mn;
+        sc->qmax = mx;
+    }
+}
+
+// rescale (src/eigen_utils.cpp:120-141): out = (Q - min) / (max - min);
+// max(Q - min) equals fl(max Q - min) because rounding is monotone.
+__global__ void rescale_kernel(long n, const float* __restrict__ Q, const SolverScalars* __restrict__ sc,
+                               float* __restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float mn = sc->qmin, mx = fsub(sc->qmax, sc->qmin);
+    float v = fsub(Q[t], mn);
+    if (mx > 0.0f) v = v / mx;
+    out[t] = v;
+}
+
+// expAndNormalize(-U) (src/densecrf.cpp:328-336).  expf is CUDA's; the
+// reference evaluates exp with Eigen's SSE packet polynomial, so results may
+// differ by an ulp.
+template <int LC>
+__global__ void unary_init_kernel(int N, int Lrt, const float* __restrict__ U, float* __restrict__ Q) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float b[PixVec<LC>::S];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) b[k] = -U[(long)i * L + k];
+    float mx = b[0];
+#pragma unroll
+    for (int k = 1; k < PixVec<LC>::S; k++)
+        if (k < L && b[k] > mx) mx = b[k];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) b[k] = expf(fsub(b[k], mx));
+    const float s = vec_sum<LC>(b, L);
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) Q[(long)i * L + k] = b[k] / s;
+}
+
+// currentMap (src/densecrf.cpp:929-938): first arg-max.
+template <int LC>
+__global__ void current_map_kernel(int N, int Lrt, const float* __restrict__ Q, int16_t* __restrict__ lab) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float* q = Q + (long)i * L;
+    float best = q[0];
+    int bi = 0;
+#pragma unroll
+    for (int k = 1; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            float v = q[k];
+            if (v > best) {
+                best = v;
+                bi = k;
+            }
+        }
+    lab[i] = (int16_t)bi;
+}
+
+// Q(j, i) = (l[i] == j) ? 0 : 1 (src/densecrf.cpp:915-917).
+__global__ void onehot_complement_kernel(int N, int L, const int16_t* __restrict__ lab, float* __restrict__ Q) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)N * L) return;
+    const int i = (int)(t / L), j = (int)(t - (long)i * L);
+    Q[t] = lab[i] == j ? 0.0f : 1.0f;
+}
+
+// r[i] += -Q(l[i], i) (src/densecrf.cpp:920-925, 908-910).
+__global__ void pairwise_pick_kernel(int N, int L, const int16_t* __restrict__ lab, const float* __restrict__ o,
+                                     float* __restrict__ pw, bool first) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = lab[i];
+    const float r = (0 <= l && l < L) ? -o[(long)i * L + l] : 0.0f;
+    pw[i] = fadd(first ? 0.0f : pw[i], r);
+}
+
+// sum_i (unary(l_i, i) + pairwise_i) in double (src/densecrf.cpp:877-884).
+__global__ void energy_sum_kernel(int N, int L, const int16_t* __restrict__ lab, const float* __restrict__ U,
+                                  const float* __restrict__ pw, double* __restrict__ partials) {
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const int l = lab[i];
+        const float u = (0 <= l && l < L) ? U[(long)i * L + l] : 0.0f;
+        v[0] += (double)fadd(u, pw[i]);
+    }
+    block_sum_store<1>(v, partials);
+}
+
+// Clique r "changes label" when l[p] != l[idx[0]] for some clique-local
+// index p (the reference compares l[pix] with pix the loop index,
+// src/densecrf.cpp:859-864).
+__global__ void clique_label_change_kernel(const int* __restrict__ off, const int* __restrict__ idx,
+                                           const int16_t* __restrict__ lab, int* __restrict__ flags) {
+    const int r = blockIdx.x;
+    const int s0 = off[r], sz = off[r + 1] - s0;
+    __shared__ int any;
+    if (threadIdx.x == 0) any = 0;
+    __syncthreads();
+    if (sz > 0) {
+        const int16_t prev = lab[idx[s0]];
+        int mine = 0;
+        for (int p = threadIdx.x; p < sz; p += blockDim.x) mine |= lab[p] != prev;
+        if (mine) any = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) flags[r] = any;
+}
+
+__global__ void energy_ho_finish_kernel(int R, const int* __restrict__ flags, const float* __restrict__ ew,
+                                        SolverScalars* sc) {
+    double e = sc->sums[0], ho = 0.0;
+    for (int r = 0; r < R; r++) {
+        if (flags[r]) e += (double)ew[r];
+        ho += (double)fmul((float)(R - 1), ew[r]);
+    }
+    sc->sums[0] = e + ho;
+}
+
+// Per clique: max over labels of (max - min of Q over the clique's pixels)
+// (src/densecrf.cpp:1020-1034).
+__global__ void clique_maxdiff_kernel(const int* __restrict__ off, const int* __restrict__ idx, int L,
+                                      const float* __restrict__ Q, float* __restrict__ diffs) {
+    const int r = blockIdx.x;
+    const int s0 = off[r], s1 = off[r + 1];
+    __shared__ float smx[32], smn[32];
+    float best = 0.0f;
+    for (int lab = 0; lab < L; lab++) {
+        float mx = -INFINITY, mn = INFINITY;
+        for (int p = s0 + threadIdx.x; p < s1; p += blockDim.x) {
+            const float q = Q[(long)idx[p] * L + lab];
+            mx = fmaxf(mx, q);
+            mn = fminf(mn, q);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+            mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            smx[threadIdx.x >> 5] = mx;
+            smn[threadIdx.x >> 5] = mn;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+                mx = fmaxf(mx, smx[w]);
+                mn = fminf(mn, smn[w]);
+            }
+            const float diff = fsub(mx, mn);
+            if (lab == 0 || diff > best) best = diff;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) diffs[r] = best;
+}
+
+__global__ void energy_lp_finish_kernel(int nterms, int R, const float* __restrict__ diffs,
+                                        const float* __restrict__ ew, SolverScalars* sc) {
+    double e = sc->sums[0];
+    for (int k = 0; k < nterms; k++) e -= sc->sums[1 + k];
+    for (int r = 0; r < R; r++) e += (double)fmul(ew[r], diffs[r]);
+    sc->energy = e;
+}
+
+// compute_LR_QP_value(Q, 0): U.Q - 0.Q + sum_k Q.(A_k Q) + Q.(0 o Q).
+__global__ void lr_finish_kernel(int nterms, SolverScalars* sc) {
+    double e = 0.0;
+    e += sc->sums[0];
+    e -= 0.0;
+    for (int k = 0; k < nterms; k++) e += sc->sums[1 + k];
+    e += 0.0;
+    sc->energy = e;
+}
+
+}  // namespace
+}  // namespace dcrf

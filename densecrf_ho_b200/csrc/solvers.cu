@@ -1,0 +1,907 @@
+// QP (Frank-Wolfe, src/densecrf.cpp:340-442) and proximal LP
+// (src/densecrf.cpp:444-830) solvers on the device, with the superpixel
+// clique terms of qp_sp / lp_sp.
+//
+// Every per-pixel / per-element update restates the reference's float
+// operation order exactly.  Global reductions are deterministic FP64 trees:
+//   - the QP line-search dots and the LP dual gap (reference: FP64 Eigen sums);
+//   - the LP gamma objective sum (reference: an FP32 Eigen sum) -- summed in
+//     FP64 and rounded to float for its stop test;
+//   - the QP clique products multiplySuperPixels(p1, p2) -> float
+//     (reference: a long sequential FP32 sum) -- evaluated in FP64.
+// These can differ from the reference only in their last bits; all other
+// clique algebra (prefix chains, running int min/max) is exact.
+#include <algorithm>
+#include <cfloat>
+#include <climits>
+#include <cmath>
+#include <cstring>
+
+#include "model_kernels.cuh"
+
+namespace dcrf {
+
+namespace {
+
+// ------------------------------------------------------------------ QP --
+
+// cond_grad_y = one-hot(first arg-min of grad_y) (src/qp.cpp:5-15);
+// sx_y = cond_grad_y - Q; partial sum of unary . sx_y.
+template <int LC>
+__global__ void qp_direction_kernel(int N, int Lrt, const float* __restrict__ grad, const float* __restrict__ Q,
+                                    const float* __restrict__ U, float* __restrict__ sx,
+                                    double* __restrict__ partials) {
+    const int L = LC ? LC : Lrt;
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const float* g = grad + (long)i * L;
+        float best = g[0];
+        int bi = 0;
+#pragma unroll
+        for (int k = 1; k < PixVec<LC>::S; k++)
+            if (k < L) {
+                float x = g[k];
+                if (x < best) {
+                    best = x;
+                    bi = k;
+                }
+            }
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) {
+                const long e = (long)i * L + k;
+                const float s = fsub(k == bi ? 1.0f : 0.0f, Q[e]);
+                sx[e] = s;
+                v[0] += (double)U[e] * (double)s;
+            }
+    }
+    block_sum_store<1>(v, partials);
+}
+
+__global__ void dots2_kernel(long n, const float* __restrict__ a, const float* __restrict__ b,
+                             const float* __restrict__ c, double* __restrict__ partials) {
+    // partial sums of a.c and b.c
+    double v[2] = {0.0, 0.0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const double cc = c[t];
+        v[0] += (double)a[t] * cc;
+        v[1] += (double)b[t] * cc;
+    }
+    block_sum_store<2>(v, partials);
+}
+
+// Line search (src/densecrf.cpp:412-421).  sums: 0 U.sx, 1 Q.psi, 2 sx.psi,
+// 3 a, 4 b, 5 sum(sx_z), 6 clique term of the denominator.
+__global__ void qp_step_kernel(SolverScalars* sc) {
+    sc->old_energy = sc->energy;
+    const double num = sc->sums[0] + 2 * sc->sums[1] + sc->sums[3] + sc->sums[4] + sc->sums[5];
+    const double denom = sc->sums[2] + sc->sums[6];
+    double step = -num / (2 * denom);
+    if (denom == 0 || num == 0) {
+        sc->zero_step = 1;
+        sc->stop = 1;
+        return;
+    }
+    if (denom < 0) step = 1;
+    sc->fstep = (float)step;
+    sc->f2step = (float)(2 * step);
+    sc->steps++;
+}
+
+// Q += step sx_y; grad_y += 2 step psisx + step ho (src/densecrf.cpp:424-431);
+// partial sum of Q . (grad_y + unary) (:434).
+__global__ void qp_update_kernel(long n, const float* __restrict__ sx, const float* __restrict__ psi,
+                                 const float* __restrict__ ho, const float* __restrict__ U, float* __restrict__ Q,
+                                 float* __restrict__ grad, const SolverScalars* __restrict__ sc,
+                                 double* __restrict__ partials) {
+    if (sc->zero_step) return;
+    const float fs = sc->fstep, f2s = sc->f2step;
+    double v[1] = {0.0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const float q = fadd(Q[t], fmul(fs, sx[t]));
+        const float h = ho ? ho[t] : 0.0f;
+        const float g = fadd(grad[t], fadd(fmul(f2s, psi[t]), fmul(fs, h)));
+        Q[t] = q;
+        grad[t] = g;
+        v[0] += (double)q * (double)fadd(g, U[t]);
+    }
+    block_sum_store<1>(v, partials);
+}
+
+// energy = sums[7] + (float) clique term sums[8]; stop rule (:390).
+__global__ void qp_energy_kernel(SolverScalars* sc, int max_iter) {
+    if (sc->zero_step) return;
+    const double e = sc->sums[7] + sc->sums[8];
+    sc->energy = e;
+    if (max_iter > 0) sc->stop = sc->steps >= max_iter;
+    else sc->stop = !((sc->old_energy - e) > 100.0);
+}
+
+__global__ void qp_init_energy_kernel(SolverScalars* sc, int nterms, int max_iter) {
+    // compute_LR_QP_value(Q, 0) + clique term (src/densecrf.cpp:386-387)
+    double e = 0.0;
+    e += sc->sums[0];
+    e -= 0.0;
+    for (int k = 0; k < nterms; k++) e += sc->sums[1 + k];
+    e += 0.0;
+    e += sc->sums[8];
+    sc->energy = e;
+    sc->old_energy = DBL_MAX;
+    sc->zero_step = 0;
+    sc->steps = 0;
+    // loop entry test of :390 (fixed-iteration mode always enters)
+    sc->stop = max_iter > 0 ? 0 : !((DBL_MAX - e) > 100.0);
+}
+
+// ------------------------------------------------------ QP clique terms --
+// Arrays over (label, clique) are stored [r*L + lab].  The clique list
+// buffer holds [R+1 offsets][R cliques by size][their sizes].
+
+struct CliqueView {
+    const int* off;
+    const int* order;
+    const int* sizes;
+    const int* idx;
+    const float* ew;  // exp_of_superpixels_
+    const float* cst; // constants_
+    int R, max_size;
+};
+
+// multiplySuperPixels(p [L x N]) with p = Q - 1 (src/densecrf.cpp:81-88): the
+// reference sums p(lab, 0..size_r-1) -- the clique-LOCAL index -- so every
+// clique's value is a prefix of one sequential chain per label.  Then
+//   mode 0: grad_z = (1 + res) o c           (:373-374)
+//   mode 1: grad_z = 1 o c + res o c         (:432)
+__global__ void ho_regions_kernel(CliqueView cv, int L, const float* __restrict__ Q, float* __restrict__ gz,
+                                  int mode, const SolverScalars* __restrict__ sc) {
+    if (sc && sc->zero_step) return;
+    const int lab = threadIdx.x;
+    if (lab >= L) return;
+    int ptr = 0;
+    float s = 0.0f;
+    auto emit = [&](float val) {
+        const int r = cv.order[ptr];
+        const float c = cv.ew[r];
+        gz[(long)r * L + lab] = mode == 0 ? fmul(fadd(1.0f, val), c) : fadd(fmul(1.0f, c), fmul(val, c));
+        ptr++;
+    };
+    while (ptr < cv.R && cv.sizes[ptr] == 0) emit(0.0f);
+    for (int q = 0; q < cv.max_size && ptr < cv.R; q++) {
+        s = fadd(s, fsub(Q[(long)q * L + lab], 1.0f));
+        while (ptr < cv.R && cv.sizes[ptr] == q + 1) emit(s);
+    }
+}
+
+// Small (label, clique) algebra of one Frank-Wolfe iteration.  One thread
+// per element, then thread 0 sums sx_z in Eigen order.
+//   cz = [gz < 0] (src/qp.cpp:17-25); sxz = cz - z; t1 = sxz o c;
+//   t2 = (cz - 1) o c.
+__global__ void ho_direction_kernel(CliqueView cv, int L, const float* __restrict__ gz, const float* __restrict__ z,
+                                    float* __restrict__ sxz, float* __restrict__ t1, float* __restrict__ t2,
+                                    float* __restrict__ cz, SolverScalars* sc) {
+    const int n = L * cv.R;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const float c = cv.ew[e / L];
+        const float czv = gz[e] >= 0.0f ? 0.0f : 1.0f;
+        const float sv = fsub(czv, z[e]);
+        cz[e] = czv;
+        sxz[e] = sv;
+        t1[e] = fmul(sv, c);
+        t2[e] = fmul(fsub(czv, 1.0f), c);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sc->sums[5] = (double)eig_sum_rt(sxz, n, 0);
+}
+
+// float multiplySuperPixels(p1 [L x R], p2 [L x N]) (src/densecrf.cpp:58-72):
+// sum_r sum_{q < size_r} sum_lab p1(lab, r) p2(lab, q), clique-local q again.
+// Evaluated in FP64 as sum_lab sum_r p1(lab, r) * prefix_lab(size_r), then
+// rounded to float.  p2 = Q - 1 (minus_one) or p2 as given.
+__global__ void ho_scalar_kernel(CliqueView cv, int L, const float* __restrict__ p1, const float* __restrict__ p2,
+                                 int minus_one, int slot, SolverScalars* sc, int add_to_slot) {
+    if (sc->zero_step && slot != 8) return;
+    __shared__ double part[kLMax];
+    const int lab = threadIdx.x;
+    double acc = 0.0;
+    if (lab < L) {
+        int ptr = 0;
+        double pre = 0.0;
+        while (ptr < cv.R && cv.sizes[ptr] == 0) ptr++;
+        for (int q = 0; q < cv.max_size && ptr < cv.R; q++) {
+            float x = p2[(long)q * L + lab];
+            if (minus_one) x = fsub(x, 1.0f);
+            pre += (double)x;
+            while (ptr < cv.R && cv.sizes[ptr] == q + 1) {
+                acc += (double)p1[(long)cv.order[ptr] * L + lab] * pre;
+                ptr++;
+            }
+        }
+    }
+    if (threadIdx.x < kLMax) part[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < L; k++) s += part[k];
+        const float f = (float)s;
+        if (add_to_slot) sc->sums[slot] = (double)fadd((float)sc->sums[slot], f);
+        else sc->sums[slot] = (double)f;
+    }
+}
+
+// multiplySuperPixels(p [L x R]) -> [L x N] (src/densecrf.cpp:90-97):
+// out(lab, q) = sum over cliques r (in order) with size_r > q of p(lab, r).
+// p = (z - 1) o c is formed on the fly.  Rows q >= max_size stay zero.
+__global__ void ho_pixels_kernel(CliqueView cv, int L, const float* __restrict__ z, float* __restrict__ out,
+                                 const SolverScalars* __restrict__ sc) {
+    if (sc && sc->zero_step) return;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)cv.max_size * L) return;
+    const int q = (int)(t / L), lab = (int)(t - (long)q * L);
+    float s = 0.0f;
+    for (int r = 0; r < cv.R; r++)
+        if (cv.off[r + 1] - cv.off[r] > q) s = fadd(s, fmul(fsub(z[(long)r * L + lab], 1.0f), cv.ew[r]));
+    out[t] = s;
+}
+
+// z += step sx_z (src/densecrf.cpp:425).
+__global__ void ho_z_update_kernel(int n, float* __restrict__ z, const float* __restrict__ sxz,
+                                   const SolverScalars* __restrict__ sc) {
+    if (sc->zero_step) return;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) z[e] = fadd(z[e], fmul(sc->fstep, sxz[e]));
+}
+
+// z o c sum (Eigen order) and (1 - z) o c, for the energy's clique term.
+__global__ void ho_zterm_prep_kernel(CliqueView cv, int L, const float* __restrict__ z, float* __restrict__ zc,
+                                     float* __restrict__ omz, SolverScalars* sc) {
+    if (sc->zero_step && sc->steps > 0) return;
+    const int n = L * cv.R;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const float c = cv.ew[e / L];
+        zc[e] = fmul(z[e], c);
+        omz[e] = fmul(fsub(1.0f, z[e]), c);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sc->sums[8] = (double)eig_sum_rt(zc, n, 0);
+}
+
+__global__ void fill_float_kernel(long n, float v, float* x) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) x[t] = v;
+}
+
+__global__ void add_inplace_kernel(long n, float* __restrict__ a, const float* __restrict__ b) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] = fadd(a[t], b[t]);
+}
+
+// a += coef * b  (grad_y += 2 * tmp, src/densecrf.cpp:380)
+__global__ void add_scaled_kernel(long n, float* __restrict__ a, const float* __restrict__ b, float coef) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] = fadd(a[t], fmul(coef, b[t]));
+}
+
+// ------------------------------------------------------------------ LP --
+
+// Y = multiplyC((alpha + u) - unary) + cur_Q (src/densecrf.cpp:627-635, 517-523).
+template <int LC>
+__global__ void lp_y_kernel(int N, int Lrt, float lambda, float cm, const float* __restrict__ alpha,
+                            const float* __restrict__ u, const float* __restrict__ U,
+                            const float* __restrict__ curQ, float* __restrict__ Y) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float x[PixVec<LC>::S];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            const long e = (long)i * L + k;
+            x[k] = fsub(fadd(alpha[e], u[e]), U[e]);
+        }
+    const float s = vec_sum<LC>(x, L);
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            const long e = (long)i * L + k;
+            Y[e] = fadd(fmul(fadd(fmul(cm, s), x[k]), lambda), curQ[e]);
+        }
+}
+
+struct GammaConsts {
+    float lambda, delta, c0, c1, c2, cm;
+};
+
+// One qp-gamma iteration for every pixel (qp_gamma_step, :495-514, and the
+// objective of :665-667); partial sums of the per-pixel objective.
+template <int LC>
+__global__ void lp_gamma_kernel(int N, int Lrt, GammaConsts gc, const float* __restrict__ Y, float* __restrict__ gamma,
+                                const SolverScalars* __restrict__ sc, double* __restrict__ partials) {
+    if (sc->stop) return;
+    const int L = LC ? LC : Lrt;
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        float g[PixVec<LC>::S], y[PixVec<LC>::S], t[PixVec<LC>::S];
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) {
+                g[k] = gamma[(long)i * L + k];
+                y[k] = Y[(long)i * L + k];
+            }
+        const float s = vec_sum<LC>(g, L);
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) {
+                const float ph = (-y[k] < 0.0f) ? 0.0f : -y[k];  // std::max(-Y, 0)
+                const float nh = (y[k] < 0.0f) ? 0.0f : y[k];    // std::max(Y, 0)
+                float st = fadd(fmul(fsub(s, g[k]), gc.c0), ph);
+                st = fadd(st, gc.delta);
+                float tt = fmul(fadd(fmul(gc.c1, s), fmul(gc.c2, g[k])), gc.lambda);
+                tt = fadd(tt, nh);
+                tt = fadd(tt, gc.delta);
+                g[k] = fmul(g[k], st / tt);
+                gamma[(long)i * L + k] = g[k];
+            }
+        const float s2 = vec_sum<LC>(g, L);
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) t[k] = fmul(g[k], fmul(fadd(fmul(gc.cm, s2), g[k]), gc.lambda));
+        const float d1 = vec_sum<LC>(t, L);
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) t[k] = fmul(g[k], y[k]);
+        const float d2 = vec_sum<LC>(t, L);
+        const float qv = (float)dadd(dmul(0.5, (double)d1), (double)d2);
+        v[0] += (double)qv;
+    }
+    block_sum_store<1>(v, partials);
+}
+
+// |qp_value - qp_value1| < qp_tol test (:670-674).
+__global__ void lp_gamma_check_kernel(const double* __restrict__ partials, int nblk, float qp_tol,
+                                      SolverScalars* sc) {
+    if (sc->stop) return;
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    for (int b = lane; b < nblk; b += 32) s += partials[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
+    if (lane == 0) {
+        const float qv1 = (float)s;
+        sc->steps++;
+        if (fabsf(fsub(sc->qp_value, qv1)) < qp_tol) sc->stop = 1;
+        else sc->qp_value = qv1;
+    }
+}
+
+__global__ void lp_gamma_reset_kernel(SolverScalars* sc) {
+    sc->stop = 0;
+    sc->steps = 0;
+    sc->qp_value = FLT_MAX;
+}
+
+// beta = -colsum(alpha + u + gamma - unary) / L (:684-691);
+// Q = lambda (alpha + beta + u + gamma - unary) + cur_Q (:697).
+template <int LC>
+__global__ void lp_q_kernel(int N, int Lrt, float lambda, const float* __restrict__ alpha, const float* __restrict__ u,
+                            const float* __restrict__ gamma, const float* __restrict__ U,
+                            const float* __restrict__ curQ, float* __restrict__ Q) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float bm[PixVec<LC>::S];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            const long e = (long)i * L + k;
+            bm[k] = fsub(fadd(fadd(alpha[e], u[e]), gamma[e]), U[e]);
+        }
+    const float beta = (-col_sum<LC>(bm, L, i)) / (float)L;
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            const long e = (long)i * L + k;
+            const float x = fsub(fadd(fadd(fadd(alpha[e], beta), u[e]), gamma[e]), U[e]);
+            Q[e] = fadd(fmul(x, lambda), curQ[e]);
+        }
+}
+
+// Partial sums of tmp.Q and tmp.tmp, tmp = (alpha + u) - (sa + su) (:725-729).
+__global__ void lp_gap_kernel(long n, const float* __restrict__ alpha, const float* __restrict__ u,
+                              const float* __restrict__ sa, const float* __restrict__ su,
+                              const float* __restrict__ Q, double* __restrict__ partials) {
+    double v[2] = {0.0, 0.0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const float tmp = fsub(fadd(alpha[t], u[t]), fadd(sa[t], su ? su[t] : 0.0f));
+        v[0] += (double)tmp * (double)Q[t];
+        v[1] += (double)tmp * (double)tmp;
+    }
+    block_sum_store<2>(v, partials);
+}
+
+__global__ void lp_delta_kernel(SolverScalars* sc, float lambda) {
+    float delta = (float)(sc->sums[0] / ((double)lambda * sc->sums[1]));
+    delta = (delta < 0.0f) ? 0.0f : delta;  // std::max(delta, 0)
+    delta = (1.0f < delta) ? 1.0f : delta;  // std::min(delta, 1)
+    sc->delta = delta;
+}
+
+// alpha += delta (sa - alpha); u += delta (su - u) (:737-738).
+__global__ void lp_alpha_kernel(long n, const float* __restrict__ sa, const float* __restrict__ su,
+                                float* __restrict__ alpha, float* __restrict__ u,
+                                const SolverScalars* __restrict__ sc) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float d = sc->delta;
+    alpha[t] = fadd(alpha[t], fmul(d, fsub(sa[t], alpha[t])));
+    const float s = su ? su[t] : 0.0f;
+    u[t] = fadd(u[t], fmul(d, fsub(s, u[t])));
+}
+
+template <int LC>
+__device__ __forceinline__ void sort_desc(float* s, int L) {
+    // insertion sort (values only: ties cannot change feasible_Q's result)
+#pragma unroll
+    for (int a = 1; a < PixVec<LC>::S; a++)
+        if (a < L) {
+            const float x = s[a];
+            int b = a - 1;
+            while (b >= 0 && s[b] < x) {
+                s[b + 1] = s[b];
+                b--;
+            }
+            s[b + 1] = x;
+        }
+}
+
+// renormalize (src/densecrf.cpp:444-455) of one pixel held in registers.
+template <int LC>
+__device__ __forceinline__ void renorm_pixel(float* t, int L, long i) {
+    const double s = (double)col_sum<LC>(t, L, i);
+    if (s == 0 || s != s) {
+        const float uni = (float)(1.0 / L);
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) t[k] = uni;
+    } else {
+        const float fs = (float)s;
+#pragma unroll
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) t[k] = t[k] / fs;
+    }
+}
+
+// feasible_Q (:470-492) + renormalize + currentMap, one thread per pixel.
+template <int LC>
+__global__ void lp_project_kernel(int N, int Lrt, float* __restrict__ Q, int16_t* __restrict__ lab) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float q[PixVec<LC>::S], s[PixVec<LC>::S];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) q[k] = s[k] = Q[(long)i * L + k];
+    sort_desc<LC>(s, L);
+    double sum = (double)fsub(col_sum<LC>(q, L, i), 1.0f);
+    int K = -1;
+    for (int k = L; k > 0; --k) {
+        const double uk = (double)s[k - 1];
+        if (sum / k < uk) {
+            K = k;
+            break;
+        }
+        sum -= uk;
+    }
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            double v = (double)q[k] - sum / K;
+            v = (v < 0.0) ? 0.0 : v;
+            v = (1.0 < v) ? 1.0 : v;
+            q[k] = (float)v;
+        }
+    renorm_pixel<LC>(q, L, i);
+    float best = q[0];
+    int bi = 0;
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            Q[(long)i * L + k] = q[k];
+            if (k > 0 && q[k] > best) {
+                best = q[k];
+                bi = k;
+            }
+        }
+    if (lab) lab[i] = (int16_t)bi;
+}
+
+template <int LC>
+__global__ void renormalize_kernel(int N, int Lrt, float* __restrict__ Q) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float q[PixVec<LC>::S];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) q[k] = Q[(long)i * L + k];
+    renorm_pixel<LC>(q, L, i);
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) Q[(long)i * L + k] = q[k];
+}
+
+// max_rounding (:832-840).
+template <int LC>
+__global__ void max_rounding_kernel(int N, int Lrt, float* __restrict__ Q) {
+    const int L = LC ? LC : Lrt;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float best = Q[(long)i * L];
+    int bi = 0;
+    for (int k = 1; k < L; k++)
+        if (Q[(long)i * L + k] > best) {
+            best = Q[(long)i * L + k];
+            bi = k;
+        }
+    for (int k = 0; k < L; k++) Q[(long)i * L + k] = k == bi ? 1.0f : 0.0f;
+}
+
+// less_confident_pixels count (:458-464).
+__global__ void less_confident_kernel(int N, int L, const float* __restrict__ Q, float tol, double* partials) {
+    double v[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        float mx = Q[(long)i * L];
+        for (int k = 1; k < L; k++) mx = fmaxf(mx, Q[(long)i * L + k]);
+        if (mx <= tol) v[0] += 1.0;
+    }
+    block_sum_store<1>(v, partials);
+}
+
+// --------------------------------------------------------- LP cliques --
+
+// float -> int as x86 cvttss2si (C++ truncation; NaN / out of range -> INT_MIN).
+__device__ __forceinline__ int trunc_x86(float q) {
+    return fabsf(q) < 2147483648.0f ? (int)q : INT_MIN;
+}
+
+template <bool IS_MIN>
+__device__ __forceinline__ int block_excl_scan_minmax(int v, int* sm, int* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int ident = IS_MIN ? INT_MAX : INT_MIN;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(kFullMask, x, o);
+        if (lane >= o) x = IS_MIN ? min(x, y) : max(x, y);
+    }
+    int ex = __shfl_up_sync(kFullMask, x, 1);
+    if (lane == 0) ex = ident;
+    if (lane == 31) sm[w] = x;
+    __syncthreads();
+    int pre = ident, tot = ident;
+    for (int ww = 0; ww < nw; ww++) {
+        if (ww < w) pre = IS_MIN ? min(pre, sm[ww]) : max(pre, sm[ww]);
+        tot = IS_MIN ? min(tot, sm[ww]) : max(tot, sm[ww]);
+    }
+    __syncthreads();
+    *total = tot;
+    return IS_MIN ? min(pre, ex) : max(pre, ex);
+}
+
+__device__ __forceinline__ int block_max_int(int v, int* sm) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(kFullMask, v, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    int r = INT_MIN;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = max(r, sm[w]);
+    __syncthreads();
+    return r;
+}
+
+// computeUCondGrad (src/densecrf.cpp:803-830) for clique r = blockIdx.x.
+// The reference keeps its running min / max in an int, so position p (in
+// label-major, clique order) updates the min iff Q_p < (float)s where s is
+// the running min of trunc(Q) over the positions before p (it starts at
+// INT_MAX); the LAST such p is selected.  Same for the max.  A block-wide
+// min / max scan gives every position its s.
+__global__ void ucond_kernel(const int* __restrict__ off, const int* __restrict__ idx, int L,
+                             const float* __restrict__ Q, int* __restrict__ pos) {
+    __shared__ int sm[32];
+    const int r = blockIdx.x;
+    const int s0 = off[r], sz = off[r + 1] - s0;
+    const long n = (long)L * sz;
+    int carry_min = INT_MAX, carry_max = INT_MIN, last_min = -1, last_max = -1;
+    for (long base = 0; base < n; base += blockDim.x) {
+        const long p = base + threadIdx.x;
+        const bool valid = p < n;
+        float q = 0.0f;
+        int tmin = INT_MAX, tmax = INT_MIN;
+        if (valid) {
+            const int lab = (int)(p / sz), j = (int)(p - (long)lab * sz);
+            q = Q[(long)idx[s0 + j] * L + lab];
+            tmin = tmax = trunc_x86(q);
+        }
+        int tot_min, tot_max;
+        const int bmin = min(carry_min, block_excl_scan_minmax<true>(tmin, sm, &tot_min));
+        const int bmax = max(carry_max, block_excl_scan_minmax<false>(tmax, sm, &tot_max));
+        const int cmin = (valid && q < (float)bmin) ? (int)p : -1;
+        const int cmax = (valid && q > (float)bmax) ? (int)p : -1;
+        last_min = max(last_min, block_max_int(cmin, sm));
+        last_max = max(last_max, block_max_int(cmax, sm));
+        carry_min = min(carry_min, tot_min);
+        carry_max = max(carry_max, tot_max);
+    }
+    if (threadIdx.x == 0) {
+        // element index pixel*L + label, or -1 when nothing was selected
+        pos[2 * r] = last_min < 0 ? -1 : idx[s0 + last_min % sz] * L + last_min / sz;
+        pos[2 * r + 1] = last_max < 0 ? -1 : idx[s0 + last_max % sz] * L + last_max / sz;
+    }
+}
+
+// Writes Us in clique order (later cliques overwrite earlier ones; an
+// unselected side keeps the previous clique's position, as the reference's
+// variables do).
+__global__ void ucond_apply_kernel(int R, const int* __restrict__ pos, const float* __restrict__ cst,
+                                   const float* __restrict__ ew, float* __restrict__ Us) {
+    int mn = 0, mx = 0;
+    for (int r = 0; r < R; r++) {
+        if (pos[2 * r] >= 0) mn = pos[2 * r];
+        if (pos[2 * r + 1] >= 0) mx = pos[2 * r + 1];
+        Us[mn] = fmul(cst[r], ew[r]);
+        Us[mx] = fmul(-cst[r], ew[r]);
+    }
+}
+
+constexpr int kPix = 128;
+
+}  // namespace
+
+// ---------------------------------------------------------------- QP host --
+int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
+    require(has_unary, DCRF_E_STATE, "qp: no unary energy set");
+    const long NL = (long)N * L;
+    float* Q = out;  // iterate in place in the output buffer
+    float* grad = buf(0);
+    float* sx = buf(1);
+    float* psi = buf(2);
+    float* tmp = buf(3);
+    float* ho = nullptr;
+    if (Q != init) DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    DCRF_CUDA(cudaMemcpyAsync(grad, unary.get(), sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    DCRF_CUDA(cudaMemsetAsync(scal.get(), 0, sizeof(SolverScalars), stream));
+    SolverScalars* sc = scal.get();
+    double* part = partials.get();
+    const int nt = (int)terms.size();
+
+    CliqueView cv{};
+    float *gz = nullptr, *z = nullptr, *sxz = nullptr, *t1 = nullptr, *t2 = nullptr, *cz = nullptr, *zc = nullptr,
+          *omz = nullptr;
+    const int LR = L * R;
+    if (R > 0) {
+        const int* base = cl_off.get();
+        cv = CliqueView{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R, clique_max};
+        float* small = b[14].ensure((size_t)8 * LR);
+        gz = small;
+        z = small + LR;
+        sxz = small + 2 * LR;
+        t1 = small + 3 * LR;
+        t2 = small + 4 * LR;
+        cz = small + 5 * LR;
+        zc = small + 6 * LR;
+        omz = small + 7 * LR;
+        fill_float_kernel<<<ceil_div(LR, 256), 256, 0, stream>>>(LR, 1.0f, z);
+        ho = buf(4);
+        DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
+        ho_regions_kernel<<<1, kLMax, 0, stream>>>(cv, L, Q, gz, 0, nullptr);
+    }
+    // grad_y = unary + sum_k 2 A_k Q; energy terms Q . A_k Q (same applies).
+    for (int k = 0; k < nt; k++) {
+        apply(k, false, tmp, Q);
+        add_scaled_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, grad, tmp, 2.0f);
+        dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, Q, tmp, part);
+        finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 1 + k, sc);
+    }
+    if (R > 0) {
+        ho_pixels_kernel<<<ceil_div((long)clique_max * L, 256), 256, 0, stream>>>(cv, L, z, ho, nullptr);
+        add_inplace_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, grad, ho);
+        ho_zterm_prep_kernel<<<1, 256, 0, stream>>>(cv, L, z, zc, omz, sc);
+        ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, omz, Q, 1, 8, sc, 1);
+    }
+    dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, unary.get(), Q, part);
+    finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 0, sc);
+    qp_init_energy_kernel<<<1, 1, 0, stream>>>(sc, nt, max_iter);
+    DCRF_LAUNCH_CHECK();
+    fetch_scalars();
+    int guard = 0;
+    while (!h_scal->stop) {
+        require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            qp_direction_kernel<LC><<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, grad, Q, unary.get(), sx, part);
+        });
+        finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 0, sc);
+        if (R > 0) {
+            ho_direction_kernel<<<1, 256, 0, stream>>>(cv, L, gz, z, sxz, t1, t2, cz, sc);
+            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, t1, Q, 1, 3, sc, 0);    // a
+            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, t2, sx, 0, 4, sc, 0);   // b
+            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, t1, sx, 0, 6, sc, 0);   // denom term
+        }
+        for (int k = 0; k < nt; k++) {
+            if (k == 0) apply(k, false, psi, sx, nullptr, 1.0f, true);
+            else apply(k, false, psi, sx, psi, 1.0f, false);
+        }
+        dots2_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, Q, sx, psi, part);
+        finalize_sums_kernel<<<1, 64, 0, stream>>>(part, kRedBlocks, 2, 1, sc);
+        qp_step_kernel<<<1, 1, 0, stream>>>(sc);
+        if (R > 0) {
+            ho_z_update_kernel<<<1, 256, 0, stream>>>(LR, z, sxz, sc);
+            ho_pixels_kernel<<<ceil_div((long)clique_max * L, 256), 256, 0, stream>>>(cv, L, z, ho, sc);
+        }
+        qp_update_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, sx, psi, ho, unary.get(), Q, grad, sc, part);
+        finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 7, sc);
+        if (R > 0) {
+            ho_regions_kernel<<<1, kLMax, 0, stream>>>(cv, L, Q, gz, 1, sc);
+            ho_zterm_prep_kernel<<<1, 256, 0, stream>>>(cv, L, z, zc, omz, sc);
+            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, omz, Q, 1, 8, sc, 1);
+        }
+        qp_energy_kernel<<<1, 1, 0, stream>>>(sc, max_iter);
+        DCRF_LAUNCH_CHECK();
+        fetch_scalars();
+    }
+    if (energy_out) *energy_out = h_scal->energy;
+    return h_scal->steps;
+}
+
+// ---------------------------------------------------------------- LP host --
+int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve_stats* stats) {
+    require(has_unary, DCRF_E_STATE, "lp: no unary energy set");
+    const long NL = (long)N * L;
+    float* Q = buf(0);
+    float* bestQ = out;
+    float* alpha = buf(1);
+    float* u = buf(2);
+    float* sa = buf(3);
+    float* su = R > 0 ? buf(4) : nullptr;
+    float* gamma = buf(5);
+    float* curQ = buf(6);
+    float* rq = buf(7);
+    float* Y = buf(8);
+    int16_t* lab = labels.ensure(N);
+    SolverScalars* sc = scal.get();
+    double* part = partials.get();
+    const int nt = (int)terms.size();
+    const int pg = ceil_div(N, kPix);
+
+    DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    with_lc(L, [&](auto lc) {
+        constexpr int LC = decltype(lc)::value;
+        renormalize_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, Q);
+    });
+    DCRF_CUDA(cudaMemcpyAsync(bestQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    current_map(Q, lab);
+    double int_energy = energy_true(lab, true);
+    double energy = energy_lp(Q);
+    if (energy > int_energy) {
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            max_rounding_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, Q);
+        });
+        energy = energy_lp(Q);
+    }
+    double best_energy = energy, best_int_energy = int_energy;
+
+    const float lambda = p.prox_reg_const;
+    GammaConsts gc;
+    gc.lambda = lambda;
+    gc.delta = p.qp_const;
+    gc.c0 = 2 * lambda / float(L);
+    gc.c1 = (float)(1.0 / float(L));
+    gc.c2 = (float)(1 - 2.0 / float(L));
+    gc.cm = (float)(-1.0 / float(L));
+    CliqueView cv{};
+    int* upos = nullptr;
+    if (R > 0) {
+        const int* base = cl_off.get();
+        cv = CliqueView{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R, clique_max};
+        upos = ipart.ensure(2 * (size_t)R);
+    }
+
+    int it = 0, count = 0, fw_total = 0, gamma_total = 0;
+    do {
+        ++it;
+        fill_float_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, 1.0f, gamma);
+        DCRF_CUDA(cudaMemcpyAsync(curQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+        DCRF_CUDA(cudaMemsetAsync(alpha, 0, sizeof(float) * NL, stream));
+        DCRF_CUDA(cudaMemsetAsync(u, 0, sizeof(float) * NL, stream));
+        int pit = 0;
+        do {
+            ++pit;
+            with_lc(L, [&](auto lc) {
+                constexpr int LC = decltype(lc)::value;
+                lp_y_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y);
+            });
+            lp_gamma_reset_kernel<<<1, 1, 0, stream>>>(sc);
+            // qp-gamma iterations; the reference needs at least two (its first
+            // test compares against FLT_MAX), so launch in pairs and look at
+            // the stop flag after each pair.
+            int launched = 0;
+            for (;;) {
+                const int batch = std::min(2, p.qp_max_iter - launched);
+                for (int bi = 0; bi < batch; bi++) {
+                    with_lc(L, [&](auto lc) {
+                        constexpr int LC = decltype(lc)::value;
+                        lp_gamma_kernel<LC><<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, gc, Y, gamma, sc, part);
+                    });
+                    lp_gamma_check_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, p.qp_tol, sc);
+                }
+                launched += batch;
+                DCRF_LAUNCH_CHECK();
+                fetch_scalars();
+                if (h_scal->stop || launched >= p.qp_max_iter || batch <= 0) break;
+            }
+            gamma_total += h_scal->steps;
+            with_lc(L, [&](auto lc) {
+                constexpr int LC = decltype(lc)::value;
+                lp_q_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q);
+            });
+            rescale(rq, Q);
+            for (int k = 0; k < nt; k++) {
+                if (k == 0) apply_ord(k, sa, rq, nullptr, true);
+                else apply_ord(k, sa, rq, sa, false);
+            }
+            if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));
+            if (R > 0) {
+                DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
+                ucond_kernel<<<R, 256, 0, stream>>>(cl_off.get(), cl_idx.get(), L, Q, upos);
+                ucond_apply_kernel<<<1, 1, 0, stream>>>(R, upos, cl_const.get(), cl_exp.get(), su);
+            }
+            lp_gap_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, alpha, u, sa, su, Q, part);
+            finalize_sums_kernel<<<1, 64, 0, stream>>>(part, kRedBlocks, 2, 0, sc);
+            lp_delta_kernel<<<1, 1, 0, stream>>>(sc, lambda);
+            lp_alpha_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, sa, su, alpha, u, sc);
+            DCRF_LAUNCH_CHECK();
+        } while (pit < p.fw_max_iter);
+        fw_total += pit;
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            lp_project_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, Q, lab);
+        });
+        const double prev_int_energy = int_energy;
+        int_energy = energy_true(lab, true);
+        if (p.best_int) {
+            if (std::abs(int_energy - prev_int_energy) < p.prox_energy_tol) ++count;
+            else count = 0;
+            if (count >= 5) break;
+            if (int_energy < best_int_energy) {
+                DCRF_CUDA(cudaMemcpyAsync(bestQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+                best_int_energy = int_energy;
+            }
+        } else {
+            const double prev_energy = energy;
+            energy = energy_lp(Q);
+            if (std::abs(energy - prev_energy) < p.prox_energy_tol) ++count;
+            else count = 0;
+            if (count >= 5) break;
+            if (energy < best_energy) {
+                DCRF_CUDA(cudaMemcpyAsync(bestQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+                best_energy = energy;
+            }
+        }
+        if (p.less_confident_percent > 0) {
+            less_confident_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, bestQ, p.confidence_tol, part);
+            finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 0, sc);
+            fetch_scalars();
+            const double percent = h_scal->sums[0] / (double)N * 100;
+            if (percent > p.less_confident_percent) break;
+        }
+    } while (it < p.prox_max_iter);
+    sync();
+    if (stats) {
+        stats->iterations = it;
+        stats->inner_iters = fw_total;
+        stats->gamma_iters = gamma_total;
+        stats->energy = p.best_int ? best_int_energy : best_energy;
+    }
+    return it;
+}
+
+}  // namespace dcrf

@@ -1,0 +1,185 @@
+/* dcrf.h -- C ABI of the B200 dense-CRF engine (libdcrf_cuda.so).
+ *
+ * A drop-in for the hot path of densecrf_ho: the permutohedral lattice, the
+ * Potts pairwise potentials, and the qp / lp / qp_sp / lp_sp solvers.  The
+ * reference has no FFI; its boundary is its C++ class API, and every entry
+ * point below names the reference member function it replaces (file:line in
+ * the densecrf_ho tree).  A C++ shim with the reference's own class names and
+ * signatures is layered on top of this ABI (densecrf_ho_b200/cpp/).
+ *
+ * Conventions
+ *  - Every call returns a dcrf_status; dcrf_last_error() gives the message of
+ *    the last failure on the calling thread.
+ *  - Label matrices are float32 in the reference's Eigen column-major L x N
+ *    storage: element (label k, pixel i) at [i*L + k].
+ *  - Feature matrices are float32 [i*d + c] (Eigen d x N column-major).
+ *  - Functions without a suffix take HOST pointers and copy through pinned
+ *    staging buffers; *_dev variants take device pointers, run on the
+ *    handle's stream and return without synchronising.
+ *  - A handle owns one CUDA stream and its device buffers; handles are
+ *    independent, a handle is not re-entrant (like the reference objects).
+ *  - All compute runs on the device that was current when the handle was
+ *    created.  There is no CPU fallback: without a usable GPU every call
+ *    fails with DCRF_E_CUDA.
+ */
+#ifndef DCRF_H
+#define DCRF_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    DCRF_OK = 0,
+    DCRF_E_ARG = 1,     /* invalid argument / size                               */
+    DCRF_E_CUDA = 2,    /* CUDA runtime or launch failure                        */
+    DCRF_E_RANGE = 3,   /* "Value out of bounds" (src/pairwise.cpp:218-219)      */
+    DCRF_E_STATE = 4,   /* call order (e.g. solve before set_unary)              */
+    DCRF_E_NOMEM = 5,   /* device allocation failed                              */
+    DCRF_E_NUMERIC = 6, /* "Maxval < 0, skipping" (src/eigen_utils.cpp:138)      */
+    DCRF_E_TIMEOUT = 7  /* a bounded device loop hit its iteration cap           */
+} dcrf_status;
+
+typedef struct dcrf_lattice_s* dcrf_lattice;
+typedef struct dcrf_model_s* dcrf_model;
+
+const char* dcrf_last_error(void);
+/* Library version string. */
+const char* dcrf_version(void);
+
+/* ------------------------------------------------------------------------
+ * Permutohedral lattice -- class Permutohedral (include/permutohedral.h:50-88)
+ * ---------------------------------------------------------------------- */
+
+/* Permutohedral::Permutohedral() (src/permutohedral.cpp:139). */
+dcrf_status dcrf_lattice_create(dcrf_lattice* out);
+/* Permutohedral::~Permutohedral() (src/permutohedral.cpp:142). */
+dcrf_status dcrf_lattice_destroy(dcrf_lattice lat);
+/* Permutohedral::init(const MatrixXf& features) (src/permutohedral.cpp:152):
+ * features [N][d], 1 <= d <= 16. */
+dcrf_status dcrf_lattice_init(dcrf_lattice lat, const float* features, int d, int N);
+dcrf_status dcrf_lattice_init_dev(dcrf_lattice lat, const float* d_features, int d, int N);
+/* M_ (number of lattice vertices), N_ and d_. */
+dcrf_status dcrf_lattice_info(dcrf_lattice lat, int* M, int* N, int* d);
+/* Permutohedral::compute(MatrixXf& out, const MatrixXf& in, bool reverse)
+ * (src/permutohedral.cpp:1079-1087): out = alpha S^T B S in, in/out [N][L]. */
+dcrf_status dcrf_lattice_compute(dcrf_lattice lat, float* out, const float* in, int L, int reverse);
+dcrf_status dcrf_lattice_compute_dev(dcrf_lattice lat, float* d_out, const float* d_in, int L,
+                                     int reverse);
+/* Permutohedral::compute_upper_minus_lower_ord(MatrixXf& out, const MatrixXf& Q)
+ * (src/permutohedral.cpp:1071-1073, 590-701): the 10-bin ordered filter. */
+dcrf_status dcrf_lattice_compute_ord(dcrf_lattice lat, float* out, const float* Q, int L);
+dcrf_status dcrf_lattice_compute_ord_dev(dcrf_lattice lat, float* d_out, const float* d_Q, int L);
+/* Read back the lattice tables for parity checks (host buffers, any may be
+ * NULL): offset/rank/bary [N*(d+1)] (offset_, rank_, barycentric_), keys
+ * [M*d] int16 in vertex-id order, nbr [(d+1)*M*2] = blur_neighbors_ (n1, n2),
+ * -1 where the neighbour is absent. */
+dcrf_status dcrf_lattice_export(dcrf_lattice lat, int32_t* offset, int32_t* rank, float* bary,
+                                int16_t* keys, int32_t* nbr);
+/* The stream the lattice's work is queued on (a cudaStream_t). */
+dcrf_status dcrf_lattice_stream(dcrf_lattice lat, void** stream);
+
+/* ------------------------------------------------------------------------
+ * Dense CRF model -- class DenseCRF / DenseCRF2D (include/densecrf.h:73-194)
+ * ---------------------------------------------------------------------- */
+
+/* LP_inf_params (include/densecrf.h:43-69); dcrf_lp_params_default() gives
+ * the reference defaults of LP_inf_params() (src/densecrf.cpp:287-302). */
+typedef struct {
+    float prox_reg_const;
+    float dual_gap_tol;
+    float prox_energy_tol;
+    int prox_max_iter;
+    int fw_max_iter;
+    int qp_max_iter;
+    float qp_tol;
+    float qp_const;
+    int best_int;
+    int accel_prox;
+    int work_set_size;
+    int approx_fw_iter;
+    float less_confident_percent;
+    float confidence_tol;
+} dcrf_lp_params;
+void dcrf_lp_params_default(dcrf_lp_params* p);
+
+typedef struct {
+    /* 0: the reference stop rule, iterate while the energy decreases by more
+     * than 100 (src/densecrf.cpp:390, DIFF_ENG).  n > 0: at most n
+     * Frank-Wolfe steps (the loop still ends when the step numerator or
+     * denominator is exactly zero, src/densecrf.cpp:419). */
+    int max_iter;
+} dcrf_qp_params;
+
+typedef struct {
+    int iterations;   /* QP: Frank-Wolfe steps taken; LP: proximal iterations */
+    int inner_iters;  /* LP: total Frank-Wolfe (dual) iterations              */
+    int gamma_iters;  /* LP: total qp-gamma iterations                        */
+    double energy;    /* QP: last relaxed energy; LP: best integer energy     */
+} dcrf_solve_stats;
+
+/* DenseCRF2D(int W, int H, int M) (src/densecrf.cpp:149). */
+dcrf_status dcrf_model_create(dcrf_model* out, int W, int H, int L);
+/* ~DenseCRF (src/densecrf.cpp:141-148). */
+dcrf_status dcrf_model_destroy(dcrf_model m);
+/* setUnaryEnergy(const MatrixXf& unary) (src/densecrf.cpp:261): U [N][L]. */
+dcrf_status dcrf_model_set_unary(dcrf_model m, const float* unary);
+dcrf_status dcrf_model_set_unary_dev(dcrf_model m, const float* d_unary);
+/* addPairwiseGaussian(sx, sy, new PottsCompatibility(w)) (src/densecrf.cpp:170). */
+dcrf_status dcrf_model_add_gaussian(dcrf_model m, float sx, float sy, float w_potts);
+/* addPairwiseBilateral(sx, sy, sr, sg, sb, im, new PottsCompatibility(w))
+ * (src/densecrf.cpp:179); rgb is the uint8 [H][W][3] image. */
+dcrf_status dcrf_model_add_bilateral(dcrf_model m, float sx, float sy, float sr, float sg,
+                                     float sb, const uint8_t* rgb, float w_potts);
+/* addPairwiseEnergy(features, new PottsCompatibility(w), DIAG_KERNEL,
+ * NORMALIZE_SYMMETRIC) (src/densecrf.cpp:157-169); features [N][d]. */
+dcrf_status dcrf_model_add_pairwise(dcrf_model m, const float* features, int d, float w_potts);
+/* The clique state that addSuperPixel (src/densecrf.cpp:193-251) leaves in
+ * super_pixel_container_, exp_of_superpixels_ and constants_, supplied
+ * directly: R cliques, pixel ids idx[offsets[r] .. offsets[r+1]), their
+ * weights exp_weight[r] and LP constants[r].  Replaces any earlier cliques. */
+dcrf_status dcrf_model_set_cliques(dcrf_model m, int R, const int32_t* offsets,
+                                   const int32_t* idx, const float* exp_weight,
+                                   const float* constants);
+/* unary_init() (src/densecrf.cpp:321-336): softmax of -U, [N][L]. */
+dcrf_status dcrf_model_unary_init(dcrf_model m, float* Q);
+/* pairwise_[k]->apply(out, in) (src/pairwise.cpp:203-208); nonorm selects the
+ * NO_NORMALIZATION copy no_norm_pairwise_[k] (src/densecrf.cpp:161-169). */
+dcrf_status dcrf_model_pairwise_apply(dcrf_model m, int k, int nonorm, float* out, const float* in);
+dcrf_status dcrf_model_pairwise_apply_dev(dcrf_model m, int k, int nonorm, float* d_out,
+                                          const float* d_in);
+/* pairwise_[k]->apply_upper_minus_lower_ord(out, Q) (src/pairwise.cpp:214-228);
+ * fails with DCRF_E_RANGE when Q leaves [0, 1]. */
+dcrf_status dcrf_model_pairwise_apply_ord(dcrf_model m, int k, float* out, const float* Q);
+/* qp_inference_super_pixels_non_convex(init) (src/densecrf.cpp:340-442);
+ * runs qp or, when cliques are set, qp_sp.  params/stats may be NULL. */
+dcrf_status dcrf_model_qp(dcrf_model m, const float* init, float* out,
+                          const dcrf_qp_params* params, dcrf_solve_stats* stats);
+dcrf_status dcrf_model_qp_dev(dcrf_model m, const float* d_init, float* d_out,
+                              const dcrf_qp_params* params, dcrf_solve_stats* stats);
+/* lp_inference_prox_super_pixels(init, params) (src/densecrf.cpp:526-799);
+ * lp or, when cliques are set, lp_sp.  params NULL = reference defaults. */
+dcrf_status dcrf_model_lp(dcrf_model m, const float* init, float* out,
+                          const dcrf_lp_params* params, dcrf_solve_stats* stats);
+dcrf_status dcrf_model_lp_dev(dcrf_model m, const float* d_init, float* d_out,
+                              const dcrf_lp_params* params, dcrf_solve_stats* stats);
+/* currentMap(Q) (src/densecrf.cpp:929-938): first arg-max per pixel. */
+dcrf_status dcrf_model_current_map(dcrf_model m, const float* Q, int16_t* labels);
+/* assignment_energy_true(l) (src/densecrf.cpp:873-885). */
+dcrf_status dcrf_model_energy_true(dcrf_model m, const int16_t* labels, double* energy);
+/* assignment_energy_higher_order(l) (src/densecrf.cpp:844-870). */
+dcrf_status dcrf_model_energy_ho(dcrf_model m, const int16_t* labels, double* energy);
+/* compute_energy_LP_higher_order(Q) (src/densecrf.cpp:982-1037). */
+dcrf_status dcrf_model_energy_lp(dcrf_model m, const float* Q, double* energy);
+/* compute_LR_QP_value(Q, 0) (src/densecrf.cpp:940-957). */
+dcrf_status dcrf_model_lr_qp_value(dcrf_model m, const float* Q, double* energy);
+/* Number of pairwise terms, and vertex count of term k's lattice. */
+dcrf_status dcrf_model_info(dcrf_model m, int* n_terms, int* N, int* L);
+dcrf_status dcrf_model_lattice_size(dcrf_model m, int k, int* M);
+dcrf_status dcrf_model_stream(dcrf_model m, void** stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DCRF_H */

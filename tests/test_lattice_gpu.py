@@ -1,0 +1,110 @@
+"""CUDA lattice vs the oracle and the reference's golden vectors.
+
+Lattice tables (vertex count M, offsets, ranks, barycentric weights, keys,
+neighbours) and filter outputs are required to be BIT-EXACT: the CUDA path
+reproduces the reference's float operation order and the splat gathers in
+the order the reference's scatter accumulates.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, golden_names
+from densecrf_ho_b200 import Permutohedral, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _eq(a, b):
+    return np.array_equal(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.parametrize("name", golden_names("lattice_"))
+def test_lattice_matches_reference_golden(name):
+    g = golden(name)
+    for t in ("g", "b"):
+        lat = Permutohedral().init(g[f"{t}_f"])
+        ex = lat.export()
+        assert ex["M"] == int(g[f"{t}_M"])
+        for k in ("offset", "rank", "bary", "nbr"):
+            assert _eq(ex[k], g[f"{t}_{k}"]), (name, t, k)
+        assert _eq(lat.compute(g["x"]), g[f"{t}_compute"])
+        assert _eq(lat.compute(g["x"], reverse=True), g[f"{t}_compute_rev"])
+        assert _eq(lat.compute(g["x1"]), g[f"{t}_compute_l1"])
+        assert _eq(lat.compute_upper_minus_lower_ord(g["x"]), g[f"{t}_ord"])
+
+
+CASES = [(1, 1), (3, 1), (5, 3), (17, 13), (64, 48), (97, 61), (160, 120)]
+
+
+@pytest.mark.parametrize("W,H", CASES)
+@pytest.mark.parametrize("kind", ["gauss", "bilat"])
+def test_lattice_tables_bit_exact(W, H, kind, oracle_mod):
+    img = synth.make_image(W, H, 21, W * 31 + H)
+    f = (synth.gaussian_features(W, H, 3, 3) if kind == "gauss"
+         else synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"]))
+    a = Permutohedral().init(f).export()
+    b = oracle_mod.OracleLattice(f).export()
+    assert a["M"] == b["M"]
+    for k in ("offset", "rank", "bary", "keys", "nbr"):
+        assert _eq(a[k], b[k]), k
+
+
+@pytest.mark.parametrize("d", [1, 3, 4, 7, 9])
+def test_lattice_other_dimensions(d, oracle_mod):
+    rng = np.random.default_rng(d)
+    N = 1001
+    f = (rng.random((N, d)) * 6).astype(np.float32)
+    lat = Permutohedral().init(f)
+    a, b = lat.export(), oracle_mod.OracleLattice(f).export()
+    assert a["M"] == b["M"]
+    for k in ("offset", "rank", "bary", "keys", "nbr"):
+        assert _eq(a[k], b[k]), k
+    x = rng.random((N, 5)).astype(np.float32)
+    assert _eq(lat.compute(x), oracle_mod.OracleLattice(f).compute(x))
+
+
+@pytest.mark.parametrize("L", [1, 2, 3, 21, 33])
+def test_filter_bit_exact(L, oracle_mod):
+    W, H = 80, 60
+    img = synth.make_image(W, H, 21, 7)
+    for f in (synth.gaussian_features(W, H, 3, 3),
+              synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])):
+        lat, orc = Permutohedral().init(f), oracle_mod.OracleLattice(f)
+        x = np.random.default_rng(L).standard_normal((W * H, L)).astype(np.float32)
+        assert _eq(lat.compute(x), orc.compute(x))
+        assert _eq(lat.compute(x, reverse=True), orc.compute(x, True))
+        q = np.random.default_rng(L + 1).random((W * H, L)).astype(np.float32)
+        q[::7] = 0.0
+        q[::11] = 1.0
+        assert _eq(lat.compute_upper_minus_lower_ord(q), orc.compute_ord(q))
+
+
+def test_filter_error_vs_fp64_oracle(oracle_mod):
+    """Relative error of the FP32 filter against the FP64 lattice oracle."""
+    W, H = 160, 120
+    img = synth.make_image(W, H, 21, 3)
+    f = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    x = np.random.default_rng(0).random((W * H, 21)).astype(np.float32)
+    out = Permutohedral().init(f).compute(x)
+    ref64 = oracle_mod.OracleLattice(f).compute_f64(x.astype(np.float64))
+    rel = np.linalg.norm(out - ref64) / np.linalg.norm(ref64)
+    assert rel < 1e-6, rel
+
+
+def test_full_size_properties(oracle_mod):
+    """640x480: M and the tables of both lattices match the oracle; the filter
+    is linear (K(a x + y) = a K x + K y to float accuracy) and deterministic."""
+    W, H = 640, 480
+    img = synth.make_image(W, H, 21, 1)
+    f = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    lat = Permutohedral().init(f)
+    a, b = lat.export(), oracle_mod.OracleLattice(f).export()
+    assert a["M"] == b["M"]
+    for k in ("offset", "bary", "nbr"):
+        assert _eq(a[k], b[k])
+    rng = np.random.default_rng(2)
+    x = rng.random((W * H, 21)).astype(np.float32)
+    y = rng.random((W * H, 21)).astype(np.float32)
+    kx, ky, kxy = lat.compute(x), lat.compute(y), lat.compute(2 * x + y)
+    assert np.linalg.norm(kxy - (2 * kx + ky)) / np.linalg.norm(kxy) < 1e-6
+    assert _eq(lat.compute(x), kx)

@@ -1,0 +1,111 @@
+"""The CPU oracle (our C restatement) pinned against the reference.
+
+Every check is bit-exact (``np.array_equal``): the restatement follows the
+reference's float operation order, including Eigen's SSE2 reduction order.
+Only ``unary_init`` differs (the reference evaluates exp with Eigen's packet
+polynomial): there the bound is 8 ulp.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden, golden_names
+from densecrf_ho_b200 import synth
+
+LAT = golden_names("lattice_")
+MOD = golden_names("model_")
+
+
+def _bits_equal(a, b):
+    return np.array_equal(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.parametrize("name", LAT)
+def test_lattice_pinned_to_golden(name, oracle_mod):
+    g = golden(name)
+    for t in ("g", "b"):
+        lat = oracle_mod.OracleLattice(g[f"{t}_f"])
+        ex = lat.export()
+        assert ex["M"] == int(g[f"{t}_M"])
+        for k in ("offset", "rank", "bary", "nbr"):
+            assert _bits_equal(ex[k], g[f"{t}_{k}"]), (name, t, k)
+        assert _bits_equal(lat.compute(g["x"]), g[f"{t}_compute"])
+        assert _bits_equal(lat.compute(g["x"], True), g[f"{t}_compute_rev"])
+        assert _bits_equal(lat.compute(g["x1"]), g[f"{t}_compute_l1"])
+        assert _bits_equal(lat.compute_ord(g["x"]), g[f"{t}_ord"])
+
+
+def _oracle_model(O, g):
+    img = dict(W=int(g["W"]), H=int(g["H"]), L=21, rgb=g["rgb"], unary=g["unary"])
+    m = O.build_model(O.OracleModel, img)
+    if "cl_off" in g:
+        m.set_cliques(g["cl_off"], g["cl_idx"], g["cl_exp"], g["cl_const"])
+    return m
+
+
+@pytest.mark.parametrize("name", MOD)
+def test_model_pinned_to_golden(name, oracle_mod):
+    g = golden(name)
+    m = _oracle_model(oracle_mod, g)
+    Q = g["unary_init"]  # the reference's own initialisation
+    ulp = np.abs(m.unary_init().view(np.int32) - Q.view(np.int32)).max()
+    assert ulp <= 8  # expf vs Eigen's packet exp, then one division
+    rq = (Q - Q.min()) / (Q - Q.min()).max()
+    for k in range(2):
+        assert _bits_equal(m.apply(k, Q), g[f"apply{k}"])
+        assert _bits_equal(m.apply(k, Q, True), g[f"apply{k}_nonorm"])
+        assert _bits_equal(m.apply_ord(k, rq), g[f"ord{k}"])
+    lab = m.current_map(Q)
+    assert _bits_equal(lab, g["map"])
+    assert m.energy_true(lab) == float(g["e_true"])
+    assert m.energy_ho(lab) == float(g["e_ho"])
+    assert m.energy_lp(Q) == float(g["e_lp"])
+    assert m.lr_qp_value(Q) == float(g["e_lrqp"])
+    assert _bits_equal(m.qp(Q)[0], g["qp"])
+    q100, it, en = m.qp(Q, 100)
+    assert it == int(g["qp100_iters"])
+    assert _bits_equal(q100, g["qp100"])
+    assert _bits_equal(en, g["qp100_energies"])
+    out, _ = m.lp(Q, prox_max_iter=4, fw_max_iter=4)
+    assert _bits_equal(out, g["lp"])
+
+
+def test_oracle_f64_filter_close_to_f32(oracle_mod):
+    """The FP64 lattice oracle agrees with the FP32 filter to float accuracy."""
+    W, H = 40, 30
+    img = synth.make_image(W, H, 21, 5)
+    f = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    lat = oracle_mod.OracleLattice(f)
+    x = np.random.default_rng(1).random((W * H, 21)).astype(np.float32)
+    a = lat.compute(x)
+    b = lat.compute_f64(x.astype(np.float64))
+    assert np.abs(a - b).max() / np.abs(b).max() < 1e-5
+
+
+@pytest.mark.skipif("not __import__('oracle.oracle', fromlist=['x']).reference_available()")
+@pytest.mark.parametrize("W,H,seed", [(37, 23, 1), (64, 48, 2), (33, 31, 3)])
+def test_oracle_matches_reference_live(W, H, seed, oracle_mod):
+    """Fresh seeded cases against the compiled reference (this container only)."""
+    O = oracle_mod
+    img = synth.make_image(W, H, 21, seed)
+    for f in (synth.gaussian_features(W, H, 3, 3),
+              synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])):
+        a, b = O.OracleLattice(f).export(), O.ReferenceLattice(f).export()
+        assert a["M"] == b["M"]
+        for k in ("offset", "rank", "bary", "nbr"):
+            assert np.array_equal(a[k], b[k])
+    mo = O.build_model(O.OracleModel, img)
+    mr = O.build_model(O.ReferenceModel, img)
+    Q = mr.unary_init()
+    assert np.array_equal(mo.qp(Q)[0], mr.qp(Q)[0])
+    assert np.array_equal(mo.lp(Q, prox_max_iter=3, fw_max_iter=3)[0],
+                          mr.lp(Q, prox_max_iter=3, fw_max_iter=3)[0])
+
+
+def test_apply_ord_rejects_out_of_range(oracle_mod):
+    """apply_upper_minus_lower_ord throws "Value out of bounds" outside [0, 1]."""
+    img = synth.make_image(16, 12, 21, 0)
+    m = oracle_mod.build_model(oracle_mod.OracleModel, img)
+    bad = np.full((16 * 12, 21), 0.5, np.float32)
+    bad[3, 4] = 1.5
+    with pytest.raises(RuntimeError, match="Value out of bounds"):
+        m.apply_ord(0, bad)
