@@ -1,0 +1,442 @@
+#!/usr/bin/env python
+"""Benchmark of the dense-CRF hot path on B200 (one JSON line on stdout).
+
+Workload (default ``--workload lp``): the proximal LP solve
+``lp_inference_prox_super_pixels`` on a 640x480 image with 21 labels, a
+Gaussian (sxy=3, w=3) and a bilateral (sxy=50, srgb=15, w=5) Potts term,
+LP_inf_params() defaults with prox_max_iter=50 and prox_energy_tol =
+dual_gap_tol (as the reference CLI sets it).  Input: seeded synthetic Voronoi
+image + unaries (densecrf_ho_b200.synth).  One step = one LP solve.
+
+  value        solves/s with init / output resident in HBM (dcrf_model_lp_dev)
+  e2e          solves/s through the host-buffer C-ABI call dcrf_model_lp, i.e.
+               with the H2D copy of the initial Q and the D2H copy of the result
+               inside every step
+  roofline     the LP's dominant operation, the 10-bin ordered lattice filter
+               (splat + d+1 blur passes + slice), timed alone with CUDA events on
+               the library's stream, against the measured HBM copy bandwidth
+  cpu_baseline the reference itself (oracle/_ref, compiled from its sources) on
+               the host cores: a bounded sample (one proximal iteration) scaled
+               to a full solve
+
+``--impl reference`` times the reference alone, on all usable host cores.
+Under torchrun (N > 1) every rank solves its own image (replicas, no
+collective on the data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from densecrf_ho_b200 import synth  # noqa: E402
+
+L = 21
+GAUSS = (3.0, 3.0)                # sxy, w
+BILAT = (50.0, 15.0, 5.0)         # sxy, srgb, w
+LP_OVERRIDES = dict(prox_max_iter=50, prox_energy_tol=1e3)
+# Proximal iterations the reference's LP runs on the default image (640x480,
+# seed 2) before its |dE| < prox_energy_tol five-times stop rule fires,
+# counted with the bit-exact CPU restatement (oracle/dcrf_oracle.c).  Used only
+# by --impl reference to scale its one-iteration sample to a full solve; the
+# GPU arm reports its own count (which matches).
+REF_PROX_ITERS = {(640, 480, 2): 50}
+ROOFLINE_TRAFFIC = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--size", default="640x480")
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--prox-iters", type=int, default=50,
+                    help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
+    return ap.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def workload_name(W, H):
+    return (f"lp_inference_prox_super_pixels {W}x{H} L={L}, Potts gaussian sxy={GAUSS[0]} w={GAUSS[1]} "
+            f"+ bilateral sxy={BILAT[0]} srgb={BILAT[1]} w={BILAT[2]}, prox_max_iter=50, "
+            f"prox_energy_tol=1e3")
+
+
+def ord_filter_bytes(N, M, d, Lv=L, R=10):
+    """Algorithmic bytes of one 10-bin ordered filter call:
+    N (8L + 16(d+1)) + 2 M (8 R L + (d+1) (8 R L + 8))."""
+    return N * (8 * Lv + 16 * (d + 1)) + 2 * M * (8 * R * Lv + (d + 1) * (8 * R * Lv + 8))
+
+
+def filter_bytes(N, M, d, Lv=L):
+    """Algorithmic bytes of one splat/blur/slice call:
+    N (8L + 16(d+1) + 8) + M (8L + (d+1)(8L + 8))."""
+    return N * (8 * Lv + 16 * (d + 1) + 8) + M * (8 * Lv + (d + 1) * (8 * Lv + 8))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks --
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            if len(r) >= 9:
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------ reference on CPU --
+def _ref_worker(args):
+    """Times the reference LP on one core: t_call for prox_max_iter=1 (one
+    proximal iteration of fw Frank-Wolfe steps), and the per-call overheads it
+    contains: t_init (the energy evaluations done before the first
+    iteration) and t_proj (the integer energy after each iteration)."""
+    W, H, seed, fw, reps, barrier = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    use_ref = O.reference_available()
+    cls = O.ReferenceModel if use_ref else O.OracleModel
+    img = synth.make_image(W, H, L, seed)
+    m = O.build_model(cls, img, gaussian=GAUSS, bilateral=BILAT)
+    Q = m.unary_init()
+    t0 = time.perf_counter()
+    lab = m.current_map(Q)
+    m.energy_lp(Q)
+    m.energy_ho(lab)
+    t_init = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    m.energy_ho(lab)
+    t_proj = time.perf_counter() - t0
+    times = []
+    for _ in range(reps):
+        if barrier is not None:
+            barrier.wait()
+        t0 = time.perf_counter()
+        m.lp(Q, prox_max_iter=1, fw_max_iter=fw, prox_energy_tol=1e3)
+        times.append(time.perf_counter() - t0)
+    return dict(t_init=t_init, t_proj=t_proj, times=times, kind="reference" if use_ref else "port")
+
+
+def solve_time_from_sample(t_call, t_init, t_proj, fw, n_prox, fw_full=10):
+    """Full-solve time from a one-iteration sample: one init, then n_prox
+    proximal iterations of fw_full Frank-Wolfe steps and one projection."""
+    t_fw = max(t_call - t_init - t_proj, 1e-9) / fw
+    return t_init + n_prox * (fw_full * t_fw + t_proj)
+
+
+def cpu_reference(W, H, seed, n_prox, workers, fw, reps):
+    ctx = mp.get_context("spawn")
+    if workers == 1:
+        res = [_ref_worker((W, H, seed, fw, reps, None))]
+    else:
+        barrier = ctx.Manager().Barrier(workers)
+        with ctx.Pool(workers) as pool:
+            res = pool.map(_ref_worker, [(W, H, seed, fw, reps, barrier)] * workers)
+    per_rep = [max(r["times"][i] for r in res) for i in range(reps)]
+    t_init = statistics.median(r["t_init"] for r in res)
+    t_proj = statistics.median(r["t_proj"] for r in res)
+    solve_s = [solve_time_from_sample(t, t_init, t_proj, fw, n_prox) for t in per_rep]
+    return dict(kind=res[0]["kind"], per_rep=per_rep, solve_s=solve_s, t_init=t_init, t_proj=t_proj)
+
+
+def usable_cores():
+    n = os.cpu_count() or 1
+    try:
+        n = len(os.sched_getaffinity(0))
+    except Exception:
+        pass
+    avail_gb = 64.0
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable"):
+                    avail_gb = int(ln.split()[1]) / 2**20
+    except Exception:
+        pass
+    return max(1, min(n, int(avail_gb / 2.0), 64))
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return
+    W, H = map(int, args.size.split("x"))
+    n_prox = REF_PROX_ITERS.get((W, H, args.seed))
+    if n_prox is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"no proximal-iteration count recorded for {W}x{H} seed {args.seed}"}))
+        return
+    workers = usable_cores()
+    steps = args.steps + args.warmup
+    fw = max(1, min(10, int(round(10 * 12 / max(steps, 1)))))
+    r = cpu_reference(W, H, args.seed, n_prox, workers, fw, steps)
+    timed = r["solve_s"][args.warmup:] or r["solve_s"]
+    per_solve = statistics.mean(timed)
+    value = workers / per_solve
+    sample = (f"{workers} concurrent single-threaded solves; each step times one proximal iteration "
+              f"({fw} Frank-Wolfe steps, prox_max_iter=1) of the reference LP and scales it to a full "
+              f"solve of {n_prox} proximal x 10 Frank-Wolfe iterations (init {r['t_init']:.2f} s and "
+              f"per-iteration projection {r['t_proj']:.2f} s measured separately)")
+    line = {"metric": "LP solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3 / workers,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_name(W, H), "global_batch": workers,
+                       "parallelism": f"{workers} host processes"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": r["kind"],
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ ours --
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from densecrf_ho_b200 import DenseCRF2D, LPParams, Permutohedral, SolveStats, lib, check
+
+    rank, local, world = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    W, H = map(int, args.size.split("x"))
+    N = W * H
+    seed = args.seed + rank
+    img = synth.make_image(W, H, L, seed)
+    t0 = time.perf_counter()
+    crf = DenseCRF2D(W, H, L)
+    crf.setUnaryEnergy(img["unary"])
+    crf.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+    crf.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"], BILAT[2])
+    Q0 = crf.unary_init()
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    params = LPParams.default()
+    for k, v in LP_OVERRIDES.items():
+        setattr(params, k, v)
+    params.prox_max_iter = args.prox_iters
+    Ls = lib()
+    sptr = C.c_void_p()
+    check(Ls.dcrf_model_stream(crf.handle, C.byref(sptr)))
+    stream = torch.cuda.ExternalStream(sptr.value)
+    init_d = torch.from_numpy(Q0).cuda()
+    out_d = torch.empty_like(init_d)
+    st = SolveStats()
+
+    def step_dev():
+        check(Ls.dcrf_model_lp_dev(crf.handle, C.c_void_p(init_d.data_ptr()), C.c_void_p(out_d.data_ptr()),
+                                   C.byref(params), C.byref(st)))
+
+    for _ in range(args.warmup):
+        step_dev()
+    torch.cuda.synchronize()
+
+    def timed(fn, k):
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    l0 = Ls.dcrf_kernel_launches()
+    ms = timed(step_dev, args.steps)
+    launches = Ls.dcrf_kernel_launches() - l0
+    clk = clocks.stop()
+    prox_iters, fw_iters, gamma_iters = st.iterations, st.inner_iters, st.gamma_iters
+    value = world * args.steps / (ms / 1e3)
+
+    # e2e: the host-buffer C-ABI call, pinned host input and output.
+    init_h = torch.from_numpy(Q0).pin_memory()
+    out_h = torch.empty_like(init_h).pin_memory()
+
+    def step_host():
+        check(Ls.dcrf_model_lp(crf.handle, C.c_void_p(init_h.data_ptr()), C.c_void_p(out_h.data_ptr()),
+                               C.byref(params), C.byref(st)))
+
+    step_host()
+    ms_e2e = timed(step_host, args.steps)
+    e2e_value = world * args.steps / (ms_e2e / 1e3)
+    same = bool(torch.equal(out_h, out_d.cpu()))
+
+    # Roofline of the dominant operation: the ordered filter on the model's
+    # bilateral and Gaussian lattices (separate Permutohedral objects with the
+    # same features), timed with events on the lattice's own stream.
+    peak, peak_kind = measured_peaks()
+    roof = {}
+    rq = torch.rand((N, L), device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    ro = torch.empty_like(rq)
+    feats = {"bilateral": synth.bilateral_features(W, H, BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
+                                                   img["rgb"]),
+             "gaussian": synth.gaussian_features(W, H, GAUSS[0], GAUSS[0])}
+    reps = 20
+    for name, f in feats.items():
+        lat = Permutohedral().init(f)
+        lptr = C.c_void_p()
+        check(Ls.dcrf_lattice_stream(lat._h, C.byref(lptr)))
+        ls = torch.cuda.ExternalStream(lptr.value)
+        run = lambda: check(Ls.dcrf_lattice_compute_ord_dev(lat._h, C.c_void_p(ro.data_ptr()),
+                                                            C.c_void_p(rq.data_ptr()), L))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ls)
+        for _ in range(reps):
+            run()
+        e1.record(ls)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / reps / 1e3
+        ab = ord_filter_bytes(N, lat.M, lat.d)
+        roof[name] = dict(M=lat.M, d=lat.d, seconds=t, bytes=ab, gbs=ab / t / 1e9)
+        # plain splat/blur/slice filter for the secondary lattice-filter metric
+        x = torch.rand((N, L), device="cuda")
+        y = torch.empty_like(x)
+        runp = lambda: check(Ls.dcrf_lattice_compute_dev(lat._h, C.c_void_p(y.data_ptr()),
+                                                          C.c_void_p(x.data_ptr()), L, 0))
+        for _ in range(3):
+            runp()
+        torch.cuda.synchronize()
+        e0.record(ls)
+        for _ in range(reps):
+            runp()
+        e1.record(ls)
+        torch.cuda.synchronize()
+        tp = e0.elapsed_time(e1) / reps / 1e3
+        fb = filter_bytes(N, lat.M, lat.d)
+        roof[name].update(filter_seconds=tp, filter_bytes=fb, filter_gbs=fb / tp / 1e9,
+                          filter_gpix_label_s=N * L / tp / 1e9)
+        del lat
+    dom = roof["bilateral"]
+    traffic = None
+    if os.path.exists(ROOFLINE_TRAFFIC):
+        with open(ROOFLINE_TRAFFIC) as f:
+            tr = json.load(f)
+        traffic = tr.get("ord_filter_bytes_per_call", {}).get(f"{W}x{H}")
+    roofline = {"bound": "hbm", "achieved": dom["gbs"], "peak": peak, "unit": "GB/s",
+                "frac": dom["gbs"] / peak, "traffic": traffic,
+                "kernel": f"ordered lattice filter, bilateral d=5 lattice (M={dom['M']}), {W}x{H}, L={L}",
+                "peak_kind": peak_kind,
+                "gaussian_d2": {"M": roof["gaussian"]["M"], "gbs": roof["gaussian"]["gbs"],
+                                "frac": roof["gaussian"]["gbs"] / peak}}
+
+    line = {"metric": "LP solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Voronoi image + -log softmax unaries)",
+            "config": {"workload": workload_name(W, H), "global_batch": world,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "solver state ~12 x N x L x 4 B = 310 MB > 126 MB L2; no flush needed",
+                       "prox_iters": prox_iters, "fw_iters": fw_iters, "gamma_iters": gamma_iters},
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": N * L * 4,
+                    "d2h_bytes_per_step": N * L * 4, "output_matches_device_path": same},
+            "clocks": clk, "gpu_launches": int(launches),
+            "extra": {"setup_ms": setup_ms,
+                      "lattice_filter_gpix_label_s": {k: v["filter_gpix_label_s"] for k, v in roof.items()},
+                      "lattice_filter_gbs": {k: v["filter_gbs"] for k, v in roof.items()},
+                      "ord_filter_ms": {k: v["seconds"] * 1e3 for k, v in roof.items()}}}
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference(W, H, args.seed, prox_iters, 1, 10, 1)
+        v = 1.0 / r["solve_s"][0]
+        line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": 1, "kind": r["kind"],
+                                "sample": (f"one proximal iteration (prox_max_iter=1, 10 Frank-Wolfe steps) of "
+                                           f"the reference LP on 1 core, {r['per_rep'][0]:.1f} s, scaled to "
+                                           f"{prox_iters} iterations (init {r['t_init']:.2f} s, projection "
+                                           f"{r['t_proj']:.2f} s per iteration)")}
+    if rank == 0:
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -66,6 +66,9 @@ def lib():
                     fn.argtypes = []
                 elif name == "dcrf_lp_params_default":
                     fn.restype = None
+                elif name == "dcrf_kernel_launches":
+                    fn.restype = C.c_ulonglong
+                    fn.argtypes = []
                 else:
                     fn.restype = C.c_int
             _lib = L

@@ -9,6 +9,8 @@
 using dcrf::DevBuf;
 using dcrf::Error;
 
+std::atomic<unsigned long long> dcrf::g_kernel_launches{0};
+
 struct dcrf_lattice_s {
     dcrf::Lattice lat;
     cudaStream_t stream = nullptr;
@@ -82,6 +84,7 @@ extern "C" {
 
 const char* dcrf_last_error(void) { return g_err.c_str(); }
 const char* dcrf_version(void) { return "dcrf-b200 0.1 (sm_100a)"; }
+unsigned long long dcrf_kernel_launches(void) { return dcrf::g_kernel_launches.load(); }
 
 void dcrf_lp_params_default(dcrf_lp_params* p) {
     if (!p) return;

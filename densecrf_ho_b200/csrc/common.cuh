@@ -4,9 +4,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 #include "dcrf.h"
 
@@ -59,6 +61,18 @@ struct DevBuf {
 };
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Process-wide count of kernels this library has launched (benchmarks read
+// it through dcrf_kernel_launches()).
+extern std::atomic<unsigned long long> g_kernel_launches;
+
+// Every kernel of the library is launched through here.
+template <typename... KArgs, typename... Args>
+inline void launch(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                   Args&&... args) {
+    kernel<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+    g_kernel_launches.fetch_add(1, std::memory_order_relaxed);
+}
 
 // Number of SMs of the current device (cached per process; one device per
 // process is the supported deployment).

@@ -33,6 +33,12 @@ namespace {
 constexpr int kEmpty = -1;
 constexpr int kRes = 10;       // RESOLUTION (include/permutohedral.h:41)
 constexpr int kOrdW = 2 * kRes;  // lower + upper bins per (vertex, label)
+constexpr int kStageWarps = 4;   // warps (splat lists) per splat block
+constexpr int kStages = 4;       // shared-memory ring depth, in chunks
+constexpr int kChunk = 16;       // entries per chunk (8.5 KB of ring per warp: 24 warps / SM)
+constexpr int kMaxOrderKey = (1 << 24) - 1;
+constexpr int kLongList = 64;    // lists longer than this use the staged warp kernels
+constexpr int kTB = 256;         // threads per block of the element-wise kernels
 
 template <int KW>
 struct Key {
@@ -303,16 +309,120 @@ __global__ void seg_fill_kernel(int E, int d1, const int* __restrict__ sorted_en
 // Splat as a gather: value(v, k) = sum over v's entries, in entry order, of
 // w * in[p][k] (times the symmetric normalisation when pre_norm is given,
 // which DenseKernel::filter applies before the lattice, src/pairwise.cpp:61).
+//
+// One warp per vertex, lanes = labels (in chunks of 32).  The sum must stay
+// sequential in entry order to reproduce the reference's scatter, so each
+// lane's float adds form one dependent chain; everything else is kept off
+// that chain.  The list is streamed in chunks of 32 entries through a ring
+// of kStages shared-memory buffers with cp.async: while chunk c is summed,
+// chunks c+1 .. c+kStages-1 (up to 96 entries x L values, plus their weights
+// and normalisation factors) are in flight, so a single long list is not
+// serialised on L2 latency.  Vertices are visited longest list first
+// (`order`) so the few very long lists of a coarse lattice start early.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(sdst)), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// Streams the list [s0, s1) of one vertex through the per-warp ring:
+// `vals_of(slot, e)` is this lane's staged word for entry e, and
+// consume(slot, n) is called once per chunk, in order.
+template <typename T, bool NORM, typename Consume>
+__device__ __forceinline__ void stream_list(int s0, int s1, int L, int k, bool act, int lane,
+                                            const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                                            const T* __restrict__ src, const float* __restrict__ norm,
+                                            T (*ring)[kChunk][32], float (*mw)[kChunk], float (*mn)[kChunk],
+                                            Consume&& consume) {
+    const int nch = (s1 - s0 + kChunk - 1) / kChunk;
+    auto pix_of = [&](int c) {
+        const int base = s0 + c * kChunk;
+        return (c < nch && lane < s1 - base) ? seg_pix[base + lane] : 0;
+    };
+    auto issue = [&](int c, int pc) {
+        const int slot = c % kStages, base = s0 + c * kChunk, n = min(kChunk, s1 - base);
+        if (lane < n) {
+            cp_async4(&mw[slot][lane], seg_w + base + lane);
+            if (NORM) cp_async4(&mn[slot][lane], norm + pc);
+        }
+        for (int e = 0; e < n; e++) {
+            const int p = __shfl_sync(0xffffffffu, pc, e);
+            if (act) cp_async4(&ring[slot][e][lane], src + (long)p * L + k);
+        }
+    };
+    int pcur = pix_of(0);
+#pragma unroll
+    for (int c = 0; c < kStages - 1; c++) {
+        const int pn = pix_of(c + 1);
+        if (c < nch) issue(c, pcur);
+        cp_async_commit();
+        pcur = pn;
+    }
+    for (int c = 0; c < nch; c++) {
+        const int ci = c + kStages - 1;
+        const int pn = pix_of(ci + 1);
+        if (ci < nch) issue(ci, pcur);
+        cp_async_commit();
+        pcur = pn;
+        cp_async_wait<kStages - 1>();  // chunk c has landed (this lane's copies)
+        __syncwarp();                  // ... and every other lane's
+        consume(c % kStages, min(kChunk, s1 - (s0 + c * kChunk)));
+        __syncwarp();                  // the slot is refilled kStages-1 chunks later
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+}
+
 template <bool PRE_NORM>
-__global__ void splat_kernel(int M, int L, const int* __restrict__ seg_start,
-                             const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
-                             const float* __restrict__ in, const float* __restrict__ norm,
-                             float* __restrict__ vals) {
+__global__ void __launch_bounds__(32 * kStageWarps)
+    splat_kernel(int M, int L, const int* __restrict__ order, const int* __restrict__ seg_start,
+                 const int* __restrict__ seg_pix, const float* __restrict__ seg_w, const float* __restrict__ in,
+                 const float* __restrict__ norm, float* __restrict__ vals) {
+    __shared__ float ring[kStageWarps][kStages][kChunk][32];
+    __shared__ float mw[kStageWarps][kStages][kChunk];
+    __shared__ float mn[kStageWarps][kStages][kChunk];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int unit = blockIdx.x * kStageWarps + wib;
+    if (unit >= M) return;  // warp-uniform; the kernel has no block-wide barrier
+    const int v = order[unit];
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    for (int kb = 0; kb < L; kb += 32) {
+        const int k = kb + lane;
+        const bool act = k < L;
+        float acc = 0.0f;
+        stream_list<float, PRE_NORM>(s0, s1, L, k, act, lane, seg_pix, seg_w, in, norm, ring[wib], mw[wib],
+                                     mn[wib], [&](int slot, int n) {
+#pragma unroll 4
+                                         for (int e = 0; e < n; e++) {
+                                             float x = ring[wib][slot][e][lane];
+                                             if (PRE_NORM) x = fmul(x, mn[wib][slot][e]);
+                                             acc = fadd(acc, fmul(mw[wib][slot][e], x));
+                                         }
+                                     });
+        if (act) vals[(long)(v + 1) * L + k] = acc;
+    }
+}
+
+// Short lists (at most kLongList entries; the tail of `order`): one thread
+// per (vertex, label), the same in-order sum without staging.
+template <bool PRE_NORM>
+__global__ void splat_short_kernel(int n_short, int L, const int* __restrict__ order,
+                                   const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
+                                   const float* __restrict__ seg_w, const float* __restrict__ in,
+                                   const float* __restrict__ norm, float* __restrict__ vals) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)M * L) return;
-    const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    if (t >= (long)n_short * L) return;
+    const int u = (int)(t / L), k = (int)(t - (long)u * L);
+    const int v = order[u];
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
     float acc = 0.0f;
+#pragma unroll 4
     for (int s = s0; s < s1; s++) {
         const int p = seg_pix[s];
         float x = in[(long)p * L + k];
@@ -320,6 +430,22 @@ __global__ void splat_kernel(int M, int L, const int* __restrict__ seg_start,
         acc = fadd(acc, fmul(seg_w[s], x));
     }
     vals[(long)(v + 1) * L + k] = acc;
+}
+
+__global__ void count_long_kernel(int M, const int* __restrict__ counts, int threshold, int* __restrict__ n) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool is_long = v < M && counts[v] > threshold;
+    const unsigned b = __ballot_sync(0xffffffffu, is_long);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(n, __popc(b));
+}
+
+// Sort key that puts long splat lists first (stable radix sort ascending).
+__global__ void order_key_kernel(int M, const int* __restrict__ counts, int* __restrict__ keys,
+                                 int* __restrict__ vals) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= M) return;
+    keys[v] = kMaxOrderKey - min(counts[v], kMaxOrderKey);
+    vals[v] = v;
 }
 
 // One blur pass along one lattice axis: new = old + 1/2 (n1 + n2).  seqCompute
@@ -386,34 +512,98 @@ __device__ __forceinline__ int bin_upper(float q) {
     return c < kRes - 1 ? c : kRes - 1;
 }
 
-// Ordered splat, both passes at once: bins [0,10) lower, [10,20) upper.
-__global__ void ord_splat_kernel(int M, int L, const int* __restrict__ seg_start,
-                                 const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
-                                 const float* __restrict__ Q, float* __restrict__ vals) {
+// Bin indices of every (pixel, label), computed once per ordered filter:
+// lower | upper << 8 (each pixel appears in d+1 splat lists and in the slice).
+__global__ void ord_bins_kernel(long n, const float* __restrict__ Q, int* __restrict__ bins) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)M * L) return;
-    const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    if (t >= n) return;
+    const float q = Q[t];
+    bins[t] = bin_lower(q) | (bin_upper(q) << 8);
+}
+
+// Each of the 10 bins accumulates, in entry order, the weights of the entries
+// that reach it: bins 0..c (lower pass) or c..9 (upper pass), addSplitArray
+// (:548-569).
+template <bool UPPER>
+__device__ __forceinline__ void ord_consume(float (&acc)[kRes], const int (*ring)[32], const float* mw, int lane,
+                                            int n) {
+#pragma unroll 2
+    for (int e = 0; e < n; e++) {
+        const int word = ring[e][lane];
+        const int c = UPPER ? (word >> 8) : (word & 0xff);
+        const float w = mw[e];
+#pragma unroll
+        for (int b = 0; b < kRes; b++)
+            if (UPPER ? b >= c : b <= c) acc[b] = fadd(acc[b], w);
+    }
+}
+
+// Ordered splat: one warp per (vertex, pass), streaming the vertex's list as
+// splat_kernel does.  A vertex row holds 20 bins x L labels, bin-major
+// ([v][bin][label]; bins [0,10) lower, [10,20) upper) so that the slice's
+// per-label bin reads coalesce.
+__global__ void __launch_bounds__(32 * kStageWarps)
+    ord_splat_kernel(int M, int L, const int* __restrict__ order, const int* __restrict__ seg_start,
+                     const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                     const int* __restrict__ bins, float* __restrict__ vals) {
+    __shared__ int ring[kStageWarps][kStages][kChunk][32];
+    __shared__ float mw[kStageWarps][kStages][kChunk];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int unit = blockIdx.x * kStageWarps + wib;
+    if (unit >= 2 * M) return;  // warp-uniform
+    const int v = order[unit >> 1];
+    const bool upper = unit & 1;
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    for (int kb = 0; kb < L; kb += 32) {
+        const int k = kb + lane;
+        const bool act = k < L;
+        float acc[kRes];
+#pragma unroll
+        for (int b = 0; b < kRes; b++) acc[b] = 0.0f;
+        stream_list<int, false>(s0, s1, L, k, act, lane, seg_pix, seg_w, bins, nullptr, ring[wib], mw[wib],
+                                nullptr, [&](int slot, int n) {
+                                    if (upper) ord_consume<true>(acc, ring[wib][slot], mw[wib][slot], lane, n);
+                                    else ord_consume<false>(acc, ring[wib][slot], mw[wib][slot], lane, n);
+                                });
+        if (act) {
+            float* row = vals + ((long)(v + 1) * kOrdW + (upper ? kRes : 0)) * L + k;
+#pragma unroll
+            for (int b = 0; b < kRes; b++) row[(long)b * L] = acc[b];
+        }
+    }
+}
+
+// Ordered splat of the short lists: one thread per (vertex, label), both
+// passes, without staging.
+__global__ void ord_splat_short_kernel(int n_short, int L, const int* __restrict__ order,
+                                       const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
+                                       const float* __restrict__ seg_w, const int* __restrict__ bins,
+                                       float* __restrict__ vals) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)n_short * L) return;
+    const int u = (int)(t / L), k = (int)(t - (long)u * L);
+    const int v = order[u];
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
     float lo[kRes], up[kRes];
 #pragma unroll
     for (int b = 0; b < kRes; b++) lo[b] = up[b] = 0.0f;
+#pragma unroll 2
     for (int s = s0; s < s1; s++) {
-        const int p = seg_pix[s];
+        const int word = bins[(long)seg_pix[s] * L + k];
+        const int cl = word & 0xff, cu = word >> 8;
         const float w = seg_w[s];
-        const float q = Q[(long)p * L + k];
-        const int cl = bin_lower(q), cu = bin_upper(q);
 #pragma unroll
         for (int b = 0; b < kRes; b++) {
-            if (b <= cl) lo[b] = fadd(lo[b], w);
-            if (b >= cu) up[b] = fadd(up[b], w);
+            lo[b] = fadd(lo[b], b <= cl ? w : 0.0f);
+            up[b] = fadd(up[b], b >= cu ? w : 0.0f);
         }
     }
-    float4* dst = reinterpret_cast<float4*>(vals + ((long)(v + 1) * L + k) * kOrdW);
-    dst[0] = make_float4(lo[0], lo[1], lo[2], lo[3]);
-    dst[1] = make_float4(lo[4], lo[5], lo[6], lo[7]);
-    dst[2] = make_float4(lo[8], lo[9], up[0], up[1]);
-    dst[3] = make_float4(up[2], up[3], up[4], up[5]);
-    dst[4] = make_float4(up[6], up[7], up[8], up[9]);
+    float* row = vals + (long)(v + 1) * kOrdW * L + k;
+#pragma unroll
+    for (int b = 0; b < kRes; b++) {
+        row[(long)b * L] = lo[b];
+        row[(long)(kRes + b) * L] = up[b];
+    }
 }
 
 // Ordered blur: every bin independently, weightedAddSplitArray (:570-578).
@@ -435,29 +625,74 @@ __global__ void ord_blur_kernel(int M, int row4, const int2* __restrict__ nbr,
 }
 
 // Ordered slice: lower pass with weight -w*alpha, then upper with w*alpha
-// (:639-650, :687-696), accumulated into one value.
+// (:639-650, :687-696), accumulated into one value.  With GAP the LP's dual
+// gap terms are folded in: tmp = (alpha + u) - (v + 0) for the final slice
+// value v, and per-block sums of tmp.Q and tmp.tmp (src/densecrf.cpp:725-729).
+template <bool GAP>
 __global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ offset,
                                  const float* __restrict__ bary, const float* __restrict__ vals,
-                                 const float* __restrict__ Q, float alpha, float* out,
-                                 SliceEpilogue ep) {
+                                 const int* __restrict__ bins, float alpha, float* out, SliceEpilogue ep,
+                                 GapFusion gf) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)N * L) return;
-    const int i = (int)(t / L), k = (int)(t - (long)i * L);
-    const int d1 = d + 1;
-    const float q = Q[t];
-    const int cl = bin_lower(q), cu = bin_upper(q);
-    float acc = 0.0f;
-    for (int j = 0; j <= d; j++) {
-        const int o = offset[(long)i * d1 + j];
-        const float w = bary[(long)i * d1 + j];
-        acc = fadd(acc, fmul(vals[((long)(o + 1) * L + k) * kOrdW + cl], fmul(-w, alpha)));
+    double g0 = 0.0, g1 = 0.0;
+    if (t < (long)N * L) {
+        const int i = (int)(t / L), k = (int)(t - (long)i * L);
+        const int d1 = d + 1;
+        const int word = bins[t];
+        const int cl = word & 0xff, cu = word >> 8;
+        float acc = 0.0f;
+        for (int j = 0; j <= d; j++) {
+            const int o = offset[(long)i * d1 + j];
+            const float w = bary[(long)i * d1 + j];
+            acc = fadd(acc, fmul(vals[((long)(o + 1) * kOrdW + cl) * L + k], fmul(-w, alpha)));
+        }
+        for (int j = 0; j <= d; j++) {
+            const int o = offset[(long)i * d1 + j];
+            const float w = bary[(long)i * d1 + j];
+            acc = fadd(acc, fmul(vals[((long)(o + 1) * kOrdW + kRes + cu) * L + k], fmul(w, alpha)));
+        }
+        const float v = apply_epilogue(acc, t, i, ep);
+        out[t] = v;
+        if (GAP) {
+            const float tmp = fsub(fadd(gf.alpha[t], gf.u[t]), fadd(v, 0.0f));
+            g0 = (double)tmp * (double)gf.Q[t];
+            g1 = (double)tmp * (double)tmp;
+        }
     }
-    for (int j = 0; j <= d; j++) {
-        const int o = offset[(long)i * d1 + j];
-        const float w = bary[(long)i * d1 + j];
-        acc = fadd(acc, fmul(vals[((long)(o + 1) * L + k) * kOrdW + kRes + cu], fmul(w, alpha)));
+    if (GAP) {
+        __shared__ double s0[kTB / 32], s1[kTB / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g0 += __shfl_down_sync(0xffffffffu, g0, o);
+            g1 += __shfl_down_sync(0xffffffffu, g1, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            s0[threadIdx.x >> 5] = g0;
+            s1[threadIdx.x >> 5] = g1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < kTB / 32; w++) {
+                a += s0[w];
+                b += s1[w];
+            }
+            gf.partials[blockIdx.x] = a;
+            gf.partials[gridDim.x + blockIdx.x] = b;
+        }
     }
-    out[t] = apply_epilogue(acc, t, i, ep);
+}
+
+// Bins of rescale(Q) (src/eigen_utils.cpp:120-141) without materialising it:
+// rq = (Q - min) / (max - min), with min / max at qmm[0], qmm[1].
+__global__ void rescaled_bins_kernel(long n, const float* __restrict__ Q, const float* __restrict__ qmm,
+                                     int* __restrict__ bins) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float mn = qmm[0], range = fsub(qmm[1], qmm[0]);
+    float rq = fsub(Q[t], mn);
+    if (range > 0.0f) rq = rq / range;
+    bins[t] = bin_lower(rq) | (bin_upper(rq) << 8);
 }
 
 int bits_for(int n) {  // bits needed to hold values 0..n-1
@@ -465,8 +700,6 @@ int bits_for(int n) {  // bits needed to hold values 0..n-1
     while ((1LL << b) < (long long)n) b++;
     return b;
 }
-
-constexpr int kTB = 256;
 
 template <int DM>
 void build_impl(Lattice& L, const float* d_features) {
@@ -487,7 +720,7 @@ void build_impl(Lattice& L, const float* d_features) {
     int4* ekeys = L.ekeys.ensure((size_t)E * KW);
     int* rank = L.rank.ensure(Ereal);
     float* bary = L.bary.ensure(Ereal);
-    elevate_kernel<DM><<<ceil_div(Np, kTB), kTB, 0, st>>>(d_features, N, Np, d, dscale, ekeys, rank, bary);
+    launch(elevate_kernel<DM>, ceil_div(Np, kTB), kTB, 0, st, d_features, N, Np, d, dscale, ekeys, rank, bary);
     DCRF_LAUNCH_CHECK();
 
     unsigned cap = 1;
@@ -495,9 +728,9 @@ void build_impl(Lattice& L, const float* d_features) {
     int* table = L.table.ensure(cap);
     DCRF_CUDA(cudaMemsetAsync(table, 0xff, sizeof(int) * cap, st));
     int* eslot = L.entry_slot.ensure(E);
-    insert_kernel<KW><<<ceil_div(E, kTB), kTB, 0, st>>>(ekeys, (int)E, table, cap - 1, eslot);
+    launch(insert_kernel<KW>, ceil_div(E, kTB), kTB, 0, st, ekeys, (int)E, table, cap - 1, eslot);
     int* flags = L.flags.ensure(E);
-    first_flag_kernel<<<ceil_div(E, kTB), kTB, 0, st>>>((int)E, eslot, table, flags);
+    launch(first_flag_kernel, ceil_div(E, kTB), kTB, 0, st, (int)E, eslot, table, flags);
     DCRF_LAUNCH_CHECK();
     int* dtotal = L.total.ensure(1);
     exclusive_scan(flags, flags, (int)E, dtotal, L.scan, st);
@@ -509,28 +742,38 @@ void build_impl(Lattice& L, const float* d_features) {
     int* offset = L.offset.ensure(Ereal);
     int16_t* vkeys = L.vkeys.ensure((size_t)M * d);
     int* slot_vid = L.slot_vid.ensure(cap);
-    finalize_kernel<KW><<<ceil_div(E, kTB), kTB, 0, st>>>((int)E, (int)Ereal, d, eslot, table, flags,
+    launch(finalize_kernel<KW>, ceil_div(E, kTB), kTB, 0, st, (int)E, (int)Ereal, d, eslot, table, flags,
                                                          ekeys, offset, vkeys, slot_vid);
     int2* nbr = L.nbr.ensure((size_t)d1 * M);
-    neighbor_kernel<KW><<<ceil_div((long)d1 * M, kTB), kTB, 0, st>>>(M, d, vkeys, table, cap - 1,
+    launch(neighbor_kernel<KW>, ceil_div((long)d1 * M, kTB), kTB, 0, st, M, d, vkeys, table, cap - 1,
                                                                      ekeys, slot_vid, nbr);
     DCRF_LAUNCH_CHECK();
 
     // Splat lists: per-vertex counts -> starts; stable sort of entries by vertex.
     int* counts = L.counts.ensure((size_t)M + 1);
     DCRF_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * ((size_t)M + 1), st));
-    count_kernel<<<ceil_div(Ereal, kTB), kTB, 0, st>>>((int)Ereal, offset, counts);
+    launch(count_kernel, ceil_div(Ereal, kTB), kTB, 0, st, (int)Ereal, offset, counts);
     int* seg_start = L.seg_start.ensure((size_t)M + 1);
     exclusive_scan(counts, seg_start, M + 1, nullptr, L.scan, st);
     int* skeys = L.sort_keys.ensure(Ereal);
     int* svals = L.sort_vals.ensure(Ereal);
-    iota_copy_kernel<<<ceil_div(Ereal, kTB), kTB, 0, st>>>((int)Ereal, offset, skeys, svals);
+    launch(iota_copy_kernel, ceil_div(Ereal, kTB), kTB, 0, st, (int)Ereal, offset, skeys, svals);
     DCRF_LAUNCH_CHECK();
     radix_sort_pairs(skeys, svals, (int)Ereal, bits_for(M), L.sort, st);
     int* seg_pix = L.seg_pix.ensure(Ereal);
     float* seg_w = L.seg_w.ensure(Ereal);
-    seg_fill_kernel<<<ceil_div(Ereal, kTB), kTB, 0, st>>>((int)Ereal, d1, svals, bary, seg_pix, seg_w);
+    launch(seg_fill_kernel, ceil_div(Ereal, kTB), kTB, 0, st, (int)Ereal, d1, svals, bary, seg_pix, seg_w);
+    // Splat visiting order: longest lists first.
+    int* vorder = L.vorder.ensure(M);
+    int* okeys = L.vorder_keys.ensure(M);
+    launch(order_key_kernel, ceil_div(M, kTB), kTB, 0, st, M, counts, okeys, vorder);
+    radix_sort_pairs(okeys, vorder, M, 24, L.sort, st);
+    int* dlong = L.total.ensure(1);
+    DCRF_CUDA(cudaMemsetAsync(dlong, 0, sizeof(int), st));
+    launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, counts, kLongList, dlong);
     DCRF_LAUNCH_CHECK();
+    DCRF_CUDA(cudaMemcpyAsync(&L.n_long, dlong, sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCRF_CUDA(cudaStreamSynchronize(st));
     L.va_floats = 0;
 }
 
@@ -566,50 +809,86 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     cudaStream_t st = stream;
     const long ML = (long)M * L, NL = (long)N * L;
     float *src = va.get(), *dst = vb.get();
-    if (pre_norm)
-        splat_kernel<true><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, seg_start.get(), seg_pix.get(),
-                                                              seg_w.get(), in, pre_norm, src);
-    else
-        splat_kernel<false><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, seg_start.get(), seg_pix.get(),
-                                                               seg_w.get(), in, nullptr, src);
+    const int n_short = M - n_long;
+    const long SL = (long)n_short * L;
+    if (pre_norm) {
+        if (n_long)
+            launch(splat_kernel<true>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src);
+        if (n_short)
+            launch(splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src);
+    } else {
+        if (n_long)
+            launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+        if (n_short)
+            launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+    }
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
         if (seq)
-            blur_kernel<true><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, nbr.get() + (long)j * M, src, dst);
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
         else
-            blur_kernel<false><<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, nbr.get() + (long)j * M, src, dst);
+            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     if (seq)
-        slice_kernel<true><<<ceil_div(NL, kTB), kTB, 0, st>>>(N, L, d, offset.get(), bary.get(), src,
+        launch(slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
                                                               alpha, out, ep);
     else
-        slice_kernel<false><<<ceil_div(NL, kTB), kTB, 0, st>>>(N, L, d, offset.get(), bary.get(), src,
+        launch(slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
                                                                alpha, out, ep);
     DCRF_LAUNCH_CHECK();
 }
 
 void Lattice::compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep) {
     require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
+    const long NL = (long)N * L;
+    int* bins = obins.ensure((size_t)NL);
+    launch(ord_bins_kernel, ceil_div(NL, kTB), kTB, 0, stream, NL, Q, bins);
+    compute_ord_bins(out, bins, L, ep, nullptr);
+}
+
+void rescaled_bins(int* bins, const float* Q, long n, const float* qminmax, cudaStream_t st) {
+    launch(rescaled_bins_kernel, ceil_div(n, kTB), kTB, 0, st, n, Q, qminmax, bins);
+    DCRF_LAUNCH_CHECK();
+}
+
+int slice_grid(long n) { return ceil_div(n, kTB); }
+
+void Lattice::compute_ord_bins(float* out, const int* bins, int L, const SliceEpilogue& ep,
+                               const GapFusion* gap) {
+    require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
     const size_t row = (size_t)L * kOrdW;
     ensure_values(row);
     cudaStream_t st = stream;
-    const long ML = (long)M * L, NL = (long)N * L;
+    const long NL = (long)N * L;
     float *src = va.get(), *dst = vb.get();
-    ord_splat_kernel<<<ceil_div(ML, kTB), kTB, 0, st>>>(M, L, seg_start.get(), seg_pix.get(),
-                                                        seg_w.get(), Q, src);
+    const int n_short = M - n_long;
+    if (n_long)
+        launch(ord_splat_kernel, ceil_div(2L * n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
+               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
+    if (n_short)
+        launch(ord_splat_short_kernel, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
+               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
     const int row4 = (int)(row / 4);
     for (int j = 0; j <= d; j++) {
-        ord_blur_kernel<<<ceil_div((long)M * row4, kTB), kTB, 0, st>>>(
+        launch(ord_blur_kernel, ceil_div((long)M * row4, kTB), kTB, 0, st, 
             M, row4, nbr.get() + (long)j * M, reinterpret_cast<const float4*>(src),
             reinterpret_cast<float4*>(dst));
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
-    ord_slice_kernel<<<ceil_div(NL, kTB), kTB, 0, st>>>(N, L, d, offset.get(), bary.get(), src, Q,
-                                                        alpha, out, ep);
+    if (gap)
+        launch(ord_slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
+               bins, alpha, out, ep, *gap);
+    else
+        launch(ord_slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
+               bins, alpha, out, ep, GapFusion{});
     DCRF_LAUNCH_CHECK();
 }
 

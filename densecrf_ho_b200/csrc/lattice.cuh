@@ -29,15 +29,31 @@ struct SliceEpilogue {
     bool zero_base = false;       // out = 0.0f + coef * v  (Eigen fill(0); +=)
 };
 
+// LP dual-gap sums folded into an ordered slice (see ord_slice_kernel).
+struct GapFusion {
+    const float* alpha = nullptr;
+    const float* u = nullptr;
+    const float* Q = nullptr;
+    double* partials = nullptr;  // [2][slice_grid(N*L)]
+};
+
+// Packed ordered-filter bin indices of rescale(Q) (min / max at qminmax[0..1]).
+void rescaled_bins(int* bins, const float* Q, long n, const float* qminmax, cudaStream_t st);
+// Blocks of the element-wise slice kernels for n elements.
+int slice_grid(long n);
+
 struct Lattice {
     int N = 0, d = 0, M = 0;
+    int n_long = 0;  // vertices whose splat list exceeds the staging threshold
     cudaStream_t stream = nullptr;  // borrowed
 
     DevBuf<int> offset, rank, seg_start, seg_pix;
+    DevBuf<int> vorder, vorder_keys;  // splat visiting order: longest lists first
     DevBuf<float> bary, seg_w;
     DevBuf<int16_t> vkeys;
     DevBuf<int2> nbr;
     DevBuf<float> va, vb;    // filter value buffers
+    DevBuf<int> obins;       // ordered filter: packed bin indices per (pixel, label)
     size_t va_floats = 0;    // rows (M+1) * width currently zero-headed
 
     // build scratch
@@ -54,6 +70,8 @@ struct Lattice {
                  const float* pre_norm = nullptr);
     // Ordered (upper minus lower, 10-bin) filter of Q in [0,1]; out = epilogue(v).
     void compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep);
+    // The same from precomputed packed bins (lower | upper << 8 per element).
+    void compute_ord_bins(float* out, const int* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
 
     void ensure_values(size_t row_width);
 };

@@ -65,7 +65,9 @@ Model::Model(int W_, int H_, int L_) : W(W_), H(H_), N(W_ * H_), L(L_) {
     DCRF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     DCRF_CUDA(cudaMallocHost(&h_scal, sizeof(SolverScalars)));
     scal.ensure(1);
-    partials.ensure((size_t)kRedBlocks * 16);
+    // per-block partials: fixed-grid reductions, and the per-pixel / per-element
+    // kernels that fold a reduction in (two values per block)
+    partials.ensure(std::max<size_t>((size_t)kRedBlocks * 16, 2 * (size_t)slice_grid((long)N * L) + 64));
 }
 
 Model::~Model() {
@@ -88,10 +90,10 @@ void Model::add_term(const float* d_features, int d, float w) {
     t->w = w;
     t->d = d;
     float* nrm = t->norm.ensure(N);
-    fill_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, 1.0f, nrm);
+    launch(fill_kernel, ceil_div(N, 256), 256, 0, stream, N, 1.0f, nrm);
     SliceEpilogue ep;  // plain output
     t->lat->compute(nrm, nrm, 1, false, ep);
-    norm_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, nrm);
+    launch(norm_kernel, ceil_div(N, 256), 256, 0, stream, N, nrm);
     DCRF_LAUNCH_CHECK();
     terms.push_back(std::move(t));
 }
@@ -154,18 +156,29 @@ void Model::apply_ord(int k, float* out, const float* rq, const float* base, boo
     t.lat->compute_ord(out, rq, L, ep);
 }
 
+void Model::apply_ord_bins(int k, float* out, const int* bins, const float* base, bool zero_base,
+                           const GapFusion* gap) {
+    Term& t = *terms[k];
+    SliceEpilogue ep;
+    ep.potts = true;
+    ep.scale = -t.w;
+    ep.base = base;
+    ep.zero_base = zero_base;
+    t.lat->compute_ord_bins(out, bins, L, ep, gap);
+}
+
 void Model::check_unit_range(const float* Q) {
-    minmax_partial_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, partials.get());
-    minmax_finish_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, scal.get());
+    launch(minmax_partial_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, Q, partials.get());
+    launch(minmax_finish_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, scal.get());
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
     if (h_scal->qmax > 1.0f || h_scal->qmin < 0.0f) throw Error(DCRF_E_RANGE, "Value out of bounds");
 }
 
 void Model::rescale(float* out, const float* Q) {
-    minmax_partial_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, partials.get());
-    minmax_finish_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, scal.get());
-    rescale_kernel<<<ceil_div((long)N * L, 256), 256, 0, stream>>>((long)N * L, Q, scal.get(), out);
+    launch(minmax_partial_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, Q, partials.get());
+    launch(minmax_finish_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, scal.get());
+    launch(rescale_kernel, ceil_div((long)N * L, 256), 256, 0, stream, (long)N * L, Q, scal.get(), out);
     DCRF_LAUNCH_CHECK();
 }
 
@@ -173,7 +186,7 @@ void Model::unary_init(float* Q) {
     require(has_unary, DCRF_E_STATE, "unary_init: no unary energy set");
     with_lc(L, [&](auto lc) {
         constexpr int LC = decltype(lc)::value;
-        unary_init_kernel<LC><<<ceil_div(N, 128), 128, 0, stream>>>(N, L, unary.get(), Q);
+        launch(unary_init_kernel<LC>, ceil_div(N, 128), 128, 0, stream, N, L, unary.get(), Q);
     });
     DCRF_LAUNCH_CHECK();
 }
@@ -181,7 +194,7 @@ void Model::unary_init(float* Q) {
 void Model::current_map(const float* Q, int16_t* lab) {
     with_lc(L, [&](auto lc) {
         constexpr int LC = decltype(lc)::value;
-        current_map_kernel<LC><<<ceil_div(N, 128), 128, 0, stream>>>(N, L, Q, lab);
+        launch(current_map_kernel<LC>, ceil_div(N, 128), 128, 0, stream, N, L, Q, lab);
     });
     DCRF_LAUNCH_CHECK();
 }
@@ -193,18 +206,18 @@ double Model::energy_true(const int16_t* d_lab, bool ho) {
     float* qc = buf(10);
     float* o = buf(11);
     float* pw = b[12].ensure(N);
-    onehot_complement_kernel<<<ceil_div((long)N * L, 256), 256, 0, stream>>>(N, L, d_lab, qc);
+    launch(onehot_complement_kernel, ceil_div((long)N * L, 256), 256, 0, stream, N, L, d_lab, qc);
     for (size_t k = 0; k < terms.size(); k++) {
         apply((int)k, true, o, qc);
-        pairwise_pick_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, L, d_lab, o, pw, k == 0);
+        launch(pairwise_pick_kernel, ceil_div(N, 256), 256, 0, stream, N, L, d_lab, o, pw, k == 0);
     }
-    if (terms.empty()) fill_kernel<<<ceil_div(N, 256), 256, 0, stream>>>(N, 0.0f, pw);
-    energy_sum_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, d_lab, unary.get(), pw, partials.get());
-    finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 0, scal.get());
+    if (terms.empty()) launch(fill_kernel, ceil_div(N, 256), 256, 0, stream, N, 0.0f, pw);
+    launch(energy_sum_kernel, kRedBlocks, kRedThreads, 0, stream, N, L, d_lab, unary.get(), pw, partials.get());
+    launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 0, scal.get());
     if (ho && R > 0) {
         int* flags = ipart.ensure(std::max(R, 1));
-        clique_label_change_kernel<<<R, 256, 0, stream>>>(cl_off.get(), cl_idx.get(), d_lab, flags);
-        energy_ho_finish_kernel<<<1, 1, 0, stream>>>(R, flags, cl_exp.get(), scal.get());
+        launch(clique_label_change_kernel, R, 256, 0, stream, cl_off.get(), cl_idx.get(), d_lab, flags);
+        launch(energy_ho_finish_kernel, 1, 1, 0, stream, R, flags, cl_exp.get(), scal.get());
     }
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
@@ -217,18 +230,18 @@ double Model::energy_lp(const float* Q) {
     float* rq = buf(10);
     float* o = buf(11);
     rescale(rq, Q);
-    dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, unary.get(), Q, partials.get());
-    finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 0, scal.get());
+    launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, unary.get(), Q, partials.get());
+    launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 0, scal.get());
     for (size_t k = 0; k < terms.size(); k++) {
         apply_ord((int)k, o, rq);
-        dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, o, partials.get());
-        finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
+        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, Q, o, partials.get());
+        launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
     }
     if (R > 0) {
         float* diffs = b[13].ensure(std::max(R, 1));
-        clique_maxdiff_kernel<<<R, 256, 0, stream>>>(cl_off.get(), cl_idx.get(), L, Q, diffs);
+        launch(clique_maxdiff_kernel, R, 256, 0, stream, cl_off.get(), cl_idx.get(), L, Q, diffs);
     }
-    energy_lp_finish_kernel<<<1, 1, 0, stream>>>((int)terms.size(), R, b[13].get(), cl_exp.get(), scal.get());
+    launch(energy_lp_finish_kernel, 1, 1, 0, stream, (int)terms.size(), R, b[13].get(), cl_exp.get(), scal.get());
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
     return h_scal->energy;
@@ -238,14 +251,14 @@ double Model::energy_lp(const float* Q) {
 double Model::lr_qp_value(const float* Q) {
     require(has_unary, DCRF_E_STATE, "energy: no unary energy set");
     float* o = buf(11);
-    dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, unary.get(), Q, partials.get());
-    finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 0, scal.get());
+    launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, unary.get(), Q, partials.get());
+    launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 0, scal.get());
     for (size_t k = 0; k < terms.size(); k++) {
         apply((int)k, false, o, Q);
-        dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>((long)N * L, Q, o, partials.get());
-        finalize_sums_kernel<<<1, 32, 0, stream>>>(partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
+        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, Q, o, partials.get());
+        launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
     }
-    lr_finish_kernel<<<1, 1, 0, stream>>>((int)terms.size(), scal.get());
+    launch(lr_finish_kernel, 1, 1, 0, stream, (int)terms.size(), scal.get());
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
     return h_scal->energy;

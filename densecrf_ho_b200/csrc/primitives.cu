@@ -173,9 +173,9 @@ void exclusive_scan(const int* in, int* out, int n, int* d_total, ScanScratch& s
     }
     int nb = ceil_div(n, kScanTile);
     int* bs = s.block_sums.ensure(nb);
-    scan_reduce_kernel<<<nb, kScanThreads, 0, st>>>(in, n, bs);
-    scan_top_kernel<<<1, kScanThreads, 0, st>>>(bs, nb, d_total);
-    scan_apply_kernel<<<nb, kScanThreads, 0, st>>>(in, out, n, bs);
+    launch(scan_reduce_kernel, nb, kScanThreads, 0, st, in, n, bs);
+    launch(scan_top_kernel, 1, kScanThreads, 0, st, bs, nb, d_total);
+    launch(scan_apply_kernel, nb, kScanThreads, 0, st, in, out, n, bs);
     DCRF_LAUNCH_CHECK();
 }
 
@@ -188,9 +188,9 @@ void radix_sort_pairs(int* keys, int* vals, int n, int key_bits, SortScratch& s,
     int *kin = keys, *vin = vals, *kout = ka, *vout = va;
     int passes = 0;
     for (int shift = 0; shift < key_bits; shift += 8, passes++) {
-        radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(kin, n, shift, ntiles, hist);
+        launch(radix_hist_kernel, ntiles, kSortThreads, 0, st, kin, n, shift, ntiles, hist);
         exclusive_scan(hist, hist, kRadix * ntiles, nullptr, s.scan, st);
-        radix_scatter_kernel<<<ntiles, kSortThreads, 0, st>>>(kin, vin, n, shift, ntiles, hist, kout,
+        launch(radix_scatter_kernel, ntiles, kSortThreads, 0, st, kin, vin, n, shift, ntiles, hist, kout,
                                                              vout);
         DCRF_LAUNCH_CHECK();
         std::swap(kin, kout);

@@ -283,19 +283,32 @@ __global__ void add_scaled_kernel(long n, float* __restrict__ a, const float* __
 // ------------------------------------------------------------------ LP --
 
 // Y = multiplyC((alpha + u) - unary) + cur_Q (src/densecrf.cpp:627-635, 517-523).
+// With `pending`, the previous Frank-Wolfe iteration's update
+// alpha += delta (sa - alpha), u += delta (su - u) (:737-738) is applied here
+// first (and stored), saving a pass; su == nullptr means no cliques (su = 0).
 template <int LC>
-__global__ void lp_y_kernel(int N, int Lrt, float lambda, float cm, const float* __restrict__ alpha,
-                            const float* __restrict__ u, const float* __restrict__ U,
-                            const float* __restrict__ curQ, float* __restrict__ Y) {
+__global__ void lp_y_kernel(int N, int Lrt, float lambda, float cm, float* __restrict__ alpha,
+                            float* __restrict__ u, const float* __restrict__ U,
+                            const float* __restrict__ curQ, float* __restrict__ Y, bool pending,
+                            const float* __restrict__ sa, const float* __restrict__ su,
+                            const SolverScalars* __restrict__ sc) {
     const int L = LC ? LC : Lrt;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     float x[PixVec<LC>::S];
+    const float dl = pending ? sc->delta : 0.0f;
 #pragma unroll
     for (int k = 0; k < PixVec<LC>::S; k++)
         if (k < L) {
             const long e = (long)i * L + k;
-            x[k] = fsub(fadd(alpha[e], u[e]), U[e]);
+            float a = alpha[e], uu = u[e];
+            if (pending) {
+                a = fadd(a, fmul(dl, fsub(sa[e], a)));
+                uu = fadd(uu, fmul(dl, fsub(su ? su[e] : 0.0f, uu)));
+                alpha[e] = a;
+                u[e] = uu;
+            }
+            x[k] = fsub(fadd(a, uu), U[e]);
         }
     const float s = vec_sum<LC>(x, L);
 #pragma unroll
@@ -380,28 +393,54 @@ __global__ void lp_gamma_reset_kernel(SolverScalars* sc) {
 
 // beta = -colsum(alpha + u + gamma - unary) / L (:684-691);
 // Q = lambda (alpha + beta + u + gamma - unary) + cur_Q (:697).
+// Also writes per-block min / max of Q (the first half of rescale) to
+// partials[b] and partials[gridDim.x + b].
 template <int LC>
 __global__ void lp_q_kernel(int N, int Lrt, float lambda, const float* __restrict__ alpha, const float* __restrict__ u,
                             const float* __restrict__ gamma, const float* __restrict__ U,
-                            const float* __restrict__ curQ, float* __restrict__ Q) {
+                            const float* __restrict__ curQ, float* __restrict__ Q, double* __restrict__ partials) {
     const int L = LC ? LC : Lrt;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= N) return;
-    float bm[PixVec<LC>::S];
+    float mn = INFINITY, mx = -INFINITY;
+    if (i < N) {
+        float bm[PixVec<LC>::S];
 #pragma unroll
-    for (int k = 0; k < PixVec<LC>::S; k++)
-        if (k < L) {
-            const long e = (long)i * L + k;
-            bm[k] = fsub(fadd(fadd(alpha[e], u[e]), gamma[e]), U[e]);
-        }
-    const float beta = (-col_sum<LC>(bm, L, i)) / (float)L;
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) {
+                const long e = (long)i * L + k;
+                bm[k] = fsub(fadd(fadd(alpha[e], u[e]), gamma[e]), U[e]);
+            }
+        const float beta = (-col_sum<LC>(bm, L, i)) / (float)L;
 #pragma unroll
-    for (int k = 0; k < PixVec<LC>::S; k++)
-        if (k < L) {
-            const long e = (long)i * L + k;
-            const float x = fsub(fadd(fadd(fadd(alpha[e], beta), u[e]), gamma[e]), U[e]);
-            Q[e] = fadd(fmul(x, lambda), curQ[e]);
+        for (int k = 0; k < PixVec<LC>::S; k++)
+            if (k < L) {
+                const long e = (long)i * L + k;
+                const float x = fsub(fadd(fadd(fadd(alpha[e], beta), u[e]), gamma[e]), U[e]);
+                const float q = fadd(fmul(x, lambda), curQ[e]);
+                Q[e] = q;
+                mn = fminf(mn, q);
+                mx = fmaxf(mx, q);
+            }
+    }
+    __shared__ float smn[32], smx[32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        smn[threadIdx.x >> 5] = mn;
+        smx[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            mn = fminf(mn, smn[w]);
+            mx = fmaxf(mx, smx[w]);
         }
+        partials[blockIdx.x] = mn;
+        partials[gridDim.x + blockIdx.x] = mx;
+    }
 }
 
 // Partial sums of tmp.Q and tmp.tmp, tmp = (alpha + u) - (sa + su) (:725-729).
@@ -688,27 +727,27 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         cz = small + 5 * LR;
         zc = small + 6 * LR;
         omz = small + 7 * LR;
-        fill_float_kernel<<<ceil_div(LR, 256), 256, 0, stream>>>(LR, 1.0f, z);
+        launch(fill_float_kernel, ceil_div(LR, 256), 256, 0, stream, LR, 1.0f, z);
         ho = buf(4);
         DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
-        ho_regions_kernel<<<1, kLMax, 0, stream>>>(cv, L, Q, gz, 0, nullptr);
+        launch(ho_regions_kernel, 1, kLMax, 0, stream, cv, L, Q, gz, 0, nullptr);
     }
     // grad_y = unary + sum_k 2 A_k Q; energy terms Q . A_k Q (same applies).
     for (int k = 0; k < nt; k++) {
         apply(k, false, tmp, Q);
-        add_scaled_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, grad, tmp, 2.0f);
-        dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, Q, tmp, part);
-        finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 1 + k, sc);
+        launch(add_scaled_kernel, ceil_div(NL, 256), 256, 0, stream, NL, grad, tmp, 2.0f);
+        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, Q, tmp, part);
+        launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 1 + k, sc);
     }
     if (R > 0) {
-        ho_pixels_kernel<<<ceil_div((long)clique_max * L, 256), 256, 0, stream>>>(cv, L, z, ho, nullptr);
-        add_inplace_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, grad, ho);
-        ho_zterm_prep_kernel<<<1, 256, 0, stream>>>(cv, L, z, zc, omz, sc);
-        ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, omz, Q, 1, 8, sc, 1);
+        launch(ho_pixels_kernel, ceil_div((long)clique_max * L, 256), 256, 0, stream, cv, L, z, ho, nullptr);
+        launch(add_inplace_kernel, ceil_div(NL, 256), 256, 0, stream, NL, grad, ho);
+        launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
+        launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, Q, 1, 8, sc, 1);
     }
-    dot_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, unary.get(), Q, part);
-    finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 0, sc);
-    qp_init_energy_kernel<<<1, 1, 0, stream>>>(sc, nt, max_iter);
+    launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, part);
+    launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
+    launch(qp_init_energy_kernel, 1, 1, 0, stream, sc, nt, max_iter);
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
     int guard = 0;
@@ -716,34 +755,34 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
         with_lc(L, [&](auto lc) {
             constexpr int LC = decltype(lc)::value;
-            qp_direction_kernel<LC><<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, grad, Q, unary.get(), sx, part);
+            launch(qp_direction_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, grad, Q, unary.get(), sx, part);
         });
-        finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 0, sc);
+        launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
         if (R > 0) {
-            ho_direction_kernel<<<1, 256, 0, stream>>>(cv, L, gz, z, sxz, t1, t2, cz, sc);
-            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, t1, Q, 1, 3, sc, 0);    // a
-            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, t2, sx, 0, 4, sc, 0);   // b
-            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, t1, sx, 0, 6, sc, 0);   // denom term
+            launch(ho_direction_kernel, 1, 256, 0, stream, cv, L, gz, z, sxz, t1, t2, cz, sc);
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, Q, 1, 3, sc, 0);    // a
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t2, sx, 0, 4, sc, 0);   // b
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, sx, 0, 6, sc, 0);   // denom term
         }
         for (int k = 0; k < nt; k++) {
             if (k == 0) apply(k, false, psi, sx, nullptr, 1.0f, true);
             else apply(k, false, psi, sx, psi, 1.0f, false);
         }
-        dots2_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, Q, sx, psi, part);
-        finalize_sums_kernel<<<1, 64, 0, stream>>>(part, kRedBlocks, 2, 1, sc);
-        qp_step_kernel<<<1, 1, 0, stream>>>(sc);
+        launch(dots2_kernel, kRedBlocks, kRedThreads, 0, stream, NL, Q, sx, psi, part);
+        launch(finalize_sums_kernel, 1, 64, 0, stream, part, kRedBlocks, 2, 1, sc);
+        launch(qp_step_kernel, 1, 1, 0, stream, sc);
         if (R > 0) {
-            ho_z_update_kernel<<<1, 256, 0, stream>>>(LR, z, sxz, sc);
-            ho_pixels_kernel<<<ceil_div((long)clique_max * L, 256), 256, 0, stream>>>(cv, L, z, ho, sc);
+            launch(ho_z_update_kernel, 1, 256, 0, stream, LR, z, sxz, sc);
+            launch(ho_pixels_kernel, ceil_div((long)clique_max * L, 256), 256, 0, stream, cv, L, z, ho, sc);
         }
-        qp_update_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, sx, psi, ho, unary.get(), Q, grad, sc, part);
-        finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 7, sc);
+        launch(qp_update_kernel, kRedBlocks, kRedThreads, 0, stream, NL, sx, psi, ho, unary.get(), Q, grad, sc, part);
+        launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 7, sc);
         if (R > 0) {
-            ho_regions_kernel<<<1, kLMax, 0, stream>>>(cv, L, Q, gz, 1, sc);
-            ho_zterm_prep_kernel<<<1, 256, 0, stream>>>(cv, L, z, zc, omz, sc);
-            ho_scalar_kernel<<<1, kLMax, 0, stream>>>(cv, L, omz, Q, 1, 8, sc, 1);
+            launch(ho_regions_kernel, 1, kLMax, 0, stream, cv, L, Q, gz, 1, sc);
+            launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, Q, 1, 8, sc, 1);
         }
-        qp_energy_kernel<<<1, 1, 0, stream>>>(sc, max_iter);
+        launch(qp_energy_kernel, 1, 1, 0, stream, sc, max_iter);
         DCRF_LAUNCH_CHECK();
         fetch_scalars();
     }
@@ -763,7 +802,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     float* su = R > 0 ? buf(4) : nullptr;
     float* gamma = buf(5);
     float* curQ = buf(6);
-    float* rq = buf(7);
+    int* bins = lp_bins.ensure(NL);
     float* Y = buf(8);
     int16_t* lab = labels.ensure(N);
     SolverScalars* sc = scal.get();
@@ -774,7 +813,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
     with_lc(L, [&](auto lc) {
         constexpr int LC = decltype(lc)::value;
-        renormalize_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, Q);
+        launch(renormalize_kernel<LC>, pg, kPix, 0, stream, N, L, Q);
     });
     DCRF_CUDA(cudaMemcpyAsync(bestQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
     current_map(Q, lab);
@@ -783,7 +822,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     if (energy > int_energy) {
         with_lc(L, [&](auto lc) {
             constexpr int LC = decltype(lc)::value;
-            max_rounding_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, Q);
+            launch(max_rounding_kernel<LC>, pg, kPix, 0, stream, N, L, Q);
         });
         energy = energy_lp(Q);
     }
@@ -808,18 +847,23 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     int it = 0, count = 0, fw_total = 0, gamma_total = 0;
     do {
         ++it;
-        fill_float_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, 1.0f, gamma);
+        launch(fill_float_kernel, ceil_div(NL, 256), 256, 0, stream, NL, 1.0f, gamma);
         DCRF_CUDA(cudaMemcpyAsync(curQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
         DCRF_CUDA(cudaMemsetAsync(alpha, 0, sizeof(float) * NL, stream));
         DCRF_CUDA(cudaMemsetAsync(u, 0, sizeof(float) * NL, stream));
         int pit = 0;
         do {
             ++pit;
+            // alpha / u of the previous iteration are updated inside lp_y
+            // (the update after the last iteration is never read: both are
+            // reset before the next proximal step).
+            const bool pending = pit > 1;
             with_lc(L, [&](auto lc) {
                 constexpr int LC = decltype(lc)::value;
-                lp_y_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y);
+                launch(lp_y_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y,
+                       pending, sa, su, sc);
             });
-            lp_gamma_reset_kernel<<<1, 1, 0, stream>>>(sc);
+            launch(lp_gamma_reset_kernel, 1, 1, 0, stream, sc);
             // qp-gamma iterations; the reference needs at least two (its first
             // test compares against FLT_MAX), so launch in pairs and look at
             // the stop flag after each pair.
@@ -829,9 +873,9 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
                 for (int bi = 0; bi < batch; bi++) {
                     with_lc(L, [&](auto lc) {
                         constexpr int LC = decltype(lc)::value;
-                        lp_gamma_kernel<LC><<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, gc, Y, gamma, sc, part);
+                        launch(lp_gamma_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, gc, Y, gamma, sc, part);
                     });
-                    lp_gamma_check_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, p.qp_tol, sc);
+                    launch(lp_gamma_check_kernel, 1, 32, 0, stream, part, kRedBlocks, p.qp_tol, sc);
                 }
                 launched += batch;
                 DCRF_LAUNCH_CHECK();
@@ -839,31 +883,40 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
                 if (h_scal->stop || launched >= p.qp_max_iter || batch <= 0) break;
             }
             gamma_total += h_scal->steps;
+            // Q, with the min / max of rescale folded in; then the bins of
+            // rescale(Q) once for all pairwise terms.
             with_lc(L, [&](auto lc) {
                 constexpr int LC = decltype(lc)::value;
-                lp_q_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q);
+                launch(lp_q_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q,
+                       part);
             });
-            rescale(rq, Q);
-            for (int k = 0; k < nt; k++) {
-                if (k == 0) apply_ord(k, sa, rq, nullptr, true);
-                else apply_ord(k, sa, rq, sa, false);
-            }
+            launch(minmax_finish_kernel, 1, 32, 0, stream, part, pg, sc);
+            rescaled_bins(bins, Q, NL, &sc->qmin, stream);
+            // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; with
+            // no cliques the dual-gap sums ride along the last term's slice.
+            const bool fuse_gap = R == 0 && nt > 0;
+            GapFusion gf{alpha, u, Q, part};
+            for (int k = 0; k < nt; k++)
+                apply_ord_bins(k, sa, bins, k == 0 ? nullptr : sa, k == 0, fuse_gap && k == nt - 1 ? &gf : nullptr);
             if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));
             if (R > 0) {
                 DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
-                ucond_kernel<<<R, 256, 0, stream>>>(cl_off.get(), cl_idx.get(), L, Q, upos);
-                ucond_apply_kernel<<<1, 1, 0, stream>>>(R, upos, cl_const.get(), cl_exp.get(), su);
+                launch(ucond_kernel, R, 256, 0, stream, cl_off.get(), cl_idx.get(), L, Q, upos);
+                launch(ucond_apply_kernel, 1, 1, 0, stream, R, upos, cl_const.get(), cl_exp.get(), su);
             }
-            lp_gap_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(NL, alpha, u, sa, su, Q, part);
-            finalize_sums_kernel<<<1, 64, 0, stream>>>(part, kRedBlocks, 2, 0, sc);
-            lp_delta_kernel<<<1, 1, 0, stream>>>(sc, lambda);
-            lp_alpha_kernel<<<ceil_div(NL, 256), 256, 0, stream>>>(NL, sa, su, alpha, u, sc);
+            if (fuse_gap) {
+                launch(finalize_sums_kernel, 1, 64, 0, stream, part, slice_grid(NL), 2, 0, sc);
+            } else {
+                launch(lp_gap_kernel, kRedBlocks, kRedThreads, 0, stream, NL, alpha, u, sa, su, Q, part);
+                launch(finalize_sums_kernel, 1, 64, 0, stream, part, kRedBlocks, 2, 0, sc);
+            }
+            launch(lp_delta_kernel, 1, 1, 0, stream, sc, lambda);
             DCRF_LAUNCH_CHECK();
         } while (pit < p.fw_max_iter);
         fw_total += pit;
         with_lc(L, [&](auto lc) {
             constexpr int LC = decltype(lc)::value;
-            lp_project_kernel<LC><<<pg, kPix, 0, stream>>>(N, L, Q, lab);
+            launch(lp_project_kernel<LC>, pg, kPix, 0, stream, N, L, Q, lab);
         });
         const double prev_int_energy = int_energy;
         int_energy = energy_true(lab, true);
@@ -887,8 +940,8 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             }
         }
         if (p.less_confident_percent > 0) {
-            less_confident_kernel<<<kRedBlocks, kRedThreads, 0, stream>>>(N, L, bestQ, p.confidence_tol, part);
-            finalize_sums_kernel<<<1, 32, 0, stream>>>(part, kRedBlocks, 1, 0, sc);
+            launch(less_confident_kernel, kRedBlocks, kRedThreads, 0, stream, N, L, bestQ, p.confidence_tol, part);
+            launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
             fetch_scalars();
             const double percent = h_scal->sums[0] / (double)N * 100;
             if (percent > p.less_confident_percent) break;

@@ -47,6 +47,9 @@ typedef struct dcrf_model_s* dcrf_model;
 const char* dcrf_last_error(void);
 /* Library version string. */
 const char* dcrf_version(void);
+/* Number of CUDA kernels this process has launched through the library
+ * (diagnostics; no counterpart in the reference). */
+unsigned long long dcrf_kernel_launches(void);
 
 /* ------------------------------------------------------------------------
  * Permutohedral lattice -- class Permutohedral (include/permutohedral.h:50-88)

@@ -103,3 +103,28 @@ def test_state_and_argument_errors():
     with pytest.raises(DCRFError, match="ARG"):
         m.setCliques(np.array([0, 3], np.int32), np.array([0, 1, 64], np.int32),
                      np.ones(1, np.float32), np.ones(1, np.float32))
+
+
+def test_lp_full_size_bit_exact_to_reference(oracle_mod):
+    """The benchmark workload itself: 640x480, 21 labels, 50 proximal
+    iterations (500 Frank-Wolfe steps).  The GPU solve must reproduce the
+    reference's output bit for bit (SHA-256 of Q recorded from the bit-exact
+    CPU restatement by tests/golden/make_full_size.py)."""
+    import hashlib
+    import json
+    import os
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "lp_640x480_seed2.json")) as f:
+        rec = json.load(f)
+    img = synth.make_image(rec["W"], rec["H"], rec["L"], rec["seed"])
+    Q = oracle_mod.build_model(oracle_mod.OracleModel, img).unary_init()
+    assert hashlib.sha256(Q.tobytes()).hexdigest() == rec["init_sha256"]
+    m = DenseCRF2D(rec["W"], rec["H"], rec["L"])
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    out, st = m.lp_inference_prox_super_pixels(Q, stats=True, prox_max_iter=rec["prox_max_iter"],
+                                               prox_energy_tol=rec["prox_energy_tol"])
+    assert st.iterations == rec["prox_iters"]
+    assert hashlib.sha256(out.tobytes()).hexdigest() == rec["q_sha256"]
+    assert m.assignment_energy_true(m.currentMap(out)) == pytest.approx(rec["energy_true"], rel=1e-12)
