@@ -33,9 +33,9 @@ namespace {
 constexpr int kEmpty = -1;
 constexpr int kRes = 10;       // RESOLUTION (include/permutohedral.h:41)
 constexpr int kOrdW = 2 * kRes;  // lower + upper bins per (vertex, label)
-constexpr int kStageWarps = 4;   // warps (splat lists) per splat block
-constexpr int kStages = 4;       // shared-memory ring depth, in chunks
-constexpr int kChunk = 16;       // entries per chunk (8.5 KB of ring per warp: 24 warps / SM)
+constexpr int kStageWarps = 2;   // warps (splat lists) per splat block
+constexpr int kStages = 3;       // shared-memory ring depth, in chunks
+constexpr int kChunk = 32;       // entries per chunk (13 KB of ring per warp: 16 warps / SM)
 constexpr int kMaxOrderKey = (1 << 24) - 1;
 constexpr int kLongList = 64;    // lists longer than this use the staged warp kernels
 constexpr int kTB = 256;         // threads per block of the element-wise kernels
@@ -523,18 +523,27 @@ __global__ void ord_bins_kernel(long n, const float* __restrict__ Q, int* __rest
 
 // Each of the 10 bins accumulates, in entry order, the weights of the entries
 // that reach it: bins 0..c (lower pass) or c..9 (upper pass), addSplitArray
-// (:548-569).
+// (:548-569).  Branch-free and bit-identical: the mask m = sat(c - b + 1)
+// (lower) or sat(b - c + 1) (upper) is exactly 0 or 1, so fma(m, w, acc)
+// rounds acc + w once when the entry reaches the bin, and otherwise returns
+// acc (acc + (+-0) = acc: the accumulator starts at +0 and is never -0).
+template <bool UPPER>
+__device__ __forceinline__ void ord_accumulate(float (&acc)[kRes], int c, float w) {
+    const float cf = (float)c;
+#pragma unroll
+    for (int b = 0; b < kRes; b++) {
+        const float m = UPPER ? __saturatef(__fadd_rn((float)(b + 1), -cf)) : __saturatef(__fadd_rn(cf, (float)(1 - b)));
+        acc[b] = __fmaf_rn(m, w, acc[b]);
+    }
+}
+
 template <bool UPPER>
 __device__ __forceinline__ void ord_consume(float (&acc)[kRes], const int (*ring)[32], const float* mw, int lane,
                                             int n) {
 #pragma unroll 2
     for (int e = 0; e < n; e++) {
         const int word = ring[e][lane];
-        const int c = UPPER ? (word >> 8) : (word & 0xff);
-        const float w = mw[e];
-#pragma unroll
-        for (int b = 0; b < kRes; b++)
-            if (UPPER ? b >= c : b <= c) acc[b] = fadd(acc[b], w);
+        ord_accumulate<UPPER>(acc, UPPER ? (word >> 8) : (word & 0xff), mw[e]);
     }
 }
 
@@ -590,13 +599,9 @@ __global__ void ord_splat_short_kernel(int n_short, int L, const int* __restrict
 #pragma unroll 2
     for (int s = s0; s < s1; s++) {
         const int word = bins[(long)seg_pix[s] * L + k];
-        const int cl = word & 0xff, cu = word >> 8;
         const float w = seg_w[s];
-#pragma unroll
-        for (int b = 0; b < kRes; b++) {
-            lo[b] = fadd(lo[b], b <= cl ? w : 0.0f);
-            up[b] = fadd(up[b], b >= cu ? w : 0.0f);
-        }
+        ord_accumulate<false>(lo, word & 0xff, w);
+        ord_accumulate<true>(up, word >> 8, w);
     }
     float* row = vals + (long)(v + 1) * kOrdW * L + k;
 #pragma unroll

@@ -22,6 +22,49 @@ struct PixVec {
     static constexpr int S = LC > 0 ? LC : kLMax;
 };
 
+// ---------------------------------------------------------------------------
+// Row tiles: the [32][LC] rows of 32 consecutive pixels are contiguous in
+// global memory; a warp moves them through shared memory so that its global
+// loads and stores coalesce, while each lane works on one pixel's row
+// (stride LC; odd LC is bank-conflict free).  Rows of lanes >= npix hold
+// stale data and are never written back.
+constexpr int kTileWarps = 4;
+
+template <int LC>
+__device__ __forceinline__ void tile_in(float* buf, const float* __restrict__ g, long pix0, int npix, int lane) {
+    const float* src = g + pix0 * LC;
+    const int n = npix * LC;
+#pragma unroll
+    for (int j = 0; j < LC; j++) {
+        const int idx = j * 32 + lane;
+        if (idx < n) buf[idx] = src[idx];
+    }
+}
+
+template <int LC>
+__device__ __forceinline__ void tile_out(const float* buf, float* __restrict__ g, long pix0, int npix, int lane) {
+    float* dst = g + pix0 * LC;
+    const int n = npix * LC;
+#pragma unroll
+    for (int j = 0; j < LC; j++) {
+        const int idx = j * 32 + lane;
+        if (idx < n) dst[idx] = buf[idx];
+    }
+}
+
+// Sum of one double per thread over a block of any size (multiple of 32);
+// the result is valid in thread 0.  Fixed order: deterministic.
+__device__ __forceinline__ double block_sum_any(double v, double* s32) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) s32[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x == 0)
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s32[w];
+    return t;
+}
+
 namespace {
 
 // One warp per value: sums nblk partials in a fixed order.
@@ -34,6 +77,23 @@ __global__ void finalize_sums_kernel(const double* __restrict__ partials, int nb
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
     if (lane == 0) sc->sums[dst + j] = s;
+}
+
+// One 1024-thread block per value, for large partial counts: fixed order.
+__global__ void finalize_large_kernel(const double* __restrict__ partials, int nblk, int dst, SolverScalars* sc) {
+    __shared__ double s[32];
+    const int j = blockIdx.x;
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v += partials[(long)j * nblk + b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFullMask, v, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s[w];
+        sc->sums[dst + j] = t;
+    }
 }
 
 __global__ void dot_kernel(long n, const float* __restrict__ a, const float* __restrict__ b,
@@ -75,10 +135,11 @@ __global__ void minmax_partial_kernel(long n, const float* __restrict__ x, doubl
     }
 }
 
+// Launched with one block of any multiple of 32 threads (<= 1024).
 __global__ void minmax_finish_kernel(const double* __restrict__ partials, int nblk, SolverScalars* sc) {
-    const int lane = threadIdx.x;
+    __shared__ float smn[32], smx[32];
     float mn = INFINITY, mx = -INFINITY;
-    for (int b = lane; b < nblk; b += 32) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
         mn = fminf(mn, (float)partials[b]);
         mx = fmaxf(mx, (float)partials[nblk + b]);
     }
@@ -87,7 +148,16 @@ __global__ void minmax_finish_kernel(const double* __restrict__ partials, int nb
         mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
         mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
     }
-    if (lane == 0) {
+    if ((threadIdx.x & 31) == 0) {
+        smn[threadIdx.x >> 5] = mn;
+        smx[threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
+            mn = fminf(mn, smn[w]);
+            mx = fmaxf(mx, smx[w]);
+        }
         sc->qmin = mn;
         sc->qmax = mx;
     }

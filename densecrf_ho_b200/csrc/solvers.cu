@@ -369,15 +369,15 @@ __global__ void lp_gamma_kernel(int N, int Lrt, GammaConsts gc, const float* __r
 }
 
 // |qp_value - qp_value1| < qp_tol test (:670-674).
+// Launched with one block of any multiple of 32 threads.
 __global__ void lp_gamma_check_kernel(const double* __restrict__ partials, int nblk, float qp_tol,
                                       SolverScalars* sc) {
     if (sc->stop) return;
-    const int lane = threadIdx.x;
+    __shared__ double s32[32];
     double s = 0.0;
-    for (int b = lane; b < nblk; b += 32) s += partials[b];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
-    if (lane == 0) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partials[b];
+    s = block_sum_any(s, s32);
+    if (threadIdx.x == 0) {
         const float qv1 = (float)s;
         sc->steps++;
         if (fabsf(fsub(sc->qp_value, qv1)) < qp_tol) sc->stop = 1;
@@ -441,6 +441,225 @@ __global__ void lp_q_kernel(int N, int Lrt, float lambda, const float* __restric
         partials[blockIdx.x] = mn;
         partials[gridDim.x + blockIdx.x] = mx;
     }
+}
+
+// --------------------------------------------- row-tiled variants (L = LC) --
+// Same arithmetic as lp_y_kernel / lp_q_kernel / lp_gamma_kernel /
+// qp_direction_kernel, one warp per 32 pixels, rows staged in shared memory.
+
+template <int LC>
+__global__ void __launch_bounds__(32 * kTileWarps)
+    lp_y_tiled(int N, float lambda, float cm, float* __restrict__ alpha, float* __restrict__ u,
+               const float* __restrict__ U, const float* __restrict__ curQ, float* __restrict__ Y, bool pending,
+               const float* __restrict__ sa, const float* __restrict__ su, const SolverScalars* __restrict__ sc) {
+    __shared__ float sm[kTileWarps][2][32 * LC];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long pix0 = ((long)blockIdx.x * kTileWarps + wib) * 32;
+    if (pix0 >= N) return;
+    const int npix = (int)min(32L, (long)N - pix0);
+    float* A = sm[wib][0];
+    float* B = sm[wib][1];
+    float* ra = A + lane * LC;
+    float* rb = B + lane * LC;
+    const float dl = pending ? sc->delta : 0.0f;
+    float x[LC];
+    // alpha (+ pending update)
+    tile_in<LC>(A, alpha, pix0, npix, lane);
+    if (pending) tile_in<LC>(B, sa, pix0, npix, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < LC; k++) {
+        float a = ra[k];
+        if (pending) {
+            a = fadd(a, fmul(dl, fsub(rb[k], a)));
+            ra[k] = a;
+        }
+        x[k] = a;
+    }
+    __syncwarp();
+    if (pending) tile_out<LC>(A, alpha, pix0, npix, lane);
+    __syncwarp();
+    // u (+ pending update)
+    tile_in<LC>(A, u, pix0, npix, lane);
+    if (pending && su) tile_in<LC>(B, su, pix0, npix, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < LC; k++) {
+        float uu = ra[k];
+        if (pending) {
+            uu = fadd(uu, fmul(dl, fsub(su ? rb[k] : 0.0f, uu)));
+            ra[k] = uu;
+        }
+        x[k] = fadd(x[k], uu);
+    }
+    __syncwarp();
+    if (pending) tile_out<LC>(A, u, pix0, npix, lane);
+    __syncwarp();
+    // x = (alpha + u) - unary;  Y = multiplyC(x) + cur_Q
+    tile_in<LC>(A, U, pix0, npix, lane);
+    tile_in<LC>(B, curQ, pix0, npix, lane);
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < LC; k++) x[k] = fsub(x[k], ra[k]);
+    const float s = eig_sum_ct<LC, 0>(x);
+#pragma unroll
+    for (int k = 0; k < LC; k++) rb[k] = fadd(fmul(fadd(fmul(cm, s), x[k]), lambda), rb[k]);
+    __syncwarp();
+    tile_out<LC>(B, Y, pix0, npix, lane);
+}
+
+template <int LC>
+__global__ void __launch_bounds__(32 * kTileWarps)
+    lp_q_tiled(int N, float lambda, const float* __restrict__ alpha, const float* __restrict__ u,
+               const float* __restrict__ gamma, const float* __restrict__ U, const float* __restrict__ curQ,
+               float* __restrict__ Q, double* __restrict__ partials) {
+    __shared__ float sm[kTileWarps][4][32 * LC];
+    __shared__ float smn[kTileWarps], smx[kTileWarps];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long pix0 = ((long)blockIdx.x * kTileWarps + wib) * 32;
+    float mn = INFINITY, mx = -INFINITY;
+    if (pix0 < N) {
+        const int npix = (int)min(32L, (long)N - pix0);
+        float* T[4] = {sm[wib][0], sm[wib][1], sm[wib][2], sm[wib][3]};
+        tile_in<LC>(T[0], alpha, pix0, npix, lane);
+        tile_in<LC>(T[1], u, pix0, npix, lane);
+        tile_in<LC>(T[2], gamma, pix0, npix, lane);
+        tile_in<LC>(T[3], U, pix0, npix, lane);
+        __syncwarp();
+        const float *ra = T[0] + lane * LC, *ru = T[1] + lane * LC, *rg = T[2] + lane * LC, *rU = T[3] + lane * LC;
+        float t[LC];
+#pragma unroll
+        for (int k = 0; k < LC; k++) t[k] = fsub(fadd(fadd(ra[k], ru[k]), rg[k]), rU[k]);
+        const float beta = (-col_sum<LC>(t, LC, pix0 + lane)) / (float)LC;
+#pragma unroll
+        for (int k = 0; k < LC; k++) t[k] = fsub(fadd(fadd(fadd(ra[k], beta), ru[k]), rg[k]), rU[k]);
+        __syncwarp();
+        tile_in<LC>(T[0], curQ, pix0, npix, lane);
+        __syncwarp();
+        float* rq = T[0] + lane * LC;
+        const bool act = lane < npix;
+#pragma unroll
+        for (int k = 0; k < LC; k++) {
+            const float q = fadd(fmul(t[k], lambda), rq[k]);
+            rq[k] = q;
+            if (act) {
+                mn = fminf(mn, q);
+                mx = fmaxf(mx, q);
+            }
+        }
+        __syncwarp();
+        tile_out<LC>(T[0], Q, pix0, npix, lane);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+    }
+    if (lane == 0) {
+        smn[wib] = mn;
+        smx[wib] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kTileWarps; w++) {
+            mn = fminf(mn, smn[w]);
+            mx = fmaxf(mx, smx[w]);
+        }
+        partials[blockIdx.x] = mn;
+        partials[gridDim.x + blockIdx.x] = mx;
+    }
+}
+
+template <int LC>
+__global__ void __launch_bounds__(32 * kTileWarps)
+    lp_gamma_tiled(int N, GammaConsts gc, const float* __restrict__ Y, float* __restrict__ gamma,
+                   const SolverScalars* __restrict__ sc, double* __restrict__ partials) {
+    if (sc->stop) return;  // uniform across the grid
+    __shared__ float sm[kTileWarps][2][32 * LC];
+    __shared__ double s32[32];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long pix0 = ((long)blockIdx.x * kTileWarps + wib) * 32;
+    double acc = 0.0;
+    if (pix0 < N) {
+        const int npix = (int)min(32L, (long)N - pix0);
+        float* G = sm[wib][0];
+        float* Yt = sm[wib][1];
+        tile_in<LC>(G, gamma, pix0, npix, lane);
+        tile_in<LC>(Yt, Y, pix0, npix, lane);
+        __syncwarp();
+        float* rg = G + lane * LC;
+        const float* ry = Yt + lane * LC;
+        float g[LC], t[LC];
+#pragma unroll
+        for (int k = 0; k < LC; k++) g[k] = rg[k];
+        const float s = eig_sum_ct<LC, 0>(g);
+#pragma unroll
+        for (int k = 0; k < LC; k++) {
+            const float y = ry[k];
+            const float ph = (-y < 0.0f) ? 0.0f : -y;  // std::max(-Y, 0)
+            const float nh = (y < 0.0f) ? 0.0f : y;    // std::max(Y, 0)
+            float st = fadd(fmul(fsub(s, g[k]), gc.c0), ph);
+            st = fadd(st, gc.delta);
+            float tt = fmul(fadd(fmul(gc.c1, s), fmul(gc.c2, g[k])), gc.lambda);
+            tt = fadd(tt, nh);
+            tt = fadd(tt, gc.delta);
+            g[k] = fmul(g[k], st / tt);
+            rg[k] = g[k];
+        }
+        const float s2 = eig_sum_ct<LC, 0>(g);
+#pragma unroll
+        for (int k = 0; k < LC; k++) t[k] = fmul(g[k], fmul(fadd(fmul(gc.cm, s2), g[k]), gc.lambda));
+        const float d1 = eig_sum_ct<LC, 0>(t);
+#pragma unroll
+        for (int k = 0; k < LC; k++) t[k] = fmul(g[k], ry[k]);
+        const float d2 = eig_sum_ct<LC, 0>(t);
+        if (lane < npix) acc = (double)(float)dadd(dmul(0.5, (double)d1), (double)d2);
+        __syncwarp();
+        tile_out<LC>(G, gamma, pix0, npix, lane);
+    }
+    const double tot = block_sum_any(acc, s32);
+    if (threadIdx.x == 0) partials[blockIdx.x] = tot;
+}
+
+template <int LC>
+__global__ void __launch_bounds__(32 * kTileWarps)
+    qp_direction_tiled(int N, const float* __restrict__ grad, const float* __restrict__ Q,
+                       const float* __restrict__ U, float* __restrict__ sx, double* __restrict__ partials) {
+    __shared__ float sm[kTileWarps][3][32 * LC];
+    __shared__ double s32[32];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long pix0 = ((long)blockIdx.x * kTileWarps + wib) * 32;
+    double acc = 0.0;
+    if (pix0 < N) {
+        const int npix = (int)min(32L, (long)N - pix0);
+        float *Gt = sm[wib][0], *Qt = sm[wib][1], *Ut = sm[wib][2];
+        tile_in<LC>(Gt, grad, pix0, npix, lane);
+        tile_in<LC>(Qt, Q, pix0, npix, lane);
+        tile_in<LC>(Ut, U, pix0, npix, lane);
+        __syncwarp();
+        const float* rg = Gt + lane * LC;
+        float* rq = Qt + lane * LC;
+        const float* ru = Ut + lane * LC;
+        float best = rg[0];
+        int bi = 0;
+#pragma unroll
+        for (int k = 1; k < LC; k++)
+            if (rg[k] < best) {
+                best = rg[k];
+                bi = k;
+            }
+        const bool act = lane < npix;
+#pragma unroll
+        for (int k = 0; k < LC; k++) {
+            const float s = fsub(k == bi ? 1.0f : 0.0f, rq[k]);
+            rq[k] = s;
+            if (act) acc += (double)ru[k] * (double)s;
+        }
+        __syncwarp();
+        tile_out<LC>(Qt, sx, pix0, npix, lane);
+    }
+    const double tot = block_sum_any(acc, s32);
+    if (threadIdx.x == 0) partials[blockIdx.x] = tot;
 }
 
 // Partial sums of tmp.Q and tmp.tmp, tmp = (alpha + u) - (sa + su) (:725-729).
@@ -710,6 +929,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
     SolverScalars* sc = scal.get();
     double* part = partials.get();
     const int nt = (int)terms.size();
+    const int tgrid = ceil_div(ceil_div(N, 32), kTileWarps);  // row-tiled kernels
 
     CliqueView cv{};
     float *gz = nullptr, *z = nullptr, *sxz = nullptr, *t1 = nullptr, *t2 = nullptr, *cz = nullptr, *zc = nullptr,
@@ -755,9 +975,15 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
         with_lc(L, [&](auto lc) {
             constexpr int LC = decltype(lc)::value;
-            launch(qp_direction_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, grad, Q, unary.get(), sx, part);
+            if constexpr (LC > 0) {
+                launch(qp_direction_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, grad, Q, unary.get(), sx, part);
+                launch(finalize_large_kernel, 1, 1024, 0, stream, part, tgrid, 0, sc);
+            } else {
+                launch(qp_direction_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, grad, Q, unary.get(), sx,
+                       part);
+                launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
+            }
         });
-        launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
         if (R > 0) {
             launch(ho_direction_kernel, 1, 256, 0, stream, cv, L, gz, z, sxz, t1, t2, cz, sc);
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, Q, 1, 3, sc, 0);    // a
@@ -809,6 +1035,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     double* part = partials.get();
     const int nt = (int)terms.size();
     const int pg = ceil_div(N, kPix);
+    const int tgrid = ceil_div(ceil_div(N, 32), kTileWarps);  // row-tiled kernels
 
     DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
     with_lc(L, [&](auto lc) {
@@ -860,8 +1087,12 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             const bool pending = pit > 1;
             with_lc(L, [&](auto lc) {
                 constexpr int LC = decltype(lc)::value;
-                launch(lp_y_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y,
-                       pending, sa, su, sc);
+                if constexpr (LC > 0)
+                    launch(lp_y_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, lambda, gc.cm, alpha, u, unary.get(),
+                           curQ, Y, pending, sa, su, sc);
+                else
+                    launch(lp_y_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y,
+                           pending, sa, su, sc);
             });
             launch(lp_gamma_reset_kernel, 1, 1, 0, stream, sc);
             // qp-gamma iterations; the reference needs at least two (its first
@@ -873,9 +1104,15 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
                 for (int bi = 0; bi < batch; bi++) {
                     with_lc(L, [&](auto lc) {
                         constexpr int LC = decltype(lc)::value;
-                        launch(lp_gamma_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, gc, Y, gamma, sc, part);
+                        if constexpr (LC > 0) {
+                            launch(lp_gamma_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, gc, Y, gamma, sc, part);
+                            launch(lp_gamma_check_kernel, 1, 1024, 0, stream, part, tgrid, p.qp_tol, sc);
+                        } else {
+                            launch(lp_gamma_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, gc, Y, gamma, sc,
+                                   part);
+                            launch(lp_gamma_check_kernel, 1, 1024, 0, stream, part, kRedBlocks, p.qp_tol, sc);
+                        }
                     });
-                    launch(lp_gamma_check_kernel, 1, 32, 0, stream, part, kRedBlocks, p.qp_tol, sc);
                 }
                 launched += batch;
                 DCRF_LAUNCH_CHECK();
@@ -887,10 +1124,16 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             // rescale(Q) once for all pairwise terms.
             with_lc(L, [&](auto lc) {
                 constexpr int LC = decltype(lc)::value;
-                launch(lp_q_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q,
-                       part);
+                if constexpr (LC > 0) {
+                    launch(lp_q_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, lambda, alpha, u, gamma, unary.get(),
+                           curQ, Q, part);
+                    launch(minmax_finish_kernel, 1, 1024, 0, stream, part, tgrid, sc);
+                } else {
+                    launch(lp_q_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q,
+                           part);
+                    launch(minmax_finish_kernel, 1, 1024, 0, stream, part, pg, sc);
+                }
             });
-            launch(minmax_finish_kernel, 1, 32, 0, stream, part, pg, sc);
             rescaled_bins(bins, Q, NL, &sc->qmin, stream);
             // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; with
             // no cliques the dual-gap sums ride along the last term's slice.
@@ -905,7 +1148,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
                 launch(ucond_apply_kernel, 1, 1, 0, stream, R, upos, cl_const.get(), cl_exp.get(), su);
             }
             if (fuse_gap) {
-                launch(finalize_sums_kernel, 1, 64, 0, stream, part, slice_grid(NL), 2, 0, sc);
+                launch(finalize_large_kernel, 2, 1024, 0, stream, part, slice_grid(NL), 0, sc);
             } else {
                 launch(lp_gap_kernel, kRedBlocks, kRedThreads, 0, stream, NL, alpha, u, sa, su, Q, part);
                 launch(finalize_sums_kernel, 1, 64, 0, stream, part, kRedBlocks, 2, 0, sc);
