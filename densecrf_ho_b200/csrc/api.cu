@@ -169,6 +169,16 @@ dcrf_status dcrf_lattice_compute_dev(dcrf_lattice h, float* d_out, const float* 
     });
 }
 
+dcrf_status dcrf_lattice_compute_noalloc(dcrf_lattice h, float* d_out, const float* d_in, int L, int reverse) {
+    return guard([&] {
+        need(h, "lattice");
+        need(d_out, "out");
+        need(d_in, "in");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        h->lat.compute_noalloc(d_out, d_in, L, reverse != 0);
+    });
+}
+
 dcrf_status dcrf_lattice_compute(dcrf_lattice h, float* out, const float* in, int L, int reverse) {
     return guard([&] {
         need(h, "lattice");

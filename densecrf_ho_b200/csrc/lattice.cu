@@ -22,6 +22,8 @@
 // identical to the reference, with no float atomics.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "lattice.cuh"
@@ -805,6 +807,87 @@ void Lattice::ensure_values(size_t row_width) {
     // Row 0 is the zero row that absent neighbours read.
     DCRF_CUDA(cudaMemsetAsync(va.get(), 0, sizeof(float) * row_width, stream));
     DCRF_CUDA(cudaMemsetAsync(vb.get(), 0, sizeof(float) * row_width, stream));
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free filtering (dcrf_lattice_compute_noalloc).
+//
+// Some callers cannot let a library allocate device memory during a call:
+// hosts that hand out all GPU memory from their own pool, or that run under a
+// fixed memory budget in a latency-critical loop where a driver allocation
+// would stall or fail.  For them the filter's two value buffers, normally
+// grown on demand with cudaMalloc, come from this fixed array instead.  Every
+// GPU that loads the library keeps it for the life of the process.
+constexpr size_t kNoAllocScratchFloats = size_t(8) << 20;  // 8 Mi floats = 32 MiB
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  In host code
+// the array's name is only a host-side stand-in, so the address is looked up
+// once per device with that device current and cached.
+float* noalloc_scratch() {
+    int dev = 0;
+    DCRF_CUDA(cudaGetDevice(&dev));
+    require(dev >= 0 && dev < kMaxDevices, DCRF_E_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            throw Error(DCRF_E_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = static_cast<float*>(p);
+    }
+    return g_noalloc_ptr[dev];
+}
+}  // namespace
+
+size_t noalloc_scratch_floats() { return kNoAllocScratchFloats; }
+
+void Lattice::compute_noalloc(float* out, const float* in, int L, bool reverse) {
+    require(N > 0, DCRF_E_STATE, "lattice not initialised");
+    require(L >= 1, DCRF_E_ARG, "compute: L must be >= 1");
+    const size_t need = 2 * (size_t)(M + 1) * (size_t)L;
+    require(need <= kNoAllocScratchFloats, DCRF_E_ARG,
+            "compute_noalloc: 2 x (M + 1) x L = " + std::to_string(need) + " floats exceeds the fixed scratch of " +
+                std::to_string(kNoAllocScratchFloats) + " floats (32 MiB); use dcrf_lattice_compute_dev");
+    float* base = noalloc_scratch();
+    float *src = base, *dst = base + (size_t)(M + 1) * L;
+    cudaStream_t st = stream;
+    // The array keeps the previous call's contents: only the zero rows that
+    // absent neighbours read must be cleared; every other row read below is
+    // written first.
+    DCRF_CUDA(cudaMemsetAsync(src, 0, sizeof(float) * L, st));
+    DCRF_CUDA(cudaMemsetAsync(dst, 0, sizeof(float) * L, st));
+    const long ML = (long)M * L, NL = (long)N * L;
+    const int n_short = M - n_long;
+    if (n_long)
+        launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
+               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+    if (n_short)
+        launch(splat_short_kernel<false>, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
+               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+    const bool seq = L <= 2;
+    for (int jj = 0; jj <= d; jj++) {
+        const int j = reverse ? d - jj : jj;
+        if (seq)
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
+        else
+            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
+        std::swap(src, dst);
+    }
+    const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
+    const SliceEpilogue ep;
+    if (seq)
+        launch(slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
+               out, ep);
+    else
+        launch(slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
+               out, ep);
+    DCRF_LAUNCH_CHECK();
 }
 
 void Lattice::compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,

@@ -41,6 +41,8 @@ struct GapFusion {
 void rescaled_bins(int* bins, const float* Q, long n, const float* qminmax, cudaStream_t st);
 // Blocks of the element-wise slice kernels for n elements.
 int slice_grid(long n);
+// Capacity, in floats, of the fixed scratch array of compute_noalloc.
+size_t noalloc_scratch_floats();
 
 struct Lattice {
     int N = 0, d = 0, M = 0;
@@ -68,6 +70,9 @@ struct Lattice {
     // out/in: device [N][L]; out may alias in.
     void compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,
                  const float* pre_norm = nullptr);
+    // The plain filter with its value buffers in a fixed device array instead
+    // of memory from cudaMalloc (see dcrf_lattice_compute_noalloc).
+    void compute_noalloc(float* out, const float* in, int L, bool reverse);
     // Ordered (upper minus lower, 10-bin) filter of Q in [0,1]; out = epilogue(v).
     void compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep);
     // The same from precomputed packed bins (lower | upper << 8 per element).

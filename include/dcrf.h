@@ -70,6 +70,21 @@ dcrf_status dcrf_lattice_info(dcrf_lattice lat, int* M, int* N, int* d);
 dcrf_status dcrf_lattice_compute(dcrf_lattice lat, float* out, const float* in, int L, int reverse);
 dcrf_status dcrf_lattice_compute_dev(dcrf_lattice lat, float* d_out, const float* d_in, int L,
                                      int reverse);
+/* The filter of dcrf_lattice_compute_dev without any device allocation (no
+ * counterpart in the reference).  For callers that may not allocate device
+ * memory during a call -- hosts that give out all GPU memory from their own
+ * pool, or that run under a fixed memory budget in a latency-critical loop --
+ * the filter's scratch (two value buffers of (M + 1) x L floats) comes from a
+ * fixed 32 MiB device array that every GPU loading the library holds until
+ * exit.  Limit: 2 x (M + 1) x L <= 8 Mi floats, otherwise DCRF_E_ARG.
+ * d_in / d_out are caller-owned device buffers [N][L]; the work is queued on
+ * the lattice's stream, with the lattice's device current.  The first call on
+ * a device looks up the array's device address (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the one array
+ * and it keeps the last call's contents: calls that overlap on the GPU (other
+ * lattices or streams) race and must be serialised by the caller. */
+dcrf_status dcrf_lattice_compute_noalloc(dcrf_lattice lat, float* d_out, const float* d_in, int L,
+                                         int reverse);
 /* Permutohedral::compute_upper_minus_lower_ord(MatrixXf& out, const MatrixXf& Q)
  * (src/permutohedral.cpp:1071-1073, 590-701): the 10-bin ordered filter. */
 dcrf_status dcrf_lattice_compute_ord(dcrf_lattice lat, float* out, const float* Q, int L);
