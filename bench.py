@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--size", default="640x480")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--only-roofline", action="store_true",
+                    help="time only the ordered and plain lattice filters (a short command for ncu)")
     ap.add_argument("--prox-iters", type=int, default=50,
                     help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
     return ap.parse_args()
@@ -273,6 +275,113 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ ours --
+def measure_filters(W, H, img, reps=20):
+    """Times the ordered filter (the LP's dominant operation) and the plain
+    splat/blur/slice filter on the bilateral and Gaussian lattices of the
+    workload image, with CUDA events on each lattice's own stream."""
+    import torch
+    from densecrf_ho_b200 import Permutohedral, lib, check
+    Ls = lib()
+    N = W * H
+    roof = {}
+    rq = torch.rand((N, L), device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    ro = torch.empty_like(rq)
+    feats = {"bilateral": synth.bilateral_features(W, H, BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
+                                                   img["rgb"]),
+             "gaussian": synth.gaussian_features(W, H, GAUSS[0], GAUSS[0])}
+    for name, f in feats.items():
+        lat = Permutohedral().init(f)
+        lptr = C.c_void_p()
+        check(Ls.dcrf_lattice_stream(lat._h, C.byref(lptr)))
+        ls = torch.cuda.ExternalStream(lptr.value)
+        run = lambda: check(Ls.dcrf_lattice_compute_ord_dev(lat._h, C.c_void_p(ro.data_ptr()),
+                                                            C.c_void_p(rq.data_ptr()), L))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ls)
+        for _ in range(reps):
+            run()
+        e1.record(ls)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / reps / 1e3
+        ab = ord_filter_bytes(N, lat.M, lat.d)
+        roof[name] = dict(M=lat.M, d=lat.d, seconds=t, bytes=ab, gbs=ab / t / 1e9)
+        # plain splat/blur/slice filter: the lattice-filter metric
+        x = torch.rand((N, L), device="cuda")
+        y = torch.empty_like(x)
+        runp = lambda: check(Ls.dcrf_lattice_compute_dev(lat._h, C.c_void_p(y.data_ptr()),
+                                                          C.c_void_p(x.data_ptr()), L, 0))
+        for _ in range(3):
+            runp()
+        torch.cuda.synchronize()
+        e0.record(ls)
+        for _ in range(reps):
+            runp()
+        e1.record(ls)
+        torch.cuda.synchronize()
+        tp = e0.elapsed_time(e1) / reps / 1e3
+        fb = filter_bytes(N, lat.M, lat.d)
+        roof[name].update(filter_seconds=tp, filter_bytes=fb, filter_gbs=fb / tp / 1e9,
+                          filter_gpix_label_s=N * L / tp / 1e9)
+        del lat
+    return roof
+
+
+def measure_qp(reps=10, cpu=True):
+    """Config 1: the plain QP (Frank-Wolfe, up to 100 iterations; it stops earlier
+    when the step numerator is exactly zero, as the reference does) on a
+    320x240 image.  Device-resident solves/s, the set-up (two lattice builds +
+    normalisation) time, and the reference's own CPU time for the same solve."""
+    import torch
+    from densecrf_ho_b200 import DenseCRF2D, SolveStats, lib, check
+    Ls = lib()
+    W, H = 320, 240
+    img = synth.make_image(W, H, L, 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    crf = DenseCRF2D(W, H, L)
+    crf.setUnaryEnergy(img["unary"])
+    crf.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+    crf.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"], BILAT[2])
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    Q0 = crf.unary_init()
+    init = torch.from_numpy(Q0).cuda()
+    out = torch.empty_like(init)
+    p = C.c_int(100)
+    st = SolveStats()
+    sptr = C.c_void_p()
+    check(Ls.dcrf_model_stream(crf.handle, C.byref(sptr)))
+    stream = torch.cuda.ExternalStream(sptr.value)
+    run = lambda: check(Ls.dcrf_model_qp_dev(crf.handle, C.c_void_p(init.data_ptr()), C.c_void_p(out.data_ptr()),
+                                             C.byref(p), C.byref(st)))
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    res = {"workload": "qp_inference_super_pixels_non_convex 320x240 L=21, max_iter=100",
+           "solves_per_s": 1e3 / ms, "ms_per_solve": ms, "fw_steps": st.iterations, "setup_ms": setup_ms}
+    if cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as O
+        cls = O.ReferenceModel if O.reference_available() else O.OracleModel
+        m = O.build_model(cls, img, gaussian=GAUSS, bilateral=BILAT)
+        t0 = time.perf_counter()
+        _, it, _ = m.qp(Q0, 100)
+        dt = time.perf_counter() - t0
+        res["cpu_reference"] = {"seconds_per_solve": dt, "cores": 1, "fw_steps": it,
+                                "kind": "reference" if O.reference_available() else "port"}
+        res["cpu_vs_gpu"] = dt * 1e3 / ms
+    return res
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -287,6 +396,9 @@ def run_ours(args):
     N = W * H
     seed = replica_seed(args.seed, rank)
     img = synth.make_image(W, H, L, seed)
+    if args.only_roofline:
+        print(json.dumps(measure_filters(W, H, img, reps=3)))
+        return
     t0 = time.perf_counter()
     crf = DenseCRF2D(W, H, L)
     crf.setUnaryEnergy(img["unary"])
@@ -350,54 +462,8 @@ def run_ours(args):
     e2e_value = world * args.steps / (ms_e2e / 1e3)
     same = bool(torch.equal(out_h, out_d.cpu()))
 
-    # Roofline of the dominant operation: the ordered filter on the model's
-    # bilateral and Gaussian lattices (separate Permutohedral objects with the
-    # same features), timed with events on the lattice's own stream.
+    roof = measure_filters(W, H, img, reps=20)
     peak, peak_kind = measured_peaks()
-    roof = {}
-    rq = torch.rand((N, L), device="cuda", generator=torch.Generator("cuda").manual_seed(0))
-    ro = torch.empty_like(rq)
-    feats = {"bilateral": synth.bilateral_features(W, H, BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
-                                                   img["rgb"]),
-             "gaussian": synth.gaussian_features(W, H, GAUSS[0], GAUSS[0])}
-    reps = 20
-    for name, f in feats.items():
-        lat = Permutohedral().init(f)
-        lptr = C.c_void_p()
-        check(Ls.dcrf_lattice_stream(lat._h, C.byref(lptr)))
-        ls = torch.cuda.ExternalStream(lptr.value)
-        run = lambda: check(Ls.dcrf_lattice_compute_ord_dev(lat._h, C.c_void_p(ro.data_ptr()),
-                                                            C.c_void_p(rq.data_ptr()), L))
-        for _ in range(3):
-            run()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(ls)
-        for _ in range(reps):
-            run()
-        e1.record(ls)
-        torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) / reps / 1e3
-        ab = ord_filter_bytes(N, lat.M, lat.d)
-        roof[name] = dict(M=lat.M, d=lat.d, seconds=t, bytes=ab, gbs=ab / t / 1e9)
-        # plain splat/blur/slice filter for the secondary lattice-filter metric
-        x = torch.rand((N, L), device="cuda")
-        y = torch.empty_like(x)
-        runp = lambda: check(Ls.dcrf_lattice_compute_dev(lat._h, C.c_void_p(y.data_ptr()),
-                                                          C.c_void_p(x.data_ptr()), L, 0))
-        for _ in range(3):
-            runp()
-        torch.cuda.synchronize()
-        e0.record(ls)
-        for _ in range(reps):
-            runp()
-        e1.record(ls)
-        torch.cuda.synchronize()
-        tp = e0.elapsed_time(e1) / reps / 1e3
-        fb = filter_bytes(N, lat.M, lat.d)
-        roof[name].update(filter_seconds=tp, filter_bytes=fb, filter_gbs=fb / tp / 1e9,
-                          filter_gpix_label_s=N * L / tp / 1e9)
-        del lat
     dom = roof["bilateral"]
     traffic = None
     if os.path.exists(ROOFLINE_TRAFFIC):
@@ -427,6 +493,8 @@ def run_ours(args):
                       "lattice_filter_gpix_label_s": {k: v["filter_gpix_label_s"] for k, v in roof.items()},
                       "lattice_filter_gbs": {k: v["filter_gbs"] for k, v in roof.items()},
                       "ord_filter_ms": {k: v["seconds"] * 1e3 for k, v in roof.items()}}}
+    if rank == 0 and world == 1:
+        line["extra"]["qp_320x240"] = measure_qp(cpu=not args.no_cpu_baseline)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference(W, H, args.seed, prox_iters, 1, 10, 1)
