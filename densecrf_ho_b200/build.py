@@ -81,5 +81,27 @@ def build(force: bool = False, verbose: bool = False) -> str:
     return LIB
 
 
+SHIM_DIR = os.path.join(PKG, "cpp")
+SHIM_BIN = os.path.join(SHIM_DIR, "shim_selftest")
+
+
+def build_shim(eigen_include: str) -> str:
+    """Compiles the drop-in C++ API self-test (densecrf_ho_b200/cpp) with g++
+    against `eigen_include` (a directory holding Eigen/Core, e.g. the one the
+    reference vendors) and libdcrf_cuda.so."""
+    lib = build()
+    src = os.path.join(SHIM_DIR, "shim_selftest.cpp")
+    deps = [src] + glob.glob(os.path.join(SHIM_DIR, "*.h")) + [lib]
+    if os.path.exists(SHIM_BIN) and all(os.path.getmtime(p) <= os.path.getmtime(SHIM_BIN) for p in deps):
+        return SHIM_BIN
+    cmd = ["g++", "-std=c++14", "-O2", "-w", "-I", INCLUDE, "-I", SHIM_DIR, "-I", eigen_include,
+           "-I", "/usr/local/cuda/include", src, "-o", SHIM_BIN, "-L", PKG, "-ldcrf_cuda",
+           "-Wl,-rpath,$ORIGIN/.."]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"shim build failed:\n{r.stderr}")
+    return SHIM_BIN
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,394 @@
+// densecrf.h -- drop-in C++ API of densecrf_ho, running on the B200 engine.
+//
+// The classes and signatures below are those of the reference's public
+// headers (include/densecrf.h:43-194, include/pairwise.h:33-95,
+// include/permutohedral.h:50-88, include/labelcompatibility.h,
+// include/unary.h); a caller switches by putting this directory first on its
+// include path and linking libdcrf_cuda.so.  Every method forwards to the C
+// ABI of include/dcrf.h; errors the reference reports with exceptions
+// ("Value out of bounds", "Maxval < 0, skipping") are thrown as
+// std::runtime_error with the same text, every other failure too.
+//
+// Scope (the B200 path): Potts compatibilities, DIAG_KERNEL with
+// NORMALIZE_SYMMETRIC (and its NO_NORMALIZATION copy), constant unaries, the
+// qp / lp / qp_sp / lp_sp solvers.  Superpixel cliques are given as a
+// per-pixel region map (addSuperPixel's segmentation step, EDISON mean-shift,
+// stays with the caller); the clique weights are derived from the image
+// exactly as src/densecrf.cpp:212-247 does.  Other compatibilities, kernel
+// types and normalisations throw std::runtime_error.
+//
+// Header-only; needs Eigen (the reference vendors 3.2.7) and include/dcrf.h.
+#pragma once
+#include <Eigen/Core>
+
+#include <cmath>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "dcrf.h"
+
+using namespace Eigen;
+
+typedef Matrix<short, Dynamic, 1> VectorXs;
+
+namespace dcrf_shim {
+inline void check(dcrf_status s) {
+    if (s != DCRF_OK) throw std::runtime_error(dcrf_last_error());
+}
+}  // namespace dcrf_shim
+
+// ---------------------------------------------------------------- pairwise.h --
+enum NormalizationType { NO_NORMALIZATION, NORMALIZE_BEFORE, NORMALIZE_AFTER, NORMALIZE_SYMMETRIC };
+enum KernelType { CONST_KERNEL, DIAG_KERNEL, FULL_KERNEL };
+
+// ------------------------------------------------------ labelcompatibility.h --
+class LabelCompatibility {
+public:
+    virtual ~LabelCompatibility() {}
+    // Potts weight w of mu(a, b) = -w [a == b]; only Potts runs on the B200 path.
+    virtual bool potts(float* w) const { return false; }
+};
+
+class PottsCompatibility : public LabelCompatibility {
+protected:
+    float w_;
+public:
+    PottsCompatibility(float weight = 1.0) : w_(weight) {}
+    bool potts(float* w) const override {
+        *w = w_;
+        return true;
+    }
+    VectorXf parameters() const {
+        VectorXf r(1);
+        r[0] = w_;
+        return r;
+    }
+    void setParameters(const VectorXf& v) { w_ = v[0]; }
+};
+
+class DiagonalCompatibility : public LabelCompatibility {
+public:
+    DiagonalCompatibility(const VectorXf&) {}
+};
+
+class MatrixCompatibility : public LabelCompatibility {
+public:
+    MatrixCompatibility(const MatrixXf&) {}
+};
+
+namespace dcrf_shim {
+// Takes ownership of f (as the reference does) and returns its Potts weight.
+inline float potts_weight(LabelCompatibility* f) {
+    std::unique_ptr<LabelCompatibility> own(f);
+    float w = 0;
+    if (!f || !f->potts(&w))
+        throw std::runtime_error("only PottsCompatibility runs on the B200 path");
+    return w;
+}
+inline void check_kernel(KernelType k, NormalizationType n) {
+    if (k != DIAG_KERNEL && k != CONST_KERNEL)
+        throw std::runtime_error("only DIAG_KERNEL pairwise kernels run on the B200 path");
+    if (n != NORMALIZE_SYMMETRIC)
+        throw std::runtime_error("only NORMALIZE_SYMMETRIC pairwise kernels run on the B200 path");
+}
+}  // namespace dcrf_shim
+
+// -------------------------------------------------------------------- unary.h --
+class UnaryEnergy {
+public:
+    virtual ~UnaryEnergy() {}
+    virtual MatrixXf get() const = 0;
+};
+
+class ConstUnaryEnergy : public UnaryEnergy {
+protected:
+    MatrixXf unary_;
+public:
+    ConstUnaryEnergy(const MatrixXf& unary) : unary_(unary) {}
+    MatrixXf get() const override { return unary_; }
+};
+
+// ------------------------------------------------------------ permutohedral.h --
+class Permutohedral {
+    dcrf_lattice h_ = nullptr;
+    int N_ = 0, M_ = 0, d_ = 0;
+    Permutohedral(const Permutohedral&) = delete;
+    Permutohedral& operator=(const Permutohedral&) = delete;
+public:
+    Permutohedral() { dcrf_shim::check(dcrf_lattice_create(&h_)); }
+    ~Permutohedral() {
+        if (h_) dcrf_lattice_destroy(h_);
+    }
+    // Permutohedral::init (src/permutohedral.cpp:152): features d x N.
+    void init(const MatrixXf& features) {
+        d_ = (int)features.rows();
+        N_ = (int)features.cols();
+        dcrf_shim::check(dcrf_lattice_init(h_, features.data(), d_, N_));
+        dcrf_shim::check(dcrf_lattice_info(h_, &M_, nullptr, nullptr));
+    }
+    MatrixXf compute(const MatrixXf& v, bool reverse = false) const {
+        MatrixXf r;
+        compute(r, v, reverse);
+        return r;
+    }
+    // Permutohedral::compute (src/permutohedral.cpp:1079): in L x N.
+    void compute(MatrixXf& out, const MatrixXf& in, bool reverse = false) const {
+        MatrixXf src = in;  // out may alias in
+        out.resize(in.rows(), in.cols());
+        dcrf_shim::check(dcrf_lattice_compute(h_, out.data(), src.data(), (int)in.rows(), reverse ? 1 : 0));
+    }
+    // Permutohedral::compute_upper_minus_lower_ord (src/permutohedral.cpp:1071).
+    void compute_upper_minus_lower_ord(MatrixXf& out, const MatrixXf& Q) {
+        out.resize(Q.rows(), Q.cols());
+        dcrf_shim::check(dcrf_lattice_compute_ord(h_, out.data(), Q.data(), (int)Q.rows()));
+    }
+    int size() const { return M_; }
+};
+
+// ---------------------------------------------------------------- densecrf.h --
+class LP_inf_params {
+public:
+    float prox_reg_const, dual_gap_tol, prox_energy_tol;
+    int prox_max_iter, fw_max_iter, qp_max_iter;
+    float qp_tol, qp_const;
+    bool best_int, accel_prox;
+    int work_set_size, approx_fw_iter;
+    float less_confident_percent, confidence_tol;
+    LP_inf_params(float prox_reg_const, float dual_gap_tol, float prox_energy_tol, int prox_max_iter,
+                  int fw_max_iter, int qp_max_iter, float qp_tol, float qp_const, bool best_int, bool accel_prox,
+                  int work_set_size, int approx_fw_iter, float less_confident_percent, float confident_tol)
+        : prox_reg_const(prox_reg_const), dual_gap_tol(dual_gap_tol), prox_energy_tol(prox_energy_tol),
+          prox_max_iter(prox_max_iter), fw_max_iter(fw_max_iter), qp_max_iter(qp_max_iter), qp_tol(qp_tol),
+          qp_const(qp_const), best_int(best_int), accel_prox(accel_prox), work_set_size(work_set_size),
+          approx_fw_iter(approx_fw_iter), less_confident_percent(less_confident_percent),
+          confidence_tol(confident_tol) {}
+    // LP_inf_params() (src/densecrf.cpp:287-302)
+    LP_inf_params() {
+        dcrf_lp_params p;
+        dcrf_lp_params_default(&p);
+        *this = from(p);
+    }
+    dcrf_lp_params to_c() const {
+        dcrf_lp_params p;
+        p.prox_reg_const = prox_reg_const;
+        p.dual_gap_tol = dual_gap_tol;
+        p.prox_energy_tol = prox_energy_tol;
+        p.prox_max_iter = prox_max_iter;
+        p.fw_max_iter = fw_max_iter;
+        p.qp_max_iter = qp_max_iter;
+        p.qp_tol = qp_tol;
+        p.qp_const = qp_const;
+        p.best_int = best_int;
+        p.accel_prox = accel_prox;
+        p.work_set_size = work_set_size;
+        p.approx_fw_iter = approx_fw_iter;
+        p.less_confident_percent = less_confident_percent;
+        p.confidence_tol = confidence_tol;
+        return p;
+    }
+private:
+    static LP_inf_params from(const dcrf_lp_params& p) {
+        return LP_inf_params(p.prox_reg_const, p.dual_gap_tol, p.prox_energy_tol, p.prox_max_iter, p.fw_max_iter,
+                             p.qp_max_iter, p.qp_tol, p.qp_const, p.best_int != 0, p.accel_prox != 0,
+                             p.work_set_size, p.approx_fw_iter, p.less_confident_percent, p.confidence_tol);
+    }
+};
+
+// A standalone PairwisePotential (include/pairwise.h:63-95): its lattice lives
+// in a one-term model over N = features.cols() pixels, created for the label
+// count of the first apply.
+class PairwisePotential {
+    MatrixXf f_;
+    float w_;
+    int L_ = 0;
+    dcrf_model m_ = nullptr;
+    PairwisePotential(const PairwisePotential&) = delete;
+    void ensure(int L) {
+        if (m_ && L == L_) return;
+        if (m_) dcrf_model_destroy(m_);
+        m_ = nullptr;
+        dcrf_shim::check(dcrf_model_create(&m_, (int)f_.cols(), 1, L));
+        dcrf_shim::check(dcrf_model_add_pairwise(m_, f_.data(), (int)f_.rows(), w_));
+        L_ = L;
+    }
+public:
+    PairwisePotential(const MatrixXf& features, LabelCompatibility* compatibility, KernelType ktype = CONST_KERNEL,
+                      NormalizationType ntype = NORMALIZE_SYMMETRIC)
+        : f_(features), w_(dcrf_shim::potts_weight(compatibility)) {
+        dcrf_shim::check_kernel(ktype, ntype);
+    }
+    ~PairwisePotential() {
+        if (m_) dcrf_model_destroy(m_);
+    }
+    // PairwisePotential::apply (src/pairwise.cpp:203-208)
+    void apply(MatrixXf& out, const MatrixXf& Q) const {
+        auto* self = const_cast<PairwisePotential*>(this);
+        self->ensure((int)Q.rows());
+        MatrixXf src = Q;
+        out.resize(Q.rows(), Q.cols());
+        dcrf_shim::check(dcrf_model_pairwise_apply(m_, 0, 0, out.data(), src.data()));
+    }
+    // PairwisePotential::apply_upper_minus_lower_ord (src/pairwise.cpp:214-228)
+    void apply_upper_minus_lower_ord(MatrixXf& out, const MatrixXf& Q) {
+        ensure((int)Q.rows());
+        MatrixXf src = Q;
+        out.resize(Q.rows(), Q.cols());
+        dcrf_shim::check(dcrf_model_pairwise_apply_ord(m_, 0, out.data(), src.data()));
+    }
+    VectorXf parameters() const {
+        VectorXf r(1);
+        r[0] = w_;
+        return r;
+    }
+    MatrixXf features() const { return f_; }
+};
+
+class DenseCRF {
+protected:
+    int N_, M_, R_ = 0;
+    dcrf_model m_ = nullptr;
+    int n_terms_ = 0;
+    // cliques (super_pixel_container_, exp_of_superpixels_, constants_)
+    std::vector<int> cl_off_{0}, cl_idx_;
+    std::vector<float> cl_exp_, cl_const_;
+    DenseCRF(DenseCRF&) = delete;
+    void push_cliques() {
+        dcrf_shim::check(dcrf_model_set_cliques(m_, R_, cl_off_.data(), cl_idx_.empty() ? nullptr : cl_idx_.data(),
+                                                cl_exp_.data(), cl_const_.data()));
+    }
+    DenseCRF(int W, int H, int M) : N_(W * H), M_(M) { dcrf_shim::check(dcrf_model_create(&m_, W, H, M)); }
+
+public:
+    virtual ~DenseCRF() {
+        if (m_) dcrf_model_destroy(m_);
+    }
+    // DenseCRF::addPairwiseEnergy (src/densecrf.cpp:157-169)
+    virtual void addPairwiseEnergy(const MatrixXf& features, LabelCompatibility* function,
+                                   KernelType kernel_type = DIAG_KERNEL,
+                                   NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
+        const float w = dcrf_shim::potts_weight(function);
+        dcrf_shim::check_kernel(kernel_type, normalization_type);
+        dcrf_shim::check(dcrf_model_add_pairwise(m_, features.data(), (int)features.rows(), w));
+        n_terms_++;
+    }
+    void setUnaryEnergy(const MatrixXf& unary) { dcrf_shim::check(dcrf_model_set_unary(m_, unary.data())); }
+    void setUnaryEnergy(UnaryEnergy* unary) {
+        std::unique_ptr<UnaryEnergy> own(unary);
+        setUnaryEnergy(unary->get());
+    }
+    // unary_init (src/densecrf.cpp:321-325)
+    MatrixXf unary_init() const {
+        MatrixXf Q(M_, N_);
+        dcrf_shim::check(dcrf_model_unary_init(m_, Q.data()));
+        return Q;
+    }
+    // qp_inference_super_pixels_non_convex (src/densecrf.cpp:340-442)
+    const MatrixXf qp_inference_super_pixels_non_convex(const MatrixXf& init) {
+        MatrixXf out(M_, N_);
+        dcrf_shim::check(dcrf_model_qp(m_, init.data(), out.data(), nullptr, nullptr));
+        return out;
+    }
+    // lp_inference_prox_super_pixels (src/densecrf.cpp:526-799)
+    const MatrixXf lp_inference_prox_super_pixels(const MatrixXf& init, const LP_inf_params& params) const {
+        MatrixXf out(M_, N_);
+        const dcrf_lp_params p = params.to_c();
+        dcrf_shim::check(dcrf_model_lp(m_, init.data(), out.data(), &p, nullptr));
+        return out;
+    }
+    MatrixXf max_rounding(const MatrixXf& estimates) const {
+        MatrixXf r = MatrixXf::Zero(estimates.rows(), estimates.cols());
+        const VectorXs l = currentMap(estimates);
+        for (int i = 0; i < (int)estimates.cols(); i++) r(l[i], i) = 1;
+        return r;
+    }
+    VectorXs currentMap(const MatrixXf& Q) const {
+        VectorXs l(Q.cols());
+        dcrf_shim::check(dcrf_model_current_map(m_, Q.data(), l.data()));
+        return l;
+    }
+    double assignment_energy_higher_order(const VectorXs& l) const {
+        double e = 0;
+        dcrf_shim::check(dcrf_model_energy_ho(m_, l.data(), &e));
+        return e;
+    }
+    double assignment_energy_true(const VectorXs& l) const {
+        double e = 0;
+        dcrf_shim::check(dcrf_model_energy_true(m_, l.data(), &e));
+        return e;
+    }
+    double compute_energy_LP_higher_order(const MatrixXf& Q) const {
+        double e = 0;
+        dcrf_shim::check(dcrf_model_energy_lp(m_, Q.data(), &e));
+        return e;
+    }
+    double compute_LR_QP_value(const MatrixXf& Q, const MatrixXf& diag_dom) const {
+        if (diag_dom.size() && diag_dom.cwiseAbs().maxCoeff() != 0)
+            throw std::runtime_error("compute_LR_QP_value: only diag_dom = 0 runs on the B200 path");
+        double e = 0;
+        dcrf_shim::check(dcrf_model_lr_qp_value(m_, Q.data(), &e));
+        return e;
+    }
+    // The clique state addSuperPixel leaves behind (src/densecrf.cpp:212-247),
+    // from a segmentation computed by the caller: region_of_pixel[i] in
+    // [0, n_regions).  Means and grey-level deviations follow the reference,
+    // including its img[i], img[i+1], img[i+2] reads (:222-233).
+    void addSuperPixel(const std::vector<int>& region_of_pixel, int n_regions, const unsigned char* img,
+                       float constant, float normaliser) {
+        std::vector<std::vector<int>> members(n_regions);
+        VectorXf count = VectorXf::Zero(n_regions), mean = VectorXf::Zero(n_regions),
+                 sd = VectorXf::Zero(n_regions);
+        for (int i = 0; i < N_; i++) {
+            const int r = region_of_pixel[i];
+            members[r].push_back(i);
+            mean(r) += 0.2989 * (double)img[i];
+            mean(r) += 0.5870 * (double)img[i + 1];
+            mean(r) += 0.1140 * (double)img[i + 2];
+            count(r) += 1;
+        }
+        mean = mean.cwiseQuotient(count);
+        for (int i = 0; i < N_; i++) {
+            const int r = region_of_pixel[i];
+            const double g = 0.2989 * (double)img[i] + 0.5870 * (double)img[i + 1] + 0.1140 * (double)img[i + 2];
+            sd(r) += (mean(r) - g) * (mean(r) - g);
+        }
+        sd = sd.cwiseQuotient(normaliser * count);
+        const VectorXf ex = constant * (-1 * sd.array()).exp();
+        for (int r = 0; r < n_regions; r++) {
+            cl_idx_.insert(cl_idx_.end(), members[r].begin(), members[r].end());
+            cl_off_.push_back((int)cl_idx_.size());
+            cl_exp_.push_back(ex[r]);
+            cl_const_.push_back(constant);
+        }
+        R_ += n_regions;
+        push_cliques();
+    }
+};
+
+class DenseCRF2D : public DenseCRF {
+protected:
+    int W_, H_;
+public:
+    DenseCRF2D(int W, int H, int M) : DenseCRF(W, H, M), W_(W), H_(H) {}
+    // addPairwiseGaussian (src/densecrf.cpp:170-178)
+    void addPairwiseGaussian(float sx, float sy, LabelCompatibility* function = NULL,
+                             KernelType kernel_type = DIAG_KERNEL,
+                             NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
+        const float w = dcrf_shim::potts_weight(function);
+        dcrf_shim::check_kernel(kernel_type, normalization_type);
+        dcrf_shim::check(dcrf_model_add_gaussian(m_, sx, sy, w));
+        n_terms_++;
+    }
+    // addPairwiseBilateral (src/densecrf.cpp:179-190)
+    void addPairwiseBilateral(float sx, float sy, float sr, float sg, float sb, const unsigned char* im,
+                              LabelCompatibility* function = NULL, KernelType kernel_type = DIAG_KERNEL,
+                              NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
+        const float w = dcrf_shim::potts_weight(function);
+        dcrf_shim::check_kernel(kernel_type, normalization_type);
+        dcrf_shim::check(dcrf_model_add_bilateral(m_, sx, sy, sr, sg, sb, im, w));
+        n_terms_++;
+    }
+    using DenseCRF::setUnaryEnergy;
+};

@@ -1,0 +1,3 @@
+// permutohedral.h of the densecrf_ho API: declared together in densecrf.h.
+#pragma once
+#include "densecrf.h"
