@@ -40,6 +40,8 @@ constexpr int kStages = 3;       // shared-memory ring depth, in chunks
 constexpr int kChunk = 32;       // entries per chunk (13 KB of ring per warp: 16 warps / SM)
 constexpr int kMaxOrderKey = (1 << 24) - 1;
 constexpr int kLongList = 64;    // lists longer than this use the staged warp kernels
+constexpr int kHugeList = 1024;  // lists longer than this get the finest ordered-splat split
+constexpr int kHugeLabels = 12;  // labels per block for those lists (120 threads)
 constexpr int kTB = 256;         // threads per block of the element-wise kernels
 
 template <int KW>
@@ -327,6 +329,9 @@ __device__ __forceinline__ unsigned smem_addr(const void* p) {
 __device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(sdst)), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(sdst)), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -514,50 +519,84 @@ __device__ __forceinline__ int bin_upper(float q) {
     return c < kRes - 1 ? c : kRes - 1;
 }
 
-// Bin indices of every (pixel, label), computed once per ordered filter:
-// lower | upper << 8 (each pixel appears in d+1 splat lists and in the slice).
-__global__ void ord_bins_kernel(long n, const float* __restrict__ Q, int* __restrict__ bins) {
+// Ordered bins of every (pixel, label), computed once per ordered filter
+// (each pixel appears in d+1 splat lists and in the slice): the lower and
+// upper bin indices, held as floats (exact small integers) because the splat
+// compares them with float bin numbers.
+__device__ __forceinline__ float2 ord_bin_pair(float q) {
+    return make_float2((float)bin_lower(q), (float)bin_upper(q));
+}
+__device__ __forceinline__ int ord_lower_of(float2 b) { return (int)b.x; }
+__device__ __forceinline__ int ord_upper_of(float2 b) { return (int)b.y; }
+
+__global__ void ord_bins_kernel(long n, const float* __restrict__ Q, float2* __restrict__ bins) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const float q = Q[t];
-    bins[t] = bin_lower(q) | (bin_upper(q) << 8);
+    bins[t] = ord_bin_pair(Q[t]);
 }
 
 // Each of the 10 bins accumulates, in entry order, the weights of the entries
 // that reach it: bins 0..c (lower pass) or c..9 (upper pass), addSplitArray
-// (:548-569).  Branch-free and bit-identical: the mask m = sat(c - b + 1)
-// (lower) or sat(b - c + 1) (upper) is exactly 0 or 1, so fma(m, w, acc)
-// rounds acc + w once when the entry reaches the bin, and otherwise returns
-// acc (acc + (+-0) = acc: the accumulator starts at +0 and is never -0).
+// (:548-569).  Branch-free and bit-identical: the mask m = [c_lower >= b]
+// (lower) or [b >= c_upper] (upper) is exactly 1.0 or 0.0 (one PTX `set`,
+// NaN giving 0), so fma(m, w, acc) rounds acc + w once when the entry reaches
+// the bin and otherwise returns acc (acc + (+-0) = acc: the accumulator
+// starts at +0 and is never -0).
+__device__ __forceinline__ float step_ge(float a, float b) {  // a >= b ? 1 : 0
+    float r;
+    asm("set.ge.f32.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+    return r;
+}
+
+// One entry into the bin-b pair (lower, upper) of packed accumulators:
+// acc = fma({[cl >= b], [b >= cu]}, w2, acc) with one f32x2 FMA, which rounds
+// each half exactly as fma.rn.f32 does.  w2 holds (w, w).
+__device__ __forceinline__ void ord_step2(unsigned long long& acc, float cl, float cu, float b,
+                                          unsigned long long w2) {
+    asm("{\n\t.reg .f32 ml, mu;\n\t.reg .b64 m;\n\t"
+        "set.ge.f32.f32 ml, %1, %3;\n\t"
+        "set.ge.f32.f32 mu, %3, %2;\n\t"
+        "mov.b64 m, {ml, mu};\n\t"
+        "fma.rn.f32x2 %0, m, %4, %0;\n\t}"
+        : "+l"(acc)
+        : "f"(cl), "f"(cu), "f"(b), "l"(w2));
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v) {
+    float2 r;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+    return r;
+}
+
 template <bool UPPER>
-__device__ __forceinline__ void ord_accumulate(float (&acc)[kRes], int c, float w) {
-    const float cf = (float)c;
+__device__ __forceinline__ void ord_accumulate(float (&acc)[kRes], float c, float w) {
 #pragma unroll
     for (int b = 0; b < kRes; b++) {
-        const float m = UPPER ? __saturatef(__fadd_rn((float)(b + 1), -cf)) : __saturatef(__fadd_rn(cf, (float)(1 - b)));
+        const float m = UPPER ? step_ge((float)b, c) : step_ge(c, (float)b);
         acc[b] = __fmaf_rn(m, w, acc[b]);
     }
 }
 
 template <bool UPPER>
-__device__ __forceinline__ void ord_consume(float (&acc)[kRes], const int (*ring)[32], const float* mw, int lane,
+__device__ __forceinline__ void ord_consume(float (&acc)[kRes], const float (*ring)[32], const float* mw, int lane,
                                             int n) {
 #pragma unroll 2
-    for (int e = 0; e < n; e++) {
-        const int word = ring[e][lane];
-        ord_accumulate<UPPER>(acc, UPPER ? (word >> 8) : (word & 0xff), mw[e]);
-    }
+    for (int e = 0; e < n; e++) ord_accumulate<UPPER>(acc, ring[e][lane], mw[e]);
 }
 
-// Ordered splat: one warp per (vertex, pass), streaming the vertex's list as
-// splat_kernel does.  A vertex row holds 20 bins x L labels, bin-major
-// ([v][bin][label]; bins [0,10) lower, [10,20) upper) so that the slice's
-// per-label bin reads coalesce.
+// Ordered splat, general L: one warp per (vertex, pass), streaming the
+// vertex's list as splat_kernel does.  A vertex row holds 20 bins x L
+// labels, bin-major ([v][bin][label]; bins [0,10) lower, [10,20) upper) so
+// that the slice's per-label bin reads coalesce.
 __global__ void __launch_bounds__(32 * kStageWarps)
     ord_splat_kernel(int M, int L, const int* __restrict__ order, const int* __restrict__ seg_start,
                      const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
-                     const int* __restrict__ bins, float* __restrict__ vals) {
-    __shared__ int ring[kStageWarps][kStages][kChunk][32];
+                     const float2* __restrict__ bins, float* __restrict__ vals) {
+    __shared__ float ring[kStageWarps][kStages][kChunk][32];
     __shared__ float mw[kStageWarps][kStages][kChunk];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int unit = blockIdx.x * kStageWarps + wib;
@@ -565,17 +604,18 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     const int v = order[unit >> 1];
     const bool upper = unit & 1;
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    const float* bf = reinterpret_cast<const float*>(bins);  // [pixel][label][lower, upper]
     for (int kb = 0; kb < L; kb += 32) {
         const int k = kb + lane;
         const bool act = k < L;
         float acc[kRes];
 #pragma unroll
         for (int b = 0; b < kRes; b++) acc[b] = 0.0f;
-        stream_list<int, false>(s0, s1, L, k, act, lane, seg_pix, seg_w, bins, nullptr, ring[wib], mw[wib],
-                                nullptr, [&](int slot, int n) {
-                                    if (upper) ord_consume<true>(acc, ring[wib][slot], mw[wib][slot], lane, n);
-                                    else ord_consume<false>(acc, ring[wib][slot], mw[wib][slot], lane, n);
-                                });
+        stream_list<float, false>(s0, s1, 2 * L, 2 * k + (upper ? 1 : 0), act, lane, seg_pix, seg_w, bf, nullptr,
+                                  ring[wib], mw[wib], nullptr, [&](int slot, int n) {
+                                      if (upper) ord_consume<true>(acc, ring[wib][slot], mw[wib][slot], lane, n);
+                                      else ord_consume<false>(acc, ring[wib][slot], mw[wib][slot], lane, n);
+                                  });
         if (act) {
             float* row = vals + ((long)(v + 1) * kOrdW + (upper ? kRes : 0)) * L + k;
 #pragma unroll
@@ -584,32 +624,212 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     }
 }
 
+// Ordered splat of the long lists by blocks.  The 20 x L bin sums of a
+// vertex are 20 L independent in-order chains; thread (k, g) carries the
+// chains of label k, bins g*NB .. g*NB+NB-1, both passes, so a block shares
+// a long list's work and the longest lists no longer set the kernel's
+// length.
+//
+// The list streams through shared memory in chunks of kOE entries: the
+// pixel ids and weights of chunk c + 2 kODX and the (c_lower, c_upper) bins
+// of chunk c + kODX are copied with cp.async while chunk c is summed, one
+// block barrier per chunk.  Ring rows are label-major ([k][entry][lower,
+// upper], padded to an odd number of 16-byte units) so a thread reads two
+// entries per 16-byte load and eight consecutive labels hit distinct banks.
+// Weights are staged as (w, w) pairs; entries past the end of the list get
+// weight 0, which leaves every accumulator unchanged (the masks are 0 or 1
+// for any stale bin value).
+constexpr int kOE = 32;                 // entries per chunk
+constexpr int kODX = 4;                 // bins are copied kODX chunks ahead of use, pixel ids 2 kODX
+constexpr int kOXS = kODX + 1;          // bin ring slots (chunks c .. c+kODX)
+constexpr int kOPS = 2 * kODX + 1;      // pixel / weight ring slots (chunks c .. c+2 kODX)
+constexpr int kORow = 2 * kOE + 4;      // floats per ring row: 17 x 16 bytes
+constexpr int kOrdBlockMaxL = 160;      // larger L use ord_splat_kernel (shared-memory ring size)
+constexpr int kGroupChoices[] = {1, 2, 3, 5, 10};
+
+// Bin split with the fewest warp instructions per list entry: warps x (three
+// instructions per bin slot + about two for the shared-memory loads).
+int ord_groups_cheapest(int L) {
+    int best = 1;
+    long best_cost = -1;
+    for (int G : kGroupChoices) {
+        if (L * G > 1024) break;
+        const long warps = (L * G + 31) / 32, nb = (kRes + G - 1) / G;
+        const long cost = warps * (3 * nb + 2);
+        if (best_cost < 0 || cost <= best_cost) {
+            best = G;
+            best_cost = cost;
+        }
+    }
+    return best;
+}
+
+size_t ord_block_smem(int kb) {
+    return sizeof(float) * ((size_t)kOXS * kb * kORow + (size_t)kOPS * kOE * 2) + sizeof(int) * kOPS * kOE;
+}
+
+// G bin groups per label, NB = ceil(10 / G) bin slots per thread; slots past
+// bin 9 (when G does not divide 10) run on a dummy bin that is not stored.
+// Block b covers labels [k0, k0 + nk) of vertex order[b / kblocks], k0 =
+// (b % kblocks) * kb: a very long list can be shared by several blocks.
+// Compute threads are label-major (t = k * G + g), so the G threads reading
+// one label's bins sit in one warp and their shared-memory loads broadcast;
+// staging threads are entry-major (t = g * nk + k) so one warp's copies read
+// consecutive labels of one pixel.
+template <int G>
+__global__ void __launch_bounds__(1024)
+    ord_splat_block_kernel(int L, int kb, int kblocks, const int* __restrict__ order,
+                           const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
+                           const float* __restrict__ seg_w, const float2* __restrict__ bins,
+                           float* __restrict__ vals) {
+    extern __shared__ __align__(16) float osm[];
+    float* xr = osm;                            // [kOXS][kb][kORow]
+    float* wr = xr + (size_t)kOXS * kb * kORow;  // [kOPS][kOE][2]
+    int* pr = reinterpret_cast<int*>(wr + kOPS * kOE * 2);  // [kOPS][kOE]
+    constexpr int NB = (kRes + G - 1) / G;
+    const int t = threadIdx.x;
+    const int v = order[blockIdx.x / kblocks];
+    const int k0 = (blockIdx.x % kblocks) * kb, nk = min(kb, L - k0);
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    const int nch = (s1 - s0 + kOE - 1) / kOE;
+    const bool worker = t < nk * G;
+    const int k = t / G, g = t - k * G;      // compute role
+    const int sk = t % nk, sg = t / nk;      // staging role (sg < G for workers)
+
+    auto stage_pw = [&](int c) {  // pixel ids and weights of chunk c
+        if (c < nch && t < kOE) {
+            const int slot = c % kOPS, e = s0 + c * kOE + t;
+            if (e < s1) {
+                cp_async4(&pr[slot * kOE + t], seg_pix + e);
+                cp_async4(&wr[(slot * kOE + t) * 2], seg_w + e);
+                cp_async4(&wr[(slot * kOE + t) * 2 + 1], seg_w + e);
+            } else {
+                pr[slot * kOE + t] = 0;
+                wr[(slot * kOE + t) * 2] = 0.0f;
+                wr[(slot * kOE + t) * 2 + 1] = 0.0f;
+            }
+        }
+    };
+    // (c_lower, c_upper) of chunk c; needs chunk c's pixel ids in place.
+    // Staging thread (sk, sg) copies label k0 + sk of entries sg, sg + G, ...
+    // All pixel ids are read before the first copy is issued (the copies'
+    // memory clobber would otherwise order each read after the last copy).
+    auto stage_x = [&](int c) {
+        if (c >= nch || !worker) return;
+        constexpr int MX = (kOE + G - 1) / G;
+        const int slot = c % kOXS, ps = c % kOPS;
+        const int n = min(kOE, s1 - (s0 + c * kOE));
+        float* dst = &xr[((size_t)slot * kb + sk) * kORow];
+        const float2* src = bins + k0 + sk;
+        int pix[MX];
+#pragma unroll
+        for (int i = 0; i < MX; i++) {
+            const int e = sg + i * G;
+            pix[i] = e < n ? pr[ps * kOE + e] : 0;
+        }
+#pragma unroll
+        for (int i = 0; i < MX; i++) {
+            const int e = sg + i * G;
+            if (e < n) cp_async8(dst + 2 * e, src + (long)pix[i] * L);
+        }
+    };
+
+    // Group j (committed at iteration j; j < 0 in the prologue) holds the
+    // bins of chunk j + kODX and the pixel ids / weights of chunk j + 2 kODX.
+#pragma unroll
+    for (int c = 0; c < kODX; c++) stage_pw(c);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < kODX; c++) {
+        stage_x(c);
+        stage_pw(c + kODX);
+        cp_async_commit();
+    }
+
+    float lo[NB], up[NB], bf[NB];  // lower / upper sums of bin g*NB + i
+#pragma unroll
+    for (int i = 0; i < NB; i++) {
+        lo[i] = up[i] = 0.0f;
+        bf[i] = (float)(g * NB + i);
+    }
+    for (int c = 0; c < nch; c++) {
+        cp_async_wait<kODX - 1>();  // group c - kODX: bins of chunk c, pixel ids of chunk c + kODX
+        __syncthreads();            // ... everyone's copies; and chunk c-1's slots are free
+        stage_x(c + kODX);
+        stage_pw(c + 2 * kODX);
+        cp_async_commit();
+        if (worker) {
+            const float4* xs = reinterpret_cast<const float4*>(&xr[((size_t)(c % kOXS) * kb + k) * kORow]);
+            const float4* ws = reinterpret_cast<const float4*>(&wr[(c % kOPS) * kOE * 2]);
+            const int n2 = (min(kOE, s1 - (s0 + c * kOE)) + 1) >> 1;
+            // Eight entries per batch: their loads are issued together, then
+            // summed.  A batch may run past n2 into the chunk's zero-weight
+            // tail (the ring rows hold kOE entries).
+            for (int b0 = 0; b0 < n2; b0 += 4) {
+                float4 x[4], w[4];  // (c_lower, c_upper) and (w, w) of entries 2 j, 2 j + 1
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    x[j] = xs[b0 + j];
+                    w[j] = ws[b0 + j];
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+#pragma unroll
+                    for (int i = 0; i < NB; i++) {
+                        lo[i] = __fmaf_rn(step_ge(x[j].x, bf[i]), w[j].x, lo[i]);
+                        up[i] = __fmaf_rn(step_ge(bf[i], x[j].y), w[j].y, up[i]);
+                    }
+#pragma unroll
+                    for (int i = 0; i < NB; i++) {
+                        lo[i] = __fmaf_rn(step_ge(x[j].z, bf[i]), w[j].z, lo[i]);
+                        up[i] = __fmaf_rn(step_ge(bf[i], x[j].w), w[j].w, up[i]);
+                    }
+                }
+            }
+        }
+    }
+    cp_async_wait<0>();
+    if (worker) {
+        float* row = vals + (long)(v + 1) * kOrdW * L + k0 + k;
+#pragma unroll
+        for (int i = 0; i < NB; i++) {
+            if (g * NB + i >= kRes) break;
+            row[(long)(g * NB + i) * L] = lo[i];
+            row[(long)(kRes + g * NB + i) * L] = up[i];
+        }
+    }
+}
+
 // Ordered splat of the short lists: one thread per (vertex, label), both
 // passes, without staging.
 __global__ void ord_splat_short_kernel(int n_short, int L, const int* __restrict__ order,
                                        const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
-                                       const float* __restrict__ seg_w, const int* __restrict__ bins,
+                                       const float* __restrict__ seg_w, const float2* __restrict__ bins,
                                        float* __restrict__ vals) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n_short * L) return;
     const int u = (int)(t / L), k = (int)(t - (long)u * L);
     const int v = order[u];
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
-    float lo[kRes], up[kRes];
+    unsigned long long acc[kRes];  // (lower, upper) sums of bin b
 #pragma unroll
-    for (int b = 0; b < kRes; b++) lo[b] = up[b] = 0.0f;
+    for (int b = 0; b < kRes; b++) acc[b] = 0ull;
 #pragma unroll 2
     for (int s = s0; s < s1; s++) {
-        const int word = bins[(long)seg_pix[s] * L + k];
+        const float2 x = bins[(long)seg_pix[s] * L + k];
         const float w = seg_w[s];
-        ord_accumulate<false>(lo, word & 0xff, w);
-        ord_accumulate<true>(up, word >> 8, w);
+        const unsigned long long w2 = pack2(w, w);
+#pragma unroll
+        for (int b = 0; b < kRes; b++) ord_step2(acc[b], x.x, x.y, (float)b, w2);
     }
     float* row = vals + (long)(v + 1) * kOrdW * L + k;
 #pragma unroll
     for (int b = 0; b < kRes; b++) {
-        row[(long)b * L] = lo[b];
-        row[(long)(kRes + b) * L] = up[b];
+        const float2 r = unpack2(acc[b]);
+        row[(long)b * L] = r.x;
+        row[(long)(kRes + b) * L] = r.y;
     }
 }
 
@@ -638,15 +858,15 @@ __global__ void ord_blur_kernel(int M, int row4, const int2* __restrict__ nbr,
 template <bool GAP>
 __global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ offset,
                                  const float* __restrict__ bary, const float* __restrict__ vals,
-                                 const int* __restrict__ bins, float alpha, float* out, SliceEpilogue ep,
+                                 const float2* __restrict__ bins, float alpha, float* out, SliceEpilogue ep,
                                  GapFusion gf) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double g0 = 0.0, g1 = 0.0;
     if (t < (long)N * L) {
         const int i = (int)(t / L), k = (int)(t - (long)i * L);
         const int d1 = d + 1;
-        const int word = bins[t];
-        const int cl = word & 0xff, cu = word >> 8;
+        const float2 bp = bins[t];
+        const int cl = ord_lower_of(bp), cu = ord_upper_of(bp);
         float acc = 0.0f;
         for (int j = 0; j <= d; j++) {
             const int o = offset[(long)i * d1 + j];
@@ -693,13 +913,13 @@ __global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ of
 // Bins of rescale(Q) (src/eigen_utils.cpp:120-141) without materialising it:
 // rq = (Q - min) / (max - min), with min / max at qmm[0], qmm[1].
 __global__ void rescaled_bins_kernel(long n, const float* __restrict__ Q, const float* __restrict__ qmm,
-                                     int* __restrict__ bins) {
+                                     float2* __restrict__ bins) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const float mn = qmm[0], range = fsub(qmm[1], qmm[0]);
     float rq = fsub(Q[t], mn);
     if (range > 0.0f) rq = rq / range;
-    bins[t] = bin_lower(rq) | (bin_upper(rq) << 8);
+    bins[t] = ord_bin_pair(rq);
 }
 
 int bits_for(int n) {  // bits needed to hold values 0..n-1
@@ -775,12 +995,16 @@ void build_impl(Lattice& L, const float* d_features) {
     int* okeys = L.vorder_keys.ensure(M);
     launch(order_key_kernel, ceil_div(M, kTB), kTB, 0, st, M, counts, okeys, vorder);
     radix_sort_pairs(okeys, vorder, M, 24, L.sort, st);
-    int* dlong = L.total.ensure(1);
-    DCRF_CUDA(cudaMemsetAsync(dlong, 0, sizeof(int), st));
+    int* dlong = L.total.ensure(2);
+    DCRF_CUDA(cudaMemsetAsync(dlong, 0, 2 * sizeof(int), st));
     launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, counts, kLongList, dlong);
+    launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, counts, kHugeList, dlong + 1);
     DCRF_LAUNCH_CHECK();
-    DCRF_CUDA(cudaMemcpyAsync(&L.n_long, dlong, sizeof(int), cudaMemcpyDeviceToHost, st));
+    int nl[2];
+    DCRF_CUDA(cudaMemcpyAsync(nl, dlong, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     DCRF_CUDA(cudaStreamSynchronize(st));
+    L.n_long = nl[0];
+    L.n_huge = nl[1];
     L.va_floats = 0;
 }
 
@@ -936,19 +1160,19 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
 void Lattice::compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep) {
     require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
     const long NL = (long)N * L;
-    int* bins = obins.ensure((size_t)NL);
+    float2* bins = obins.ensure((size_t)NL);
     launch(ord_bins_kernel, ceil_div(NL, kTB), kTB, 0, stream, NL, Q, bins);
     compute_ord_bins(out, bins, L, ep, nullptr);
 }
 
-void rescaled_bins(int* bins, const float* Q, long n, const float* qminmax, cudaStream_t st) {
+void rescaled_bins(float2* bins, const float* Q, long n, const float* qminmax, cudaStream_t st) {
     launch(rescaled_bins_kernel, ceil_div(n, kTB), kTB, 0, st, n, Q, qminmax, bins);
     DCRF_LAUNCH_CHECK();
 }
 
 int slice_grid(long n) { return ceil_div(n, kTB); }
 
-void Lattice::compute_ord_bins(float* out, const int* bins, int L, const SliceEpilogue& ep,
+void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const SliceEpilogue& ep,
                                const GapFusion* gap) {
     require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
     const size_t row = (size_t)L * kOrdW;
@@ -957,9 +1181,32 @@ void Lattice::compute_ord_bins(float* out, const int* bins, int L, const SliceEp
     const long NL = (long)N * L;
     float *src = va.get(), *dst = vb.get();
     const int n_short = M - n_long;
-    if (n_long)
+    if (n_long && L <= kOrdBlockMaxL) {
+        // Lists longer than kHugeList (the first n_huge of the order) are
+        // shared by blocks of kHugeLabels labels x 10 bins, so that they
+        // finish early; the rest take one block per list with the bin split
+        // that issues the fewest instructions per entry.
+        auto run = [&](int G, int kb, int first, int count) {
+            if (count <= 0) return;
+            const int kblocks = (L + kb - 1) / kb;
+            const int threads = ((kb * G + 31) / 32) * 32;
+            const size_t smem = ord_block_smem(kb);
+            auto kern = G == 10 ? ord_splat_block_kernel<10>
+                      : G == 5  ? ord_splat_block_kernel<5>
+                      : G == 3  ? ord_splat_block_kernel<3>
+                      : G == 2  ? ord_splat_block_kernel<2>
+                                : ord_splat_block_kernel<1>;
+            if (smem > 48 * 1024)  // opt-in size: a per-device function attribute, set on every such call
+                DCRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            launch(kern, count * kblocks, threads, smem, st, L, kb, kblocks, vorder.get() + first,
+                   seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
+        };
+        run(10, kHugeLabels, 0, n_huge);
+        run(ord_groups_cheapest(L), L, n_huge, n_long - n_huge);
+    } else if (n_long) {
         launch(ord_splat_kernel, ceil_div(2L * n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
                vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
+    }
     if (n_short)
         launch(ord_splat_short_kernel, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
                vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);

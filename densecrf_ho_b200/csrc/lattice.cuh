@@ -38,7 +38,7 @@ struct GapFusion {
 };
 
 // Packed ordered-filter bin indices of rescale(Q) (min / max at qminmax[0..1]).
-void rescaled_bins(int* bins, const float* Q, long n, const float* qminmax, cudaStream_t st);
+void rescaled_bins(float2* bins, const float* Q, long n, const float* qminmax, cudaStream_t st);
 // Blocks of the element-wise slice kernels for n elements.
 int slice_grid(long n);
 // Capacity, in floats, of the fixed scratch array of compute_noalloc.
@@ -47,6 +47,7 @@ size_t noalloc_scratch_floats();
 struct Lattice {
     int N = 0, d = 0, M = 0;
     int n_long = 0;  // vertices whose splat list exceeds the staging threshold
+    int n_huge = 0;  // ... and the (leading) ones whose list is very long
     cudaStream_t stream = nullptr;  // borrowed
 
     DevBuf<int> offset, rank, seg_start, seg_pix;
@@ -55,7 +56,7 @@ struct Lattice {
     DevBuf<int16_t> vkeys;
     DevBuf<int2> nbr;
     DevBuf<float> va, vb;    // filter value buffers
-    DevBuf<int> obins;       // ordered filter: packed bin indices per (pixel, label)
+    DevBuf<float2> obins;    // ordered filter: (c_lower, c_upper) per (pixel, label)
     size_t va_floats = 0;    // rows (M+1) * width currently zero-headed
 
     // build scratch
@@ -76,7 +77,7 @@ struct Lattice {
     // Ordered (upper minus lower, 10-bin) filter of Q in [0,1]; out = epilogue(v).
     void compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep);
     // The same from precomputed packed bins (lower | upper << 8 per element).
-    void compute_ord_bins(float* out, const int* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
+    void compute_ord_bins(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
 
     void ensure_values(size_t row_width);
 };

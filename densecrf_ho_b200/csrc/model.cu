@@ -156,7 +156,7 @@ void Model::apply_ord(int k, float* out, const float* rq, const float* base, boo
     t.lat->compute_ord(out, rq, L, ep);
 }
 
-void Model::apply_ord_bins(int k, float* out, const int* bins, const float* base, bool zero_base,
+void Model::apply_ord_bins(int k, float* out, const float2* bins, const float* base, bool zero_base,
                            const GapFusion* gap) {
     Term& t = *terms[k];
     SliceEpilogue ep;

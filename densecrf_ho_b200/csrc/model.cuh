@@ -56,7 +56,7 @@ struct Model {
     DevBuf<double> partials;
     DevBuf<SolverScalars> scal;
     DevBuf<int16_t> labels;
-    DevBuf<int> lp_bins;  // packed ordered-filter bins of rescale(Q), shared by all terms
+    DevBuf<float2> lp_bins;  // ordered-filter bins of rescale(Q), shared by all terms
     DevBuf<int> ipart;
     SolverScalars* h_scal = nullptr;  // pinned mirror
 
@@ -71,7 +71,7 @@ struct Model {
     // out = base + coef * (-w K~ in)  (see SliceEpilogue).
     void apply(int k, bool nonorm, float* out, const float* in, const float* base = nullptr,
                float coef = 1.0f, bool zero_base = false);
-    void apply_ord_bins(int k, float* out, const int* bins, const float* base, bool zero_base,
+    void apply_ord_bins(int k, float* out, const float2* bins, const float* base, bool zero_base,
                         const GapFusion* gap);
     void apply_ord(int k, float* out, const float* rq, const float* base = nullptr,
                    bool zero_base = false);

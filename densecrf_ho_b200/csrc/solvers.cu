@@ -1028,7 +1028,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     float* su = R > 0 ? buf(4) : nullptr;
     float* gamma = buf(5);
     float* curQ = buf(6);
-    int* bins = lp_bins.ensure(NL);
+    float2* bins = lp_bins.ensure(NL);
     float* Y = buf(8);
     int16_t* lab = labels.ensure(N);
     SolverScalars* sc = scal.get();

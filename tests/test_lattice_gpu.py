@@ -79,6 +79,36 @@ def test_filter_bit_exact(L, oracle_mod):
         assert _eq(lat.compute_upper_minus_lower_ord(q), orc.compute_ord(q))
 
 
+@pytest.mark.parametrize("L", [60, 130, 200])
+def test_ordered_filter_wide_labels(L, oracle_mod):
+    """The long-list ordered splat splits a vertex's 20 L bin chains over a
+    block whose shape depends on L (opt-in shared memory above 48 KB) and
+    falls back to a warp per list past 160 labels."""
+    W, H = 72, 54
+    img = synth.make_image(W, H, 21, 9)
+    f = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    lat, orc = Permutohedral().init(f), oracle_mod.OracleLattice(f)
+    q = np.random.default_rng(L).random((W * H, L)).astype(np.float32)
+    q[::5] = 1.0
+    q[::13] = 0.0
+    assert _eq(lat.compute_upper_minus_lower_ord(q), orc.compute_ord(q))
+
+
+@pytest.mark.parametrize("L", [5, 21])
+def test_ordered_filter_huge_lists(L, oracle_mod):
+    """A coarse lattice whose splat lists run to thousands of entries: the
+    longest lists are shared by several blocks, the rest take one each."""
+    W, H = 128, 96
+    img = synth.make_image(W, H, 21, 9)
+    f = synth.bilateral_features(W, H, 500, 500, 100, 100, 100, img["rgb"])
+    lat, orc = Permutohedral().init(f), oracle_mod.OracleLattice(f)
+    q = np.random.default_rng(L).random((W * H, L)).astype(np.float32)
+    q[::3] = np.float32(0.3)  # exact multiples of 0.1: lower and upper bins differ
+    assert _eq(lat.compute_upper_minus_lower_ord(q), orc.compute_ord(q))
+    x = np.random.default_rng(L + 5).standard_normal((W * H, L)).astype(np.float32)
+    assert _eq(lat.compute(x), orc.compute(x))
+
+
 def test_filter_error_vs_fp64_oracle(oracle_mod):
     """Relative error of the FP32 filter against the FP64 lattice oracle."""
     W, H = 160, 120
