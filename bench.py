@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only-roofline", action="store_true",
                     help="time only the ordered and plain lattice filters (a short command for ncu)")
+    ap.add_argument("--only-batch", action="store_true",
+                    help="time only the 64-image batched QP against sequential solves")
     ap.add_argument("--prox-iters", type=int, default=50,
                     help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
     return ap.parse_args()
@@ -382,6 +384,86 @@ def measure_qp(reps=10, cpu=True):
     return res
 
 
+def measure_batch(n=64, max_iter=100, reps=3):
+    """Config 4: the plain QP (as config 1, up to 100 Frank-Wolfe iterations)
+    of n images of uneven sizes (H ~ U[240, 500], W ~ U[320, 500], seeded),
+    solved as one batch (dcrf_batch_qp_dev: concatenated lattices, per-image
+    scalars, the iteration replayed as a CUDA graph) and as n sequential
+    single-image solves (dcrf_model_qp_dev), both device-resident and timed
+    with CUDA events on the solvers' streams.  The batch's output must equal
+    the sequential outputs bit for bit."""
+    import torch
+    from densecrf_ho_b200 import DenseCRF2D, DenseCRF2DBatch, SolveStats, lib, check
+    Ls = lib()
+    sizes = synth.batch_sizes(n, 4)
+    imgs = [synth.make_image(w, h, L, 1000 + i) for i, (w, h) in enumerate(sizes)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b = DenseCRF2DBatch(sizes, L)
+    b.setUnaryEnergy(np.concatenate([im["unary"] for im in imgs]))
+    b.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+    b.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
+                           np.concatenate([im["rgb"] for im in imgs]), BILAT[2])
+    setup_ms = (time.perf_counter() - t0) * 1e3
+    q0 = b.unary_init()
+    init = torch.from_numpy(q0).cuda()
+    out = torch.empty_like(init)
+    p = C.c_int(max_iter)
+    st = (SolveStats * n)()
+    sptr = C.c_void_p()
+    check(Ls.dcrf_batch_stream(b._h, C.byref(sptr)))
+    bstream = torch.cuda.ExternalStream(sptr.value)
+    run_b = lambda: check(Ls.dcrf_batch_qp_dev(b._h, C.c_void_p(init.data_ptr()), C.c_void_p(out.data_ptr()),
+                                               C.byref(p), st))
+    run_b()  # eager first iteration + capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = Ls.dcrf_kernel_launches()
+    e0.record(bstream)
+    for _ in range(reps):
+        run_b()
+    e1.record(bstream)
+    torch.cuda.synchronize()
+    batch_launches = (Ls.dcrf_kernel_launches() - l0) // reps
+    batch_ms = e0.elapsed_time(e1) / reps
+    steps = [s.iterations for s in st]
+
+    models, seq_ms, same = [], 0.0, True
+    outs = b.split(out)
+    inits = b.split(init)
+    for i, ((w, h), im) in enumerate(zip(sizes, imgs)):
+        m = DenseCRF2D(w, h, L)
+        m.setUnaryEnergy(im["unary"])
+        m.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+        m.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], im["rgb"], BILAT[2])
+        models.append(m)
+    for i, m in enumerate(models):
+        mi = inits[i].contiguous()
+        mo = torch.empty_like(mi)
+        check(Ls.dcrf_model_stream(m.handle, C.byref(sptr)))
+        ms_ = torch.cuda.ExternalStream(sptr.value)
+        one = SolveStats()
+        run_m = lambda: check(Ls.dcrf_model_qp_dev(m.handle, C.c_void_p(mi.data_ptr()), C.c_void_p(mo.data_ptr()),
+                                                   C.byref(p), C.byref(one)))
+        run_m()
+        torch.cuda.synchronize()
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(ms_)
+        for _ in range(reps):
+            run_m()
+        a1.record(ms_)
+        torch.cuda.synchronize()
+        seq_ms += a0.elapsed_time(a1) / reps
+        same = same and bool(torch.equal(mo, outs[i])) and one.iterations == steps[i]
+    return {"workload": f"batched qp_inference_super_pixels_non_convex, {n} images H~U[240,500] W~U[320,500] "
+                        f"(seeded), L={L}, max_iter={max_iter}",
+            "images": n, "pixels": int(b.N), "batch_ms": batch_ms, "sequential_ms": seq_ms,
+            "batch_solves_per_s": n / (batch_ms / 1e3), "sequential_solves_per_s": n / (seq_ms / 1e3),
+            "speedup_vs_sequential": seq_ms / batch_ms, "fw_steps_max": max(steps), "fw_steps_min": min(steps),
+            "batch_launches_per_solve": int(batch_launches), "setup_ms": setup_ms,
+            "outputs_match_sequential": same}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -398,6 +480,9 @@ def run_ours(args):
     img = synth.make_image(W, H, L, seed)
     if args.only_roofline:
         print(json.dumps(measure_filters(W, H, img, reps=3)))
+        return
+    if args.only_batch:
+        print(json.dumps(measure_batch()))
         return
     t0 = time.perf_counter()
     crf = DenseCRF2D(W, H, L)
@@ -495,6 +580,7 @@ def run_ours(args):
                       "ord_filter_ms": {k: v["seconds"] * 1e3 for k, v in roof.items()}}}
     if rank == 0 and world == 1:
         line["extra"]["qp_320x240"] = measure_qp(cpu=not args.no_cpu_baseline)
+        line["extra"]["batch_qp_64"] = measure_batch()
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference(W, H, args.seed, prox_iters, 1, 10, 1)

@@ -227,3 +227,75 @@ class DenseCRF2D:
         e = C.c_double()
         check(lib().dcrf_model_lr_qp_value(self._h, x.ctypes.data_as(C.c_void_p), C.byref(e)))
         return e.value
+
+
+class DenseCRF2DBatch:
+    """Several images of different sizes solved together (``dcrf_batch_*``).
+
+    Images share the label count and the pairwise parameters; pixel arrays
+    are the images' ``[W_i*H_i, ...]`` arrays stacked in order.  Each image's
+    QP result equals :meth:`DenseCRF2D.qp_inference_super_pixels_non_convex`
+    of that image alone.
+    """
+
+    def __init__(self, sizes, L):
+        self.sizes = [(int(w), int(h)) for w, h in sizes]
+        self.L = int(L)
+        w = (C.c_int * len(self.sizes))(*[s[0] for s in self.sizes])
+        h = (C.c_int * len(self.sizes))(*[s[1] for s in self.sizes])
+        self._h = C.c_void_p()
+        check(lib().dcrf_batch_create(C.byref(self._h), len(self.sizes), w, h, self.L))
+        n = C.c_int64()
+        off = (C.c_int64 * (len(self.sizes) + 1))()
+        check(lib().dcrf_batch_info(self._h, C.byref(n), off))
+        self.N = n.value
+        self.offsets = np.array(off[:], np.int64)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                lib().dcrf_batch_destroy(h)
+            except Exception:
+                pass
+
+    def _mat(self, a):
+        return _f32(a, (self.N, self.L))
+
+    def _new(self):
+        return np.empty((self.N, self.L), np.float32)
+
+    def split(self, a):
+        """The per-image pieces of a stacked ``[N, ...]`` array."""
+        return [a[self.offsets[i]:self.offsets[i + 1]] for i in range(len(self.sizes))]
+
+    def setUnaryEnergy(self, unary):
+        u = self._mat(unary)
+        check(lib().dcrf_batch_set_unary(self._h, u.ctypes.data_as(C.c_void_p)))
+
+    def addPairwiseGaussian(self, sx, sy, w):
+        check(lib().dcrf_batch_add_gaussian(self._h, C.c_float(sx), C.c_float(sy), C.c_float(w)))
+
+    def addPairwiseBilateral(self, sx, sy, sr, sg, sb, rgb, w):
+        im = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1)
+        if im.size != 3 * self.N:
+            raise DCRFError(1, "rgb must hold 3 bytes per pixel of every image")
+        check(lib().dcrf_batch_add_bilateral(self._h, *(C.c_float(v) for v in (sx, sy, sr, sg, sb)),
+                                             im.ctypes.data_as(C.c_void_p), C.c_float(w)))
+
+    def unary_init(self):
+        q = self._new()
+        check(lib().dcrf_batch_unary_init(self._h, q.ctypes.data_as(C.c_void_p)))
+        return q
+
+    def qp_inference_super_pixels_non_convex(self, init, max_iter=0, stats=False):
+        x = self._mat(init)
+        out = self._new()
+        p = C.c_int(max_iter)
+        st = (SolveStats * len(self.sizes))()
+        check(lib().dcrf_batch_qp(self._h, x.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p),
+                                  C.byref(p), st))
+        return (out, list(st)) if stats else out
+
+
+__all__.append("DenseCRF2DBatch")

@@ -4,6 +4,7 @@
 #include <cstring>
 #include <string>
 
+#include "batch.cuh"
 #include "model.cuh"
 
 using dcrf::DevBuf;
@@ -15,6 +16,11 @@ struct dcrf_lattice_s {
     dcrf::Lattice lat;
     cudaStream_t stream = nullptr;
     DevBuf<float> feat, in, out;
+};
+
+struct dcrf_batch_s {
+    dcrf::Batch* b = nullptr;
+    DevBuf<float> io0, io1, feat;
 };
 
 struct dcrf_model_s {
@@ -575,6 +581,164 @@ dcrf_status dcrf_model_stream(dcrf_model h, void** stream) {
         auto& m = M(h);
         need(stream, "stream");
         *stream = (void*)m.stream;
+    });
+}
+
+// ------------------------------------------------------------- batches --
+
+static dcrf::Batch& BT(dcrf_batch h) {
+    if (!h || !h->b) throw Error(DCRF_E_ARG, "invalid batch handle");
+    return *h->b;
+}
+
+dcrf_status dcrf_batch_create(dcrf_batch* out, int n_images, const int* widths, const int* heights, int L) {
+    return guard([&] {
+        need(out, "out");
+        need(widths, "widths");
+        need(heights, "heights");
+        check_device();
+        auto* h = new dcrf_batch_s();
+        try {
+            h->b = new dcrf::Batch(n_images, widths, heights, L);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+dcrf_status dcrf_batch_destroy(dcrf_batch h) {
+    return guard([&] {
+        if (!h) return;
+        delete h->b;
+        delete h;
+    });
+}
+
+dcrf_status dcrf_batch_info(dcrf_batch h, int64_t* n_pixels, int64_t* offsets) {
+    return guard([&] {
+        auto& b = BT(h);
+        if (n_pixels) *n_pixels = b.Ntot;
+        if (offsets)
+            for (int i = 0; i <= b.B; i++) offsets[i] = b.pix_off[i];
+    });
+}
+
+dcrf_status dcrf_batch_set_unary_dev(dcrf_batch h, const float* d_unary) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(d_unary, "unary");
+        float* u = b.unary.ensure((size_t)b.Ntot * b.L);
+        DCRF_CUDA(cudaMemcpyAsync(u, d_unary, sizeof(float) * b.Ntot * b.L, cudaMemcpyDeviceToDevice, b.stream));
+        b.has_unary = true;
+    });
+}
+
+dcrf_status dcrf_batch_set_unary(dcrf_batch h, const float* unary) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(unary, "unary");
+        upload(b.unary, unary, (size_t)b.Ntot * b.L, b.stream);
+        DCRF_CUDA(cudaStreamSynchronize(b.stream));
+        b.has_unary = true;
+    });
+}
+
+dcrf_status dcrf_batch_add_gaussian(dcrf_batch h, float sx, float sy, float w_potts) {
+    return guard([&] {
+        auto& b = BT(h);
+        std::vector<float> f((size_t)2 * b.Ntot);
+        for (int n = 0; n < b.B; n++)
+            for (int j = 0; j < b.H[n]; j++)
+                for (int i = 0; i < b.W[n]; i++) {
+                    const size_t p = (size_t)b.pix_off[n] + (size_t)j * b.W[n] + i;
+                    f[2 * p] = i / sx;
+                    f[2 * p + 1] = j / sy;
+                }
+        const float* df = upload(h->feat, f.data(), f.size(), b.stream);
+        b.add_term(df, 2, w_potts);
+        DCRF_CUDA(cudaStreamSynchronize(b.stream));
+    });
+}
+
+dcrf_status dcrf_batch_add_bilateral(dcrf_batch h, float sx, float sy, float sr, float sg, float sb,
+                                     const uint8_t* rgb, float w_potts) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(rgb, "rgb");
+        std::vector<float> f((size_t)5 * b.Ntot);
+        for (int n = 0; n < b.B; n++)
+            for (int j = 0; j < b.H[n]; j++)
+                for (int i = 0; i < b.W[n]; i++) {
+                    const size_t p = (size_t)b.pix_off[n] + (size_t)j * b.W[n] + i;
+                    f[5 * p] = i / sx;
+                    f[5 * p + 1] = j / sy;
+                    f[5 * p + 2] = rgb[3 * p] / sr;
+                    f[5 * p + 3] = rgb[3 * p + 1] / sg;
+                    f[5 * p + 4] = rgb[3 * p + 2] / sb;
+                }
+        const float* df = upload(h->feat, f.data(), f.size(), b.stream);
+        b.add_term(df, 5, w_potts);
+        DCRF_CUDA(cudaStreamSynchronize(b.stream));
+    });
+}
+
+dcrf_status dcrf_batch_unary_init(dcrf_batch h, float* Q) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(Q, "Q");
+        const size_t n = (size_t)b.Ntot * b.L;
+        float* d = h->io0.ensure(n);
+        b.unary_init(d);
+        download(Q, d, n, b.stream);
+    });
+}
+
+static void batch_qp(dcrf::Batch& b, const float* d_init, float* d_out, const dcrf_qp_params* params,
+                     dcrf_solve_stats* stats) {
+    const int max_iter = params ? params->max_iter : 0;
+    if (max_iter < 0) throw Error(DCRF_E_ARG, "max_iter must be >= 0");
+    std::vector<int> steps(b.B);
+    std::vector<double> en(b.B);
+    b.qp(d_init, d_out, max_iter, steps.data(), en.data());
+    if (stats)
+        for (int i = 0; i < b.B; i++) {
+            std::memset(stats + i, 0, sizeof(*stats));
+            stats[i].iterations = steps[i];
+            stats[i].energy = en[i];
+        }
+}
+
+dcrf_status dcrf_batch_qp_dev(dcrf_batch h, const float* d_init, float* d_out, const dcrf_qp_params* params,
+                              dcrf_solve_stats* stats) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(d_init, "init");
+        need(d_out, "out");
+        batch_qp(b, d_init, d_out, params, stats);
+    });
+}
+
+dcrf_status dcrf_batch_qp(dcrf_batch h, const float* init, float* out, const dcrf_qp_params* params,
+                          dcrf_solve_stats* stats) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(init, "init");
+        need(out, "out");
+        const size_t n = (size_t)b.Ntot * b.L;
+        float* di = upload(h->io0, init, n, b.stream);
+        float* dout = h->io1.ensure(n);
+        batch_qp(b, di, dout, params, stats);
+        download(out, dout, n, b.stream);
+    });
+}
+
+dcrf_status dcrf_batch_stream(dcrf_batch h, void** stream) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(stream, "stream");
+        *stream = (void*)b.stream;
     });
 }
 

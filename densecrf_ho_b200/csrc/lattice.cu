@@ -323,6 +323,15 @@ __global__ void seg_fill_kernel(int E, int d1, const int* __restrict__ sorted_en
 // and normalisation factors) are in flight, so a single long list is not
 // serialised on L2 latency.  Vertices are visited longest list first
 // (`order`) so the few very long lists of a coarse lattice start early.
+// Images whose work a batched solve no longer needs: the filters skip the
+// vertices (and pixels, by their first vertex) of image vimg[v] when
+// done[vimg[v]] is set.  done == nullptr (single images) skips nothing.
+struct Skip {
+    const int* vimg = nullptr;
+    const int* done = nullptr;
+};
+__device__ __forceinline__ bool skipped(const Skip& sk, int v) { return sk.done && sk.done[sk.vimg[v]]; }
+
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
 }
@@ -390,7 +399,7 @@ template <bool PRE_NORM>
 __global__ void __launch_bounds__(32 * kStageWarps)
     splat_kernel(int M, int L, const int* __restrict__ order, const int* __restrict__ seg_start,
                  const int* __restrict__ seg_pix, const float* __restrict__ seg_w, const float* __restrict__ in,
-                 const float* __restrict__ norm, float* __restrict__ vals) {
+                 const float* __restrict__ norm, float* __restrict__ vals, Skip sk) {
     __shared__ float ring[kStageWarps][kStages][kChunk][32];
     __shared__ float mw[kStageWarps][kStages][kChunk];
     __shared__ float mn[kStageWarps][kStages][kChunk];
@@ -398,6 +407,7 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     const int unit = blockIdx.x * kStageWarps + wib;
     if (unit >= M) return;  // warp-uniform; the kernel has no block-wide barrier
     const int v = order[unit];
+    if (skipped(sk, v)) return;
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
     for (int kb = 0; kb < L; kb += 32) {
         const int k = kb + lane;
@@ -422,11 +432,12 @@ template <bool PRE_NORM>
 __global__ void splat_short_kernel(int n_short, int L, const int* __restrict__ order,
                                    const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
                                    const float* __restrict__ seg_w, const float* __restrict__ in,
-                                   const float* __restrict__ norm, float* __restrict__ vals) {
+                                   const float* __restrict__ norm, float* __restrict__ vals, Skip sk) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n_short * L) return;
     const int u = (int)(t / L), k = (int)(t - (long)u * L);
     const int v = order[u];
+    if (skipped(sk, v)) return;
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
     float acc = 0.0f;
 #pragma unroll 4
@@ -459,10 +470,11 @@ __global__ void order_key_kernel(int M, const int* __restrict__ counts, int* __r
 // evaluates it in double (0.5 is a double literal there, :518).
 template <bool SEQ>
 __global__ void blur_kernel(int M, int L, const int2* __restrict__ nbr,
-                            const float* __restrict__ src, float* __restrict__ dst) {
+                            const float* __restrict__ src, float* __restrict__ dst, Skip sk) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)M * L) return;
     const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    if (skipped(sk, v)) return;
     const int2 nb = nbr[v];
     const float a = src[(long)(v + 1) * L + k];
     const float s = fadd(src[(long)nb.x * L + k], src[(long)nb.y * L + k]);
@@ -487,11 +499,12 @@ __device__ __forceinline__ float apply_epilogue(float v, long t, int i, const Sl
 template <bool SEQ>
 __global__ void slice_kernel(int N, int L, int d, const int* __restrict__ offset,
                              const float* __restrict__ bary, const float* __restrict__ vals,
-                             float alpha, float* out, SliceEpilogue ep) {
+                             float alpha, float* out, SliceEpilogue ep, Skip sk) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)N * L) return;
     const int i = (int)(t / L), k = (int)(t - (long)i * L);
     const int d1 = d + 1;
+    if (skipped(sk, offset[(long)i * d1])) return;
     float acc = 0.0f;
     for (int j = 0; j <= d; j++) {
         const int o = offset[(long)i * d1 + j];
@@ -1010,6 +1023,106 @@ void build_impl(Lattice& L, const float* d_features) {
 
 }  // namespace
 
+// ------------------------------------------------------ concatenation --
+// Several images' lattices as one: vertex, pixel and entry ids of part i are
+// shifted by the parts before it, so one filter launch sequence runs every
+// image at once and each image's values are those of its own lattice (no
+// list, neighbour or slice crosses an image).
+namespace {
+
+__global__ void add_offset_kernel(long n, const int* __restrict__ src, int add, int* __restrict__ dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = src[t] + add;
+}
+
+// Neighbour rows are vertex + 1, with 0 for "absent".
+__global__ void nbr_offset_kernel(long n, const int2* __restrict__ src, int add, int2* __restrict__ dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int2 a = src[t];
+    dst[t] = make_int2(a.x > 0 ? a.x + add : 0, a.y > 0 ? a.y + add : 0);
+}
+
+__global__ void fill_int_kernel(long n, int v, int* __restrict__ x) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) x[t] = v;
+}
+
+__global__ void seg_count_kernel(int M, const int* __restrict__ seg_start, int* __restrict__ counts) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < M) counts[v] = seg_start[v + 1] - seg_start[v];
+}
+
+}  // namespace
+
+void Lattice::concat(const std::vector<const Lattice*>& parts) {
+    require(!parts.empty(), DCRF_E_ARG, "lattice concat: no parts");
+    cudaStream_t st = stream;
+    d = parts[0]->d;
+    const int d1 = d + 1;
+    long Nt = 0, Mt = 0;
+    for (const Lattice* p : parts) {
+        require(p->d == d, DCRF_E_ARG, "lattice concat: parts differ in feature dimension");
+        Nt += p->N;
+        Mt += p->M;
+    }
+    require(Nt * d1 < (1L << 30) && Mt < (1L << 30), DCRF_E_ARG, "lattice concat: too large");
+    N = (int)Nt;
+    M = (int)Mt;
+    const long E = Nt * d1;
+    int* off = offset.ensure(E);
+    int* rk = rank.ensure(E);
+    float* by = bary.ensure(E);
+    int* ss = seg_start.ensure(M + 1);
+    int* sp = seg_pix.ensure(E);
+    float* sw = seg_w.ensure(E);
+    int2* nb = nbr.ensure((size_t)d1 * M);
+    int* vi = vimg.ensure(std::max(M, 1));
+    long pb = 0, vb_ = 0;
+    int part = 0;
+    for (const Lattice* p : parts) {
+        const long e = (long)p->N * d1, eb = pb * d1;
+        DCRF_CUDA(cudaStreamSynchronize(p->stream));  // the part was built on its own stream
+        launch(add_offset_kernel, ceil_div(e, kTB), kTB, 0, st, e, p->offset.get(), (int)vb_, off + eb);
+        DCRF_CUDA(cudaMemcpyAsync(rk + eb, p->rank.get(), sizeof(int) * e, cudaMemcpyDeviceToDevice, st));
+        DCRF_CUDA(cudaMemcpyAsync(by + eb, p->bary.get(), sizeof(float) * e, cudaMemcpyDeviceToDevice, st));
+        if (p->M) {
+            launch(add_offset_kernel, ceil_div(p->M, kTB), kTB, 0, st, (long)p->M, p->seg_start.get(), (int)eb,
+                   ss + vb_);
+            for (int j = 0; j < d1; j++)
+                launch(nbr_offset_kernel, ceil_div(p->M, kTB), kTB, 0, st, (long)p->M,
+                       p->nbr.get() + (long)j * p->M, (int)vb_, nb + (long)j * M + vb_);
+        }
+        launch(add_offset_kernel, ceil_div(e, kTB), kTB, 0, st, e, p->seg_pix.get(), (int)pb, sp + eb);
+        DCRF_CUDA(cudaMemcpyAsync(sw + eb, p->seg_w.get(), sizeof(float) * e, cudaMemcpyDeviceToDevice, st));
+        if (p->M) launch(fill_int_kernel, ceil_div(p->M, kTB), kTB, 0, st, (long)p->M, part, vi + vb_);
+        pb += p->N;
+        vb_ += p->M;
+        part++;
+    }
+    const int Ei = (int)E;
+    DCRF_CUDA(cudaMemcpyAsync(ss + M, &Ei, sizeof(int), cudaMemcpyHostToDevice, st));
+    // Longest lists first, over all images.
+    int* cnt = counts.ensure(std::max(M, 1));
+    launch(seg_count_kernel, ceil_div(M, kTB), kTB, 0, st, M, ss, cnt);
+    int* vo = vorder.ensure(M);
+    int* ok = vorder_keys.ensure(M);
+    launch(order_key_kernel, ceil_div(M, kTB), kTB, 0, st, M, cnt, ok, vo);
+    radix_sort_pairs(ok, vo, M, 24, sort, st);
+    int* dl = total.ensure(2);
+    DCRF_CUDA(cudaMemsetAsync(dl, 0, 2 * sizeof(int), st));
+    launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, cnt, kLongList, dl);
+    launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, cnt, kHugeList, dl + 1);
+    DCRF_LAUNCH_CHECK();
+    int nl[2];
+    DCRF_CUDA(cudaMemcpyAsync(nl, dl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCRF_CUDA(cudaStreamSynchronize(st));  // also keeps &Ei alive until its copy ran
+    n_long = nl[0];
+    n_huge = nl[1];
+    va_floats = 0;
+    concatenated = true;
+}
+
 void Lattice::build(const float* d_features, int d_, int N_) {
     require(N_ > 0, DCRF_E_ARG, "lattice: N must be positive");
     require(d_ >= 1 && d_ <= 16, DCRF_E_ARG, "lattice: feature dimension must be in [1, 16]");
@@ -1090,27 +1203,27 @@ void Lattice::compute_noalloc(float* out, const float* in, int L, bool reverse) 
     const int n_short = M - n_long;
     if (n_long)
         launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{});
     if (n_short)
         launch(splat_short_kernel<false>, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
-               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{});
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
         if (seq)
-            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{});
         else
-            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
+            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{});
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     const SliceEpilogue ep;
     if (seq)
         launch(slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
-               out, ep);
+               out, ep, Skip{});
     else
         launch(slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
-               out, ep);
+               out, ep, Skip{});
     DCRF_LAUNCH_CHECK();
 }
 
@@ -1126,34 +1239,34 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     if (pre_norm) {
         if (n_long)
             launch(splat_kernel<true>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src);
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, Skip{vimg.get(), skip_done});
         if (n_short)
             launch(splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src);
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, Skip{vimg.get(), skip_done});
     } else {
         if (n_long)
             launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{vimg.get(), skip_done});
         if (n_short)
             launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src);
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{vimg.get(), skip_done});
     }
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
         if (seq)
-            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
         else
-            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst);
+            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     if (seq)
         launch(slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-                                                              alpha, out, ep);
+                                                              alpha, out, ep, Skip{vimg.get(), skip_done});
     else
         launch(slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-                                                               alpha, out, ep);
+                                                               alpha, out, ep, Skip{vimg.get(), skip_done});
     DCRF_LAUNCH_CHECK();
 }
 

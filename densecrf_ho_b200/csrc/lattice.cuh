@@ -17,6 +17,8 @@
 #include "common.cuh"
 #include "primitives.cuh"
 
+#include <vector>
+
 namespace dcrf {
 
 // What the slice kernel does with the filtered value v of (pixel i, label k).
@@ -66,8 +68,14 @@ struct Lattice {
     ScanScratch scan;
     SortScratch sort;
 
+    bool concatenated = false;  // built by concat(): no vertex keys
+    DevBuf<int> vimg;           // concat(): image of each vertex
+    const int* skip_done = nullptr;  // concat(): per-image flags; compute() skips flagged images
+
     // features: device [N][d]
     void build(const float* d_features, int d_, int N_);
+    // Several images' lattices as one (see Lattice::concat in lattice.cu).
+    void concat(const std::vector<const Lattice*>& parts);
     // out/in: device [N][L]; out may alias in.
     void compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,
                  const float* pre_norm = nullptr);

@@ -35,6 +35,7 @@ struct SolverScalars {
     int zero_step;        // QP: num == 0 or denom == 0
     int steps;
     int err;              // DCRF_E_* raised by a device check
+    int done;             // batched QP: the image had stopped before this iteration
 };
 
 struct Model {

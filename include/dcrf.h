@@ -197,6 +197,39 @@ dcrf_status dcrf_model_info(dcrf_model m, int* n_terms, int* N, int* L);
 dcrf_status dcrf_model_lattice_size(dcrf_model m, int k, int* M);
 dcrf_status dcrf_model_stream(dcrf_model m, void** stream);
 
+/* ---- Batches: many images of different sizes in one solve ----------------
+ * No counterpart in the reference, which solves one DenseCRF2D at a time
+ * (src/example_inference.cpp:39-63); a batch holds n images that share the
+ * label count and the pairwise parameters.  Pixel arrays are the images'
+ * arrays one after another: unaries / Q [sum W_i H_i][L], rgb
+ * [sum W_i H_i][3].  Each image's QP result equals the single-image
+ * dcrf_model_qp of that image. */
+typedef struct dcrf_batch_s* dcrf_batch;
+
+dcrf_status dcrf_batch_create(dcrf_batch* out, int n_images, const int* widths,
+                              const int* heights, int L);
+dcrf_status dcrf_batch_destroy(dcrf_batch b);
+/* Total pixel count and pixel offset of each image (offsets: n_images + 1
+ * entries, may be NULL). */
+dcrf_status dcrf_batch_info(dcrf_batch b, int64_t* n_pixels, int64_t* offsets);
+/* setUnaryEnergy for every image (src/densecrf.cpp:151-156). */
+dcrf_status dcrf_batch_set_unary(dcrf_batch b, const float* unary);
+dcrf_status dcrf_batch_set_unary_dev(dcrf_batch b, const float* d_unary);
+/* addPairwiseGaussian / addPairwiseBilateral with Potts weights for every
+ * image (src/densecrf.cpp:170-190). */
+dcrf_status dcrf_batch_add_gaussian(dcrf_batch b, float sx, float sy, float w_potts);
+dcrf_status dcrf_batch_add_bilateral(dcrf_batch b, float sx, float sy, float sr, float sg,
+                                     float sb, const uint8_t* rgb, float w_potts);
+/* unary_init of every image. */
+dcrf_status dcrf_batch_unary_init(dcrf_batch b, float* Q);
+/* qp_inference_super_pixels_non_convex of every image (plain QP, no
+ * cliques).  stats: NULL or an array of n_images. */
+dcrf_status dcrf_batch_qp(dcrf_batch b, const float* init, float* out,
+                          const dcrf_qp_params* params, dcrf_solve_stats* stats);
+dcrf_status dcrf_batch_qp_dev(dcrf_batch b, const float* d_init, float* d_out,
+                              const dcrf_qp_params* params, dcrf_solve_stats* stats);
+dcrf_status dcrf_batch_stream(dcrf_batch b, void** stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,81 @@
+"""Batched QP over images of different sizes (dcrf_batch_*) against the
+single-image solver, image by image.
+
+The batch concatenates the images' lattices and keeps one set of solver
+scalars per image, with every reduction partitioned per image as the
+single-image solver partitions it: outputs, step counts and energies must
+be identical, bit for bit.
+"""
+import numpy as np
+import pytest
+
+from densecrf_ho_b200 import DCRFError, DenseCRF2D, DenseCRF2DBatch, synth
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(37, 29), (64, 48), (50, 50), (23, 41), (96, 31)]
+
+
+def _images(sizes, seed0=11):
+    return [synth.make_image(w, h, 21, seed0 + i) for i, (w, h) in enumerate(sizes)]
+
+
+def _batch(sizes, imgs):
+    b = DenseCRF2DBatch(sizes, 21)
+    b.setUnaryEnergy(np.concatenate([im["unary"] for im in imgs]))
+    b.addPairwiseGaussian(3.0, 3.0, 3.0)
+    b.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, np.concatenate([im["rgb"] for im in imgs]), 5.0)
+    return b
+
+
+def _single(w, h, im):
+    m = DenseCRF2D(w, h, 21)
+    m.setUnaryEnergy(im["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, im["rgb"], 5.0)
+    return m
+
+
+@pytest.mark.parametrize("max_iter", [0, 7])
+def test_batch_qp_equals_single_solves(max_iter):
+    imgs = _images(SIZES)
+    b = _batch(SIZES, imgs)
+    q0 = b.unary_init()
+    out, st = b.qp_inference_super_pixels_non_convex(q0, max_iter=max_iter, stats=True)
+    for i, ((w, h), im) in enumerate(zip(SIZES, imgs)):
+        m = _single(w, h, im)
+        qi = m.unary_init()
+        assert np.array_equal(b.split(q0)[i], qi)
+        o, s = m.qp_inference_super_pixels_non_convex(qi, max_iter=max_iter, stats=True)
+        assert np.array_equal(b.split(out)[i], o), i
+        assert st[i].iterations == s.iterations
+        assert st[i].energy == s.energy
+
+
+def test_batch_qp_repeat_is_deterministic():
+    """The second solve replays the captured iteration graph."""
+    imgs = _images(SIZES[:3], 40)
+    b = _batch(SIZES[:3], imgs)
+    q0 = b.unary_init()
+    a = b.qp_inference_super_pixels_non_convex(q0, max_iter=5)
+    c = b.qp_inference_super_pixels_non_convex(q0, max_iter=5)
+    d = b.qp_inference_super_pixels_non_convex(q0)
+    e = b.qp_inference_super_pixels_non_convex(q0)
+    assert np.array_equal(a, c)
+    assert np.array_equal(d, e)
+
+
+def test_batch_single_image_and_errors():
+    (w, h), = [(41, 33)]
+    im = synth.make_image(w, h, 21, 3)
+    b = _batch([(w, h)], [im])
+    q0 = b.unary_init()
+    m = _single(w, h, im)
+    assert np.array_equal(b.qp_inference_super_pixels_non_convex(q0), m.qp_inference_super_pixels_non_convex(q0))
+    with pytest.raises(DCRFError) as e:
+        DenseCRF2DBatch([(10, 0)], 21)
+    assert e.value.code == 1
+    nb = DenseCRF2DBatch([(8, 8), (4, 4)], 21)
+    with pytest.raises(DCRFError) as e:
+        nb.qp_inference_super_pixels_non_convex(np.zeros((80, 21), np.float32))
+    assert e.value.code == 4
