@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--only-roofline", action="store_true",
                     help="time only the ordered and plain lattice filters (a short command for ncu)")
     ap.add_argument("--only-batch", action="store_true",
-                    help="time only the 64-image batched QP against sequential solves")
+                    help="time only the 64-image batched QP and the 16-image mean-field adjoint")
     ap.add_argument("--prox-iters", type=int, default=50,
                     help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
     return ap.parse_args()
@@ -464,6 +464,72 @@ def measure_batch(n=64, max_iter=100, reps=3):
             "outputs_match_sequential": same}
 
 
+def measure_adjoint(n=16, size=512, T=10, reps=3):
+    """Config 5: unrolled mean-field (T iterations) forward and its hand-written
+    adjoint (dcrf_batch_meanfield_dev / _backward_dev) on n size x size images,
+    21 labels, gradients with respect to the unaries and both Potts weights;
+    device-resident, CUDA events on the batch's stream.  The gradient is
+    checked here against a central difference of the FP32 forward along a
+    random direction (the FP64 finite-difference check at 256 coordinates is
+    tests/test_adjoint_gpu.py)."""
+    import torch
+    from densecrf_ho_b200 import DenseCRF2DBatch, lib, check
+    Ls = lib()
+    sizes = [(size, size)] * n
+    imgs = [synth.make_image(size, size, L, 2000 + i) for i in range(n)]
+    b = DenseCRF2DBatch(sizes, L)
+    U = np.concatenate([im["unary"] for im in imgs])
+    b.setUnaryEnergy(U)
+    b.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+    b.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
+                           np.concatenate([im["rgb"] for im in imgs]), BILAT[2])
+    rng = np.random.default_rng(5)
+    c = torch.from_numpy(rng.standard_normal(U.shape).astype(np.float32)).cuda()
+    Q = torch.empty_like(c)
+    gU = torch.empty_like(c)
+    gw = np.zeros(2, np.float64)
+    sptr = C.c_void_p()
+    check(Ls.dcrf_batch_stream(b._h, C.byref(sptr)))
+    st = torch.cuda.ExternalStream(sptr.value)
+    fwd = lambda: check(Ls.dcrf_batch_meanfield_dev(b._h, T, C.c_void_p(Q.data_ptr())))
+    bwd = lambda: check(Ls.dcrf_batch_meanfield_backward_dev(b._h, C.c_void_p(c.data_ptr()), C.c_void_p(gU.data_ptr()),
+                                                             gw.ctypes.data_as(C.c_void_p)))
+    fwd()
+    bwd()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    tf = tb = 0.0
+    for _ in range(reps):
+        ev[0].record(st)
+        fwd()
+        ev[1].record(st)
+        bwd()
+        ev[2].record(st)
+        torch.cuda.synchronize()
+        tf += ev[0].elapsed_time(ev[1])
+        tb += ev[1].elapsed_time(ev[2])
+    tf, tb = tf / reps, tb / reps
+    # directional check: <dL/dU, V> vs (L(U + eV) - L(U - eV)) / 2e, L = sum(c o Q_T)
+    V = rng.standard_normal(U.shape).astype(np.float32)
+    eps = 1e-2
+    cd = c.double()
+
+    def loss(UU):
+        b.setUnaryEnergy(UU)
+        fwd()
+        torch.cuda.synchronize()
+        return float((cd * Q.double()).sum())
+
+    pred = float((gU.double() * torch.from_numpy(V).cuda().double()).sum())
+    dd = (loss(U + eps * V) - loss(U - eps * V)) / (2 * eps)
+    b.setUnaryEnergy(U)
+    return {"workload": f"unrolled mean-field, {n} images {size}x{size}, L={L}, {T} iterations, forward + adjoint "
+                        f"(dL/dU and dL/dw for the Gaussian and bilateral Potts weights)",
+            "forward_ms": tf, "backward_ms": tb, "images_per_s": n / ((tf + tb) / 1e3),
+            "pixels": n * size * size, "directional_check_rel_err": abs(dd - pred) / abs(pred),
+            "grad_w": [float(x) for x in gw]}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -483,6 +549,7 @@ def run_ours(args):
         return
     if args.only_batch:
         print(json.dumps(measure_batch()))
+        print(json.dumps(measure_adjoint()))
         return
     t0 = time.perf_counter()
     crf = DenseCRF2D(W, H, L)
@@ -581,6 +648,7 @@ def run_ours(args):
     if rank == 0 and world == 1:
         line["extra"]["qp_320x240"] = measure_qp(cpu=not args.no_cpu_baseline)
         line["extra"]["batch_qp_64"] = measure_batch()
+        line["extra"]["adjoint_16x512x512"] = measure_adjoint()
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference(W, H, args.seed, prox_iters, 1, 10, 1)

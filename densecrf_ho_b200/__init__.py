@@ -297,5 +297,30 @@ class DenseCRF2DBatch:
                                   C.byref(p), st))
         return (out, list(st)) if stats else out
 
+    # -- differentiation (unrolled mean-field) --------------------------
+    def n_terms(self):
+        n = C.c_int()
+        check(lib().dcrf_batch_terms(self._h, C.byref(n)))
+        return n.value
+
+    def set_weight(self, k, w):
+        check(lib().dcrf_batch_set_weight(self._h, int(k), C.c_float(w)))
+
+    def meanfield(self, iterations):
+        """Q_T of ``iterations`` mean-field steps (Q_0 .. Q_T are kept for
+        :meth:`meanfield_backward`)."""
+        out = self._new()
+        check(lib().dcrf_batch_meanfield(self._h, int(iterations), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def meanfield_backward(self, grad_Q):
+        """``(dL/dU, dL/dw)`` for ``grad_Q = dL/dQ_T`` of the last :meth:`meanfield`."""
+        g = self._mat(grad_Q)
+        gu = self._new()
+        gw = np.zeros(max(self.n_terms(), 1), np.float64)
+        check(lib().dcrf_batch_meanfield_backward(self._h, g.ctypes.data_as(C.c_void_p),
+                                                  gu.ctypes.data_as(C.c_void_p), gw.ctypes.data_as(C.c_void_p)))
+        return gu, gw[:self.n_terms()]
+
 
 __all__.append("DenseCRF2DBatch")

@@ -734,6 +734,57 @@ dcrf_status dcrf_batch_qp(dcrf_batch h, const float* init, float* out, const dcr
     });
 }
 
+dcrf_status dcrf_batch_meanfield_dev(dcrf_batch h, int iterations, float* d_Q) {
+    return guard([&] { BT(h).meanfield(iterations, d_Q); });
+}
+
+dcrf_status dcrf_batch_meanfield(dcrf_batch h, int iterations, float* Q) {
+    return guard([&] {
+        auto& b = BT(h);
+        const size_t n = (size_t)b.Ntot * b.L;
+        float* d = Q ? h->io1.ensure(n) : nullptr;
+        b.meanfield(iterations, d);
+        if (Q) download(Q, d, n, b.stream);
+        DCRF_CUDA(cudaStreamSynchronize(b.stream));
+    });
+}
+
+dcrf_status dcrf_batch_meanfield_backward_dev(dcrf_batch h, const float* d_grad_Q, float* d_grad_U,
+                                              double* grad_w) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(d_grad_Q, "grad_Q");
+        need(d_grad_U, "grad_U");
+        if (!b.terms.empty()) need(grad_w, "grad_w");
+        b.meanfield_backward(d_grad_Q, d_grad_U, grad_w);
+    });
+}
+
+dcrf_status dcrf_batch_meanfield_backward(dcrf_batch h, const float* grad_Q, float* grad_U, double* grad_w) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(grad_Q, "grad_Q");
+        need(grad_U, "grad_U");
+        if (!b.terms.empty()) need(grad_w, "grad_w");
+        const size_t n = (size_t)b.Ntot * b.L;
+        const float* dg = upload(h->io0, grad_Q, n, b.stream);
+        float* du = h->io1.ensure(n);
+        b.meanfield_backward(dg, du, grad_w);
+        download(grad_U, du, n, b.stream);
+    });
+}
+
+dcrf_status dcrf_batch_set_weight(dcrf_batch h, int k, float w_potts) {
+    return guard([&] { BT(h).set_weight(k, w_potts); });
+}
+
+dcrf_status dcrf_batch_terms(dcrf_batch h, int* n_terms) {
+    return guard([&] {
+        need(n_terms, "n_terms");
+        *n_terms = (int)BT(h).terms.size();
+    });
+}
+
 dcrf_status dcrf_batch_stream(dcrf_batch h, void** stream) {
     return guard([&] {
         auto& b = BT(h);

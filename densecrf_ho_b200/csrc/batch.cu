@@ -280,6 +280,70 @@ __global__ void bnorm_kernel(long N, float* x) {
     if (i < N) x[i] = (float)(1.0 / sqrt(dadd((double)x[i], 1e-20)));
 }
 
+// ---- mean-field ---------------------------------------------------------
+
+// expAndNormalize (src/densecrf.cpp:328-336) of the logits a: per pixel
+// exp(a - max) / sum, the sum in Eigen's packet order.
+template <int LC>
+__global__ void softmax_kernel(long N, int Lrt, const float* __restrict__ a, float* __restrict__ Q) {
+    const int L = LC ? LC : Lrt;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    float b[PixVec<LC>::S];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) b[k] = a[i * L + k];
+    float mx = b[0];
+#pragma unroll
+    for (int k = 1; k < PixVec<LC>::S; k++)
+        if (k < L && b[k] > mx) mx = b[k];
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) b[k] = expf(fsub(b[k], mx));
+    const float sm = vec_sum<LC>(b, L);
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) Q[i * L + k] = b[k] / sm;
+}
+
+// Softmax adjoint: ga = Q o (g - <g, Q>) per pixel; dU = (first ? 0 : dU) - ga
+// (the logits are -U + messages).
+template <int LC>
+__global__ void softmax_bwd_kernel(long N, int Lrt, const float* __restrict__ Q, const float* __restrict__ g,
+                                   float* __restrict__ ga, float* __restrict__ dU, int first) {
+    const int L = LC ? LC : Lrt;
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) s += (double)g[i * L + k] * (double)Q[i * L + k];
+    const float sf = (float)s;
+#pragma unroll
+    for (int k = 0; k < PixVec<LC>::S; k++)
+        if (k < L) {
+            const long e = i * L + k;
+            const float v = Q[e] * (g[e] - sf);
+            ga[e] = v;
+            dU[e] = (first ? 0.0f : dU[e]) - v;
+        }
+}
+
+__global__ void negate_kernel(long n, const float* __restrict__ x, float* __restrict__ y) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) y[t] = -x[t];
+}
+
+// acc[j] += sum of the nblk partials (one warp, fixed order).
+__global__ void accumulate_total_kernel(const double* __restrict__ partials, int nblk, double* acc) {
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    for (int b = lane; b < nblk; b += 32) s += partials[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
+    if (lane == 0) *acc += s;
+}
+
 }  // namespace
 
 Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_) {
@@ -492,6 +556,96 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
         most = std::max(most, h_scal[i].steps);
     }
     return most;
+}
+
+// ---- mean-field and its adjoint --------------------------------------------
+
+void Batch::set_weight(int k, float w) {
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+    terms[k]->w = w;
+    drop_graph();  // the captured QP iteration holds the old weight
+}
+
+// out = base + scale * n o K(n o in), K transposed (blur axes reversed) when
+// `transpose`.  The blur of one axis is symmetric, so K^T is the filter with
+// the axes in reverse order.
+static void normalised_filter(Term& t, int L, float* out, const float* in, float scale, const float* base,
+                              bool transpose) {
+    SliceEpilogue ep;
+    ep.potts = true;
+    ep.norm = t.norm.get();
+    ep.scale = scale;
+    ep.base = base;
+    ep.coef = 1.0f;
+    t.lat->compute(out, in, L, transpose, ep, t.norm.get());
+}
+
+void Batch::meanfield(int iterations, float* Q) {
+    require(has_unary, DCRF_E_STATE, "meanfield: no unary energy set");
+    require(iterations >= 0 && iterations <= 1000, DCRF_E_ARG, "meanfield: iterations must be in [0, 1000]");
+    const long NL = Ntot * L;
+    float* ck = mf_ck.ensure((size_t)(iterations + 1) * NL);
+    float* negU = buf(4);
+    float* logits = buf(5);
+    launch(negate_kernel, ceil_div(NL, 256), 256, 0, stream, NL, unary.get(), negU);
+    unary_init(ck);  // Q_0 = softmax(-U)
+    const int nt = (int)terms.size();
+    for (int it = 0; it < iterations; it++) {
+        const float* q = ck + (size_t)it * NL;
+        if (nt == 0)
+            DCRF_CUDA(cudaMemcpyAsync(logits, negU, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+        for (int k = 0; k < nt; k++)  // logits = -U + sum_k w_k K~_k Q
+            normalised_filter(*terms[k], L, logits, q, terms[k]->w, k == 0 ? negU : logits, false);
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            launch(softmax_kernel<LC>, ceil_div(Ntot, 128), 128, 0, stream, Ntot, L, logits,
+                   ck + (size_t)(it + 1) * NL);
+        });
+    }
+    DCRF_LAUNCH_CHECK();
+    if (Q) DCRF_CUDA(cudaMemcpyAsync(Q, ck + (size_t)iterations * NL, sizeof(float) * NL,
+                                     cudaMemcpyDeviceToDevice, stream));
+    mf_T = iterations;
+}
+
+void Batch::meanfield_backward(const float* grad_Q, float* grad_U, double* grad_w) {
+    require(mf_T >= 0, DCRF_E_STATE, "meanfield_backward: no meanfield() to differentiate");
+    const long NL = Ntot * L;
+    const int nt = (int)terms.size();
+    const float* ck = mf_ck.get();
+    float* g = mf_g0.ensure(NL);
+    float* gn = mf_g1.ensure(NL);
+    float* ga = mf_ga.ensure(NL);
+    float* m = mf_m.ensure(NL);
+    double* dw = mf_dw.ensure(std::max(nt, 1));
+    double* part = partials.get();
+    DCRF_CUDA(cudaMemcpyAsync(g, grad_Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    if (nt) DCRF_CUDA(cudaMemsetAsync(dw, 0, sizeof(double) * nt, stream));
+    auto softmax_bwd = [&](const float* q, int first) {
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            launch(softmax_bwd_kernel<LC>, ceil_div(Ntot, 128), 128, 0, stream, Ntot, L, q, g, ga, grad_U, first);
+        });
+    };
+    for (int it = mf_T - 1; it >= 0; it--) {
+        const float* q0 = ck + (size_t)it * NL;
+        const float* q1 = ck + (size_t)(it + 1) * NL;
+        softmax_bwd(q1, it == mf_T - 1);  // ga = dL/dlogits_t; grad_U -= ga
+        for (int k = 0; k < nt; k++) {
+            // dL/dw_k += <ga, K~_k Q_t>, the message recomputed from the checkpoint
+            normalised_filter(*terms[k], L, m, q0, 1.0f, nullptr, false);
+            launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, ga, m, part);
+            launch(accumulate_total_kernel, 1, 32, 0, stream, part, kRedBlocks, dw + k);
+            // dL/dQ_t = sum_k w_k K~_k^T ga
+            normalised_filter(*terms[k], L, gn, ga, terms[k]->w, k == 0 ? nullptr : gn, true);
+        }
+        if (nt == 0) DCRF_CUDA(cudaMemsetAsync(gn, 0, sizeof(float) * NL, stream));
+        std::swap(g, gn);
+    }
+    softmax_bwd(ck, mf_T == 0);  // Q_0 = softmax(-U)
+    DCRF_LAUNCH_CHECK();
+    if (nt) DCRF_CUDA(cudaMemcpyAsync(grad_w, dw, sizeof(double) * nt, cudaMemcpyDeviceToHost, stream));
+    DCRF_CUDA(cudaStreamSynchronize(stream));
 }
 
 }  // namespace dcrf

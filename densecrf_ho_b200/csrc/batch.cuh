@@ -34,6 +34,11 @@ struct Batch {
     SolverScalars* h_scal = nullptr;  // pinned, B
     int max_tiles = 0;           // row-tile blocks of the largest image
 
+    // mean-field checkpoints Q_0 .. Q_mf_T, [mf_T + 1][Ntot][L]
+    DevBuf<float> mf_ck, mf_g0, mf_g1, mf_ga, mf_m;
+    DevBuf<double> mf_dw;
+    int mf_T = -1;
+
     // the captured QP iteration (valid while the output buffer and max_iter are the same)
     cudaGraphExec_t graph = nullptr;
     const float* graph_q = nullptr;
@@ -52,6 +57,15 @@ struct Batch {
     // Returns the largest per-image step count; per-image counts / energies
     // go to steps / energies when given (host arrays of B).
     int qp(const float* init, float* out, int max_iter, int* steps, double* energies);
+
+    // Mean-field iterations Q_0 = softmax(-U), Q_{t+1} = softmax(-U + sum_k
+    // w_k K~_k Q_t) (K~ = the normalised Gaussian / bilateral filter), with
+    // Q_0 .. Q_T kept as checkpoints for meanfield_backward.
+    void meanfield(int iterations, float* Q);
+    // Gradients of a loss through the last meanfield(): grad_Q = dL/dQ_T in,
+    // dL/dU and dL/dw_k (summed over all images, FP64) out.
+    void meanfield_backward(const float* grad_Q, float* grad_U, double* grad_w);
+    void set_weight(int k, float w);
 
   private:
     void qp_iteration(float* Q, int max_iter);

@@ -230,6 +230,30 @@ dcrf_status dcrf_batch_qp_dev(dcrf_batch b, const float* d_init, float* d_out,
                               const dcrf_qp_params* params, dcrf_solve_stats* stats);
 dcrf_status dcrf_batch_stream(dcrf_batch b, void** stream);
 
+/* ---- Differentiation: unrolled mean-field and its adjoint ----------------
+ * No counterpart in the reference, whose solvers are not differentiable
+ * (the QP's conditional gradient is an arg-min).  These run Krahenbuhl's
+ * mean-field iterations on every image of the batch,
+ *   Q_0 = softmax(-U),  Q_{t+1} = softmax(-U + sum_k w_k K~_k Q_t),
+ * K~_k = the k-th term's normalised filter n o K(n o .) (src/pairwise.cpp:
+ * 54-75), and back-propagate a loss gradient through them with the adjoint
+ * filter (blur axes in reverse order, src/permutohedral.cpp:1079-1093).
+ * meanfield keeps Q_0 .. Q_T on the device; meanfield_backward recomputes
+ * the messages K~_k Q_t from them. */
+/* Q (may be NULL): the final iterate [N][L]. */
+dcrf_status dcrf_batch_meanfield(dcrf_batch b, int iterations, float* Q);
+dcrf_status dcrf_batch_meanfield_dev(dcrf_batch b, int iterations, float* d_Q);
+/* grad_Q = dL/dQ_T [N][L] in; dL/dU [N][L] and dL/dw_k (n_terms doubles,
+ * summed over all images) out. */
+dcrf_status dcrf_batch_meanfield_backward(dcrf_batch b, const float* grad_Q, float* grad_U,
+                                          double* grad_w);
+dcrf_status dcrf_batch_meanfield_backward_dev(dcrf_batch b, const float* d_grad_Q, float* d_grad_U,
+                                              double* grad_w);
+/* Potts weight of pairwise term k (the PottsCompatibility parameter,
+ * src/labelcompatibility.cpp:68-70), and the number of terms. */
+dcrf_status dcrf_batch_set_weight(dcrf_batch b, int k, float w_potts);
+dcrf_status dcrf_batch_terms(dcrf_batch b, int* n_terms);
+
 #ifdef __cplusplus
 }
 #endif
