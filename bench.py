@@ -68,7 +68,7 @@ def parse():
     ap.add_argument("--only-roofline", action="store_true",
                     help="time only the ordered and plain lattice filters (a short command for ncu)")
     ap.add_argument("--only-batch", action="store_true",
-                    help="time only the 64-image batched QP and the 16-image mean-field adjoint")
+                    help="time only qp_sp / lp_sp, the 64-image batched QP and the 16-image mean-field adjoint")
     ap.add_argument("--prox-iters", type=int, default=50,
                     help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
     return ap.parse_args()
@@ -384,6 +384,79 @@ def measure_qp(reps=10, cpu=True):
     return res
 
 
+def measure_ho(W=640, H=480, seed=2, cpu=True):
+    """Config 3: qp_sp and lp_sp (the QP / LP with sparse superpixel cliques)
+    at 640x480.  Cliques: three seeded superpixel scales (synth.superpixels,
+    the stand-in for the reference's mean-shift at spatial 8 / 16 / 32), each
+    clique 500-2000 pixels, with addSuperPixel's weights for the HO settings
+    (constant, normaliser) = (1.0, 0.5) and the CLI's (50, 1000).  GPU solves/s
+    (device-resident) and the energies; for the (50, 1000) setting also the
+    reference's own qp_sp on one CPU core and the relative energy gap."""
+    import torch
+    from densecrf_ho_b200 import DenseCRF2D, LPParams, SolveStats, lib, check
+    Ls = lib()
+    img = synth.make_image(W, H, L, seed)
+    out = {"workload": f"qp_sp / lp_sp {W}x{H} L={L}, synthetic superpixel cliques at 3 scales (500-2000 px)"}
+    for const, norm in ((1.0, 0.5), (50.0, 1000.0)):
+        off, idx, ew, cs = synth.cliques_three_scales(img, const, norm, seed)
+        crf = DenseCRF2D(W, H, L)
+        crf.setUnaryEnergy(img["unary"])
+        crf.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+        crf.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"], BILAT[2])
+        crf.setCliques(off, idx, ew, cs)
+        Q0 = crf.unary_init()
+        init = torch.from_numpy(Q0).cuda()
+        res = torch.empty_like(init)
+        sptr = C.c_void_p()
+        check(Ls.dcrf_model_stream(crf.handle, C.byref(sptr)))
+        stream = torch.cuda.ExternalStream(sptr.value)
+        st = SolveStats()
+        params = LPParams.default()
+        for k, v in LP_OVERRIDES.items():
+            setattr(params, k, v)
+        qp = lambda: check(Ls.dcrf_model_qp_dev(crf.handle, C.c_void_p(init.data_ptr()), C.c_void_p(res.data_ptr()),
+                                                None, C.byref(st)))
+        lp = lambda: check(Ls.dcrf_model_lp_dev(crf.handle, C.c_void_p(init.data_ptr()), C.c_void_p(res.data_ptr()),
+                                                C.byref(params), C.byref(st)))
+        row = {"cliques": int(len(off) - 1), "clique_pixels": int(off[-1]),
+               "exp_weight_range": [float(ew.min()), float(ew.max())]}
+        for name, fn, reps in (("qp_sp", qp, 5), ("lp_sp", lp, 1)):
+            fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            q = res.cpu().numpy()
+            lab = crf.currentMap(q)
+            row[name] = {"solves_per_s": 1e3 / ms, "ms_per_solve": ms, "iterations": st.iterations,
+                         "energy_true": crf.assignment_energy_true(lab),
+                         "energy_higher_order": crf.assignment_energy_higher_order(lab)}
+            if name == "qp_sp":
+                qp_q = q
+        if cpu and const == 50.0:
+            sys.path.insert(0, ROOT)
+            from oracle import oracle as O
+            if O.reference_available():
+                m = O.build_model(O.ReferenceModel, img, gaussian=GAUSS, bilateral=BILAT)
+                m.set_cliques(off, idx, ew, cs)
+                t0 = time.perf_counter()
+                rq, _, _ = m.qp(Q0)
+                dt = time.perf_counter() - t0
+                e_ref = m.energy_ho(m.current_map(rq))
+                e_gpu = row["qp_sp"]["energy_higher_order"]
+                row["qp_sp"]["cpu_reference"] = {"seconds_per_solve": dt, "cores": 1, "kind": "reference",
+                                                 "energy_higher_order": e_ref,
+                                                 "energy_rel_gap": abs(e_gpu - e_ref) / abs(e_ref),
+                                                 "labels_identical": float(np.mean(m.current_map(rq) ==
+                                                                                   crf.currentMap(qp_q)))}
+        out[f"ho_{const:g}_{norm:g}"] = row
+    return out
+
+
 def measure_batch(n=64, max_iter=100, reps=3):
     """Config 4: the plain QP (as config 1, up to 100 Frank-Wolfe iterations)
     of n images of uneven sizes (H ~ U[240, 500], W ~ U[320, 500], seeded),
@@ -548,6 +621,7 @@ def run_ours(args):
         print(json.dumps(measure_filters(W, H, img, reps=3)))
         return
     if args.only_batch:
+        print(json.dumps(measure_ho()))
         print(json.dumps(measure_batch()))
         print(json.dumps(measure_adjoint()))
         return
@@ -647,6 +721,7 @@ def run_ours(args):
                       "ord_filter_ms": {k: v["seconds"] * 1e3 for k, v in roof.items()}}}
     if rank == 0 and world == 1:
         line["extra"]["qp_320x240"] = measure_qp(cpu=not args.no_cpu_baseline)
+        line["extra"]["ho_640x480"] = measure_ho(cpu=not args.no_cpu_baseline)
         line["extra"]["batch_qp_64"] = measure_batch()
         line["extra"]["adjoint_16x512x512"] = measure_adjoint()
 
