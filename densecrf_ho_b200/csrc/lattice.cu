@@ -866,8 +866,9 @@ __global__ void ord_blur_kernel(int M, int row4, const int2* __restrict__ nbr,
 
 // Ordered slice: lower pass with weight -w*alpha, then upper with w*alpha
 // (:639-650, :687-696), accumulated into one value.  With GAP the LP's dual
-// gap terms are folded in: tmp = (alpha + u) - (v + 0) for the final slice
-// value v, and per-block sums of tmp.Q and tmp.tmp (src/densecrf.cpp:725-729).
+// gap terms are folded in: tmp = (alpha + u) - (v + su) for the final slice
+// value v, the clique term su (0 without cliques), and per-block sums of
+// tmp.Q and tmp.tmp (src/densecrf.cpp:725-729).
 template <bool GAP>
 __global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ offset,
                                  const float* __restrict__ bary, const float* __restrict__ vals,
@@ -894,7 +895,7 @@ __global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ of
         const float v = apply_epilogue(acc, t, i, ep);
         out[t] = v;
         if (GAP) {
-            const float tmp = fsub(fadd(gf.alpha[t], gf.u[t]), fadd(v, 0.0f));
+            const float tmp = fsub(fadd(gf.alpha[t], gf.u[t]), fadd(v, gf.su ? gf.su[t] : 0.0f));
             g0 = (double)tmp * (double)gf.Q[t];
             g1 = (double)tmp * (double)tmp;
         }

@@ -37,6 +37,7 @@ struct GapFusion {
     const float* u = nullptr;
     const float* Q = nullptr;
     double* partials = nullptr;  // [2][slice_grid(N*L)]
+    const float* su = nullptr;   // clique conditional gradient (lp_sp), or none
 };
 
 // Packed ordered-filter bin indices of rescale(Q) (min / max at qminmax[0..1]).

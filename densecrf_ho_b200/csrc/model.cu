@@ -119,6 +119,12 @@ void Model::set_cliques(int R_, const int* off, const int* idx, const float* exp
         packed[R + 1 + r] = order[r];
         packed[2 * R + 1 + r] = off[order[r] + 1] - off[order[r]];
     }
+    // bucket starts over the by-size order: cliques of size s are [bs[s], bs[s+1])
+    std::vector<int> bs((size_t)clique_max + 2, 0);
+    for (int r = 0; r < R; r++) bs[packed[2 * R + 1 + r] + 1]++;
+    for (size_t s = 1; s < bs.size(); s++) bs[s] += bs[s - 1];
+    int* dbs = cl_bstart.ensure(bs.size());
+    DCRF_CUDA(cudaMemcpyAsync(dbs, bs.data(), sizeof(int) * bs.size(), cudaMemcpyHostToDevice, stream));
     int* doff = cl_off.ensure(packed.size());
     DCRF_CUDA(cudaMemcpyAsync(doff, packed.data(), sizeof(int) * packed.size(), cudaMemcpyHostToDevice, stream));
     int* didx = cl_idx.ensure(std::max(clique_total, 1));

@@ -50,6 +50,7 @@ struct Model {
     std::vector<int> h_cl_off, h_cl_idx;
     std::vector<float> h_cl_exp, h_cl_const;
     DevBuf<int> cl_off, cl_idx;
+    DevBuf<int> cl_bstart;  // [max + 2]: in by-size order, the first clique of size >= s
     DevBuf<float> cl_exp, cl_const;
 
     // work buffers
@@ -59,6 +60,8 @@ struct Model {
     DevBuf<int16_t> labels;
     DevBuf<float2> lp_bins;  // ordered-filter bins of rescale(Q), shared by all terms
     DevBuf<int> ipart;
+    DevBuf<double> ho_pre;  // qp_sp: FP64 clique prefixes [2][R][L]
+    DevBuf<int> lp_win;  // lp_sp: per element, the latest clique write claiming it (-1 between calls)
     SolverScalars* h_scal = nullptr;  // pinned mirror
 
     Model(int W_, int H_, int L_);

@@ -16,6 +16,7 @@
 #include <climits>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "model_kernels.cuh"
 
@@ -145,31 +146,65 @@ struct CliqueView {
     const float* ew;  // exp_of_superpixels_
     const float* cst; // constants_
     int R, max_size;
+    const int* bstart;  // [max_size + 2]: cliques (in size order) of size < s start at bstart[s]
 };
+
+// The clique-local prefix chains below walk q = 0 .. max_size-1 with one
+// thread per label; the rows Q[q][*] they read are staged through shared
+// memory kHoChunk at a time by the whole block.
+constexpr int kHoChunk = 128;
+constexpr int kHoThreads = 256;
+
+// The clique-local prefix chains of multiplySuperPixels: pre(lab, s) =
+// sum_{q < s} p(lab, q) with p = Q - 1 (or p as given), one sequential chain
+// per label -- in float (FP32 = 1) as the reference sums it, or in FP64 --
+// recorded at every clique size: out[ptr * L + lab] = pre(lab, size of the
+// ptr-th clique in size order).  Rows of p are staged through shared memory
+// kHoChunk at a time; the bucket starts of the chunk too.
+template <bool FP32>
+__global__ void __launch_bounds__(kHoThreads)
+    ho_prefix_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one,
+                     typename std::conditional<FP32, float, double>::type* __restrict__ out,
+                     const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
+    using T = typename std::conditional<FP32, float, double>::type;
+    if (sc && skip_on_zero_step && sc->zero_step) return;
+    __shared__ float rows[kHoChunk * kLMax];
+    __shared__ int bs[kHoChunk + 1];
+    const int lab = threadIdx.x;
+    if (lab < L)
+        for (int ptr = 0; ptr < cv.bstart[1]; ptr++) out[(long)ptr * L + lab] = T(0);  // empty cliques
+    T s = T(0);
+    for (int c0 = 0; c0 < cv.max_size; c0 += kHoChunk) {
+        const int nq = min(kHoChunk, cv.max_size - c0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < nq * L; e += blockDim.x) rows[e] = p[(long)c0 * L + e];
+        for (int e = threadIdx.x; e <= nq; e += blockDim.x) bs[e] = cv.bstart[c0 + 1 + e];
+        __syncthreads();
+        if (lab < L)
+            for (int qq = 0; qq < nq; qq++) {
+                float x = rows[qq * L + lab];
+                if (minus_one) x = fsub(x, 1.0f);
+                if constexpr (FP32) s = fadd(s, x);
+                else s += (double)x;
+                for (int ptr = bs[qq]; ptr < bs[qq + 1]; ptr++) out[(long)ptr * L + lab] = s;
+            }
+    }
+}
 
 // multiplySuperPixels(p [L x N]) with p = Q - 1 (src/densecrf.cpp:81-88): the
 // reference sums p(lab, 0..size_r-1) -- the clique-LOCAL index -- so every
-// clique's value is a prefix of one sequential chain per label.  Then
+// clique's value is a prefix of one chain per label (ho_prefix_kernel).  Then
 //   mode 0: grad_z = (1 + res) o c           (:373-374)
 //   mode 1: grad_z = 1 o c + res o c         (:432)
-__global__ void ho_regions_kernel(CliqueView cv, int L, const float* __restrict__ Q, float* __restrict__ gz,
+__global__ void ho_regions_kernel(CliqueView cv, int L, const float* __restrict__ pre, float* __restrict__ gz,
                                   int mode, const SolverScalars* __restrict__ sc) {
     if (sc && sc->zero_step) return;
-    const int lab = threadIdx.x;
-    if (lab >= L) return;
-    int ptr = 0;
-    float s = 0.0f;
-    auto emit = [&](float val) {
-        const int r = cv.order[ptr];
-        const float c = cv.ew[r];
-        gz[(long)r * L + lab] = mode == 0 ? fmul(fadd(1.0f, val), c) : fadd(fmul(1.0f, c), fmul(val, c));
-        ptr++;
-    };
-    while (ptr < cv.R && cv.sizes[ptr] == 0) emit(0.0f);
-    for (int q = 0; q < cv.max_size && ptr < cv.R; q++) {
-        s = fadd(s, fsub(Q[(long)q * L + lab], 1.0f));
-        while (ptr < cv.R && cv.sizes[ptr] == q + 1) emit(s);
-    }
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)cv.R * L) return;
+    const int ptr = (int)(t / L), lab = (int)(t - (long)ptr * L);
+    const int r = cv.order[ptr];
+    const float c = cv.ew[r], val = pre[t];
+    gz[(long)r * L + lab] = mode == 0 ? fmul(fadd(1.0f, val), c) : fadd(fmul(1.0f, c), fmul(val, c));
 }
 
 // Small (label, clique) algebra of one Frank-Wolfe iteration.  One thread
@@ -189,40 +224,31 @@ __global__ void ho_direction_kernel(CliqueView cv, int L, const float* __restric
         t1[e] = fmul(sv, c);
         t2[e] = fmul(fsub(czv, 1.0f), c);
     }
-    __syncthreads();
-    if (threadIdx.x == 0) sc->sums[5] = (double)eig_sum_rt(sxz, n, 0);
 }
 
 // float multiplySuperPixels(p1 [L x R], p2 [L x N]) (src/densecrf.cpp:58-72):
 // sum_r sum_{q < size_r} sum_lab p1(lab, r) p2(lab, q), clique-local q again.
-// Evaluated in FP64 as sum_lab sum_r p1(lab, r) * prefix_lab(size_r), then
-// rounded to float.  p2 = Q - 1 (minus_one) or p2 as given.
-__global__ void ho_scalar_kernel(CliqueView cv, int L, const float* __restrict__ p1, const float* __restrict__ p2,
-                                 int minus_one, int slot, SolverScalars* sc, int add_to_slot) {
+// Evaluated in FP64 as sum_lab sum_r p1(lab, r) * prefix_lab(size_r), the r
+// in size order, then rounded to float; the FP64 prefixes come from
+// ho_prefix_kernel<false>.  One thread per label; its loads do not depend on
+// its sum, so they run ahead of it.
+__global__ void ho_scalar_kernel(CliqueView cv, int L, const float* __restrict__ p1, const double* __restrict__ pre,
+                                 int slot, SolverScalars* sc, int add_to_slot) {
     if (sc->zero_step && slot != 8) return;
     __shared__ double part[kLMax];
     const int lab = threadIdx.x;
     double acc = 0.0;
     if (lab < L) {
-        int ptr = 0;
-        double pre = 0.0;
-        while (ptr < cv.R && cv.sizes[ptr] == 0) ptr++;
-        for (int q = 0; q < cv.max_size && ptr < cv.R; q++) {
-            float x = p2[(long)q * L + lab];
-            if (minus_one) x = fsub(x, 1.0f);
-            pre += (double)x;
-            while (ptr < cv.R && cv.sizes[ptr] == q + 1) {
-                acc += (double)p1[(long)cv.order[ptr] * L + lab] * pre;
-                ptr++;
-            }
-        }
+#pragma unroll 4
+        for (int ptr = cv.bstart[1]; ptr < cv.R; ptr++)
+            acc += (double)p1[(long)cv.order[ptr] * L + lab] * pre[(long)ptr * L + lab];
     }
     if (threadIdx.x < kLMax) part[threadIdx.x] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
-        double s = 0.0;
-        for (int k = 0; k < L; k++) s += part[k];
-        const float f = (float)s;
+        double t = 0.0;
+        for (int k = 0; k < L; k++) t += part[k];
+        const float f = (float)t;
         if (add_to_slot) sc->sums[slot] = (double)fadd((float)sc->sums[slot], f);
         else sc->sums[slot] = (double)f;
     }
@@ -260,8 +286,51 @@ __global__ void ho_zterm_prep_kernel(CliqueView cv, int L, const float* __restri
         zc[e] = fmul(z[e], c);
         omz[e] = fmul(fsub(1.0f, z[e]), c);
     }
+}
+
+// sc->sums[slot] = VectorXf sum of x[0..n) in Eigen's order (eig_sum_rt with
+// an aligned start): the eight packet lanes are eight independent chains,
+// run here by eight threads over shared-memory chunks of the vector, and
+// combined in the reference's order.  skip: the QP step's zero_step rule of
+// the kernel that produced x.
+__global__ void __launch_bounds__(kHoThreads)
+    eig_sum_kernel(const float* __restrict__ x, int n, int slot, SolverScalars* sc, int skip) {
+    if ((skip == 1 && sc->zero_step) || (skip == 2 && sc->zero_step && sc->steps > 0)) return;
+    constexpr int kC = 2048;  // chunk, a multiple of 8
+    __shared__ float buf[kC];
+    __shared__ float lanes[8];
+    const int asz = (n / 4) * 4, asz2 = (n / 8) * 8;
+    if (asz <= 4) {  // no paired-packet loop: the sequential routine
+        if (threadIdx.x == 0) sc->sums[slot] = (double)eig_sum_rt(x, n, 0);
+        return;
+    }
+    const int l = threadIdx.x;
+    float acc = 0.0f;
+    for (int c0 = 0; c0 < asz2; c0 += kC) {
+        const int m = min(kC, asz2 - c0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < m; e += blockDim.x) buf[e] = x[c0 + e];
+        __syncthreads();
+        if (l < 8) {
+            int i = l;
+            if (c0 == 0) {
+                acc = buf[l];  // p0 = x[0..3], p1 = x[4..7]
+                i += 8;
+            }
+            for (; i < m; i += 8) acc = fadd(acc, buf[i]);
+        }
+    }
+    if (l < 8) lanes[l] = acc;
     __syncthreads();
-    if (threadIdx.x == 0) sc->sums[8] = (double)eig_sum_rt(zc, n, 0);
+    if (threadIdx.x == 0) {
+        float p0[4];
+        for (int k = 0; k < 4; k++) p0[k] = fadd(lanes[k], lanes[4 + k]);
+        if (asz > asz2)
+            for (int k = 0; k < 4; k++) p0[k] = fadd(p0[k], x[asz2 + k]);
+        float r = fadd(fadd(p0[0], p0[2]), fadd(p0[1], p0[3]));
+        for (int i = asz; i < n; i++) r = fadd(r, x[i]);
+        sc->sums[slot] = (double)r;
+    }
 }
 
 __global__ void fill_float_kernel(long n, float v, float* x) {
@@ -820,93 +889,158 @@ __device__ __forceinline__ int trunc_x86(float q) {
     return fabsf(q) < 2147483648.0f ? (int)q : INT_MIN;
 }
 
-template <bool IS_MIN>
-__device__ __forceinline__ int block_excl_scan_minmax(int v, int* sm, int* total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int ident = IS_MIN ? INT_MAX : INT_MIN;
-    int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int y = __shfl_up_sync(kFullMask, x, o);
-        if (lane >= o) x = IS_MIN ? min(x, y) : max(x, y);
-    }
-    int ex = __shfl_up_sync(kFullMask, x, 1);
-    if (lane == 0) ex = ident;
-    if (lane == 31) sm[w] = x;
-    __syncthreads();
-    int pre = ident, tot = ident;
-    for (int ww = 0; ww < nw; ww++) {
-        if (ww < w) pre = IS_MIN ? min(pre, sm[ww]) : max(pre, sm[ww]);
-        tot = IS_MIN ? min(tot, sm[ww]) : max(tot, sm[ww]);
-    }
-    __syncthreads();
-    *total = tot;
-    return IS_MIN ? min(pre, ex) : max(pre, ex);
-}
-
-__device__ __forceinline__ int block_max_int(int v, int* sm) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_down_sync(kFullMask, v, o));
-    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
-    __syncthreads();
-    int r = INT_MIN;
-    for (int w = 0; w < (int)(blockDim.x >> 5); w++) r = max(r, sm[w]);
-    __syncthreads();
-    return r;
-}
-
 // computeUCondGrad (src/densecrf.cpp:803-830) for clique r = blockIdx.x.
 // The reference keeps its running min / max in an int, so position p (in
-// label-major, clique order) updates the min iff Q_p < (float)s where s is
-// the running min of trunc(Q) over the positions before p (it starts at
-// INT_MAX); the LAST such p is selected.  Same for the max.  A block-wide
-// min / max scan gives every position its s.
-__global__ void ucond_kernel(const int* __restrict__ off, const int* __restrict__ idx, int L,
-                             const float* __restrict__ Q, int* __restrict__ pos) {
-    __shared__ int sm[32];
-    const int r = blockIdx.x;
+// label-major, clique order: p = lab * size + j) updates the min iff
+// Q_p < (float)s, where s is the running min of trunc(Q) over the positions
+// before p (it starts at INT_MAX); the LAST such p is selected.  Same for the
+// max.  Each thread takes a contiguous run of positions: pass 1 finds its
+// run's min / max of trunc(Q), one block-wide exclusive scan gives every run
+// its carry-in, and pass 2 replays the run from that carry exactly as the
+// reference's loop does.
+constexpr int kUcondThreads = 1024;
+
+__global__ void __launch_bounds__(kUcondThreads)
+    ucond_kernel(const int* __restrict__ off, const int* __restrict__ idx, int L, const float* __restrict__ Q,
+                 int* __restrict__ pos) {
+    __shared__ int smin[kUcondThreads / 32], smax[kUcondThreads / 32];
+    const int r = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
     const int s0 = off[r], sz = off[r + 1] - s0;
     const long n = (long)L * sz;
-    int carry_min = INT_MAX, carry_max = INT_MIN, last_min = -1, last_max = -1;
-    for (long base = 0; base < n; base += blockDim.x) {
-        const long p = base + threadIdx.x;
-        const bool valid = p < n;
-        float q = 0.0f;
-        int tmin = INT_MAX, tmax = INT_MIN;
-        if (valid) {
-            const int lab = (int)(p / sz), j = (int)(p - (long)lab * sz);
-            q = Q[(long)idx[s0 + j] * L + lab];
-            tmin = tmax = trunc_x86(q);
-        }
-        int tot_min, tot_max;
-        const int bmin = min(carry_min, block_excl_scan_minmax<true>(tmin, sm, &tot_min));
-        const int bmax = max(carry_max, block_excl_scan_minmax<false>(tmax, sm, &tot_max));
-        const int cmin = (valid && q < (float)bmin) ? (int)p : -1;
-        const int cmax = (valid && q > (float)bmax) ? (int)p : -1;
-        last_min = max(last_min, block_max_int(cmin, sm));
-        last_max = max(last_max, block_max_int(cmax, sm));
-        carry_min = min(carry_min, tot_min);
-        carry_max = max(carry_max, tot_max);
+    const long per = (n + kUcondThreads - 1) / kUcondThreads;
+    const long p0 = min((long)t * per, n), p1 = min(p0 + per, n);
+    auto q_at = [&](long p) {
+        const int lab = (int)(p / sz), j = (int)(p - (long)lab * sz);
+        return Q[(long)idx[s0 + j] * L + lab];
+    };
+    int tmin = INT_MAX, tmax = INT_MIN;
+    for (long p = p0; p < p1; p++) {
+        const int v = trunc_x86(q_at(p));
+        tmin = min(tmin, v);
+        tmax = max(tmax, v);
     }
-    if (threadIdx.x == 0) {
+    // exclusive scan of (min, max) over the threads' runs, in thread order
+    int xmin = tmin, xmax = tmax;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int ymin = __shfl_up_sync(kFullMask, xmin, o), ymax = __shfl_up_sync(kFullMask, xmax, o);
+        if (lane >= o) {
+            xmin = min(xmin, ymin);
+            xmax = max(xmax, ymax);
+        }
+    }
+    int emin = __shfl_up_sync(kFullMask, xmin, 1), emax = __shfl_up_sync(kFullMask, xmax, 1);
+    if (lane == 0) {
+        emin = INT_MAX;
+        emax = INT_MIN;
+    }
+    if (lane == 31) {
+        smin[w] = xmin;
+        smax[w] = xmax;
+    }
+    __syncthreads();
+    for (int ww = 0; ww < w; ww++) {
+        emin = min(emin, smin[ww]);
+        emax = max(emax, smax[ww]);
+    }
+    int cmin = -1, cmax = -1;
+    for (long p = p0; p < p1; p++) {
+        const float q = q_at(p);
+        if (q < (float)emin) cmin = (int)p;
+        if (q > (float)emax) cmax = (int)p;
+        const int v = trunc_x86(q);
+        emin = min(emin, v);
+        emax = max(emax, v);
+    }
+    // the last selected position: block max
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        cmin = max(cmin, __shfl_down_sync(kFullMask, cmin, o));
+        cmax = max(cmax, __shfl_down_sync(kFullMask, cmax, o));
+    }
+    __syncthreads();
+    if (lane == 0) {
+        smin[w] = cmin;
+        smax[w] = cmax;
+    }
+    __syncthreads();
+    if (t == 0) {
+        int lmin = -1, lmax = -1;
+        for (int ww = 0; ww < kUcondThreads / 32; ww++) {
+            lmin = max(lmin, smin[ww]);
+            lmax = max(lmax, smax[ww]);
+        }
         // element index pixel*L + label, or -1 when nothing was selected
-        pos[2 * r] = last_min < 0 ? -1 : idx[s0 + last_min % sz] * L + last_min / sz;
-        pos[2 * r + 1] = last_max < 0 ? -1 : idx[s0 + last_max % sz] * L + last_max / sz;
+        pos[2 * r] = lmin < 0 ? -1 : idx[s0 + lmin % sz] * L + lmin / sz;
+        pos[2 * r + 1] = lmax < 0 ? -1 : idx[s0 + lmax % sz] * L + lmax / sz;
     }
 }
 
-// Writes Us in clique order (later cliques overwrite earlier ones; an
-// unselected side keeps the previous clique's position, as the reference's
-// variables do).
-__global__ void ucond_apply_kernel(int R, const int* __restrict__ pos, const float* __restrict__ cst,
-                                   const float* __restrict__ ew, float* __restrict__ Us) {
-    int mn = 0, mx = 0;
-    for (int r = 0; r < R; r++) {
-        if (pos[2 * r] >= 0) mn = pos[2 * r];
-        if (pos[2 * r + 1] >= 0) mx = pos[2 * r + 1];
-        Us[mn] = fmul(cst[r], ew[r]);
-        Us[mx] = fmul(-cst[r], ew[r]);
+// The reference then writes, clique after clique, Us[min] = c_r w_r and
+// Us[max] = -c_r w_r, where an unselected side keeps the previous clique's
+// position (both start at element 0), and later writes overwrite earlier
+// ones.  Write 2r targets the min position of clique r, write 2r+1 its max.
+// ucond_targets resolves every write's target (a running "last selected"
+// scan over r); ucond_claim keeps, per target, the latest write (atomicMax
+// into win[], which is -1 everywhere between calls); ucond_write lets that
+// write store its value and resets win[].
+__global__ void __launch_bounds__(1024) ucond_targets_kernel(int R, const int* __restrict__ pos,
+                                                             int* __restrict__ tgt) {
+    __shared__ int sl[2][32];
+    __shared__ int carry[2];
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (t < 2) carry[t] = -1;
+    __syncthreads();
+    for (int base = 0; base < R; base += 1024) {
+        const int r = base + t;
+        int last[2];
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            int x = (r < R && pos[2 * r + side] >= 0) ? r : -1;  // inclusive running max of selected r
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(kFullMask, x, o);
+                if (lane >= o) x = max(x, y);
+            }
+            if (lane == 31) sl[side][w] = x;
+            last[side] = x;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int side = 0; side < 2; side++) {
+            int x = max(last[side], carry[side]);
+            for (int ww = 0; ww < w; ww++) x = max(x, sl[side][ww]);
+            last[side] = x;
+        }
+        __syncthreads();
+        if (r < R)
+#pragma unroll
+            for (int side = 0; side < 2; side++)
+                tgt[2 * r + side] = last[side] < 0 ? 0 : pos[2 * last[side] + side];
+        if (t == 1023 || r == R - 1) {
+            carry[0] = last[0];
+            carry[1] = last[1];
+        }
+        __syncthreads();
     }
+}
+
+__global__ void ucond_claim_kernel(int W, const int* __restrict__ tgt, int* __restrict__ win) {
+    const int wi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wi < W) atomicMax(win + tgt[wi], wi);
+}
+
+__global__ void ucond_write_kernel(int W, const int* __restrict__ tgt, const float* __restrict__ cst,
+                                   const float* __restrict__ ew, int* __restrict__ win, float* __restrict__ Us) {
+    const int wi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wi >= W) return;
+    const int e = tgt[wi], r = wi >> 1;
+    if (win[e] == wi) Us[e] = (wi & 1) ? fmul(-cst[r], ew[r]) : fmul(cst[r], ew[r]);
+}
+
+__global__ void ucond_reset_kernel(int W, const int* __restrict__ tgt, int* __restrict__ win) {
+    const int wi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (wi < W) win[tgt[wi]] = -1;
 }
 
 constexpr int kPix = 128;
@@ -932,13 +1066,20 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
     const int tgrid = ceil_div(ceil_div(N, 32), kTileWarps);  // row-tiled kernels
 
     CliqueView cv{};
+    float* pre32 = nullptr;                   // float prefixes of Q - 1 at the clique sizes
+    double *preQ = nullptr, *preS = nullptr;  // FP64 prefixes of Q - 1 and of sx
     float *gz = nullptr, *z = nullptr, *sxz = nullptr, *t1 = nullptr, *t2 = nullptr, *cz = nullptr, *zc = nullptr,
           *omz = nullptr;
     const int LR = L * R;
     if (R > 0) {
         const int* base = cl_off.get();
-        cv = CliqueView{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R, clique_max};
+        cv = CliqueView{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R, clique_max,
+                        cl_bstart.get()};
         float* small = b[14].ensure((size_t)8 * LR);
+        pre32 = b[15].ensure((size_t)LR);
+        double* dpre = ho_pre.ensure((size_t)2 * LR);
+        preQ = dpre;
+        preS = dpre + LR;
         gz = small;
         z = small + LR;
         sxz = small + 2 * LR;
@@ -950,7 +1091,8 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(fill_float_kernel, ceil_div(LR, 256), 256, 0, stream, LR, 1.0f, z);
         ho = buf(4);
         DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
-        launch(ho_regions_kernel, 1, kLMax, 0, stream, cv, L, Q, gz, 0, nullptr);
+        launch(ho_prefix_kernel<true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, nullptr, 0);
+        launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 0, nullptr);
     }
     // grad_y = unary + sum_k 2 A_k Q; energy terms Q . A_k Q (same applies).
     for (int k = 0; k < nt; k++) {
@@ -963,7 +1105,9 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(ho_pixels_kernel, ceil_div((long)clique_max * L, 256), 256, 0, stream, cv, L, z, ho, nullptr);
         launch(add_inplace_kernel, ceil_div(NL, 256), 256, 0, stream, NL, grad, ho);
         launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
-        launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, Q, 1, 8, sc, 1);
+        launch(eig_sum_kernel, 1, kHoThreads, 0, stream, zc, LR, 8, sc, 2);
+        launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, preQ, nullptr, 0);
+        launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, preQ, 8, sc, 1);
     }
     launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, part);
     launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
@@ -986,9 +1130,11 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         });
         if (R > 0) {
             launch(ho_direction_kernel, 1, 256, 0, stream, cv, L, gz, z, sxz, t1, t2, cz, sc);
-            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, Q, 1, 3, sc, 0);    // a
-            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t2, sx, 0, 4, sc, 0);   // b
-            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, sx, 0, 6, sc, 0);   // denom term
+            launch(eig_sum_kernel, 1, kHoThreads, 0, stream, sxz, LR, 5, sc, 0);
+            launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, sx, 0, preS, sc, 0);
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preQ, 3, sc, 0);    // a
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t2, preS, 4, sc, 0);   // b
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preS, 6, sc, 0);   // denom term
         }
         for (int k = 0; k < nt; k++) {
             if (k == 0) apply(k, false, psi, sx, nullptr, 1.0f, true);
@@ -1004,9 +1150,12 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(qp_update_kernel, kRedBlocks, kRedThreads, 0, stream, NL, sx, psi, ho, unary.get(), Q, grad, sc, part);
         launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 7, sc);
         if (R > 0) {
-            launch(ho_regions_kernel, 1, kLMax, 0, stream, cv, L, Q, gz, 1, sc);
+            launch(ho_prefix_kernel<true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, sc, 1);
+            launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 1, sc);
             launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
-            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, Q, 1, 8, sc, 1);
+            launch(eig_sum_kernel, 1, kHoThreads, 0, stream, zc, LR, 8, sc, 2);
+            launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, preQ, nullptr, 0);
+            launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, preQ, 8, sc, 1);
         }
         launch(qp_energy_kernel, 1, 1, 0, stream, sc, max_iter);
         DCRF_LAUNCH_CHECK();
@@ -1067,8 +1216,13 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     int* upos = nullptr;
     if (R > 0) {
         const int* base = cl_off.get();
-        cv = CliqueView{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R, clique_max};
-        upos = ipart.ensure(2 * (size_t)R);
+        cv = CliqueView{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R, clique_max,
+                        cl_bstart.get()};
+        upos = ipart.ensure(4 * (size_t)R);  // [2R] selected positions, [2R] write targets
+        if (!lp_win.get()) {
+            int* w = lp_win.ensure((size_t)N * L);
+            DCRF_CUDA(cudaMemsetAsync(w, 0xff, sizeof(int) * (size_t)N * L, stream));  // -1: no claim
+        }
     }
 
     int it = 0, count = 0, fw_total = 0, gamma_total = 0;
@@ -1135,18 +1289,27 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
                 }
             });
             rescaled_bins(bins, Q, NL, &sc->qmin, stream);
-            // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; with
-            // no cliques the dual-gap sums ride along the last term's slice.
-            const bool fuse_gap = R == 0 && nt > 0;
-            GapFusion gf{alpha, u, Q, part};
+            // Clique conditional gradient su (computeUCondGrad), before the
+            // ordered filters so that the dual-gap sums can ride along the
+            // last term's slice with su included.
+            if (R > 0) {
+                const int nw = 2 * R;
+                int* tgt = upos + 2 * R;
+                DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
+                launch(ucond_kernel, R, kUcondThreads, 0, stream, cl_off.get(), cl_idx.get(), L, Q, upos);
+                launch(ucond_targets_kernel, 1, 1024, 0, stream, R, upos, tgt);
+                launch(ucond_claim_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
+                launch(ucond_write_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, cl_const.get(), cl_exp.get(),
+                       lp_win.get(), su);
+                launch(ucond_reset_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
+            }
+            // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; the
+            // dual-gap sums ride along the last term's slice.
+            const bool fuse_gap = nt > 0;
+            GapFusion gf{alpha, u, Q, part, R > 0 ? su : nullptr};
             for (int k = 0; k < nt; k++)
                 apply_ord_bins(k, sa, bins, k == 0 ? nullptr : sa, k == 0, fuse_gap && k == nt - 1 ? &gf : nullptr);
             if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));
-            if (R > 0) {
-                DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
-                launch(ucond_kernel, R, 256, 0, stream, cl_off.get(), cl_idx.get(), L, Q, upos);
-                launch(ucond_apply_kernel, 1, 1, 0, stream, R, upos, cl_const.get(), cl_exp.get(), su);
-            }
             if (fuse_gap) {
                 launch(finalize_large_kernel, 2, 1024, 0, stream, part, slice_grid(NL), 0, sc);
             } else {

@@ -128,3 +128,35 @@ def test_lp_full_size_bit_exact_to_reference(oracle_mod):
     assert st.iterations == rec["prox_iters"]
     assert hashlib.sha256(out.tobytes()).hexdigest() == rec["q_sha256"]
     assert m.assignment_energy_true(m.currentMap(out)) == pytest.approx(rec["energy_true"], rel=1e-12)
+
+
+def test_many_cliques_vs_oracle(oracle_mod):
+    """1500 small overlapping cliques (more than one 1024-clique chunk of the
+    clique-gradient write resolution), heavy weights: qp_sp bit-exact and
+    lp_sp within the LP tolerances of the oracle."""
+    W, H = 36, 28
+    img = synth.make_image(W, H, 21, 5)
+    rng = np.random.default_rng(9)
+    sizes = rng.integers(2, 7, 1500)
+    idx = np.concatenate([rng.choice(W * H, s, replace=False) for s in sizes]).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    ew = rng.uniform(1.0, 30.0, 1500).astype(np.float32)
+    cs = np.full(1500, 50.0, np.float32)
+    orc = oracle_mod.build_model(oracle_mod.OracleModel, img)
+    orc.set_cliques(off, idx, ew, cs)
+    m = DenseCRF2D(W, H, 21)
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    m.setCliques(off, idx, ew, cs)
+    Q = orc.unary_init()
+    a, st = m.qp_inference_super_pixels_non_convex(Q, max_iter=20, stats=True)
+    b, it, en = orc.qp(Q, 20)
+    assert st.iterations == it
+    assert _eq(a, b)
+    a = m.lp_inference_prox_super_pixels(Q, prox_max_iter=3, fw_max_iter=5)
+    b, _ = orc.lp(Q, prox_max_iter=3, fw_max_iter=5)
+    la, lb = m.currentMap(a), orc.current_map(b)
+    assert (la == lb).mean() >= 0.999
+    ea, eb = orc.energy_ho(la), orc.energy_ho(lb)
+    assert abs(ea - eb) <= ENERGY_RTOL * abs(eb)
