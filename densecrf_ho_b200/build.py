@@ -83,24 +83,31 @@ def build(force: bool = False, verbose: bool = False) -> str:
 
 SHIM_DIR = os.path.join(PKG, "cpp")
 SHIM_BIN = os.path.join(SHIM_DIR, "shim_selftest")
+CLI_BIN = os.path.join(SHIM_DIR, "example_inference")
 
 
-def build_shim(eigen_include: str) -> str:
-    """Compiles the drop-in C++ API self-test (densecrf_ho_b200/cpp) with g++
-    against `eigen_include` (a directory holding Eigen/Core, e.g. the one the
-    reference vendors) and libdcrf_cuda.so."""
+def _build_cpp(src_name: str, out: str, eigen_include: str) -> str:
     lib = build()
-    src = os.path.join(SHIM_DIR, "shim_selftest.cpp")
+    src = os.path.join(SHIM_DIR, src_name)
     deps = [src] + glob.glob(os.path.join(SHIM_DIR, "*.h")) + [lib]
-    if os.path.exists(SHIM_BIN) and all(os.path.getmtime(p) <= os.path.getmtime(SHIM_BIN) for p in deps):
-        return SHIM_BIN
+    if os.path.exists(out) and all(os.path.getmtime(p) <= os.path.getmtime(out) for p in deps):
+        return out
     cmd = ["g++", "-std=c++14", "-O2", "-w", "-I", INCLUDE, "-I", SHIM_DIR, "-I", eigen_include,
-           "-I", "/usr/local/cuda/include", src, "-o", SHIM_BIN, "-L", PKG, "-ldcrf_cuda",
+           "-I", "/usr/local/cuda/include", src, "-o", out, "-L", PKG, "-ldcrf_cuda",
            "-Wl,-rpath,$ORIGIN/.."]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
-        raise RuntimeError(f"shim build failed:\n{r.stderr}")
-    return SHIM_BIN
+        raise RuntimeError(f"{src_name} build failed:\n{r.stderr}")
+    return out
+
+
+def build_shim(eigen_include: str) -> str:
+    """Compiles the drop-in C++ API self-test and the headless example program
+    (densecrf_ho_b200/cpp) with g++ against `eigen_include` (a directory
+    holding Eigen/Core, e.g. the one the reference vendors) and
+    libdcrf_cuda.so."""
+    _build_cpp("example_inference.cpp", CLI_BIN, eigen_include)
+    return _build_cpp("shim_selftest.cpp", SHIM_BIN, eigen_include)
 
 
 if __name__ == "__main__":

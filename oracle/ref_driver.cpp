@@ -18,6 +18,10 @@
 #include <limits>
 
 #include "densecrf.h"
+#include "probimage.h"
+
+#include <cmath>
+#include <netinet/in.h>
 #include "eigen_utils.hpp"
 #include "permutohedral.h"
 #include "qp.hpp"
@@ -306,6 +310,46 @@ double refm_lr_qp_value(void* h, const float* Q) {
     RefModel* m = (RefModel*)h;
     MatrixXf I = Map<const MatrixXf>(Q, m->L(), m->N());
     return m->compute_LR_QP_value(I, MatrixXf::Zero(m->L(), m->N()));
+}
+
+// ---- ProbImage (.c_unary) codec ------------------------------------------
+// ref_probimage_compress: ProbImage::compress of a [H][W][D] float image
+// (external/ProbImage/probimage.cpp:87-139).
+int ref_probimage_compress(int W, int H, int D, const float* data, float eps, const char* path) {
+    ProbImage p;
+    FILE* fp = fopen(path, "wb");  // the codec only writes via its own save path: stage through a raw file
+    if (!fp) return 1;
+    uint32_t hdr[3] = {htonl((uint32_t)W), htonl((uint32_t)H), htonl((uint32_t)D)};
+    fwrite(hdr, 4, 3, fp);
+    std::vector<uint32_t> buf((size_t)W * H * D);
+    for (size_t i = 0; i < buf.size(); i++) {
+        uint32_t u;
+        std::memcpy(&u, data + i, 4);
+        buf[i] = htonl(u);
+    }
+    fwrite(buf.data(), 4, buf.size(), fp);
+    fclose(fp);
+    p.load(path);
+    p.compress(path, eps);
+    return 0;
+}
+// The unaries load_unary derives from a .c_unary file (src/file_storage.cpp:
+// 261-285): decompress, boostToProb, then -log per (pixel, label); out is
+// [N][D] (pixel = y * W + x).  Returns W, H, D through the pointers; out may
+// be NULL to query the size.
+int ref_load_unary(const char* path, float* out, int* W, int* H, int* D) {
+    ProbImage t;
+    t.decompress(path);
+    t.boostToProb();
+    *W = t.width();
+    *H = t.height();
+    *D = t.depth();
+    if (out)
+        for (int i = 0; i < t.height(); i++)
+            for (int j = 0; j < t.width(); j++)
+                for (int k = 0; k < t.depth(); k++)
+                    out[((size_t)i * t.width() + j) * t.depth() + k] = -log(t(j, i, k));
+    return 0;
 }
 
 }  // extern "C"
