@@ -67,6 +67,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--only-roofline", action="store_true",
                     help="time only the ordered and plain lattice filters (a short command for ncu)")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the extra workloads (QP, qp_sp / lp_sp, batch, adjoint): a short command for ncu")
     ap.add_argument("--only-batch", action="store_true",
                     help="time only qp_sp / lp_sp, the 64-image batched QP and the 16-image mean-field adjoint")
     ap.add_argument("--prox-iters", type=int, default=50,
@@ -719,7 +721,7 @@ def run_ours(args):
                       "lattice_filter_gpix_label_s": {k: v["filter_gpix_label_s"] for k, v in roof.items()},
                       "lattice_filter_gbs": {k: v["filter_gbs"] for k, v in roof.items()},
                       "ord_filter_ms": {k: v["seconds"] * 1e3 for k, v in roof.items()}}}
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not args.no_extra:
         line["extra"]["qp_320x240"] = measure_qp(cpu=not args.no_cpu_baseline)
         line["extra"]["ho_640x480"] = measure_ho(cpu=not args.no_cpu_baseline)
         line["extra"]["batch_qp_64"] = measure_batch()
