@@ -78,6 +78,16 @@ class Permutohedral:
                                              x.ctypes.data_as(C.c_void_p), x.shape[1]))
         return out
 
+    def gradient(self, a, b):
+        """``df [N, d]`` = d(a^T K b) / d(features) (``Permutohedral::gradient``)."""
+        a, b = _f32(a), _f32(b)
+        if a.ndim == 1:
+            a, b = a.reshape(-1, 1), b.reshape(-1, 1)
+        df = np.empty((self.N, self.d), np.float32)
+        check(lib().dcrf_lattice_gradient(self._h, df.ctypes.data_as(C.c_void_p), a.ctypes.data_as(C.c_void_p),
+                                          b.ctypes.data_as(C.c_void_p), a.shape[1]))
+        return df
+
     def export(self):
         d1, N, M, d = self.d + 1, self.N, self.M, self.d
         off = np.empty(N * d1, np.int32)

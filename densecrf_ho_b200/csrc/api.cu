@@ -201,6 +201,34 @@ dcrf_status dcrf_lattice_compute(dcrf_lattice h, float* out, const float* in, in
     });
 }
 
+dcrf_status dcrf_lattice_gradient_dev(dcrf_lattice h, float* d_df, const float* d_a, const float* d_b, int L) {
+    return guard([&] {
+        need(h, "lattice");
+        need(d_df, "df");
+        need(d_a, "a");
+        need(d_b, "b");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        h->lat.gradient(d_df, d_a, d_b, L);
+    });
+}
+
+dcrf_status dcrf_lattice_gradient(dcrf_lattice h, float* df, const float* a, const float* b, int L) {
+    return guard([&] {
+        need(h, "lattice");
+        need(df, "df");
+        need(a, "a");
+        need(b, "b");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        if (L < 1) throw Error(DCRF_E_ARG, "L must be >= 1");
+        const size_t n = (size_t)L * h->lat.N;
+        float* da = upload(h->in, a, n, h->stream);
+        float* db = upload(h->feat, b, n, h->stream);
+        float* ddf = h->out.ensure((size_t)h->lat.N * h->lat.d);
+        h->lat.gradient(ddf, da, db, L);
+        download(df, ddf, (size_t)h->lat.N * h->lat.d, h->stream);
+    });
+}
+
 dcrf_status dcrf_lattice_compute_ord_dev(dcrf_lattice h, float* d_out, const float* d_Q, int L) {
     return guard([&] {
         need(h, "lattice");

@@ -1024,6 +1024,108 @@ void build_impl(Lattice& L, const float* d_features) {
 
 }  // namespace
 
+namespace {
+
+// ----------------------------------------------------- feature gradient --
+// Permutohedral::gradient (src/permutohedral.cpp:1095-1178): df [N][d] of
+// a^T K b with respect to the (scaled) features.  For each direction the
+// host splats one side, blurs with the double-evaluated 1/2 weights in axis
+// order (reversed for the second direction), and this kernel forms the
+// slice-side derivative per pixel in the reference's float order: for each
+// label k, r_j = (0 + alpha v(o0_j)) - alpha v(o1_j) with o0/o1 from the
+// pixel's ranks, then for j = 1..d, grad_j += x_k * sf_{j-1} (s - j r_j),
+// s += r_j, s starting at r_0; finally df += grad.
+struct GradScale {
+    float s[16];
+};
+
+template <int DM>
+__global__ void grad_slice_kernel(int N, int L, int d, const int* __restrict__ offset, const int* __restrict__ rank,
+                                  const float* __restrict__ vals, const float* __restrict__ x, float alpha,
+                                  GradScale sf, float* __restrict__ df) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int d1 = d + 1;
+    int o0[DM + 1], o1[DM + 1];
+#pragma unroll
+    for (int j = 0; j <= DM; j++)
+        if (j <= d) {
+            const int r0 = d - rank[(long)i * d1 + j];
+            const int r1 = r0 + 1 > d ? 0 : r0 + 1;
+            o0[j] = offset[(long)i * d1 + r0] + 1;
+            o1[j] = offset[(long)i * d1 + r1] + 1;
+        }
+    float grad[DM];
+#pragma unroll
+    for (int j = 0; j < DM; j++) grad[j] = 0.0f;
+    for (int k = 0; k < L; k++) {
+        float ra[DM + 1];
+#pragma unroll
+        for (int j = 0; j <= DM; j++)
+            if (j <= d)
+                ra[j] = fsub(fadd(0.0f, fmul(alpha, vals[(long)o0[j] * L + k])), fmul(alpha, vals[(long)o1[j] * L + k]));
+        const float xk = x[(long)i * L + k];
+        float sm = ra[0];
+#pragma unroll
+        for (int j = 1; j <= DM; j++)
+            if (j <= d) {
+                const float v = fmul(sf.s[j - 1], fsub(sm, fmul((float)j, ra[j])));
+                grad[j - 1] = fadd(grad[j - 1], fmul(xk, v));
+                sm = fadd(sm, ra[j]);
+            }
+    }
+#pragma unroll
+    for (int j = 0; j < DM; j++)
+        if (j < d) df[(long)i * d + j] = fadd(df[(long)i * d + j], grad[j]);
+}
+
+template <int DM>
+void gradient_impl(Lattice& lat, float* df, const float* a, const float* b, int L) {
+    cudaStream_t st = lat.stream;
+    const int N = lat.N, d = lat.d, M = lat.M;
+    lat.ensure_values((size_t)L);
+    DCRF_CUDA(cudaMemsetAsync(df, 0, sizeof(float) * (size_t)N * d, st));
+    // scale_factor and alpha as the reference computes them (:1104-1111)
+    GradScale sf{};
+    const float inv_std_dev = std::sqrt(2.0 / 3.0) * (d + 1);
+    for (int i = 0; i < d; i++) sf.s[i] = 1.0 / std::sqrt(double((i + 2) * (i + 1))) * inv_std_dev;
+    const float alpha = 1.0f / (1 + std::pow(2.0f, (float)-d)) / (d + 1);
+    const int n_short = M - lat.n_long;
+    const long ML = (long)M * L, SL = (long)n_short * L;
+    for (int dir = 0; dir < 2; dir++) {
+        const float* in = dir ? b : a;
+        float *src = lat.va.get(), *dst = lat.vb.get();
+        if (lat.n_long)
+            launch(splat_kernel<false>, ceil_div(lat.n_long, kStageWarps), 32 * kStageWarps, 0, st, lat.n_long, L,
+                   lat.vorder.get(), lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in, nullptr, src,
+                   Skip{});
+        if (n_short)
+            launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L,
+                   lat.vorder.get() + lat.n_long, lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in,
+                   nullptr, src, Skip{});
+        for (int jj = 0; jj <= d; jj++) {
+            const int j = dir ? d - jj : jj;
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, lat.nbr.get() + (long)j * M, src, dst,
+                   Skip{});
+            std::swap(src, dst);
+        }
+        launch(grad_slice_kernel<DM>, ceil_div(N, 128), 128, 0, st, N, L, d, lat.offset.get(), lat.rank.get(), src,
+               dir ? a : b, alpha, sf, df);
+    }
+    DCRF_LAUNCH_CHECK();
+}
+
+}  // namespace
+
+void Lattice::gradient(float* df, const float* a, const float* b, int L) {
+    require(L >= 1, DCRF_E_ARG, "gradient: L must be >= 1");
+    require(!concatenated, DCRF_E_STATE, "gradient: not available on a concatenated lattice");
+    if (d <= 2) gradient_impl<2>(*this, df, a, b, L);
+    else if (d <= 5) gradient_impl<5>(*this, df, a, b, L);
+    else if (d <= 8) gradient_impl<8>(*this, df, a, b, L);
+    else gradient_impl<16>(*this, df, a, b, L);
+}
+
 // ------------------------------------------------------ concatenation --
 // Several images' lattices as one: vertex, pixel and entry ids of part i are
 // shifted by the parts before it, so one filter launch sequence runs every

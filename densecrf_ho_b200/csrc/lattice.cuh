@@ -88,6 +88,9 @@ struct Lattice {
     // The same from precomputed packed bins (lower | upper << 8 per element).
     void compute_ord_bins(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
 
+    // Permutohedral::gradient: df [N][d] = d(a^T K b)/d(features); a, b [N][L].
+    void gradient(float* df, const float* a, const float* b, int L);
+
     void ensure_values(size_t row_width);
 };
 

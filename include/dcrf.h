@@ -89,6 +89,12 @@ dcrf_status dcrf_lattice_compute_noalloc(dcrf_lattice lat, float* d_out, const f
  * (src/permutohedral.cpp:1071-1073, 590-701): the 10-bin ordered filter. */
 dcrf_status dcrf_lattice_compute_ord(dcrf_lattice lat, float* out, const float* Q, int L);
 dcrf_status dcrf_lattice_compute_ord_dev(dcrf_lattice lat, float* d_out, const float* d_Q, int L);
+/* gradient(df, a, b, value_size) (include/permutohedral.h:86-87,
+ * src/permutohedral.cpp:1095-1178): df [N][d] = d(a^T K b)/d(features) for
+ * a, b [N][L], bit-identical to the reference's float evaluation. */
+dcrf_status dcrf_lattice_gradient(dcrf_lattice lat, float* df, const float* a, const float* b, int L);
+dcrf_status dcrf_lattice_gradient_dev(dcrf_lattice lat, float* d_df, const float* d_a, const float* d_b,
+                                      int L);
 /* Read back the lattice tables for parity checks (host buffers, any may be
  * NULL): offset/rank/bary [N*(d+1)] (offset_, rank_, barycentric_), keys
  * [M*d] int16 in vertex-id order, nbr [(d+1)*M*2] = blur_neighbors_ (n1, n2),

@@ -120,6 +120,7 @@ def ref_lib():
         L.refl_export.argtypes = [vp, _i32p, _i32p, _f32p, _i32p]
         L.refl_compute.argtypes = [vp, _f32p, _f32p, C.c_int, C.c_int]
         L.refl_compute_ord.argtypes = [vp, _f32p, _f32p, C.c_int]
+        L.refl_gradient.argtypes = [vp, _f32p, _f32p, _f32p, C.c_int]
         L.refm_new.restype = vp
         L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         L.refm_free.argtypes = [vp]
@@ -218,6 +219,14 @@ class ReferenceLattice(_Lattice):
         nbr = np.empty(max(2 * d1 * M, 1), np.int32)
         self._lib.refl_export(self._h, off, rk, by, nbr)
         return dict(offset=off, rank=rk, bary=by, nbr=nbr[:2 * d1 * M], M=M)
+
+    def gradient(self, a, b):
+        """df [N][d] = d(a^T K b)/d(features) (Permutohedral::gradient)."""
+        a = _c(a, np.float32)
+        b = _c(b, np.float32)
+        df = np.empty((self.N, self.d), np.float32)
+        self._lib.refl_gradient(self._h, df, a, b, a.shape[1])
+        return df
 
 
 class _Model:

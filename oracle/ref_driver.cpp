@@ -186,6 +186,12 @@ void refl_compute(void* h, float* out, const float* in, int L, int reverse) {
     p->compute(O, I, reverse != 0);
     std::memcpy(out, O.data(), sizeof(float) * (size_t)L * p->N());
 }
+// Permutohedral::gradient (src/permutohedral.cpp:1095-1178): df [N][d] of
+// a^T K b with respect to the features; a, b [N][L].
+void refl_gradient(void* h, float* df, const float* a, const float* b, int L) {
+    LatticeProbe* p = (LatticeProbe*)h;
+    p->gradient(df, a, b, L);
+}
 void refl_compute_ord(void* h, float* out, const float* in, int L) {
     LatticeProbe* p = (LatticeProbe*)h;
     MatrixXf I = Map<const MatrixXf>(in, L, p->N());

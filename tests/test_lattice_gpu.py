@@ -138,3 +138,12 @@ def test_full_size_properties(oracle_mod):
     kx, ky, kxy = lat.compute(x), lat.compute(y), lat.compute(2 * x + y)
     assert np.linalg.norm(kxy - (2 * kx + ky)) / np.linalg.norm(kxy) < 1e-6
     assert _eq(lat.compute(x), kx)
+
+
+@pytest.mark.parametrize("name", golden_names("gradient_"))
+def test_feature_gradient_matches_reference(name):
+    """Permutohedral::gradient, bit for bit, against the reference's own
+    values (tests/golden/make_gradient_golden.py)."""
+    g = golden(name)
+    lat = Permutohedral().init(g["f"])
+    assert _eq(lat.gradient(g["a"], g["b"]), g["df"])
