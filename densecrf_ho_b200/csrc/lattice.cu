@@ -1237,6 +1237,24 @@ void Lattice::build(const float* d_features, int d_, int N_) {
     else build_impl<16>(*this, d_features);
 }
 
+void Lattice::ensure_aux() {
+    if (aux) return;
+    int lo = 0, hi = 0;
+    DCRF_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    DCRF_CUDA(cudaStreamCreateWithPriority(&aux, cudaStreamNonBlocking, hi));
+    DCRF_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    DCRF_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+}
+
+Lattice::~Lattice() {
+    if (aux) {
+        cudaStreamSynchronize(aux);
+        cudaEventDestroy(ev_fork);
+        cudaEventDestroy(ev_join);
+        cudaStreamDestroy(aux);
+    }
+}
+
 void Lattice::ensure_values(size_t row_width) {
     size_t need = (size_t)(M + 1) * row_width;
     if (need > va_floats) {
@@ -1339,20 +1357,21 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     float *src = va.get(), *dst = vb.get();
     const int n_short = M - n_long;
     const long SL = (long)n_short * L;
+    const Skip sk{vimg.get(), skip_done};
     if (pre_norm) {
         if (n_long)
             launch(splat_kernel<true>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, Skip{vimg.get(), skip_done});
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
         if (n_short)
             launch(splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, Skip{vimg.get(), skip_done});
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
     } else {
         if (n_long)
             launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{vimg.get(), skip_done});
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
         if (n_short)
             launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{vimg.get(), skip_done});
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
     }
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
@@ -1402,7 +1421,7 @@ void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const Slic
         // shared by blocks of kHugeLabels labels x 10 bins, so that they
         // finish early; the rest take one block per list with the bin split
         // that issues the fewest instructions per entry.
-        auto run = [&](int G, int kb, int first, int count) {
+        auto run = [&](int G, int kb, int first, int count, cudaStream_t rs) {
             if (count <= 0) return;
             const int kblocks = (L + kb - 1) / kb;
             const int threads = ((kb * G + 31) / 32) * 32;
@@ -1414,11 +1433,21 @@ void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const Slic
                                 : ord_splat_block_kernel<1>;
             if (smem > 48 * 1024)  // opt-in size: a per-device function attribute, set on every such call
                 DCRF_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            launch(kern, count * kblocks, threads, smem, st, L, kb, kblocks, vorder.get() + first,
+            launch(kern, count * kblocks, threads, smem, rs, L, kb, kblocks, vorder.get() + first,
                    seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
         };
-        run(10, kHugeLabels, 0, n_huge);
-        run(ord_groups_cheapest(L), L, n_huge, n_long - n_huge);
+        // The very long lists set the length of their kernel while leaving
+        // most SMs idle; they run on a high-priority side stream, forked
+        // after the value buffers are ready and joined before the blur, so
+        // the other splats (disjoint vertex rows) fill those SMs meanwhile.
+        if (n_huge > 0) {
+            ensure_aux();
+            DCRF_CUDA(cudaEventRecord(ev_fork, st));
+            DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
+            run(10, kHugeLabels, 0, n_huge, aux);
+            DCRF_CUDA(cudaEventRecord(ev_join, aux));
+        }
+        run(ord_groups_cheapest(L), L, n_huge, n_long - n_huge, st);
     } else if (n_long) {
         launch(ord_splat_kernel, ceil_div(2L * n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
                vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
@@ -1426,6 +1455,7 @@ void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const Slic
     if (n_short)
         launch(ord_splat_short_kernel, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
                vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
+    if (n_long && L <= kOrdBlockMaxL && n_huge > 0) DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     const int row4 = (int)(row / 4);
     for (int j = 0; j <= d; j++) {
         launch(ord_blur_kernel, ceil_div((long)M * row4, kTB), kTB, 0, st, 

@@ -52,6 +52,9 @@ struct Lattice {
     int n_long = 0;  // vertices whose splat list exceeds the staging threshold
     int n_huge = 0;  // ... and the (leading) ones whose list is very long
     cudaStream_t stream = nullptr;  // borrowed
+    // side stream (highest priority) for splat work that overlaps the rest
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 
     DevBuf<int> offset, rank, seg_start, seg_pix;
     DevBuf<int> vorder, vorder_keys;  // splat visiting order: longest lists first
@@ -92,6 +95,12 @@ struct Lattice {
     void gradient(float* df, const float* a, const float* b, int L);
 
     void ensure_values(size_t row_width);
+    void ensure_aux();
+
+    Lattice() = default;
+    Lattice(const Lattice&) = delete;
+    Lattice& operator=(const Lattice&) = delete;
+    ~Lattice();
 };
 
 }  // namespace dcrf
