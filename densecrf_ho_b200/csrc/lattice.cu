@@ -1358,20 +1358,37 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     const int n_short = M - n_long;
     const long SL = (long)n_short * L;
     const Skip sk{vimg.get(), skip_done};
-    if (pre_norm) {
-        if (n_long)
-            launch(splat_kernel<true>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
-        if (n_short)
+    // As in the ordered filter, the lists longer than kHugeList run on the
+    // high-priority side stream while the others are splatted.
+    const int nh = n_huge;
+    const bool forked = nh > 0;
+    if (forked) {
+        ensure_aux();
+        DCRF_CUDA(cudaEventRecord(ev_fork, st));
+        DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
+    }
+    auto long_range = [&](int first, int count, cudaStream_t ls) {
+        if (count <= 0) return;
+        if (pre_norm)
+            launch(splat_kernel<true>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count, L,
+                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
+        else
+            launch(splat_kernel<false>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count, L,
+                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
+    };
+    long_range(0, nh, forked ? aux : st);
+    long_range(nh, n_long - nh, st);
+    if (n_short) {
+        if (pre_norm)
             launch(splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
                    seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
-    } else {
-        if (n_long)
-            launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
-        if (n_short)
+        else
             launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
                    seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
+    }
+    if (forked) {
+        DCRF_CUDA(cudaEventRecord(ev_join, aux));
+        DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     }
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
