@@ -468,9 +468,10 @@ __global__ void order_key_kernel(int M, const int* __restrict__ counts, int* __r
 
 // One blur pass along one lattice axis: new = old + 1/2 (n1 + n2).  seqCompute
 // evaluates it in double (0.5 is a double literal there, :518).
-template <bool SEQ>
-__global__ void blur_kernel(int M, int L, const int2* __restrict__ nbr,
+template <bool SEQ, int LC = 0>
+__global__ void blur_kernel(int M, int Lrt, const int2* __restrict__ nbr,
                             const float* __restrict__ src, float* __restrict__ dst, Skip sk) {
+    const int L = LC ? LC : Lrt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)M * L) return;
     const int v = (int)(t / L), k = (int)(t - (long)v * L);
@@ -496,16 +497,18 @@ __device__ __forceinline__ float apply_epilogue(float v, long t, int i, const Sl
 
 // Slice: out(i, k) = sum_j (bary_ij * alpha) * value(o_ij, k) (sseCompute,
 // :1046-1051) or sum_j (bary_ij * value) * alpha (seqCompute, :529-534).
-template <bool SEQ>
-__global__ void slice_kernel(int N, int L, int d, const int* __restrict__ offset,
+template <bool SEQ, int DC, int LC>
+__global__ void slice_kernel(int N, int Lrt, int drt, const int* __restrict__ offset,
                              const float* __restrict__ bary, const float* __restrict__ vals,
                              float alpha, float* out, SliceEpilogue ep, Skip sk) {
+    const int L = LC ? LC : Lrt, d = DC ? DC : drt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)N * L) return;
     const int i = (int)(t / L), k = (int)(t - (long)i * L);
     const int d1 = d + 1;
     if (skipped(sk, offset[(long)i * d1])) return;
     float acc = 0.0f;
+#pragma unroll
     for (int j = 0; j <= d; j++) {
         const int o = offset[(long)i * d1 + j];
         const float w = bary[(long)i * d1 + j];
@@ -847,8 +850,10 @@ __global__ void ord_splat_short_kernel(int n_short, int L, const int* __restrict
 }
 
 // Ordered blur: every bin independently, weightedAddSplitArray (:570-578).
-__global__ void ord_blur_kernel(int M, int row4, const int2* __restrict__ nbr,
+template <int R4>  // row width in float4 as a compile-time constant (0 = run-time row4r)
+__global__ void ord_blur_kernel(int M, int row4r, const int2* __restrict__ nbr,
                                 const float4* __restrict__ src, float4* __restrict__ dst) {
+    const int row4 = R4 ? R4 : row4r;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)M * row4) return;
     const int v = (int)(t / row4), c = (int)(t - (long)v * row4);
@@ -869,11 +874,13 @@ __global__ void ord_blur_kernel(int M, int row4, const int2* __restrict__ nbr,
 // gap terms are folded in: tmp = (alpha + u) - (v + su) for the final slice
 // value v, the clique term su (0 without cliques), and per-block sums of
 // tmp.Q and tmp.tmp (src/densecrf.cpp:725-729).
-template <bool GAP>
-__global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ offset,
+// DC / LC: d and L as compile-time constants (0 = run-time drt / Lrt).
+template <bool GAP, int DC, int LC>
+__global__ void ord_slice_kernel(int N, int Lrt, int drt, const int* __restrict__ offset,
                                  const float* __restrict__ bary, const float* __restrict__ vals,
                                  const float2* __restrict__ bins, float alpha, float* out, SliceEpilogue ep,
                                  GapFusion gf) {
+    const int L = LC ? LC : Lrt, d = DC ? DC : drt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     double g0 = 0.0, g1 = 0.0;
     if (t < (long)N * L) {
@@ -882,11 +889,13 @@ __global__ void ord_slice_kernel(int N, int L, int d, const int* __restrict__ of
         const float2 bp = bins[t];
         const int cl = ord_lower_of(bp), cu = ord_upper_of(bp);
         float acc = 0.0f;
+#pragma unroll
         for (int j = 0; j <= d; j++) {
             const int o = offset[(long)i * d1 + j];
             const float w = bary[(long)i * d1 + j];
             acc = fadd(acc, fmul(vals[((long)(o + 1) * kOrdW + cl) * L + k], fmul(-w, alpha)));
         }
+#pragma unroll
         for (int j = 0; j <= d; j++) {
             const int o = offset[(long)i * d1 + j];
             const float w = bary[(long)i * d1 + j];
@@ -1340,10 +1349,10 @@ void Lattice::compute_noalloc(float* out, const float* in, int L, bool reverse) 
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     const SliceEpilogue ep;
     if (seq)
-        launch(slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
+        launch(slice_kernel<true, 0, 0>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
                out, ep, Skip{});
     else
-        launch(slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
+        launch(slice_kernel<false, 0, 0>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
                out, ep, Skip{});
     DCRF_LAUNCH_CHECK();
 }
@@ -1395,17 +1404,21 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
         const int j = reverse ? d - jj : jj;
         if (seq)
             launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
+        else if (L == 21)
+            launch(blur_kernel<false, 21>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
         else
             launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
-    if (seq)
-        launch(slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-                                                              alpha, out, ep, Skip{vimg.get(), skip_done});
-    else
-        launch(slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-                                                               alpha, out, ep, Skip{vimg.get(), skip_done});
+    const Skip sks{vimg.get(), skip_done};
+    auto sl = [&](auto kern) {
+        launch(kern, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha, out, ep, sks);
+    };
+    if (seq) sl(slice_kernel<true, 0, 0>);
+    else if (L == 21 && d == 5) sl(slice_kernel<false, 5, 21>);
+    else if (L == 21 && d == 2) sl(slice_kernel<false, 2, 21>);
+    else sl(slice_kernel<false, 0, 0>);
     DCRF_LAUNCH_CHECK();
 }
 
@@ -1475,18 +1488,25 @@ void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const Slic
     if (n_long && L <= kOrdBlockMaxL && n_huge > 0) DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     const int row4 = (int)(row / 4);
     for (int j = 0; j <= d; j++) {
-        launch(ord_blur_kernel, ceil_div((long)M * row4, kTB), kTB, 0, st, 
-            M, row4, nbr.get() + (long)j * M, reinterpret_cast<const float4*>(src),
-            reinterpret_cast<float4*>(dst));
+        auto kern = row4 == 105 ? ord_blur_kernel<105> : ord_blur_kernel<0>;  // 105 = 20 bins x 21 labels / 4
+        launch(kern, ceil_div((long)M * row4, kTB), kTB, 0, st, M, row4, nbr.get() + (long)j * M,
+               reinterpret_cast<const float4*>(src), reinterpret_cast<float4*>(dst));
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
-    if (gap)
-        launch(ord_slice_kernel<true>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-               bins, alpha, out, ep, *gap);
-    else
-        launch(ord_slice_kernel<false>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-               bins, alpha, out, ep, GapFusion{});
+    const GapFusion gf = gap ? *gap : GapFusion{};
+    auto sl = [&](auto kern) {
+        launch(kern, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, bins, alpha, out, ep, gf);
+    };
+    if (gap) {
+        if (L == 21 && d == 5) sl(ord_slice_kernel<true, 5, 21>);
+        else if (L == 21 && d == 2) sl(ord_slice_kernel<true, 2, 21>);
+        else sl(ord_slice_kernel<true, 0, 0>);
+    } else {
+        if (L == 21 && d == 5) sl(ord_slice_kernel<false, 5, 21>);
+        else if (L == 21 && d == 2) sl(ord_slice_kernel<false, 2, 21>);
+        else sl(ord_slice_kernel<false, 0, 0>);
+    }
     DCRF_LAUNCH_CHECK();
 }
 
