@@ -395,11 +395,12 @@ __device__ __forceinline__ void stream_list(int s0, int s1, int L, int k, bool a
     __syncwarp();
 }
 
-template <bool PRE_NORM>
+template <bool PRE_NORM, int LC = 0>
 __global__ void __launch_bounds__(32 * kStageWarps)
-    splat_kernel(int M, int L, const int* __restrict__ order, const int* __restrict__ seg_start,
+    splat_kernel(int M, int Lrt, const int* __restrict__ order, const int* __restrict__ seg_start,
                  const int* __restrict__ seg_pix, const float* __restrict__ seg_w, const float* __restrict__ in,
                  const float* __restrict__ norm, float* __restrict__ vals, Skip sk) {
+    const int L = LC ? LC : Lrt;
     __shared__ float ring[kStageWarps][kStages][kChunk][32];
     __shared__ float mw[kStageWarps][kStages][kChunk];
     __shared__ float mn[kStageWarps][kStages][kChunk];
@@ -428,11 +429,12 @@ __global__ void __launch_bounds__(32 * kStageWarps)
 
 // Short lists (at most kLongList entries; the tail of `order`): one thread
 // per (vertex, label), the same in-order sum without staging.
-template <bool PRE_NORM>
-__global__ void splat_short_kernel(int n_short, int L, const int* __restrict__ order,
+template <bool PRE_NORM, int LC = 0>
+__global__ void splat_short_kernel(int n_short, int Lrt, const int* __restrict__ order,
                                    const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
                                    const float* __restrict__ seg_w, const float* __restrict__ in,
                                    const float* __restrict__ norm, float* __restrict__ vals, Skip sk) {
+    const int L = LC ? LC : Lrt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n_short * L) return;
     const int u = (int)(t / L), k = (int)(t - (long)u * L);
@@ -820,10 +822,12 @@ __global__ void __launch_bounds__(1024)
 
 // Ordered splat of the short lists: one thread per (vertex, label), both
 // passes, without staging.
-__global__ void ord_splat_short_kernel(int n_short, int L, const int* __restrict__ order,
+template <int LC = 0>
+__global__ void ord_splat_short_kernel(int n_short, int Lrt, const int* __restrict__ order,
                                        const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
                                        const float* __restrict__ seg_w, const float2* __restrict__ bins,
                                        float* __restrict__ vals) {
+    const int L = LC ? LC : Lrt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long)n_short * L) return;
     const int u = (int)(t / L), k = (int)(t - (long)u * L);
@@ -1379,20 +1383,24 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     auto long_range = [&](int first, int count, cudaStream_t ls) {
         if (count <= 0) return;
         if (pre_norm)
-            launch(splat_kernel<true>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count, L,
+            launch(L == 21 ? splat_kernel<true, 21> : splat_kernel<true>, ceil_div(count, kStageWarps),
+                   32 * kStageWarps, 0, ls, count, L,
                    vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
         else
-            launch(splat_kernel<false>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count, L,
+            launch(L == 21 ? splat_kernel<false, 21> : splat_kernel<false>, ceil_div(count, kStageWarps),
+                   32 * kStageWarps, 0, ls, count, L,
                    vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
     };
     long_range(0, nh, forked ? aux : st);
     long_range(nh, n_long - nh, st);
     if (n_short) {
         if (pre_norm)
-            launch(splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
+            launch(L == 21 ? splat_short_kernel<true, 21> : splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st,
+                   n_short, L, vorder.get() + n_long,
                    seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
         else
-            launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long,
+            launch(L == 21 ? splat_short_kernel<false, 21> : splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st,
+                   n_short, L, vorder.get() + n_long,
                    seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
     }
     if (forked) {
@@ -1483,7 +1491,7 @@ void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const Slic
                vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
     }
     if (n_short)
-        launch(ord_splat_short_kernel, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
+        launch(ord_splat_short_kernel<0>, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
                vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), bins, src);
     if (n_long && L <= kOrdBlockMaxL && n_huge > 0) DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     const int row4 = (int)(row / 4);
