@@ -1447,11 +1447,15 @@ int slice_grid(long n) { return ceil_div(n, kTB); }
 
 void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const SliceEpilogue& ep,
                                const GapFusion* gap) {
+    ord_splat_blur(bins, L);
+    ord_slice(out, bins, L, ep, gap);
+}
+
+void Lattice::ord_splat_blur(const float2* bins, int L) {
     require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
     const size_t row = (size_t)L * kOrdW;
     ensure_values(row);
     cudaStream_t st = stream;
-    const long NL = (long)N * L;
     float *src = va.get(), *dst = vb.get();
     const int n_short = M - n_long;
     if (n_long && L <= kOrdBlockMaxL) {
@@ -1501,6 +1505,14 @@ void Lattice::compute_ord_bins(float* out, const float2* bins, int L, const Slic
                reinterpret_cast<const float4*>(src), reinterpret_cast<float4*>(dst));
         std::swap(src, dst);
     }
+    ord_vals = src;
+}
+
+void Lattice::ord_slice(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap) {
+    require(ord_vals, DCRF_E_STATE, "ord_slice: no ord_splat_blur before it");
+    cudaStream_t st = stream;
+    const long NL = (long)N * L;
+    const float* src = ord_vals;
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     const GapFusion gf = gap ? *gap : GapFusion{};
     auto sl = [&](auto kern) {

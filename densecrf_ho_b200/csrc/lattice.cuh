@@ -90,6 +90,11 @@ struct Lattice {
     void compute_ord(float* out, const float* Q, int L, const SliceEpilogue& ep);
     // The same from precomputed packed bins (lower | upper << 8 per element).
     void compute_ord_bins(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
+    // The same in two phases: splat + blur (leaves the vertex values in
+    // ord_vals), then the slice.  Other work may run between them.
+    void ord_splat_blur(const float2* bins, int L);
+    void ord_slice(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
+    const float* ord_vals = nullptr;
 
     // Permutohedral::gradient: df [N][d] = d(a^T K b)/d(features); a, b [N][L].
     void gradient(float* df, const float* a, const float* b, int L);

@@ -72,6 +72,12 @@ Model::Model(int W_, int H_, int L_) : W(W_), H(H_), N(W_ * H_), L(L_) {
 
 Model::~Model() {
     if (stream) cudaStreamSynchronize(stream);
+    if (side) {
+        cudaStreamSynchronize(side);
+        cudaEventDestroy(ev_side_fork);
+        cudaEventDestroy(ev_side_join);
+        cudaStreamDestroy(side);
+    }
     terms.clear();
     if (h_scal) cudaFreeHost(h_scal);
     if (stream) cudaStreamDestroy(stream);
@@ -160,6 +166,47 @@ void Model::apply_ord(int k, float* out, const float* rq, const float* base, boo
     ep.base = base;
     ep.zero_base = zero_base;
     t.lat->compute_ord(out, rq, L, ep);
+}
+
+// sa = sum_k apply_upper_minus_lower_ord_k(rescale(Q)) from shared bins, the
+// sum in term order (sa = 0 + t_0, then sa += t_k) as the reference adds it
+// (src/densecrf.cpp:705-716).  The splat and blur phases of terms 1.. run on
+// a side stream while term 0's run on the model's stream; the slices, which
+// carry the accumulation, then run in term order.  `gap`: the dual-gap sums
+// folded into the last slice.
+void Model::apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap) {
+    const int nt = (int)terms.size();
+    if (nt >= 2) {
+        if (!side) {
+            DCRF_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+            DCRF_CUDA(cudaEventCreateWithFlags(&ev_side_fork, cudaEventDisableTiming));
+            DCRF_CUDA(cudaEventCreateWithFlags(&ev_side_join, cudaEventDisableTiming));
+        }
+        DCRF_CUDA(cudaEventRecord(ev_side_fork, stream));
+        DCRF_CUDA(cudaStreamWaitEvent(side, ev_side_fork, 0));
+        for (int k = 1; k < nt; k++) {
+            Lattice& lat = *terms[k]->lat;
+            lat.stream = side;
+            try {
+                lat.ord_splat_blur(bins, L);
+            } catch (...) {
+                lat.stream = stream;
+                throw;
+            }
+            lat.stream = stream;
+        }
+        DCRF_CUDA(cudaEventRecord(ev_side_join, side));
+    }
+    if (nt >= 1) terms[0]->lat->ord_splat_blur(bins, L);
+    if (nt >= 2) DCRF_CUDA(cudaStreamWaitEvent(stream, ev_side_join, 0));
+    for (int k = 0; k < nt; k++) {
+        SliceEpilogue ep;
+        ep.potts = true;
+        ep.scale = -terms[k]->w;
+        ep.base = k == 0 ? nullptr : sa;
+        ep.zero_base = k == 0;
+        terms[k]->lat->ord_slice(sa, bins, L, ep, k == nt - 1 ? gap : nullptr);
+    }
 }
 
 void Model::apply_ord_bins(int k, float* out, const float2* bins, const float* base, bool zero_base,

@@ -41,6 +41,8 @@ struct SolverScalars {
 struct Model {
     int W = 0, H = 0, N = 0, L = 0, device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // second stream for the other terms' filter work
+    cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
     bool has_unary = false;
     DevBuf<float> unary;
     std::vector<std::unique_ptr<Term>> terms;
@@ -75,6 +77,7 @@ struct Model {
     // out = base + coef * (-w K~ in)  (see SliceEpilogue).
     void apply(int k, bool nonorm, float* out, const float* in, const float* base = nullptr,
                float coef = 1.0f, bool zero_base = false);
+    void apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap);
     void apply_ord_bins(int k, float* out, const float2* bins, const float* base, bool zero_base,
                         const GapFusion* gap);
     void apply_ord(int k, float* out, const float* rq, const float* base = nullptr,

@@ -1307,8 +1307,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             // dual-gap sums ride along the last term's slice.
             const bool fuse_gap = nt > 0;
             GapFusion gf{alpha, u, Q, part, R > 0 ? su : nullptr};
-            for (int k = 0; k < nt; k++)
-                apply_ord_bins(k, sa, bins, k == 0 ? nullptr : sa, k == 0, fuse_gap && k == nt - 1 ? &gf : nullptr);
+            apply_ord_sum(sa, bins, fuse_gap ? &gf : nullptr);
             if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));
             if (fuse_gap) {
                 launch(finalize_large_kernel, 2, 1024, 0, stream, part, slice_grid(NL), 0, sc);
