@@ -334,3 +334,28 @@ class DenseCRF2DBatch:
 
 
 __all__.append("DenseCRF2DBatch")
+
+
+def _pairwise_kernel_gradient(self, k, b, Q):
+    """``pairwise_[k]->kernelGradient(b, Q)``: gradient of the term's diagonal
+    kernel feature scales (d floats)."""
+    bb, qq = self._mat(b), self._mat(Q)
+    out = np.zeros(16, np.float32)
+    d = C.c_int()
+    check(lib().dcrf_model_pairwise_kernel_gradient(self._h, int(k), bb.ctypes.data_as(C.c_void_p),
+                                                    qq.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p),
+                                                    C.byref(d)))
+    return out[:d.value]
+
+
+def _pairwise_gradient(self, k, b, Q):
+    """``pairwise_[k]->gradient(b, Q)``: gradient of the term's Potts weight."""
+    bb, qq = self._mat(b), self._mat(Q)
+    out = np.zeros(1, np.float32)
+    check(lib().dcrf_model_pairwise_gradient(self._h, int(k), bb.ctypes.data_as(C.c_void_p),
+                                             qq.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+DenseCRF2D.pairwise_kernel_gradient = _pairwise_kernel_gradient
+DenseCRF2D.pairwise_gradient = _pairwise_gradient

@@ -604,6 +604,36 @@ dcrf_status dcrf_model_lattice_size(dcrf_model h, int k, int* Mv) {
     });
 }
 
+dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model h, int k, const float* b, const float* Q, float* grad,
+                                                int* d) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(b, "b");
+        need(Q, "Q");
+        need(grad, "grad");
+        const size_t n = (size_t)m.N * m.L;
+        const float* db = upload(h->io0, b, n, m.stream);
+        const float* dq = upload(h->io1, Q, n, m.stream);
+        m.kernel_gradient(k, db, dq, grad);
+        if (d) *d = m.terms[k]->d;
+    });
+}
+
+dcrf_status dcrf_model_pairwise_gradient(dcrf_model h, int k, const float* b, const float* Q, float* grad) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(b, "b");
+        need(Q, "Q");
+        need(grad, "grad");
+        const size_t n = (size_t)m.N * m.L;
+        const float* db = upload(h->io0, b, n, m.stream);
+        const float* dq = upload(h->io1, Q, n, m.stream);
+        *grad = m.weight_gradient(k, db, dq);
+    });
+}
+
 dcrf_status dcrf_model_stream(dcrf_model h, void** stream) {
     return guard([&] {
         auto& m = M(h);

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <vector>
 
 #include "reduce.cuh"
 #include "model_kernels.cuh"
@@ -58,6 +59,68 @@ __global__ void norm_kernel(int N, float* x) {
     if (i < N) x[i] = (float)(1.0 / sqrt(dadd((double)x[i], 1e-20)));
 }
 
+// ---- kernel-parameter gradient (src/pairwise.cpp:90-122, 170-181, 402-407) --
+
+// out(i, l) = in(i, l) * s(i)  (Eigen: M * v.asDiagonal()); s == null: out = c * in.
+__global__ void scale_cols_kernel(long n, int L, const float* __restrict__ in, const float* __restrict__ s, float c,
+                                  float* __restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    out[t] = s ? fmul(in[t], s[t / L]) : fmul(c, in[t]);
+}
+
+// X = (0.5 (a o fb + fa o b)) * n^3 per column (featureGradient, symmetric).
+__global__ void sym_grad_input_kernel(long n, int L, const float* __restrict__ a, const float* __restrict__ fb,
+                                      const float* __restrict__ fa, const float* __restrict__ b,
+                                      const float* __restrict__ nrm, float* __restrict__ X) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float ni = nrm[t / L];
+    const float n3 = fmul(fmul(ni, ni), ni);
+    X[t] = fmul(fmul(fadd(fmul(a[t], fb[t]), fmul(fa[t], b[t])), 0.5f), n3);
+}
+
+// Per feature dimension j: sum_i f(i, j) * (-r(i, j) + g(i, j)), in FP64
+// (block partials, then a fixed-order finish); (f o fg).rowwise().sum().
+__global__ void diag_grad_partial_kernel(int N, int d, const float* __restrict__ f, const float* __restrict__ r,
+                                         const float* __restrict__ g, double* __restrict__ part) {
+    __shared__ double sm[256];
+    const int j = blockIdx.y;
+    double acc = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        const long e = (long)i * d + j;
+        acc += (double)fmul(f[e], fadd(-r[e], g[e]));
+    }
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(long)j * gridDim.x + blockIdx.x] = sm[0];
+}
+
+// -(b o x).sum() in FP64 partials (PottsCompatibility::gradient).
+__global__ void neg_dot_partial_kernel(long n, const float* __restrict__ b, const float* __restrict__ x,
+                                       double* __restrict__ part) {
+    __shared__ double sm[256];
+    double acc = 0.0;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+        acc += (double)fmul(b[t], x[t]);
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x] = -sm[0];
+}
+
+__global__ void fill_ones_kernel(long n, float* x) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) x[t] = 1.0f;
+}
+
 }  // namespace
 
 Model::Model(int W_, int H_, int L_) : W(W_), H(H_), N(W_ * H_), L(L_) {
@@ -95,6 +158,8 @@ void Model::add_term(const float* d_features, int d, float w) {
     t->lat->build(d_features, d, N);
     t->w = w;
     t->d = d;
+    float* tf = t->feat.ensure((size_t)N * d);
+    DCRF_CUDA(cudaMemcpyAsync(tf, d_features, sizeof(float) * (size_t)N * d, cudaMemcpyDeviceToDevice, stream));
     float* nrm = t->norm.ensure(N);
     launch(fill_kernel, ceil_div(N, 256), 256, 0, stream, N, 1.0f, nrm);
     SliceEpilogue ep;  // plain output
@@ -102,6 +167,69 @@ void Model::add_term(const float* d_features, int d, float w) {
     launch(norm_kernel, ceil_div(N, 256), 256, 0, stream, N, nrm);
     DCRF_LAUNCH_CHECK();
     terms.push_back(std::move(t));
+}
+
+// pairwise_[k]->kernelGradient(b, Q) for a diagonal kernel with symmetric
+// normalisation: lbl = -w Q (PottsCompatibility::apply), then
+// featureGradient(b, lbl) = -G(X, 1) + G(b n, lbl n) with G = the lattice's
+// gradient, fa = K^T(b n), fb = K(lbl n), X = 0.5 (b o fb + fa o lbl) n^3;
+// the result is sum_i f(i, j) fg(i, j) per dimension j (FP64 sum, rounded to
+// float -- the reference sums in float).
+void Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
+    Term& t = *terms[k];
+    Lattice& lat = *t.lat;
+    const long NL = (long)N * L;
+    const int d = t.d, g = ceil_div(NL, 256);
+    float *lbl = buf(8), *bn = buf(9), *ln = buf(10), *fa = buf(11), *fb = buf(12), *X = buf(13);
+    float* ones = this->b[7].ensure((size_t)NL);
+    float* r = this->b[14].ensure((size_t)N * d);
+    float* gg = this->b[15].ensure((size_t)N * d);
+    const float* nrm = t.norm.get();
+    launch(scale_cols_kernel, g, 256, 0, stream, NL, L, Q, (const float*)nullptr, -t.w, lbl);
+    launch(scale_cols_kernel, g, 256, 0, stream, NL, L, b, nrm, 1.0f, bn);
+    launch(scale_cols_kernel, g, 256, 0, stream, NL, L, lbl, nrm, 1.0f, ln);
+    SliceEpilogue plain;
+    lat.compute(fa, bn, L, true, plain);
+    lat.compute(fb, ln, L, false, plain);
+    launch(sym_grad_input_kernel, g, 256, 0, stream, NL, L, b, fb, fa, lbl, nrm, X);
+    launch(fill_ones_kernel, g, 256, 0, stream, NL, ones);
+    lat.gradient(r, X, ones, L);
+    lat.gradient(gg, bn, ln, L);
+    const int nb = 64;
+    double* part = partials.get();
+    launch(diag_grad_partial_kernel, dim3(nb, d), 256, 0, stream, N, d, t.feat.get(), r, gg, part);
+    DCRF_LAUNCH_CHECK();
+    std::vector<double> h((size_t)nb * d);
+    DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
+    sync();
+    for (int j = 0; j < d; j++) {
+        double s = 0.0;
+        for (int i = 0; i < nb; i++) s += h[(size_t)j * nb + i];
+        out[j] = (float)s;
+    }
+}
+
+// pairwise_[k]->gradient(b, Q) = -(b o n K(n Q)).sum() for a Potts term
+// (src/pairwise.cpp:390-395, src/labelcompatibility.cpp:72-76); FP64 sum.
+float Model::weight_gradient(int k, const float* b, const float* Q) {
+    Term& t = *terms[k];
+    const long NL = (long)N * L;
+    float* fq = buf(8);
+    SliceEpilogue ep;
+    ep.potts = true;
+    ep.norm = t.norm.get();
+    ep.scale = 1.0f;
+    t.lat->compute(fq, Q, L, false, ep, t.norm.get());
+    const int nb = 128;
+    double* part = partials.get();
+    launch(neg_dot_partial_kernel, nb, 256, 0, stream, NL, b, (const float*)fq, part);
+    DCRF_LAUNCH_CHECK();
+    std::vector<double> h(nb);
+    DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost, stream));
+    sync();
+    double s = 0.0;
+    for (int i = 0; i < nb; i++) s += h[i];
+    return (float)s;
 }
 
 void Model::set_cliques(int R_, const int* off, const int* idx, const float* expw, const float* cst) {

@@ -13,6 +13,7 @@ namespace dcrf {
 struct Term {
     std::unique_ptr<Lattice> lat;
     DevBuf<float> norm;  // 1/sqrt(K 1 + 1e-20) (src/pairwise.cpp:46-50)
+    DevBuf<float> feat;  // the features [N][d] (DenseKernel::f_), for the kernel gradient
     float w = 0.0f;      // Potts weight
     int d = 0;
 };
@@ -78,6 +79,11 @@ struct Model {
     void apply(int k, bool nonorm, float* out, const float* in, const float* base = nullptr,
                float coef = 1.0f, bool zero_base = false);
     void apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap);
+    // pairwise_[k]->kernelGradient(b, Q) (d floats: the diagonal kernel's
+    // feature-scale gradient) and ->gradient(b, Q) (the Potts weight's);
+    // b, Q device [N][L], results to host.
+    void kernel_gradient(int k, const float* b, const float* Q, float* out);
+    float weight_gradient(int k, const float* b, const float* Q);
     void apply_ord_bins(int k, float* out, const float2* bins, const float* base, bool zero_base,
                         const GapFusion* gap);
     void apply_ord(int k, float* out, const float* rq, const float* base = nullptr,

@@ -198,6 +198,14 @@ dcrf_status dcrf_model_energy_ho(dcrf_model m, const int16_t* labels, double* en
 dcrf_status dcrf_model_energy_lp(dcrf_model m, const float* Q, double* energy);
 /* compute_LR_QP_value(Q, 0) (src/densecrf.cpp:940-957). */
 dcrf_status dcrf_model_lr_qp_value(dcrf_model m, const float* Q, double* energy);
+/* pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 90-122,
+ * 170-181): the gradient of the diagonal kernel's feature scales, d floats
+ * (d = 2 Gaussian, 5 bilateral; d is returned when not NULL; grad holds
+ * at least 16 floats), and pairwise_[k]->gradient(b, Q)
+ * (:390-395): the Potts weight's, 1 float.  b, Q [N][L]. */
+dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model m, int k, const float* b, const float* Q,
+                                                float* grad, int* d);
+dcrf_status dcrf_model_pairwise_gradient(dcrf_model m, int k, const float* b, const float* Q, float* grad);
 /* Number of pairwise terms, and vertex count of term k's lattice. */
 dcrf_status dcrf_model_info(dcrf_model m, int* n_terms, int* N, int* L);
 dcrf_status dcrf_model_lattice_size(dcrf_model m, int k, int* M);

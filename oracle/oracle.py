@@ -123,6 +123,8 @@ def ref_lib():
         L.refl_gradient.argtypes = [vp, _f32p, _f32p, _f32p, C.c_int]
         L.refm_new.restype = vp
         L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
+        L.refm_kernel_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
+        L.refm_weight_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
         L.refm_free.argtypes = [vp]
         L.refm_add_gaussian.argtypes = [vp, C.c_float, C.c_float, C.c_float]
         L.refm_add_bilateral.argtypes = [vp] + [C.c_float] * 5 + [_u8p, C.c_float]
@@ -293,6 +295,18 @@ class _Model:
 
     def lr_qp_value(self, Q):
         return self._fn("lr_qp_value")(self._h, _c(Q, np.float32))
+
+    def kernel_gradient(self, k, b, Q):
+        """pairwise_[k]->kernelGradient(b, Q): d floats (reference model only)."""
+        out = np.zeros(16, np.float32)
+        n = self._lib.refm_kernel_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
+        return out[:n]
+
+    def weight_gradient(self, k, b, Q):
+        """pairwise_[k]->gradient(b, Q): the Potts weight's gradient (reference model only)."""
+        out = np.zeros(16, np.float32)
+        n = self._lib.refm_weight_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
+        return out[:n]
 
 
 class OracleModel(_Model):

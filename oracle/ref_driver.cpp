@@ -47,6 +47,13 @@ struct LatticeProbe : public Permutohedral {
 // so a fixed-iteration QP can be run from the reference's own building blocks.
 struct RefModel : public DenseCRF2D {
     RefModel(int W, int H, int L) : DenseCRF2D(W, H, L) {}
+    // pairwise_[k]->kernelGradient(b, Q) and ->gradient(b, Q) (src/pairwise.cpp:390-407)
+    VectorXf kernel_gradient(int k, const MatrixXf& b, const MatrixXf& Q) const {
+        return pairwise_[k]->kernelGradient(b, Q);
+    }
+    VectorXf weight_gradient(int k, const MatrixXf& b, const MatrixXf& Q) const {
+        return pairwise_[k]->gradient(b, Q);
+    }
     int N() const { return N_; }
     int L() const { return M_; }
     int R() const { return R_; }
@@ -301,6 +308,22 @@ double refm_energy_true(void* h, const short* labels) {
     RefModel* m = (RefModel*)h;
     VectorXs l = Map<const VectorXs>(labels, m->N());
     return m->assignment_energy_true(l);
+}
+// Kernel-parameter (feature scale) and Potts-weight gradients of term k;
+// b, Q [N][L]; out receives d (kernel) or 1 (weight) floats.
+int refm_kernel_gradient(void* h, int k, const float* b, const float* Q, float* out) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf B = Map<const MatrixXf>(b, m->L(), m->N()), QQ = Map<const MatrixXf>(Q, m->L(), m->N());
+    VectorXf g = m->kernel_gradient(k, B, QQ);
+    std::memcpy(out, g.data(), sizeof(float) * g.size());
+    return (int)g.size();
+}
+int refm_weight_gradient(void* h, int k, const float* b, const float* Q, float* out) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf B = Map<const MatrixXf>(b, m->L(), m->N()), QQ = Map<const MatrixXf>(Q, m->L(), m->N());
+    VectorXf g = m->weight_gradient(k, B, QQ);
+    std::memcpy(out, g.data(), sizeof(float) * g.size());
+    return (int)g.size();
 }
 double refm_energy_ho(void* h, const short* labels) {
     RefModel* m = (RefModel*)h;

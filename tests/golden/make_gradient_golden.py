@@ -36,3 +36,23 @@ def main():
 
 if __name__ == "__main__":
     main()
+
+
+def model_case():
+    """pairwise_[k]->kernelGradient(b, Q) and ->gradient(b, Q) of the example's
+    Gaussian + bilateral model, from the reference itself."""
+    img = synth.make_image(24, 18, 5, 3)
+    m = O.build_model(O.ReferenceModel, img)
+    rng = np.random.default_rng(0)
+    b = rng.standard_normal((24 * 18, 5)).astype(np.float32)
+    Q = rng.random((24 * 18, 5)).astype(np.float32)
+    out = dict(W=24, H=18, L=5, seed=3, b=b, Q=Q)
+    for k in range(2):
+        out[f"kgrad{k}"] = m.kernel_gradient(k, b, Q)
+        out[f"wgrad{k}"] = m.weight_gradient(k, b, Q)
+    np.savez_compressed(os.path.join(HERE, "mgrad_24x18_L5.npz"), **out)
+    print("model", {k: v for k, v in out.items() if "grad" in k})
+
+
+if __name__ == "__main__":
+    model_case()

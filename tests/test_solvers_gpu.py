@@ -160,3 +160,25 @@ def test_many_cliques_vs_oracle(oracle_mod):
     assert (la == lb).mean() >= 0.999
     ea, eb = orc.energy_ho(la), orc.energy_ho(lb)
     assert abs(ea - eb) <= ENERGY_RTOL * abs(eb)
+
+
+def test_kernel_and_weight_gradients_vs_reference():
+    """pairwise_[k]->kernelGradient(b, Q) (feature-scale gradient of the
+    diagonal kernel, symmetric normalisation) and ->gradient(b, Q) (Potts
+    weight), against the reference's own values.  Every step is the
+    reference's float arithmetic except the final sums over pixels (FP64
+    here, float there): 1e-4 relative of the largest component."""
+    g = golden("mgrad_24x18_L5.npz")
+    W, H = int(g["W"]), int(g["H"])
+    img = synth.make_image(W, H, int(g["L"]), int(g["seed"]))
+    m = DenseCRF2D(W, H, int(g["L"]))
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    for k in range(2):
+        kg = m.pairwise_kernel_gradient(k, g["b"], g["Q"])
+        ref = g[f"kgrad{k}"]
+        assert kg.shape == ref.shape
+        assert np.abs(kg - ref).max() <= 1e-4 * np.abs(ref).max(), (k, kg, ref)
+        wg = m.pairwise_gradient(k, g["b"], g["Q"])
+        assert abs(wg[0] - g[f"wgrad{k}"][0]) <= 1e-5 * abs(g[f"wgrad{k}"][0])
