@@ -147,6 +147,23 @@ class DenseCRF2D:
         check(lib().dcrf_model_add_pairwise(self._h, f.ctypes.data_as(C.c_void_p), f.shape[1],
                                             C.c_float(w)))
 
+    def setCompatibility(self, k, diagonal=None, matrix=None, potts=None):
+        """Label compatibility of term k: ``diagonal`` (L weights,
+        DiagonalCompatibility), ``matrix`` (L x L, MatrixCompatibility, used as
+        0.5 (m + m^T)) or ``potts`` (the weight)."""
+        if diagonal is not None:
+            kind, p = 1, np.ascontiguousarray(diagonal, np.float32).reshape(-1)
+            if p.size != self.L:
+                raise DCRFError(1, "diagonal needs L weights")
+        elif matrix is not None:
+            m = np.asarray(matrix, np.float32)
+            if m.shape != (self.L, self.L):
+                raise DCRFError(1, "matrix must be L x L")
+            kind, p = 2, np.ascontiguousarray(m.T).reshape(-1)  # column-major, as Eigen stores it
+        else:
+            kind, p = 0, np.array([potts], np.float32)
+        check(lib().dcrf_model_set_compat(self._h, int(k), kind, p.ctypes.data_as(C.c_void_p)))
+
     def setCliques(self, offsets, idx, exp_weight, constants):
         offsets = np.ascontiguousarray(offsets, np.int32)
         idx = np.ascontiguousarray(idx, np.int32)
@@ -348,14 +365,35 @@ def _pairwise_kernel_gradient(self, k, b, Q):
     return out[:d.value]
 
 
+def _pairwise_parameters(self, k):
+    """``pairwise_[k]->parameters()``: Potts [w], Diagonal [w_l], Matrix the
+    upper triangle of the symmetric matrix by column."""
+    n = C.c_int(0)
+    check(lib().dcrf_model_pairwise_parameters(self._h, int(k), None, C.byref(n)))
+    out = np.zeros(n.value, np.float32)
+    check(lib().dcrf_model_pairwise_parameters(self._h, int(k), out.ctypes.data_as(C.c_void_p), None))
+    return out
+
+
+def _pairwise_set_parameters(self, k, v):
+    """``pairwise_[k]->setParameters(v)``, v as ``parameters()`` returns it."""
+    v = np.ascontiguousarray(v, np.float32).reshape(-1)
+    if v.size != self.pairwise_parameters(k).size:
+        raise DCRFError(1, "wrong number of compatibility parameters")
+    check(lib().dcrf_model_pairwise_set_parameters(self._h, int(k), v.ctypes.data_as(C.c_void_p)))
+
+
 def _pairwise_gradient(self, k, b, Q):
-    """``pairwise_[k]->gradient(b, Q)``: gradient of the term's Potts weight."""
+    """``pairwise_[k]->gradient(b, Q)``: gradient of the term's compatibility
+    parameters (the layout of ``parameters()``)."""
     bb, qq = self._mat(b), self._mat(Q)
-    out = np.zeros(1, np.float32)
+    out = np.zeros(self.pairwise_parameters(k).size, np.float32)
     check(lib().dcrf_model_pairwise_gradient(self._h, int(k), bb.ctypes.data_as(C.c_void_p),
                                              qq.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
     return out
 
 
+DenseCRF2D.pairwise_parameters = _pairwise_parameters
+DenseCRF2D.pairwise_set_parameters = _pairwise_set_parameters
 DenseCRF2D.pairwise_kernel_gradient = _pairwise_kernel_gradient
 DenseCRF2D.pairwise_gradient = _pairwise_gradient

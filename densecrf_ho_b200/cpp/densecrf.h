@@ -9,13 +9,13 @@
 // ("Value out of bounds", "Maxval < 0, skipping") are thrown as
 // std::runtime_error with the same text, every other failure too.
 //
-// Scope (the B200 path): Potts compatibilities, DIAG_KERNEL with
+// Scope (the B200 path): Potts, Diagonal and Matrix compatibilities, DIAG_KERNEL with
 // NORMALIZE_SYMMETRIC (and its NO_NORMALIZATION copy), constant unaries, the
 // qp / lp / qp_sp / lp_sp solvers.  Superpixel cliques are given as a
 // per-pixel region map (addSuperPixel's segmentation step, EDISON mean-shift,
 // stays with the caller); the clique weights are derived from the image
-// exactly as src/densecrf.cpp:212-247 does.  Other compatibilities, kernel
-// types and normalisations throw std::runtime_error.
+// exactly as src/densecrf.cpp:212-247 does.  Other kernel types and
+// normalisations throw std::runtime_error.
 //
 // Header-only; needs Eigen (the reference vendors 3.2.7) and include/dcrf.h.
 #pragma once
@@ -45,11 +45,17 @@ enum NormalizationType { NO_NORMALIZATION, NORMALIZE_BEFORE, NORMALIZE_AFTER, NO
 enum KernelType { CONST_KERNEL, DIAG_KERNEL, FULL_KERNEL };
 
 // ------------------------------------------------------ labelcompatibility.h --
+// The compatibilities hold their parameters on the host; the model gets them
+// through dcrf_model_set_compat when the term is added.
 class LabelCompatibility {
 public:
     virtual ~LabelCompatibility() {}
-    // Potts weight w of mu(a, b) = -w [a == b]; only Potts runs on the B200 path.
-    virtual bool potts(float* w) const { return false; }
+    virtual MatrixXf matrixForm(int nb_labels) const = 0;
+    virtual VectorXf parameters() const = 0;
+    virtual void setParameters(const VectorXf& v) = 0;
+    // DCRF_COMPAT_* kind and its dcrf_model_set_compat parameters.
+    virtual int kind() const = 0;
+    virtual std::vector<float> abi_params() const = 0;
 };
 
 class PottsCompatibility : public LabelCompatibility {
@@ -57,36 +63,70 @@ protected:
     float w_;
 public:
     PottsCompatibility(float weight = 1.0) : w_(weight) {}
-    bool potts(float* w) const override {
-        *w = w_;
-        return true;
+    MatrixXf matrixForm(int nb_labels) const override {
+        return MatrixXf(-w_ * MatrixXf::Identity(nb_labels, nb_labels));
     }
-    VectorXf parameters() const {
+    VectorXf parameters() const override {
         VectorXf r(1);
         r[0] = w_;
         return r;
     }
-    void setParameters(const VectorXf& v) { w_ = v[0]; }
+    void setParameters(const VectorXf& v) override { w_ = v[0]; }
+    int kind() const override { return DCRF_COMPAT_POTTS; }
+    std::vector<float> abi_params() const override { return {w_}; }
 };
 
 class DiagonalCompatibility : public LabelCompatibility {
+protected:
+    VectorXf w_;
 public:
-    DiagonalCompatibility(const VectorXf&) {}
+    DiagonalCompatibility(const VectorXf& v) : w_(v) {}
+    MatrixXf matrixForm(int) const override { return MatrixXf(w_.asDiagonal()); }
+    VectorXf parameters() const override { return w_; }
+    void setParameters(const VectorXf& v) override { w_ = v; }
+    int kind() const override { return DCRF_COMPAT_DIAGONAL; }
+    std::vector<float> abi_params() const override { return std::vector<float>(w_.data(), w_.data() + w_.size()); }
 };
 
 class MatrixCompatibility : public LabelCompatibility {
+protected:
+    MatrixXf w_;
 public:
-    MatrixCompatibility(const MatrixXf&) {}
+    MatrixCompatibility(const MatrixXf& m) : w_(0.5 * (m + m.transpose())) {}
+    MatrixXf matrixForm(int) const override { return w_; }
+    VectorXf parameters() const override {
+        VectorXf r(w_.cols() * (w_.rows() + 1) / 2);
+        for (int i = 0, k = 0; i < w_.cols(); i++)
+            for (int j = i; j < w_.rows(); j++, k++) r[k] = w_(i, j);
+        return r;
+    }
+    void setParameters(const VectorXf& v) override {
+        for (int i = 0, k = 0; i < w_.cols(); i++)
+            for (int j = i; j < w_.rows(); j++, k++) w_(j, i) = w_(i, j) = v[k];
+    }
+    int kind() const override { return DCRF_COMPAT_MATRIX; }
+    // already symmetric, so the model's symmetrisation leaves it as it is
+    std::vector<float> abi_params() const override { return std::vector<float>(w_.data(), w_.data() + w_.size()); }
 };
 
 namespace dcrf_shim {
-// Takes ownership of f (as the reference does) and returns its Potts weight.
-inline float potts_weight(LabelCompatibility* f) {
+// A term's compatibility as the C ABI takes it; owns f, as the reference does.
+struct Compat {
+    int kind = DCRF_COMPAT_POTTS;
+    std::vector<float> p;  // p[0] is parameters()(0) for every kind
+};
+inline Compat take_compat(LabelCompatibility* f) {
     std::unique_ptr<LabelCompatibility> own(f);
-    float w = 0;
-    if (!f || !f->potts(&w))
-        throw std::runtime_error("only PottsCompatibility runs on the B200 path");
-    return w;
+    if (!f) throw std::runtime_error("a pairwise term needs a LabelCompatibility");
+    Compat c;
+    c.kind = f->kind();
+    c.p = f->abi_params();
+    return c;
+}
+// Gives term k of model m, added with weight c.p[0], compatibility c.
+inline void set_compat(dcrf_model m, int k, const Compat& c) {
+    if (c.kind != DCRF_COMPAT_POTTS && dcrf_model_set_compat(m, k, c.kind, c.p.data()) != DCRF_OK)
+        throw std::runtime_error(dcrf_last_error());
 }
 inline void check_kernel(KernelType k, NormalizationType n) {
     if (k != DIAG_KERNEL && k != CONST_KERNEL)
@@ -202,7 +242,7 @@ private:
 // count of the first apply.
 class PairwisePotential {
     MatrixXf f_;
-    float w_;
+    dcrf_shim::Compat c_;
     int L_ = 0;
     dcrf_model m_ = nullptr;
     PairwisePotential(const PairwisePotential&) = delete;
@@ -211,13 +251,14 @@ class PairwisePotential {
         if (m_) dcrf_model_destroy(m_);
         m_ = nullptr;
         dcrf_shim::check(dcrf_model_create(&m_, (int)f_.cols(), 1, L));
-        dcrf_shim::check(dcrf_model_add_pairwise(m_, f_.data(), (int)f_.rows(), w_));
+        dcrf_shim::check(dcrf_model_add_pairwise(m_, f_.data(), (int)f_.rows(), c_.p.at(0)));
+        dcrf_shim::set_compat(m_, 0, c_);
         L_ = L;
     }
 public:
     PairwisePotential(const MatrixXf& features, LabelCompatibility* compatibility, KernelType ktype = CONST_KERNEL,
                       NormalizationType ntype = NORMALIZE_SYMMETRIC)
-        : f_(features), w_(dcrf_shim::potts_weight(compatibility)) {
+        : f_(features), c_(dcrf_shim::take_compat(compatibility)) {
         dcrf_shim::check_kernel(ktype, ntype);
     }
     ~PairwisePotential() {
@@ -239,9 +280,14 @@ public:
         dcrf_shim::check(dcrf_model_pairwise_apply_ord(m_, 0, out.data(), src.data()));
     }
     VectorXf parameters() const {
-        VectorXf r(1);
-        r[0] = w_;
-        return r;
+        if (c_.kind == DCRF_COMPAT_MATRIX) {  // the upper triangle by column
+            const int L = (int)std::lround(std::sqrt((double)c_.p.size()));
+            VectorXf r(L * (L + 1) / 2);
+            for (int i = 0, k = 0; i < L; i++)
+                for (int j = i; j < L; j++, k++) r[k] = c_.p[(size_t)j * L + i];
+            return r;
+        }
+        return Map<const VectorXf>(c_.p.data(), (long)c_.p.size());
     }
     MatrixXf features() const { return f_; }
 };
@@ -269,10 +315,10 @@ public:
     virtual void addPairwiseEnergy(const MatrixXf& features, LabelCompatibility* function,
                                    KernelType kernel_type = DIAG_KERNEL,
                                    NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
-        const float w = dcrf_shim::potts_weight(function);
+        const dcrf_shim::Compat c = dcrf_shim::take_compat(function);
         dcrf_shim::check_kernel(kernel_type, normalization_type);
-        dcrf_shim::check(dcrf_model_add_pairwise(m_, features.data(), (int)features.rows(), w));
-        n_terms_++;
+        dcrf_shim::check(dcrf_model_add_pairwise(m_, features.data(), (int)features.rows(), c.p.at(0)));
+        dcrf_shim::set_compat(m_, n_terms_++, c);
     }
     void setUnaryEnergy(const MatrixXf& unary) { dcrf_shim::check(dcrf_model_set_unary(m_, unary.data())); }
     void setUnaryEnergy(UnaryEnergy* unary) {
@@ -376,19 +422,19 @@ public:
     void addPairwiseGaussian(float sx, float sy, LabelCompatibility* function = NULL,
                              KernelType kernel_type = DIAG_KERNEL,
                              NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
-        const float w = dcrf_shim::potts_weight(function);
+        const dcrf_shim::Compat c = dcrf_shim::take_compat(function);
         dcrf_shim::check_kernel(kernel_type, normalization_type);
-        dcrf_shim::check(dcrf_model_add_gaussian(m_, sx, sy, w));
-        n_terms_++;
+        dcrf_shim::check(dcrf_model_add_gaussian(m_, sx, sy, c.p.at(0)));
+        dcrf_shim::set_compat(m_, n_terms_++, c);
     }
     // addPairwiseBilateral (src/densecrf.cpp:179-190)
     void addPairwiseBilateral(float sx, float sy, float sr, float sg, float sb, const unsigned char* im,
                               LabelCompatibility* function = NULL, KernelType kernel_type = DIAG_KERNEL,
                               NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
-        const float w = dcrf_shim::potts_weight(function);
+        const dcrf_shim::Compat c = dcrf_shim::take_compat(function);
         dcrf_shim::check_kernel(kernel_type, normalization_type);
-        dcrf_shim::check(dcrf_model_add_bilateral(m_, sx, sy, sr, sg, sb, im, w));
-        n_terms_++;
+        dcrf_shim::check(dcrf_model_add_bilateral(m_, sx, sy, sr, sg, sb, im, c.p.at(0)));
+        dcrf_shim::set_compat(m_, n_terms_++, c);
     }
     using DenseCRF::setUnaryEnergy;
 };

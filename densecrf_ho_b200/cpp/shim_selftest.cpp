@@ -2,9 +2,10 @@
 // Usage: shim_selftest W H L rgb.u8 unary.f32 out_prefix
 // Builds the example's Gaussian + bilateral Potts model through the
 // reference-named classes, runs unary_init, the QP and a short LP, a
-// standalone Permutohedral filter and PairwisePotential, and writes the
-// results as raw float32 files <out_prefix>.{init,qp,lp,filt,pw}; energies and
-// the error-path check go to stdout.
+// standalone Permutohedral filter and PairwisePotential, and a QP of a model
+// with Diagonal and Matrix compatibilities; writes the results as raw float32
+// files <out_prefix>.{init,qp,lp,filt,pw,qpc}; energies and the error-path
+// checks go to stdout.
 #include <cstdio>
 #include <fstream>
 #include <iostream>
@@ -76,11 +77,26 @@ int main(int argc, char** argv) {
             printf("range_error %s\n", e.what());
         }
         try {
-            crf.addPairwiseGaussian(3, 3, new MatrixCompatibility(MatrixXf::Identity(L, L)));
-            printf("compat_error missing\n");
+            crf.addPairwiseGaussian(3, 3, new PottsCompatibility(1), DIAG_KERNEL, NORMALIZE_AFTER);
+            printf("kernel_error missing\n");
         } catch (const std::runtime_error& e) {
-            printf("compat_error ok\n");
+            printf("kernel_error ok\n");
         }
+
+        // Diagonal on the Gaussian term, Matrix on the bilateral one.
+        VectorXf dg(L);
+        MatrixXf mt(L, L);
+        for (int a = 0; a < L; a++) {
+            dg[a] = -(2.0f + 0.1f * a);
+            for (int b = 0; b < L; b++) mt(a, b) = a == b ? -5.0f : 0.1f * (a + 2 * b) / L;
+        }
+        DenseCRF2D crf2(W, H, L);
+        crf2.setUnaryEnergy(U);
+        crf2.addPairwiseGaussian(3, 3, new DiagonalCompatibility(dg));
+        crf2.addPairwiseBilateral(50, 50, 15, 15, 15, rgb.data(), new MatrixCompatibility(mt));
+        MatrixXf qpc = crf2.qp_inference_super_pixels_non_convex(crf2.unary_init());
+        printf("compat_energy %.10f\n", crf2.assignment_energy_true(crf2.currentMap(qpc)));
+        write_raw(out + ".qpc", qpc);
         write_raw(out + ".init", Q);
         write_raw(out + ".qp", qp);
         write_raw(out + ".lp", lp);

@@ -379,6 +379,15 @@ dcrf_status dcrf_model_add_bilateral(dcrf_model h, float sx, float sy, float sr,
     });
 }
 
+dcrf_status dcrf_model_set_compat(dcrf_model h, int k, int kind, const float* params) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(params, "params");
+        m.set_compat(k, kind, params);
+    });
+}
+
 dcrf_status dcrf_model_set_cliques(dcrf_model h, int R, const int32_t* offsets, const int32_t* idx,
                                    const float* exp_weight, const float* constants) {
     return guard([&] {
@@ -630,7 +639,25 @@ dcrf_status dcrf_model_pairwise_gradient(dcrf_model h, int k, const float* b, co
         const size_t n = (size_t)m.N * m.L;
         const float* db = upload(h->io0, b, n, m.stream);
         const float* dq = upload(h->io1, Q, n, m.stream);
-        *grad = m.weight_gradient(k, db, dq);
+        m.compat_gradient(k, db, dq, grad);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_parameters(dcrf_model h, int k, float* params, int* n) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        if (n) *n = m.n_parameters(k);
+        if (params) m.parameters(k, params);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_set_parameters(dcrf_model h, int k, const float* params) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(params, "params");
+        m.set_parameters(k, params);
     });
 }
 

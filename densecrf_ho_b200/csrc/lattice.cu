@@ -487,10 +487,10 @@ __global__ void blur_kernel(int M, int Lrt, const int2* __restrict__ nbr,
     dst[(long)(v + 1) * L + k] = r;
 }
 
-__device__ __forceinline__ float apply_epilogue(float v, long t, int i, const SliceEpilogue& ep) {
+__device__ __forceinline__ float apply_epilogue(float v, long t, int i, int k, const SliceEpilogue& ep) {
     if (ep.potts) {
         if (ep.norm) v = fmul(v, ep.norm[i]);
-        v = fmul(ep.scale, v);
+        v = ep.scale_vec ? fmul(ep.scale_vec[k], v) : fmul(ep.scale, v);
     }
     if (ep.base) v = fadd(ep.base[t], fmul(ep.coef, v));
     else if (ep.zero_base) v = fadd(0.0f, fmul(ep.coef, v));
@@ -518,7 +518,7 @@ __global__ void slice_kernel(int N, int Lrt, int drt, const int* __restrict__ of
         if (SEQ) acc = fadd(acc, fmul(fmul(w, v), alpha));
         else acc = fadd(acc, fmul(fmul(w, alpha), v));
     }
-    out[t] = apply_epilogue(acc, t, i, ep);
+    out[t] = apply_epilogue(acc, t, i, k, ep);
 }
 
 // addSplitArray / sliceSplitArray bins (:548-589): the lower pass rounds
@@ -905,7 +905,7 @@ __global__ void ord_slice_kernel(int N, int Lrt, int drt, const int* __restrict_
             const float w = bary[(long)i * d1 + j];
             acc = fadd(acc, fmul(vals[((long)(o + 1) * kOrdW + kRes + cu) * L + k], fmul(w, alpha)));
         }
-        const float v = apply_epilogue(acc, t, i, ep);
+        const float v = apply_epilogue(acc, t, i, k, ep);
         out[t] = v;
         if (GAP) {
             const float tmp = fsub(fadd(gf.alpha[t], gf.u[t]), fadd(v, gf.su ? gf.su[t] : 0.0f));

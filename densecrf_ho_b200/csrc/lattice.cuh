@@ -26,6 +26,7 @@ struct SliceEpilogue {
     const float* norm = nullptr;  // multiply by norm[i] (symmetric normalisation)
     float scale = 1.0f;           // then by this (Potts: -w); exactly 1 = skip
     bool potts = false;           // apply norm / scale at all
+    const float* scale_vec = nullptr;  // per-label scale instead of `scale` (DiagonalCompatibility)
     const float* base = nullptr;  // then out = base[...] + coef * v
     float coef = 1.0f;
     bool zero_base = false;       // out = 0.0f + coef * v  (Eigen fill(0); +=)

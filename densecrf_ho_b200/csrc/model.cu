@@ -116,6 +116,49 @@ __global__ void neg_dot_partial_kernel(long n, const float* __restrict__ b, cons
     if (threadIdx.x == 0) part[blockIdx.x] = -sm[0];
 }
 
+// MatrixCompatibility::apply (src/labelcompatibility.cpp:102-104): out(:, i)
+// = W raw(:, i), W column-major L x L, the product summed over m in order;
+// then the epilogue's base: out = base + coef * (W raw).
+__global__ void matrix_compat_kernel(long n, int L, const float* __restrict__ W, const float* __restrict__ raw,
+                                     const float* __restrict__ base, float coef, int zero_base, float* out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const long i = t / L;
+    const int l = (int)(t - i * L);
+    const float* x = raw + i * L;
+    float r = fmul(W[l], x[0]);
+    for (int m = 1; m < L; m++) r = fadd(r, fmul(W[l + (long)m * L], x[m]));
+    if (base) r = fadd(base[t], fmul(coef, r));
+    else if (zero_base) r = fadd(0.0f, fmul(coef, r));
+    out[t] = r;
+}
+
+// DiagonalCompatibility::apply: out(l, i) = w_l in(l, i).
+__global__ void scale_labels_kernel(long n, int L, const float* __restrict__ in, const float* __restrict__ w,
+                                    float* __restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = fmul(w[t % L], in[t]);
+}
+
+// part[p * gridDim.x + blk]: this block's share of sum_i b(r, i) x(c, i) for
+// pair p = c * L + r (r = c = p when diag_only).
+__global__ void label_outer_partial_kernel(int N, int L, const float* __restrict__ b, const float* __restrict__ x,
+                                           int diag_only, double* __restrict__ part) {
+    __shared__ double sm[256];
+    const int p = blockIdx.y;
+    const int c = diag_only ? p : p / L, r = diag_only ? p : p - (p / L) * L;
+    double acc = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        acc += (double)fmul(b[i * L + r], x[i * L + c]);
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(long)p * gridDim.x + blockIdx.x] = sm[0];
+}
+
 __global__ void fill_ones_kernel(long n, float* x) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) x[t] = 1.0f;
@@ -185,7 +228,13 @@ void Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
     float* r = this->b[14].ensure((size_t)N * d);
     float* gg = this->b[15].ensure((size_t)N * d);
     const float* nrm = t.norm.get();
-    launch(scale_cols_kernel, g, 256, 0, stream, NL, L, Q, (const float*)nullptr, -t.w, lbl);
+    if (t.compat == kPotts)
+        launch(scale_cols_kernel, g, 256, 0, stream, NL, L, Q, (const float*)nullptr, -t.w, lbl);
+    else if (t.compat == kDiagonal)
+        launch(scale_labels_kernel, g, 256, 0, stream, NL, L, Q, (const float*)t.cw.get(), lbl);
+    else
+        launch(matrix_compat_kernel, g, 256, 0, stream, NL, L, (const float*)t.cw.get(), Q, (const float*)nullptr,
+               1.0f, 0, lbl);
     launch(scale_cols_kernel, g, 256, 0, stream, NL, L, b, nrm, 1.0f, bn);
     launch(scale_cols_kernel, g, 256, 0, stream, NL, L, lbl, nrm, 1.0f, ln);
     SliceEpilogue plain;
@@ -209,9 +258,13 @@ void Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
     }
 }
 
-// pairwise_[k]->gradient(b, Q) = -(b o n K(n Q)).sum() for a Potts term
-// (src/pairwise.cpp:390-395, src/labelcompatibility.cpp:72-76); FP64 sum.
-float Model::weight_gradient(int k, const float* b, const float* Q) {
+// pairwise_[k]->gradient(b, Q) (src/pairwise.cpp:390-395): the
+// compatibility's gradient at fq = n K(n Q) (src/labelcompatibility.cpp):
+// Potts -(b o fq).sum() (:72-76), Diagonal (b o fq).rowwise().sum() (:94-96),
+// Matrix g = b fq^T folded to its upper triangle, g(i,j) + g(j,i) off the
+// diagonal (:123-129).  FP64 sums over pixels, rounded to float.
+int Model::compat_gradient(int k, const float* b, const float* Q, float* out) {
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
     Term& t = *terms[k];
     const long NL = (long)N * L;
     float* fq = buf(8);
@@ -220,16 +273,74 @@ float Model::weight_gradient(int k, const float* b, const float* Q) {
     ep.norm = t.norm.get();
     ep.scale = 1.0f;
     t.lat->compute(fq, Q, L, false, ep, t.norm.get());
-    const int nb = 128;
     double* part = partials.get();
-    launch(neg_dot_partial_kernel, nb, 256, 0, stream, NL, b, (const float*)fq, part);
+    if (t.compat == kPotts) {
+        const int nb = 128;
+        launch(neg_dot_partial_kernel, nb, 256, 0, stream, NL, b, (const float*)fq, part);
+        DCRF_LAUNCH_CHECK();
+        std::vector<double> h(nb);
+        DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost, stream));
+        sync();
+        double s = 0.0;
+        for (int i = 0; i < nb; i++) s += h[i];
+        out[0] = (float)s;
+        return 1;
+    }
+    const bool diag = t.compat == kDiagonal;
+    const int pairs = diag ? L : L * L;
+    const int nb = 32;
+    part = partials.ensure((size_t)nb * pairs);
+    launch(label_outer_partial_kernel, dim3(nb, pairs), 256, 0, stream, N, L, b, (const float*)fq, (int)diag, part);
     DCRF_LAUNCH_CHECK();
-    std::vector<double> h(nb);
-    DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * nb, cudaMemcpyDeviceToHost, stream));
+    std::vector<double> h((size_t)nb * pairs);
+    DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
     sync();
-    double s = 0.0;
-    for (int i = 0; i < nb; i++) s += h[i];
-    return (float)s;
+    std::vector<double> g(pairs, 0.0);
+    for (int p = 0; p < pairs; p++)
+        for (int i = 0; i < nb; i++) g[p] += h[(size_t)p * nb + i];
+    if (diag) {
+        for (int l = 0; l < L; l++) out[l] = (float)g[l];
+        return L;
+    }
+    int n = 0;  // g(r, c) at r * L + c: sum_p b(r, p) fq(c, p)
+    for (int c = 0; c < L; c++)
+        for (int r = c; r < L; r++, n++) out[n] = (float)(g[(size_t)c * L + r] + (r != c ? g[(size_t)r * L + c] : 0.0));
+    return n;
+}
+
+int Model::n_parameters(int k) const {
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+    const int c = terms[k]->compat;
+    return c == kPotts ? 1 : c == kDiagonal ? L : L * (L + 1) / 2;
+}
+
+// parameters() (src/labelcompatibility.cpp:64-68, 88-90, 109-115).
+int Model::parameters(int k, float* out) const {
+    const int n = n_parameters(k);
+    const Term& t = *terms[k];
+    if (t.compat == kPotts) {
+        out[0] = t.w;
+    } else if (t.compat == kDiagonal) {
+        for (int l = 0; l < L; l++) out[l] = t.hcw[l];
+    } else {
+        int q = 0;
+        for (int c = 0; c < L; c++)
+            for (int r = c; r < L; r++) out[q++] = t.hcw[(size_t)c * L + r];
+    }
+    return n;
+}
+
+// setParameters(v) (src/labelcompatibility.cpp:69-71, 91-93, 116-122).
+void Model::set_parameters(int k, const float* v) {
+    const int kind = terms.at(k)->compat;
+    if (kind != kMatrix) {
+        set_compat(k, kind, v);
+        return;
+    }
+    std::vector<float> m((size_t)L * L);
+    for (int c = 0, q = 0; c < L; c++)
+        for (int r = c; r < L; r++, q++) m[(size_t)c * L + r] = m[(size_t)r * L + c] = v[q];
+    set_compat(k, kMatrix, m.data());  // already symmetric: the symmetrisation is exact
 }
 
 void Model::set_cliques(int R_, const int* off, const int* idx, const float* expw, const float* cst) {
@@ -273,27 +384,91 @@ void Model::set_cliques(int R_, const int* off, const int* idx, const float* exp
     sync();  // host vectors above are the caller's; finish the copies
 }
 
+// The term's compatibility as a slice epilogue.  Potts: -w v; Diagonal:
+// w_l v (both folded into the slice, with the base accumulation).  Matrix:
+// the slice writes the filtered values to a scratch buffer and `finish` runs
+// the L x L product with the base accumulation; the caller's epilogue fields
+// are returned through `ep` and `*dst` redirected.
+namespace {
+struct CompatRoute {
+    float* slice_out;   // where the slice writes
+    bool matrix;        // a matrix pass follows
+};
+}  // namespace
+
+static CompatRoute route_compat(Model& m, const Term& t, SliceEpilogue& ep, float* out, const float* base,
+                                float coef, bool zero_base, bool potts_only = false) {
+    ep.potts = true;
+    const int kind = potts_only ? (int)kPotts : t.compat;
+    if (kind == kMatrix) {
+        ep.scale = 1.0f;
+        return {m.compat_tmp.ensure((size_t)m.N * m.L), true};
+    }
+    if (kind == kDiagonal) {
+        ep.scale = 1.0f;
+        ep.scale_vec = t.cw.get();
+    } else {
+        ep.scale = -t.w;
+    }
+    ep.base = base;
+    ep.coef = coef;
+    ep.zero_base = zero_base;
+    return {out, false};
+}
+
+static void finish_compat(Model& m, const Term& t, const CompatRoute& r, float* out, const float* base, float coef,
+                          bool zero_base) {
+    if (!r.matrix) return;
+    const long NL = (long)m.N * m.L;
+    launch(matrix_compat_kernel, ceil_div(NL, 256), 256, 0, m.stream, NL, m.L, t.cw.get(),
+           (const float*)r.slice_out, base, coef, (int)zero_base, out);
+    DCRF_LAUNCH_CHECK();
+}
+
+void Model::set_compat(int k, int kind, const float* params) {
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+    Term& t = *terms[k];
+    // Every compatibility's parameters()(0) is also the weight of the term's
+    // unnormalised Potts twin (no_norm_pairwise_, src/densecrf.cpp:161-168):
+    // Potts w, Diagonal w_0, Matrix w_(0,0).
+    t.w = params[0];
+    if (kind == kPotts) {
+        t.compat = kPotts;
+        return;
+    }
+    require(kind == kDiagonal || kind == kMatrix, DCRF_E_ARG, "unknown label compatibility");
+    std::vector<float> h;
+    if (kind == kDiagonal) {
+        h.assign(params, params + L);
+    } else {  // MatrixCompatibility(m): w_ = 0.5 (m + m^T) (src/labelcompatibility.cpp:99-101)
+        h.resize((size_t)L * L);
+        for (int c = 0; c < L; c++)
+            for (int r = 0; r < L; r++) h[(size_t)c * L + r] = (params[(size_t)c * L + r] + params[(size_t)r * L + c]) * 0.5f;
+    }
+    t.hcw = h;
+    float* d = t.cw.ensure(h.size());
+    DCRF_CUDA(cudaMemcpyAsync(d, h.data(), sizeof(float) * h.size(), cudaMemcpyHostToDevice, stream));
+    sync();
+    t.compat = kind;
+}
+
 void Model::apply(int k, bool nonorm, float* out, const float* in, const float* base, float coef,
                   bool zero_base) {
     Term& t = *terms[k];
     SliceEpilogue ep;
-    ep.potts = true;
     ep.norm = nonorm ? nullptr : t.norm.get();
-    ep.scale = -t.w;
-    ep.base = base;
-    ep.coef = coef;
-    ep.zero_base = zero_base;
-    t.lat->compute(out, in, L, false, ep, nonorm ? nullptr : t.norm.get());
+    // nonorm: the unnormalised Potts twin of the term, whatever its compatibility
+    const CompatRoute r = route_compat(*this, t, ep, out, base, coef, zero_base, nonorm);
+    t.lat->compute(r.slice_out, in, L, false, ep, nonorm ? nullptr : t.norm.get());
+    finish_compat(*this, t, r, out, base, coef, zero_base);
 }
 
 void Model::apply_ord(int k, float* out, const float* rq, const float* base, bool zero_base) {
     Term& t = *terms[k];
     SliceEpilogue ep;
-    ep.potts = true;
-    ep.scale = -t.w;
-    ep.base = base;
-    ep.zero_base = zero_base;
-    t.lat->compute_ord(out, rq, L, ep);
+    const CompatRoute r = route_compat(*this, t, ep, out, base, 1.0f, zero_base);
+    t.lat->compute_ord(r.slice_out, rq, L, ep);
+    finish_compat(*this, t, r, out, base, 1.0f, zero_base);
 }
 
 // sa = sum_k apply_upper_minus_lower_ord_k(rescale(Q)) from shared bins, the
@@ -329,11 +504,11 @@ void Model::apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap) {
     if (nt >= 2) DCRF_CUDA(cudaStreamWaitEvent(stream, ev_side_join, 0));
     for (int k = 0; k < nt; k++) {
         SliceEpilogue ep;
-        ep.potts = true;
-        ep.scale = -terms[k]->w;
-        ep.base = k == 0 ? nullptr : sa;
-        ep.zero_base = k == 0;
-        terms[k]->lat->ord_slice(sa, bins, L, ep, k == nt - 1 ? gap : nullptr);
+        const Term& t = *terms[k];
+        const float* base = k == 0 ? nullptr : sa;
+        const CompatRoute r = route_compat(*this, t, ep, sa, base, 1.0f, k == 0);
+        terms[k]->lat->ord_slice(r.slice_out, bins, L, ep, k == nt - 1 && !r.matrix ? gap : nullptr);
+        finish_compat(*this, t, r, sa, base, 1.0f, k == 0);
     }
 }
 
@@ -341,11 +516,9 @@ void Model::apply_ord_bins(int k, float* out, const float2* bins, const float* b
                            const GapFusion* gap) {
     Term& t = *terms[k];
     SliceEpilogue ep;
-    ep.potts = true;
-    ep.scale = -t.w;
-    ep.base = base;
-    ep.zero_base = zero_base;
-    t.lat->compute_ord_bins(out, bins, L, ep, gap);
+    const CompatRoute r = route_compat(*this, t, ep, out, base, 1.0f, zero_base);
+    t.lat->compute_ord_bins(r.slice_out, bins, L, ep, r.matrix ? nullptr : gap);
+    finish_compat(*this, t, r, out, base, 1.0f, zero_base);
 }
 
 void Model::check_unit_range(const float* Q) {

@@ -10,8 +10,14 @@
 
 namespace dcrf {
 
+// Label compatibility of a pairwise term (include/labelcompatibility.h).
+enum CompatKind { kPotts = 0, kDiagonal = 1, kMatrix = 2 };
+
 struct Term {
     std::unique_ptr<Lattice> lat;
+    int compat = kPotts;  // Potts: mu = -w [a == b]; Diagonal: cw[L]; Matrix: cw[L x L], symmetrised
+    DevBuf<float> cw;
+    std::vector<float> hcw;  // host copy of cw
     DevBuf<float> norm;  // 1/sqrt(K 1 + 1e-20) (src/pairwise.cpp:46-50)
     DevBuf<float> feat;  // the features [N][d] (DenseKernel::f_), for the kernel gradient
     float w = 0.0f;      // Potts weight
@@ -79,11 +85,21 @@ struct Model {
     void apply(int k, bool nonorm, float* out, const float* in, const float* base = nullptr,
                float coef = 1.0f, bool zero_base = false);
     void apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap);
+    // Replaces term k's Potts compatibility: kDiagonal (params: L weights)
+    // or kMatrix (params: L x L column-major, used as 0.5 (m + m^T)).
+    void set_compat(int k, int kind, const float* params);
+    DevBuf<float> compat_tmp;
     // pairwise_[k]->kernelGradient(b, Q) (d floats: the diagonal kernel's
     // feature-scale gradient) and ->gradient(b, Q) (the Potts weight's);
     // b, Q device [N][L], results to host.
     void kernel_gradient(int k, const float* b, const float* Q, float* out);
-    float weight_gradient(int k, const float* b, const float* Q);
+    // LabelCompatibility::parameters / setParameters / gradient of term k:
+    // 1 (Potts), L (Diagonal) or L (L + 1) / 2 (Matrix, upper triangle by
+    // column) values; each returns that count.
+    int n_parameters(int k) const;
+    int parameters(int k, float* out) const;
+    void set_parameters(int k, const float* v);
+    int compat_gradient(int k, const float* b, const float* Q, float* out);
     void apply_ord_bins(int k, float* out, const float2* bins, const float* base, bool zero_base,
                         const GapFusion* gap);
     void apply_ord(int k, float* out, const float* rq, const float* base = nullptr,

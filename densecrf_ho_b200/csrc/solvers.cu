@@ -1305,7 +1305,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             }
             // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; the
             // dual-gap sums ride along the last term's slice.
-            const bool fuse_gap = nt > 0;
+            const bool fuse_gap = nt > 0 && terms[nt - 1]->compat != kMatrix;
             GapFusion gf{alpha, u, Q, part, R > 0 ? su : nullptr};
             apply_ord_sum(sa, bins, fuse_gap ? &gf : nullptr);
             if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));

@@ -159,6 +159,16 @@ dcrf_status dcrf_model_add_bilateral(dcrf_model m, float sx, float sy, float sr,
 /* addPairwiseEnergy(features, new PottsCompatibility(w), DIAG_KERNEL,
  * NORMALIZE_SYMMETRIC) (src/densecrf.cpp:157-169); features [N][d]. */
 dcrf_status dcrf_model_add_pairwise(dcrf_model m, const float* features, int d, float w_potts);
+/* The label compatibility of pairwise term k (the LabelCompatibility passed to
+ * addPairwise*, include/labelcompatibility.h): kind 0 PottsCompatibility
+ * (params[0] = w), 1 DiagonalCompatibility (params[0..L): w_l), 2
+ * MatrixCompatibility (params: L x L column-major m, used as 0.5 (m + m^T),
+ * src/labelcompatibility.cpp:79-129).  A term starts as the Potts weight it
+ * was added with. */
+#define DCRF_COMPAT_POTTS 0
+#define DCRF_COMPAT_DIAGONAL 1
+#define DCRF_COMPAT_MATRIX 2
+dcrf_status dcrf_model_set_compat(dcrf_model m, int k, int kind, const float* params);
 /* The clique state that addSuperPixel (src/densecrf.cpp:193-251) leaves in
  * super_pixel_container_, exp_of_superpixels_ and constants_, supplied
  * directly: R cliques, pixel ids idx[offsets[r] .. offsets[r+1]), their
@@ -201,11 +211,17 @@ dcrf_status dcrf_model_lr_qp_value(dcrf_model m, const float* Q, double* energy)
 /* pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 90-122,
  * 170-181): the gradient of the diagonal kernel's feature scales, d floats
  * (d = 2 Gaussian, 5 bilateral; d is returned when not NULL; grad holds
- * at least 16 floats), and pairwise_[k]->gradient(b, Q)
- * (:390-395): the Potts weight's, 1 float.  b, Q [N][L]. */
+ * at least 16 floats), and pairwise_[k]->gradient(b, Q) (:390-395): the
+ * compatibility's gradient, as many floats as its parameters.  b, Q [N][L]. */
 dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model m, int k, const float* b, const float* Q,
                                                 float* grad, int* d);
 dcrf_status dcrf_model_pairwise_gradient(dcrf_model m, int k, const float* b, const float* Q, float* grad);
+/* pairwise_[k]->parameters() / setParameters(v) (src/pairwise.cpp:384-389,
+ * src/labelcompatibility.cpp:64-71, 88-93, 109-122): Potts 1 value, Diagonal
+ * L, Matrix L (L + 1) / 2 (w_(i, j), j >= i, by column i).  *n receives the
+ * count when not NULL; params may be NULL to query it. */
+dcrf_status dcrf_model_pairwise_parameters(dcrf_model m, int k, float* params, int* n);
+dcrf_status dcrf_model_pairwise_set_parameters(dcrf_model m, int k, const float* params);
 /* Number of pairwise terms, and vertex count of term k's lattice. */
 dcrf_status dcrf_model_info(dcrf_model m, int* n_terms, int* N, int* L);
 dcrf_status dcrf_model_lattice_size(dcrf_model m, int k, int* M);

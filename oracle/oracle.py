@@ -124,6 +124,9 @@ def ref_lib():
         L.refm_new.restype = vp
         L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         L.refm_kernel_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
+        L.refm_parameters.argtypes = [vp, C.c_int, _f32p]
+        L.refm_add_gaussian_compat.argtypes = [vp, C.c_float, C.c_float, C.c_int, _f32p]
+        L.refm_add_bilateral_compat.argtypes = [vp] + [C.c_float] * 5 + [_u8p, C.c_int, _f32p]
         L.refm_weight_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
         L.refm_free.argtypes = [vp]
         L.refm_add_gaussian.argtypes = [vp, C.c_float, C.c_float, C.c_float]
@@ -302,9 +305,15 @@ class _Model:
         n = self._lib.refm_kernel_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
         return out[:n]
 
+    def parameters(self, k):
+        """pairwise_[k]->parameters() (reference model only)."""
+        out = np.zeros(self.L * (self.L + 1) // 2 + 1, np.float32)
+        n = self._lib.refm_parameters(self._h, k, out)
+        return out[:n]
+
     def weight_gradient(self, k, b, Q):
-        """pairwise_[k]->gradient(b, Q): the Potts weight's gradient (reference model only)."""
-        out = np.zeros(16, np.float32)
+        """pairwise_[k]->gradient(b, Q): the compatibility's gradient (reference model only)."""
+        out = np.zeros(self.L * (self.L + 1) // 2 + 16, np.float32)
         n = self._lib.refm_weight_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
         return out[:n]
 
@@ -359,6 +368,17 @@ class ReferenceModel(_Model):
         buf = _c(rgb, np.uint8).copy()
         return self._lib.refm_add_superpixel(self._h, buf, spatial, rng, min_region, constant,
                                              normaliser)
+
+    def add_gaussian_compat(self, sx, sy, kind, params):
+        """addPairwiseGaussian with a Diagonal (kind 1, L weights) or Matrix
+        (kind 2, L x L, column-major) compatibility."""
+        self._lib.refm_add_gaussian_compat(self._h, sx, sy, kind, _c(params, np.float32))
+        self.nterms += 1
+
+    def add_bilateral_compat(self, sx, sy, sr, sg, sb, rgb, kind, params):
+        self._lib.refm_add_bilateral_compat(self._h, sx, sy, sr, sg, sb, _c(rgb, np.uint8), kind,
+                                            _c(params, np.float32))
+        self.nterms += 1
 
     def get_cliques(self):
         R = self._lib.refm_num_cliques(self._h)

@@ -54,6 +54,7 @@ struct RefModel : public DenseCRF2D {
     VectorXf weight_gradient(int k, const MatrixXf& b, const MatrixXf& Q) const {
         return pairwise_[k]->gradient(b, Q);
     }
+    VectorXf parameters(int k) const { return pairwise_[k]->parameters(); }
     int N() const { return N_; }
     int L() const { return M_; }
     int R() const { return R_; }
@@ -227,6 +228,22 @@ void refm_add_features(void* h, const float* f, int d, float w) {
     MatrixXf F = Map<const MatrixXf>(f, d, m->N());
     m->addPairwiseEnergy(F, new PottsCompatibility(w));
 }
+// Gaussian / bilateral term with a Diagonal (kind 1, params[L]) or Matrix
+// (kind 2, params[L*L] column-major) compatibility.
+static LabelCompatibility* make_compat(int kind, const float* params, int L) {
+    if (kind == 1) return new DiagonalCompatibility(Map<const VectorXf>(params, L));
+    if (kind == 2) return new MatrixCompatibility(Map<const MatrixXf>(params, L, L));
+    return new PottsCompatibility(params[0]);
+}
+void refm_add_gaussian_compat(void* h, float sx, float sy, int kind, const float* params) {
+    RefModel* m = (RefModel*)h;
+    m->addPairwiseGaussian(sx, sy, make_compat(kind, params, m->L()));
+}
+void refm_add_bilateral_compat(void* h, float sx, float sy, float sr, float sg, float sb, const unsigned char* rgb,
+                               int kind, const float* params) {
+    RefModel* m = (RefModel*)h;
+    m->addPairwiseBilateral(sx, sy, sr, sg, sb, rgb, make_compat(kind, params, m->L()));
+}
 int refm_add_superpixel(void* h, unsigned char* rgb, int sr, int rr, int minreg, float c, float nrm) {
     RefModel* m = (RefModel*)h;
     int before = m->R();
@@ -324,6 +341,11 @@ int refm_weight_gradient(void* h, int k, const float* b, const float* Q, float* 
     VectorXf g = m->weight_gradient(k, B, QQ);
     std::memcpy(out, g.data(), sizeof(float) * g.size());
     return (int)g.size();
+}
+int refm_parameters(void* h, int k, float* out) {
+    VectorXf p = ((RefModel*)h)->parameters(k);
+    std::memcpy(out, p.data(), sizeof(float) * p.size());
+    return (int)p.size();
 }
 double refm_energy_ho(void* h, const short* labels) {
     RefModel* m = (RefModel*)h;

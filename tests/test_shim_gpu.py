@@ -67,4 +67,17 @@ def test_cpp_shim_matches_c_abi(tmp_path):
     assert np.array_equal(load("pw"), pw.pairwise_apply(0, Q))
 
     assert lines["range_error"] == "Value out of bounds"
-    assert lines["compat_error"] == "ok"
+    assert lines["kernel_error"] == "ok"
+
+    dg = -(2.0 + np.float32(0.1) * np.arange(L, dtype=np.float32))
+    a, b = np.mgrid[0:L, 0:L]
+    mt = np.where(a == b, np.float32(-5.0), np.float32(0.1) * (a + 2 * b).astype(np.float32) / np.float32(L))
+    m2 = DenseCRF2D(W, H, L)
+    m2.setUnaryEnergy(unary)
+    m2.addPairwiseGaussian(3.0, 3.0, 1.0)
+    m2.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, rgb, 1.0)
+    m2.setCompatibility(0, diagonal=dg.astype(np.float32))
+    m2.setCompatibility(1, matrix=mt.astype(np.float32))
+    qpc = m2.qp_inference_super_pixels_non_convex(m2.unary_init())
+    assert np.array_equal(load("qpc"), qpc)
+    assert float(lines["compat_energy"]) == pytest.approx(m2.assignment_energy_true(m2.currentMap(qpc)), rel=1e-9)

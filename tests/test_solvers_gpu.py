@@ -182,3 +182,83 @@ def test_kernel_and_weight_gradients_vs_reference():
         assert np.abs(kg - ref).max() <= 1e-4 * np.abs(ref).max(), (k, kg, ref)
         wg = m.pairwise_gradient(k, g["b"], g["Q"])
         assert abs(wg[0] - g[f"wgrad{k}"][0]) <= 1e-5 * abs(g[f"wgrad{k}"][0])
+
+
+@pytest.mark.parametrize("name", golden_names("compat_"))
+def test_label_compatibilities_vs_reference(name):
+    """DiagonalCompatibility and MatrixCompatibility terms against the
+    reference's own values (tests/golden/make_compat_golden.py).  Diagonal
+    folds into the slice epilogue and stays bit-exact; Matrix is an L x L
+    product per pixel after the filter, summed in order where Eigen's GEMM
+    blocks it: 1e-5 of the largest magnitude.  The unnormalised twin of every
+    term is Potts with parameters()(0) in both."""
+    g = golden(name)
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    m = DenseCRF2D(W, H, L)
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 1.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 1.0)
+    exact = int(g["kind"]) == 1
+    for k, p in enumerate((g["p0"], g["p1"])):
+        if exact:
+            m.setCompatibility(k, diagonal=p)
+        else:
+            m.setCompatibility(k, matrix=p.reshape(L, L).T)   # p is column-major
+
+    def close(a, b, tol=1e-5):
+        if exact:
+            return _eq(a, b)
+        return np.abs(a - b).max() <= tol * np.abs(b).max()
+
+    Q = g["unary_init"]   # the reference's exp: unary_init itself agrees to a few ulp
+    assert np.abs(m.unary_init().view(np.int32) - Q.view(np.int32)).max() <= 8
+    rq = (Q - Q.min()) / (Q - Q.min()).max()
+    for k in range(2):
+        assert close(m.pairwise_apply(k, Q), g[f"apply{k}"]), k
+        assert _eq(m.pairwise_apply(k, Q, nonorm=True), g[f"apply{k}_nonorm"]), k
+        assert close(m.pairwise_apply_upper_minus_lower_ord(k, rq), g[f"ord{k}"]), k
+    for k in range(2):
+        assert np.array_equal(m.pairwise_parameters(k), g[f"params{k}"]), k
+        kg, ref = m.pairwise_kernel_gradient(k, g["b"], Q), g[f"kgrad{k}"]
+        assert np.abs(kg - ref).max() <= 1e-4 * np.abs(ref).max(), (k, kg, ref)
+        wg, ref = m.pairwise_gradient(k, g["b"], Q), g[f"wgrad{k}"]
+        assert wg.shape == ref.shape
+        assert np.abs(wg - ref).max() <= 1e-4 * np.abs(ref).max(), (k, wg, ref)
+    lab = m.currentMap(Q)
+    assert _eq(lab, g["map"])
+    rel = 1e-12 if exact else 1e-6
+    assert m.assignment_energy_true(lab) == pytest.approx(float(g["e_true"]), rel=1e-12)
+    assert m.compute_energy_LP_higher_order(Q) == pytest.approx(float(g["e_lp"]), rel=rel)
+    assert m.compute_LR_QP_value(Q) == pytest.approx(float(g["e_lrqp"]), rel=rel)
+    out, st = m.qp_inference_super_pixels_non_convex(Q, max_iter=20, stats=True)
+    assert st.iterations == int(g["qp_iters"])
+    assert close(out, g["qp"], 1e-4)
+    assert st.energy == pytest.approx(float(g["qp_energies"][-1]), rel=rel)
+    out = m.lp_inference_prox_super_pixels(Q, prox_max_iter=3, fw_max_iter=4)
+    assert (m.currentMap(out) == m.currentMap(g["lp"])).mean() >= 0.999
+    assert np.abs(out - g["lp"]).max() < 1e-3
+
+
+def test_compatibility_argument_errors():
+    m = DenseCRF2D(8, 6, 4)
+    m.setUnaryEnergy(np.zeros((48, 4), np.float32))
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    with pytest.raises(DCRFError):
+        m.setCompatibility(0, diagonal=np.ones(3, np.float32))
+    with pytest.raises(DCRFError):
+        m.setCompatibility(0, matrix=np.ones((4, 3), np.float32))
+    with pytest.raises(DCRFError):
+        m.setCompatibility(1, diagonal=np.ones(4, np.float32))
+    with pytest.raises(DCRFError):
+        m.pairwise_set_parameters(0, np.ones(2, np.float32))
+    assert np.array_equal(m.pairwise_parameters(0), [3.0])
+    m.setCompatibility(0, diagonal=np.arange(4, dtype=np.float32))
+    assert np.array_equal(m.pairwise_parameters(0), np.arange(4))
+    mat = np.arange(16, dtype=np.float32).reshape(4, 4)
+    m.setCompatibility(0, matrix=mat)
+    sym = 0.5 * (mat + mat.T)
+    packed = np.concatenate([sym[i, i:] for i in range(4)])
+    assert np.array_equal(m.pairwise_parameters(0), packed)
+    m.pairwise_set_parameters(0, packed[::-1].copy())
+    assert np.array_equal(m.pairwise_parameters(0), packed[::-1])
