@@ -78,6 +78,23 @@ class Permutohedral:
                                              x.ctypes.data_as(C.c_void_p), x.shape[1]))
         return out
 
+    def compute_upper_minus_lower_ord_restricted(self, rQ, pI, Q=None, store=True):
+        """``compute_upper_minus_lower_ord_restricted(rout, rQ, pI, Q, store)``:
+        the ordered filter at the pixels pI (strictly ascending) with values
+        rQ [len(pI), L]; the other pixels splat Q [N, L] (store) or the splat
+        kept by the last store call (store=False)."""
+        pi = np.ascontiguousarray(pI, np.int32).reshape(-1)
+        x = _f32(rQ)
+        L = x.shape[1] if x.ndim == 2 else _f32(Q).shape[1]
+        x = x.reshape(pi.size, L)
+        out = np.zeros((pi.size, L), np.float32)
+        q = _f32(Q) if store else None
+        check(lib().dcrf_lattice_compute_ord_restricted(
+            self._h, out.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p),
+            pi.ctypes.data_as(C.c_void_p), int(pi.size), None if q is None else q.ctypes.data_as(C.c_void_p),
+            int(L), int(bool(store))))
+        return out
+
     def gradient(self, a, b):
         """``df [N, d]`` = d(a^T K b) / d(features) (``Permutohedral::gradient``)."""
         a, b = _f32(a), _f32(b)
@@ -131,6 +148,45 @@ class DenseCRF2D:
     def setUnaryEnergy(self, unary):
         u = self._mat(unary)
         check(lib().dcrf_model_set_unary(self._h, u.ctypes.data_as(C.c_void_p)))
+
+    def setUnaryEnergyLogistic(self, weights, features):
+        """``setUnaryEnergy(new LogisticUnaryEnergy(W, f))``: weights W [L][F],
+        features f [N][F]; the unary is W f."""
+        w = np.asarray(weights, np.float32)
+        if w.ndim != 2 or w.shape[0] != self.L:
+            raise DCRFError(1, "weights must be L x F")
+        F = w.shape[1]
+        f = _f32(features, (self.N, F))
+        wc = np.ascontiguousarray(w.T)  # column-major W
+        check(lib().dcrf_model_set_unary_logistic(self._h, wc.ctypes.data_as(C.c_void_p),
+                                                  f.ctypes.data_as(C.c_void_p), F))
+
+    def unary_parameters(self):
+        """``unary_->parameters()`` as W [L][F] (empty for a constant unary)."""
+        n = C.c_int(0)
+        check(lib().dcrf_model_unary_parameters(self._h, None, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        check(lib().dcrf_model_unary_parameters(self._h, out.ctypes.data_as(C.c_void_p), None))
+        return out.reshape(-1, self.L).T if n.value else out
+
+    def unary_set_parameters(self, weights):
+        """``unary_->setParameters(W)``, W [L][F]; the unary is recomputed."""
+        w = np.ascontiguousarray(np.asarray(weights, np.float32).T)
+        if w.size != self.unary_parameters().size:
+            raise DCRFError(1, "wrong number of unary parameters")
+        check(lib().dcrf_model_unary_set_parameters(self._h, w.ctypes.data_as(C.c_void_p)))
+
+    def unary_gradient(self, b):
+        """``unary_->gradient(b)`` = b f^T as [L][F] (empty for a constant unary)."""
+        bb = self._mat(b)
+        n = C.c_int(0)
+        check(lib().dcrf_model_unary_gradient(self._h, bb.ctypes.data_as(C.c_void_p), None, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        if n.value:
+            check(lib().dcrf_model_unary_gradient(self._h, bb.ctypes.data_as(C.c_void_p),
+                                                  out.ctypes.data_as(C.c_void_p), None))
+            return out.reshape(-1, self.L).T
+        return out
 
     def addPairwiseGaussian(self, sx, sy, w):
         check(lib().dcrf_model_add_gaussian(self._h, C.c_float(sx), C.c_float(sy), C.c_float(w)))
@@ -202,6 +258,19 @@ class DenseCRF2D:
         out = self._new()
         check(lib().dcrf_model_pairwise_apply_ord(self._h, k, out.ctypes.data_as(C.c_void_p),
                                                   x.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def pairwise_apply_upper_minus_lower_ord_restricted(self, k, rQ, pI, Q=None, store=True):
+        """``pairwise_[k]->apply_upper_minus_lower_ord_restricted(rout, rQ, pI,
+        Q, store)``: rQ, rout [len(pI), L]; Q [N, L] read on a store call."""
+        pi = np.ascontiguousarray(pI, np.int32).reshape(-1)
+        x = _f32(rQ).reshape(pi.size, self.L)
+        out = np.zeros((pi.size, self.L), np.float32)
+        q = self._mat(Q) if store else None
+        check(lib().dcrf_model_pairwise_apply_ord_restricted(
+            self._h, int(k), out.ctypes.data_as(C.c_void_p), x.ctypes.data_as(C.c_void_p),
+            pi.ctypes.data_as(C.c_void_p), int(pi.size), None if q is None else q.ctypes.data_as(C.c_void_p),
+            int(bool(store))))
         return out
 
     def qp_inference_super_pixels_non_convex(self, init, max_iter=0, stats=False):

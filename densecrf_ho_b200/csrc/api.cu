@@ -16,6 +16,7 @@ struct dcrf_lattice_s {
     dcrf::Lattice lat;
     cudaStream_t stream = nullptr;
     DevBuf<float> feat, in, out;
+    DevBuf<int> ipi;
 };
 
 struct dcrf_batch_s {
@@ -25,7 +26,8 @@ struct dcrf_batch_s {
 
 struct dcrf_model_s {
     dcrf::Model* m = nullptr;
-    DevBuf<float> io0, io1, feat;
+    DevBuf<float> io0, io1, io2, feat;
+    DevBuf<int> ipi;
     DevBuf<uint8_t> img;
     DevBuf<int16_t> lab;
 };
@@ -258,6 +260,46 @@ dcrf_status dcrf_lattice_compute_ord(dcrf_lattice h, float* out, const float* Q,
     });
 }
 
+namespace {
+// pI: 0 <= pI[i] < N, strictly ascending (the reference walks it in step with
+// the pixel loop); rQ (and Q for a store call) in [0, 1].
+void check_restricted(int N, int L, const int32_t* pI, int nP, const float* rQ, const float* Q, int store) {
+    if (nP < 0 || nP > N) throw Error(DCRF_E_ARG, "pI larger than the lattice");
+    if (nP) need(pI, "pI");
+    for (int i = 0; i < nP; i++)
+        if (pI[i] < 0 || pI[i] >= N || (i && pI[i] <= pI[i - 1]))
+            throw Error(DCRF_E_ARG, "pI must be strictly ascending pixel indices");
+    if (nP) need(rQ, "rQ");
+    for (size_t i = 0; i < (size_t)nP * L; i++)
+        if (!(rQ[i] >= 0.0f && rQ[i] <= 1.0f)) throw Error(DCRF_E_RANGE, "Value out of bounds");
+    if (store) {
+        need(Q, "Q");
+        for (size_t i = 0; i < (size_t)N * L; i++)
+            if (!(Q[i] >= 0.0f && Q[i] <= 1.0f)) throw Error(DCRF_E_RANGE, "Value out of bounds");
+    }
+}
+}  // namespace
+
+dcrf_status dcrf_lattice_compute_ord_restricted(dcrf_lattice h, float* rout, const float* rQ, const int32_t* pI,
+                                                int nP, const float* Q, int L, int store) {
+    return guard([&] {
+        need(h, "lattice");
+        if (h->lat.N == 0) throw Error(DCRF_E_STATE, "lattice not initialised");
+        if (L < 1) throw Error(DCRF_E_ARG, "L must be >= 1");
+        check_restricted(h->lat.N, L, pI, nP, rQ, Q, store);
+        if (nP) need(rout, "rout");
+        const size_t n = (size_t)nP * L;
+        const float* drq = n ? upload(h->in, rQ, n, h->stream) : nullptr;
+        const float* dq = store ? upload(h->feat, Q, (size_t)h->lat.N * L, h->stream) : nullptr;
+        const int* dpi = nP ? upload(h->ipi, pI, (size_t)nP, h->stream) : nullptr;
+        float* dout = h->out.ensure(std::max<size_t>(n, 1));
+        dcrf::SliceEpilogue ep;
+        h->lat.compute_ord_restricted(dout, drq, dpi, nP, dq, L, store != 0, ep);
+        if (n) download(rout, dout, n, h->stream);
+        else DCRF_CUDA(cudaStreamSynchronize(h->stream));
+    });
+}
+
 dcrf_status dcrf_lattice_export(dcrf_lattice h, int32_t* offset, int32_t* rank, float* bary, int16_t* keys,
                                 int32_t* nbr) {
     return guard([&] {
@@ -319,6 +361,7 @@ dcrf_status dcrf_model_set_unary_dev(dcrf_model h, const float* d_unary) {
         float* u = m.unary.ensure((size_t)m.N * m.L);
         DCRF_CUDA(cudaMemcpyAsync(u, d_unary, sizeof(float) * m.N * m.L, cudaMemcpyDeviceToDevice, m.stream));
         m.has_unary = true;
+        m.logit_F = 0;  // a constant unary replaces the unary energy
     });
 }
 
@@ -328,7 +371,45 @@ dcrf_status dcrf_model_set_unary(dcrf_model h, const float* unary) {
         need(unary, "unary");
         upload(m.unary, unary, (size_t)m.N * m.L, m.stream);
         m.has_unary = true;
+        m.logit_F = 0;  // a constant unary replaces the unary energy
         m.sync();
+    });
+}
+
+dcrf_status dcrf_model_set_unary_logistic(dcrf_model h, const float* weights, const float* features, int F) {
+    return guard([&] {
+        auto& m = M(h);
+        need(weights, "weights");
+        need(features, "features");
+        m.set_unary_logistic(weights, features, F);
+    });
+}
+
+dcrf_status dcrf_model_unary_parameters(dcrf_model h, float* params, int* n) {
+    return guard([&] {
+        auto& m = M(h);
+        if (n) *n = m.logit_F > 0 ? (int)m.h_logit_w.size() : 0;
+        if (params && m.logit_F > 0) std::copy(m.h_logit_w.begin(), m.h_logit_w.end(), params);
+    });
+}
+
+dcrf_status dcrf_model_unary_set_parameters(dcrf_model h, const float* params) {
+    return guard([&] {
+        auto& m = M(h);
+        if (m.logit_F == 0) return;
+        need(params, "params");
+        m.set_unary_parameters(params);
+    });
+}
+
+dcrf_status dcrf_model_unary_gradient(dcrf_model h, const float* b, float* grad, int* n) {
+    return guard([&] {
+        auto& m = M(h);
+        need(b, "b");
+        if (n) *n = m.L * m.logit_F;
+        if (m.logit_F == 0 || !grad) return;  // grad NULL: query the count
+        const float* db = upload(h->io0, b, (size_t)m.N * m.L, m.stream);
+        m.unary_gradient(db, grad);
     });
 }
 
@@ -459,6 +540,24 @@ dcrf_status dcrf_model_pairwise_apply_ord(dcrf_model h, int k, float* out, const
         float* dout = h->io1.ensure(n);
         m.apply_ord(k, dout, dq);
         download(out, dout, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply_ord_restricted(dcrf_model h, int k, float* rout, const float* rQ,
+                                                     const int32_t* pI, int nP, const float* Q, int store) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        check_restricted(m.N, m.L, pI, nP, rQ, Q, store);
+        if (nP) need(rout, "rout");
+        const size_t n = (size_t)nP * m.L;
+        const float* drq = n ? upload(h->io0, rQ, n, m.stream) : nullptr;
+        const float* dq = store ? upload(h->io2, Q, (size_t)m.N * m.L, m.stream) : nullptr;
+        const int* dpi = nP ? upload(h->ipi, pI, (size_t)nP, m.stream) : nullptr;
+        float* dout = h->io1.ensure(std::max<size_t>(n, 1));
+        m.apply_ord_restricted(k, dout, drq, dpi, nP, dq, store != 0);
+        if (n) download(rout, dout, n, m.stream);
+        else DCRF_CUDA(cudaStreamSynchronize(m.stream));
     });
 }
 

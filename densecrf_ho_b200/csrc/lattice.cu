@@ -1530,4 +1530,172 @@ void Lattice::ord_slice(float* out, const float2* bins, int L, const SliceEpilog
     DCRF_LAUNCH_CHECK();
 }
 
+
+// ---------------------------------------------------------------------------
+// The restricted ordered filter (seqCompute_upper_minus_lower_ord_restricted,
+// src/permutohedral.cpp:702-900).
+//
+// Splat, per (vertex, label) and both passes: the vertex's list in pixel
+// order, first the pixels outside pI with their Q values (only in a store
+// call; the sums are then kept), then the pixels of pI with their rQ values.
+// That is the reference's order per bin: its outside-pI loop runs over all
+// pixels before its pI loop.
+__global__ void ord_splat_restricted_kernel(int M, int L, const int* __restrict__ seg_start,
+                                            const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                                            const int* __restrict__ pos, const float2* __restrict__ ebins,
+                                            const float2* __restrict__ rbins, float* __restrict__ stored,
+                                            float* __restrict__ vals, unsigned char* __restrict__ active, int store) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * L) return;
+    const int v = (int)(t / L), k = (int)(t - (long)v * L);
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    const long rowoff = (long)(v + 1) * kOrdW * L + k;
+    unsigned long long acc[kRes];  // (lower, upper) sums of bin b
+    if (store) {
+#pragma unroll
+        for (int b = 0; b < kRes; b++) acc[b] = 0ull;
+        bool any = false;
+        for (int s = s0; s < s1; s++) {
+            const int p = seg_pix[s];
+            if (pos[p] >= 0) {
+                any = true;
+                continue;
+            }
+            const float2 x = ebins[(long)p * L + k];
+            const float w = seg_w[s];
+            const unsigned long long w2 = pack2(w, w);
+#pragma unroll
+            for (int b = 0; b < kRes; b++) ord_step2(acc[b], x.x, x.y, (float)b, w2);
+        }
+#pragma unroll
+        for (int b = 0; b < kRes; b++) {
+            const float2 r = unpack2(acc[b]);
+            stored[rowoff + (long)b * L] = r.x;
+            stored[rowoff + (long)(kRes + b) * L] = r.y;
+        }
+        if (k == 0) active[v] = any ? 1 : 0;
+    } else {
+#pragma unroll
+        for (int b = 0; b < kRes; b++)
+            acc[b] = pack2(stored[rowoff + (long)b * L], stored[rowoff + (long)(kRes + b) * L]);
+    }
+    for (int s = s0; s < s1; s++) {
+        const int ii = pos[seg_pix[s]];
+        if (ii < 0) continue;
+        const float2 x = rbins[(long)ii * L + k];
+        const float w = seg_w[s];
+        const unsigned long long w2 = pack2(w, w);
+#pragma unroll
+        for (int b = 0; b < kRes; b++) ord_step2(acc[b], x.x, x.y, (float)b, w2);
+    }
+#pragma unroll
+    for (int b = 0; b < kRes; b++) {
+        const float2 r = unpack2(acc[b]);
+        vals[rowoff + (long)b * L] = r.x;
+        vals[rowoff + (long)(kRes + b) * L] = r.y;
+    }
+}
+
+// Blur of the active vertices only; the others keep whatever their row of dst
+// holds (:773-789: the reference's two buffers swap after every axis, so an
+// inactive vertex reads as 0 after odd axes and as its splat after even ones).
+__global__ void ord_blur_active_kernel(int M, int row4, const int2* __restrict__ nbr,
+                                       const unsigned char* __restrict__ active, const float4* __restrict__ src,
+                                       float4* __restrict__ dst) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * row4) return;
+    const int v = (int)(t / row4), c = (int)(t - (long)v * row4);
+    if (!active[v]) return;
+    const int2 nb = nbr[v];
+    const float4 a = src[(long)(v + 1) * row4 + c];
+    const float4 p = src[(long)nb.x * row4 + c];
+    const float4 q = src[(long)nb.y * row4 + c];
+    float4 r;
+    r.x = fadd(a.x, fmul(0.5f, fadd(p.x, q.x)));
+    r.y = fadd(a.y, fmul(0.5f, fadd(p.y, q.y)));
+    r.z = fadd(a.z, fmul(0.5f, fadd(p.z, q.z)));
+    r.w = fadd(a.w, fmul(0.5f, fadd(p.w, q.w)));
+    dst[(long)(v + 1) * row4 + c] = r;
+}
+
+// Slice at the pI pixels (:791-802, :885-896), as ord_slice_kernel does for
+// every pixel; out [nP][L] starts from 0.
+__global__ void ord_slice_restricted_kernel(int nP, int L, int d, const int* __restrict__ pI,
+                                            const int* __restrict__ offset, const float* __restrict__ bary,
+                                            const float* __restrict__ vals, const float2* __restrict__ rbins,
+                                            float alpha, float* out, SliceEpilogue ep) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)nP * L) return;
+    const int ii = (int)(t / L), k = (int)(t - (long)ii * L);
+    const int i = pI[ii], d1 = d + 1;
+    const float2 bp = rbins[t];
+    const int cl = ord_lower_of(bp), cu = ord_upper_of(bp);
+    float acc = 0.0f;
+    for (int j = 0; j <= d; j++) {
+        const int o = offset[(long)i * d1 + j];
+        const float w = bary[(long)i * d1 + j];
+        acc = fadd(acc, fmul(vals[((long)(o + 1) * kOrdW + cl) * L + k], fmul(-w, alpha)));
+    }
+    for (int j = 0; j <= d; j++) {
+        const int o = offset[(long)i * d1 + j];
+        const float w = bary[(long)i * d1 + j];
+        acc = fadd(acc, fmul(vals[((long)(o + 1) * kOrdW + kRes + cu) * L + k], fmul(w, alpha)));
+    }
+    out[t] = apply_epilogue(acc, t, i, k, ep);
+}
+
+__global__ void scatter_pos_kernel(int nP, const int* __restrict__ pI, int* __restrict__ pos) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nP) pos[pI[t]] = t;
+}
+
+void Lattice::compute_ord_restricted(float* rout, const float* rQ, const int* pI, int nP, const float* Q, int L,
+                                     bool store, const SliceEpilogue& ep) {
+    require(L >= 1, DCRF_E_ARG, "compute_ord_restricted: L must be >= 1");
+    require(nP >= 0 && nP <= N, DCRF_E_ARG, "compute_ord_restricted: pI larger than the lattice");
+    require(store || r_L == L, DCRF_E_STATE,
+            "compute_ord_restricted: no stored splat for this label count (call with store first)");
+    require(!store || Q, DCRF_E_ARG, "compute_ord_restricted: store needs Q");
+    cudaStream_t st = stream;
+    const long row = (long)L * kOrdW, cells = (long)(M + 1) * row;
+    float* stored = r_stored.ensure((size_t)cells);
+    float* a = r_a.ensure((size_t)cells);
+    float* b = r_b.ensure((size_t)cells);
+    unsigned char* active = r_active.ensure((size_t)std::max(M, 1));
+    int* pos = r_pos.ensure((size_t)N);
+    float2* rb = r_bins.ensure((size_t)std::max<long>((long)nP * L, 1));
+    launch(fill_int_kernel, ceil_div(N, kTB), kTB, 0, st, (long)N, -1, pos);
+    if (nP) {
+        launch(scatter_pos_kernel, ceil_div(nP, kTB), kTB, 0, st, nP, pI, pos);
+        launch(ord_bins_kernel, ceil_div((long)nP * L, kTB), kTB, 0, st, (long)nP * L, rQ, rb);
+    }
+    const float2* eb = nullptr;
+    if (store) {
+        float2* e = r_ebins.ensure((size_t)N * L);
+        launch(ord_bins_kernel, ceil_div((long)N * L, kTB), kTB, 0, st, (long)N * L, Q, e);
+        eb = e;
+        r_L = 0;  // until this call has stored its splat
+    }
+    DCRF_CUDA(cudaMemsetAsync(a, 0, sizeof(float) * row, st));      // row 0: the absent neighbour
+    DCRF_CUDA(cudaMemsetAsync(b, 0, sizeof(float) * cells, st));    // new_values_ starts zeroed
+    if (M)
+        launch(ord_splat_restricted_kernel, ceil_div((long)M * L, kTB), kTB, 0, st, M, L, seg_start.get(),
+               seg_pix.get(), seg_w.get(), (const int*)pos, eb, (const float2*)rb, stored, a, active, (int)store);
+    float *src = a, *dst = b;
+    const int row4 = (int)(row / 4);
+    for (int j = 0; j <= d; j++) {
+        if (M)
+            launch(ord_blur_active_kernel, ceil_div((long)M * row4, kTB), kTB, 0, st, M, row4,
+                   nbr.get() + (long)j * M, (const unsigned char*)active, reinterpret_cast<const float4*>(src),
+                   reinterpret_cast<float4*>(dst));
+        std::swap(src, dst);
+    }
+    const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
+    if (nP)
+        launch(ord_slice_restricted_kernel, ceil_div((long)nP * L, kTB), kTB, 0, st, nP, L, d, pI, offset.get(),
+               bary.get(), (const float*)src, (const float2*)rb, alpha, rout, ep);
+    DCRF_LAUNCH_CHECK();
+    if (store) r_L = L;
+}
+
 }  // namespace dcrf

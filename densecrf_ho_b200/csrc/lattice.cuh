@@ -97,6 +97,19 @@ struct Lattice {
     void ord_slice(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
     const float* ord_vals = nullptr;
 
+    // compute_upper_minus_lower_ord_restricted: the ordered filter at the nP
+    // pixels pI (device array, strictly ascending) with values rQ [nP][L] ->
+    // rout [nP][L]; the other pixels splat their values Q [N][L] (store), or
+    // the splat stored by the last store call is reused with the vertex set
+    // of that call (store = false).
+    void compute_ord_restricted(float* rout, const float* rQ, const int* pI, int nP, const float* Q, int L,
+                                bool store, const SliceEpilogue& ep);
+    DevBuf<float> r_stored, r_a, r_b;  // [(M + 1)][20][L]: the stored splat, the blur's two buffers
+    DevBuf<unsigned char> r_active;    // vertices the pI pixels reach (store call)
+    DevBuf<int> r_pos;                 // pixel -> index in pI, or -1
+    DevBuf<float2> r_bins, r_ebins;    // bins of rQ and of Q
+    int r_L = 0;                       // label count of the stored splat (0: none)
+
     // Permutohedral::gradient: df [N][d] = d(a^T K b)/d(features); a, b [N][L].
     void gradient(float* df, const float* a, const float* b, int L);
 

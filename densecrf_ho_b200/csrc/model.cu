@@ -159,6 +159,39 @@ __global__ void label_outer_partial_kernel(int N, int L, const float* __restrict
     if (threadIdx.x == 0) part[(long)p * gridDim.x + blockIdx.x] = sm[0];
 }
 
+// LogisticUnaryEnergy::get: U(l, i) = sum_f W(l, f) F(f, i), summed over f in
+// order (Eigen's GEMM blocks the sum differently: float tolerance).
+__global__ void logistic_unary_kernel(long n, int L, int F, const float* __restrict__ W,
+                                      const float* __restrict__ feat, float* __restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const long i = t / L;
+    const int l = (int)(t - i * L);
+    const float* f = feat + i * F;
+    float r = fmul(W[l], f[0]);
+    for (int c = 1; c < F; c++) r = fadd(r, fmul(W[l + (long)c * L], f[c]));
+    out[t] = r;
+}
+
+// part[p * gridDim.x + blk]: this block's share of sum_i b(l, i) F(c, i) for
+// p = c * L + l (LogisticUnaryEnergy::gradient, b F^T).
+__global__ void logistic_grad_partial_kernel(int N, int L, int F, const float* __restrict__ b,
+                                             const float* __restrict__ feat, double* __restrict__ part) {
+    __shared__ double sm[256];
+    const int p = blockIdx.y;
+    const int c = p / L, l = p - c * L;
+    double acc = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (long)gridDim.x * blockDim.x)
+        acc += (double)fmul(b[i * L + l], feat[i * F + c]);
+    sm[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(long)p * gridDim.x + blockIdx.x] = sm[0];
+}
+
 __global__ void fill_ones_kernel(long n, float* x) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) x[t] = 1.0f;
@@ -306,6 +339,50 @@ int Model::compat_gradient(int k, const float* b, const float* Q, float* out) {
     for (int c = 0; c < L; c++)
         for (int r = c; r < L; r++, n++) out[n] = (float)(g[(size_t)c * L + r] + (r != c ? g[(size_t)r * L + c] : 0.0));
     return n;
+}
+
+// setUnaryEnergy(new LogisticUnaryEnergy(lw, lf)) (src/unary.cpp:47-52).
+void Model::set_unary_logistic(const float* lw, const float* lf, int F) {
+    require(F >= 1, DCRF_E_ARG, "logistic unary: F must be >= 1");
+    logit_F = F;
+    DCRF_CUDA(cudaMemcpyAsync(logit_f.ensure((size_t)F * N), lf, sizeof(float) * F * N, cudaMemcpyHostToDevice,
+                              stream));
+    set_unary_parameters(lw);
+}
+
+// LogisticUnaryEnergy::setParameters (:58-63); the unary is recomputed, as
+// get() recomputes it at every use.
+void Model::set_unary_parameters(const float* lw) {
+    if (logit_F == 0) return;  // UnaryEnergy::setParameters is a no-op
+    const size_t nw = (size_t)L * logit_F;
+    h_logit_w.assign(lw, lw + nw);
+    DCRF_CUDA(cudaMemcpyAsync(logit_w.ensure(nw), h_logit_w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice,
+                              stream));
+    const long NL = (long)N * L;
+    launch(logistic_unary_kernel, ceil_div(NL, 256), 256, 0, stream, NL, L, logit_F, (const float*)logit_w.get(),
+           (const float*)logit_f.get(), unary.ensure((size_t)NL));
+    DCRF_LAUNCH_CHECK();
+    has_unary = true;
+    sync();
+}
+
+// LogisticUnaryEnergy::gradient(b) = b f^T (:64-68); FP64 sums over pixels.
+int Model::unary_gradient(const float* b, float* out) {
+    if (logit_F == 0) return 0;  // UnaryEnergy::gradient: empty
+    const int F = logit_F, pairs = L * F, nb = 32;
+    double* part = partials.ensure((size_t)nb * pairs);
+    launch(logistic_grad_partial_kernel, dim3(nb, pairs), 256, 0, stream, N, L, F, b, (const float*)logit_f.get(),
+           part);
+    DCRF_LAUNCH_CHECK();
+    std::vector<double> h((size_t)nb * pairs);
+    DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
+    sync();
+    for (int p = 0; p < pairs; p++) {
+        double s = 0.0;
+        for (int i = 0; i < nb; i++) s += h[(size_t)p * nb + i];
+        out[p] = (float)s;
+    }
+    return pairs;
 }
 
 int Model::n_parameters(int k) const {
@@ -509,6 +586,20 @@ void Model::apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap) {
         const CompatRoute r = route_compat(*this, t, ep, sa, base, 1.0f, k == 0);
         terms[k]->lat->ord_slice(r.slice_out, bins, L, ep, k == nt - 1 && !r.matrix ? gap : nullptr);
         finish_compat(*this, t, r, sa, base, 1.0f, k == 0);
+    }
+}
+
+void Model::apply_ord_restricted(int k, float* rout, const float* rQ, const int* pI, int nP, const float* Q,
+                                 bool store) {
+    Term& t = *terms[k];
+    SliceEpilogue ep;
+    const CompatRoute r = route_compat(*this, t, ep, rout, nullptr, 1.0f, false);
+    t.lat->compute_ord_restricted(r.slice_out, rQ, pI, nP, Q, L, store, ep);
+    if (r.matrix && nP) {
+        const long n = (long)nP * L;
+        launch(matrix_compat_kernel, ceil_div(n, 256), 256, 0, stream, n, L, t.cw.get(), (const float*)r.slice_out,
+               (const float*)nullptr, 1.0f, 0, rout);
+        DCRF_LAUNCH_CHECK();
     }
 }
 

@@ -52,6 +52,11 @@ struct Model {
     cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
     bool has_unary = false;
     DevBuf<float> unary;
+    // LogisticUnaryEnergy (src/unary.cpp:47-70): unary = lw * lf, lw L x F and
+    // lf F x N, both column-major; logit_F = 0 for a constant unary.
+    int logit_F = 0;
+    DevBuf<float> logit_w, logit_f;
+    std::vector<float> h_logit_w;
     std::vector<std::unique_ptr<Term>> terms;
 
     // cliques (super_pixel_container_, exp_of_superpixels_, constants_)
@@ -96,6 +101,14 @@ struct Model {
     // LabelCompatibility::parameters / setParameters / gradient of term k:
     // 1 (Potts), L (Diagonal) or L (L + 1) / 2 (Matrix, upper triangle by
     // column) values; each returns that count.
+    // PairwisePotential::apply_upper_minus_lower_ord_restricted
+    // (src/pairwise.cpp:229-240): the term's restricted ordered filter and
+    // compatibility; rout, rQ [nP][L], pI (device) strictly ascending.
+    void apply_ord_restricted(int k, float* rout, const float* rQ, const int* pI, int nP, const float* Q,
+                              bool store);
+    void set_unary_logistic(const float* lw, const float* lf, int F);  // host arrays
+    void set_unary_parameters(const float* lw);
+    int unary_gradient(const float* b, float* out);  // b f^T, L x F column-major; returns L F
     int n_parameters(int k) const;
     int parameters(int k, float* out) const;
     void set_parameters(int k, const float* v);

@@ -88,6 +88,19 @@ dcrf_status dcrf_lattice_compute_noalloc(dcrf_lattice lat, float* d_out, const f
 /* Permutohedral::compute_upper_minus_lower_ord(MatrixXf& out, const MatrixXf& Q)
  * (src/permutohedral.cpp:1071-1073, 590-701): the 10-bin ordered filter. */
 dcrf_status dcrf_lattice_compute_ord(dcrf_lattice lat, float* out, const float* Q, int L);
+/* Permutohedral::compute_upper_minus_lower_ord_restricted(rout, rQ, pI, Q,
+ * store) (include/permutohedral.h:83-84, src/permutohedral.cpp:702-900,
+ * 1074-1078): the ordered filter evaluated at the nP pixels pI (strictly
+ * ascending), whose values are rQ [nP][L]; rout [nP][L].  The other pixels
+ * enter the splat with their values in Q [N][L]: a call with store != 0
+ * splats them and keeps that splat and the set of vertices the pI pixels
+ * reach; a call with store = 0 ignores Q and reuses both (DCRF_E_STATE
+ * without an earlier store call for this L).  The blur runs over that vertex
+ * set only, with the reference's alternating buffers.  rQ and, when read, Q
+ * must lie in [0, 1] (DCRF_E_RANGE).  The reference reads pI[nP] past its
+ * end after the last pI pixel; here the pixels after it are outside pI. */
+dcrf_status dcrf_lattice_compute_ord_restricted(dcrf_lattice lat, float* rout, const float* rQ, const int32_t* pI,
+                                                int nP, const float* Q, int L, int store);
 dcrf_status dcrf_lattice_compute_ord_dev(dcrf_lattice lat, float* d_out, const float* d_Q, int L);
 /* gradient(df, a, b, value_size) (include/permutohedral.h:86-87,
  * src/permutohedral.cpp:1095-1178): df [N][d] = d(a^T K b)/d(features) for
@@ -150,6 +163,17 @@ dcrf_status dcrf_model_destroy(dcrf_model m);
 /* setUnaryEnergy(const MatrixXf& unary) (src/densecrf.cpp:261): U [N][L]. */
 dcrf_status dcrf_model_set_unary(dcrf_model m, const float* unary);
 dcrf_status dcrf_model_set_unary_dev(dcrf_model m, const float* d_unary);
+/* setUnaryEnergy(new LogisticUnaryEnergy(W, f)) (include/unary.h:48-57,
+ * src/unary.cpp:47-70): weights W, L x F column-major; features f, F x N
+ * column-major ([N][F]); the unary is W f.  parameters() is W (L F values,
+ * column-major; *n = 0 for a constant unary), setParameters(v) replaces W and
+ * recomputes the unary, gradient(b) = b f^T (L F values, column-major; b
+ * [N][L]; *n = L F, 0 for a constant unary, whose gradient is empty; grad
+ * may be NULL to query the count). */
+dcrf_status dcrf_model_set_unary_logistic(dcrf_model m, const float* weights, const float* features, int F);
+dcrf_status dcrf_model_unary_parameters(dcrf_model m, float* params, int* n);
+dcrf_status dcrf_model_unary_set_parameters(dcrf_model m, const float* params);
+dcrf_status dcrf_model_unary_gradient(dcrf_model m, const float* b, float* grad, int* n);
 /* addPairwiseGaussian(sx, sy, new PottsCompatibility(w)) (src/densecrf.cpp:170). */
 dcrf_status dcrf_model_add_gaussian(dcrf_model m, float sx, float sy, float w_potts);
 /* addPairwiseBilateral(sx, sy, sr, sg, sb, im, new PottsCompatibility(w))
@@ -186,6 +210,12 @@ dcrf_status dcrf_model_pairwise_apply_dev(dcrf_model m, int k, int nonorm, float
 /* pairwise_[k]->apply_upper_minus_lower_ord(out, Q) (src/pairwise.cpp:214-228);
  * fails with DCRF_E_RANGE when Q leaves [0, 1]. */
 dcrf_status dcrf_model_pairwise_apply_ord(dcrf_model m, int k, float* out, const float* Q);
+/* PairwisePotential::apply_upper_minus_lower_ord_restricted(rout, rQ, pI, Q,
+ * store) (src/pairwise.cpp:229-240, include/pairwise.h:78-79): the term's
+ * restricted ordered filter (dcrf_lattice_compute_ord_restricted) followed by
+ * its label compatibility; rout, rQ [nP][L], Q [N][L]. */
+dcrf_status dcrf_model_pairwise_apply_ord_restricted(dcrf_model m, int k, float* rout, const float* rQ,
+                                                     const int32_t* pI, int nP, const float* Q, int store);
 /* qp_inference_super_pixels_non_convex(init) (src/densecrf.cpp:340-442);
  * runs qp or, when cliques are set, qp_sp.  params/stats may be NULL. */
 dcrf_status dcrf_model_qp(dcrf_model m, const float* init, float* out,

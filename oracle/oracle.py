@@ -125,6 +125,11 @@ def ref_lib():
         L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         L.refm_kernel_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
         L.refm_parameters.argtypes = [vp, C.c_int, _f32p]
+        L.refl_compute_ord_restricted.argtypes = [vp, _f32p, _f32p, _i32p, C.c_int, vp, C.c_int, C.c_int]
+        L.refm_apply_ord_restricted.argtypes = [vp, C.c_int, _f32p, _f32p, _i32p, C.c_int, vp, C.c_int]
+        L.refm_set_unary_logistic.argtypes = [vp, _f32p, _f32p, C.c_int]
+        L.refm_unary_get.argtypes = [vp, _f32p]
+        L.refm_unary_gradient.argtypes = [vp, _f32p, _f32p]
         L.refm_add_gaussian_compat.argtypes = [vp, C.c_float, C.c_float, C.c_int, _f32p]
         L.refm_add_bilateral_compat.argtypes = [vp] + [C.c_float] * 5 + [_u8p, C.c_int, _f32p]
         L.refm_weight_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
@@ -225,6 +230,18 @@ class ReferenceLattice(_Lattice):
         self._lib.refl_export(self._h, off, rk, by, nbr)
         return dict(offset=off, rank=rk, bary=by, nbr=nbr[:2 * d1 * M], M=M)
 
+    def compute_ord_restricted(self, rQ, pI, Q, store):
+        """compute_upper_minus_lower_ord_restricted(rout, rQ, pI, Q, store)
+        on a zeroed rout [nP][L]."""
+        pI = _c(pI, np.int32)
+        rQ = _c(rQ, np.float32).reshape(len(pI), -1)
+        L = rQ.shape[1]
+        out = np.zeros((len(pI), L), np.float32)
+        q = None if Q is None else _c(Q, np.float32)
+        self._lib.refl_compute_ord_restricted(self._h, out, rQ, pI, len(pI),
+                                              None if q is None else q.ctypes.data_as(C.c_void_p), L, int(store))
+        return out
+
     def gradient(self, a, b):
         """df [N][d] = d(a^T K b)/d(features) (Permutohedral::gradient)."""
         a = _c(a, np.float32)
@@ -304,6 +321,23 @@ class _Model:
         out = np.zeros(16, np.float32)
         n = self._lib.refm_kernel_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
         return out[:n]
+
+    def set_unary_logistic(self, w, f):
+        """setUnaryEnergy(new LogisticUnaryEnergy(W, f)): w [L][F] (row-major
+        numpy, i.e. W), f [N][F] (reference model only)."""
+        w = np.asarray(w, np.float32)
+        self._lib.refm_set_unary_logistic(self._h, _c(w.T, np.float32), _c(f, np.float32), w.shape[1])
+
+    def unary_get(self):
+        out = self._new()
+        self._lib.refm_unary_get(self._h, out)
+        return out
+
+    def unary_gradient(self, b, F):
+        """unary_->gradient(b) = b f^T as [L][F] (reference model only)."""
+        out = np.zeros(self.L * F, np.float32)
+        n = self._lib.refm_unary_gradient(self._h, _c(b, np.float32), out)
+        return out[:n].reshape(F, self.L).T
 
     def parameters(self, k):
         """pairwise_[k]->parameters() (reference model only)."""
@@ -390,6 +424,16 @@ class ReferenceModel(_Model):
         self._lib.refm_get_cliques(self._h, off, idx, ex, cs)
         return off, idx[:T], ex[:R], cs[:R]
 
+    def apply_ord_restricted(self, k, rQ, pI, Q, store):
+        """pairwise_[k]->apply_upper_minus_lower_ord_restricted(rout, rQ, pI, Q, store)."""
+        pI = _c(pI, np.int32)
+        rQ = _c(rQ, np.float32).reshape(len(pI), self.L)
+        out = np.zeros((len(pI), self.L), np.float32)
+        q = None if Q is None else _c(Q, np.float32)
+        self._lib.refm_apply_ord_restricted(self._h, k, out, rQ, pI, len(pI),
+                                            None if q is None else q.ctypes.data_as(C.c_void_p), int(store))
+        return out
+
     def apply_ord(self, k, x):
         out = self._new()
         if self._lib.refm_apply_ord(self._h, k, out, _c(x, np.float32)) != 0:
@@ -428,3 +472,84 @@ def build_model(cls, img, gaussian=(3.0, 3.0), bilateral=(50.0, 15.0, 5.0)):
     s, c, w = bilateral
     m.add_bilateral(s, s, c, c, c, img["rgb"], w)
     return m
+
+
+class RestrictedOrd:
+    """numpy float32 restatement of the restricted ordered filter,
+    ``seqCompute_upper_minus_lower_ord_restricted``
+    (src/permutohedral.cpp:702-900), from a lattice's exported tables
+    (offset, barycentric, blur neighbours); the stored splat and vertex set of
+    the last store call are kept between calls as the reference keeps them.
+
+    Bins follow addSplitArray / sliceSplitArray (:548-589): lower bin
+    min(floor(q*10 in float), 9), upper bin max(floor((q - 1e-9)*10 in double), 0).
+    """
+
+    def __init__(self, ex, d):
+        self.d, self.M = d, int(ex["M"])
+        d1 = d + 1
+        self.N = len(ex["offset"]) // d1
+        self.off = np.asarray(ex["offset"]).reshape(self.N, d1)
+        self.bary = np.asarray(ex["bary"], np.float32).reshape(self.N, d1)
+        self.nbr = np.asarray(ex["nbr"]).reshape(d1, self.M, 2)
+        self.stored = None
+        self.active = None
+
+    @staticmethod
+    def _bins(q, upper):
+        q = np.asarray(q, np.float32)
+        if upper:
+            return np.maximum(np.floor((q.astype(np.float64) - 1e-9) * 10.0).astype(np.int64), 0)
+        return np.minimum(np.floor(q * np.float32(10)).astype(np.int64), 9)
+
+    def _splat(self, vals, i, q, upper):
+        c = self._bins(q, upper)[:, None]
+        b = np.arange(10)[None, :]
+        mask = b >= c if upper else b <= c
+        for j in range(self.d + 1):
+            o = self.off[i, j] + 1
+            vals[o] = vals[o] + np.where(mask, self.bary[i, j], np.float32(0))
+
+    def compute(self, rQ, pI, Q, store):
+        rQ = np.asarray(rQ, np.float32)
+        pI = [int(i) for i in pI]
+        L, M, d = rQ.shape[1], self.M, self.d
+        alpha = np.float32(1) / (np.float32(1) + np.float32(2.0 ** -d))
+        out = np.zeros((len(pI), L), np.float32)
+        inside = set(pI)
+        if store:
+            self.stored = {}
+            act, seen = [], set()
+            for i in pI:
+                for j in range(d + 1):
+                    o = int(self.off[i, j])
+                    if o not in seen:
+                        seen.add(o)
+                        act.append(o)
+            self.active = np.array(act, np.int64)
+        for upper in (False, True):
+            if store:
+                vals = np.zeros((M + 2, L, 10), np.float32)
+                for i in range(self.N):
+                    if i not in inside:
+                        self._splat(vals, i, Q[i], upper)
+                self.stored[upper] = vals.copy()
+            else:
+                vals = self.stored[upper].copy()
+            for ii, i in enumerate(pI):
+                self._splat(vals, i, rQ[ii], upper)
+            new = np.zeros_like(vals)
+            a = self.active
+            for j in range(d + 1):
+                if len(a):
+                    n = self.nbr[j, a]
+                    new[a + 1] = vals[a + 1] + np.float32(0.5) * (vals[n[:, 0] + 1] + vals[n[:, 1] + 1])
+                vals, new = new, vals
+            for ii, i in enumerate(pI):
+                c = self._bins(rQ[ii], upper)
+                for j in range(d + 1):
+                    o = self.off[i, j] + 1
+                    w = self.bary[i, j]
+                    coef = np.float32(w) * alpha if upper else np.float32(-w) * alpha
+                    out[ii] = out[ii] + vals[o, np.arange(L), c] * coef
+        return out

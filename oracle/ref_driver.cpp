@@ -55,6 +55,8 @@ struct RefModel : public DenseCRF2D {
         return pairwise_[k]->gradient(b, Q);
     }
     VectorXf parameters(int k) const { return pairwise_[k]->parameters(); }
+    VectorXf unary_gradient(const MatrixXf& b) const { return unary_->gradient(b); }
+    MatrixXf unary_get() const { return unary_->get(); }
     int N() const { return N_; }
     int L() const { return M_; }
     int R() const { return R_; }
@@ -207,6 +209,27 @@ void refl_compute_ord(void* h, float* out, const float* in, int L) {
     p->compute_upper_minus_lower_ord(O, I);
     std::memcpy(out, O.data(), sizeof(float) * (size_t)L * p->N());
 }
+// pI as the reference takes it, with one sentinel -1 in reserved storage
+// right after its last element: the reference reads pI[pI.size()] once it
+// has passed the last pI pixel (src/permutohedral.cpp:727-731), and the
+// sentinel keeps that read defined and equal to "not in pI".
+static std::vector<int> restricted_set(const int* pI, int nP) {
+    std::vector<int> v;
+    v.reserve((size_t)nP + 1);
+    v.assign(pI, pI + nP);
+    v.data()[nP] = -1;
+    return v;
+}
+void refl_compute_ord_restricted(void* h, float* rout, const float* rQ, const int* pI, int nP, const float* Q, int L,
+                                 int store) {
+    LatticeProbe* p = (LatticeProbe*)h;
+    std::vector<int> idx = restricted_set(pI, nP);
+    MatrixXf RQ = Map<const MatrixXf>(rQ, L, nP);
+    MatrixXf QQ = Q ? MatrixXf(Map<const MatrixXf>(Q, L, p->N())) : MatrixXf::Zero(L, p->N());
+    MatrixXf O = MatrixXf::Zero(L, nP);
+    p->compute_upper_minus_lower_ord_restricted(O, RQ, idx, QQ, store != 0);
+    if (nP) std::memcpy(rout, O.data(), sizeof(float) * (size_t)L * nP);
+}
 
 // ------------------------------------------------------------------ model --
 void* refm_new(int W, int H, int L, const float* unary) {
@@ -269,6 +292,16 @@ void refm_apply(void* h, int k, int nonorm, float* out, const float* in) {
     MatrixXf O;
     (nonorm ? m->pw_nonorm(k) : m->pw(k))->apply(O, I);
     std::memcpy(out, O.data(), sizeof(float) * O.size());
+}
+void refm_apply_ord_restricted(void* h, int k, float* rout, const float* rQ, const int* pI, int nP, const float* Q,
+                               int store) {
+    RefModel* m = (RefModel*)h;
+    std::vector<int> idx = restricted_set(pI, nP);
+    MatrixXf RQ = Map<const MatrixXf>(rQ, m->L(), nP);
+    MatrixXf QQ = Q ? MatrixXf(Map<const MatrixXf>(Q, m->L(), m->N())) : MatrixXf::Zero(m->L(), m->N());
+    MatrixXf O(m->L(), nP);
+    m->pw(k)->apply_upper_minus_lower_ord_restricted(O, RQ, idx, QQ, store != 0);
+    if (nP) std::memcpy(rout, O.data(), sizeof(float) * (size_t)m->L() * nP);
 }
 int refm_apply_ord(void* h, int k, float* out, const float* in) {
     RefModel* m = (RefModel*)h;
@@ -339,6 +372,22 @@ int refm_weight_gradient(void* h, int k, const float* b, const float* Q, float* 
     RefModel* m = (RefModel*)h;
     MatrixXf B = Map<const MatrixXf>(b, m->L(), m->N()), QQ = Map<const MatrixXf>(Q, m->L(), m->N());
     VectorXf g = m->weight_gradient(k, B, QQ);
+    std::memcpy(out, g.data(), sizeof(float) * g.size());
+    return (int)g.size();
+}
+// setUnaryEnergy(new LogisticUnaryEnergy(W (L x F), f (F x N))).
+void refm_set_unary_logistic(void* h, const float* w, const float* f, int F) {
+    RefModel* m = (RefModel*)h;
+    m->setUnaryEnergy(new LogisticUnaryEnergy(Map<const MatrixXf>(w, m->L(), F), Map<const MatrixXf>(f, F, m->N())));
+}
+int refm_unary_get(void* h, float* out) {
+    MatrixXf u = ((RefModel*)h)->unary_get();
+    std::memcpy(out, u.data(), sizeof(float) * u.size());
+    return (int)u.size();
+}
+int refm_unary_gradient(void* h, const float* b, float* out) {
+    RefModel* m = (RefModel*)h;
+    VectorXf g = m->unary_gradient(Map<const MatrixXf>(b, m->L(), m->N()));
     std::memcpy(out, g.data(), sizeof(float) * g.size());
     return (int)g.size();
 }

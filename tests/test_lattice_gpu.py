@@ -147,3 +147,75 @@ def test_feature_gradient_matches_reference(name):
     g = golden(name)
     lat = Permutohedral().init(g["f"])
     assert _eq(lat.gradient(g["a"], g["b"]), g["df"])
+
+
+def test_restricted_ord_matches_reference_golden():
+    """compute_upper_minus_lower_ord_restricted and the pairwise terms'
+    apply_upper_minus_lower_ord_restricted, bit for bit against the
+    reference's own outputs (tests/golden/make_restricted_golden.py): a store
+    call, a reuse call with new values, and a reuse call on a smaller pixel
+    set whose blur still covers the first call's vertices."""
+    from densecrf_ho_b200 import DenseCRF2D
+    g = golden("restricted_32x24.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    Q, pI = g["Q"], g["pI"]
+    for name in ("g", "b"):
+        lat = Permutohedral().init(g[f"{name}_f"])
+        assert _eq(lat.compute_upper_minus_lower_ord_restricted(Q[pI], pI, Q, True), g[f"{name}_out1"])
+        assert _eq(lat.compute_upper_minus_lower_ord_restricted(g["rQ2"], pI, None, False), g[f"{name}_out2"])
+        assert _eq(lat.compute_upper_minus_lower_ord_restricted(g["rQ3"], g["pI3"], None, False),
+                   g[f"{name}_out3"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    m = DenseCRF2D(W, H, L)
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    for k in range(2):
+        f = m.pairwise_apply_upper_minus_lower_ord_restricted
+        assert _eq(f(k, Q[pI], pI, Q, True), g[f"m{k}_out1"])
+        assert _eq(f(k, g["rQ2"], pI, None, False), g[f"m{k}_out2"])
+        assert _eq(f(k, g["rQ3"], g["pI3"], None, False), g[f"m{k}_out3"])
+
+
+@pytest.mark.parametrize("L", [1, 5])
+def test_restricted_ord_vs_restatement(L, oracle_mod):
+    """Against the numpy restatement on the C oracle's tables: a larger
+    bilateral lattice, an empty pixel set, and the full pixel set, where
+    every vertex is active and the restricted filter is the ordered filter."""
+    W, H = 97, 61
+    N = W * H
+    img = synth.make_image(W, H, 21, 4)
+    f = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    rng = np.random.default_rng(L)
+    Q = rng.random((N, L)).astype(np.float32)
+    Q[::7] = np.float32(0.3)
+    lat = Permutohedral().init(f)
+    ref = oracle_mod.RestrictedOrd(oracle_mod.OracleLattice(f).export(), 5)
+    pI = np.sort(rng.choice(N, N // 3, replace=False)).astype(np.int32)
+    rQ = rng.random((len(pI), L)).astype(np.float32)
+    assert _eq(lat.compute_upper_minus_lower_ord_restricted(rQ, pI, Q, True), ref.compute(rQ, pI, Q, True))
+    rQ2 = rng.random((len(pI), L)).astype(np.float32)
+    assert _eq(lat.compute_upper_minus_lower_ord_restricted(rQ2, pI, None, False),
+               ref.compute(rQ2, pI, None, False))
+    empty = np.zeros(0, np.int32)
+    assert lat.compute_upper_minus_lower_ord_restricted(np.zeros((0, L), np.float32), empty, Q, True).shape == (0, L)
+    allp = np.arange(N, dtype=np.int32)
+    full = lat.compute_upper_minus_lower_ord_restricted(Q, allp, Q, True)
+    assert _eq(full, lat.compute_upper_minus_lower_ord(Q))
+
+
+def test_restricted_ord_errors():
+    from densecrf_ho_b200 import DCRFError
+    W, H, L = 16, 12, 3
+    lat = Permutohedral().init(synth.gaussian_features(W, H, 3, 3))
+    Q = np.full((W * H, L), 0.5, np.float32)
+    pI = np.array([3, 9, 40], np.int32)
+    with pytest.raises(DCRFError):   # nothing stored yet
+        lat.compute_upper_minus_lower_ord_restricted(Q[pI], pI, None, False)
+    with pytest.raises(DCRFError):   # not ascending
+        lat.compute_upper_minus_lower_ord_restricted(Q[pI], pI[::-1].copy(), Q, True)
+    with pytest.raises(DCRFError):   # out of [0, 1]
+        lat.compute_upper_minus_lower_ord_restricted(Q[pI] + 1, pI, Q, True)
+    lat.compute_upper_minus_lower_ord_restricted(Q[pI], pI, Q, True)
+    with pytest.raises(DCRFError):   # stored for another label count
+        lat.compute_upper_minus_lower_ord_restricted(np.zeros((3, 2), np.float32), pI, None, False)

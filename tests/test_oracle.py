@@ -109,3 +109,21 @@ def test_apply_ord_rejects_out_of_range(oracle_mod):
     bad[3, 4] = 1.5
     with pytest.raises(RuntimeError, match="Value out of bounds"):
         m.apply_ord(0, bad)
+
+
+def test_restricted_restatement_pinned_to_golden(oracle_mod):
+    """The numpy restatement of the restricted ordered filter on the C
+    oracle's lattice tables reproduces the reference's own outputs
+    (tests/golden/make_restricted_golden.py) bit for bit: store call, reuse
+    call, reuse call on a smaller pixel set; and the pairwise terms' Potts
+    compatibility on top."""
+    g = golden("restricted_32x24.npz")
+    for name, d, w in (("g", 2, 3.0), ("b", 5, 5.0)):
+        r = oracle_mod.RestrictedOrd(oracle_mod.OracleLattice(g[f"{name}_f"]).export(), d)
+        o1 = r.compute(g["Q"][g["pI"]], g["pI"], g["Q"], True)
+        o2 = r.compute(g["rQ2"], g["pI"], None, False)
+        o3 = r.compute(g["rQ3"], g["pI3"], None, False)
+        for o, key in ((o1, "out1"), (o2, "out2"), (o3, "out3")):
+            assert np.array_equal(o, g[f"{name}_{key}"]), (name, key)
+            k = 0 if name == "g" else 1
+            assert np.array_equal(np.float32(-w) * o, g[f"m{k}_{key}"]), (name, key)

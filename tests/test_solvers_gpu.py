@@ -262,3 +262,33 @@ def test_compatibility_argument_errors():
     assert np.array_equal(m.pairwise_parameters(0), packed)
     m.pairwise_set_parameters(0, packed[::-1].copy())
     assert np.array_equal(m.pairwise_parameters(0), packed[::-1])
+
+
+def test_logistic_unary_vs_reference():
+    """LogisticUnaryEnergy (unary W f, gradient b f^T) against the reference's
+    own values (tests/golden/make_unary_golden.py); Eigen's GEMM orders the
+    sums differently, so float tolerances: 1e-5 of the largest magnitude."""
+    g = golden("unary_logistic_24x18_L5.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    m = DenseCRF2D(W, H, L)
+    assert m.unary_parameters().size == 0
+    m.setUnaryEnergyLogistic(g["w"], g["f"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    assert np.array_equal(m.unary_parameters(), g["w"])
+    Q = m.unary_init()
+    assert np.abs(Q - g["unary_init"]).max() <= 1e-5
+    gr = m.unary_gradient(g["b"])
+    assert gr.shape == g["ugrad"].shape
+    assert np.abs(gr - g["ugrad"]).max() <= 1e-5 * np.abs(g["ugrad"]).max()
+    out, st = m.qp_inference_super_pixels_non_convex(g["unary_init"], max_iter=20, stats=True)
+    assert st.iterations == int(g["qp_iters"])
+    assert (m.currentMap(out) == m.currentMap(g["qp"])).mean() >= 0.999
+    assert st.energy == pytest.approx(float(g["qp_energies"][-1]), rel=1e-5)
+    # setParameters recomputes the unary; a constant unary drops the logistic one
+    m.unary_set_parameters(2 * g["w"])
+    assert np.array_equal(m.unary_parameters(), 2 * g["w"])
+    assert not np.array_equal(m.unary_init(), Q)
+    m.setUnaryEnergy(np.zeros((W * H, L), np.float32))
+    assert m.unary_gradient(g["b"]).size == 0
