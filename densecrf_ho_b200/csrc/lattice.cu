@@ -937,6 +937,85 @@ __global__ void ord_slice_kernel(int N, int Lrt, int drt, const int* __restrict_
     }
 }
 
+// One term of a fused two-term ordered slice.
+struct OrdSliceTerm {
+    const int* offset;
+    const float* bary;
+    const float* vals;
+    int d;
+    float alpha;
+    SliceEpilogue ep;
+};
+
+template <int DC>
+__device__ __forceinline__ float ord_slice_acc(const OrdSliceTerm& s, int i, int k, int L, int cl, int cu) {
+    const int d = DC ? DC : s.d, d1 = d + 1;
+    const int* __restrict__ off = s.offset + (long)i * d1;
+    const float* __restrict__ by = s.bary + (long)i * d1;
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j <= d; j++)
+        acc = fadd(acc, fmul(s.vals[((long)(off[j] + 1) * kOrdW + cl) * L + k], fmul(-by[j], s.alpha)));
+#pragma unroll
+    for (int j = 0; j <= d; j++)
+        acc = fadd(acc, fmul(s.vals[((long)(off[j] + 1) * kOrdW + kRes + cu) * L + k], fmul(by[j], s.alpha)));
+    return acc;
+}
+
+// sa = t1's slice on top of t0's (Model::apply_ord_sum with two terms): v0 =
+// epilogue_0(slice_0) exactly as ord_slice_kernel writes it, then v0 +
+// coef_1 * scaled(slice_1) as ord_slice_kernel computes it from base = v0.
+// The value v0 never leaves the register; GAP as in ord_slice_kernel.
+template <bool GAP, int D0, int D1, int LC>
+__global__ void ord_slice_pair_kernel(int N, int Lrt, OrdSliceTerm t0, OrdSliceTerm t1,
+                                      const float2* __restrict__ bins, float* out, GapFusion gf) {
+    const int L = LC ? LC : Lrt;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    double g0 = 0.0, g1 = 0.0;
+    if (t < (long)N * L) {
+        const int i = (int)(t / L), k = (int)(t - (long)i * L);
+        const float2 bp = bins[t];
+        const int cl = ord_lower_of(bp), cu = ord_upper_of(bp);
+        const float a0 = ord_slice_acc<D0>(t0, i, k, L, cl, cu);
+        const float a1 = ord_slice_acc<D1>(t1, i, k, L, cl, cu);
+        const float v0 = apply_epilogue(a0, t, i, k, t0.ep);
+        float s1 = a1;
+        if (t1.ep.potts) {
+            if (t1.ep.norm) s1 = fmul(s1, t1.ep.norm[i]);
+            s1 = t1.ep.scale_vec ? fmul(t1.ep.scale_vec[k], s1) : fmul(t1.ep.scale, s1);
+        }
+        const float v = fadd(v0, fmul(t1.ep.coef, s1));
+        out[t] = v;
+        if (GAP) {
+            const float tmp = fsub(fadd(gf.alpha[t], gf.u[t]), fadd(v, gf.su ? gf.su[t] : 0.0f));
+            g0 = (double)tmp * (double)gf.Q[t];
+            g1 = (double)tmp * (double)tmp;
+        }
+    }
+    if (GAP) {
+        __shared__ double s0[kTB / 32], s1[kTB / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g0 += __shfl_down_sync(0xffffffffu, g0, o);
+            g1 += __shfl_down_sync(0xffffffffu, g1, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            s0[threadIdx.x >> 5] = g0;
+            s1[threadIdx.x >> 5] = g1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < kTB / 32; w++) {
+                a += s0[w];
+                b += s1[w];
+            }
+            gf.partials[blockIdx.x] = a;
+            gf.partials[gridDim.x + blockIdx.x] = b;
+        }
+    }
+}
+
 // Bins of rescale(Q) (src/eigen_utils.cpp:120-141) without materialising it:
 // rq = (Q - min) / (max - min), with min / max at qmm[0], qmm[1].
 __global__ void rescaled_bins_kernel(long n, const float* __restrict__ Q, const float* __restrict__ qmm,
@@ -1506,6 +1585,25 @@ void Lattice::ord_splat_blur(const float2* bins, int L) {
         std::swap(src, dst);
     }
     ord_vals = src;
+}
+
+void Lattice::ord_slice_pair(float* out, const float2* bins, int L, const Lattice& a, const SliceEpilogue& ea,
+                             const Lattice& b, const SliceEpilogue& eb, const GapFusion* gap) {
+    require(a.ord_vals && b.ord_vals, DCRF_E_STATE, "ord_slice_pair: no ord_splat_blur before it");
+    require(a.N == b.N, DCRF_E_ARG, "ord_slice_pair: lattices over different pixel counts");
+    const long NL = (long)a.N * L;
+    const OrdSliceTerm t0{a.offset.get(), a.bary.get(), a.ord_vals, a.d, 1.0f / (1.0f + std::pow(2.0f, (float)-a.d)),
+                          ea};
+    const OrdSliceTerm t1{b.offset.get(), b.bary.get(), b.ord_vals, b.d, 1.0f / (1.0f + std::pow(2.0f, (float)-b.d)),
+                          eb};
+    const GapFusion gf = gap ? *gap : GapFusion{};
+    auto sl = [&](auto kern) {
+        launch(kern, ceil_div(NL, kTB), kTB, 0, a.stream, a.N, L, t0, t1, bins, out, gf);
+    };
+    const bool common = L == 21 && a.d == 2 && b.d == 5;
+    if (gap) sl(common ? ord_slice_pair_kernel<true, 2, 5, 21> : ord_slice_pair_kernel<true, 0, 0, 0>);
+    else sl(common ? ord_slice_pair_kernel<false, 2, 5, 21> : ord_slice_pair_kernel<false, 0, 0, 0>);
+    DCRF_LAUNCH_CHECK();
 }
 
 void Lattice::ord_slice(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap) {

@@ -95,6 +95,12 @@ struct Lattice {
     // ord_vals), then the slice.  Other work may run between them.
     void ord_splat_blur(const float2* bins, int L);
     void ord_slice(float* out, const float2* bins, int L, const SliceEpilogue& ep, const GapFusion* gap);
+    // Both slices of a two-term sum in one pass: out = eb(b's slice) on top of
+    // ea(a's slice), the arithmetic of ord_slice(a, ea with zero_base) then
+    // ord_slice(b, eb with base = out); a and b share N and the bins, and each
+    // has had its ord_splat_blur.  Runs on a's stream.
+    static void ord_slice_pair(float* out, const float2* bins, int L, const Lattice& a, const SliceEpilogue& ea,
+                               const Lattice& b, const SliceEpilogue& eb, const GapFusion* gap);
     const float* ord_vals = nullptr;
 
     // compute_upper_minus_lower_ord_restricted: the ordered filter at the nP

@@ -579,6 +579,14 @@ void Model::apply_ord_sum(float* sa, const float2* bins, const GapFusion* gap) {
     }
     if (nt >= 1) terms[0]->lat->ord_splat_blur(bins, L);
     if (nt >= 2) DCRF_CUDA(cudaStreamWaitEvent(stream, ev_side_join, 0));
+    if (nt == 2 && terms[0]->compat != kMatrix && terms[1]->compat != kMatrix) {
+        // the two slices in one pass (the sum in term order, bit for bit)
+        SliceEpilogue e0, e1;
+        route_compat(*this, *terms[0], e0, sa, nullptr, 1.0f, true);
+        route_compat(*this, *terms[1], e1, sa, sa, 1.0f, false);
+        Lattice::ord_slice_pair(sa, bins, L, *terms[0]->lat, e0, *terms[1]->lat, e1, gap);
+        return;
+    }
     for (int k = 0; k < nt; k++) {
         SliceEpilogue ep;
         const Term& t = *terms[k];
