@@ -217,6 +217,7 @@ Model::~Model() {
         cudaEventDestroy(ev_side_join);
         cudaStreamDestroy(side);
     }
+    if (gstream) cudaStreamDestroy(gstream);
     terms.clear();
     if (h_scal) cudaFreeHost(h_scal);
     if (stream) cudaStreamDestroy(stream);

@@ -43,12 +43,14 @@ struct SolverScalars {
     int steps;
     int err;              // DCRF_E_* raised by a device check
     int done;             // batched QP: the image had stopped before this iteration
+    int gamma_sum;        // LP: qp-gamma iterations of the whole solve
 };
 
 struct Model {
     int W = 0, H = 0, N = 0, L = 0, device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // second stream for the other terms' filter work
+    cudaStream_t gstream = nullptr;  // captures the body of the LP's qp-gamma loop
     cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
     bool has_unary = false;
     DevBuf<float> unary;

@@ -449,8 +449,30 @@ __global__ void lp_gamma_check_kernel(const double* __restrict__ partials, int n
     if (threadIdx.x == 0) {
         const float qv1 = (float)s;
         sc->steps++;
+        sc->gamma_sum++;
         if (fabsf(fsub(sc->qp_value, qv1)) < qp_tol) sc->stop = 1;
         else sc->qp_value = qv1;
+    }
+}
+
+// The same test as the exit condition of a graph's `while` node: the loop
+// goes on while the iterate has not converged and fewer than max_iter
+// iterations have run (the body always runs at least once).
+__global__ void lp_gamma_check_cond_kernel(const double* __restrict__ partials, int nblk, float qp_tol,
+                                           SolverScalars* sc, int max_iter, cudaGraphConditionalHandle h) {
+    __shared__ double s32[32];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) s += partials[b];
+    s = block_sum_any(s, s32);
+    if (threadIdx.x == 0) {
+        if (!sc->stop) {
+            const float qv1 = (float)s;
+            sc->steps++;
+            sc->gamma_sum++;
+            if (fabsf(fsub(sc->qp_value, qv1)) < qp_tol) sc->stop = 1;
+            else sc->qp_value = qv1;
+        }
+        cudaGraphSetConditional(h, (!sc->stop && sc->steps < max_iter) ? 1u : 0u);
     }
 }
 
@@ -1225,7 +1247,170 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
         }
     }
 
-    int it = 0, count = 0, fw_total = 0, gamma_total = 0;
+    int it = 0, count = 0, fw_total = 0;
+    DCRF_CUDA(cudaMemsetAsync(&sc->gamma_sum, 0, sizeof(int), stream));
+
+    // One Frank-Wolfe iteration in three parts: lp_y and the qp-gamma reset
+    // (s1), the qp-gamma iterations, and Q, the bins, the clique and ordered
+    // subgradients and the dual-gap step (s2).
+    auto s1 = [&](bool pending) {
+        // alpha / u of the previous iteration are updated inside lp_y (the
+        // update after the last iteration is never read: both are reset
+        // before the next proximal step).
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            if constexpr (LC > 0)
+                launch(lp_y_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, lambda, gc.cm, alpha, u, unary.get(),
+                       curQ, Y, pending, sa, su, sc);
+            else
+                launch(lp_y_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y,
+                       pending, sa, su, sc);
+        });
+        launch(lp_gamma_reset_kernel, 1, 1, 0, stream, sc);
+    };
+    // One qp-gamma iteration on stream st; with a graph handle its test also
+    // sets the graph's loop condition.
+    auto gamma_step = [&](cudaStream_t st, const cudaGraphConditionalHandle* h) {
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            const int nblk = LC > 0 ? tgrid : kRedBlocks;
+            if constexpr (LC > 0)
+                launch(lp_gamma_tiled<LC>, tgrid, 32 * kTileWarps, 0, st, N, gc, Y, gamma, sc, part);
+            else
+                launch(lp_gamma_kernel<LC>, kRedBlocks, kRedThreads, 0, st, N, L, gc, Y, gamma, sc, part);
+            if (h)
+                launch(lp_gamma_check_cond_kernel, 1, 1024, 0, st, part, nblk, p.qp_tol, sc, p.qp_max_iter, *h);
+            else
+                launch(lp_gamma_check_kernel, 1, 1024, 0, st, part, nblk, p.qp_tol, sc);
+        });
+    };
+    auto s2 = [&]() {
+        // Q, with the min / max of rescale folded in; then the bins of
+        // rescale(Q) once for all pairwise terms.
+        with_lc(L, [&](auto lc) {
+            constexpr int LC = decltype(lc)::value;
+            if constexpr (LC > 0) {
+                launch(lp_q_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, lambda, alpha, u, gamma, unary.get(),
+                       curQ, Q, part);
+                launch(minmax_finish_kernel, 1, 1024, 0, stream, part, tgrid, sc);
+            } else {
+                launch(lp_q_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q,
+                       part);
+                launch(minmax_finish_kernel, 1, 1024, 0, stream, part, pg, sc);
+            }
+        });
+        rescaled_bins(bins, Q, NL, &sc->qmin, stream);
+        // Clique conditional gradient su (computeUCondGrad), before the
+        // ordered filters so that the dual-gap sums can ride along the
+        // last term's slice with su included.
+        if (R > 0) {
+            const int nw = 2 * R;
+            int* tgt = upos + 2 * R;
+            DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
+            launch(ucond_kernel, R, kUcondThreads, 0, stream, cl_off.get(), cl_idx.get(), L, Q, upos);
+            launch(ucond_targets_kernel, 1, 1024, 0, stream, R, upos, tgt);
+            launch(ucond_claim_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
+            launch(ucond_write_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, cl_const.get(), cl_exp.get(),
+                   lp_win.get(), su);
+            launch(ucond_reset_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
+        }
+        // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; the
+        // dual-gap sums ride along the last term's slice.
+        const bool fuse_gap = nt > 0 && terms[nt - 1]->compat != kMatrix;
+        GapFusion gf{alpha, u, Q, part, R > 0 ? su : nullptr};
+        apply_ord_sum(sa, bins, fuse_gap ? &gf : nullptr);
+        if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));
+        if (fuse_gap) {
+            launch(finalize_large_kernel, 2, 1024, 0, stream, part, slice_grid(NL), 0, sc);
+        } else {
+            launch(lp_gap_kernel, kRedBlocks, kRedThreads, 0, stream, NL, alpha, u, sa, su, Q, part);
+            launch(finalize_sums_kernel, 1, 64, 0, stream, part, kRedBlocks, 2, 0, sc);
+        }
+        launch(lp_delta_kernel, 1, 1, 0, stream, sc, lambda);
+        DCRF_LAUNCH_CHECK();
+    };
+    // The whole iteration as one CUDA graph: s1, a `while` node whose body is
+    // one qp-gamma iteration and whose condition its test kernel sets, s2.
+    // Built after the first iteration has run eagerly (it sizes every buffer
+    // the iteration touches) and used for the rest of the solve: no host
+    // round trip per iteration.  Kernel launch counts: the graph's own
+    // kernels per launch plus two per qp-gamma iteration inside it.
+    struct FwGraphs {  // released on every exit from the solve
+        cudaGraphExec_t g[2] = {nullptr, nullptr};  // pending = false / true
+        void drop() {
+            for (auto& x : g)
+                if (x) {
+                    cudaGraphExecDestroy(x);
+                    x = nullptr;
+                }
+        }
+        ~FwGraphs() { drop(); }
+    } fwg;
+    cudaGraphExec_t* fw_graph = fwg.g;
+    unsigned long long fw_graph_kernels = 0;
+    bool graphs_ok = true;
+    int eager_gamma = 0;
+    auto drop_graphs = [&]() { fwg.drop(); };
+    auto build_graph = [&](bool pending) -> cudaGraphExec_t {
+        if (!gstream) DCRF_CUDA(cudaStreamCreateWithFlags(&gstream, cudaStreamNonBlocking));
+        cudaGraph_t g = nullptr;
+        DCRF_CUDA(cudaGraphCreate(&g, 0));
+        bool main_cap = false, body_cap = false;
+        try {
+            cudaGraphConditionalHandle h;
+            DCRF_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+            const unsigned long long k0 = g_kernel_launches.load();
+            DCRF_CUDA(cudaStreamBeginCaptureToGraph(stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+            main_cap = true;
+            s1(pending);
+            cudaStreamCaptureStatus cs;
+            cudaGraph_t cg = nullptr;
+            const cudaGraphNode_t* deps = nullptr;
+            size_t nd = 0;
+            DCRF_CUDA(cudaStreamGetCaptureInfo(stream, &cs, nullptr, &cg, &deps, &nd));
+            cudaGraphNodeParams np = {};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            cudaGraphNode_t wn;
+            DCRF_CUDA(cudaGraphAddNode(&wn, cg, deps, nd, &np));
+            DCRF_CUDA(cudaStreamUpdateCaptureDependencies(stream, &wn, 1, cudaStreamSetCaptureDependencies));
+            const unsigned long long kb = g_kernel_launches.load();
+            DCRF_CUDA(cudaStreamBeginCaptureToGraph(gstream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeRelaxed));
+            body_cap = true;
+            gamma_step(gstream, &h);
+            cudaGraph_t bo = nullptr;
+            body_cap = false;
+            DCRF_CUDA(cudaStreamEndCapture(gstream, &bo));
+            const unsigned long long body_kernels = g_kernel_launches.load() - kb;
+            // The loop ends only through its test kernel: a body without it
+            // would never stop, so anything but the two kernels is refused.
+            size_t body_nodes = 0;
+            DCRF_CUDA(cudaGraphGetNodes(np.conditional.phGraph_out[0], nullptr, &body_nodes));
+            require(body_nodes == 2 && body_kernels == 2, DCRF_E_STATE, "lp: unexpected qp-gamma loop body");
+            s2();
+            cudaGraph_t out = nullptr;
+            main_cap = false;
+            DCRF_CUDA(cudaStreamEndCapture(stream, &out));
+            const unsigned long long captured = g_kernel_launches.load() - k0;
+            g_kernel_launches.fetch_sub(captured);  // counted when the graph runs
+            fw_graph_kernels = captured - body_kernels;
+            cudaGraphExec_t ex = nullptr;
+            DCRF_CUDA(cudaGraphInstantiate(&ex, g, 0));
+            cudaGraphDestroy(g);
+            return ex;
+        } catch (...) {
+            cudaGraph_t junk = nullptr;
+            if (body_cap) cudaStreamEndCapture(gstream, &junk);
+            if (main_cap) cudaStreamEndCapture(stream, &junk);
+            cudaGraphDestroy(g);
+            cudaGetLastError();
+            throw;
+        }
+    };
+
     do {
         ++it;
         launch(fill_float_kernel, ceil_div(NL, 256), 256, 0, stream, NL, 1.0f, gamma);
@@ -1235,88 +1420,36 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
         int pit = 0;
         do {
             ++pit;
-            // alpha / u of the previous iteration are updated inside lp_y
-            // (the update after the last iteration is never read: both are
-            // reset before the next proximal step).
             const bool pending = pit > 1;
-            with_lc(L, [&](auto lc) {
-                constexpr int LC = decltype(lc)::value;
-                if constexpr (LC > 0)
-                    launch(lp_y_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, lambda, gc.cm, alpha, u, unary.get(),
-                           curQ, Y, pending, sa, su, sc);
-                else
-                    launch(lp_y_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, gc.cm, alpha, u, unary.get(), curQ, Y,
-                           pending, sa, su, sc);
-            });
-            launch(lp_gamma_reset_kernel, 1, 1, 0, stream, sc);
+            if (graphs_ok && fw_graph[pending]) {
+                DCRF_CUDA(cudaGraphLaunch(fw_graph[pending], stream));
+                g_kernel_launches.fetch_add(fw_graph_kernels);
+                continue;
+            }
+            s1(pending);
             // qp-gamma iterations; the reference needs at least two (its first
             // test compares against FLT_MAX), so launch in pairs and look at
             // the stop flag after each pair.
             int launched = 0;
             for (;;) {
                 const int batch = std::min(2, p.qp_max_iter - launched);
-                for (int bi = 0; bi < batch; bi++) {
-                    with_lc(L, [&](auto lc) {
-                        constexpr int LC = decltype(lc)::value;
-                        if constexpr (LC > 0) {
-                            launch(lp_gamma_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, gc, Y, gamma, sc, part);
-                            launch(lp_gamma_check_kernel, 1, 1024, 0, stream, part, tgrid, p.qp_tol, sc);
-                        } else {
-                            launch(lp_gamma_kernel<LC>, kRedBlocks, kRedThreads, 0, stream, N, L, gc, Y, gamma, sc,
-                                   part);
-                            launch(lp_gamma_check_kernel, 1, 1024, 0, stream, part, kRedBlocks, p.qp_tol, sc);
-                        }
-                    });
-                }
+                for (int bi = 0; bi < batch; bi++) gamma_step(stream, nullptr);
                 launched += batch;
                 DCRF_LAUNCH_CHECK();
                 fetch_scalars();
                 if (h_scal->stop || launched >= p.qp_max_iter || batch <= 0) break;
             }
-            gamma_total += h_scal->steps;
-            // Q, with the min / max of rescale folded in; then the bins of
-            // rescale(Q) once for all pairwise terms.
-            with_lc(L, [&](auto lc) {
-                constexpr int LC = decltype(lc)::value;
-                if constexpr (LC > 0) {
-                    launch(lp_q_tiled<LC>, tgrid, 32 * kTileWarps, 0, stream, N, lambda, alpha, u, gamma, unary.get(),
-                           curQ, Q, part);
-                    launch(minmax_finish_kernel, 1, 1024, 0, stream, part, tgrid, sc);
-                } else {
-                    launch(lp_q_kernel<LC>, pg, kPix, 0, stream, N, L, lambda, alpha, u, gamma, unary.get(), curQ, Q,
-                           part);
-                    launch(minmax_finish_kernel, 1, 1024, 0, stream, part, pg, sc);
+            eager_gamma += h_scal->steps;
+            s2();
+            if (graphs_ok && !fw_graph[0]) {
+                try {
+                    fw_graph[0] = build_graph(false);
+                    fw_graph[1] = build_graph(true);
+                } catch (const Error&) {
+                    drop_graphs();
+                    graphs_ok = false;  // this device or driver cannot run them: stay eager
                 }
-            });
-            rescaled_bins(bins, Q, NL, &sc->qmin, stream);
-            // Clique conditional gradient su (computeUCondGrad), before the
-            // ordered filters so that the dual-gap sums can ride along the
-            // last term's slice with su included.
-            if (R > 0) {
-                const int nw = 2 * R;
-                int* tgt = upos + 2 * R;
-                DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
-                launch(ucond_kernel, R, kUcondThreads, 0, stream, cl_off.get(), cl_idx.get(), L, Q, upos);
-                launch(ucond_targets_kernel, 1, 1024, 0, stream, R, upos, tgt);
-                launch(ucond_claim_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
-                launch(ucond_write_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, cl_const.get(), cl_exp.get(),
-                       lp_win.get(), su);
-                launch(ucond_reset_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
             }
-            // Ordered subgradient sa = sum_k apply_upper_minus_lower_ord_k; the
-            // dual-gap sums ride along the last term's slice.
-            const bool fuse_gap = nt > 0 && terms[nt - 1]->compat != kMatrix;
-            GapFusion gf{alpha, u, Q, part, R > 0 ? su : nullptr};
-            apply_ord_sum(sa, bins, fuse_gap ? &gf : nullptr);
-            if (nt == 0) DCRF_CUDA(cudaMemsetAsync(sa, 0, sizeof(float) * NL, stream));
-            if (fuse_gap) {
-                launch(finalize_large_kernel, 2, 1024, 0, stream, part, slice_grid(NL), 0, sc);
-            } else {
-                launch(lp_gap_kernel, kRedBlocks, kRedThreads, 0, stream, NL, alpha, u, sa, su, Q, part);
-                launch(finalize_sums_kernel, 1, 64, 0, stream, part, kRedBlocks, 2, 0, sc);
-            }
-            launch(lp_delta_kernel, 1, 1, 0, stream, sc, lambda);
-            DCRF_LAUNCH_CHECK();
         } while (pit < p.fw_max_iter);
         fw_total += pit;
         with_lc(L, [&](auto lc) {
@@ -1352,11 +1485,13 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             if (percent > p.less_confident_percent) break;
         }
     } while (it < p.prox_max_iter);
-    sync();
+    fetch_scalars();
+    // the two kernels of each qp-gamma iteration that ran inside a graph
+    g_kernel_launches.fetch_add(2ull * (unsigned long long)std::max(0, h_scal->gamma_sum - eager_gamma));
     if (stats) {
         stats->iterations = it;
         stats->inner_iters = fw_total;
-        stats->gamma_iters = gamma_total;
+        stats->gamma_iters = h_scal->gamma_sum;
         stats->energy = p.best_int ? best_int_energy : best_energy;
     }
     return it;
