@@ -362,6 +362,7 @@ dcrf_status dcrf_model_set_unary_dev(dcrf_model h, const float* d_unary) {
         DCRF_CUDA(cudaMemcpyAsync(u, d_unary, sizeof(float) * m.N * m.L, cudaMemcpyDeviceToDevice, m.stream));
         m.has_unary = true;
         m.logit_F = 0;  // a constant unary replaces the unary energy
+        m.gen++;
     });
 }
 
@@ -372,6 +373,7 @@ dcrf_status dcrf_model_set_unary(dcrf_model h, const float* unary) {
         upload(m.unary, unary, (size_t)m.N * m.L, m.stream);
         m.has_unary = true;
         m.logit_F = 0;  // a constant unary replaces the unary energy
+        m.gen++;
         m.sync();
     });
 }

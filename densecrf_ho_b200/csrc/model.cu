@@ -217,6 +217,7 @@ Model::~Model() {
         cudaEventDestroy(ev_side_join);
         cudaStreamDestroy(side);
     }
+    drop_qp_graph();
     if (gstream) cudaStreamDestroy(gstream);
     terms.clear();
     if (h_scal) cudaFreeHost(h_scal);
@@ -229,6 +230,7 @@ void Model::fetch_scalars() {
 }
 
 void Model::add_term(const float* d_features, int d, float w) {
+    gen++;  // a captured QP graph may hold what this changes
     auto t = std::make_unique<Term>();
     t->lat = std::make_unique<Lattice>();
     t->lat->stream = stream;
@@ -354,6 +356,7 @@ void Model::set_unary_logistic(const float* lw, const float* lf, int F) {
 // LogisticUnaryEnergy::setParameters (:58-63); the unary is recomputed, as
 // get() recomputes it at every use.
 void Model::set_unary_parameters(const float* lw) {
+    gen++;  // a captured QP graph may hold what this changes
     if (logit_F == 0) return;  // UnaryEnergy::setParameters is a no-op
     const size_t nw = (size_t)L * logit_F;
     h_logit_w.assign(lw, lw + nw);
@@ -422,6 +425,7 @@ void Model::set_parameters(int k, const float* v) {
 }
 
 void Model::set_cliques(int R_, const int* off, const int* idx, const float* expw, const float* cst) {
+    gen++;  // a captured QP graph may hold what this changes
     R = R_;
     h_cl_off.assign(off, off + R + 1);
     clique_total = off[R];
@@ -504,6 +508,7 @@ static void finish_compat(Model& m, const Term& t, const CompatRoute& r, float* 
 }
 
 void Model::set_compat(int k, int kind, const float* params) {
+    gen++;  // a captured QP graph may hold what this changes
     require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
     Term& t = *terms[k];
     // Every compatibility's parameters()(0) is also the weight of the term's

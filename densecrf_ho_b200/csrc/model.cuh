@@ -44,13 +44,27 @@ struct SolverScalars {
     int err;              // DCRF_E_* raised by a device check
     int done;             // batched QP: the image had stopped before this iteration
     int gamma_sum;        // LP: qp-gamma iterations of the whole solve
+    int chunk;            // QP graph: iterations in the current launch
 };
+
+constexpr int kQpChunk = 64;  // QP iterations per graph launch at most
 
 struct Model {
     int W = 0, H = 0, N = 0, L = 0, device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;  // second stream for the other terms' filter work
     cudaStream_t gstream = nullptr;  // captures the body of the LP's qp-gamma loop
+    // The QP loop as a graph (see Model::qp), its key and its kernels per
+    // iteration; gen counts the changes to the model that a graph may hold.
+    cudaGraphExec_t qp_graph = nullptr;
+    std::vector<const void*> qp_key;
+    unsigned long long qp_graph_kernels = 0;
+    bool qp_graph_failed = false;
+    unsigned long long gen = 0;
+    std::vector<const void*> qp_graph_key(const float* Q, int max_iter);
+    void drop_qp_graph();
+    template <typename F>
+    void build_qp_graph(F&& qp_iter);
     cudaEvent_t ev_side_fork = nullptr, ev_side_join = nullptr;
     bool has_unary = false;
     DevBuf<float> unary;

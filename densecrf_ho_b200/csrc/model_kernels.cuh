@@ -73,7 +73,16 @@ __global__ void finalize_sums_kernel(const double* __restrict__ partials, int nb
     const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (j >= nv) return;
     double s = 0.0;
-    for (int b = lane; b < nblk; b += 32) s += partials[(long)j * nblk + b];
+    const double* p = partials + (long)j * nblk;
+    int b = lane;
+    for (; b + 7 * 32 < nblk; b += 8 * 32) {  // loads batched, sums in order
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = p[b + i * 32];
+#pragma unroll
+        for (int i = 0; i < 8; i++) s += x[i];
+    }
+    for (; b < nblk; b += 32) s += p[b];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
     if (lane == 0) sc->sums[dst + j] = s;
@@ -84,7 +93,18 @@ __global__ void finalize_large_kernel(const double* __restrict__ partials, int n
     __shared__ double s[32];
     const int j = blockIdx.x;
     double v = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v += partials[(long)j * nblk + b];
+    const double* p = partials + (long)j * nblk;
+    const int bd = blockDim.x;
+    int b = threadIdx.x;
+    // eight loads in flight, then their sums in the same order as one at a time
+    for (; b + 7 * bd < nblk; b += 8 * bd) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = p[b + i * bd];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v += x[i];
+    }
+    for (; b < nblk; b += bd) v += p[b];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFullMask, v, o);
     if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;

@@ -118,6 +118,13 @@ __global__ void qp_energy_kernel(SolverScalars* sc, int max_iter) {
     else sc->stop = !((sc->old_energy - e) > 100.0);
 }
 
+// Loop condition of the QP graph: go on while the stop rule has not fired,
+// for at most `cap` iterations per graph launch.
+__global__ void qp_cond_kernel(SolverScalars* sc, int cap, cudaGraphConditionalHandle h) {
+    const int c = ++sc->chunk;
+    cudaGraphSetConditional(h, (!sc->stop && c < cap) ? 1u : 0u);
+}
+
 __global__ void qp_init_energy_kernel(SolverScalars* sc, int nterms, int max_iter) {
     // compute_LR_QP_value(Q, 0) + clique term (src/densecrf.cpp:386-387)
     double e = 0.0;
@@ -1070,6 +1077,76 @@ constexpr int kPix = 128;
 }  // namespace
 
 // ---------------------------------------------------------------- QP host --
+// Everything a captured QP iteration holds by address or by value that can
+// change between solves.
+std::vector<const void*> Model::qp_graph_key(const float* Q, int max_iter) {
+    std::vector<const void*> k = {Q, (const void*)(intptr_t)max_iter, (const void*)(uintptr_t)gen, unary.get(),
+                                  scal.get(), partials.get(), ipart.get(), ho_pre.get(), cl_off.get(), cl_idx.get()};
+    for (int i = 0; i < 16; i++) k.push_back(b[i].get());
+    for (const auto& t : terms) {
+        k.push_back(t->lat->va.get());
+        k.push_back(t->lat->vb.get());
+        k.push_back(t->norm.get());
+        k.push_back(t->cw.get());
+    }
+    k.push_back(compat_tmp.get());
+    return k;
+}
+
+void Model::drop_qp_graph() {
+    if (qp_graph) cudaGraphExecDestroy(qp_graph);
+    qp_graph = nullptr;
+    qp_key.clear();
+}
+
+template <typename F>
+void Model::build_qp_graph(F&& qp_iter) {
+    drop_qp_graph();
+    SolverScalars* sc = scal.get();
+    cudaGraph_t g = nullptr;
+    DCRF_CUDA(cudaGraphCreate(&g, 0));
+    bool capturing = false;
+    try {
+        cudaGraphConditionalHandle h;
+        DCRF_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaMemsetParams mp = {};
+        mp.dst = &sc->chunk;
+        mp.value = 0;
+        mp.elementSize = sizeof(int);
+        mp.width = 1;
+        mp.height = 1;
+        cudaGraphNode_t mn, wn;
+        DCRF_CUDA(cudaGraphAddMemsetNode(&mn, g, nullptr, 0, &mp));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        DCRF_CUDA(cudaGraphAddNode(&wn, g, &mn, 1, &np));
+        const unsigned long long k0 = g_kernel_launches.load();
+        DCRF_CUDA(cudaStreamBeginCaptureToGraph(stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeRelaxed));
+        capturing = true;
+        qp_iter();
+        launch(qp_cond_kernel, 1, 1, 0, stream, sc, kQpChunk, h);
+        cudaGraph_t bo = nullptr;
+        capturing = false;
+        DCRF_CUDA(cudaStreamEndCapture(stream, &bo));
+        const unsigned long long captured = g_kernel_launches.load() - k0;
+        g_kernel_launches.fetch_sub(captured);  // counted per iteration when the graph runs
+        require(captured >= 2, DCRF_E_STATE, "qp: unexpected loop body");
+        qp_graph_kernels = captured;
+        DCRF_CUDA(cudaGraphInstantiate(&qp_graph, g, 0));
+        cudaGraphDestroy(g);
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        if (capturing) cudaStreamEndCapture(stream, &junk);
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+}
+
 int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
     require(has_unary, DCRF_E_STATE, "qp: no unary energy set");
     const long NL = (long)N * L;
@@ -1136,9 +1213,8 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
     launch(qp_init_energy_kernel, 1, 1, 0, stream, sc, nt, max_iter);
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
-    int guard = 0;
-    while (!h_scal->stop) {
-        require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
+    // One Frank-Wolfe iteration (src/densecrf.cpp:389-436) and its stop test.
+    auto qp_iter = [&]() {
         with_lc(L, [&](auto lc) {
             constexpr int LC = decltype(lc)::value;
             if constexpr (LC > 0) {
@@ -1181,7 +1257,34 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         }
         launch(qp_energy_kernel, 1, 1, 0, stream, sc, max_iter);
         DCRF_LAUNCH_CHECK();
+    };
+    // After the first iteration (eager: it sizes every buffer) the loop runs
+    // as a CUDA graph: a `while` node whose body is one iteration and whose
+    // condition qp_cond_kernel sets -- until the stop rule fires, or kQpChunk
+    // iterations per launch, after which the host looks at the stop flag and
+    // launches it again.  The graph is kept for later solves with the same
+    // buffers and model.
+    const std::vector<const void*> key = qp_graph_key(Q, max_iter);
+    int guard = 0;
+    while (!h_scal->stop) {
+        require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
+        if (qp_graph && key == qp_key) {
+            DCRF_CUDA(cudaGraphLaunch(qp_graph, stream));
+            fetch_scalars();
+            g_kernel_launches.fetch_add(qp_graph_kernels * (unsigned long long)h_scal->chunk);
+            continue;
+        }
+        qp_iter();
         fetch_scalars();
+        if (!h_scal->stop && !qp_graph_failed) {
+            try {
+                build_qp_graph(qp_iter);
+                qp_key = key;
+            } catch (const Error&) {
+                drop_qp_graph();
+                qp_graph_failed = true;  // this device or driver cannot run it: stay eager
+            }
+        }
     }
     if (energy_out) *energy_out = h_scal->energy;
     return h_scal->steps;

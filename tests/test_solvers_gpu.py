@@ -292,3 +292,30 @@ def test_logistic_unary_vs_reference():
     assert not np.array_equal(m.unary_init(), Q)
     m.setUnaryEnergy(np.zeros((W * H, L), np.float32))
     assert m.unary_gradient(g["b"]).size == 0
+
+
+def test_qp_graph_follows_model_changes():
+    """The QP loop runs as a CUDA graph kept between solves; a change of the
+    model (a term's weight) must reach the next solve: its output equals a
+    fresh model's with the new weight, bit for bit, as does a repeat solve."""
+    W, H, L = 64, 48, 21
+    img = synth.make_image(W, H, L, 11)
+
+    def model(w_bilat):
+        m = DenseCRF2D(W, H, L)
+        m.setUnaryEnergy(img["unary"])
+        m.addPairwiseGaussian(3.0, 3.0, 3.0)
+        m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], w_bilat)
+        return m
+
+    a = model(5.0)
+    Q0 = a.unary_init()
+    first, st1 = a.qp_inference_super_pixels_non_convex(Q0, max_iter=30, stats=True)
+    again, st2 = a.qp_inference_super_pixels_non_convex(Q0, max_iter=30, stats=True)
+    assert _eq(first, again) and st1.iterations == st2.iterations
+    a.pairwise_set_parameters(1, np.array([60.0], np.float32))
+    changed = a.qp_inference_super_pixels_non_convex(Q0, max_iter=30)
+    fresh = model(60.0).qp_inference_super_pixels_non_convex(Q0, max_iter=30)
+    assert _eq(changed, fresh)
+    assert not _eq(changed, first)
+    assert _eq(a.qp_inference_super_pixels_non_convex(Q0), model(60.0).qp_inference_super_pixels_non_convex(Q0))
