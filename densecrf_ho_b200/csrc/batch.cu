@@ -30,6 +30,13 @@ __global__ void bqp_begin_kernel(int B, SolverScalars* sc, int* __restrict__ don
 }
 
 // Number of images still iterating, for the host's loop test.
+// Loop condition of the batched QP graph: some image still running, at most
+// `cap` iterations per launch (counted in active[1]).
+__global__ void bqp_cond_kernel(int* active, int cap, cudaGraphConditionalHandle h) {
+    const int c = ++active[1];
+    cudaGraphSetConditional(h, (active[0] > 0 && c < cap) ? 1u : 0u);
+}
+
 __global__ void bqp_count_kernel(int B, const SolverScalars* __restrict__ sc, int* __restrict__ active) {
     __shared__ int s;
     if (threadIdx.x == 0) s = 0;
@@ -362,9 +369,9 @@ Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_)
     DCRF_CUDA(cudaGetDevice(&device));
     DCRF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
     DCRF_CUDA(cudaMallocHost(&h_scal, sizeof(SolverScalars) * B));
-    DCRF_CUDA(cudaMallocHost(&h_active, sizeof(int)));
+    DCRF_CUDA(cudaMallocHost(&h_active, 2 * sizeof(int)));
     scal.ensure(B);
-    d_active.ensure(1);
+    d_active.ensure(2);
     DCRF_CUDA(cudaMemsetAsync(d_done.ensure(B), 0, sizeof(int) * B, stream));
     long* po = d_pix_off.ensure(n + 1);
     DCRF_CUDA(cudaMemcpyAsync(po, pix_off.data(), sizeof(long) * (n + 1), cudaMemcpyHostToDevice, stream));
@@ -440,7 +447,7 @@ void Batch::unary_init(float* Q) {
 
 // One Frank-Wolfe iteration for every image that has not stopped, then the
 // count of images still running, copied to pinned host memory.
-void Batch::qp_iteration(float* Q, int max_iter) {
+void Batch::qp_iteration(float* Q, int max_iter, bool copy_active) {
     float* grad = buf(0);
     float* sx = buf(1);
     float* psi = buf(2);
@@ -474,7 +481,8 @@ void Batch::qp_iteration(float* Q, int max_iter) {
     launch(bfinalize_sums_kernel, B, 32, 0, stream, part, kRedBlocks, 1, 7, sc);
     launch(bqp_energy_kernel, sgrid, 256, 0, stream, B, sc, max_iter);
     launch(bqp_count_kernel, 1, 256, 0, stream, B, sc, d_active.get());
-    DCRF_CUDA(cudaMemcpyAsync(h_active, d_active.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+    if (copy_active)
+        DCRF_CUDA(cudaMemcpyAsync(h_active, d_active.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
 }
 
 int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* energies) {
@@ -512,8 +520,9 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
         require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
         if (graph && graph_q == Q && graph_max_iter == max_iter) {
             DCRF_CUDA(cudaGraphLaunch(graph, stream));
-            g_kernel_launches.fetch_add(graph_kernels);
+            DCRF_CUDA(cudaMemcpyAsync(h_active, d_active.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
             DCRF_CUDA(cudaStreamSynchronize(stream));
+            g_kernel_launches.fetch_add(graph_kernels * (unsigned long long)h_active[1]);
             continue;
         }
         if (!eager) {
@@ -525,24 +534,49 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
             eager = true;
             continue;
         }
-        // Capture one iteration; the loop then launches it.
+        // Capture the loop: [iteration counter = 0] -> while (running) { iteration }.
         drop_graph();
         cudaGraph_t g = nullptr;
-        const unsigned long long k0 = g_kernel_launches.load();
-        DCRF_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        DCRF_CUDA(cudaGraphCreate(&g, 0));
+        bool capturing = false;
         try {
-            qp_iteration(Q, max_iter);
+            cudaGraphConditionalHandle h;
+            DCRF_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+            cudaMemsetParams mp = {};
+            mp.dst = d_active.get() + 1;
+            mp.value = 0;
+            mp.elementSize = sizeof(int);
+            mp.width = 1;
+            mp.height = 1;
+            cudaGraphNode_t mn, wn;
+            DCRF_CUDA(cudaGraphAddMemsetNode(&mn, g, nullptr, 0, &mp));
+            cudaGraphNodeParams np = {};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = h;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            DCRF_CUDA(cudaGraphAddNode(&wn, g, &mn, 1, &np));
+            const unsigned long long k0 = g_kernel_launches.load();
+            DCRF_CUDA(cudaStreamBeginCaptureToGraph(stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeRelaxed));
+            capturing = true;
+            qp_iteration(Q, max_iter, false);
+            launch(bqp_cond_kernel, 1, 1, 0, stream, d_active.get(), kQpChunk, h);
+            cudaGraph_t bo = nullptr;
+            capturing = false;
+            DCRF_CUDA(cudaStreamEndCapture(stream, &bo));
+            graph_kernels = g_kernel_launches.load() - k0;
+            g_kernel_launches.fetch_sub(graph_kernels);  // counted per iteration when the graph runs
+            require(graph_kernels >= 2, DCRF_E_STATE, "qp: unexpected loop body");
+            DCRF_CUDA(cudaGraphInstantiate(&graph, g, 0));
+            cudaGraphDestroy(g);
         } catch (...) {
-            cudaStreamEndCapture(stream, &g);
-            if (g) cudaGraphDestroy(g);
+            cudaGraph_t junk = nullptr;
+            if (capturing) cudaStreamEndCapture(stream, &junk);
+            cudaGraphDestroy(g);
+            graph = nullptr;
             throw;
         }
-        DCRF_CUDA(cudaStreamEndCapture(stream, &g));
-        graph_kernels = g_kernel_launches.load() - k0;
-        g_kernel_launches.fetch_sub(graph_kernels);  // counted when the graph runs
-        const cudaError_t e = cudaGraphInstantiate(&graph, g, 0);
-        cudaGraphDestroy(g);
-        DCRF_CUDA(e);
         graph_q = Q;
         graph_max_iter = max_iter;
     }

@@ -5,7 +5,9 @@
 // its own single-image solve while each filter, direction and update runs as
 // one launch over all images; the filters skip the lattice vertices and
 // pixels of images that have already stopped.  After a first eager
-// iteration, an iteration is captured once as a CUDA graph and replayed.
+// iteration the loop is captured once as a CUDA graph -- a `while` node whose
+// body is one iteration and whose condition is "some image still running"
+// (at most kQpChunk iterations per launch) -- and replayed.
 #pragma once
 #include <memory>
 #include <vector>
@@ -28,9 +30,9 @@ struct Batch {
     DevBuf<float> b[6];
     DevBuf<double> partials;
     DevBuf<SolverScalars> scal;  // one per image
-    DevBuf<int> d_active;
+    DevBuf<int> d_active;        // [0] images still running, [1] iterations in the current graph launch
     DevBuf<int> d_done;          // per image: stopped before the current iteration (filters skip it)
-    int* h_active = nullptr;     // pinned
+    int* h_active = nullptr;     // pinned, [2]: copy of d_active
     SolverScalars* h_scal = nullptr;  // pinned, B
     int max_tiles = 0;           // row-tile blocks of the largest image
 
@@ -68,7 +70,7 @@ struct Batch {
     void set_weight(int k, float w);
 
   private:
-    void qp_iteration(float* Q, int max_iter);
+    void qp_iteration(float* Q, int max_iter, bool copy_active = true);
     void drop_graph();
 };
 
