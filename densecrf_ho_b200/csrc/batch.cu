@@ -525,7 +525,7 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
             g_kernel_launches.fetch_add(graph_kernels * (unsigned long long)h_active[1]);
             continue;
         }
-        if (!eager) {
+        if (!eager || !graphs_enabled()) {
             // The first iteration runs eagerly: it sizes every buffer that an
             // iteration touches, so none is allocated during the capture.
             qp_iteration(Q, max_iter);

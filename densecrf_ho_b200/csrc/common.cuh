@@ -1,6 +1,7 @@
 // Shared helpers of libdcrf_cuda: status plumbing, device buffers, and the
 // exact-rounding arithmetic the reference's SSE2 build performs.
 #pragma once
+#include <cstdlib>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -61,6 +62,18 @@ struct DevBuf {
 };
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// The solver loops run as CUDA graphs with device-side while nodes unless the
+// environment sets DCRF_GRAPHS=0 (then every iteration is launched from the
+// host, kernel by kernel: for profilers that do not follow conditional graph
+// nodes).  Results are the same either way.
+inline bool graphs_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("DCRF_GRAPHS");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
 
 // Process-wide count of kernels this library has launched (benchmarks read
 // it through dcrf_kernel_launches()).

@@ -1276,7 +1276,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         }
         qp_iter();
         fetch_scalars();
-        if (!h_scal->stop && !qp_graph_failed) {
+        if (!h_scal->stop && !qp_graph_failed && graphs_enabled()) {
             try {
                 build_qp_graph(qp_iter);
                 qp_key = key;
@@ -1451,7 +1451,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     } fwg;
     cudaGraphExec_t* fw_graph = fwg.g;
     unsigned long long fw_graph_kernels = 0;
-    bool graphs_ok = true;
+    bool graphs_ok = graphs_enabled();
     int eager_gamma = 0;
     auto drop_graphs = [&]() { fwg.drop(); };
     auto build_graph = [&](bool pending) -> cudaGraphExec_t {
