@@ -880,7 +880,7 @@ __global__ void ord_blur_kernel(int M, int row4r, const int2* __restrict__ nbr,
 // tmp.Q and tmp.tmp (src/densecrf.cpp:725-729).
 // DC / LC: d and L as compile-time constants (0 = run-time drt / Lrt).
 template <bool GAP, int DC, int LC>
-__global__ void ord_slice_kernel(int N, int Lrt, int drt, const int* __restrict__ offset,
+__global__ void __launch_bounds__(kTB, 8) ord_slice_kernel(int N, int Lrt, int drt, const int* __restrict__ offset,
                                  const float* __restrict__ bary, const float* __restrict__ vals,
                                  const float2* __restrict__ bins, float alpha, float* out, SliceEpilogue ep,
                                  GapFusion gf) {
@@ -967,7 +967,7 @@ __device__ __forceinline__ float ord_slice_acc(const OrdSliceTerm& s, int i, int
 // coef_1 * scaled(slice_1) as ord_slice_kernel computes it from base = v0.
 // The value v0 never leaves the register; GAP as in ord_slice_kernel.
 template <bool GAP, int D0, int D1, int LC>
-__global__ void ord_slice_pair_kernel(int N, int Lrt, OrdSliceTerm t0, OrdSliceTerm t1,
+__global__ void __launch_bounds__(kTB, 8) ord_slice_pair_kernel(int N, int Lrt, OrdSliceTerm t0, OrdSliceTerm t1,
                                       const float2* __restrict__ bins, float* out, GapFusion gf) {
     const int L = LC ? LC : Lrt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
