@@ -203,6 +203,32 @@ class DenseCRF2D:
         check(lib().dcrf_model_add_pairwise(self._h, f.ctypes.data_as(C.c_void_p), f.shape[1],
                                             C.c_float(w)))
 
+    CONST_KERNEL, DIAG_KERNEL, FULL_KERNEL = 0, 1, 2
+    NO_NORMALIZATION, NORMALIZE_BEFORE, NORMALIZE_AFTER, NORMALIZE_SYMMETRIC = 0, 1, 2, 3
+
+    def setKernel(self, k, ktype=1, ntype=3):
+        """Term k's KernelType and NormalizationType (addPairwiseEnergy's last
+        two arguments; the defaults are DIAG_KERNEL, NORMALIZE_SYMMETRIC)."""
+        check(lib().dcrf_model_set_kernel(self._h, int(k), int(ktype), int(ntype)))
+
+    def pairwise_kernel_parameters(self, k):
+        """``pairwise_[k]->kernelParameters()``."""
+        n = C.c_int(0)
+        check(lib().dcrf_model_pairwise_kernel_parameters(self._h, int(k), None, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        if n.value:
+            check(lib().dcrf_model_pairwise_kernel_parameters(self._h, int(k), out.ctypes.data_as(C.c_void_p),
+                                                              None))
+        return out
+
+    def pairwise_set_kernel_parameters(self, k, p):
+        """``pairwise_[k]->setKernelParameters(p)``: rebuilds the term's lattice
+        on the scaled (DIAG) or transformed (FULL, p column-major) features."""
+        p = np.ascontiguousarray(p, np.float32).reshape(-1)
+        if p.size != self.pairwise_kernel_parameters(k).size:
+            raise DCRFError(1, "wrong number of kernel parameters")
+        check(lib().dcrf_model_pairwise_set_kernel_parameters(self._h, int(k), p.ctypes.data_as(C.c_void_p)))
+
     def setCompatibility(self, k, diagonal=None, matrix=None, potts=None):
         """Label compatibility of term k: ``diagonal`` (L weights,
         DiagonalCompatibility), ``matrix`` (L x L, MatrixCompatibility, used as

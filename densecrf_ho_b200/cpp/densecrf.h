@@ -9,13 +9,12 @@
 // ("Value out of bounds", "Maxval < 0, skipping") are thrown as
 // std::runtime_error with the same text, every other failure too.
 //
-// Scope (the B200 path): Potts, Diagonal and Matrix compatibilities, DIAG_KERNEL with
-// NORMALIZE_SYMMETRIC (and its NO_NORMALIZATION copy), constant unaries, the
+// Scope (the B200 path): Potts, Diagonal and Matrix compatibilities, every
+// KernelType and NormalizationType (and the NO_NORMALIZATION copy), constant unaries, the
 // qp / lp / qp_sp / lp_sp solvers.  Superpixel cliques are given as a
 // per-pixel region map (addSuperPixel's segmentation step, EDISON mean-shift,
 // stays with the caller); the clique weights are derived from the image
-// exactly as src/densecrf.cpp:212-247 does.  Other kernel types and
-// normalisations throw std::runtime_error.
+// exactly as src/densecrf.cpp:212-247 does.
 //
 // Header-only; needs Eigen (the reference vendors 3.2.7) and include/dcrf.h.
 #pragma once
@@ -128,11 +127,16 @@ inline void set_compat(dcrf_model m, int k, const Compat& c) {
     if (c.kind != DCRF_COMPAT_POTTS && dcrf_model_set_compat(m, k, c.kind, c.p.data()) != DCRF_OK)
         throw std::runtime_error(dcrf_last_error());
 }
-inline void check_kernel(KernelType k, NormalizationType n) {
-    if (k != DIAG_KERNEL && k != CONST_KERNEL)
-        throw std::runtime_error("only DIAG_KERNEL pairwise kernels run on the B200 path");
-    if (n != NORMALIZE_SYMMETRIC)
-        throw std::runtime_error("only NORMALIZE_SYMMETRIC pairwise kernels run on the B200 path");
+// Gives term k of model m the kernel and normalisation types (the model's
+// terms start as DIAG_KERNEL, NORMALIZE_SYMMETRIC).
+inline void check_types(KernelType kt, NormalizationType nt) {  // before a term is added
+    if ((int)kt < CONST_KERNEL || (int)kt > FULL_KERNEL) throw std::runtime_error("unknown kernel type");
+    if ((int)nt < NO_NORMALIZATION || (int)nt > NORMALIZE_SYMMETRIC)
+        throw std::runtime_error("unknown normalization type");
+}
+inline void set_kernel(dcrf_model m, int k, KernelType kt, NormalizationType nt) {
+    if (kt == DIAG_KERNEL && nt == NORMALIZE_SYMMETRIC) return;
+    if (dcrf_model_set_kernel(m, k, (int)kt, (int)nt) != DCRF_OK) throw std::runtime_error(dcrf_last_error());
 }
 }  // namespace dcrf_shim
 
@@ -243,6 +247,8 @@ private:
 class PairwisePotential {
     MatrixXf f_;
     dcrf_shim::Compat c_;
+    KernelType kt_;
+    NormalizationType nt_;
     int L_ = 0;
     dcrf_model m_ = nullptr;
     PairwisePotential(const PairwisePotential&) = delete;
@@ -253,13 +259,14 @@ class PairwisePotential {
         dcrf_shim::check(dcrf_model_create(&m_, (int)f_.cols(), 1, L));
         dcrf_shim::check(dcrf_model_add_pairwise(m_, f_.data(), (int)f_.rows(), c_.p.at(0)));
         dcrf_shim::set_compat(m_, 0, c_);
+        dcrf_shim::set_kernel(m_, 0, kt_, nt_);
         L_ = L;
     }
 public:
     PairwisePotential(const MatrixXf& features, LabelCompatibility* compatibility, KernelType ktype = CONST_KERNEL,
                       NormalizationType ntype = NORMALIZE_SYMMETRIC)
-        : f_(features), c_(dcrf_shim::take_compat(compatibility)) {
-        dcrf_shim::check_kernel(ktype, ntype);
+        : f_(features), c_(dcrf_shim::take_compat(compatibility)), kt_(ktype), nt_(ntype) {
+        dcrf_shim::check_types(ktype, ntype);
     }
     ~PairwisePotential() {
         if (m_) dcrf_model_destroy(m_);
@@ -316,9 +323,11 @@ public:
                                    KernelType kernel_type = DIAG_KERNEL,
                                    NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
         const dcrf_shim::Compat c = dcrf_shim::take_compat(function);
-        dcrf_shim::check_kernel(kernel_type, normalization_type);
+        dcrf_shim::check_types(kernel_type, normalization_type);
         dcrf_shim::check(dcrf_model_add_pairwise(m_, features.data(), (int)features.rows(), c.p.at(0)));
-        dcrf_shim::set_compat(m_, n_terms_++, c);
+        const int k = n_terms_++;
+        dcrf_shim::set_compat(m_, k, c);
+        dcrf_shim::set_kernel(m_, k, kernel_type, normalization_type);
     }
     void setUnaryEnergy(const MatrixXf& unary) { dcrf_shim::check(dcrf_model_set_unary(m_, unary.data())); }
     void setUnaryEnergy(UnaryEnergy* unary) {
@@ -423,18 +432,22 @@ public:
                              KernelType kernel_type = DIAG_KERNEL,
                              NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
         const dcrf_shim::Compat c = dcrf_shim::take_compat(function);
-        dcrf_shim::check_kernel(kernel_type, normalization_type);
+        dcrf_shim::check_types(kernel_type, normalization_type);
         dcrf_shim::check(dcrf_model_add_gaussian(m_, sx, sy, c.p.at(0)));
-        dcrf_shim::set_compat(m_, n_terms_++, c);
+        const int k = n_terms_++;
+        dcrf_shim::set_compat(m_, k, c);
+        dcrf_shim::set_kernel(m_, k, kernel_type, normalization_type);
     }
     // addPairwiseBilateral (src/densecrf.cpp:179-190)
     void addPairwiseBilateral(float sx, float sy, float sr, float sg, float sb, const unsigned char* im,
                               LabelCompatibility* function = NULL, KernelType kernel_type = DIAG_KERNEL,
                               NormalizationType normalization_type = NORMALIZE_SYMMETRIC) {
         const dcrf_shim::Compat c = dcrf_shim::take_compat(function);
-        dcrf_shim::check_kernel(kernel_type, normalization_type);
+        dcrf_shim::check_types(kernel_type, normalization_type);
         dcrf_shim::check(dcrf_model_add_bilateral(m_, sx, sy, sr, sg, sb, im, c.p.at(0)));
-        dcrf_shim::set_compat(m_, n_terms_++, c);
+        const int k = n_terms_++;
+        dcrf_shim::set_compat(m_, k, c);
+        dcrf_shim::set_kernel(m_, k, kernel_type, normalization_type);
     }
     using DenseCRF::setUnaryEnergy;
 };

@@ -77,7 +77,7 @@ int main(int argc, char** argv) {
             printf("range_error %s\n", e.what());
         }
         try {
-            crf.addPairwiseGaussian(3, 3, new PottsCompatibility(1), DIAG_KERNEL, NORMALIZE_AFTER);
+            crf.addPairwiseGaussian(3, 3, new PottsCompatibility(1), DIAG_KERNEL, (NormalizationType)7);
             printf("kernel_error missing\n");
         } catch (const std::runtime_error& e) {
             printf("kernel_error ok\n");

@@ -462,6 +462,33 @@ dcrf_status dcrf_model_add_bilateral(dcrf_model h, float sx, float sy, float sr,
     });
 }
 
+dcrf_status dcrf_model_set_kernel(dcrf_model h, int k, int ktype, int ntype) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        m.set_kernel(k, ktype, ntype);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_kernel_parameters(dcrf_model h, int k, float* params, int* n) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        const int c = m.kernel_parameters(k, params);
+        if (n) *n = c;
+    });
+}
+
+dcrf_status dcrf_model_pairwise_set_kernel_parameters(dcrf_model h, int k, const float* params) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        if (m.kernel_parameters(k, nullptr) == 0) return;
+        need(params, "params");
+        m.set_kernel_parameters(k, params);
+    });
+}
+
 dcrf_status dcrf_model_set_compat(dcrf_model h, int k, int kind, const float* params) {
     return guard([&] {
         auto& m = M(h);
@@ -725,8 +752,8 @@ dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model h, int k, const float
         const size_t n = (size_t)m.N * m.L;
         const float* db = upload(h->io0, b, n, m.stream);
         const float* dq = upload(h->io1, Q, n, m.stream);
-        m.kernel_gradient(k, db, dq, grad);
-        if (d) *d = m.terms[k]->d;
+        const int n_out = m.kernel_gradient(k, db, dq, grad);
+        if (d) *d = n_out;
     });
 }
 

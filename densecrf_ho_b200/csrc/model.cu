@@ -53,10 +53,30 @@ __global__ void fill_kernel(long n, float v, float* x) {
     if (t < n) x[t] = v;
 }
 
-// norm = 1 / sqrt(K 1 + 1e-20), in double like src/pairwise.cpp:50.
-__global__ void norm_kernel(int N, float* x) {
+// norm = 1 / sqrt(K 1 + 1e-20) (symmetric) or 1 / (K 1 + 1e-20), in double
+// like src/pairwise.cpp:44-56.
+__global__ void norm_kernel(int N, float* x, int symmetric) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < N) x[i] = (float)(1.0 / sqrt(dadd((double)x[i], 1e-20)));
+    if (i >= N) return;
+    const double s = dadd((double)x[i], 1e-20);
+    x[i] = (float)(symmetric ? 1.0 / sqrt(s) : 1.0 / s);
+}
+
+// f'(i, :) = diag(p) f(i, :) (DIAG_KERNEL) or P f(i, :) with P d x d
+// column-major, summed over the inner index in order (FULL_KERNEL).
+__global__ void scale_features_kernel(int N, int d, const float* __restrict__ f, const float* __restrict__ p,
+                                      int full, float* __restrict__ out) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)N * d) return;
+    const long i = t / d;
+    const int r = (int)(t - i * d);
+    if (!full) {
+        out[t] = fmul(p[r], f[t]);
+        return;
+    }
+    float acc = fmul(p[r], f[i * d]);
+    for (int c = 1; c < d; c++) acc = fadd(acc, fmul(p[r + (long)c * d], f[i * d + c]));
+    out[t] = acc;
 }
 
 // ---- kernel-parameter gradient (src/pairwise.cpp:90-122, 170-181, 402-407) --
@@ -239,13 +259,74 @@ void Model::add_term(const float* d_features, int d, float w) {
     t->d = d;
     float* tf = t->feat.ensure((size_t)N * d);
     DCRF_CUDA(cudaMemcpyAsync(tf, d_features, sizeof(float) * (size_t)N * d, cudaMemcpyDeviceToDevice, stream));
-    float* nrm = t->norm.ensure(N);
+    t->kparams.assign(d, 1.0f);
+    compute_norm(*t);
+    terms.push_back(std::move(t));
+}
+
+// DenseKernel::initLattice's normalisation (src/pairwise.cpp:40-57): K 1 on
+// the term's lattice, then per NormalizationType.
+void Model::compute_norm(Term& t) {
+    if (t.ntype == kNoNorm) return;
+    float* nrm = t.norm.ensure(N);
     launch(fill_kernel, ceil_div(N, 256), 256, 0, stream, N, 1.0f, nrm);
     SliceEpilogue ep;  // plain output
-    t->lat->compute(nrm, nrm, 1, false, ep);
-    launch(norm_kernel, ceil_div(N, 256), 256, 0, stream, N, nrm);
+    t.lat->compute(nrm, nrm, 1, false, ep);
+    launch(norm_kernel, ceil_div(N, 256), 256, 0, stream, N, nrm, (int)(t.ntype == kNormSymmetric));
     DCRF_LAUNCH_CHECK();
-    terms.push_back(std::move(t));
+}
+
+void Model::set_kernel(int k, int ktype, int ntype) {
+    gen++;  // a captured QP graph may hold what this changes
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+    require(ktype >= kConstKernel && ktype <= kFullKernel, DCRF_E_ARG, "unknown kernel type");
+    require(ntype >= kNoNorm && ntype <= kNormSymmetric, DCRF_E_ARG, "unknown normalization type");
+    Term& t = *terms[k];
+    t.ktype = ktype;
+    if (ktype == kDiagKernel) t.kparams.assign(t.d, 1.0f);
+    else if (ktype == kFullKernel) {
+        t.kparams.assign((size_t)t.d * t.d, 0.0f);
+        for (int j = 0; j < t.d; j++) t.kparams[(size_t)j * t.d + j] = 1.0f;
+    } else t.kparams.clear();
+    if (ntype != t.ntype) {
+        t.ntype = ntype;
+        compute_norm(t);
+    }
+    sync();
+}
+
+int Model::kernel_parameters(int k, float* out) const {
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+    const Term& t = *terms[k];
+    if (out) std::copy(t.kparams.begin(), t.kparams.end(), out);
+    return (int)t.kparams.size();
+}
+
+// DenseKernel::setParameters (src/pairwise.cpp:157-168): the lattice is
+// rebuilt on diag(p) f or P f; the unnormalised twin keeps the lattice of the
+// features the term was added with, as the reference's no_norm_pairwise_
+// does.  CONST_KERNEL has no parameters (no-op).
+void Model::set_kernel_parameters(int k, const float* p) {
+    gen++;
+    require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+    Term& t = *terms[k];
+    if (t.ktype == kConstKernel) return;
+    const bool full = t.ktype == kFullKernel;
+    const size_t np = full ? (size_t)t.d * t.d : (size_t)t.d;
+    t.kparams.assign(p, p + np);
+    DevBuf<float> dp, sf;
+    DCRF_CUDA(cudaMemcpyAsync(dp.ensure(np), p, sizeof(float) * np, cudaMemcpyHostToDevice, stream));
+    float* scaled = sf.ensure((size_t)N * t.d);
+    launch(scale_features_kernel, ceil_div((long)N * t.d, 256), 256, 0, stream, N, t.d, (const float*)t.feat.get(),
+           (const float*)dp.get(), (int)full, scaled);
+    DCRF_LAUNCH_CHECK();
+    auto lat = std::make_unique<Lattice>();
+    lat->stream = stream;
+    lat->build(scaled, t.d, N);
+    if (!t.twin) t.twin = std::move(t.lat);
+    t.lat = std::move(lat);
+    compute_norm(t);
+    sync();
 }
 
 // pairwise_[k]->kernelGradient(b, Q) for a diagonal kernel with symmetric
@@ -254,8 +335,11 @@ void Model::add_term(const float* d_features, int d, float w) {
 // gradient, fa = K^T(b n), fb = K(lbl n), X = 0.5 (b o fb + fa o lbl) n^3;
 // the result is sum_i f(i, j) fg(i, j) per dimension j (FP64 sum, rounded to
 // float -- the reference sums in float).
-void Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
+int Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
     Term& t = *terms[k];
+    if (t.ktype == kConstKernel) return 0;  // DenseKernel::gradient: no parameters
+    require(t.ktype == kDiagKernel && t.ntype == kNormSymmetric, DCRF_E_STATE,
+            "kernel gradient: DIAG_KERNEL with NORMALIZE_SYMMETRIC only");
     Lattice& lat = *t.lat;
     const long NL = (long)N * L;
     const int d = t.d, g = ceil_div(NL, 256);
@@ -292,6 +376,7 @@ void Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
         for (int i = 0; i < nb; i++) s += h[(size_t)j * nb + i];
         out[j] = (float)s;
     }
+    return d;
 }
 
 // pairwise_[k]->gradient(b, Q) (src/pairwise.cpp:390-395): the
@@ -306,9 +391,9 @@ int Model::compat_gradient(int k, const float* b, const float* Q, float* out) {
     float* fq = buf(8);
     SliceEpilogue ep;
     ep.potts = true;
-    ep.norm = t.norm.get();
+    ep.norm = t.post_norm();
     ep.scale = 1.0f;
-    t.lat->compute(fq, Q, L, false, ep, t.norm.get());
+    t.lat->compute(fq, Q, L, false, ep, t.pre_norm());
     double* part = partials.get();
     if (t.compat == kPotts) {
         const int nb = 128;
@@ -539,10 +624,12 @@ void Model::apply(int k, bool nonorm, float* out, const float* in, const float* 
                   bool zero_base) {
     Term& t = *terms[k];
     SliceEpilogue ep;
-    ep.norm = nonorm ? nullptr : t.norm.get();
-    // nonorm: the unnormalised Potts twin of the term, whatever its compatibility
+    ep.norm = nonorm ? nullptr : t.post_norm();
+    // nonorm: the unnormalised Potts twin of the term, whatever its
+    // compatibility, on the lattice of the features the term was added with
     const CompatRoute r = route_compat(*this, t, ep, out, base, coef, zero_base, nonorm);
-    t.lat->compute(r.slice_out, in, L, false, ep, nonorm ? nullptr : t.norm.get());
+    Lattice& lat = nonorm ? t.twin_lat() : *t.lat;
+    lat.compute(r.slice_out, in, L, false, ep, nonorm ? nullptr : t.pre_norm());
     finish_compat(*this, t, r, out, base, coef, zero_base);
 }
 

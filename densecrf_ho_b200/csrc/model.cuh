@@ -13,12 +13,29 @@ namespace dcrf {
 // Label compatibility of a pairwise term (include/labelcompatibility.h).
 enum CompatKind { kPotts = 0, kDiagonal = 1, kMatrix = 2 };
 
+// DenseKernel's KernelType and NormalizationType (include/pairwise.h).
+enum KernelKind { kConstKernel = 0, kDiagKernel = 1, kFullKernel = 2 };
+enum NormKind { kNoNorm = 0, kNormBefore = 1, kNormAfter = 2, kNormSymmetric = 3 };
+
 struct Term {
     std::unique_ptr<Lattice> lat;
+    // The unnormalised twin's lattice (no_norm_pairwise_, built on the
+    // features the term was added with) once setKernelParameters has rebuilt
+    // lat on scaled features; until then the twin shares lat.
+    std::unique_ptr<Lattice> twin;
+    int ktype = kDiagKernel, ntype = kNormSymmetric;
+    std::vector<float> kparams;  // DenseKernel::parameters_: DIAG d scales, FULL d x d (column-major)
     int compat = kPotts;  // Potts: mu = -w [a == b]; Diagonal: cw[L]; Matrix: cw[L x L], symmetrised
     DevBuf<float> cw;
     std::vector<float> hcw;  // host copy of cw
-    DevBuf<float> norm;  // 1/sqrt(K 1 + 1e-20) (src/pairwise.cpp:46-50)
+    DevBuf<float> norm;  // 1/sqrt(K 1 + 1e-20) (symmetric) or 1/(K 1 + 1e-20) (src/pairwise.cpp:44-56)
+    const float* pre_norm() const {  // scale before the filter (DenseKernel::filter, not transposed)
+        return (ntype == kNormSymmetric || ntype == kNormBefore) ? norm.get() : nullptr;
+    }
+    const float* post_norm() const {  // scale after it
+        return (ntype == kNormSymmetric || ntype == kNormAfter) ? norm.get() : nullptr;
+    }
+    Lattice& twin_lat() { return twin ? *twin : *lat; }
     DevBuf<float> feat;  // the features [N][d] (DenseKernel::f_), for the kernel gradient
     float w = 0.0f;      // Potts weight
     int d = 0;
@@ -113,7 +130,13 @@ struct Model {
     // pairwise_[k]->kernelGradient(b, Q) (d floats: the diagonal kernel's
     // feature-scale gradient) and ->gradient(b, Q) (the Potts weight's);
     // b, Q device [N][L], results to host.
-    void kernel_gradient(int k, const float* b, const float* Q, float* out);
+    int kernel_gradient(int k, const float* b, const float* Q, float* out);  // returns the count
+    // addPairwiseEnergy's KernelType / NormalizationType for term k, and
+    // DenseKernel::parameters / setParameters (src/pairwise.cpp:123-168).
+    void set_kernel(int k, int ktype, int ntype);
+    int kernel_parameters(int k, float* out) const;
+    void set_kernel_parameters(int k, const float* p);
+    void compute_norm(Term& t);
     // LabelCompatibility::parameters / setParameters / gradient of term k:
     // 1 (Potts), L (Diagonal) or L (L + 1) / 2 (Matrix, upper triangle by
     // column) values; each returns that count.

@@ -189,6 +189,31 @@ dcrf_status dcrf_model_add_pairwise(dcrf_model m, const float* features, int d, 
  * MatrixCompatibility (params: L x L column-major m, used as 0.5 (m + m^T),
  * src/labelcompatibility.cpp:79-129).  A term starts as the Potts weight it
  * was added with. */
+/* The KernelType and NormalizationType of term k (addPairwiseEnergy's last
+ * two arguments, include/pairwise.h:33-40, src/pairwise.cpp:32-168).  A term
+ * starts as DIAG_KERNEL, NORMALIZE_SYMMETRIC (the reference's defaults).  The
+ * kernel type changes only the parameters (CONST none, DIAG d feature scales
+ * starting at 1, FULL a d x d column-major matrix starting at the identity);
+ * the normalisation changes the filter: out = n o K(n o in) (symmetric,
+ * n = 1/sqrt(K1 + 1e-20)), n o K(in) (after) or K(n o in) (before) with
+ * n = 1/(K1 + 1e-20), K(in) (none). */
+#define DCRF_KERNEL_CONST 0
+#define DCRF_KERNEL_DIAG 1
+#define DCRF_KERNEL_FULL 2
+#define DCRF_NORM_NONE 0
+#define DCRF_NORM_BEFORE 1
+#define DCRF_NORM_AFTER 2
+#define DCRF_NORM_SYMMETRIC 3
+dcrf_status dcrf_model_set_kernel(dcrf_model m, int k, int ktype, int ntype);
+/* pairwise_[k]->kernelParameters() / setKernelParameters(p)
+ * (src/pairwise.cpp:396-401, 146-168): *n receives the count (0 for
+ * CONST_KERNEL); params may be NULL to query it.  Setting them rebuilds the
+ * term's lattice on diag(p) f (DIAG) or P f (FULL, the product summed in
+ * order: float tolerance against Eigen's) from the features it was added
+ * with; the term's unnormalised twin (assignment energies) keeps the lattice
+ * of the original features, as the reference's no_norm_pairwise_ does. */
+dcrf_status dcrf_model_pairwise_kernel_parameters(dcrf_model m, int k, float* params, int* n);
+dcrf_status dcrf_model_pairwise_set_kernel_parameters(dcrf_model m, int k, const float* params);
 #define DCRF_COMPAT_POTTS 0
 #define DCRF_COMPAT_DIAGONAL 1
 #define DCRF_COMPAT_MATRIX 2
@@ -240,8 +265,9 @@ dcrf_status dcrf_model_energy_lp(dcrf_model m, const float* Q, double* energy);
 dcrf_status dcrf_model_lr_qp_value(dcrf_model m, const float* Q, double* energy);
 /* pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 90-122,
  * 170-181): the gradient of the diagonal kernel's feature scales, d floats
- * (d = 2 Gaussian, 5 bilateral; d is returned when not NULL; grad holds
- * at least 16 floats), and pairwise_[k]->gradient(b, Q) (:390-395): the
+ * (d = 2 Gaussian, 5 bilateral; the count is returned when not NULL, 0 for
+ * CONST_KERNEL; DIAG_KERNEL with NORMALIZE_SYMMETRIC, else DCRF_E_STATE;
+ * grad holds at least 16 floats), and pairwise_[k]->gradient(b, Q) (:390-395): the
  * compatibility's gradient, as many floats as its parameters.  b, Q [N][L]. */
 dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model m, int k, const float* b, const float* Q,
                                                 float* grad, int* d);

@@ -125,6 +125,9 @@ def ref_lib():
         L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         L.refm_kernel_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
         L.refm_parameters.argtypes = [vp, C.c_int, _f32p]
+        L.refm_add_features_kernel.argtypes = [vp, _f32p, C.c_int, C.c_float, C.c_int, C.c_int]
+        L.refm_kernel_parameters.argtypes = [vp, C.c_int, _f32p]
+        L.refm_set_kernel_parameters.argtypes = [vp, C.c_int, _f32p, C.c_int]
         L.refl_compute_ord_restricted.argtypes = [vp, _f32p, _f32p, _i32p, C.c_int, vp, C.c_int, C.c_int]
         L.refm_apply_ord_restricted.argtypes = [vp, C.c_int, _f32p, _f32p, _i32p, C.c_int, vp, C.c_int]
         L.refm_set_unary_logistic.argtypes = [vp, _f32p, _f32p, C.c_int]
@@ -321,6 +324,21 @@ class _Model:
         out = np.zeros(16, np.float32)
         n = self._lib.refm_kernel_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
         return out[:n]
+
+    def add_features_kernel(self, f, w, ktype, ntype):
+        """addPairwiseEnergy(f, Potts(w), ktype, ntype) (reference model only)."""
+        f = _c(f, np.float32)
+        self._lib.refm_add_features_kernel(self._h, f, f.shape[1], w, ktype, ntype)
+        self.nterms += 1
+
+    def kernel_parameters(self, k):
+        out = np.zeros(64, np.float32)
+        n = self._lib.refm_kernel_parameters(self._h, k, out)
+        return out[:n]
+
+    def set_kernel_parameters(self, k, p):
+        p = _c(p, np.float32).reshape(-1)
+        self._lib.refm_set_kernel_parameters(self._h, k, p, p.size)
 
     def set_unary_logistic(self, w, f):
         """setUnaryEnergy(new LogisticUnaryEnergy(W, f)): w [L][F] (row-major

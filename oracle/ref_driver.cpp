@@ -55,6 +55,8 @@ struct RefModel : public DenseCRF2D {
         return pairwise_[k]->gradient(b, Q);
     }
     VectorXf parameters(int k) const { return pairwise_[k]->parameters(); }
+    VectorXf kernel_parameters(int k) const { return pairwise_[k]->kernelParameters(); }
+    void set_kernel_parameters(int k, const VectorXf& v) { pairwise_[k]->setKernelParameters(v); }
     VectorXf unary_gradient(const MatrixXf& b) const { return unary_->gradient(b); }
     MatrixXf unary_get() const { return unary_->get(); }
     int N() const { return N_; }
@@ -250,6 +252,20 @@ void refm_add_features(void* h, const float* f, int d, float w) {
     RefModel* m = (RefModel*)h;
     MatrixXf F = Map<const MatrixXf>(f, d, m->N());
     m->addPairwiseEnergy(F, new PottsCompatibility(w));
+}
+// addPairwiseEnergy(F, Potts(w), KernelType ktype, NormalizationType ntype).
+void refm_add_features_kernel(void* h, const float* f, int d, float w, int ktype, int ntype) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf F = Map<const MatrixXf>(f, d, m->N());
+    m->addPairwiseEnergy(F, new PottsCompatibility(w), (KernelType)ktype, (NormalizationType)ntype);
+}
+int refm_kernel_parameters(void* h, int k, float* out) {
+    VectorXf p = ((RefModel*)h)->kernel_parameters(k);
+    if (p.size()) std::memcpy(out, p.data(), sizeof(float) * p.size());
+    return (int)p.size();
+}
+void refm_set_kernel_parameters(void* h, int k, const float* p, int n) {
+    ((RefModel*)h)->set_kernel_parameters(k, Map<const VectorXf>(p, n));
 }
 // Gaussian / bilateral term with a Diagonal (kind 1, params[L]) or Matrix
 // (kind 2, params[L*L] column-major) compatibility.

@@ -319,3 +319,59 @@ def test_qp_graph_follows_model_changes():
     assert _eq(changed, fresh)
     assert not _eq(changed, first)
     assert _eq(a.qp_inference_super_pixels_non_convex(Q0), model(60.0).qp_inference_super_pixels_non_convex(Q0))
+
+
+def test_kernel_and_normalization_types_vs_reference():
+    """NormalizationType none / before / after, setKernelParameters (a
+    diagonal kernel rebuilt on scaled features, its unnormalised twin on the
+    original ones) and CONST_KERNEL, against the reference's own values
+    (tests/golden/make_kernel_golden.py): filters, energies and QP bit for
+    bit, the kernel gradient to 1e-4 of its largest component."""
+    g = golden("kernel_24x18_L5.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+
+    def model(ktype=1, ntype=3):
+        m = DenseCRF2D(W, H, L)
+        m.setUnaryEnergy(img["unary"])
+        m.addPairwiseEnergy(synth.gaussian_features(W, H, 3.0, 3.0), 3.0)
+        m.setKernel(0, ktype, ntype)
+        m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+        return m
+
+    for t in (0, 1, 2):
+        pre = f"norm{t}_"
+        m = model(1, t)
+        Q = g[pre + "unary_init"]
+        for k in range(2):
+            assert _eq(m.pairwise_apply(k, Q), g[f"{pre}apply{k}"]), (t, k)
+            assert _eq(m.pairwise_apply(k, Q, nonorm=True), g[f"{pre}apply{k}_nonorm"]), (t, k)
+        assert m.compute_LR_QP_value(Q) == pytest.approx(float(g[pre + "e_lrqp"]), rel=1e-12)
+        out, st = m.qp_inference_super_pixels_non_convex(Q, max_iter=20, stats=True)
+        assert st.iterations == int(g[pre + "qp_iters"])
+        assert _eq(out, g[pre + "qp"])
+
+    pre = "kparam_"
+    m = model()
+    m.pairwise_set_kernel_parameters(1, g["kparam"])
+    Q = g[pre + "unary_init"]
+    for k in range(2):
+        assert np.array_equal(m.pairwise_kernel_parameters(k), g[f"{pre}kparams{k}"])
+        assert _eq(m.pairwise_apply(k, Q), g[f"{pre}apply{k}"]), k
+        assert _eq(m.pairwise_apply(k, Q, nonorm=True), g[f"{pre}apply{k}_nonorm"]), k
+        kg, ref = m.pairwise_kernel_gradient(k, g["b"], Q), g[f"{pre}kgrad{k}"]
+        assert np.abs(kg - ref).max() <= 1e-4 * np.abs(ref).max(), (k, kg, ref)
+    lab = m.currentMap(Q)
+    assert m.assignment_energy_true(lab) == pytest.approx(float(g[pre + "e_true"]), rel=1e-12)
+    assert m.compute_LR_QP_value(Q) == pytest.approx(float(g[pre + "e_lrqp"]), rel=1e-12)
+    out, st = m.qp_inference_super_pixels_non_convex(Q, max_iter=20, stats=True)
+    assert st.iterations == int(g[pre + "qp_iters"])
+    assert _eq(out, g[pre + "qp"])
+
+    m = model(0, 3)
+    assert m.pairwise_kernel_parameters(0).size == g["const_kparams0"].size == 0
+    assert m.pairwise_kernel_gradient(0, g["b"], Q).size == g["const_kgrad0"].size == 0
+    with pytest.raises(DCRFError):
+        model(1, 2).pairwise_kernel_gradient(0, g["b"], Q)   # DIAG + NORMALIZE_AFTER: not built
+    with pytest.raises(DCRFError):
+        m.setKernel(0, 3, 3)
