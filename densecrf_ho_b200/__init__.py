@@ -206,6 +206,36 @@ class DenseCRF2D:
     CONST_KERNEL, DIAG_KERNEL, FULL_KERNEL = 0, 1, 2
     NO_NORMALIZATION, NORMALIZE_BEFORE, NORMALIZE_AFTER, NORMALIZE_SYMMETRIC = 0, 1, 2, 3
 
+    def unaryEnergy(self, labels):
+        """``unaryEnergy(l)``: the per-pixel unary energy of a labelling."""
+        lab = np.ascontiguousarray(labels, np.int16).reshape(-1)
+        out = np.zeros(self.N, np.float32)
+        check(lib().dcrf_model_unary_energy(self._h, lab.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def pairwise_energy_true(self, labels, term=-1):
+        """``pairwise_energy_true(l, term)``: per-pixel pairwise energy (term -1: all)."""
+        lab = np.ascontiguousarray(labels, np.int16).reshape(-1)
+        out = np.zeros(self.N, np.float32)
+        check(lib().dcrf_model_pairwise_energy(self._h, lab.ctypes.data_as(C.c_void_p), int(term),
+                                               out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def max_rounding(self, Q):
+        """``max_rounding(Q)``: one-hot at each pixel's first maximum."""
+        x = self._mat(Q)
+        out = self._new()
+        check(lib().dcrf_model_max_rounding(self._h, x.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def compute_LR_QP_value_diag(self, Q, diag_dom):
+        """``compute_LR_QP_value(Q, diag_dom)``."""
+        x, d = self._mat(Q), self._mat(diag_dom)
+        e = C.c_double()
+        check(lib().dcrf_model_lr_qp_value_diag(self._h, x.ctypes.data_as(C.c_void_p), d.ctypes.data_as(C.c_void_p),
+                                                C.byref(e)))
+        return e.value
+
     def setKernel(self, k, ktype=1, ntype=3):
         """Term k's KernelType and NormalizationType (addPairwiseEnergy's last
         two arguments; the defaults are DIAG_KERNEL, NORMALIZE_SYMMETRIC)."""

@@ -723,6 +723,54 @@ dcrf_status dcrf_model_lr_qp_value(dcrf_model h, const float* Q, double* energy)
     });
 }
 
+dcrf_status dcrf_model_lr_qp_value_diag(dcrf_model h, const float* Q, const float* diag_dom, double* energy) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        need(energy, "energy");
+        const size_t n = (size_t)m.N * m.L;
+        float* dq = upload(h->io0, Q, n, m.stream);
+        const float* dd = diag_dom ? upload(h->io1, diag_dom, n, m.stream) : nullptr;
+        *energy = m.lr_qp_value(dq, dd);
+    });
+}
+
+dcrf_status dcrf_model_unary_energy(dcrf_model h, const int16_t* labels, float* out) {
+    return guard([&] {
+        auto& m = M(h);
+        need(labels, "labels");
+        need(out, "out");
+        int16_t* dl = upload(h->lab, labels, m.N, m.stream);
+        float* dout = h->io1.ensure((size_t)m.N);
+        m.unary_energy(dl, dout);
+        download(out, dout, (size_t)m.N, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_energy(dcrf_model h, const int16_t* labels, int term, float* out) {
+    return guard([&] {
+        auto& m = M(h);
+        need(labels, "labels");
+        need(out, "out");
+        int16_t* dl = upload(h->lab, labels, m.N, m.stream);
+        float* dout = h->io2.ensure((size_t)m.N);
+        m.pairwise_energy(dl, term, dout);
+        download(out, dout, (size_t)m.N, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_max_rounding(dcrf_model h, const float* Q, float* out) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        need(out, "out");
+        const size_t n = (size_t)m.N * m.L;
+        float* dq = upload(h->io0, Q, n, m.stream);
+        m.max_rounding(dq, dq);
+        download(out, dq, n, m.stream);
+    });
+}
+
 dcrf_status dcrf_model_info(dcrf_model h, int* n_terms, int* N, int* L) {
     return guard([&] {
         auto& m = M(h);

@@ -793,21 +793,57 @@ double Model::energy_lp(const float* Q) {
     return h_scal->energy;
 }
 
-// compute_LR_QP_value(Q, 0) (src/densecrf.cpp:940-957).
-double Model::lr_qp_value(const float* Q) {
+// compute_LR_QP_value(Q, diag_dom) (src/densecrf.cpp:940-957); diag_dom
+// null stands for 0.
+double Model::lr_qp_value(const float* Q, const float* dd) {
     require(has_unary, DCRF_E_STATE, "energy: no unary energy set");
+    const int nt = (int)terms.size();
+    require(nt + 3 <= 16, DCRF_E_ARG, "energy: too many pairwise terms");
+    const long NL = (long)N * L;
     float* o = buf(11);
-    launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, unary.get(), Q, partials.get());
+    launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, partials.get());
     launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 0, scal.get());
-    for (size_t k = 0; k < terms.size(); k++) {
-        apply((int)k, false, o, Q);
-        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, (long)N * L, Q, o, partials.get());
-        launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 1 + (int)k, scal.get());
+    if (dd) {
+        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, dd, Q, partials.get());
+        launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, nt + 1, scal.get());
+        launch(dot3_kernel, kRedBlocks, kRedThreads, 0, stream, NL, Q, dd, Q, partials.get());
+        launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, nt + 2, scal.get());
     }
-    launch(lr_finish_kernel, 1, 1, 0, stream, (int)terms.size(), scal.get());
+    for (int k = 0; k < nt; k++) {
+        apply(k, false, o, Q);
+        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, Q, o, partials.get());
+        launch(finalize_sums_kernel, 1, 32, 0, stream, partials.get(), kRedBlocks, 1, 1 + k, scal.get());
+    }
+    launch(lr_finish_kernel, 1, 1, 0, stream, nt, scal.get(), (int)(dd != nullptr));
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
     return h_scal->energy;
+}
+
+void Model::unary_energy(const int16_t* d_lab, float* out) {
+    if (!has_unary) {  // no unary energy: zeros, as the reference's r.fill(0)
+        launch(fill_kernel, ceil_div(N, 256), 256, 0, stream, N, 0.0f, out);
+    } else {
+        launch(unary_pick_kernel, ceil_div(N, 256), 256, 0, stream, N, L, d_lab, (const float*)unary.get(), out);
+    }
+    DCRF_LAUNCH_CHECK();
+}
+
+// pairwise_energy_true: the unnormalised twin applied to the one-hot
+// complement of l, r_i = -(.)(l_i, i); term -1: r = 0 + r_0 + r_1 + ...
+void Model::pairwise_energy(const int16_t* d_lab, int term, float* out) {
+    const int nt = (int)terms.size();
+    require(term >= -1 && term < nt, DCRF_E_ARG, "pairwise term index out of range");
+    float* qc = buf(10);
+    float* o = buf(11);
+    launch(onehot_complement_kernel, ceil_div((long)N * L, 256), 256, 0, stream, N, L, d_lab, qc);
+    const int k0 = term < 0 ? 0 : term, k1 = term < 0 ? nt : term + 1;
+    if (k0 == k1) launch(fill_kernel, ceil_div(N, 256), 256, 0, stream, N, 0.0f, out);
+    for (int k = k0; k < k1; k++) {
+        apply(k, true, o, qc);
+        launch(pairwise_pick_kernel, ceil_div(N, 256), 256, 0, stream, N, L, d_lab, (const float*)o, out, k == k0);
+    }
+    DCRF_LAUNCH_CHECK();
 }
 
 }  // namespace dcrf

@@ -163,7 +163,12 @@ struct Model {
     void current_map(const float* Q, int16_t* lab);
     double energy_true(const int16_t* d_lab, bool ho);
     double energy_lp(const float* Q);
-    double lr_qp_value(const float* Q);
+    double lr_qp_value(const float* Q, const float* diag_dom = nullptr);
+    // unaryEnergy(l) / pairwise_energy_true(l, term) (src/densecrf.cpp:887-927): per-pixel
+    // energies into out[N] (device); term -1 sums every term in order.
+    void unary_energy(const int16_t* d_lab, float* out);
+    void pairwise_energy(const int16_t* d_lab, int term, float* out);
+    void max_rounding(const float* Q, float* out);  // max_rounding (:832-840)
     void rescale(float* out, const float* Q);  // rescale (src/eigen_utils.cpp:120-141)
 
     int qp(const float* init, float* out, int max_iter, double* energy);

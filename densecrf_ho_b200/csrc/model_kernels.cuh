@@ -348,13 +348,34 @@ __global__ void energy_lp_finish_kernel(int nterms, int R, const float* __restri
 }
 
 // compute_LR_QP_value(Q, 0): U.Q - 0.Q + sum_k Q.(A_k Q) + Q.(0 o Q).
-__global__ void lr_finish_kernel(int nterms, SolverScalars* sc) {
+// compute_LR_QP_value's sum (src/densecrf.cpp:940-957) from sums[0] (U.Q),
+// sums[1..nterms] (Q.A_k Q) and, with diag_dom, sums[nterms + 1] (D.Q) and
+// sums[nterms + 2] (Q.(D o Q)).
+__global__ void lr_finish_kernel(int nterms, SolverScalars* sc, int has_dd) {
     double e = 0.0;
     e += sc->sums[0];
-    e -= 0.0;
+    e -= has_dd ? sc->sums[nterms + 1] : 0.0;
     for (int k = 0; k < nterms; k++) e += sc->sums[1 + k];
-    e += 0.0;
+    e += has_dd ? sc->sums[nterms + 2] : 0.0;
     sc->energy = e;
+}
+
+// sum (double) a o float(b o c) (dotProduct(Q, D.cwiseProduct(Q))).
+__global__ void dot3_kernel(long n, const float* __restrict__ a, const float* __restrict__ b,
+                            const float* __restrict__ c, double* __restrict__ partials) {
+    double v[1] = {0.0};
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+        v[0] += (double)a[t] * (double)fmul(b[t], c[t]);
+    block_sum_store<1>(v, partials);
+}
+
+// unaryEnergy(l) (src/densecrf.cpp:887-900): r_i = U(l_i, i), 0 off the label range.
+__global__ void unary_pick_kernel(int N, int L, const int16_t* __restrict__ lab, const float* __restrict__ U,
+                                  float* __restrict__ r) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int l = lab[i];
+    r[i] = (0 <= l && l < L) ? U[(long)i * L + l] : 0.0f;
 }
 
 }  // namespace

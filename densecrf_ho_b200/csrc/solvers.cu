@@ -1076,6 +1076,18 @@ constexpr int kPix = 128;
 
 }  // namespace
 
+// max_rounding (src/densecrf.cpp:832-840): a one-hot column at the first
+// maximum of each pixel.
+void Model::max_rounding(const float* Q, float* out) {
+    const long NL = (long)N * L;
+    if (out != Q) DCRF_CUDA(cudaMemcpyAsync(out, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    with_lc(L, [&](auto lc) {
+        constexpr int LC = decltype(lc)::value;
+        launch(max_rounding_kernel<LC>, ceil_div(N, kPix), kPix, 0, stream, N, L, out);
+    });
+    DCRF_LAUNCH_CHECK();
+}
+
 // ---------------------------------------------------------------- QP host --
 // Everything a captured QP iteration holds by address or by value that can
 // change between solves.

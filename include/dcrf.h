@@ -263,6 +263,17 @@ dcrf_status dcrf_model_energy_ho(dcrf_model m, const int16_t* labels, double* en
 dcrf_status dcrf_model_energy_lp(dcrf_model m, const float* Q, double* energy);
 /* compute_LR_QP_value(Q, 0) (src/densecrf.cpp:940-957). */
 dcrf_status dcrf_model_lr_qp_value(dcrf_model m, const float* Q, double* energy);
+/* compute_LR_QP_value(Q, diag_dom) (src/densecrf.cpp:940-957) with a
+ * diag_dom [N][L] (NULL: 0, as dcrf_model_lr_qp_value). */
+dcrf_status dcrf_model_lr_qp_value_diag(dcrf_model m, const float* Q, const float* diag_dom, double* energy);
+/* The per-pixel energies of a labelling (src/densecrf.cpp:887-927):
+ * unaryEnergy(l) -> out[N], and pairwise_energy_true(l, term) -> out[N]
+ * (term -1: all terms summed in order). */
+dcrf_status dcrf_model_unary_energy(dcrf_model m, const int16_t* labels, float* out);
+dcrf_status dcrf_model_pairwise_energy(dcrf_model m, const int16_t* labels, int term, float* out);
+/* max_rounding(Q) (src/densecrf.cpp:832-840): out [N][L], a one-hot row at
+ * each pixel's first maximum. */
+dcrf_status dcrf_model_max_rounding(dcrf_model m, const float* Q, float* out);
 /* pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 90-122,
  * 170-181): the gradient of the diagonal kernel's feature scales, d floats
  * (d = 2 Gaussian, 5 bilateral; the count is returned when not NULL, 0 for

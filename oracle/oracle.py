@@ -125,6 +125,12 @@ def ref_lib():
         L.refm_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         L.refm_kernel_gradient.argtypes = [vp, C.c_int, _f32p, _f32p, _f32p]
         L.refm_parameters.argtypes = [vp, C.c_int, _f32p]
+        L.refm_unary_energy.argtypes = [vp, np.ctypeslib.ndpointer(np.int16, flags="C_CONTIGUOUS"), _f32p]
+        L.refm_pairwise_energy.argtypes = [vp, np.ctypeslib.ndpointer(np.int16, flags="C_CONTIGUOUS"), C.c_int,
+                                           _f32p]
+        L.refm_max_rounding.argtypes = [vp, _f32p, _f32p]
+        L.refm_lr_qp_diag.argtypes = [vp, _f32p, _f32p]
+        L.refm_lr_qp_diag.restype = C.c_double
         L.refm_add_features_kernel.argtypes = [vp, _f32p, C.c_int, C.c_float, C.c_int, C.c_int]
         L.refm_kernel_parameters.argtypes = [vp, C.c_int, _f32p]
         L.refm_set_kernel_parameters.argtypes = [vp, C.c_int, _f32p, C.c_int]
@@ -324,6 +330,24 @@ class _Model:
         out = np.zeros(16, np.float32)
         n = self._lib.refm_kernel_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
         return out[:n]
+
+    def unary_energy(self, lab):
+        out = np.zeros(self.N, np.float32)
+        self._lib.refm_unary_energy(self._h, _c(lab, np.int16), out)
+        return out
+
+    def pairwise_energy(self, lab, term=-1):
+        out = np.zeros(self.N, np.float32)
+        self._lib.refm_pairwise_energy(self._h, _c(lab, np.int16), term, out)
+        return out
+
+    def max_rounding(self, Q):
+        out = self._new()
+        self._lib.refm_max_rounding(self._h, _c(Q, np.float32), out)
+        return out
+
+    def lr_qp_value_diag(self, Q, dd):
+        return self._lib.refm_lr_qp_diag(self._h, _c(Q, np.float32), _c(dd, np.float32))
 
     def add_features_kernel(self, f, w, ktype, ntype):
         """addPairwiseEnergy(f, Potts(w), ktype, ntype) (reference model only)."""

@@ -407,6 +407,26 @@ int refm_unary_gradient(void* h, const float* b, float* out) {
     std::memcpy(out, g.data(), sizeof(float) * g.size());
     return (int)g.size();
 }
+// The reference's debugging energies and max_rounding (src/densecrf.cpp:832-957).
+void refm_unary_energy(void* h, const short* labels, float* out) {
+    RefModel* m = (RefModel*)h;
+    VectorXf r = m->unaryEnergy(Map<const VectorXs>(labels, m->N()));
+    std::memcpy(out, r.data(), sizeof(float) * r.size());
+}
+void refm_pairwise_energy(void* h, const short* labels, int term, float* out) {
+    RefModel* m = (RefModel*)h;
+    VectorXf r = m->pairwise_energy_true(Map<const VectorXs>(labels, m->N()), term);
+    std::memcpy(out, r.data(), sizeof(float) * r.size());
+}
+void refm_max_rounding(void* h, const float* Q, float* out) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf r = m->max_rounding(Map<const MatrixXf>(Q, m->L(), m->N()));
+    std::memcpy(out, r.data(), sizeof(float) * r.size());
+}
+double refm_lr_qp_diag(void* h, const float* Q, const float* dd) {
+    RefModel* m = (RefModel*)h;
+    return m->compute_LR_QP_value(Map<const MatrixXf>(Q, m->L(), m->N()), Map<const MatrixXf>(dd, m->L(), m->N()));
+}
 int refm_parameters(void* h, int k, float* out) {
     VectorXf p = ((RefModel*)h)->parameters(k);
     std::memcpy(out, p.data(), sizeof(float) * p.size());

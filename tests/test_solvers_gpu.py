@@ -375,3 +375,27 @@ def test_kernel_and_normalization_types_vs_reference():
         model(1, 2).pairwise_kernel_gradient(0, g["b"], Q)   # DIAG + NORMALIZE_AFTER: not built
     with pytest.raises(DCRFError):
         m.setKernel(0, 3, 3)
+
+
+def test_per_pixel_energies_and_rounding_vs_reference():
+    """unaryEnergy, pairwise_energy_true (each term and all), max_rounding
+    (ties to the first maximum) bit for bit, and compute_LR_QP_value with a
+    diag_dom (FP64 sums in another order: 1e-12), against the reference's own
+    values (tests/golden/make_energy_golden.py)."""
+    g = golden("energies_24x18.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    m = DenseCRF2D(W, H, L)
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    assert _eq(m.unaryEnergy(g["lab"]), g["unary_e"])
+    assert _eq(m.pairwise_energy_true(g["lab"]), g["pw_all"])
+    assert _eq(m.pairwise_energy_true(g["lab"], 0), g["pw0"])
+    assert _eq(m.pairwise_energy_true(g["lab"], 1), g["pw1"])
+    assert _eq(m.max_rounding(g["Q"]), g["maxround"])
+    assert m.compute_LR_QP_value_diag(g["Q"], g["dd"]) == pytest.approx(float(g["lrqp_dd"]), rel=1e-12)
+    zero = np.zeros_like(g["Q"])
+    assert m.compute_LR_QP_value_diag(g["Q"], zero) == pytest.approx(m.compute_LR_QP_value(g["Q"]), rel=1e-12)
+    with pytest.raises(DCRFError):
+        m.pairwise_energy_true(g["lab"], 2)
