@@ -228,6 +228,13 @@ class DenseCRF2D:
         check(lib().dcrf_model_max_rounding(self._h, x.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def compute_energy_higher_order(self, Q):
+        """``compute_energy_higher_order(Q)``, with the clique variables of the last QP."""
+        x = self._mat(Q)
+        e = C.c_double()
+        check(lib().dcrf_model_energy_higher_order(self._h, x.ctypes.data_as(C.c_void_p), C.byref(e)))
+        return e.value
+
     def compute_LR_QP_value_diag(self, Q, diag_dom):
         """``compute_LR_QP_value(Q, diag_dom)``."""
         x, d = self._mat(Q), self._mat(diag_dom)

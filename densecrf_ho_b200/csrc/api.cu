@@ -735,6 +735,16 @@ dcrf_status dcrf_model_lr_qp_value_diag(dcrf_model h, const float* Q, const floa
     });
 }
 
+dcrf_status dcrf_model_energy_higher_order(dcrf_model h, const float* Q, double* energy) {
+    return guard([&] {
+        auto& m = M(h);
+        need(Q, "Q");
+        need(energy, "energy");
+        float* dq = upload(h->io0, Q, (size_t)m.N * m.L, m.stream);
+        *energy = m.energy_qp_ho(dq);
+    });
+}
+
 dcrf_status dcrf_model_unary_energy(dcrf_model h, const int16_t* labels, float* out) {
     return guard([&] {
         auto& m = M(h);

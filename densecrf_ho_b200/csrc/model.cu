@@ -511,6 +511,7 @@ void Model::set_parameters(int k, const float* v) {
 
 void Model::set_cliques(int R_, const int* off, const int* idx, const float* expw, const float* cst) {
     gen++;  // a captured QP graph may hold what this changes
+    has_z_last = false;
     R = R_;
     h_cl_off.assign(off, off + R + 1);
     clique_total = off[R];

@@ -108,6 +108,11 @@ struct Model {
     DevBuf<float2> lp_bins;  // ordered-filter bins of rescale(Q), shared by all terms
     DevBuf<int> ipart;
     DevBuf<double> ho_pre;  // qp_sp: FP64 clique prefixes [2][R][L]
+    DevBuf<float> z_last;   // the clique variables z [R][L] at the end of the last QP (z_labels_)
+    bool has_z_last = false;
+    // compute_energy_higher_order(Q) (src/densecrf.cpp:960-980), with the z of
+    // the last QP (DCRF_E_STATE with cliques and no QP since they were set).
+    double energy_qp_ho(const float* Q);
     DevBuf<int> lp_win;  // lp_sp: per element, the latest clique write claiming it (-1 between calls)
     SolverScalars* h_scal = nullptr;  // pinned mirror
 

@@ -1076,6 +1076,59 @@ constexpr int kPix = 128;
 
 }  // namespace
 
+__global__ void ho_energy_finish_kernel(int nterms, SolverScalars* sc, int has_ho) {
+    double e = 0.0;
+    e += sc->sums[0];
+    for (int k = 0; k < nterms; k++) e += sc->sums[1 + k];
+    e += has_ho ? sc->sums[8] : 0.0;
+    sc->energy = e;
+}
+
+__global__ void clear_step_flags_kernel(SolverScalars* sc) {
+    sc->zero_step = 0;
+    sc->steps = 0;
+}
+
+// compute_energy_higher_order(Q): U.Q + sum_k Q.A_k Q + the clique term
+// (z o c).sum() + multiplySuperPixels((1 - z) o c, Q - 1) in float, with z
+// the clique variables the last QP left (src/densecrf.cpp:960-980, 439).
+double Model::energy_qp_ho(const float* Q) {
+    require(has_unary, DCRF_E_STATE, "energy: no unary energy set");
+    require(R == 0 || has_z_last, DCRF_E_STATE,
+            "compute_energy_higher_order: no QP has run since the cliques were set");
+    const int nt = (int)terms.size();
+    require(nt + 1 <= 8, DCRF_E_ARG, "energy: too many pairwise terms");
+    const long NL = (long)N * L;
+    SolverScalars* sc = scal.get();
+    double* part = partials.get();
+    float* o = buf(11);
+    launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, part);
+    launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
+    for (int k = 0; k < nt; k++) {
+        apply(k, false, o, Q);
+        launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, Q, o, part);
+        launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 1 + k, sc);
+    }
+    if (R > 0) {
+        const int LR = L * R;
+        const int* base = cl_off.get();
+        const CliqueView cv{base, base + R + 1, base + 2 * R + 1, cl_idx.get(), cl_exp.get(), cl_const.get(), R,
+                            clique_max, cl_bstart.get()};
+        float* small = b[14].ensure((size_t)8 * LR);
+        float *zc = small + 6 * LR, *omz = small + 7 * LR;
+        double* preQ = ho_pre.ensure((size_t)2 * LR);
+        launch(clear_step_flags_kernel, 1, 1, 0, stream, sc);
+        launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, (const float*)z_last.get(), zc, omz, sc);
+        launch(eig_sum_kernel, 1, kHoThreads, 0, stream, (const float*)zc, LR, 8, sc, 2);
+        launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, preQ, nullptr, 0);
+        launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, (const float*)omz, (const double*)preQ, 8, sc, 1);
+    }
+    launch(ho_energy_finish_kernel, 1, 1, 0, stream, nt, sc, (int)(R > 0));
+    DCRF_LAUNCH_CHECK();
+    fetch_scalars();
+    return h_scal->energy;
+}
+
 // max_rounding (src/densecrf.cpp:832-840): a one-hot column at the first
 // maximum of each pixel.
 void Model::max_rounding(const float* Q, float* out) {
@@ -1298,6 +1351,12 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
             }
         }
     }
+    if (R > 0) {  // z_labels_ = z (src/densecrf.cpp:439)
+        DCRF_CUDA(cudaMemcpyAsync(z_last.ensure((size_t)LR), z, sizeof(float) * LR, cudaMemcpyDeviceToDevice,
+                                  stream));
+        sync();
+    }
+    has_z_last = true;
     if (energy_out) *energy_out = h_scal->energy;
     return h_scal->steps;
 }

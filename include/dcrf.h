@@ -266,6 +266,11 @@ dcrf_status dcrf_model_lr_qp_value(dcrf_model m, const float* Q, double* energy)
 /* compute_LR_QP_value(Q, diag_dom) (src/densecrf.cpp:940-957) with a
  * diag_dom [N][L] (NULL: 0, as dcrf_model_lr_qp_value). */
 dcrf_status dcrf_model_lr_qp_value_diag(dcrf_model m, const float* Q, const float* diag_dom, double* energy);
+/* compute_energy_higher_order(Q) (src/densecrf.cpp:960-980): U.Q + the
+ * pairwise Q.A_k Q + the clique term with the clique variables the last QP
+ * left (z_labels_, :439); DCRF_E_STATE when cliques are set and no QP has
+ * run since. */
+dcrf_status dcrf_model_energy_higher_order(dcrf_model m, const float* Q, double* energy);
 /* The per-pixel energies of a labelling (src/densecrf.cpp:887-927):
  * unaryEnergy(l) -> out[N], and pairwise_energy_true(l, term) -> out[N]
  * (term -1: all terms summed in order). */

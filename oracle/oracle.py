@@ -131,6 +131,8 @@ def ref_lib():
         L.refm_max_rounding.argtypes = [vp, _f32p, _f32p]
         L.refm_lr_qp_diag.argtypes = [vp, _f32p, _f32p]
         L.refm_lr_qp_diag.restype = C.c_double
+        L.refm_energy_qp_ho.argtypes = [vp, _f32p]
+        L.refm_energy_qp_ho.restype = C.c_double
         L.refm_add_features_kernel.argtypes = [vp, _f32p, C.c_int, C.c_float, C.c_int, C.c_int]
         L.refm_kernel_parameters.argtypes = [vp, C.c_int, _f32p]
         L.refm_set_kernel_parameters.argtypes = [vp, C.c_int, _f32p, C.c_int]
@@ -345,6 +347,10 @@ class _Model:
         out = self._new()
         self._lib.refm_max_rounding(self._h, _c(Q, np.float32), out)
         return out
+
+    def energy_qp_ho(self, Q):
+        """compute_energy_higher_order(Q) (z of the last QP; reference model only)."""
+        return self._lib.refm_energy_qp_ho(self._h, _c(Q, np.float32))
 
     def lr_qp_value_diag(self, Q, dd):
         return self._lib.refm_lr_qp_diag(self._h, _c(Q, np.float32), _c(dd, np.float32))

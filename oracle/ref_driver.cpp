@@ -423,6 +423,10 @@ void refm_max_rounding(void* h, const float* Q, float* out) {
     MatrixXf r = m->max_rounding(Map<const MatrixXf>(Q, m->L(), m->N()));
     std::memcpy(out, r.data(), sizeof(float) * r.size());
 }
+double refm_energy_qp_ho(void* h, const float* Q) {
+    RefModel* m = (RefModel*)h;
+    return m->compute_energy_higher_order(Map<const MatrixXf>(Q, m->L(), m->N()));
+}
 double refm_lr_qp_diag(void* h, const float* Q, const float* dd) {
     RefModel* m = (RefModel*)h;
     return m->compute_LR_QP_value(Map<const MatrixXf>(Q, m->L(), m->N()), Map<const MatrixXf>(dd, m->L(), m->N()));

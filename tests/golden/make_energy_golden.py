@@ -34,6 +34,17 @@ def main():
     out = dict(W=W, H=H, L=L, seed=SEED, lab=lab, Q=Q, dd=dd, unary_e=m.unary_energy(lab),
                pw_all=m.pairwise_energy(lab, -1), pw0=m.pairwise_energy(lab, 0), pw1=m.pairwise_energy(lab, 1),
                maxround=m.max_rounding(Q), lrqp_dd=np.float64(m.lr_qp_value_diag(Q, dd)))
+    # compute_energy_higher_order after a QP, with the reference's own
+    # mean-shift cliques (spatial 8, range 8, min region 20; weights 50 / 1000)
+    mh = O.build_model(O.ReferenceModel, img)
+    mh.add_superpixel(img["rgb"], 8, 8, 20, 50.0, 1000.0)
+    off, idx, ex, cs = mh.get_cliques()
+    Q0 = mh.unary_init()
+    qf, it, _ = mh.qp(Q0, 5)
+    out.update(cl_off=off, cl_idx=idx, cl_exp=ex, cl_const=cs, ho_unary_init=Q0, ho_qp=qf,
+               e_qp_ho_after=np.float64(mh.energy_qp_ho(Q)), e_qp_ho_qp=np.float64(mh.energy_qp_ho(qf)))
+    m.qp(m.unary_init(), 5)
+    out["e_qp_ho_nocliques"] = np.float64(m.energy_qp_ho(Q))
     np.savez_compressed(os.path.join(HERE, f"energies_{W}x{H}.npz"), **out)
     print({k: float(np.abs(v).sum()) for k, v in out.items() if k not in ("W", "H", "L", "seed")})
 

@@ -399,3 +399,29 @@ def test_per_pixel_energies_and_rounding_vs_reference():
     assert m.compute_LR_QP_value_diag(g["Q"], zero) == pytest.approx(m.compute_LR_QP_value(g["Q"]), rel=1e-12)
     with pytest.raises(DCRFError):
         m.pairwise_energy_true(g["lab"], 2)
+
+
+def test_energy_higher_order_vs_reference():
+    """compute_energy_higher_order(Q) with the clique variables the last QP
+    left (the reference's z_labels_), on the reference's own mean-shift
+    cliques, and without cliques (tests/golden/make_energy_golden.py)."""
+    g = golden("energies_24x18.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+
+    def model():
+        m = DenseCRF2D(W, H, L)
+        m.setUnaryEnergy(img["unary"])
+        m.addPairwiseGaussian(3.0, 3.0, 3.0)
+        m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+        return m
+
+    m = model()
+    assert m.compute_energy_higher_order(g["Q"]) == pytest.approx(float(g["e_qp_ho_nocliques"]), rel=1e-12)
+    m.setCliques(g["cl_off"], g["cl_idx"], g["cl_exp"], g["cl_const"])
+    with pytest.raises(DCRFError):   # no QP since the cliques were set: no z yet
+        m.compute_energy_higher_order(g["Q"])
+    out = m.qp_inference_super_pixels_non_convex(g["ho_unary_init"], max_iter=5)
+    assert _eq(out, g["ho_qp"])
+    assert m.compute_energy_higher_order(g["Q"]) == pytest.approx(float(g["e_qp_ho_after"]), rel=1e-12)
+    assert m.compute_energy_higher_order(out) == pytest.approx(float(g["e_qp_ho_qp"]), rel=1e-12)
