@@ -353,11 +353,32 @@ public:
         dcrf_shim::check(dcrf_model_lp(m_, init.data(), out.data(), &p, nullptr));
         return out;
     }
+    // max_rounding (src/densecrf.cpp:832-840)
     MatrixXf max_rounding(const MatrixXf& estimates) const {
-        MatrixXf r = MatrixXf::Zero(estimates.rows(), estimates.cols());
-        const VectorXs l = currentMap(estimates);
-        for (int i = 0; i < (int)estimates.cols(); i++) r(l[i], i) = 1;
+        MatrixXf r(estimates.rows(), estimates.cols());
+        dcrf_shim::check(dcrf_model_max_rounding(m_, estimates.data(), r.data()));
         return r;
+    }
+    // unaryEnergy / pairwise_energy_true (src/densecrf.cpp:887-927)
+    VectorXf unaryEnergy(const VectorXs& l) const {
+        VectorXf r(N_);
+        dcrf_shim::check(dcrf_model_unary_energy(m_, l.data(), r.data()));
+        return r;
+    }
+    VectorXf pairwise_energy_true(const VectorXs& l, int term = -1) const {
+        VectorXf r(N_);
+        dcrf_shim::check(dcrf_model_pairwise_energy(m_, l.data(), term, r.data()));
+        return r;
+    }
+    // compute_energy_higher_order (src/densecrf.cpp:960-980)
+    double compute_energy_higher_order(const MatrixXf& Q) const {
+        double e = 0;
+        dcrf_shim::check(dcrf_model_energy_higher_order(m_, Q.data(), &e));
+        return e;
+    }
+    // setUnaryEnergy(L, f): LogisticUnaryEnergy (src/densecrf.cpp:264-267)
+    void setUnaryEnergy(const MatrixXf& L, const MatrixXf& f) {
+        dcrf_shim::check(dcrf_model_set_unary_logistic(m_, L.data(), f.data(), (int)f.rows()));
     }
     VectorXs currentMap(const MatrixXf& Q) const {
         VectorXs l(Q.cols());
@@ -380,10 +401,8 @@ public:
         return e;
     }
     double compute_LR_QP_value(const MatrixXf& Q, const MatrixXf& diag_dom) const {
-        if (diag_dom.size() && diag_dom.cwiseAbs().maxCoeff() != 0)
-            throw std::runtime_error("compute_LR_QP_value: only diag_dom = 0 runs on the B200 path");
         double e = 0;
-        dcrf_shim::check(dcrf_model_lr_qp_value(m_, Q.data(), &e));
+        dcrf_shim::check(dcrf_model_lr_qp_value_diag(m_, Q.data(), diag_dom.size() ? diag_dom.data() : nullptr, &e));
         return e;
     }
     // The clique state addSuperPixel leaves behind (src/densecrf.cpp:212-247),
