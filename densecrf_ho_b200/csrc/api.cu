@@ -346,6 +346,10 @@ dcrf_status dcrf_model_create(dcrf_model* out, int W, int H, int L) {
     });
 }
 
+dcrf_status dcrf_release_cached_memory(void) {
+    return guard([&] { dcrf::dev_trim(true); });
+}
+
 dcrf_status dcrf_model_destroy(dcrf_model h) {
     return guard([&] {
         if (!h) return;

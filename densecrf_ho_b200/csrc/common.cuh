@@ -36,24 +36,37 @@ inline void require(bool ok, dcrf_status code, const std::string& msg) {
     if (!ok) throw Error(code, msg);
 }
 
+// Device memory through a process-wide cache of freed blocks (memory.cu):
+// dev_alloc returns a block of at least `bytes` (its size class in *got),
+// from the cache or cudaMalloc; dev_release waits for the device, as
+// cudaFree does, then keeps the block for reuse up to DCRF_CACHE_MB
+// (default 2048) MiB of cached memory per process, beyond which it frees it.
+void* dev_alloc(size_t bytes, size_t* got);
+void dev_release(void* p, size_t bytes) noexcept;
+// Frees the cached blocks of the current device, or of every device
+// (dcrf_release_cached_memory).
+void dev_trim(bool all_devices) noexcept;
+
 // Owning device allocation; grows, never shrinks.
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    size_t bytes = 0;  // size of the block behind p
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
     void release() {
-        if (p) cudaFree(p);
+        if (p) dev_release(p, bytes);
         p = nullptr;
         n = 0;
+        bytes = 0;
     }
     T* ensure(size_t count) {
         if (count > n) {
             release();
-            DCRF_CUDA(cudaMalloc(&p, (count ? count : 1) * sizeof(T)));
+            p = static_cast<T*>(dev_alloc((count ? count : 1) * sizeof(T), &bytes));
             n = count;
         }
         return p;

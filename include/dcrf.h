@@ -44,6 +44,12 @@ typedef enum {
 typedef struct dcrf_lattice_s* dcrf_lattice;
 typedef struct dcrf_model_s* dcrf_model;
 
+/* Device memory freed by a destroyed model, lattice or batch stays cached in
+ * the process for the next one (up to DCRF_CACHE_MB MiB, default 2048, in
+ * the environment); this hands every cached block back to the driver.  No
+ * counterpart in the reference, which allocates on the host. */
+dcrf_status dcrf_release_cached_memory(void);
+
 const char* dcrf_last_error(void);
 /* Library version string. */
 const char* dcrf_version(void);

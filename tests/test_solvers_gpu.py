@@ -425,3 +425,39 @@ def test_energy_higher_order_vs_reference():
     assert _eq(out, g["ho_qp"])
     assert m.compute_energy_higher_order(g["Q"]) == pytest.approx(float(g["e_qp_ho_after"]), rel=1e-12)
     assert m.compute_energy_higher_order(out) == pytest.approx(float(g["e_qp_ho_qp"]), rel=1e-12)
+
+
+_EAGER_SNIPPET = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from densecrf_ho_b200 import DenseCRF2D, synth
+W, H, L = 64, 48, 21
+img = synth.make_image(W, H, L, 12)
+m = DenseCRF2D(W, H, L)
+m.setUnaryEnergy(img["unary"])
+m.addPairwiseGaussian(3.0, 3.0, 3.0)
+m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+Q = m.unary_init()
+qp = m.qp_inference_super_pixels_non_convex(Q)
+lp = m.lp_inference_prox_super_pixels(Q, prox_max_iter=3, fw_max_iter=5)
+np.savez(sys.argv[2], qp=qp, lp=lp)
+"""
+
+
+def test_graph_loops_match_eager_launches(tmp_path):
+    """The QP and LP loops run as CUDA graphs with device-side while nodes;
+    with DCRF_GRAPHS=0 the same kernels are launched from the host.  Both
+    give the same outputs, bit for bit."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    outs = {}
+    for flag in ("1", "0"):
+        f = tmp_path / f"g{flag}.npz"
+        r = subprocess.run([sys.executable, "-c", _EAGER_SNIPPET, root, str(f)], capture_output=True, text=True,
+                           timeout=600, env={**os.environ, "DCRF_GRAPHS": flag})
+        assert r.returncode == 0, r.stderr
+        outs[flag] = np.load(f)
+    for k in ("qp", "lp"):
+        assert _eq(outs["1"][k], outs["0"][k]), k
