@@ -161,6 +161,12 @@ class DenseCRF2D:
         check(lib().dcrf_model_set_unary_logistic(self._h, wc.ctypes.data_as(C.c_void_p),
                                                   f.ctypes.data_as(C.c_void_p), F))
 
+    def getUnaryEnergy(self):
+        """``getUnaryEnergy()->get()``: the unary [N, L] in use."""
+        out = self._new()
+        check(lib().dcrf_model_get_unary(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def unary_parameters(self):
         """``unary_->parameters()`` as W [L][F] (empty for a constant unary)."""
         n = C.c_int(0)

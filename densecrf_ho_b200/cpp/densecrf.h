@@ -304,6 +304,7 @@ protected:
     int N_, M_, R_ = 0;
     dcrf_model m_ = nullptr;
     int n_terms_ = 0;
+    std::unique_ptr<UnaryEnergy> unary_snapshot_;
     // cliques (super_pixel_container_, exp_of_superpixels_, constants_)
     std::vector<int> cl_off_{0}, cl_idx_;
     std::vector<float> cl_exp_, cl_const_;
@@ -375,6 +376,14 @@ public:
         double e = 0;
         dcrf_shim::check(dcrf_model_energy_higher_order(m_, Q.data(), &e));
         return e;
+    }
+    // getUnaryEnergy (src/densecrf.cpp:268-270): a snapshot of the unary in
+    // use, owned by the model like the reference's pointer.
+    UnaryEnergy* getUnaryEnergy() {
+        MatrixXf u(M_, N_);
+        dcrf_shim::check(dcrf_model_get_unary(m_, u.data()));
+        unary_snapshot_.reset(new ConstUnaryEnergy(u));
+        return unary_snapshot_.get();
     }
     // setUnaryEnergy(L, f): LogisticUnaryEnergy (src/densecrf.cpp:264-267)
     void setUnaryEnergy(const MatrixXf& L, const MatrixXf& f) {

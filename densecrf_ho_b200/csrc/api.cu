@@ -382,6 +382,15 @@ dcrf_status dcrf_model_set_unary(dcrf_model h, const float* unary) {
     });
 }
 
+dcrf_status dcrf_model_get_unary(dcrf_model h, float* unary) {
+    return guard([&] {
+        auto& m = M(h);
+        need(unary, "unary");
+        if (!m.has_unary) throw Error(DCRF_E_STATE, "no unary energy set");
+        download(unary, m.unary.get(), (size_t)m.N * m.L, m.stream);
+    });
+}
+
 dcrf_status dcrf_model_set_unary_logistic(dcrf_model h, const float* weights, const float* features, int F) {
     return guard([&] {
         auto& m = M(h);

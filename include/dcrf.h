@@ -177,6 +177,9 @@ dcrf_status dcrf_model_set_unary_dev(dcrf_model m, const float* d_unary);
  * [N][L]; *n = L F, 0 for a constant unary, whose gradient is empty; grad
  * may be NULL to query the count). */
 dcrf_status dcrf_model_set_unary_logistic(dcrf_model m, const float* weights, const float* features, int F);
+/* getUnaryEnergy()->get() (src/densecrf.cpp:268-270, src/unary.cpp:44-53):
+ * the unary [N][L] in use (the constant one, or W f). */
+dcrf_status dcrf_model_get_unary(dcrf_model m, float* unary);
 dcrf_status dcrf_model_unary_parameters(dcrf_model m, float* params, int* n);
 dcrf_status dcrf_model_unary_set_parameters(dcrf_model m, const float* params);
 dcrf_status dcrf_model_unary_gradient(dcrf_model m, const float* b, float* grad, int* n);

@@ -290,8 +290,10 @@ def test_logistic_unary_vs_reference():
     m.unary_set_parameters(2 * g["w"])
     assert np.array_equal(m.unary_parameters(), 2 * g["w"])
     assert not np.array_equal(m.unary_init(), Q)
+    assert np.abs(m.getUnaryEnergy() - (g["f"] @ (2 * g["w"]).T)).max() <= 1e-4
     m.setUnaryEnergy(np.zeros((W * H, L), np.float32))
     assert m.unary_gradient(g["b"]).size == 0
+    assert not m.getUnaryEnergy().any()
 
 
 def test_qp_graph_follows_model_changes():
