@@ -539,6 +539,102 @@ def measure_batch(n=64, max_iter=100, reps=3):
             "outputs_match_sequential": same}
 
 
+def measure_next_rows(W=640, H=480, seed=2, cpu=True, reps=5):
+    """The reference's learning and restricted-filter building blocks, through
+    the C ABI with host buffers (so host<->device copies included), on the
+    workload image: kernelGradient and gradient of both pairwise terms, the
+    LogisticUnaryEnergy gradient, a MatrixCompatibility apply, and the
+    restricted ordered filter (a store call and a reuse call on 20 % of the
+    pixels).  Beside each, the reference's own CPU code (oracle/_ref, one
+    core) on the same inputs at 320x240 (the CPU side is slow at 640x480),
+    scaled to 640x480 by the pixel count."""
+    from densecrf_ho_b200 import DenseCRF2D, Permutohedral
+    O = None
+    if cpu:
+        from oracle import oracle as O
+    out = {"workload": f"{W}x{H} L={L}; CPU reference at 320x240 scaled by the pixel count", "ms": {}}
+
+    def model_for(w, h, cls=None):
+        img = synth.make_image(w, h, L, seed)
+        if cls is None:
+            m = DenseCRF2D(w, h, L)
+            m.setUnaryEnergy(img["unary"])
+            m.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+            m.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"], BILAT[2])
+        else:
+            m = cls(w, h, L, img["unary"])
+            m.add_gaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+            m.add_bilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"], BILAT[2])
+        return m, img
+
+    def ops(m, img, w, h, ref):
+        rng = np.random.default_rng(0)
+        N = w * h
+        b = rng.standard_normal((N, L)).astype(np.float32)
+        Q = m.unary_init()
+        rq = (Q - Q.min()) / (Q - Q.min()).max()
+        pI = np.sort(rng.choice(N, N // 5, replace=False)).astype(np.int32)
+        f = synth.bilateral_features(w, h, BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"])
+        if ref:
+            lat = O.ReferenceLattice(f)
+            return {
+                "kernel_gradient_bilateral": lambda: m.kernel_gradient(1, b, Q),
+                "kernel_gradient_gaussian": lambda: m.kernel_gradient(0, b, Q),
+                "weight_gradient_bilateral": lambda: m.weight_gradient(1, b, Q),
+                "restricted_ord_store": lambda: lat.compute_ord_restricted(rq[pI], pI, rq, True),
+                "restricted_ord_reuse": lambda: lat.compute_ord_restricted(rq[pI], pI, None, False),
+            }
+        lat = Permutohedral().init(f)
+        return {
+            "kernel_gradient_bilateral": lambda: m.pairwise_kernel_gradient(1, b, Q),
+            "kernel_gradient_gaussian": lambda: m.pairwise_kernel_gradient(0, b, Q),
+            "weight_gradient_bilateral": lambda: m.pairwise_gradient(1, b, Q),
+            "restricted_ord_store": lambda: lat.compute_upper_minus_lower_ord_restricted(rq[pI], pI, rq, True),
+            "restricted_ord_reuse": lambda: lat.compute_upper_minus_lower_ord_restricted(rq[pI], pI, None, False),
+        }
+
+    m, img = model_for(W, H)
+    for name, fn in ops(m, img, W, H, False).items():
+        fn()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        out["ms"][name] = (time.perf_counter() - t0) / reps * 1e3
+    # the compatibility and unary-energy variants on their own models
+    mm = np.random.default_rng(1).random((L, L)).astype(np.float32)
+    np.fill_diagonal(mm, -5.0)
+    m.setCompatibility(1, matrix=mm)
+    Q = m.unary_init()
+    m.pairwise_apply(1, Q)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m.pairwise_apply(1, Q)
+    out["ms"]["matrix_compat_apply_bilateral"] = (time.perf_counter() - t0) / reps * 1e3
+    F = 8
+    wl = np.random.default_rng(2).standard_normal((L, F)).astype(np.float32)
+    fl = np.random.default_rng(3).random((W * H, F)).astype(np.float32)
+    m.setUnaryEnergyLogistic(wl, fl)
+    bb = np.random.default_rng(4).standard_normal((W * H, L)).astype(np.float32)
+    m.unary_gradient(bb)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        m.unary_gradient(bb)
+    out["ms"]["logistic_unary_gradient"] = (time.perf_counter() - t0) / reps * 1e3
+    del m
+    if cpu and O is not None and O.reference_available():
+        w, h = 320, 240
+        scale = (W * H) / (w * h)
+        rm, rimg = model_for(w, h, O.ReferenceModel)
+        cpu_ms = {}
+        for name, fn in ops(rm, rimg, w, h, True).items():
+            t0 = time.perf_counter()
+            fn()
+            cpu_ms[name] = (time.perf_counter() - t0) * 1e3 * scale
+        out["cpu_reference_ms_scaled"] = cpu_ms
+        out["cpu_vs_gpu"] = {k: cpu_ms[k] / out["ms"][k] for k in cpu_ms}
+    return out
+
+
 def measure_adjoint(n=16, size=512, T=10, reps=3):
     """Config 5: unrolled mean-field (T iterations) forward and its hand-written
     adjoint (dcrf_batch_meanfield_dev / _backward_dev) on n size x size images,
@@ -726,6 +822,7 @@ def run_ours(args):
         line["extra"]["ho_640x480"] = measure_ho(cpu=not args.no_cpu_baseline)
         line["extra"]["batch_qp_64"] = measure_batch()
         line["extra"]["adjoint_16x512x512"] = measure_adjoint()
+        line["extra"]["next_rows_640x480"] = measure_next_rows(cpu=not args.no_cpu_baseline)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference(W, H, args.seed, prox_iters, 1, 10, 1)
