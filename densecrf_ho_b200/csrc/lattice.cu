@@ -427,6 +427,93 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     }
 }
 
+// The longest lists with L = 21: the cp.async ring of splat_kernel, kStages chunks
+// of 32 entries deep, but each lane copies its own entry's 21 values into a
+// [label][entry] ring (no shuffles, 21 copies per chunk instead of 32), and
+// lane k < 21 sums its label in entry order with float4 reads of four
+// entries' values, weights (and norms) at a time.
+constexpr int kRS = 36;  // ring row stride: float4-aligned, 4 banks apart per label
+template <bool PRE_NORM>
+__global__ void __launch_bounds__(32 * kStageWarps)
+    splat_ring21_kernel(int M, const int* __restrict__ order, const int* __restrict__ seg_start,
+                        const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                        const float* __restrict__ in, const float* __restrict__ norm, float* __restrict__ vals,
+                        Skip sk) {
+    constexpr int L = 21;
+    __shared__ __align__(16) float X[kStageWarps][kStages][L][kRS];
+    __shared__ __align__(16) float Wr[kStageWarps][kStages][kChunk];
+    __shared__ __align__(16) float Nr[kStageWarps][kStages][kChunk];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int unit = blockIdx.x * kStageWarps + wib;
+    if (unit >= M) return;  // warp-uniform; the kernel has no block-wide barrier
+    const int v = order[unit];
+    if (skipped(sk, v)) return;
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    const int nch = (s1 - s0 + kChunk - 1) / kChunk;
+    auto pix_of = [&](int c) {
+        const int e = s0 + c * kChunk + lane;
+        return (c < nch && e < s1) ? seg_pix[e] : -1;
+    };
+    auto issue = [&](int c, int p) {
+        if (p < 0) return;  // past the end of the list: never summed
+        const int slot = c % kStages, e = s0 + c * kChunk + lane;
+        const float* row = in + (long)p * L;
+#pragma unroll
+        for (int k = 0; k < L; k++) cp_async4(&X[wib][slot][k][lane], row + k);
+        cp_async4(&Wr[wib][slot][lane], seg_w + e);
+        if (PRE_NORM) cp_async4(&Nr[wib][slot][lane], norm + p);
+    };
+    float acc = 0.0f;
+    int pcur = pix_of(0);
+#pragma unroll
+    for (int c = 0; c < kStages - 1; c++) {
+        const int pn = pix_of(c + 1);
+        issue(c, pcur);
+        cp_async_commit();
+        pcur = pn;
+    }
+    for (int c = 0; c < nch; c++) {
+        const int ci = c + kStages - 1;
+        const int pn = pix_of(ci + 1);
+        issue(ci, pcur);
+        cp_async_commit();
+        pcur = pn;
+        cp_async_wait<kStages - 1>();  // chunk c has landed (this lane's copies)
+        __syncwarp();                  // ... and every other lane's
+        const int slot = c % kStages, n = min(kChunk, s1 - (s0 + c * kChunk));
+        if (lane < L) {
+            const float4* xs = reinterpret_cast<const float4*>(&X[wib][slot][lane][0]);
+            const float4* ws = reinterpret_cast<const float4*>(&Wr[wib][slot][0]);
+            const float4* ns = reinterpret_cast<const float4*>(&Nr[wib][slot][0]);
+            const int n4 = n >> 2;
+            for (int q = 0; q < n4; q++) {
+                float4 x = xs[q];
+                const float4 w = ws[q];
+                if (PRE_NORM) {
+                    const float4 nv = ns[q];
+                    x.x = fmul(x.x, nv.x);
+                    x.y = fmul(x.y, nv.y);
+                    x.z = fmul(x.z, nv.z);
+                    x.w = fmul(x.w, nv.w);
+                }
+                acc = fadd(acc, fmul(w.x, x.x));
+                acc = fadd(acc, fmul(w.y, x.y));
+                acc = fadd(acc, fmul(w.z, x.z));
+                acc = fadd(acc, fmul(w.w, x.w));
+            }
+            for (int e = n4 << 2; e < n; e++) {
+                float x = X[wib][slot][lane][e];
+                if (PRE_NORM) x = fmul(x, Nr[wib][slot][e]);
+                acc = fadd(acc, fmul(Wr[wib][slot][e], x));
+            }
+        }
+        __syncwarp();  // the slot is refilled kStages-1 chunks later
+    }
+    cp_async_wait<0>();
+    __syncwarp();
+    if (lane < L) vals[(long)(v + 1) * L + lane] = acc;
+}
+
 // Short lists (at most kLongList entries; the tail of `order`): one thread
 // per (vertex, label), the same in-order sum without staging.
 template <bool PRE_NORM, int LC = 0>
@@ -1461,6 +1548,20 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     }
     auto long_range = [&](int first, int count, cudaStream_t ls) {
         if (count <= 0) return;
+        // The lists longer than kHugeList (the first nh of the order) use the
+        // transposing ring: one warp's chain sets their time, and it issues
+        // about half the instructions per entry.  On the shorter long lists,
+        // where many warps share the SMs, splat_kernel measured faster.
+        if (L == 21 && first < nh) {
+            if (pre_norm)
+                launch(splat_ring21_kernel<true>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count,
+                       vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
+            else
+                launch(splat_ring21_kernel<false>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count,
+                       vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, (const float*)nullptr,
+                       src, sk);
+            return;
+        }
         if (pre_norm)
             launch(L == 21 ? splat_kernel<true, 21> : splat_kernel<true>, ceil_div(count, kStageWarps),
                    32 * kStageWarps, 0, ls, count, L,
