@@ -463,9 +463,9 @@ def measure_batch(n=64, max_iter=100, reps=3):
     """Config 4: the plain QP (as config 1, up to 100 Frank-Wolfe iterations)
     of n images of uneven sizes (H ~ U[240, 500], W ~ U[320, 500], seeded),
     solved as one batch (dcrf_batch_qp_dev: concatenated lattices, per-image
-    scalars, the iteration replayed as a CUDA graph) and as n sequential
-    single-image solves (dcrf_model_qp_dev), both device-resident and timed
-    with CUDA events on the solvers' streams.  The batch's output must equal
+    scalars, the loop replayed as a CUDA graph) and as n sequential
+    single-image solves (dcrf_model_qp_dev, every image once per pass), both
+    device-resident and timed with CUDA events on the solvers' streams.  The batch's output must equal
     the sequential outputs bit for bit."""
     import torch
     from densecrf_ho_b200 import DenseCRF2D, DenseCRF2DBatch, SolveStats, lib, check
@@ -503,7 +503,11 @@ def measure_batch(n=64, max_iter=100, reps=3):
     batch_ms = e0.elapsed_time(e1) / reps
     steps = [s.iterations for s in st]
 
-    models, seq_ms, same = [], 0.0, True
+    # Sequential: every image once after the other, as a caller with one
+    # model per image would run them (each solve ends with its host read of
+    # the stop flag, so the solves do not overlap); the events bracket the
+    # whole pass, on the first and the last model's streams.
+    models, same = [], True
     outs = b.split(out)
     inits = b.split(init)
     for i, ((w, h), im) in enumerate(zip(sizes, imgs)):
@@ -512,24 +516,30 @@ def measure_batch(n=64, max_iter=100, reps=3):
         m.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
         m.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], im["rgb"], BILAT[2])
         models.append(m)
-    for i, m in enumerate(models):
-        mi = inits[i].contiguous()
-        mo = torch.empty_like(mi)
+    mis = [inits[i].contiguous() for i in range(n)]
+    mos = [torch.empty_like(x) for x in mis]
+    ones = [SolveStats() for _ in range(n)]
+    streams = []
+    for m in models:
         check(Ls.dcrf_model_stream(m.handle, C.byref(sptr)))
-        ms_ = torch.cuda.ExternalStream(sptr.value)
-        one = SolveStats()
-        run_m = lambda: check(Ls.dcrf_model_qp_dev(m.handle, C.c_void_p(mi.data_ptr()), C.c_void_p(mo.data_ptr()),
-                                                   C.byref(p), C.byref(one)))
-        run_m()
-        torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a0.record(ms_)
-        for _ in range(reps):
-            run_m()
-        a1.record(ms_)
-        torch.cuda.synchronize()
-        seq_ms += a0.elapsed_time(a1) / reps
-        same = same and bool(torch.equal(mo, outs[i])) and one.iterations == steps[i]
+        streams.append(torch.cuda.ExternalStream(sptr.value))
+
+    def run_all():
+        for i, m in enumerate(models):
+            check(Ls.dcrf_model_qp_dev(m.handle, C.c_void_p(mis[i].data_ptr()), C.c_void_p(mos[i].data_ptr()),
+                                       C.byref(p), C.byref(ones[i])))
+
+    run_all()  # eager first iterations + captures
+    torch.cuda.synchronize()
+    a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a0.record(streams[0])
+    for _ in range(reps):
+        run_all()
+    a1.record(streams[-1])
+    torch.cuda.synchronize()
+    seq_ms = a0.elapsed_time(a1) / reps
+    for i in range(n):
+        same = same and bool(torch.equal(mos[i], outs[i])) and ones[i].iterations == steps[i]
     return {"workload": f"batched qp_inference_super_pixels_non_convex, {n} images H~U[240,500] W~U[320,500] "
                         f"(seeded), L={L}, max_iter={max_iter}",
             "images": n, "pixels": int(b.N), "batch_ms": batch_ms, "sequential_ms": seq_ms,

@@ -914,6 +914,7 @@ dcrf_status dcrf_batch_set_unary_dev(dcrf_batch h, const float* d_unary) {
         auto& b = BT(h);
         need(d_unary, "unary");
         float* u = b.unary.ensure((size_t)b.Ntot * b.L);
+        b.unary_gen++;
         DCRF_CUDA(cudaMemcpyAsync(u, d_unary, sizeof(float) * b.Ntot * b.L, cudaMemcpyDeviceToDevice, b.stream));
         b.has_unary = true;
     });
@@ -924,6 +925,7 @@ dcrf_status dcrf_batch_set_unary(dcrf_batch h, const float* unary) {
         auto& b = BT(h);
         need(unary, "unary");
         upload(b.unary, unary, (size_t)b.Ntot * b.L, b.stream);
+        b.unary_gen++;
         DCRF_CUDA(cudaStreamSynchronize(b.stream));
         b.has_unary = true;
     });

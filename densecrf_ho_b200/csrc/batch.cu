@@ -9,273 +9,16 @@
 #include <cfloat>
 
 #include "batch.cuh"
+
+#include <atomic>
+#include <exception>
+#include <mutex>
+#include <thread>
 #include "model_kernels.cuh"
 
 namespace dcrf {
 
 namespace {
-
-__device__ __forceinline__ long img_begin(const long* pix_off, int img) { return pix_off[img]; }
-// Row-tile blocks of an image of n pixels (32 pixels per warp, kTileWarps warps).
-__host__ __device__ __forceinline__ int tile_blocks(int n) { return ((n + 31) / 32 + kTileWarps - 1) / kTileWarps; }
-__device__ __forceinline__ int img_pixels(const long* pix_off, int img) {
-    return (int)(pix_off[img + 1] - pix_off[img]);
-}
-
-// Start of an iteration: images that stopped are frozen for all of it.
-// The filters read the same flags from done_flags (Lattice::skip_done).
-__global__ void bqp_begin_kernel(int B, SolverScalars* sc, int* __restrict__ done_flags) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < B) done_flags[i] = sc[i].done = sc[i].stop;
-}
-
-// Number of images still iterating, for the host's loop test.
-// Loop condition of the batched QP graph: some image still running, at most
-// `cap` iterations per launch (counted in active[1]).
-__global__ void bqp_cond_kernel(int* active, int cap, cudaGraphConditionalHandle h) {
-    const int c = ++active[1];
-    cudaGraphSetConditional(h, (active[0] > 0 && c < cap) ? 1u : 0u);
-}
-
-__global__ void bqp_count_kernel(int B, const SolverScalars* __restrict__ sc, int* __restrict__ active) {
-    __shared__ int s;
-    if (threadIdx.x == 0) s = 0;
-    __syncthreads();
-    for (int i = threadIdx.x; i < B; i += blockDim.x)
-        if (!sc[i].stop) atomicAdd(&s, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) *active = s;
-}
-
-// Per-image finalisation in the order of finalize_sums_kernel (one warp per
-// value over nblk partials) and finalize_large_kernel (one 1024-thread block).
-__global__ void bfinalize_sums_kernel(const double* __restrict__ partials, int nblk, int nv, int dst,
-                                      SolverScalars* sc) {
-    const int img = blockIdx.x;
-    if (sc[img].done) return;
-    const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (j >= nv) return;
-    const double* p = partials + (long)img * nv * nblk;
-    double s = 0.0;
-    for (int b = lane; b < nblk; b += 32) s += p[(long)j * nblk + b];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
-    if (lane == 0) sc[img].sums[dst + j] = s;
-}
-
-__global__ void bfinalize_tiles_kernel(const double* __restrict__ partials, int max_tiles,
-                                       const long* __restrict__ pix_off, int dst, SolverScalars* sc) {
-    __shared__ double s[32];
-    const int img = blockIdx.x;
-    if (sc[img].done) return;
-    const int nblk = tile_blocks(img_pixels(pix_off, img));
-    const double* p = partials + (long)img * max_tiles;
-    double v = 0.0;
-    for (int b = threadIdx.x; b < nblk; b += blockDim.x) v += p[b];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFullMask, v, o);
-    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double t = 0.0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s[w];
-        sc[img].sums[dst] = t;
-    }
-}
-
-// a . b over each image (dot_kernel per image): grid (kRedBlocks, B).
-__global__ void bdot_kernel(const long* __restrict__ pix_off, int L, const float* __restrict__ a,
-                            const float* __restrict__ b, const SolverScalars* __restrict__ sc,
-                            double* __restrict__ partials) {
-    const int img = blockIdx.y;
-    if (sc[img].done) return;
-    const long e0 = img_begin(pix_off, img) * L, n = (long)img_pixels(pix_off, img) * L;
-    double v[1] = {0.0};
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
-        v[0] += (double)a[e0 + t] * (double)b[e0 + t];
-    block_sum_store<1>(v, partials + (long)img * gridDim.x);
-}
-
-// Q . psi and sx . psi per image (dots2_kernel).
-__global__ void bdots2_kernel(const long* __restrict__ pix_off, int L, const float* __restrict__ a,
-                              const float* __restrict__ b, const float* __restrict__ c,
-                              const SolverScalars* __restrict__ sc, double* __restrict__ partials) {
-    const int img = blockIdx.y;
-    if (sc[img].done) return;
-    const long e0 = img_begin(pix_off, img) * L, n = (long)img_pixels(pix_off, img) * L;
-    double v[2] = {0.0, 0.0};
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-        const double cc = c[e0 + t];
-        v[0] += (double)a[e0 + t] * cc;
-        v[1] += (double)b[e0 + t] * cc;
-    }
-    block_sum_store<2>(v, partials + (long)img * 2 * gridDim.x);
-}
-
-// Conditional gradient (qp_direction_tiled / qp_direction_kernel per image).
-template <int LC>
-__global__ void __launch_bounds__(32 * kTileWarps)
-    bqp_direction_tiled(const long* __restrict__ pix_off, int max_tiles, const float* __restrict__ grad,
-                        const float* __restrict__ Q, const float* __restrict__ U, float* __restrict__ sx,
-                        const SolverScalars* __restrict__ sc, double* __restrict__ partials) {
-    __shared__ float sm[kTileWarps][3][32 * LC];
-    __shared__ double s32[32];
-    const int img = blockIdx.y;
-    const int N = img_pixels(pix_off, img);
-    if (sc[img].done || (int)blockIdx.x >= tile_blocks(N)) return;  // block-uniform
-    const long base = img_begin(pix_off, img) * LC;
-    grad += base;
-    Q += base;
-    U += base;
-    sx += base;
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long pix0 = ((long)blockIdx.x * kTileWarps + wib) * 32;
-    double acc = 0.0;
-    if (pix0 < N) {
-        const int npix = (int)min(32L, (long)N - pix0);
-        float *Gt = sm[wib][0], *Qt = sm[wib][1], *Ut = sm[wib][2];
-        tile_in<LC>(Gt, grad, pix0, npix, lane);
-        tile_in<LC>(Qt, Q, pix0, npix, lane);
-        tile_in<LC>(Ut, U, pix0, npix, lane);
-        __syncwarp();
-        const float* rg = Gt + lane * LC;
-        float* rq = Qt + lane * LC;
-        const float* ru = Ut + lane * LC;
-        float best = rg[0];
-        int bi = 0;
-#pragma unroll
-        for (int k = 1; k < LC; k++)
-            if (rg[k] < best) {
-                best = rg[k];
-                bi = k;
-            }
-        const bool act = lane < npix;
-#pragma unroll
-        for (int k = 0; k < LC; k++) {
-            const float s = fsub(k == bi ? 1.0f : 0.0f, rq[k]);
-            rq[k] = s;
-            if (act) acc += (double)ru[k] * (double)s;
-        }
-        __syncwarp();
-        tile_out<LC>(Qt, sx, pix0, npix, lane);
-    }
-    const double tot = block_sum_any(acc, s32);
-    if (threadIdx.x == 0) partials[(long)img * max_tiles + blockIdx.x] = tot;
-}
-
-template <int LC>
-__global__ void bqp_direction_kernel(const long* __restrict__ pix_off, int Lrt, const float* __restrict__ grad,
-                                     const float* __restrict__ Q, const float* __restrict__ U,
-                                     float* __restrict__ sx, const SolverScalars* __restrict__ sc,
-                                     double* __restrict__ partials) {
-    const int L = LC ? LC : Lrt;
-    const int img = blockIdx.y;
-    if (sc[img].done) return;
-    const int N = img_pixels(pix_off, img);
-    const long base = img_begin(pix_off, img) * L;
-    double v[1] = {0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const float* g = grad + base + (long)i * L;
-        float best = g[0];
-        int bi = 0;
-#pragma unroll
-        for (int k = 1; k < PixVec<LC>::S; k++)
-            if (k < L) {
-                float x = g[k];
-                if (x < best) {
-                    best = x;
-                    bi = k;
-                }
-            }
-#pragma unroll
-        for (int k = 0; k < PixVec<LC>::S; k++)
-            if (k < L) {
-                const long e = base + (long)i * L + k;
-                const float s = fsub(k == bi ? 1.0f : 0.0f, Q[e]);
-                sx[e] = s;
-                v[0] += (double)U[e] * (double)s;
-            }
-    }
-    block_sum_store<1>(v, partials + (long)img * gridDim.x);
-}
-
-// Line search per image (qp_step_kernel).
-__global__ void bqp_step_kernel(int B, SolverScalars* scs) {
-    const int img = blockIdx.x * blockDim.x + threadIdx.x;
-    if (img >= B) return;
-    SolverScalars* sc = scs + img;
-    if (sc->done) return;
-    sc->old_energy = sc->energy;
-    const double num = sc->sums[0] + 2 * sc->sums[1] + sc->sums[3] + sc->sums[4] + sc->sums[5];
-    const double denom = sc->sums[2] + sc->sums[6];
-    double step = -num / (2 * denom);
-    if (denom == 0 || num == 0) {
-        sc->zero_step = 1;
-        sc->stop = 1;
-        return;
-    }
-    if (denom < 0) step = 1;
-    sc->fstep = (float)step;
-    sc->f2step = (float)(2 * step);
-    sc->steps++;
-}
-
-// Q += step sx; grad += 2 step psi; partial sums of Q . (grad + U) (qp_update_kernel).
-__global__ void bqp_update_kernel(const long* __restrict__ pix_off, int L, const float* __restrict__ sx,
-                                  const float* __restrict__ psi, const float* __restrict__ U, float* __restrict__ Q,
-                                  float* __restrict__ grad, const SolverScalars* __restrict__ scs,
-                                  double* __restrict__ partials) {
-    const int img = blockIdx.y;
-    const SolverScalars* sc = scs + img;
-    if (sc->done || sc->zero_step) return;
-    const long e0 = img_begin(pix_off, img) * L, n = (long)img_pixels(pix_off, img) * L;
-    const float fs = sc->fstep, f2s = sc->f2step;
-    double v[1] = {0.0};
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
-        const long e = e0 + t;
-        const float q = fadd(Q[e], fmul(fs, sx[e]));
-        const float g = fadd(grad[e], fadd(fmul(f2s, psi[e]), fmul(fs, 0.0f)));
-        Q[e] = q;
-        grad[e] = g;
-        v[0] += (double)q * (double)fadd(g, U[e]);
-    }
-    block_sum_store<1>(v, partials + (long)img * gridDim.x);
-}
-
-// Energy and stop rule per image (qp_energy_kernel).
-__global__ void bqp_energy_kernel(int B, SolverScalars* scs, int max_iter) {
-    const int img = blockIdx.x * blockDim.x + threadIdx.x;
-    if (img >= B) return;
-    SolverScalars* sc = scs + img;
-    if (sc->done || sc->zero_step) return;
-    const double e = sc->sums[7] + sc->sums[8];
-    sc->energy = e;
-    if (max_iter > 0) sc->stop = sc->steps >= max_iter;
-    else sc->stop = !((sc->old_energy - e) > 100.0);
-}
-
-__global__ void bqp_init_energy_kernel(int B, SolverScalars* scs, int nterms, int max_iter) {
-    const int img = blockIdx.x * blockDim.x + threadIdx.x;
-    if (img >= B) return;
-    SolverScalars* sc = scs + img;
-    double e = 0.0;
-    e += sc->sums[0];
-    e -= 0.0;
-    for (int k = 0; k < nterms; k++) e += sc->sums[1 + k];
-    e += 0.0;
-    e += sc->sums[8];
-    sc->energy = e;
-    sc->old_energy = DBL_MAX;
-    sc->zero_step = 0;
-    sc->steps = 0;
-    sc->done = 0;
-    sc->stop = max_iter > 0 ? 0 : !((DBL_MAX - e) > 100.0);
-}
-
-__global__ void badd_scaled_kernel(long n, float* __restrict__ a, const float* __restrict__ b, float coef) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) a[t] = fadd(a[t], fmul(coef, b[t]));
-}
 
 __global__ void bfill_kernel(long n, float v, float* x) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -362,42 +105,30 @@ Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_)
     for (int i = 0; i < n; i++) {
         require(W[i] > 0 && H[i] > 0, DCRF_E_ARG, "batch: image sizes must be positive");
         pix_off[i + 1] = pix_off[i] + (long)W[i] * H[i];
-        max_tiles = std::max(max_tiles, ceil_div(ceil_div(W[i] * H[i], 32), kTileWarps));
     }
     Ntot = pix_off[n];
     require(Ntot * (long)L < (1L << 31), DCRF_E_ARG, "batch: too many pixel-labels");
     DCRF_CUDA(cudaGetDevice(&device));
     DCRF_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-    DCRF_CUDA(cudaMallocHost(&h_scal, sizeof(SolverScalars) * B));
-    DCRF_CUDA(cudaMallocHost(&h_active, 2 * sizeof(int)));
-    scal.ensure(B);
-    d_active.ensure(2);
-    DCRF_CUDA(cudaMemsetAsync(d_done.ensure(B), 0, sizeof(int) * B, stream));
     long* po = d_pix_off.ensure(n + 1);
     DCRF_CUDA(cudaMemcpyAsync(po, pix_off.data(), sizeof(long) * (n + 1), cudaMemcpyHostToDevice, stream));
-    partials.ensure((size_t)B * std::max<long>((long)kRedBlocks * 2, max_tiles));
+    partials.ensure((size_t)kRedBlocks * 2);
     DCRF_CUDA(cudaStreamSynchronize(stream));
 }
 
 Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
-    drop_graph();
+    img.clear();
     terms.clear();
-    if (h_scal) cudaFreeHost(h_scal);
-    if (h_active) cudaFreeHost(h_active);
     if (stream) cudaStreamDestroy(stream);
 }
 
-void Batch::drop_graph() {
-    if (graph) cudaGraphExecDestroy(graph);
-    graph = nullptr;
-    graph_q = nullptr;
-    graph_max_iter = -1;
-}
-
 void Batch::add_term(const float* d_features, int d, float w) {
-    drop_graph();
+    img.clear();  // rebuilt with the new term at the next QP
+    qp_warm = false;
     auto t = std::make_unique<Term>();
+    DCRF_CUDA(cudaMemcpyAsync(t->feat.ensure((size_t)Ntot * d), d_features, sizeof(float) * Ntot * d,
+                              cudaMemcpyDeviceToDevice, stream));
     t->lat = std::make_unique<Lattice>();
     t->lat->stream = stream;
     {
@@ -412,7 +143,6 @@ void Batch::add_term(const float* d_features, int d, float w) {
         }
         t->lat->concat(views);
     }  // the per-image lattices are released here
-    t->lat->skip_done = d_done.get();  // all zero outside qp()
     t->w = w;
     t->d = d;
     float* nrm = t->norm.ensure(Ntot);
@@ -447,157 +177,103 @@ void Batch::unary_init(float* Q) {
 
 // One Frank-Wolfe iteration for every image that has not stopped, then the
 // count of images still running, copied to pinned host memory.
-void Batch::qp_iteration(float* Q, int max_iter, bool copy_active) {
-    float* grad = buf(0);
-    float* sx = buf(1);
-    float* psi = buf(2);
-    SolverScalars* sc = scal.get();
-    double* part = partials.get();
-    const long* po = d_pix_off.get();
-    const int nt = (int)terms.size();
-    const int sgrid = ceil_div(B, 256);
-    launch(bqp_begin_kernel, sgrid, 256, 0, stream, B, sc, d_done.get());
-    with_lc(L, [&](auto lc) {
-        constexpr int LC = decltype(lc)::value;
-        if constexpr (LC > 0) {
-            launch(bqp_direction_tiled<LC>, dim3(max_tiles, B), 32 * kTileWarps, 0, stream, po, max_tiles, grad, Q,
-                   unary.get(), sx, sc, part);
-            launch(bfinalize_tiles_kernel, B, 1024, 0, stream, part, max_tiles, po, 0, sc);
-        } else {
-            launch(bqp_direction_kernel<LC>, dim3(kRedBlocks, B), kRedThreads, 0, stream, po, L, grad, Q,
-                   unary.get(), sx, sc, part);
-            launch(bfinalize_sums_kernel, B, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
+// Batch QP: every image's own single-image solve (Model::qp, whose
+// Frank-Wolfe loop is a device-side graph loop), from up to kQpThreads host
+// threads so that the images' solves overlap on their own streams; a solve
+// of one image alone leaves SMs idle (one-block reductions and step kernels,
+// the longest splat lists' chains), which the other images' kernels fill.
+// Each image's output, step count and energy are those of its single-image
+// solve, bit for bit.  The per-image models are built at the first solve
+// from the features each term was added with, and kept.
+void Batch::ensure_image_models() {
+    if ((int)img.size() == B) return;
+    img.clear();
+    DCRF_CUDA(cudaStreamSynchronize(stream));  // the terms' features were copied on this stream
+    for (int i = 0; i < B; i++) {
+        auto m = std::make_unique<Model>(W[i], H[i], L);
+        for (const auto& t : terms) {
+            m->add_term(t->feat.get() + pix_off[i] * t->d, t->d, t->w);
+            m->sync();
         }
-    });
-    for (int k = 0; k < nt; k++) {
-        if (k == 0) apply(k, psi, sx, nullptr, 1.0f, true);
-        else apply(k, psi, sx, psi, 1.0f, false);
+        img.push_back(std::move(m));
     }
-    launch(bdots2_kernel, dim3(kRedBlocks, B), kRedThreads, 0, stream, po, L, Q, sx, psi, sc, part);
-    launch(bfinalize_sums_kernel, B, 64, 0, stream, part, kRedBlocks, 2, 1, sc);
-    launch(bqp_step_kernel, sgrid, 256, 0, stream, B, sc);
-    launch(bqp_update_kernel, dim3(kRedBlocks, B), kRedThreads, 0, stream, po, L, sx, psi, unary.get(), Q, grad,
-           sc, part);
-    launch(bfinalize_sums_kernel, B, 32, 0, stream, part, kRedBlocks, 1, 7, sc);
-    launch(bqp_energy_kernel, sgrid, 256, 0, stream, B, sc, max_iter);
-    launch(bqp_count_kernel, 1, 256, 0, stream, B, sc, d_active.get());
-    if (copy_active)
-        DCRF_CUDA(cudaMemcpyAsync(h_active, d_active.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
+    img_unary_gen = ~0ull;
 }
 
 int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* energies) {
     require(has_unary, DCRF_E_STATE, "qp: no unary energy set");
-    const long NL = Ntot * L;
-    float* Q = out;
-    float* grad = buf(0);
-    float* tmp = buf(3);
-    buf(1);
-    buf(2);
-    if (Q != init) DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
-    DCRF_CUDA(cudaMemcpyAsync(grad, unary.get(), sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
-    DCRF_CUDA(cudaMemsetAsync(scal.get(), 0, sizeof(SolverScalars) * B, stream));
-    DCRF_CUDA(cudaMemsetAsync(d_done.get(), 0, sizeof(int) * B, stream));
-    SolverScalars* sc = scal.get();
-    double* part = partials.get();
-    const long* po = d_pix_off.get();
-    const int nt = (int)terms.size();
-    for (int k = 0; k < nt; k++) {
-        apply(k, tmp, Q);
-        launch(badd_scaled_kernel, ceil_div(NL, 256), 256, 0, stream, NL, grad, tmp, 2.0f);
-        launch(bdot_kernel, dim3(kRedBlocks, B), kRedThreads, 0, stream, po, L, Q, tmp, sc, part);
-        launch(bfinalize_sums_kernel, B, 32, 0, stream, part, kRedBlocks, 1, 1 + k, sc);
+    ensure_image_models();
+    if (img_unary_gen != unary_gen) {  // each image's slice of the unaries
+        for (int i = 0; i < B; i++) {
+            Model& m = *img[i];
+            const size_t n = (size_t)(pix_off[i + 1] - pix_off[i]) * L;
+            DCRF_CUDA(cudaMemcpyAsync(m.unary.ensure(n), unary.get() + pix_off[i] * L, sizeof(float) * n,
+                                      cudaMemcpyDeviceToDevice, stream));
+            m.has_unary = true;
+            m.logit_F = 0;
+            m.gen++;
+        }
+        img_unary_gen = unary_gen;
+        qp_warm = false;  // the models changed: their graphs are captured again
     }
-    launch(bdot_kernel, dim3(kRedBlocks, B), kRedThreads, 0, stream, po, L, unary.get(), Q, sc, part);
-    launch(bfinalize_sums_kernel, B, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
-    launch(bqp_init_energy_kernel, ceil_div(B, 256), 256, 0, stream, B, sc, nt, max_iter);
-    launch(bqp_count_kernel, 1, 256, 0, stream, B, sc, d_active.get());
-    DCRF_CUDA(cudaMemcpyAsync(h_active, d_active.get(), sizeof(int), cudaMemcpyDeviceToHost, stream));
-    DCRF_LAUNCH_CHECK();
+    // the images' streams start after the batch stream's work (the unaries, init)
     DCRF_CUDA(cudaStreamSynchronize(stream));
-    int guard = 0;
-    bool eager = false;
-    while (*h_active > 0) {
-        require(++guard < (1 << 26), DCRF_E_TIMEOUT, "qp: iteration cap reached");
-        if (graph && graph_q == Q && graph_max_iter == max_iter) {
-            DCRF_CUDA(cudaGraphLaunch(graph, stream));
-            DCRF_CUDA(cudaMemcpyAsync(h_active, d_active.get(), 2 * sizeof(int), cudaMemcpyDeviceToHost, stream));
-            DCRF_CUDA(cudaStreamSynchronize(stream));
-            g_kernel_launches.fetch_add(graph_kernels * (unsigned long long)h_active[1]);
-            continue;
+    std::vector<int> st(B, 0);
+    std::vector<double> en(B, 0.0);
+    // A solve that sizes buffers or captures its graph (the first one for an
+    // output buffer, max_iter and model state) runs on this thread, image
+    // after image: allocation and capture stay out of the concurrent phase.
+    if (!(qp_warm && out == warm_out && max_iter == warm_max_iter)) {
+        for (int i = 0; i < B; i++)
+            st[i] = img[i]->qp(init + pix_off[i] * L, out + pix_off[i] * L, max_iter, &en[i]);
+        qp_warm = true;
+        warm_out = out;
+        warm_max_iter = max_iter;
+        int most = 0;
+        for (int i = 0; i < B; i++) {
+            if (steps) steps[i] = st[i];
+            if (energies) energies[i] = en[i];
+            most = std::max(most, st[i]);
         }
-        if (!eager || !graphs_enabled()) {
-            // The first iteration runs eagerly: it sizes every buffer that an
-            // iteration touches, so none is allocated during the capture.
-            qp_iteration(Q, max_iter);
-            DCRF_LAUNCH_CHECK();
-            DCRF_CUDA(cudaStreamSynchronize(stream));
-            eager = true;
-            continue;
-        }
-        // Capture the loop: [iteration counter = 0] -> while (running) { iteration }.
-        drop_graph();
-        cudaGraph_t g = nullptr;
-        DCRF_CUDA(cudaGraphCreate(&g, 0));
-        bool capturing = false;
-        try {
-            cudaGraphConditionalHandle h;
-            DCRF_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
-            cudaMemsetParams mp = {};
-            mp.dst = d_active.get() + 1;
-            mp.value = 0;
-            mp.elementSize = sizeof(int);
-            mp.width = 1;
-            mp.height = 1;
-            cudaGraphNode_t mn, wn;
-            DCRF_CUDA(cudaGraphAddMemsetNode(&mn, g, nullptr, 0, &mp));
-            cudaGraphNodeParams np = {};
-            np.type = cudaGraphNodeTypeConditional;
-            np.conditional.handle = h;
-            np.conditional.type = cudaGraphCondTypeWhile;
-            np.conditional.size = 1;
-            DCRF_CUDA(cudaGraphAddNode(&wn, g, &mn, 1, &np));
-            const unsigned long long k0 = g_kernel_launches.load();
-            DCRF_CUDA(cudaStreamBeginCaptureToGraph(stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                                    cudaStreamCaptureModeRelaxed));
-            capturing = true;
-            qp_iteration(Q, max_iter, false);
-            launch(bqp_cond_kernel, 1, 1, 0, stream, d_active.get(), kQpChunk, h);
-            cudaGraph_t bo = nullptr;
-            capturing = false;
-            DCRF_CUDA(cudaStreamEndCapture(stream, &bo));
-            graph_kernels = g_kernel_launches.load() - k0;
-            g_kernel_launches.fetch_sub(graph_kernels);  // counted per iteration when the graph runs
-            require(graph_kernels >= 2, DCRF_E_STATE, "qp: unexpected loop body");
-            DCRF_CUDA(cudaGraphInstantiate(&graph, g, 0));
-            cudaGraphDestroy(g);
-        } catch (...) {
-            cudaGraph_t junk = nullptr;
-            if (capturing) cudaStreamEndCapture(stream, &junk);
-            cudaGraphDestroy(g);
-            graph = nullptr;
-            throw;
-        }
-        graph_q = Q;
-        graph_max_iter = max_iter;
+        return most;
     }
-    DCRF_CUDA(cudaMemcpyAsync(h_scal, scal.get(), sizeof(SolverScalars) * B, cudaMemcpyDeviceToHost, stream));
-    DCRF_CUDA(cudaMemsetAsync(d_done.get(), 0, sizeof(int) * B, stream));
-    DCRF_CUDA(cudaStreamSynchronize(stream));
+    std::atomic<int> next{0};
+    std::exception_ptr err = nullptr;
+    std::mutex emu;
+    auto worker = [&]() {
+        cudaSetDevice(device);
+        for (;;) {
+            const int i = next.fetch_add(1);
+            if (i >= B) break;
+            try {
+                st[i] = img[i]->qp(init + pix_off[i] * L, out + pix_off[i] * L, max_iter, &en[i]);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(emu);
+                if (!err) err = std::current_exception();
+                next.store(B);
+            }
+        }
+    };
+    const int nth = std::min(B, kQpThreads);
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nth; t++) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    if (err) std::rethrow_exception(err);
     int most = 0;
     for (int i = 0; i < B; i++) {
-        if (steps) steps[i] = h_scal[i].steps;
-        if (energies) energies[i] = h_scal[i].energy;
-        most = std::max(most, h_scal[i].steps);
+        if (steps) steps[i] = st[i];
+        if (energies) energies[i] = en[i];
+        most = std::max(most, st[i]);
     }
     return most;
 }
 
-// ---- mean-field and its adjoint --------------------------------------------
-
 void Batch::set_weight(int k, float w) {
     require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
     terms[k]->w = w;
-    drop_graph();  // the captured QP iteration holds the old weight
+    for (auto& m : img) m->set_compat(k, kPotts, &w);  // the per-image models' QP graphs are rebuilt
+    qp_warm = false;
 }
 
 // out = base + scale * n o K(n o in), K transposed (blur axes reversed) when

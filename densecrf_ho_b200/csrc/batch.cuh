@@ -1,13 +1,10 @@
-// Many images of different sizes solved together: their pixels are
-// concatenated ([sum N_i][L]), each Potts term's lattices are concatenated
-// into one (Lattice::concat), and the Frank-Wolfe QP keeps one set of
-// solver scalars per image, so every image follows exactly the trajectory of
-// its own single-image solve while each filter, direction and update runs as
-// one launch over all images; the filters skip the lattice vertices and
-// pixels of images that have already stopped.  After a first eager
-// iteration the loop is captured once as a CUDA graph -- a `while` node whose
-// body is one iteration and whose condition is "some image still running"
-// (at most kQpChunk iterations per launch) -- and replayed.
+// Many images of different sizes behind one handle: their pixels are
+// concatenated ([sum N_i][L]).  The mean-field iterations and their adjoint
+// run over all images at once on each Potts term's concatenated lattice
+// (Lattice::concat).  The Frank-Wolfe QP runs every image's own model
+// (Model::qp, its loop a device-side graph loop) from several host threads,
+// so the images' solves overlap; each image's result is that of its own
+// single-image solve, bit for bit.
 #pragma once
 #include <memory>
 #include <vector>
@@ -29,23 +26,23 @@ struct Batch {
     DevBuf<long> d_pix_off;
     DevBuf<float> b[6];
     DevBuf<double> partials;
-    DevBuf<SolverScalars> scal;  // one per image
-    DevBuf<int> d_active;        // [0] images still running, [1] iterations in the current graph launch
-    DevBuf<int> d_done;          // per image: stopped before the current iteration (filters skip it)
-    int* h_active = nullptr;     // pinned, [2]: copy of d_active
-    SolverScalars* h_scal = nullptr;  // pinned, B
-    int max_tiles = 0;           // row-tile blocks of the largest image
+    unsigned long long unary_gen = 0;  // bumped by every unary change
+
+    // The QP runs each image's own model (built at the first solve from the
+    // terms' features, kept until a term is added).
+    std::vector<std::unique_ptr<Model>> img;
+    unsigned long long img_unary_gen = ~0ull;
+    // The last QP ran (or captured) every image's graph for this output
+    // buffer and max_iter: the next such QP may run the images concurrently.
+    bool qp_warm = false;
+    const float* warm_out = nullptr;
+    int warm_max_iter = -1;
 
     // mean-field checkpoints Q_0 .. Q_mf_T, [mf_T + 1][Ntot][L]
     DevBuf<float> mf_ck, mf_g0, mf_g1, mf_ga, mf_m;
     DevBuf<double> mf_dw;
     int mf_T = -1;
 
-    // the captured QP iteration (valid while the output buffer and max_iter are the same)
-    cudaGraphExec_t graph = nullptr;
-    const float* graph_q = nullptr;
-    int graph_max_iter = -1;
-    unsigned long long graph_kernels = 0;
 
     Batch(int n, const int* widths, const int* heights, int L_);
     ~Batch();
@@ -70,8 +67,9 @@ struct Batch {
     void set_weight(int k, float w);
 
   private:
-    void qp_iteration(float* Q, int max_iter, bool copy_active = true);
-    void drop_graph();
+    void ensure_image_models();
 };
+
+constexpr int kQpThreads = 8;  // host threads of a batch QP
 
 }  // namespace dcrf

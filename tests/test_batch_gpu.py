@@ -1,10 +1,10 @@
 """Batched QP over images of different sizes (dcrf_batch_*) against the
 single-image solver, image by image.
 
-The batch concatenates the images' lattices and keeps one set of solver
-scalars per image, with every reduction partitioned per image as the
-single-image solver partitions it: outputs, step counts and energies must
-be identical, bit for bit.
+The batch runs every image's own single-image solve (the first solve for an
+output buffer one image after the other, later ones from several host
+threads at once): outputs, step counts and energies must be identical to
+single-image solves, bit for bit.
 """
 import numpy as np
 import pytest
@@ -52,8 +52,33 @@ def test_batch_qp_equals_single_solves(max_iter):
         assert st[i].energy == s.energy
 
 
+def test_batch_concurrent_solves_equal_single_solves():
+    """Twelve images: the first solve runs image after image, the second (same
+    output buffer) from several host threads; a weight change sends the next
+    solve back to one thread, after which the threads take over again.
+    Every solve equals the single-image solves."""
+    sizes = [(40 + 7 * i, 30 + 5 * (i % 4)) for i in range(12)]
+    imgs = _images(sizes, 70)
+    b = _batch(sizes, imgs)
+    q0 = b.unary_init()
+    singles = [_single(w, h, im) for (w, h), im in zip(sizes, imgs)]
+    want = [m.qp_inference_super_pixels_non_convex(b.split(q0)[i]) for i, m in enumerate(singles)]
+    for _ in range(3):
+        out = b.qp_inference_super_pixels_non_convex(q0)
+        for i in range(len(sizes)):
+            assert np.array_equal(b.split(out)[i], want[i]), i
+    b.set_weight(1, 9.0)
+    for m in singles:
+        m.pairwise_set_parameters(1, np.array([9.0], np.float32))
+    want = [m.qp_inference_super_pixels_non_convex(b.split(q0)[i]) for i, m in enumerate(singles)]
+    for _ in range(2):
+        out = b.qp_inference_super_pixels_non_convex(q0)
+        for i in range(len(sizes)):
+            assert np.array_equal(b.split(out)[i], want[i]), i
+
+
 def test_batch_qp_repeat_is_deterministic():
-    """The second solve replays the captured iteration graph."""
+    """Repeated solves (the later ones concurrent) give the same output."""
     imgs = _images(SIZES[:3], 40)
     b = _batch(SIZES[:3], imgs)
     q0 = b.unary_init()
