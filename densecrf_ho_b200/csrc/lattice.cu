@@ -1529,6 +1529,11 @@ void Lattice::compute_noalloc(float* out, const float* in, int L, bool reverse) 
 
 void Lattice::compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,
                       const float* pre_norm) {
+    splat_blur(in, L, reverse, pre_norm);
+    slice(out, L, ep);
+}
+
+void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_norm) {
     require(L >= 1, DCRF_E_ARG, "compute: L must be >= 1");
     ensure_values((size_t)L);
     cudaStream_t st = stream;
@@ -1598,6 +1603,16 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
             launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
         std::swap(src, dst);
     }
+    plain_vals = src;
+    plain_L = L;
+}
+
+void Lattice::slice(float* out, int L, const SliceEpilogue& ep) {
+    require(plain_vals && plain_L == L, DCRF_E_STATE, "slice: no splat_blur for this label count before it");
+    cudaStream_t st = stream;
+    const long NL = (long)N * L;
+    const float* src = plain_vals;
+    const bool seq = L <= 2;
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     const Skip sks{vimg.get(), skip_done};
     auto sl = [&](auto kern) {

@@ -84,6 +84,12 @@ struct Lattice {
     // out/in: device [N][L]; out may alias in.
     void compute(float* out, const float* in, int L, bool reverse, const SliceEpilogue& ep,
                  const float* pre_norm = nullptr);
+    // The same in two phases: splat + blur (the vertex values stay in
+    // plain_vals), then the slice.  Other work may run between them.
+    void splat_blur(const float* in, int L, bool reverse, const float* pre_norm = nullptr);
+    void slice(float* out, int L, const SliceEpilogue& ep);
+    const float* plain_vals = nullptr;
+    int plain_L = 0;
     // The plain filter with its value buffers in a fixed device array instead
     // of memory from cudaMalloc (see dcrf_lattice_compute_noalloc).
     void compute_noalloc(float* out, const float* in, int L, bool reverse);

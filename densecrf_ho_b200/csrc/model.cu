@@ -642,6 +642,53 @@ void Model::apply_ord(int k, float* out, const float* rq, const float* base, boo
     finish_compat(*this, t, r, out, base, 1.0f, zero_base);
 }
 
+// out = sum_k apply_k(in) in term order (out = 0 + t_0, then out += t_k), as
+// the QP's pairwise sums are formed (src/densecrf.cpp:411-420): the splat and
+// blur of terms 1.. run on the side stream while term 0's run on the model's
+// stream, then the slices carry the sum in term order.  Images above
+// kSplitMaxPixels and Matrix terms (their product runs after the slice) take
+// the plain path, one term after the other.
+void Model::apply_sum(float* out, const float* in) {
+    const int nt = (int)terms.size();
+    // Concurrency pays on images that do not fill the GPU alone (measured:
+    // 320x240 QP 1123 -> 1190 solves/s); on larger ones the two filters
+    // compete for L2 and the sum is slower (240-500 px sides: -15 %).
+    bool split = nt >= 2 && N <= kSplitMaxPixels;
+    for (const auto& t : terms) split = split && t->compat != kMatrix;
+    if (!split) {
+        for (int k = 0; k < nt; k++) apply(k, false, out, in, k == 0 ? nullptr : out, 1.0f, k == 0);
+        return;
+    }
+    if (!side) {
+        DCRF_CUDA(cudaStreamCreateWithFlags(&side, cudaStreamNonBlocking));
+        DCRF_CUDA(cudaEventCreateWithFlags(&ev_side_fork, cudaEventDisableTiming));
+        DCRF_CUDA(cudaEventCreateWithFlags(&ev_side_join, cudaEventDisableTiming));
+    }
+    DCRF_CUDA(cudaEventRecord(ev_side_fork, stream));
+    DCRF_CUDA(cudaStreamWaitEvent(side, ev_side_fork, 0));
+    for (int k = 1; k < nt; k++) {
+        Term& t = *terms[k];
+        t.lat->stream = side;
+        try {
+            t.lat->splat_blur(in, L, false, t.pre_norm());
+        } catch (...) {
+            t.lat->stream = stream;
+            throw;
+        }
+        t.lat->stream = stream;
+    }
+    DCRF_CUDA(cudaEventRecord(ev_side_join, side));
+    terms[0]->lat->splat_blur(in, L, false, terms[0]->pre_norm());
+    DCRF_CUDA(cudaStreamWaitEvent(stream, ev_side_join, 0));
+    for (int k = 0; k < nt; k++) {
+        const Term& t = *terms[k];
+        SliceEpilogue ep;
+        ep.norm = t.post_norm();
+        route_compat(*this, t, ep, out, k == 0 ? nullptr : out, 1.0f, k == 0);
+        t.lat->slice(out, L, ep);
+    }
+}
+
 // sa = sum_k apply_upper_minus_lower_ord_k(rescale(Q)) from shared bins, the
 // sum in term order (sa = 0 + t_0, then sa += t_k) as the reference adds it
 // (src/densecrf.cpp:705-716).  The splat and blur phases of terms 1.. run on

@@ -65,6 +65,7 @@ struct SolverScalars {
 };
 
 constexpr int kQpChunk = 64;  // QP iterations per graph launch at most
+constexpr int kSplitMaxPixels = 1 << 17;  // apply_sum runs the terms' filters concurrently up to this size
 
 struct Model {
     int W = 0, H = 0, N = 0, L = 0, device = 0;
@@ -161,6 +162,8 @@ struct Model {
                         const GapFusion* gap);
     void apply_ord(int k, float* out, const float* rq, const float* base = nullptr,
                    bool zero_base = false);
+    // out = sum_k apply_k(in), terms in order, their splats and blurs concurrent.
+    void apply_sum(float* out, const float* in);
     // Checks Q in [0,1] like apply_upper_minus_lower_ord (throws DCRF_E_RANGE).
     void check_unit_range(const float* Q);
 

@@ -1299,10 +1299,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t2, preS, 4, sc, 0);   // b
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preS, 6, sc, 0);   // denom term
         }
-        for (int k = 0; k < nt; k++) {
-            if (k == 0) apply(k, false, psi, sx, nullptr, 1.0f, true);
-            else apply(k, false, psi, sx, psi, 1.0f, false);
-        }
+        apply_sum(psi, sx);
         launch(dots2_kernel, kRedBlocks, kRedThreads, 0, stream, NL, Q, sx, psi, part);
         launch(finalize_sums_kernel, 1, 64, 0, stream, part, kRedBlocks, 2, 1, sc);
         launch(qp_step_kernel, 1, 1, 0, stream, sc);
