@@ -6,6 +6,7 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <mutex>
 #include <cstdio>
 #include <stdexcept>
 #include <string>
@@ -42,6 +43,10 @@ inline void require(bool ok, dcrf_status code, const std::string& msg) {
 // cudaFree does, then keeps the block for reuse up to DCRF_CACHE_MB
 // (default 2048) MiB of cached memory per process, beyond which it frees it.
 void* dev_alloc(size_t bytes, size_t* got);
+// Held while a solver loop is captured into a CUDA graph, and by dev_alloc /
+// dev_release around cudaMalloc, cudaFree and the device-wide wait: a thread
+// that frees or allocates waits until another thread's capture has ended.
+std::recursive_mutex& capture_mutex();
 void dev_release(void* p, size_t bytes) noexcept;
 // Frees the cached blocks of the current device, or of every device
 // (dcrf_release_cached_memory).

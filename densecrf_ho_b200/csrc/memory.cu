@@ -47,6 +47,11 @@ size_t size_class(size_t b) {
 
 }  // namespace
 
+std::recursive_mutex& capture_mutex() {
+    static auto* m = new std::recursive_mutex();  // never destroyed
+    return *m;
+}
+
 void* dev_alloc(size_t bytes, size_t* got) {
     const size_t b = size_class(bytes);
     int dev = 0;
@@ -64,6 +69,7 @@ void* dev_alloc(size_t bytes, size_t* got) {
                 return p;
             }
     }
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
     void* p = nullptr;
     cudaError_t e = cudaMalloc(&p, b);
     if (e == cudaErrorMemoryAllocation) {  // give the cached blocks back and try once more
@@ -78,6 +84,7 @@ void* dev_alloc(size_t bytes, size_t* got) {
 
 void dev_release(void* p, size_t bytes) noexcept {
     if (!p) return;
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
     // the block's own device (the caller's current device may be another)
     int cur = 0, dev = 0;
     cudaPointerAttributes a;
@@ -107,6 +114,7 @@ void dev_release(void* p, size_t bytes) noexcept {
 }
 
 void dev_trim(bool all_devices) noexcept {
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return;
     std::vector<void*> drop;

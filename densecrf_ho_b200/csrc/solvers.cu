@@ -1166,6 +1166,7 @@ void Model::drop_qp_graph() {
 
 template <typename F>
 void Model::build_qp_graph(F&& qp_iter) {
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
     drop_qp_graph();
     SolverScalars* sc = scal.get();
     cudaGraph_t g = nullptr;
@@ -1523,6 +1524,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     int eager_gamma = 0;
     auto drop_graphs = [&]() { fwg.drop(); };
     auto build_graph = [&](bool pending) -> cudaGraphExec_t {
+        std::lock_guard<std::recursive_mutex> cap(capture_mutex());
         if (!gstream) DCRF_CUDA(cudaStreamCreateWithFlags(&gstream, cudaStreamNonBlocking));
         cudaGraph_t g = nullptr;
         DCRF_CUDA(cudaGraphCreate(&g, 0));
