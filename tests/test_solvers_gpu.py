@@ -463,3 +463,44 @@ def test_graph_loops_match_eager_launches(tmp_path):
         outs[flag] = np.load(f)
     for k in ("qp", "lp"):
         assert _eq(outs["1"][k], outs["0"][k]), k
+
+
+def test_models_solved_from_several_threads():
+    """Four models, each built and solved (QP and a short LP, first solves
+    included, so their graphs are captured) from its own host thread at the
+    same time, give the outputs of the same solves run one after the other."""
+    import threading
+    sizes = [(64, 48), (80, 40), (48, 64), (72, 56)]
+    imgs = [synth.make_image(w, h, 21, 90 + i) for i, (w, h) in enumerate(sizes)]
+
+    def solve(i, out):
+        (w, h), im = sizes[i], imgs[i]
+        m = DenseCRF2D(w, h, 21)
+        m.setUnaryEnergy(im["unary"])
+        m.addPairwiseGaussian(3.0, 3.0, 3.0)
+        m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, im["rgb"], 5.0)
+        Q = m.unary_init()
+        out[i] = (m.qp_inference_super_pixels_non_convex(Q),
+                  m.qp_inference_super_pixels_non_convex(Q, max_iter=10),
+                  m.lp_inference_prox_super_pixels(Q, prox_max_iter=2, fw_max_iter=3))
+
+    alone = {}
+    for i in range(len(sizes)):
+        solve(i, alone)
+    together, errors = {}, []
+
+    def run(i):
+        try:
+            solve(i, together)
+        except Exception as e:  # noqa: BLE001 -- reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(len(sizes))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for i in range(len(sizes)):
+        for a, b in zip(alone[i], together[i]):
+            assert _eq(a, b), i
