@@ -256,7 +256,10 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
     };
     const int nth = std::min(B, kQpThreads);
     std::vector<std::thread> pool;
-    for (int t = 1; t < nth; t++) pool.emplace_back(worker);
+    try {
+        for (int t = 1; t < nth; t++) pool.emplace_back(worker);
+    } catch (...) {  // fewer threads than asked for: the ones running finish the images
+    }
     worker();
     for (auto& th : pool) th.join();
     if (err) std::rethrow_exception(err);
