@@ -342,6 +342,39 @@ class DenseCRF2D:
             int(bool(store))))
         return out
 
+    def pairwise_apply_bf(self, k, Q, nonorm=False):
+        """``pairwise_[k]->apply_bf(out, Q)`` (``no_norm_pairwise_[k]`` with
+        nonorm): the exact Gaussian filter, O(N^2) per label."""
+        q = self._mat(Q)
+        out = self._new()
+        check(lib().dcrf_model_pairwise_apply_bf(self._h, int(k), int(bool(nonorm)), out.ctypes.data_as(C.c_void_p),
+                                                 q.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def _sorted(self, fn, k, ind, Q, nonorm):
+        i = np.ascontiguousarray(ind, np.int32).reshape(self.N, self.L)
+        out = self._new()
+        args = [self._h, int(k), int(bool(nonorm)), out.ctypes.data_as(C.c_void_p), i.ctypes.data_as(C.c_void_p)]
+        if Q is not None:
+            q = self._mat(Q)
+            args.append(q.ctypes.data_as(C.c_void_p))
+        check(getattr(lib(), fn)(*args))
+        return out
+
+    def pairwise_apply_upper_minus_lower_bf(self, k, ind, nonorm=False):
+        """``apply_upper_minus_lower_bf(out, ind)``: ind [N, L], ind[c, l] the
+        pixel at sorted position c for label l; out in sorted positions."""
+        return self._sorted("dcrf_model_pairwise_apply_upper_minus_lower_bf", k, ind, None, nonorm)
+
+    def pairwise_apply_upper_minus_lower_bf_ord(self, k, ind, Q, nonorm=False):
+        """``apply_upper_minus_lower_bf_ord(out, ind, Q)``."""
+        return self._sorted("dcrf_model_pairwise_apply_upper_minus_lower_bf_ord", k, ind, Q, nonorm)
+
+    def pairwise_apply_upper_minus_lower_dc(self, k, ind, nonorm=False):
+        """``apply_upper_minus_lower_dc(out, ind)``: the divide-and-conquer
+        ordered filter on lattices of the sorted features."""
+        return self._sorted("dcrf_model_pairwise_apply_upper_minus_lower_dc", k, ind, None, nonorm)
+
     def qp_inference_super_pixels_non_convex(self, init, max_iter=0, stats=False):
         x = self._mat(init)
         out = self._new()

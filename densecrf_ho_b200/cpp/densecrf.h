@@ -262,6 +262,20 @@ class PairwisePotential {
         dcrf_shim::set_kernel(m_, 0, kt_, nt_);
         L_ = L;
     }
+    void sorted(MatrixXf& out, const MatrixXi& ind, const MatrixXf* Q, int kind) const {
+        auto* self = const_cast<PairwisePotential*>(this);
+        self->ensure((int)ind.rows());
+        Eigen::Matrix<int32_t, Eigen::Dynamic, Eigen::Dynamic> idx = ind.cast<int32_t>();
+        out.resize(ind.rows(), ind.cols());
+        if (kind == 0)
+            dcrf_shim::check(dcrf_model_pairwise_apply_upper_minus_lower_bf(m_, 0, 0, out.data(), idx.data()));
+        else if (kind == 1) {
+            MatrixXf src = *Q;
+            dcrf_shim::check(
+                dcrf_model_pairwise_apply_upper_minus_lower_bf_ord(m_, 0, 0, out.data(), idx.data(), src.data()));
+        } else
+            dcrf_shim::check(dcrf_model_pairwise_apply_upper_minus_lower_dc(m_, 0, 0, out.data(), idx.data()));
+    }
 public:
     PairwisePotential(const MatrixXf& features, LabelCompatibility* compatibility, KernelType ktype = CONST_KERNEL,
                       NormalizationType ntype = NORMALIZE_SYMMETRIC)
@@ -285,6 +299,23 @@ public:
         MatrixXf src = Q;
         out.resize(Q.rows(), Q.cols());
         dcrf_shim::check(dcrf_model_pairwise_apply_ord(m_, 0, out.data(), src.data()));
+    }
+    // The exact filters and the divide-and-conquer filter
+    // (src/pairwise.cpp:241-380); ind is L x N (sortRows), out L x N in
+    // sorted positions for the sorted variants.
+    void apply_bf(MatrixXf& out, const MatrixXf& Q) const {
+        auto* self = const_cast<PairwisePotential*>(this);
+        self->ensure((int)Q.rows());
+        MatrixXf src = Q;
+        out.resize(Q.rows(), Q.cols());
+        dcrf_shim::check(dcrf_model_pairwise_apply_bf(m_, 0, 0, out.data(), src.data()));
+    }
+    void apply_upper_minus_lower_dc(MatrixXf& out, const MatrixXi& ind) const {
+        sorted(out, ind, nullptr, 2);
+    }
+    void apply_upper_minus_lower_bf(MatrixXf& out, const MatrixXi& ind) const { sorted(out, ind, nullptr, 0); }
+    void apply_upper_minus_lower_bf_ord(MatrixXf& out, const MatrixXi& ind, const MatrixXf& Q) const {
+        sorted(out, ind, &Q, 1);
     }
     VectorXf parameters() const {
         if (c_.kind == DCRF_COMPAT_MATRIX) {  // the upper triangle by column

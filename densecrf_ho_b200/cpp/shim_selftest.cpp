@@ -7,6 +7,7 @@
 // files <out_prefix>.{init,qp,lp,filt,pw,qpc}; energies and the error-path
 // checks go to stdout.
 #include <cstdio>
+#include <algorithm>
 #include <fstream>
 #include <iostream>
 #include <vector>
@@ -66,6 +67,16 @@ int main(int argc, char** argv) {
         PairwisePotential pw(F, new PottsCompatibility(3));
         MatrixXf pwo;
         pw.apply(pwo, Q);
+        // the divide-and-conquer filter on the positions sorted by decreasing Q
+        Eigen::MatrixXi ind(L, N);
+        for (int l = 0; l < L; l++) {
+            std::vector<int> o(N);
+            for (int c = 0; c < N; c++) o[c] = c;
+            std::stable_sort(o.begin(), o.end(), [&](int a, int b) { return Q(l, a) > Q(l, b); });
+            for (int c = 0; c < N; c++) ind(l, c) = o[c];
+        }
+        MatrixXf dco;
+        pw.apply_upper_minus_lower_dc(dco, ind);
 
         MatrixXf bad = Q;
         bad(0, 0) = 2.0f;  // out of [0, 1]
@@ -102,6 +113,7 @@ int main(int argc, char** argv) {
         write_raw(out + ".lp", lp);
         write_raw(out + ".filt", filt);
         write_raw(out + ".pw", pwo);
+        write_raw(out + ".dc", dco);
     } catch (const std::exception& e) {
         fprintf(stderr, "error: %s\n", e.what());
         return 1;

@@ -603,6 +603,77 @@ dcrf_status dcrf_model_pairwise_apply_ord_restricted(dcrf_model h, int k, float*
     });
 }
 
+namespace {
+// ind(l, c) of apply_upper_minus_lower_{bf,bf_ord,dc}: [N][L], each in [0, N).
+void check_ind(const dcrf::Model& m, const int32_t* ind) {
+    need(ind, "ind");
+    const size_t n = (size_t)m.N * m.L;
+    for (size_t t = 0; t < n; t++)
+        if (ind[t] < 0 || ind[t] >= m.N) throw Error(DCRF_E_ARG, "ind: entries must lie in [0, N)");
+}
+}  // namespace
+
+dcrf_status dcrf_model_pairwise_apply_bf(dcrf_model h, int k, int nonorm, float* out, const float* Q) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(out, "out");
+        need(Q, "Q");
+        const size_t n = (size_t)m.N * m.L;
+        const float* dq = upload(h->io0, Q, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        m.apply_bf(k, nonorm != 0, dout, dq);
+        download(out, dout, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply_upper_minus_lower_bf(dcrf_model h, int k, int nonorm, float* out,
+                                                         const int32_t* ind) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(out, "out");
+        check_ind(m, ind);
+        const size_t n = (size_t)m.N * m.L;
+        const int* di = upload(h->ipi, ind, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        m.apply_upper_minus_lower_bf(k, nonorm != 0, dout, di, nullptr);
+        download(out, dout, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply_upper_minus_lower_bf_ord(dcrf_model h, int k, int nonorm, float* out,
+                                                             const int32_t* ind, const float* Q) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(out, "out");
+        need(Q, "Q");
+        check_ind(m, ind);
+        const size_t n = (size_t)m.N * m.L;
+        const int* di = upload(h->ipi, ind, n, m.stream);
+        const float* dq = upload(h->io0, Q, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        m.apply_upper_minus_lower_bf(k, nonorm != 0, dout, di, dq);
+        download(out, dout, n, m.stream);
+    });
+}
+
+dcrf_status dcrf_model_pairwise_apply_upper_minus_lower_dc(dcrf_model h, int k, int nonorm, float* out,
+                                                         const int32_t* ind) {
+    return guard([&] {
+        auto& m = M(h);
+        check_term(m, k);
+        need(out, "out");
+        check_ind(m, ind);
+        const size_t n = (size_t)m.N * m.L;
+        const int* di = upload(h->ipi, ind, n, m.stream);
+        float* dout = h->io1.ensure(n);
+        m.apply_upper_minus_lower_dc(k, nonorm != 0, dout, di);
+        download(out, dout, n, m.stream);
+    });
+}
+
 dcrf_status dcrf_model_qp_dev(dcrf_model h, const float* d_init, float* d_out, const dcrf_qp_params* params,
                               dcrf_solve_stats* stats) {
     return guard([&] {

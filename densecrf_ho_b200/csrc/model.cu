@@ -593,6 +593,20 @@ static void finish_compat(Model& m, const Term& t, const CompatRoute& r, float* 
     DCRF_LAUNCH_CHECK();
 }
 
+void Model::apply_compat(int k, bool nonorm, float* out, const float* in) {
+    const Term& t = *terms.at(k);
+    const long NL = (long)N * L;
+    const int g = ceil_div(NL, 256), kind = nonorm ? (int)kPotts : t.compat;
+    if (kind == kPotts)  // out = -w Q (src/labelcompatibility.cpp:49-52)
+        launch(scale_cols_kernel, g, 256, 0, stream, NL, L, in, (const float*)nullptr, -t.w, out);
+    else if (kind == kDiagonal)
+        launch(scale_labels_kernel, g, 256, 0, stream, NL, L, in, (const float*)t.cw.get(), out);
+    else
+        launch(matrix_compat_kernel, g, 256, 0, stream, NL, L, (const float*)t.cw.get(), in, (const float*)nullptr,
+               1.0f, 0, out);
+    DCRF_LAUNCH_CHECK();
+}
+
 void Model::set_compat(int k, int kind, const float* params) {
     gen++;  // a captured QP graph may hold what this changes
     require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");

@@ -151,6 +151,19 @@ struct Model {
     // compatibility; rout, rQ [nP][L], pI (device) strictly ascending.
     void apply_ord_restricted(int k, float* rout, const float* rQ, const int* pI, int nP, const float* Q,
                               bool store);
+    // The exact filters and the divide-and-conquer ordered filter of
+    // PairwisePotential (src/pairwise.cpp:241-380): apply_bf(out, Q),
+    // apply_upper_minus_lower_bf(out, ind) (Q = nullptr) /
+    // apply_upper_minus_lower_bf_ord(out, ind, Q) and
+    // apply_upper_minus_lower_dc(out, ind); device [N][L] buffers, ind [N][L]
+    // (ind(l, c) at c L + l); nonorm applies the Potts compatibility of
+    // no_norm_pairwise_[k] instead of the term's.
+    void apply_bf(int k, bool nonorm, float* out, const float* Q);
+    void apply_upper_minus_lower_bf(int k, bool nonorm, float* out, const int* ind, const float* Q);
+    void apply_upper_minus_lower_dc(int k, bool nonorm, float* out, const int* ind);
+    // out = compatibility_->apply(in) of term k (nonorm: its Potts twin's);
+    // out must not alias in.
+    void apply_compat(int k, bool nonorm, float* out, const float* in);
     void set_unary_logistic(const float* lw, const float* lf, int F);  // host arrays
     void set_unary_parameters(const float* lw);
     int unary_gradient(const float* b, float* out);  // b f^T, L x F column-major; returns L F

@@ -250,6 +250,33 @@ dcrf_status dcrf_model_pairwise_apply_ord(dcrf_model m, int k, float* out, const
  * its label compatibility; rout, rQ [nP][L], Q [N][L]. */
 dcrf_status dcrf_model_pairwise_apply_ord_restricted(dcrf_model m, int k, float* rout, const float* rQ,
                                                      const int32_t* pI, int nP, const float* Q, int store);
+/* The exact filters of PairwisePotential (src/pairwise.cpp:301-380,
+ * include/pairwise.h:73-77) with k(c, b) = exp(-|f_c - f_b|^2) on the
+ * features the term was added with, each followed by the term's label
+ * compatibility (nonorm: the Potts compatibility of no_norm_pairwise_[k]).
+ * O(N^2) work per label; the reference keeps them for its BRUTE_FORCE
+ * energy check.  out, Q [N][L]; ind [N][L] with ind(l, c) at c L + l, the
+ * pixel at sorted position c for label l (sortRows, src/eigen_utils.cpp:
+ * 76-94), entries in [0, N) (DCRF_E_ARG otherwise); the sorted variants
+ * write out in sorted positions.
+ *   apply_bf(out, Q):                  out(l, c) = sum_b k(c, b) Q(l, b)
+ *   apply_upper_minus_lower_bf(out, ind): sum_{b>c} k - sum_{b<c} k
+ *   apply_upper_minus_lower_bf_ord(out, ind, Q): + k over b with
+ *       Q(l, ind(l, b)) <= Q(l, ind(l, c)), - k over b with >= */
+dcrf_status dcrf_model_pairwise_apply_bf(dcrf_model m, int k, int nonorm, float* out, const float* Q);
+dcrf_status dcrf_model_pairwise_apply_upper_minus_lower_bf(dcrf_model m, int k, int nonorm, float* out,
+                                                         const int32_t* ind);
+dcrf_status dcrf_model_pairwise_apply_upper_minus_lower_bf_ord(dcrf_model m, int k, int nonorm, float* out,
+                                                             const int32_t* ind, const float* Q);
+/* PairwisePotential::apply_upper_minus_lower_dc(out, ind) (src/pairwise.cpp:
+ * 241-300, src/permutohedral.cpp:902-997): the sorted upper-minus-lower sum
+ * by recursive halving of the sorted positions, pairs within blocks of at
+ * most 30 positions exactly (times 1 / 0.6), the cross terms of each
+ * halving by a lattice filter on a lattice of the sorted features, over the
+ * vertices of the halves only; then the compatibility.  Arguments as
+ * dcrf_model_pairwise_apply_upper_minus_lower_bf. */
+dcrf_status dcrf_model_pairwise_apply_upper_minus_lower_dc(dcrf_model m, int k, int nonorm, float* out,
+                                                         const int32_t* ind);
 /* qp_inference_super_pixels_non_convex(init) (src/densecrf.cpp:340-442);
  * runs qp or, when cliques are set, qp_sp.  params/stats may be NULL. */
 dcrf_status dcrf_model_qp(dcrf_model m, const float* init, float* out,

@@ -167,6 +167,8 @@ def ref_lib():
         for fn in ("refm_energy_lp", "refm_lr_qp_value"):
             getattr(L, fn).restype = C.c_double
             getattr(L, fn).argtypes = [vp, _f32p]
+        L.refm_apply_bf.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
+        L.refm_apply_sorted.argtypes = [vp, C.c_int, C.c_int, C.c_int, _f32p, _i32p, vp]
         L.ref_last_error.restype = C.c_char_p
         _rlib = L
     return _rlib
@@ -488,6 +490,28 @@ class ReferenceModel(_Model):
             raise RuntimeError(self._lib.ref_last_error().decode())
         return out
 
+    def apply_bf(self, k, Q, nonorm=False):
+        """pairwise_[k] (or no_norm_pairwise_[k])->apply_bf(out, Q)."""
+        out = self._new()
+        self._lib.refm_apply_bf(self._h, k, int(nonorm), out, _c(Q, np.float32))
+        return out
+
+    def _sorted(self, kind, k, ind, Q, nonorm):
+        out = self._new()
+        q = None if Q is None else _c(Q, np.float32)
+        self._lib.refm_apply_sorted(self._h, k, int(nonorm), kind, out, _c(ind, np.int32),
+                                    None if q is None else q.ctypes.data_as(C.c_void_p))
+        return out
+
+    def apply_upper_minus_lower_bf(self, k, ind, nonorm=False):
+        return self._sorted(0, k, ind, None, nonorm)
+
+    def apply_upper_minus_lower_bf_ord(self, k, ind, Q, nonorm=False):
+        return self._sorted(1, k, ind, Q, nonorm)
+
+    def apply_upper_minus_lower_dc(self, k, ind, nonorm=False):
+        return self._sorted(2, k, ind, None, nonorm)
+
     def qp(self, init, fixed_iters=0):
         out = self._new()
         if fixed_iters <= 0:
@@ -601,3 +625,176 @@ class RestrictedOrd:
                     coef = np.float32(w) * alpha if upper else np.float32(-w) * alpha
                     out[ii] = out[ii] + vals[o, np.arange(L), c] * coef
         return out
+
+
+# ----------------------------------------------- exact and D&C filters ----
+
+def sqnorm_eigen(diff):
+    """``VectorXf::squaredNorm()`` in Eigen 3.2's SSE2 order (Redux.h,
+    LinearVectorizedTraversal from an aligned start; predux of
+    SSE/PacketMath.h) over the last axis of float32 ``diff``: squares in
+    float32; fewer than 4 summed left to right; else 4-lane packets (a second
+    accumulator from 8 on), reduced as (p0 + p2) + (p1 + p3), then the tail."""
+    s = (diff * diff).astype(np.float32)
+    d = s.shape[-1]
+    al = d & ~3
+    if al == 0:
+        r = s[..., 0]
+        for i in range(1, d):
+            r = (r + s[..., i]).astype(np.float32)
+        return r
+    p = s[..., 0:4]
+    if al > 4:
+        q = s[..., 4:8]
+        al2 = d & ~7
+        for idx in range(8, al2, 8):
+            p = (p + s[..., idx:idx + 4]).astype(np.float32)
+            q = (q + s[..., idx + 4:idx + 8]).astype(np.float32)
+        p = (p + q).astype(np.float32)
+        if al > al2:
+            p = (p + s[..., al2:al2 + 4]).astype(np.float32)
+    r = ((p[..., 0] + p[..., 2]).astype(np.float32) + (p[..., 1] + p[..., 3]).astype(np.float32)).astype(np.float32)
+    for i in range(al, d):
+        r = (r + s[..., i]).astype(np.float32)
+    return r
+
+
+def _kmat(fa, fb):
+    """exp(-|f_a - f_b|^2) in float64 for all pairs (rows of fa, rows of fb),
+    the norm in float32 as the reference forms it (src/pairwise.cpp:315)."""
+    diff = (fa[:, None, :] - fb[None, :, :]).astype(np.float32)
+    return np.exp(-sqnorm_eigen(diff).astype(np.float64))
+
+
+def compat_apply(raw, kind, params):
+    """LabelCompatibility::apply (src/labelcompatibility.cpp): Potts (kind 0,
+    params = w): -w v; Diagonal (1, L weights): w_l v; Matrix (2, the
+    symmetrised L x L, column-major): W v summed over m in order."""
+    raw = raw.astype(np.float32)
+    if kind == 0:
+        return (np.float32(-params) * raw).astype(np.float32)
+    if kind == 1:
+        return (np.asarray(params, np.float32)[None, :] * raw).astype(np.float32)
+    W = np.asarray(params, np.float32).reshape(raw.shape[1], raw.shape[1]).T  # W[l, m]
+    out = (W[None, :, 0] * raw[:, 0:1]).astype(np.float32)
+    for m in range(1, raw.shape[1]):
+        out = (out + (W[None, :, m] * raw[:, m:m + 1]).astype(np.float32)).astype(np.float32)
+    return out
+
+
+def bf_apply(feat, Q):
+    """``apply_bf`` before the compatibility (src/pairwise.cpp:368-380):
+    out(l, c) = sum_b k(c, b) Q(l, b), each product in double added to the
+    float out in b order."""
+    feat = np.asarray(feat, np.float32)
+    Q = np.asarray(Q, np.float32)
+    K = _kmat(feat, feat)  # [c, b]
+    acc = np.zeros(Q.shape, np.float32)
+    for b in range(feat.shape[0]):
+        acc = (acc.astype(np.float64) + K[:, b:b + 1] * Q[b][None, :].astype(np.float64)).astype(np.float32)
+    return acc
+
+
+def bf_sorted(feat, ind, Q=None):
+    """``apply_upper_minus_lower_bf`` (Q None, src/pairwise.cpp:301-332) or
+    ``apply_upper_minus_lower_bf_ord`` (:333-367) before the compatibility;
+    ind [N][L]; out in sorted positions."""
+    feat = np.asarray(feat, np.float32)
+    ind = np.asarray(ind)
+    N, L = ind.shape
+    out = np.zeros((N, L), np.float32)
+    for l in range(L):
+        sf = feat[ind[:, l]]
+        K = _kmat(sf, sf)
+        acc = np.zeros(N, np.float32)
+        if Q is None:
+            up = np.triu(np.ones((N, N), bool), 1)  # b > c
+            lo = up.T
+        else:
+            qs = np.asarray(Q, np.float32)[ind[:, l], l]
+            up = ~(qs[None, :] > qs[:, None])
+            lo = ~(qs[None, :] < qs[:, None])
+        for sign, mask in ((1.0, up), (-1.0, lo)):
+            for b in range(N):
+                m = mask[:, b]
+                acc[m] = (acc[m].astype(np.float64) + sign * K[m, b]).astype(np.float32)
+        out[:, l] = acc
+    return out
+
+
+def _dc_cross(out, ex, lo, ml, mh, hi):
+    """``seqCompute_upper_minus_lower_dc`` (src/permutohedral.cpp:902-997) on
+    one lattice's exported tables (offset, bary [N][d+1], nbr [d+1][M][2])."""
+    off, bary, nbr, d = ex["offset"], ex["bary"], ex["nbr"], ex["d"]
+    d1 = d + 1
+    act = []
+    seen = set()
+    for rng in (range(mh, hi), range(lo, ml)):
+        for i in rng:
+            for j in range(d1):
+                o = int(off[i, j])
+                if o not in seen:
+                    seen.add(o)
+                    act.append(o)
+    alpha = np.float32(1.0) / np.float32(1.0 + 2.0 ** -d)
+    half = np.float32(0.5)
+    for splat_rng, slice_rng, sign in ((range(mh, hi), range(lo, ml), 1), (range(lo, ml), range(mh, hi), -1)):
+        vals = {}
+        for i in splat_rng:
+            for j in range(d1):
+                o = int(off[i, j])
+                vals[o] = np.float32(vals.get(o, np.float32(0.0)) + bary[i, j])
+        for j in range(d1):
+            new = {}
+            for v in act:
+                n1, n2 = int(nbr[j, v, 0]), int(nbr[j, v, 1])
+                s = np.float32(vals.get(n1, np.float32(0.0)) + vals.get(n2, np.float32(0.0)))
+                new[v] = np.float32(vals.get(v, np.float32(0.0)) + half * s)
+            vals = new
+        for i in slice_rng:
+            for j in range(d1):
+                t = np.float32(np.float32(bary[i, j] * vals[int(off[i, j])]) * alpha)
+                out[i] = np.float32(out[i] + t) if sign > 0 else np.float32(out[i] - t)
+
+
+def _dc_slice(out, sf, ex, lo, hi):
+    """``apply_upper_minus_lower_sorted_slice`` (src/pairwise.cpp:262-300)."""
+    size = hi - lo
+    if size <= 30:
+        alpha = 1.0 / 0.6
+        K = _kmat(sf[lo:hi], sf[lo:hi])
+        for c in range(lo, hi):
+            for b in range(lo, c):
+                out[c] = np.float32(np.float64(out[c]) - K[c - lo, b - lo] * alpha)
+        for c in range(lo, hi):
+            for b in range(c + 1, hi):
+                out[c] = np.float32(np.float64(out[c]) + K[c - lo, b - lo] * alpha)
+        return
+    ml = lo + size // 2
+    mh = ml if size % 2 == 0 else ml + 1
+    _dc_slice(out, sf, ex, lo, mh)
+    _dc_slice(out, sf, ex, ml, hi)
+    _dc_cross(out, ex, lo, ml, mh, hi)
+
+
+def dc_sorted(feat, ind, lattice_cls=None):
+    """``apply_upper_minus_lower_dc`` before the compatibility
+    (src/pairwise.cpp:241-260): per label a lattice of the sorted features
+    (``lattice_cls``: :class:`OracleLattice` by default) and the recursion."""
+    feat = np.asarray(feat, np.float32)
+    ind = np.asarray(ind)
+    N, L = ind.shape
+    d = feat.shape[1]
+    out = np.zeros((N, L), np.float32)
+    lat_cls = lattice_cls or OracleLattice
+    for l in range(L):
+        sf = np.ascontiguousarray(feat[ind[:, l]])
+        lat = lat_cls(sf)
+        e = lat.export()
+        M = lat.M
+        ex = {"offset": np.asarray(e["offset"]).reshape(N, d + 1), "bary": np.asarray(e["bary"]).reshape(N, d + 1),
+              "nbr": np.asarray(e["nbr"]).reshape(d + 1, M, 2), "d": d}
+        col = np.zeros(N, np.float32)
+        _dc_slice(col, sf, ex, 0, N)
+        out[:, l] = col
+    return out

@@ -319,6 +319,26 @@ void refm_apply_ord_restricted(void* h, int k, float* rout, const float* rQ, con
     m->pw(k)->apply_upper_minus_lower_ord_restricted(O, RQ, idx, QQ, store != 0);
     if (nP) std::memcpy(rout, O.data(), sizeof(float) * (size_t)m->L() * nP);
 }
+// PairwisePotential's exact and divide-and-conquer filters
+// (src/pairwise.cpp:241-380) on pairwise_[k] or no_norm_pairwise_[k]; ind
+// [N][L] (MatrixXi L x N), out [N][L].
+void refm_apply_bf(void* h, int k, int nonorm, float* out, const float* Q) {
+    RefModel* m = (RefModel*)h;
+    MatrixXf I = Map<const MatrixXf>(Q, m->L(), m->N());
+    MatrixXf O;
+    (nonorm ? m->pw_nonorm(k) : m->pw(k))->apply_bf(O, I);
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+}
+void refm_apply_sorted(void* h, int k, int nonorm, int kind, float* out, const int* ind, const float* Q) {
+    RefModel* m = (RefModel*)h;
+    MatrixXi I = Map<const MatrixXi>(ind, m->L(), m->N());
+    MatrixXf O(m->L(), m->N());
+    PairwisePotential* p = nonorm ? m->pw_nonorm(k) : m->pw(k);
+    if (kind == 0) p->apply_upper_minus_lower_bf(O, I);
+    else if (kind == 1) p->apply_upper_minus_lower_bf_ord(O, I, Map<const MatrixXf>(Q, m->L(), m->N()));
+    else p->apply_upper_minus_lower_dc(O, I);
+    std::memcpy(out, O.data(), sizeof(float) * O.size());
+}
 int refm_apply_ord(void* h, int k, float* out, const float* in) {
     RefModel* m = (RefModel*)h;
     MatrixXf I = Map<const MatrixXf>(in, m->L(), m->N());

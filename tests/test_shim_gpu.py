@@ -65,6 +65,8 @@ def test_cpp_shim_matches_c_abi(tmp_path):
     pw = DenseCRF2D(W * H, 1, L)
     pw.addPairwiseEnergy(F, 3.0)
     assert np.array_equal(load("pw"), pw.pairwise_apply(0, Q))
+    ind = np.argsort(-Q, axis=0, kind="stable").astype(np.int32)
+    assert np.array_equal(load("dc"), pw.pairwise_apply_upper_minus_lower_dc(0, ind))
 
     assert lines["range_error"] == "Value out of bounds"
     assert lines["kernel_error"] == "ok"
