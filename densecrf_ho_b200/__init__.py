@@ -525,11 +525,13 @@ __all__.append("DenseCRF2DBatch")
 
 
 def _pairwise_kernel_gradient(self, k, b, Q):
-    """``pairwise_[k]->kernelGradient(b, Q)``: gradient of the term's diagonal
-    kernel feature scales (d floats)."""
+    """``pairwise_[k]->kernelGradient(b, Q)``: gradient of the term's kernel
+    parameters (DIAG_KERNEL d feature scales, FULL_KERNEL the d x d matrix
+    column-major, CONST_KERNEL none)."""
     bb, qq = self._mat(b), self._mat(Q)
-    out = np.zeros(16, np.float32)
     d = C.c_int()
+    check(lib().dcrf_model_pairwise_kernel_gradient(self._h, int(k), None, None, None, C.byref(d)))
+    out = np.zeros(max(d.value, 1), np.float32)
     check(lib().dcrf_model_pairwise_kernel_gradient(self._h, int(k), bb.ctypes.data_as(C.c_void_p),
                                                     qq.ctypes.data_as(C.c_void_p), out.ctypes.data_as(C.c_void_p),
                                                     C.byref(d)))

@@ -888,14 +888,16 @@ dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model h, int k, const float
     return guard([&] {
         auto& m = M(h);
         check_term(m, k);
+        const auto& t = *m.terms[k];
+        const int count = t.ktype == dcrf::kConstKernel ? 0 : t.ktype == dcrf::kDiagKernel ? t.d : t.d * t.d;
+        if (d) *d = count;
+        if (!grad) return;  // query of the count
         need(b, "b");
         need(Q, "Q");
-        need(grad, "grad");
         const size_t n = (size_t)m.N * m.L;
         const float* db = upload(h->io0, b, n, m.stream);
         const float* dq = upload(h->io1, Q, n, m.stream);
-        const int n_out = m.kernel_gradient(k, db, dq, grad);
-        if (d) *d = n_out;
+        m.kernel_gradient(k, db, dq, grad);
     });
 }
 

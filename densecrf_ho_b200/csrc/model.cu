@@ -100,24 +100,39 @@ __global__ void sym_grad_input_kernel(long n, int L, const float* __restrict__ a
     X[t] = fmul(fmul(fadd(fmul(a[t], fb[t]), fmul(fa[t], b[t])), 0.5f), n3);
 }
 
-// Per feature dimension j: sum_i f(i, j) * (-r(i, j) + g(i, j)), in FP64
-// (block partials, then a fixed-order finish); (f o fg).rowwise().sum().
-__global__ void diag_grad_partial_kernel(int N, int d, const float* __restrict__ f, const float* __restrict__ r,
-                                         const float* __restrict__ g, double* __restrict__ part) {
+// X = (x o y) n^2 per column (featureGradient, NORMALIZE_AFTER with x = a,
+// y = K(b); NORMALIZE_BEFORE with x = K^T(a), y = b).
+__global__ void one_sided_grad_input_kernel(long n, int L, const float* __restrict__ x, const float* __restrict__ y,
+                                            const float* __restrict__ nrm, float* __restrict__ X) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float ni = nrm[t / L];
+    X[t] = fmul(fmul(x[t], y[t]), fmul(ni, ni));
+}
+
+// DenseKernel::gradient's sums over pixels in FP64 (block partials, then a
+// fixed-order finish), fg = -r + g (fg = g without r):
+// DIAG (full = 0): output j = sum_i f(i, j) fg(i, j);
+// FULL (full = 1): output j + k d = sum_i fg(i, j) f(i, k)  (fg f^T).
+__global__ void feature_grad_partial_kernel(int N, int d, int full, const float* __restrict__ f,
+                                            const float* __restrict__ r, const float* __restrict__ g,
+                                            double* __restrict__ part) {
     __shared__ double sm[256];
-    const int j = blockIdx.y;
+    const int o = blockIdx.y;
+    const int j = full ? o % d : o, kf = full ? o / d : o;
     double acc = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        const long e = (long)i * d + j;
-        acc += (double)fmul(f[e], fadd(-r[e], g[e]));
+        const long e = (long)i * d;
+        const float fg = r ? fadd(-r[e + j], g[e + j]) : g[e + j];
+        acc += (double)fmul(f[e + kf], fg);
     }
     sm[threadIdx.x] = acc;
     __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o) sm[threadIdx.x] += sm[threadIdx.x + o];
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
         __syncthreads();
     }
-    if (threadIdx.x == 0) part[(long)j * gridDim.x + blockIdx.x] = sm[0];
+    if (threadIdx.x == 0) part[(long)o * gridDim.x + blockIdx.x] = sm[0];
 }
 
 // -(b o x).sum() in FP64 partials (PottsCompatibility::gradient).
@@ -329,17 +344,20 @@ void Model::set_kernel_parameters(int k, const float* p) {
     sync();
 }
 
-// pairwise_[k]->kernelGradient(b, Q) for a diagonal kernel with symmetric
-// normalisation: lbl = -w Q (PottsCompatibility::apply), then
-// featureGradient(b, lbl) = -G(X, 1) + G(b n, lbl n) with G = the lattice's
-// gradient, fa = K^T(b n), fb = K(lbl n), X = 0.5 (b o fb + fa o lbl) n^3;
-// the result is sum_i f(i, j) fg(i, j) per dimension j (FP64 sum, rounded to
-// float -- the reference sums in float).
+// pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 95-122,
+// 170-181): lbl = compatibility(Q), then DenseKernel::featureGradient(a = b,
+// lbl) with G = the lattice's gradient and n the term's norm:
+//   NO_NORMALIZATION  fg = G(a, lbl)
+//   SYMMETRIC         fg = -G(X, 1) + G(a n, lbl n), X = 0.5 (a o K(lbl n) + K^T(a n) o lbl) n^3
+//   AFTER             fg = -G(X, 1) + G(a n, lbl),   X = (a o K(lbl)) n^2
+//   BEFORE            fg = -G(X, 1) + G(a, lbl n),   X = (K^T(a) o lbl) n^2
+// and DenseKernel::gradient: DIAG_KERNEL sum_i f(i, j) fg(i, j) per
+// dimension j, FULL_KERNEL fg f^T (d x d, column-major), both over the
+// features the term was added with; FP64 sums over pixels, rounded to float
+// (the reference sums in float).
 int Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
     Term& t = *terms[k];
     if (t.ktype == kConstKernel) return 0;  // DenseKernel::gradient: no parameters
-    require(t.ktype == kDiagKernel && t.ntype == kNormSymmetric, DCRF_E_STATE,
-            "kernel gradient: DIAG_KERNEL with NORMALIZE_SYMMETRIC only");
     Lattice& lat = *t.lat;
     const long NL = (long)N * L;
     const int d = t.d, g = ceil_div(NL, 256);
@@ -355,28 +373,50 @@ int Model::kernel_gradient(int k, const float* b, const float* Q, float* out) {
     else
         launch(matrix_compat_kernel, g, 256, 0, stream, NL, L, (const float*)t.cw.get(), Q, (const float*)nullptr,
                1.0f, 0, lbl);
-    launch(scale_cols_kernel, g, 256, 0, stream, NL, L, b, nrm, 1.0f, bn);
-    launch(scale_cols_kernel, g, 256, 0, stream, NL, L, lbl, nrm, 1.0f, ln);
     SliceEpilogue plain;
-    lat.compute(fa, bn, L, true, plain);
-    lat.compute(fb, ln, L, false, plain);
-    launch(sym_grad_input_kernel, g, 256, 0, stream, NL, L, b, fb, fa, lbl, nrm, X);
-    launch(fill_ones_kernel, g, 256, 0, stream, NL, ones);
-    lat.gradient(r, X, ones, L);
-    lat.gradient(gg, bn, ln, L);
-    const int nb = 64;
-    double* part = partials.get();
-    launch(diag_grad_partial_kernel, dim3(nb, d), 256, 0, stream, N, d, t.feat.get(), r, gg, part);
+    const bool has_r = t.ntype != kNoNorm;
+    if (t.ntype == kNoNorm) {
+        lat.gradient(gg, b, lbl, L);
+    } else {
+        if (t.ntype == kNormSymmetric) {
+            launch(scale_cols_kernel, g, 256, 0, stream, NL, L, b, nrm, 1.0f, bn);
+            launch(scale_cols_kernel, g, 256, 0, stream, NL, L, lbl, nrm, 1.0f, ln);
+            lat.compute(fa, bn, L, true, plain);
+            lat.compute(fb, ln, L, false, plain);
+            launch(sym_grad_input_kernel, g, 256, 0, stream, NL, L, b, fb, fa, lbl, nrm, X);
+        } else if (t.ntype == kNormAfter) {
+            lat.compute(fb, lbl, L, false, plain);
+            launch(one_sided_grad_input_kernel, g, 256, 0, stream, NL, L, b, (const float*)fb, nrm, X);
+        } else {  // kNormBefore
+            lat.compute(fa, b, L, true, plain);
+            launch(one_sided_grad_input_kernel, g, 256, 0, stream, NL, L, (const float*)fa, lbl, nrm, X);
+        }
+        launch(fill_ones_kernel, g, 256, 0, stream, NL, ones);
+        lat.gradient(r, X, ones, L);
+        if (t.ntype == kNormSymmetric) {
+            lat.gradient(gg, bn, ln, L);
+        } else if (t.ntype == kNormAfter) {
+            launch(scale_cols_kernel, g, 256, 0, stream, NL, L, b, nrm, 1.0f, bn);
+            lat.gradient(gg, bn, lbl, L);
+        } else {
+            launch(scale_cols_kernel, g, 256, 0, stream, NL, L, lbl, nrm, 1.0f, ln);
+            lat.gradient(gg, b, ln, L);
+        }
+    }
+    const int nb = 64, nout = t.ktype == kDiagKernel ? d : d * d;
+    double* part = partials.ensure((size_t)nb * nout);
+    launch(feature_grad_partial_kernel, dim3(nb, nout), 256, 0, stream, N, d, (int)(t.ktype == kFullKernel),
+           (const float*)t.feat.get(), has_r ? (const float*)r : nullptr, (const float*)gg, part);
     DCRF_LAUNCH_CHECK();
-    std::vector<double> h((size_t)nb * d);
+    std::vector<double> h((size_t)nb * nout);
     DCRF_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, stream));
     sync();
-    for (int j = 0; j < d; j++) {
+    for (int j = 0; j < nout; j++) {
         double s = 0.0;
         for (int i = 0; i < nb; i++) s += h[(size_t)j * nb + i];
         out[j] = (float)s;
     }
-    return d;
+    return nout;
 }
 
 // pairwise_[k]->gradient(b, Q) (src/pairwise.cpp:390-395): the

@@ -315,11 +315,12 @@ dcrf_status dcrf_model_pairwise_energy(dcrf_model m, const int16_t* labels, int 
 /* max_rounding(Q) (src/densecrf.cpp:832-840): out [N][L], a one-hot row at
  * each pixel's first maximum. */
 dcrf_status dcrf_model_max_rounding(dcrf_model m, const float* Q, float* out);
-/* pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 90-122,
- * 170-181): the gradient of the diagonal kernel's feature scales, d floats
- * (d = 2 Gaussian, 5 bilateral; the count is returned when not NULL, 0 for
- * CONST_KERNEL; DIAG_KERNEL with NORMALIZE_SYMMETRIC, else DCRF_E_STATE;
- * grad holds at least 16 floats), and pairwise_[k]->gradient(b, Q) (:390-395): the
+/* pairwise_[k]->kernelGradient(b, Q) (src/pairwise.cpp:402-407, 95-122,
+ * 170-181): the gradient of the kernel's parameters for every
+ * NormalizationType -- DIAG_KERNEL d floats (the feature scales; d = 2
+ * Gaussian, 5 bilateral), FULL_KERNEL d x d (column-major), CONST_KERNEL
+ * none; the count is returned in *d when d is not NULL, and grad = NULL only
+ * queries it -- and pairwise_[k]->gradient(b, Q) (:390-395): the
  * compatibility's gradient, as many floats as its parameters.  b, Q [N][L]. */
 dcrf_status dcrf_model_pairwise_kernel_gradient(dcrf_model m, int k, const float* b, const float* Q,
                                                 float* grad, int* d);

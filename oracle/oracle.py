@@ -330,8 +330,9 @@ class _Model:
         return self._fn("lr_qp_value")(self._h, _c(Q, np.float32))
 
     def kernel_gradient(self, k, b, Q):
-        """pairwise_[k]->kernelGradient(b, Q): d floats (reference model only)."""
-        out = np.zeros(16, np.float32)
+        """pairwise_[k]->kernelGradient(b, Q): d (DIAG_KERNEL) or d x d
+        (FULL_KERNEL) floats (reference model only)."""
+        out = np.zeros(256, np.float32)
         n = self._lib.refm_kernel_gradient(self._h, k, _c(b, np.float32), _c(Q, np.float32), out)
         return out[:n]
 

@@ -9,7 +9,10 @@ bilateral model:
 * "kparam": the default model after setKernelParameters on the bilateral
   term (diagonal scales): the term's apply on the rebuilt lattice, the twin's
   apply (the original features), the energies, a QP and kernelGradient;
-* "const": a CONST_KERNEL term (no kernel parameters).
+* "const": a CONST_KERNEL term (no kernel parameters);
+* "kg_<ktype><ntype>": kernelGradient of the Gaussian term as DIAG_KERNEL
+  (ktype 1, scales KDIAG set) or FULL_KERNEL (ktype 2, matrix KFULL set) for
+  each NormalizationType (0 none, 1 before, 2 after, 3 symmetric).
 
 Run: python tests/golden/make_kernel_golden.py
 """
@@ -26,6 +29,8 @@ from oracle import oracle as O  # noqa: E402
 
 W, H, L, SEED = 24, 18, 5, 9
 KPARAM = np.array([1.3, 0.8, 1.1, 0.9, 1.2], np.float32)
+KDIAG = np.array([1.3, 0.7], np.float32)
+KFULL = np.array([1.2, 0.3, -0.2, 0.9], np.float32)  # 2 x 2, column-major
 
 
 def model(img, ktype=1, ntype=3):
@@ -59,7 +64,7 @@ def main():
         sys.exit("oracle/_ref/libdcrf_ref.so missing: run `make -C oracle ref` first")
     img = synth.make_image(W, H, L, SEED)
     b = np.random.default_rng(SEED).standard_normal((W * H, L)).astype(np.float32)
-    out = dict(W=W, H=H, L=L, seed=SEED, b=b, kparam=KPARAM)
+    out = dict(W=W, H=H, L=L, seed=SEED, b=b, kparam=KPARAM, kg_kdiag=KDIAG, kg_kfull=KFULL)
     for t in (0, 1, 2):
         m = model(img, 1, t)
         Q = m.unary_init()
@@ -77,6 +82,13 @@ def main():
     m = model(img, 0, 3)
     out["const_kparams0"] = m.kernel_parameters(0)
     out["const_kgrad0"] = m.kernel_gradient(0, b, m.unary_init())
+    for kt, kp in ((1, KDIAG), (2, KFULL)):
+        for t in (0, 1, 2, 3):
+            m = model(img, kt, t)
+            m.set_kernel_parameters(0, kp)
+            Q = m.unary_init()
+            out[f"kg_{kt}{t}_unary_init"] = Q
+            out[f"kg_{kt}{t}"] = m.kernel_gradient(0, b, Q)
     np.savez_compressed(os.path.join(HERE, f"kernel_{W}x{H}_L{L}.npz"), **out)
     print(sorted(k for k in out if "kgrad" in k or "kparams" in k), out["kparam_kgrad1"])
 

@@ -328,7 +328,8 @@ def test_kernel_and_normalization_types_vs_reference():
     diagonal kernel rebuilt on scaled features, its unnormalised twin on the
     original ones) and CONST_KERNEL, against the reference's own values
     (tests/golden/make_kernel_golden.py): filters, energies and QP bit for
-    bit, the kernel gradient to 1e-4 of its largest component."""
+    bit, the kernel gradient (DIAG and FULL kernels, every normalisation) to
+    1e-4 of its largest component."""
     g = golden("kernel_24x18_L5.npz")
     W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
     img = synth.make_image(W, H, L, int(g["seed"]))
@@ -374,9 +375,17 @@ def test_kernel_and_normalization_types_vs_reference():
     assert m.pairwise_kernel_parameters(0).size == g["const_kparams0"].size == 0
     assert m.pairwise_kernel_gradient(0, g["b"], Q).size == g["const_kgrad0"].size == 0
     with pytest.raises(DCRFError):
-        model(1, 2).pairwise_kernel_gradient(0, g["b"], Q)   # DIAG + NORMALIZE_AFTER: not built
-    with pytest.raises(DCRFError):
         m.setKernel(0, 3, 3)
+
+    # kernelGradient for DIAG_KERNEL (scales set) and FULL_KERNEL (a 2 x 2
+    # matrix set) under every NormalizationType
+    for kt, kp in ((1, g["kg_kdiag"]), (2, g["kg_kfull"])):
+        for t in (0, 1, 2, 3):
+            m = model(kt, t)
+            m.pairwise_set_kernel_parameters(0, kp)
+            kg, ref = m.pairwise_kernel_gradient(0, g["b"], g[f"kg_{kt}{t}_unary_init"]), g[f"kg_{kt}{t}"]
+            assert kg.shape == ref.shape, (kt, t)
+            assert np.abs(kg - ref).max() <= 1e-4 * np.abs(ref).max(), (kt, t, kg, ref)
 
 
 def test_per_pixel_energies_and_rounding_vs_reference():
