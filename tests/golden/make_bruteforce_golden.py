@@ -11,7 +11,10 @@ from its sources).
 * "diag": the same terms with DiagonalCompatibility, for the compatibility
   after the filter and the Potts twin (nonorm).
 * "feat8": one term on random 8-dimensional features (the two-packet order
-  of the squared distance), 12x10, 2 labels.
+  of the squared distance), 12x10, 2 labels;
+* "feat3" on 5x4 (N = 20: the divide-and-conquer filter is one block of
+  pairs) and on 31x1 (N = 31: one odd halving into two blocks sharing the
+  middle position).
 
 Run: python tests/golden/make_bruteforce_golden.py
 """
@@ -82,7 +85,9 @@ def main():
         sys.exit("oracle/_ref/libdcrf_ref.so missing: run `make -C oracle ref` first")
     cases = {"potts_23x17_L3": image_case("potts", 23, 17, 3),
              "diag_23x17_L3": image_case("diag", 23, 17, 3),
-             "feat8_12x10_L2": feature_case(12, 10, 2, 8)}
+             "feat8_12x10_L2": feature_case(12, 10, 2, 8),
+             "feat3_5x4_L2": feature_case(5, 4, 2, 3),
+             "feat3_31x1_L3": feature_case(31, 1, 3, 3)}
     for name, out in cases.items():
         np.savez_compressed(os.path.join(HERE, f"bruteforce_{name}.npz"), **out)
         print(name, {k: float(np.abs(v).max()) for k, v in out.items() if k[:2] in ("bf", "dc")})
