@@ -22,6 +22,7 @@
 #include <memory>
 #include <mutex>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 #include "model.cuh"
@@ -43,7 +44,11 @@ constexpr int kDcMaxDepth = 64;
 // pairs of packets per step, the two added lane-wise, then one more packet if
 // a whole one is left), the packet reduced as (p0 + p2) + (p1 + p3)
 // (predux, SSE/PacketMath.h), then the remaining squares left to right.
-__device__ __forceinline__ float sqdist(const float* a, const float* b, int d) {
+// D > 0 fixes the dimension at compile time (the predicates below fold
+// away); D = 0 takes it from d.
+template <int D>
+__device__ __forceinline__ float sqdist(const float* a, const float* b, int d_rt) {
+    const int d = D > 0 ? D : d_rt;
     float s[kMaxD];
 #pragma unroll
     for (int i = 0; i < kMaxD; i++) {
@@ -93,8 +98,9 @@ __device__ __forceinline__ float sqdist(const float* a, const float* b, int d) {
 
 // exp(-|f_a - f_b|^2) as the reference forms it: the float norm negated,
 // then the double exp.
+template <int D>
 __device__ __forceinline__ double kval(const float* a, const float* b, int d) {
-    return exp((double)(-sqdist(a, b, d)));
+    return exp((double)(-sqdist<D>(a, b, d)));
 }
 
 // out = (float)((double)out + t)
@@ -103,8 +109,10 @@ __device__ __forceinline__ float acc_sub(float out, double t) { return __double2
 
 // apply_bf (src/pairwise.cpp:368-380): thread per (pixel c, 8 labels); the
 // pixels b in order, staged through shared memory a tile at a time.
-__global__ void __launch_bounds__(kBfTile) bf_apply_kernel(int N, int L, int d, const float* __restrict__ feat,
+template <int D>
+__global__ void __launch_bounds__(kBfTile) bf_apply_kernel(int N, int L, int d_rt, const float* __restrict__ feat,
                                                            const float* __restrict__ Q, float* __restrict__ out) {
+    const int d = D > 0 ? D : d_rt;
     __shared__ float sf[kBfTile * kMaxD];
     __shared__ float sq[kBfTile * kBfLabels];
     const int c = blockIdx.x * kBfTile + threadIdx.x;
@@ -127,7 +135,7 @@ __global__ void __launch_bounds__(kBfTile) bf_apply_kernel(int N, int L, int d, 
         __syncthreads();
         if (c < N)
             for (int bi = 0; bi < nb; bi++) {
-                const double k = kval(fc, sf + bi * d, d);
+                const double k = kval<D>(fc, sf + bi * d, d);
 #pragma unroll
                 for (int l = 0; l < kBfLabels; l++)
                     if (l < nl) acc[l] = acc_add(acc[l], __dmul_rn(k, (double)sq[bi * kBfLabels + l]));
@@ -143,10 +151,11 @@ __global__ void __launch_bounds__(kBfTile) bf_apply_kernel(int N, int L, int d, 
 // then - k over b < c.  ORD: + k over every b with Q(l, ind(l, b)) <=
 // Q(l, ind(l, c)), then - k over every b with Q(l, ind(l, b)) >= that.
 // Each sweep walks the tiles in order, so every thread meets its b in order.
-template <bool ORD>
-__global__ void __launch_bounds__(kBfTile) bf_sorted_kernel(int N, int L, int d, const float* __restrict__ feat,
+template <bool ORD, int D>
+__global__ void __launch_bounds__(kBfTile) bf_sorted_kernel(int N, int L, int d_rt, const float* __restrict__ feat,
                                                             const int* __restrict__ ind, const float* __restrict__ Q,
                                                             float* __restrict__ out) {
+    const int d = D > 0 ? D : d_rt;
     __shared__ float sf[kBfTile * kMaxD];
     __shared__ float sqv[kBfTile];
     const int c = blockIdx.x * kBfTile + threadIdx.x;
@@ -185,7 +194,7 @@ __global__ void __launch_bounds__(kBfTile) bf_sorted_kernel(int N, int L, int d,
                 if (ORD) take = sweep == 0 ? !(sqv[bi] > qc) : !(sqv[bi] < qc);
                 else take = sweep == 0 ? b > c : b < c;
                 if (!take) continue;
-                const double k = kval(fc, sf + bi * d, d);
+                const double k = kval<D>(fc, sf + bi * d, d);
                 acc = sweep == 0 ? acc_add(acc, k) : acc_sub(acc, k);
             }
         }
@@ -396,7 +405,9 @@ __global__ void dc_blur_kernel(int R, const int2* __restrict__ rnb, const float2
 }
 
 // The contributions of one node to sorted position c.
-__device__ __forceinline__ float dc_leaf(float acc, int c, const DcNode& x, int d, const float* __restrict__ sfeat) {
+template <int D>
+__device__ __forceinline__ float dc_leaf(float acc, int c, const DcNode& x, int d_rt, const float* __restrict__ sfeat) {
+    const int d = D > 0 ? D : d_rt;
     const double alpha = 1.0 / 0.6;  // src/pairwise.cpp:268
     float fc[kMaxD];
 #pragma unroll
@@ -407,7 +418,7 @@ __device__ __forceinline__ float dc_leaf(float acc, int c, const DcNode& x, int 
         if (b == c) continue;
 #pragma unroll
         for (int i = 0; i < kMaxD; i++) fb[i] = i < d ? sfeat[(long)b * d + i] : 0.0f;
-        const double t = __dmul_rn(kval(fc, fb, d), alpha);
+        const double t = __dmul_rn(kval<D>(fc, fb, d), alpha);
         acc = b < c ? acc_sub(acc, t) : acc_add(acc, t);
     }
     return acc;
@@ -449,6 +460,7 @@ __device__ __forceinline__ int dc_descend(int from, int c, const DcNode* __restr
 // node P (in both halves), the left half's chain (leaf up to P's left child)
 // runs first, then the right half's, then P (which adds nothing to c) and
 // its ancestors.
+template <int D>
 __global__ void dc_walk_kernel(int N, int L, int l, int d, const DcNode* __restrict__ nodes,
                                const float* __restrict__ sfeat, const float* __restrict__ bary,
                                const int* __restrict__ run_of_item, const float2* __restrict__ vals, float alpha,
@@ -471,11 +483,11 @@ __global__ void dc_walk_kernel(int N, int L, int l, int d, const DcNode* __restr
     }
     float acc = 0.0f;
     if (fork < 0) {
-        acc = dc_leaf(acc, c, nodes[x], d, sfeat);
+        acc = dc_leaf<D>(acc, c, nodes[x], d, sfeat);
     } else {
         for (int side = 0; side < 2; side++) {
             const int ns = dc_descend(side == 0 ? nodes[fork].left : nodes[fork].right, c, nodes, sub);
-            acc = dc_leaf(acc, c, nodes[sub[ns]], d, sfeat);
+            acc = dc_leaf<D>(acc, c, nodes[sub[ns]], d, sfeat);
             for (int k = ns - 1; k >= 0; k--) acc = dc_cross(acc, c, nodes[sub[k]], d1, bary, run_of_item, vals, alpha);
         }
     }
@@ -483,13 +495,28 @@ __global__ void dc_walk_kernel(int N, int L, int l, int d, const DcNode* __restr
     out[(long)c * L + l] = acc;
 }
 
+// Calls f with std::integral_constant<int, D>: D = d for the feature
+// dimensions of the Gaussian (2), bilateral (5) and three-dimensional
+// features, 0 (runtime d) otherwise.
+template <typename F>
+void with_dim(int d, F&& f) {
+    switch (d) {
+        case 2: f(std::integral_constant<int, 2>{}); break;
+        case 3: f(std::integral_constant<int, 3>{}); break;
+        case 5: f(std::integral_constant<int, 5>{}); break;
+        default: f(std::integral_constant<int, 0>{}); break;
+    }
+}
+
 }  // namespace
 
 void Model::apply_bf(int k, bool nonorm, float* out, const float* Q) {
     Term& t = *terms.at(k);
     float* raw = buf(8);
-    launch(bf_apply_kernel, dim3(ceil_div(N, kBfTile), ceil_div(L, kBfLabels)), kBfTile, 0, stream, N, L, t.d,
-           (const float*)t.feat.get(), Q, raw);
+    with_dim(t.d, [&](auto dc) {
+        launch(bf_apply_kernel<decltype(dc)::value>, dim3(ceil_div(N, kBfTile), ceil_div(L, kBfLabels)), kBfTile, 0,
+               stream, N, L, t.d, (const float*)t.feat.get(), Q, raw);
+    });
     DCRF_LAUNCH_CHECK();
     apply_compat(k, nonorm, out, raw);
 }
@@ -498,11 +525,15 @@ void Model::apply_upper_minus_lower_bf(int k, bool nonorm, float* out, const int
     Term& t = *terms.at(k);
     float* raw = buf(8);
     const dim3 grid(ceil_div(N, kBfTile), L);
-    if (Q)
-        launch(bf_sorted_kernel<true>, grid, kBfTile, 0, stream, N, L, t.d, (const float*)t.feat.get(), ind, Q, raw);
-    else
-        launch(bf_sorted_kernel<false>, grid, kBfTile, 0, stream, N, L, t.d, (const float*)t.feat.get(), ind,
-               (const float*)nullptr, raw);
+    with_dim(t.d, [&](auto dc) {
+        constexpr int D = decltype(dc)::value;
+        if (Q)
+            launch(bf_sorted_kernel<true, D>, grid, kBfTile, 0, stream, N, L, t.d, (const float*)t.feat.get(), ind, Q,
+                   raw);
+        else
+            launch(bf_sorted_kernel<false, D>, grid, kBfTile, 0, stream, N, L, t.d, (const float*)t.feat.get(), ind,
+                   (const float*)nullptr, raw);
+    });
     DCRF_LAUNCH_CHECK();
     apply_compat(k, nonorm, out, raw);
 }
@@ -608,8 +639,10 @@ void dc_label(DcWorker& w, const DcPlan& p, int l) {
         }
         vals = a;
     }
-    launch(dc_walk_kernel, ceil_div(N, 128), 128, 0, st, N, p.L, l, d, p.nodes, (const float*)sf,
-           (const float*)w.lat.bary.get(), (const int*)roi, vals, p.alpha, p.raw);
+    with_dim(d, [&](auto dc) {
+        launch(dc_walk_kernel<decltype(dc)::value>, ceil_div(N, 128), 128, 0, st, N, p.L, l, d, p.nodes,
+               (const float*)sf, (const float*)w.lat.bary.get(), (const int*)roi, vals, p.alpha, p.raw);
+    });
     DCRF_LAUNCH_CHECK();
     // the next label rebuilds the lattice and reuses the buffers: finish this one
     DCRF_CUDA(cudaStreamSynchronize(st));
