@@ -33,7 +33,10 @@ namespace {
 
 constexpr int kMaxD = 16;   // feature dimensions (as the lattice)
 constexpr int kBfTile = 128;  // pixels b per shared-memory tile
-constexpr int kBfLabels = 8;  // labels per thread in apply_bf
+constexpr int kBfLabels = 8;  // labels per thread in apply_bf (one exp serves them all)
+// apply_bf's grid below this many threads has one label per thread instead:
+// on small images filling the SMs matters more than sharing the exp
+constexpr long kBfFillThreads = 148L * 1024;
 constexpr int kDcLeaf = 30;   // SMALLEST_BLOCK (include/pairwise.h:31)
 constexpr int kDcMaxDepth = 64;
 
@@ -107,38 +110,38 @@ __device__ __forceinline__ double kval(const float* a, const float* b, int d) {
 __device__ __forceinline__ float acc_add(float out, double t) { return __double2float_rn(__dadd_rn((double)out, t)); }
 __device__ __forceinline__ float acc_sub(float out, double t) { return __double2float_rn(__dsub_rn((double)out, t)); }
 
-// apply_bf (src/pairwise.cpp:368-380): thread per (pixel c, 8 labels); the
+// apply_bf (src/pairwise.cpp:368-380): thread per (pixel c, LC labels); the
 // pixels b in order, staged through shared memory a tile at a time.
-template <int D>
+template <int D, int LC>
 __global__ void __launch_bounds__(kBfTile) bf_apply_kernel(int N, int L, int d_rt, const float* __restrict__ feat,
                                                            const float* __restrict__ Q, float* __restrict__ out) {
     const int d = D > 0 ? D : d_rt;
     __shared__ float sf[kBfTile * kMaxD];
-    __shared__ float sq[kBfTile * kBfLabels];
+    __shared__ float sq[kBfTile * LC];
     const int c = blockIdx.x * kBfTile + threadIdx.x;
-    const int l0 = blockIdx.y * kBfLabels;
-    const int nl = min(kBfLabels, L - l0);
+    const int l0 = blockIdx.y * LC;
+    const int nl = min(LC, L - l0);
     float fc[kMaxD];
 #pragma unroll
     for (int i = 0; i < kMaxD; i++) fc[i] = (c < N && i < d) ? feat[(long)c * d + i] : 0.0f;
-    float acc[kBfLabels];
+    float acc[LC];
 #pragma unroll
-    for (int l = 0; l < kBfLabels; l++) acc[l] = 0.0f;
+    for (int l = 0; l < LC; l++) acc[l] = 0.0f;
     for (int b0 = 0; b0 < N; b0 += kBfTile) {
         const int nb = min(kBfTile, N - b0);
         __syncthreads();
         for (int t = threadIdx.x; t < nb * d; t += kBfTile) sf[t] = feat[(long)b0 * d + t];
         for (int t = threadIdx.x; t < nb * nl; t += kBfTile) {
             const int bi = t / nl, l = t - bi * nl;
-            sq[bi * kBfLabels + l] = Q[(long)(b0 + bi) * L + l0 + l];
+            sq[bi * LC + l] = Q[(long)(b0 + bi) * L + l0 + l];
         }
         __syncthreads();
         if (c < N)
             for (int bi = 0; bi < nb; bi++) {
                 const double k = kval<D>(fc, sf + bi * d, d);
 #pragma unroll
-                for (int l = 0; l < kBfLabels; l++)
-                    if (l < nl) acc[l] = acc_add(acc[l], __dmul_rn(k, (double)sq[bi * kBfLabels + l]));
+                for (int l = 0; l < LC; l++)
+                    if (l < nl) acc[l] = acc_add(acc[l], __dmul_rn(k, (double)sq[bi * LC + l]));
             }
     }
     if (c < N)
@@ -513,9 +516,15 @@ void with_dim(int d, F&& f) {
 void Model::apply_bf(int k, bool nonorm, float* out, const float* Q) {
     Term& t = *terms.at(k);
     float* raw = buf(8);
+    const bool share = (long)N * ceil_div(L, kBfLabels) >= kBfFillThreads;
     with_dim(t.d, [&](auto dc) {
-        launch(bf_apply_kernel<decltype(dc)::value>, dim3(ceil_div(N, kBfTile), ceil_div(L, kBfLabels)), kBfTile, 0,
-               stream, N, L, t.d, (const float*)t.feat.get(), Q, raw);
+        constexpr int D = decltype(dc)::value;
+        if (share)
+            launch(bf_apply_kernel<D, kBfLabels>, dim3(ceil_div(N, kBfTile), ceil_div(L, kBfLabels)), kBfTile, 0,
+                   stream, N, L, t.d, (const float*)t.feat.get(), Q, raw);
+        else
+            launch(bf_apply_kernel<D, 1>, dim3(ceil_div(N, kBfTile), L), kBfTile, 0, stream, N, L, t.d,
+                   (const float*)t.feat.get(), Q, raw);
     });
     DCRF_LAUNCH_CHECK();
     apply_compat(k, nonorm, out, raw);

@@ -137,3 +137,25 @@ def test_gpu_sorted_filters_reject_bad_ind():
         m.pairwise_apply_upper_minus_lower_dc(0, ind)
     with pytest.raises(DCRFError):
         m.pairwise_apply_upper_minus_lower_bf(0, ind)
+
+
+@pytest.mark.gpu
+def test_gpu_apply_bf_shared_exp_on_large_images(oracle_mod):
+    """256x200 x 21 labels: apply_bf's grid is large enough for one exp per
+    pair to serve eight labels (the small images above take one label per
+    thread); sampled rows against the restatement, in the reference's order."""
+    O = oracle_mod
+    W, H, L = 256, 200, 21
+    N = W * H
+    f = synth.gaussian_features(W, H, 3.0, 3.0)
+    Q = np.random.default_rng(6).random((N, L)).astype(np.float32)
+    m = DenseCRF2D(W, H, L)
+    m.addPairwiseEnergy(f, 3.0)
+    got = m.pairwise_apply_bf(0, Q)
+    rows = np.random.default_rng(7).choice(N, 12, replace=False)
+    K = O._kmat(f[rows], f)  # [rows, b] in double
+    acc = np.zeros((len(rows), L), np.float32)
+    for b in range(N):
+        acc = (acc.astype(np.float64) + K[:, b:b + 1] * Q[b][None, :].astype(np.float64)).astype(np.float32)
+    ok, info = _close(got[rows], O.compat_apply(acc, 0, 3.0))
+    assert ok, info
