@@ -14,7 +14,9 @@ from its sources).
   of the squared distance), 12x10, 2 labels;
 * "feat3" on 5x4 (N = 20: the divide-and-conquer filter is one block of
   pairs) and on 31x1 (N = 31: one odd halving into two blocks sharing the
-  middle position).
+  middle position);
+* "dims": apply_bf on 8x5 random features of every dimension d = 1..16 (the
+  squared distance's packet order for each), 2 labels.
 
 Run: python tests/golden/make_bruteforce_golden.py
 """
@@ -80,6 +82,21 @@ def feature_case(W, H, L, d):
     return out
 
 
+def dims_case(W=8, H=5, L=2):
+    rng = np.random.default_rng(SEED + 100)
+    N = W * H
+    U = rng.random((N, L)).astype(np.float32)
+    Q = rng.random((N, L)).astype(np.float32)
+    out = dict(W=W, H=H, L=L, U=U, Q=Q)
+    for d in range(1, 17):
+        f = (rng.random((N, d)) * 1.5).astype(np.float32)
+        m = O.ReferenceModel(W, H, L, U)
+        m.add_features(f, 2.0)
+        out[f"f{d}"] = f
+        out[f"bf_d{d}"] = m.apply_bf(0, Q)
+    return out
+
+
 def main():
     if not O.reference_available():
         sys.exit("oracle/_ref/libdcrf_ref.so missing: run `make -C oracle ref` first")
@@ -88,6 +105,7 @@ def main():
              "feat8_12x10_L2": feature_case(12, 10, 2, 8),
              "feat3_5x4_L2": feature_case(5, 4, 2, 3),
              "feat3_31x1_L3": feature_case(31, 1, 3, 3)}
+    np.savez_compressed(os.path.join(HERE, "bfdims_8x5_L2.npz"), **dims_case())
     for name, out in cases.items():
         np.savez_compressed(os.path.join(HERE, f"bruteforce_{name}.npz"), **out)
         print(name, {k: float(np.abs(v).max()) for k, v in out.items() if k[:2] in ("bf", "dc")})

@@ -49,6 +49,15 @@ def test_restatement_pinned_to_reference(name, oracle_mod):
             assert np.array_equal(O.compat_apply(O.dc_sorted(f, ind), kd, pp), g[f"dc{k}{sfx}"]), (name, k, sfx)
 
 
+def test_restatement_every_dimension_pinned():
+    """apply_bf for d = 1..16 (tests/golden/bfdims_8x5_L2.npz): the squared
+    distance's packet order of every dimension, bit for bit."""
+    from oracle import oracle as O
+    g = golden("bfdims_8x5_L2.npz")
+    for d in range(1, 17):
+        assert np.array_equal(O.compat_apply(O.bf_apply(g[f"f{d}"], g["Q"]), 0, 2.0), g[f"bf_d{d}"]), d
+
+
 def test_squared_norm_order_matters():
     """The packet order of the squared distance is not the left-to-right sum:
     on these values the two differ, and the reference's is the packet one."""
@@ -159,3 +168,17 @@ def test_gpu_apply_bf_shared_exp_on_large_images(oracle_mod):
         acc = (acc.astype(np.float64) + K[:, b:b + 1] * Q[b][None, :].astype(np.float64)).astype(np.float32)
     ok, info = _close(got[rows], O.compat_apply(acc, 0, 3.0))
     assert ok, info
+
+
+@pytest.mark.gpu
+def test_gpu_apply_bf_every_dimension():
+    """apply_bf for d = 1..16 against the reference (the specialised d = 2, 3,
+    5 kernels and the generic one)."""
+    g = golden("bfdims_8x5_L2.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    for d in range(1, 17):
+        m = DenseCRF2D(W, H, L)
+        m.setUnaryEnergy(g["U"])
+        m.addPairwiseEnergy(g[f"f{d}"], 2.0)
+        ok, info = _close(m.pairwise_apply_bf(0, g["Q"]), g[f"bf_d{d}"])
+        assert ok, (d, info)
