@@ -45,6 +45,13 @@ def test_argument_errors_before_device():
     assert b"invalid model size" in L.dcrf_last_error()
     assert L.dcrf_lattice_create(None) == 1
     assert L.dcrf_model_info(None, None, None, None) == 1
+    # every model entry point checks its handle before touching the device
+    for fn, nargs in (("dcrf_model_pairwise_apply_bf", 5), ("dcrf_model_pairwise_apply_upper_minus_lower_bf", 5),
+                      ("dcrf_model_pairwise_apply_upper_minus_lower_bf_ord", 6),
+                      ("dcrf_model_pairwise_apply_upper_minus_lower_dc", 5),
+                      ("dcrf_model_pairwise_kernel_gradient", 6), ("dcrf_model_pairwise_apply_ord_restricted", 8)):
+        assert getattr(L, fn)(*([None] + [0] * (nargs - 1))) == 1, fn
+        assert b"invalid model handle" in L.dcrf_last_error(), fn
 
 
 @pytest.mark.skipif(_has_gpu(), reason="checks the no-GPU error path")
