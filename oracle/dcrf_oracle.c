@@ -383,6 +383,73 @@ static int bin_upper(float q) {
 }
 
 /* seqCompute_upper_minus_lower_ord (src/permutohedral.cpp:590-701). */
+/* Permutohedral::gradient (src/permutohedral.cpp:1095-1178).  For each of
+ * the two sides (dir 0: splat a, blur axes 0..d, contract with b; dir 1:
+ * splat b, blur axes d..0, contract with a) the side is splatted, blurred
+ * with the double-evaluated 1/2 weights (:1134), and per pixel the
+ * differences r_j of the values at the simplex corners of ranks d - rank_j
+ * and the next one (scaled by alpha / (d+1)) are elevated: sm starts at r_0,
+ * then for j = 1..d the gradient of feature j-1 gathers
+ * other(k) * s_{j-1} (sm(k) - j r_j(k)) over k and sm += r_j -- all in float
+ * in the reference's order. */
+void orc_lattice_gradient(const orc_lattice* l, float* df, const float* a, const float* b, int L) {
+    const int N = l->N, M = l->M, d = l->d, d1 = d + 1;
+    const size_t vn = (size_t)(M + 2) * L;
+    float* v = (float*)malloc(vn * sizeof(float));
+    float* nv = (float*)malloc(vn * sizeof(float));
+    float* sf = (float*)malloc((size_t)d * sizeof(float));
+    float* ra = (float*)malloc((size_t)d1 * L * sizeof(float));
+    float* sm = (float*)malloc((size_t)L * sizeof(float));
+    memset(df, 0, (size_t)N * d * sizeof(float));
+    const float inv_std_dev = (float)(sqrt(2.0 / 3.0) * (d + 1));
+    for (int i = 0; i < d; i++) sf[i] = (float)(1.0 / sqrt((double)((i + 2) * (i + 1))) * (double)inv_std_dev);
+    const float alpha = 1.0f / (1.0f + powf(2.0f, (float)-d)) / (float)(d + 1);
+    for (int dir = 0; dir < 2; dir++) {
+        const float* in = dir ? b : a;
+        const float* other = dir ? a : b;
+        for (size_t t = 0; t < vn; t++) v[t] = nv[t] = 0.0f;
+        for (int i = 0; i < N; i++)
+            for (int j = 0; j <= d; j++) {
+                const int o = l->offset[(size_t)i * d1 + j] + 1;
+                const float w = l->bary[(size_t)i * d1 + j];
+                for (int k = 0; k < L; k++) v[(size_t)o * L + k] += w * in[(size_t)i * L + k];
+            }
+        for (int jj = 0; jj <= d; jj++) {
+            const int j = dir ? d - jj : jj;
+            for (int i = 0; i < M; i++) {
+                const int n1 = l->nbr[2 * ((size_t)j * M + i)] + 1, n2 = l->nbr[2 * ((size_t)j * M + i) + 1] + 1;
+                const float *o = v + (size_t)(i + 1) * L, *p = v + (size_t)n1 * L, *q = v + (size_t)n2 * L;
+                float* nw = nv + (size_t)(i + 1) * L;
+                for (int k = 0; k < L; k++) nw[k] = (float)((double)o[k] + 0.5 * (double)(p[k] + q[k]));
+            }
+            float* t = v; v = nv; nv = t;
+        }
+        for (int i = 0; i < N; i++) {
+            for (size_t t = 0; t < (size_t)d1 * L; t++) ra[t] = 0.0f;
+            for (int j = 0; j <= d; j++) {
+                const int r0 = d - l->rank[(size_t)i * d1 + j];
+                const int r1 = r0 + 1 > d ? 0 : r0 + 1;
+                const int o0 = l->offset[(size_t)i * d1 + r0] + 1, o1 = l->offset[(size_t)i * d1 + r1] + 1;
+                for (int k = 0; k < L; k++) {
+                    ra[(size_t)j * L + k] += alpha * v[(size_t)o0 * L + k];
+                    ra[(size_t)j * L + k] -= alpha * v[(size_t)o1 * L + k];
+                }
+            }
+            for (int k = 0; k < L; k++) sm[k] = ra[k];
+            for (int j = 1; j <= d; j++) {
+                float grad = 0.0f;
+                for (int k = 0; k < L; k++) {
+                    const float e = sf[j - 1] * (sm[k] - (float)j * ra[(size_t)j * L + k]);
+                    grad += other[(size_t)i * L + k] * e;
+                    sm[k] += ra[(size_t)j * L + k];
+                }
+                df[(size_t)i * d + j - 1] += grad;
+            }
+        }
+    }
+    free(v); free(nv); free(sf); free(ra); free(sm);
+}
+
 void orc_lattice_compute_ord(const orc_lattice* l, float* out, const float* in, int L) {
     const int N = l->N, M = l->M, d = l->d, d1 = d + 1;
     const size_t rows = (size_t)(M + 2) * L;

@@ -38,6 +38,9 @@ void orc_lattice_compute(const orc_lattice* l, float* out, const float* in, int 
 void orc_lattice_compute_f64(const orc_lattice* l, double* out, const double* in, int L,
                              int reverse);
 void orc_lattice_compute_ord(const orc_lattice* l, float* out, const float* in, int L);
+/* Permutohedral::gradient (src/permutohedral.cpp:1095-1178): df [N][d] =
+ * d(a^T K b) / d(features), a and b [N][L]. */
+void orc_lattice_gradient(const orc_lattice* l, float* df, const float* a, const float* b, int L);
 
 /* DenseCRF2D model with Potts terms and optional cliques (src/densecrf.cpp). */
 orc_model* orc_model_new(int W, int H, int L, const float* unary);

@@ -74,6 +74,7 @@ def oracle_lib():
         L.orc_lattice_compute.argtypes = [vp, _f32p, _f32p, C.c_int, C.c_int]
         L.orc_lattice_compute_f64.argtypes = [vp, _f64p, _f64p, C.c_int, C.c_int]
         L.orc_lattice_compute_ord.argtypes = [vp, _f32p, _f32p, C.c_int]
+        L.orc_lattice_gradient.argtypes = [vp, _f32p, _f32p, _f32p, C.c_int]
         L.orc_model_new.restype = vp
         L.orc_model_new.argtypes = [C.c_int, C.c_int, C.c_int, _f32p]
         L.orc_model_free.argtypes = [vp]
@@ -220,6 +221,14 @@ class OracleLattice(_Lattice):
         self._lib.orc_lattice_export(self._h, off, rk, by, keys, nbr)
         return dict(offset=off, rank=rk, bary=by, keys=keys[:M * self.d],
                     nbr=nbr[:2 * d1 * M], M=M)
+
+    def gradient(self, a, b):
+        """df [N][d] = d(a^T K b)/d(features) (restated Permutohedral::gradient)."""
+        a = _c(a, np.float32)
+        b = _c(b, np.float32)
+        df = np.empty((self.N, self.d), np.float32)
+        self._lib.orc_lattice_gradient(self._h, df, a, b, a.shape[1])
+        return df
 
     def compute_f64(self, x, reverse=False):
         x = _c(x, np.float64)

@@ -127,3 +127,12 @@ def test_restricted_restatement_pinned_to_golden(oracle_mod):
             assert np.array_equal(o, g[f"{name}_{key}"]), (name, key)
             k = 0 if name == "g" else 1
             assert np.array_equal(np.float32(-w) * o, g[f"m{k}_{key}"]), (name, key)
+
+
+@pytest.mark.parametrize("name", golden_names("gradient_"))
+def test_lattice_gradient_pinned_to_golden(name, oracle_mod):
+    """The restated Permutohedral::gradient (src/permutohedral.cpp:1095-1178)
+    against the reference's own values (tests/golden/make_gradient_golden.py)."""
+    g = golden(name)
+    df = oracle_mod.OracleLattice(g["f"]).gradient(g["a"], g["b"])
+    assert _bits_equal(df, g["df"]), name
