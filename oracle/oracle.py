@@ -808,3 +808,55 @@ def dc_sorted(feat, ind, lattice_cls=None):
         _dc_slice(col, sf, ex, 0, N)
         out[:, l] = col
     return out
+
+
+# ------------------------------------------------------ kernel gradient ----
+
+def kernel_gradient_diag(f, kparams, ntype, b, Q, w):
+    """``PairwisePotential::kernelGradient(b, Q)`` of a DIAG_KERNEL term with a
+    Potts compatibility (src/pairwise.cpp:402-407): lbl = -w Q; the lattice
+    on the scaled features diag(kparams) f (``setParameters``, :155-161) and
+    its norm n (``initLattice``, :40-57: 1/sqrt(K1 + 1e-20) symmetric, else
+    1/(K1 + 1e-20), in double); ``featureGradient(b, lbl)`` (:95-122) with
+    G = the restated ``Permutohedral::gradient`` for NormalizationType
+    ``ntype`` (0 none, 1 before, 2 after, 3 symmetric); then
+    ``(f o fg).rowwise().sum()`` (:174) over the original features, a float
+    sum left to right over the pixels as Eigen's row reduction runs it.
+    f [N][d], b and Q [N][L]; float32 throughout as the reference."""
+    f = np.asarray(f, np.float32)
+    a = np.asarray(b, np.float32)
+    Q = np.asarray(Q, np.float32)
+    N = f.shape[0]
+    lat = OracleLattice(np.ascontiguousarray((f * np.asarray(kparams, np.float32)[None, :]).astype(np.float32)))
+    lbl = (np.float32(-w) * Q).astype(np.float32)
+    c = lat.compute(np.ones((N, 1), np.float32))[:, 0].astype(np.float64)
+    n = (1.0 / np.sqrt(c + 1e-20) if ntype == 3 else 1.0 / (c + 1e-20)).astype(np.float32)
+
+    def G(x, y):
+        return lat.gradient(np.ascontiguousarray(x, np.float32), np.ascontiguousarray(y, np.float32))
+
+    def col(x, s):  # x * s.asDiagonal()
+        return (x * s[:, None]).astype(np.float32)
+
+    ones = np.ones_like(a)
+    nn = (n * n).astype(np.float32)
+    if ntype == 0:
+        fg = G(a, lbl)
+    elif ntype == 3:
+        fa = lat.compute(col(a, n), True)
+        fb = lat.compute(col(lbl, n))
+        n3 = (nn * n).astype(np.float32)
+        X = col((np.float32(0.5) * ((a * fb).astype(np.float32) + (fa * lbl).astype(np.float32))).astype(np.float32),
+                n3)
+        fg = (-G(X, ones) + G(col(a, n), col(lbl, n))).astype(np.float32)
+    elif ntype == 2:
+        X = col((a * lat.compute(lbl)).astype(np.float32), nn)
+        fg = (-G(X, ones) + G(col(a, n), lbl)).astype(np.float32)
+    else:
+        X = col((lat.compute(a, True) * lbl).astype(np.float32), nn)
+        fg = (-G(X, ones) + G(a, col(lbl, n))).astype(np.float32)
+    t = (f * fg).astype(np.float32)
+    out = t[0].copy()
+    for i in range(1, N):
+        out = (out + t[i]).astype(np.float32)
+    return out

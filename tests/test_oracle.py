@@ -136,3 +136,20 @@ def test_lattice_gradient_pinned_to_golden(name, oracle_mod):
     g = golden(name)
     df = oracle_mod.OracleLattice(g["f"]).gradient(g["a"], g["b"])
     assert _bits_equal(df, g["df"]), name
+
+
+def test_kernel_gradient_pinned_to_golden(oracle_mod):
+    """The restated DIAG_KERNEL kernelGradient for every NormalizationType (the
+    Gaussian term with its scales set) and the bilateral term after
+    setKernelParameters, bit for bit against the reference's own values
+    (tests/golden/make_kernel_golden.py)."""
+    g = golden("kernel_24x18_L5.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    fg = synth.gaussian_features(W, H, 3.0, 3.0)
+    for t in range(4):
+        r = oracle_mod.kernel_gradient_diag(fg, g["kg_kdiag"], t, g["b"], g[f"kg_1{t}_unary_init"], 3.0)
+        assert _bits_equal(r, g[f"kg_1{t}"]), t
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    fb = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    r = oracle_mod.kernel_gradient_diag(fb, g["kparam"], 3, g["b"], g["kparam_unary_init"], 5.0)
+    assert _bits_equal(r, g["kparam_kgrad1"])
