@@ -388,6 +388,29 @@ def test_kernel_and_normalization_types_vs_reference():
             assert np.abs(kg - ref).max() <= 1e-4 * np.abs(ref).max(), (kt, t, kg, ref)
 
 
+@pytest.mark.parametrize("ntype", [0, 1, 2, 3])
+def test_kernel_gradient_every_normalization_vs_oracle(ntype, oracle_mod):
+    """kernelGradient of a DIAG_KERNEL Gaussian term with scales set, on a
+    61x47 image, against the restatement (oracle.kernel_gradient_diag, pinned
+    bit for bit to the reference): FP64 sums over pixels here, float there,
+    so 1e-4 of the largest component."""
+    W, H, L = 61, 47, 5
+    img = synth.make_image(W, H, L, 12)
+    f = synth.gaussian_features(W, H, 3.0, 3.0)
+    kp = np.array([1.2, 0.8], np.float32)
+    m = DenseCRF2D(W, H, L)
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseEnergy(f, 3.0)
+    m.setKernel(0, 1, ntype)
+    m.pairwise_set_kernel_parameters(0, kp)
+    rng = np.random.default_rng(ntype)
+    b = rng.standard_normal((W * H, L)).astype(np.float32)
+    Q = rng.random((W * H, L)).astype(np.float32)
+    got = m.pairwise_kernel_gradient(0, b, Q)
+    ref = oracle_mod.kernel_gradient_diag(f, kp, ntype, b, Q, 3.0)
+    assert np.abs(got - ref).max() <= 1e-4 * np.abs(ref).max(), (got, ref)
+
+
 def test_per_pixel_energies_and_rounding_vs_reference():
     """unaryEnergy, pairwise_energy_true (each term and all), max_rounding
     (ties to the first maximum) bit for bit, and compute_LR_QP_value with a
