@@ -860,3 +860,50 @@ def kernel_gradient_diag(f, kparams, ntype, b, Q, w):
     for i in range(1, N):
         out = (out + t[i]).astype(np.float32)
     return out
+
+
+def eigen_sum(x):
+    """``ArrayXf::sum()`` of a contiguous float32 array as Eigen 3.2 reduces it
+    with SSE2 (Redux.h, LinearVectorizedTraversal from an aligned start): two
+    4-lane accumulators over 8-element steps, added lane-wise, one more
+    packet if a whole one is left, ``(p0 + p2) + (p1 + p3)``, then the tail
+    left to right (fewer than 4 elements: left to right)."""
+    s = np.asarray(x, np.float32).reshape(-1)
+    S = s.size
+    al = (S // 4) * 4
+    if al == 0:
+        r = s[0]
+        for i in range(1, S):
+            r = np.float32(r + s[i])
+        return r
+    p0 = s[0:4].copy()
+    if al > 4:
+        p1 = s[4:8].copy()
+        al2 = (S // 8) * 8
+        for idx in range(8, al2, 8):
+            p0 = (p0 + s[idx:idx + 4]).astype(np.float32)
+            p1 = (p1 + s[idx + 4:idx + 8]).astype(np.float32)
+        p0 = (p0 + p1).astype(np.float32)
+        if al > al2:
+            p0 = (p0 + s[al2:al2 + 4]).astype(np.float32)
+    r = np.float32(np.float32(p0[0] + p0[2]) + np.float32(p0[1] + p0[3]))
+    for i in range(al, S):
+        r = np.float32(r + s[i])
+    return r
+
+
+def weight_gradient_potts(f, b, Q):
+    """``PairwisePotential::gradient(b, Q)`` of a Potts term with the default
+    DIAG_KERNEL / NORMALIZE_SYMMETRIC kernel (src/pairwise.cpp:390-395,
+    src/labelcompatibility.cpp:72-76): fq = n K(n Q) on the restated lattice
+    (``DenseKernel::filter``), then ``-(b o fq).sum()`` in Eigen's order.
+    f [N][d], b and Q [N][L]."""
+    f = np.asarray(f, np.float32)
+    b = np.asarray(b, np.float32)
+    Q = np.asarray(Q, np.float32)
+    lat = OracleLattice(np.ascontiguousarray(f))
+    N = f.shape[0]
+    c = lat.compute(np.ones((N, 1), np.float32))[:, 0].astype(np.float64)
+    n = (1.0 / np.sqrt(c + 1e-20)).astype(np.float32)
+    fq = (lat.compute((Q * n[:, None]).astype(np.float32)) * n[:, None]).astype(np.float32)
+    return np.float32(-eigen_sum((b * fq).astype(np.float32)))

@@ -153,3 +153,16 @@ def test_kernel_gradient_pinned_to_golden(oracle_mod):
     fb = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
     r = oracle_mod.kernel_gradient_diag(fb, g["kparam"], 3, g["b"], g["kparam_unary_init"], 5.0)
     assert _bits_equal(r, g["kparam_kgrad1"])
+
+
+def test_weight_gradient_pinned_to_golden(oracle_mod):
+    """The restated Potts weight gradient (PairwisePotential::gradient) of both
+    terms of the example model, bit for bit against the reference's own
+    values (tests/golden/make_gradient_golden.py)."""
+    g = golden("mgrad_24x18_L5.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    feats = (synth.gaussian_features(W, H, 3.0, 3.0), synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"]))
+    for k, f in enumerate(feats):
+        r = oracle_mod.weight_gradient_potts(f, g["b"], g["Q"])
+        assert _bits_equal(np.float32(r), g[f"wgrad{k}"][0]), k
