@@ -892,11 +892,14 @@ def eigen_sum(x):
     return r
 
 
-def weight_gradient_potts(f, b, Q):
-    """``PairwisePotential::gradient(b, Q)`` of a Potts term with the default
-    DIAG_KERNEL / NORMALIZE_SYMMETRIC kernel (src/pairwise.cpp:390-395,
-    src/labelcompatibility.cpp:72-76): fq = n K(n Q) on the restated lattice
-    (``DenseKernel::filter``), then ``-(b o fq).sum()`` in Eigen's order.
+def weight_gradient_potts(f, b, Q, diagonal=False):
+    """``PairwisePotential::gradient(b, Q)`` of a term with the default
+    DIAG_KERNEL / NORMALIZE_SYMMETRIC kernel (src/pairwise.cpp:390-395):
+    fq = n K(n Q) on the restated lattice (``DenseKernel::filter``), then the
+    compatibility's gradient (src/labelcompatibility.cpp:72-76, 94-96):
+    Potts ``-(b o fq).sum()`` in Eigen's vectorised order; with ``diagonal``
+    ``(b o fq).rowwise().sum()``, per label a float sum over the pixels left
+    to right (a row of a column-major array has no packet access).
     f [N][d], b and Q [N][L]."""
     f = np.asarray(f, np.float32)
     b = np.asarray(b, np.float32)
@@ -906,4 +909,10 @@ def weight_gradient_potts(f, b, Q):
     c = lat.compute(np.ones((N, 1), np.float32))[:, 0].astype(np.float64)
     n = (1.0 / np.sqrt(c + 1e-20)).astype(np.float32)
     fq = (lat.compute((Q * n[:, None]).astype(np.float32)) * n[:, None]).astype(np.float32)
-    return np.float32(-eigen_sum((b * fq).astype(np.float32)))
+    t = (b * fq).astype(np.float32)
+    if diagonal:
+        out = t[0].copy()
+        for i in range(1, N):
+            out = (out + t[i]).astype(np.float32)
+        return out
+    return np.float32(-eigen_sum(t))

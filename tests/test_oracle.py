@@ -166,3 +166,11 @@ def test_weight_gradient_pinned_to_golden(oracle_mod):
     for k, f in enumerate(feats):
         r = oracle_mod.weight_gradient_potts(f, g["b"], g["Q"])
         assert _bits_equal(np.float32(r), g[f"wgrad{k}"][0]), k
+    # DiagonalCompatibility terms (tests/golden/make_compat_golden.py)
+    g = golden("compat_diag_24x18_L5.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    feats = (synth.gaussian_features(W, H, 3.0, 3.0), synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"]))
+    for k, f in enumerate(feats):
+        r = oracle_mod.weight_gradient_potts(f, g["b"], g["unary_init"], diagonal=True)
+        assert _bits_equal(r, g[f"wgrad{k}"]), k
