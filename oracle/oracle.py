@@ -916,3 +916,47 @@ def weight_gradient_potts(f, b, Q, diagonal=False):
             out = (out + t[i]).astype(np.float32)
         return out
     return np.float32(-eigen_sum(t))
+
+
+# ------------------------------------------------ per-pixel energies ----
+
+def unary_energy(U, lab):
+    """``DenseCRF::unaryEnergy(l)`` (src/densecrf.cpp:887-899): U(l_i, i), 0
+    where l_i is off the label range.  U [N][L], lab [N] int."""
+    U = np.asarray(U, np.float32)
+    lab = np.asarray(lab)
+    L = U.shape[1]
+    ok = (lab >= 0) & (lab < L)
+    r = np.zeros(U.shape[0], np.float32)
+    r[ok] = U[np.nonzero(ok)[0], lab[ok]]
+    return r
+
+
+def pairwise_energy_true(model, lab, term=-1):
+    """``DenseCRF::pairwise_energy_true(l, term)`` (:902-927) on a model with
+    ``apply(k, x, nonorm)``: the unnormalised Potts twin applied to
+    Q = [l_i != j], r_i = -Q'(l_i, i) (0 off the label range); term -1 adds
+    the terms in order to a zero vector."""
+    lab = np.asarray(lab)
+    N, L = lab.shape[0], model.L
+    if term == -1:
+        r = np.zeros(N, np.float32)
+        for k in range(model.nterms):
+            r = (r + pairwise_energy_true(model, lab, k)).astype(np.float32)
+        return r
+    Q = np.ones((N, L), np.float32)
+    ok = (lab >= 0) & (lab < L)
+    Q[np.nonzero(ok)[0], lab[ok]] = 0.0
+    out = model.apply(term, Q, nonorm=True)
+    r = np.zeros(N, np.float32)
+    r[ok] = -out[np.nonzero(ok)[0], lab[ok]]
+    return r
+
+
+def max_rounding(Q):
+    """``DenseCRF::max_rounding`` (:832-840): one-hot at each pixel's first
+    maximum (``maxCoeff``)."""
+    Q = np.asarray(Q, np.float32)
+    out = np.zeros_like(Q)
+    out[np.arange(Q.shape[0]), np.argmax(Q, axis=1)] = 1.0
+    return out

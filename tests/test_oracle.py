@@ -174,3 +174,20 @@ def test_weight_gradient_pinned_to_golden(oracle_mod):
     for k, f in enumerate(feats):
         r = oracle_mod.weight_gradient_potts(f, g["b"], g["unary_init"], diagonal=True)
         assert _bits_equal(r, g[f"wgrad{k}"]), k
+
+
+def test_per_pixel_energies_pinned_to_golden(oracle_mod):
+    """unaryEnergy, pairwise_energy_true (each term and all) and max_rounding
+    restated on the C oracle's model, bit for bit against the reference's own
+    values (tests/golden/make_energy_golden.py)."""
+    O = oracle_mod
+    g = golden("energies_24x18.npz")
+    W, H, L = int(g["W"]), int(g["H"]), int(g["L"])
+    img = synth.make_image(W, H, L, int(g["seed"]))
+    m = O.build_model(O.OracleModel, img)
+    lab = g["lab"]
+    assert _bits_equal(O.unary_energy(img["unary"], lab), g["unary_e"])
+    assert _bits_equal(O.pairwise_energy_true(m, lab, 0), g["pw0"])
+    assert _bits_equal(O.pairwise_energy_true(m, lab, 1), g["pw1"])
+    assert _bits_equal(O.pairwise_energy_true(m, lab, -1), g["pw_all"])
+    assert _bits_equal(O.max_rounding(g["Q"]), g["maxround"])
