@@ -960,3 +960,49 @@ def max_rounding(Q):
     out = np.zeros_like(Q)
     out[np.arange(Q.shape[0]), np.argmax(Q, axis=1)] = 1.0
     return out
+
+
+def eigen_sum_d(x):
+    """``ArrayXd::sum()`` in Eigen 3.2's SSE2 order: as :func:`eigen_sum` with
+    2-lane packets (two accumulators over 4-element steps, predux p0 + p1)."""
+    s = np.asarray(x, np.float64).reshape(-1)
+    S = s.size
+    al = (S // 2) * 2
+    if al == 0:
+        return float(s[0])
+    p0 = s[0:2].copy()
+    if al > 2:
+        p1 = s[2:4].copy()
+        al2 = (S // 4) * 4
+        for idx in range(4, al2, 4):
+            p0 = p0 + s[idx:idx + 2]
+            p1 = p1 + s[idx + 2:idx + 4]
+        p0 = p0 + p1
+        if al > al2:
+            p0 = p0 + s[al2:al2 + 2]
+    r = p0[0] + p0[1]
+    for i in range(al, S):
+        r = r + s[i]
+    return float(r)
+
+
+def dot_product(a, b):
+    """``dotProduct(M1, M2, tmp)`` (src/eigen_utils.cpp:68-74): both cast to
+    double, multiplied element-wise (exactly), summed in Eigen's order."""
+    return eigen_sum_d(np.asarray(a, np.float32).astype(np.float64) * np.asarray(b, np.float32).astype(np.float64))
+
+
+def lr_qp_value_diag(model, U, Q, dd):
+    """``DenseCRF::compute_LR_QP_value(Q, diag_dom)`` (src/densecrf.cpp:940-957)
+    on a model with ``apply(k, x)``: U.Q - dd.Q + sum_k Q.apply_k(Q) +
+    Q.(dd o Q), each a :func:`dot_product`, accumulated in double in that
+    order."""
+    Q = np.asarray(Q, np.float32)
+    dd = np.asarray(dd, np.float32)
+    e = 0.0
+    e += dot_product(U, Q)
+    e -= dot_product(dd, Q)
+    for k in range(model.nterms):
+        e += dot_product(Q, model.apply(k, Q))
+    e += dot_product(Q, (dd * Q).astype(np.float32))
+    return e

@@ -191,3 +191,5 @@ def test_per_pixel_energies_pinned_to_golden(oracle_mod):
     assert _bits_equal(O.pairwise_energy_true(m, lab, 1), g["pw1"])
     assert _bits_equal(O.pairwise_energy_true(m, lab, -1), g["pw_all"])
     assert _bits_equal(O.max_rounding(g["Q"]), g["maxround"])
+    # compute_LR_QP_value(Q, diag_dom): double sums in Eigen's packet order
+    assert O.lr_qp_value_diag(m, img["unary"], g["Q"], g["dd"]) == float(g["lrqp_dd"])
