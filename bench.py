@@ -47,12 +47,6 @@ L = 21
 GAUSS = (3.0, 3.0)                # sxy, w
 BILAT = (50.0, 15.0, 5.0)         # sxy, srgb, w
 LP_OVERRIDES = dict(prox_max_iter=50, prox_energy_tol=1e3)
-# Proximal iterations the reference's LP runs on the default image (640x480,
-# seed 2): its |dE| < prox_energy_tol five-times stop rule never fires, so all
-# 50 run (counted with the bit-exact CPU restatement, oracle/dcrf_oracle.c, in
-# 886 s).  Used only by --impl reference to scale its one-iteration sample to a
-# full solve; the GPU arm reports its own count (which matches).
-REF_PROX_ITERS = {(640, 480, 2): 50}
 ROOFLINE_TRAFFIC = os.path.join(ROOT, "profiles", "roofline_traffic.json")
 
 
@@ -71,6 +65,8 @@ def parse():
                     help="skip the extra workloads (QP, qp_sp / lp_sp, batch, adjoint): a short command for ncu")
     ap.add_argument("--only-batch", action="store_true",
                     help="time only qp_sp / lp_sp, the 64-image batched QP and the 16-image mean-field adjoint")
+    ap.add_argument("--only-batch-filter", action="store_true",
+                    help="time only the batched lattice filter over the 64-image concatenated lattices")
     ap.add_argument("--prox-iters", type=int, default=50,
                     help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
     return ap.parse_args()
@@ -175,11 +171,40 @@ class ClockSampler:
 
 
 # ------------------------------------------------------ reference on CPU --
+# The reference's LP at the benchmark size takes about a quarter of an hour
+# on one core, so the CPU legs time a bounded piece of the same solve -- one
+# proximal iteration of REF_SAMPLE_FW Frank-Wolfe steps (prox_max_iter=1),
+# from the workload's initial Q -- and convert it to whole solves with the
+# ratio of the same two quantities measured by the stock reference on one
+# core in one run: tests/golden/lp_640x480_seed2.json holds the full solve's
+# CPU seconds and the sample's (written by tests/golden/make_config_goldens.py
+# lp640; summary in profiles/reference_lp_640x480_full_solve.md).
+REF_SAMPLE_FW = 2
+REF_FULL_SOLVE = os.path.join(ROOT, "tests", "golden", "lp_640x480_seed2.json")
+
+
+def ref_solve_fraction(W, H, seed):
+    """(fraction of a full solve one sample is, description) from the
+    recorded stock-reference run, or None when none is recorded for W x H."""
+    if not os.path.exists(REF_FULL_SOLVE):
+        return None
+    with open(REF_FULL_SOLVE) as f:
+        rec = json.load(f)
+    key = f"prox1_fw{REF_SAMPLE_FW}_seconds"
+    if (rec.get("W"), rec.get("H"), rec.get("seed")) != (W, H, seed) or rec.get("source") != "reference" \
+            or key not in rec.get("samples", {}):
+        return None
+    t_sample = statistics.median(rec["samples"][key])
+    return t_sample / rec["cpu_seconds"], (f"recorded on one core ({rec.get('cpu', '?')}): full solve "
+                                           f"{rec['cpu_seconds']:.1f} s ({rec['prox_iters']} proximal x 10 "
+                                           f"Frank-Wolfe iterations), sample {t_sample:.2f} s")
+
+
 def _ref_worker(args):
-    """Times the reference LP on one core: t_call for prox_max_iter=1 (one
-    proximal iteration of fw Frank-Wolfe steps), and the per-call overheads it
-    contains: t_init (the energy evaluations done before the first
-    iteration) and t_proj (the integer energy after each iteration)."""
+    """Times `reps` samples of the reference LP on one core: each is
+    lp_inference_prox_super_pixels with prox_max_iter=1, fw_max_iter=fw from
+    the workload's initial Q.  With a barrier, every sample starts together
+    with the other workers'."""
     W, H, seed, fw, reps, barrier = args
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
@@ -188,14 +213,6 @@ def _ref_worker(args):
     img = synth.make_image(W, H, L, seed)
     m = O.build_model(cls, img, gaussian=GAUSS, bilateral=BILAT)
     Q = m.unary_init()
-    t0 = time.perf_counter()
-    lab = m.current_map(Q)
-    m.energy_lp(Q)
-    m.energy_ho(lab)
-    t_init = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    m.energy_ho(lab)
-    t_proj = time.perf_counter() - t0
     times = []
     for _ in range(reps):
         if barrier is not None:
@@ -203,17 +220,12 @@ def _ref_worker(args):
         t0 = time.perf_counter()
         m.lp(Q, prox_max_iter=1, fw_max_iter=fw, prox_energy_tol=1e3)
         times.append(time.perf_counter() - t0)
-    return dict(t_init=t_init, t_proj=t_proj, times=times, kind="reference" if use_ref else "port")
+    return dict(times=times, kind="reference" if use_ref else "port")
 
 
-def solve_time_from_sample(t_call, t_init, t_proj, fw, n_prox, fw_full=10):
-    """Full-solve time from a one-iteration sample: one init, then n_prox
-    proximal iterations of fw_full Frank-Wolfe steps and one projection."""
-    t_fw = max(t_call - t_init - t_proj, 1e-9) / fw
-    return t_init + n_prox * (fw_full * t_fw + t_proj)
-
-
-def cpu_reference(W, H, seed, n_prox, workers, fw, reps):
+def cpu_reference(W, H, seed, workers, fw, reps):
+    """Per step: the wall time of `workers` concurrent samples (the slowest
+    worker's), so that steps x time is time actually spent."""
     ctx = mp.get_context("spawn")
     if workers == 1:
         res = [_ref_worker((W, H, seed, fw, reps, None))]
@@ -221,11 +233,43 @@ def cpu_reference(W, H, seed, n_prox, workers, fw, reps):
         barrier = ctx.Manager().Barrier(workers)
         with ctx.Pool(workers) as pool:
             res = pool.map(_ref_worker, [(W, H, seed, fw, reps, barrier)] * workers)
-    per_rep = [max(r["times"][i] for r in res) for i in range(reps)]
-    t_init = statistics.median(r["t_init"] for r in res)
-    t_proj = statistics.median(r["t_proj"] for r in res)
-    solve_s = [solve_time_from_sample(t, t_init, t_proj, fw, n_prox) for t in per_rep]
-    return dict(kind=res[0]["kind"], per_rep=per_rep, solve_s=solve_s, t_init=t_init, t_proj=t_proj)
+    per_step = [max(r["times"][i] for r in res) for i in range(reps)]
+    return dict(kind=res[0]["kind"], per_step=per_step)
+
+
+def cpu_filter_baseline(W, H, img, reps=5):
+    """The reference's own lattice calls on one core, on the workload image:
+    Permutohedral::init of each term's lattice, Permutohedral::compute with
+    L = 21 and PairwisePotential::apply (median of reps), beside the GPU's
+    lattice-filter rate."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    if not O.reference_available():
+        return None
+    N = W * H
+    x = np.random.default_rng(0).random((N, L)).astype(np.float32)
+    feats = {"gaussian": synth.gaussian_features(W, H, GAUSS[0], GAUSS[0]),
+             "bilateral": synth.bilateral_features(W, H, BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
+                                                   img["rgb"])}
+    m = O.build_model(O.ReferenceModel, img, gaussian=GAUSS, bilateral=BILAT)
+    out = {"cores": 1, "kind": "reference", "workload": f"{W}x{H}, L={L}"}
+    for k, (name, f) in enumerate(feats.items()):
+        ti, tc, ta = [], [], []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            lat = O.ReferenceLattice(f)
+            ti.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            lat.compute(x)
+            tc.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            m.apply(k, x)
+            ta.append(time.perf_counter() - t0)
+            del lat
+        tcm = statistics.median(tc)
+        out[name] = {"init_ms": statistics.median(ti) * 1e3, "compute_ms": tcm * 1e3,
+                     "apply_ms": statistics.median(ta) * 1e3, "compute_gpix_label_s": N * L / tcm / 1e9}
+    return out
 
 
 def usable_cores():
@@ -246,32 +290,39 @@ def usable_cores():
 
 
 def run_reference(args):
+    """The reference's own CPU LP on the host cores (oracle/_ref, compiled from
+    its sources), one single-threaded process per usable core, rank 0 only.
+    Each step: every worker runs one sample (one proximal iteration of
+    REF_SAMPLE_FW Frank-Wolfe steps); ms_per_step is the measured wall time of
+    the step, and the solves it is worth come from the recorded stock-reference
+    ratio of sample to full solve (ref_solve_fraction)."""
     rank, _, world = dist_env()
     if rank != 0:
         return
     W, H = map(int, args.size.split("x"))
-    n_prox = REF_PROX_ITERS.get((W, H, args.seed))
-    if n_prox is None:
+    frac = ref_solve_fraction(W, H, args.seed)
+    if frac is None:
         print(json.dumps({"impl": "reference", "unavailable":
-                          f"no proximal-iteration count recorded for {W}x{H} seed {args.seed}"}))
+                          f"no stock-reference full solve recorded for {W}x{H} seed {args.seed}"}))
         return
+    fraction, recorded = frac
     workers = usable_cores()
     steps = args.steps + args.warmup
-    fw = max(1, min(10, int(round(10 * 12 / max(steps, 1)))))
-    r = cpu_reference(W, H, args.seed, n_prox, workers, fw, steps)
-    timed = r["solve_s"][args.warmup:] or r["solve_s"]
-    per_solve = statistics.mean(timed)
-    value = workers / per_solve
-    sample = (f"{workers} concurrent single-threaded solves; each step times one proximal iteration "
-              f"({fw} Frank-Wolfe steps, prox_max_iter=1) of the reference LP and scales it to a full "
-              f"solve of {n_prox} proximal x 10 Frank-Wolfe iterations (init {r['t_init']:.2f} s and "
-              f"per-iteration projection {r['t_proj']:.2f} s measured separately)")
+    r = cpu_reference(W, H, args.seed, workers, REF_SAMPLE_FW, steps)
+    timed = r["per_step"][args.warmup:] or r["per_step"]
+    step_s = statistics.mean(timed)
+    value = workers * fraction / step_s
+    sample = (f"{workers} concurrent single-threaded reference LPs; each step runs one proximal iteration "
+              f"({REF_SAMPLE_FW} Frank-Wolfe steps, prox_max_iter=1) from the workload's initial Q on every "
+              f"worker, measured {step_s:.2f} s per step; one sample = {fraction:.5f} of a full solve "
+              f"({recorded})")
     line = {"metric": "LP solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_solve * 1e3 / workers,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_s * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic", "impl": "reference",
             "config": {"workload": workload_name(W, H), "global_batch": workers,
-                       "parallelism": f"{workers} host processes"},
+                       "parallelism": f"{workers} host processes",
+                       "solve_fraction_per_worker_step": fraction},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": workers, "kind": r["kind"],
                              "sample": sample},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -549,6 +600,56 @@ def measure_batch(n=64, max_iter=100, reps=3):
             "outputs_match_sequential": same}
 
 
+def measure_batch_filter(n=64, reps=10):
+    """The batched lattice filter: PairwisePotential::apply of each pairwise
+    term (normalised Potts filter, pre- and post-scaled by the norm) over the
+    term's concatenated lattice of the config-4 batch (n images, H ~ U[240,
+    500], W ~ U[320, 500], seeded, about 10 M pixels), device-resident, timed
+    with CUDA events on the batch's stream.  The pixel arrays (0.86 GB each)
+    are far larger than L2, so no flush is needed between calls.
+    Algorithmic bytes: N (8L + 16(d+1) + 8) + M (8L + (d+1)(8L + 8))."""
+    import torch
+    from densecrf_ho_b200 import DenseCRF2DBatch, lib, check
+    Ls = lib()
+    sizes = synth.batch_sizes(n, 4)
+    imgs = [synth.make_image(w, h, L, 1000 + i) for i, (w, h) in enumerate(sizes)]
+    b = DenseCRF2DBatch(sizes, L)
+    b.setUnaryEnergy(np.concatenate([im["unary"] for im in imgs]))
+    b.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+    b.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
+                           np.concatenate([im["rgb"] for im in imgs]), BILAT[2])
+    N = int(b.N)
+    x = torch.rand((N, L), device="cuda", generator=torch.Generator("cuda").manual_seed(1))
+    y = torch.empty_like(x)
+    sptr = C.c_void_p()
+    check(Ls.dcrf_batch_stream(b._h, C.byref(sptr)))
+    bs = torch.cuda.ExternalStream(sptr.value)
+    peak, peak_kind = measured_peaks()
+    out = {"workload": f"PairwisePotential::apply over the concatenated lattice of {n} images "
+                       f"H~U[240,500] W~U[320,500] (seeded), L={L}, device-resident",
+           "images": n, "pixels": N, "peak_gbs": peak, "peak_kind": peak_kind}
+    for k, (name, d) in enumerate((("gaussian", 2), ("bilateral", 5))):
+        M = b.lattice_size(k)
+        run = lambda: check(Ls.dcrf_batch_pairwise_apply_dev(b._h, k, C.c_void_p(y.data_ptr()),
+                                                             C.c_void_p(x.data_ptr())))
+        for _ in range(3):
+            run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = Ls.dcrf_kernel_launches()
+        e0.record(bs)
+        for _ in range(reps):
+            run()
+        e1.record(bs)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / reps / 1e3
+        fb = filter_bytes(N, M, d)
+        out[name] = {"M": M, "d": d, "ms": t * 1e3, "bytes": fb, "gbs": fb / t / 1e9, "frac": fb / t / 1e9 / peak,
+                     "gpix_label_s": N * L / t / 1e9,
+                     "launches_per_call": int((Ls.dcrf_kernel_launches() - l0) // reps)}
+    return out
+
+
 def measure_next_rows(W=640, H=480, seed=2, cpu=True, reps=5):
     """The reference's learning and restricted-filter building blocks, through
     the C ABI with host buffers (so host<->device copies included), on the
@@ -788,6 +889,9 @@ def run_ours(args):
     if args.only_roofline:
         print(json.dumps(measure_filters(W, H, img, reps=3)))
         return
+    if args.only_batch_filter:
+        print(json.dumps(measure_batch_filter()))
+        return
     if args.only_batch:
         print(json.dumps(measure_ho()))
         print(json.dumps(measure_batch()))
@@ -890,19 +994,31 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_extra:
         line["extra"]["qp_320x240"] = measure_qp(cpu=not args.no_cpu_baseline)
         line["extra"]["ho_640x480"] = measure_ho(cpu=not args.no_cpu_baseline)
+        line["extra"]["batch_filter_64"] = measure_batch_filter()
         line["extra"]["batch_qp_64"] = measure_batch()
         line["extra"]["adjoint_16x512x512"] = measure_adjoint()
         line["extra"]["next_rows_640x480"] = measure_next_rows(cpu=not args.no_cpu_baseline)
-        line["extra"]["exact_filters"] = measure_exact_filters(cpu=not args.no_cpu_baseline)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_reference(W, H, args.seed, prox_iters, 1, 10, 1)
-        v = 1.0 / r["solve_s"][0]
-        line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": 1, "kind": r["kind"],
-                                "sample": (f"one proximal iteration (prox_max_iter=1, 10 Frank-Wolfe steps) of "
-                                           f"the reference LP on 1 core, {r['per_rep'][0]:.1f} s, scaled to "
-                                           f"{prox_iters} iterations (init {r['t_init']:.2f} s, projection "
-                                           f"{r['t_proj']:.2f} s per iteration)")}
+        frac = ref_solve_fraction(W, H, args.seed)
+        if frac is not None:
+            fraction, recorded = frac
+            r = cpu_reference(W, H, args.seed, 1, REF_SAMPLE_FW, 3)
+            t = statistics.median(r["per_step"])
+            line["cpu_baseline"] = {"value": fraction / t, "unit": "solves/s", "cores": 1, "kind": r["kind"],
+                                    "sample": (f"3 samples of the reference LP on 1 core, each one proximal "
+                                               f"iteration ({REF_SAMPLE_FW} Frank-Wolfe steps, "
+                                               f"prox_max_iter=1), median {t:.2f} s; one sample = "
+                                               f"{fraction:.5f} of a full solve ({recorded})")}
+        fb = cpu_filter_baseline(W, H, img)
+        if fb is not None:
+            gpu = line["extra"]["lattice_filter_gpix_label_s"]
+            line["cpu_baseline_filter"] = {
+                "value": fb["bilateral"]["compute_gpix_label_s"], "unit": "Gpix.label/s", "cores": 1,
+                "kind": "reference",
+                "sample": f"Permutohedral::compute, bilateral d=5 lattice, {W}x{H}, L={L}, median of 5",
+                "detail": fb,
+                "gpu_vs_cpu": {k: gpu[k] / fb[k]["compute_gpix_label_s"] for k in ("gaussian", "bilateral")}}
     if rank == 0:
         print(json.dumps(line))
     if world > 1:

@@ -495,6 +495,22 @@ class DenseCRF2DBatch:
                                   C.byref(p), st))
         return (out, list(st)) if stats else out
 
+    def pairwise_apply(self, k, x):
+        """``pairwise_[k]->apply(out, x)`` of every image at once, over the
+        term's concatenated lattice (each image's rows equal its own
+        ``DenseCRF2D.pairwise_apply``)."""
+        xx = self._mat(x)
+        out = self._new()
+        check(lib().dcrf_batch_pairwise_apply(self._h, int(k), out.ctypes.data_as(C.c_void_p),
+                                              xx.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def lattice_size(self, k):
+        """Vertex count of term k's concatenated lattice."""
+        m = C.c_int64()
+        check(lib().dcrf_batch_lattice_size(self._h, int(k), C.byref(m)))
+        return m.value
+
     # -- differentiation (unrolled mean-field) --------------------------
     def n_terms(self):
         n = C.c_int()
@@ -503,6 +519,17 @@ class DenseCRF2DBatch:
 
     def set_weight(self, k, w):
         check(lib().dcrf_batch_set_weight(self._h, int(k), C.c_float(w)))
+
+    def set_checkpointing(self, every=1, recompute_lattice=False):
+        """Keep every ``every``-th mean-field iterate (the backward pass
+        recomputes the others); release the lattices between the passes and
+        rebuild them when ``recompute_lattice``."""
+        check(lib().dcrf_batch_set_checkpointing(self._h, int(every), int(bool(recompute_lattice))))
+
+    def meanfield_state_bytes(self, iterations):
+        n = C.c_uint64()
+        check(lib().dcrf_batch_meanfield_state_bytes(self._h, int(iterations), C.byref(n)))
+        return n.value
 
     def meanfield(self, iterations):
         """Q_T of ``iterations`` mean-field steps (Q_0 .. Q_T are kept for
@@ -570,3 +597,21 @@ DenseCRF2D.pairwise_parameters = _pairwise_parameters
 DenseCRF2D.pairwise_set_parameters = _pairwise_set_parameters
 DenseCRF2D.pairwise_kernel_gradient = _pairwise_kernel_gradient
 DenseCRF2D.pairwise_gradient = _pairwise_gradient
+
+
+def set_device_memory_limit(nbytes):
+    """Budget (bytes, 0 = none) on the device memory the library holds for
+    live models, lattices and batches; a request beyond it raises a
+    DCRFError with DCRF_E_NOMEM before any device call."""
+    check(lib().dcrf_set_device_memory_limit(C.c_uint64(int(nbytes))))
+
+
+def device_memory_stats():
+    """``(in_use, cached, mallocs)``: bytes held by live objects, bytes kept
+    in the library's cache of freed blocks, cudaMalloc calls made so far."""
+    a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    check(lib().dcrf_device_memory_stats(C.byref(a), C.byref(b), C.byref(c)))
+    return a.value, b.value, c.value
+
+
+__all__ += ["set_device_memory_limit", "device_memory_stats"]

@@ -350,6 +350,21 @@ dcrf_status dcrf_release_cached_memory(void) {
     return guard([&] { dcrf::dev_trim(true); });
 }
 
+dcrf_status dcrf_set_device_memory_limit(uint64_t bytes) {
+    return guard([&] { dcrf::set_device_memory_limit((size_t)bytes); });
+}
+
+dcrf_status dcrf_device_memory_stats(uint64_t* in_use, uint64_t* cached, uint64_t* mallocs) {
+    return guard([&] {
+        size_t l = 0, c = 0;
+        unsigned long long m = 0;
+        dcrf::device_memory_stats(&l, &c, &m);
+        if (in_use) *in_use = l;
+        if (cached) *cached = c;
+        if (mallocs) *mallocs = m;
+    });
+}
+
 dcrf_status dcrf_model_destroy(dcrf_model h) {
     return guard([&] {
         if (!h) return;
@@ -1137,10 +1152,56 @@ dcrf_status dcrf_batch_set_weight(dcrf_batch h, int k, float w_potts) {
     return guard([&] { BT(h).set_weight(k, w_potts); });
 }
 
+dcrf_status dcrf_batch_set_checkpointing(dcrf_batch h, int checkpoint_every, int recompute_lattice) {
+    return guard([&] { BT(h).set_checkpointing(checkpoint_every, recompute_lattice != 0); });
+}
+
+dcrf_status dcrf_batch_meanfield_state_bytes(dcrf_batch h, int T, uint64_t* bytes) {
+    return guard([&] {
+        need(bytes, "bytes");
+        dcrf::require(T >= 0 && T <= 1000, DCRF_E_ARG, "iterations must be in [0, 1000]");
+        *bytes = BT(h).meanfield_state_bytes(T);
+    });
+}
+
 dcrf_status dcrf_batch_terms(dcrf_batch h, int* n_terms) {
     return guard([&] {
         need(n_terms, "n_terms");
         *n_terms = (int)BT(h).terms.size();
+    });
+}
+
+dcrf_status dcrf_batch_pairwise_apply_dev(dcrf_batch h, int k, float* d_out, const float* d_in) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(d_out, "out");
+        need(d_in, "in");
+        dcrf::require(k >= 0 && k < (int)b.terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+        b.apply(k, d_out, d_in);
+    });
+}
+
+dcrf_status dcrf_batch_pairwise_apply(dcrf_batch h, int k, float* out, const float* in) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(out, "out");
+        need(in, "in");
+        dcrf::require(k >= 0 && k < (int)b.terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+        const size_t n = (size_t)b.Ntot * b.L;
+        upload(h->io0, in, n, b.stream);
+        float* d = h->io1.ensure(n);
+        b.apply(k, d, h->io0.get());
+        download(out, d, n, b.stream);
+        DCRF_CUDA(cudaStreamSynchronize(b.stream));
+    });
+}
+
+dcrf_status dcrf_batch_lattice_size(dcrf_batch h, int k, int64_t* M) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(M, "M");
+        dcrf::require(k >= 0 && k < (int)b.terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+        *M = b.terms[k]->lat->M;
     });
 }
 

@@ -68,12 +68,13 @@ __global__ void softmax_bwd_kernel(long N, int Lrt, const float* __restrict__ Q,
 #pragma unroll
     for (int k = 0; k < PixVec<LC>::S; k++)
         if (k < L) s += (double)g[i * L + k] * (double)Q[i * L + k];
-    const float sf = (float)s;
+    // g - <g, Q> cancels where g is nearly constant over the labels: formed
+    // in FP64, rounded once.
 #pragma unroll
     for (int k = 0; k < PixVec<LC>::S; k++)
         if (k < L) {
             const long e = i * L + k;
-            const float v = Q[e] * (g[e] - sf);
+            const float v = (float)((double)Q[e] * ((double)g[e] - s));
             ga[e] = v;
             dU[e] = (first ? 0.0f : dU[e]) - v;
         }
@@ -123,28 +124,38 @@ Batch::~Batch() {
     if (stream) cudaStreamDestroy(stream);
 }
 
+// Term t's lattice over all images: every image's own lattice, built from
+// the term's features, concatenated (Lattice::concat).
+void Batch::build_lattice(Term& t) {
+    t.lat = std::make_unique<Lattice>();
+    t.lat->stream = stream;
+    std::vector<std::unique_ptr<Lattice>> parts;
+    std::vector<const Lattice*> views;
+    for (int i = 0; i < B; i++) {
+        auto p = std::make_unique<Lattice>();
+        p->stream = stream;
+        p->build(t.feat.get() + pix_off[i] * t.d, t.d, W[i] * H[i]);
+        views.push_back(p.get());
+        parts.push_back(std::move(p));
+    }
+    t.lat->concat(views);
+}  // the per-image lattices are released here
+
+void Batch::ensure_lattices() {
+    for (auto& t : terms)
+        if (!t->lat) build_lattice(*t);
+}
+
 void Batch::add_term(const float* d_features, int d, float w) {
     img.clear();  // rebuilt with the new term at the next QP
     qp_warm = false;
+    ensure_lattices();
     auto t = std::make_unique<Term>();
     DCRF_CUDA(cudaMemcpyAsync(t->feat.ensure((size_t)Ntot * d), d_features, sizeof(float) * Ntot * d,
                               cudaMemcpyDeviceToDevice, stream));
-    t->lat = std::make_unique<Lattice>();
-    t->lat->stream = stream;
-    {
-        std::vector<std::unique_ptr<Lattice>> parts;
-        std::vector<const Lattice*> views;
-        for (int i = 0; i < B; i++) {
-            auto p = std::make_unique<Lattice>();
-            p->stream = stream;
-            p->build(d_features + pix_off[i] * d, d, W[i] * H[i]);
-            views.push_back(p.get());
-            parts.push_back(std::move(p));
-        }
-        t->lat->concat(views);
-    }  // the per-image lattices are released here
-    t->w = w;
     t->d = d;
+    build_lattice(*t);
+    t->w = w;
     float* nrm = t->norm.ensure(Ntot);
     launch(bfill_kernel, ceil_div(Ntot, 256), 256, 0, stream, Ntot, 1.0f, nrm);
     SliceEpilogue ep;
@@ -155,6 +166,7 @@ void Batch::add_term(const float* d_features, int d, float w) {
 }
 
 void Batch::apply(int k, float* out, const float* in, const float* base, float coef, bool zero_base) {
+    ensure_lattices();
     Term& t = *terms[k];
     SliceEpilogue ep;
     ep.potts = true;
@@ -293,36 +305,68 @@ static void normalised_filter(Term& t, int L, float* out, const float* in, float
     t.lat->compute(out, in, L, transpose, ep, t.norm.get());
 }
 
+void Batch::set_checkpointing(int every, bool recompute_lat) {
+    require(every >= 1 && every <= 1000, DCRF_E_ARG, "checkpointing: interval must be in [1, 1000]");
+    ck_every = every;
+    recompute_lattice = recompute_lat;
+    mf_T = -1;  // the checkpoints of an earlier forward pass are laid out differently
+}
+
+size_t Batch::meanfield_state_bytes(int T) const {
+    const size_t arr = sizeof(float) * (size_t)Ntot * L;
+    const size_t slots = (size_t)(T / ck_every + 1 + (T % ck_every ? 1 : 0));
+    const size_t seg = ck_every > 1 ? (size_t)std::min(ck_every - 1, std::max(T - 1, 0)) : 0;
+    return (slots + seg) * arr;
+}
+
+// Q_{t+1} = softmax(-U + sum_k w_k K~_k Q_t) from q into qn.
+void Batch::mf_iteration(const float* q, float* qn, const float* negU, float* logits) {
+    const long NL = Ntot * L;
+    const int nt = (int)terms.size();
+    if (nt == 0) DCRF_CUDA(cudaMemcpyAsync(logits, negU, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    for (int k = 0; k < nt; k++)  // logits = -U + sum_k w_k K~_k Q
+        normalised_filter(*terms[k], L, logits, q, terms[k]->w, k == 0 ? negU : logits, false);
+    with_lc(L, [&](auto lc) {
+        constexpr int LC = decltype(lc)::value;
+        launch(softmax_kernel<LC>, ceil_div(Ntot, 128), 128, 0, stream, Ntot, L, logits, qn);
+    });
+}
+
+// Forward pass.  Q_t is kept for t % ck_every == 0 and for t = T (the
+// backward pass recomputes the others); with ck_every = 1 every iterate is
+// kept.  In the recompute_lattice mode the lattices are released at the end
+// and rebuilt by the backward pass.
 void Batch::meanfield(int iterations, float* Q) {
     require(has_unary, DCRF_E_STATE, "meanfield: no unary energy set");
     require(iterations >= 0 && iterations <= 1000, DCRF_E_ARG, "meanfield: iterations must be in [0, 1000]");
+    ensure_lattices();
     const long NL = Ntot * L;
-    float* ck = mf_ck.ensure((size_t)(iterations + 1) * NL);
+    mf_T = iterations;
+    const int slots = iterations / ck_every + 1 + (iterations % ck_every ? 1 : 0);
+    float* ck = mf_ck.ensure((size_t)slots * NL);
     float* negU = buf(4);
     float* logits = buf(5);
+    float* x[2] = {mf_x0.ensure(ck_every > 1 ? NL : 1), mf_x1.ensure(ck_every > 1 ? NL : 1)};
     launch(negate_kernel, ceil_div(NL, 256), 256, 0, stream, NL, unary.get(), negU);
     unary_init(ck);  // Q_0 = softmax(-U)
-    const int nt = (int)terms.size();
+    const float* q = ck;
     for (int it = 0; it < iterations; it++) {
-        const float* q = ck + (size_t)it * NL;
-        if (nt == 0)
-            DCRF_CUDA(cudaMemcpyAsync(logits, negU, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
-        for (int k = 0; k < nt; k++)  // logits = -U + sum_k w_k K~_k Q
-            normalised_filter(*terms[k], L, logits, q, terms[k]->w, k == 0 ? negU : logits, false);
-        with_lc(L, [&](auto lc) {
-            constexpr int LC = decltype(lc)::value;
-            launch(softmax_kernel<LC>, ceil_div(Ntot, 128), 128, 0, stream, Ntot, L, logits,
-                   ck + (size_t)(it + 1) * NL);
-        });
+        float* qn = ck_stored(it + 1) ? ck + (size_t)ck_slot(it + 1) * NL : x[it & 1];
+        mf_iteration(q, qn, negU, logits);
+        q = qn;
     }
     DCRF_LAUNCH_CHECK();
-    if (Q) DCRF_CUDA(cudaMemcpyAsync(Q, ck + (size_t)iterations * NL, sizeof(float) * NL,
+    if (Q) DCRF_CUDA(cudaMemcpyAsync(Q, ck + (size_t)ck_slot(iterations) * NL, sizeof(float) * NL,
                                      cudaMemcpyDeviceToDevice, stream));
-    mf_T = iterations;
+    if (recompute_lattice) {
+        DCRF_CUDA(cudaStreamSynchronize(stream));
+        for (auto& t : terms) t->lat.reset();
+    }
 }
 
 void Batch::meanfield_backward(const float* grad_Q, float* grad_U, double* grad_w) {
     require(mf_T >= 0, DCRF_E_STATE, "meanfield_backward: no meanfield() to differentiate");
+    ensure_lattices();  // rebuilt here in the recompute_lattice mode
     const long NL = Ntot * L;
     const int nt = (int)terms.size();
     const float* ck = mf_ck.get();
@@ -330,8 +374,12 @@ void Batch::meanfield_backward(const float* grad_Q, float* grad_U, double* grad_
     float* gn = mf_g1.ensure(NL);
     float* ga = mf_ga.ensure(NL);
     float* m = mf_m.ensure(NL);
+    float* seg = ck_every > 1 ? mf_seg.ensure((size_t)(ck_every - 1) * NL) : nullptr;
+    float* negU = buf(4);
+    float* logits = buf(5);
     double* dw = mf_dw.ensure(std::max(nt, 1));
     double* part = partials.get();
+    if (ck_every > 1) launch(negate_kernel, ceil_div(NL, 256), 256, 0, stream, NL, unary.get(), negU);
     DCRF_CUDA(cudaMemcpyAsync(g, grad_Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
     if (nt) DCRF_CUDA(cudaMemsetAsync(dw, 0, sizeof(double) * nt, stream));
     auto softmax_bwd = [&](const float* q, int first) {
@@ -340,12 +388,26 @@ void Batch::meanfield_backward(const float* grad_Q, float* grad_U, double* grad_
             launch(softmax_bwd_kernel<LC>, ceil_div(Ntot, 128), 128, 0, stream, Ntot, L, q, g, ga, grad_U, first);
         });
     };
+    // Q_t: a checkpoint, or an iterate of the current segment recomputed
+    // from the checkpoint at its start.
+    int seg_s = -1;
+    auto iterate = [&](int t) -> const float* {
+        if (ck_stored(t)) return ck + (size_t)ck_slot(t) * NL;
+        return seg + (size_t)(t - seg_s - 1) * NL;
+    };
     for (int it = mf_T - 1; it >= 0; it--) {
-        const float* q0 = ck + (size_t)it * NL;
-        const float* q1 = ck + (size_t)(it + 1) * NL;
+        const int s = (it / ck_every) * ck_every;
+        if (ck_every > 1 && s != seg_s) {  // recompute Q_{s+1} .. Q_{e-1} of this segment
+            seg_s = s;
+            const int e = std::min(s + ck_every, mf_T);
+            for (int t = s; t + 1 < e; t++)
+                mf_iteration(iterate(t), seg + (size_t)(t - s) * NL, negU, logits);
+        }
+        const float* q0 = iterate(it);
+        const float* q1 = iterate(it + 1);
         softmax_bwd(q1, it == mf_T - 1);  // ga = dL/dlogits_t; grad_U -= ga
         for (int k = 0; k < nt; k++) {
-            // dL/dw_k += <ga, K~_k Q_t>, the message recomputed from the checkpoint
+            // dL/dw_k += <ga, K~_k Q_t>, the message recomputed from the iterate
             normalised_filter(*terms[k], L, m, q0, 1.0f, nullptr, false);
             launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, ga, m, part);
             launch(accumulate_total_kernel, 1, 32, 0, stream, part, kRedBlocks, dw + k);
@@ -359,6 +421,8 @@ void Batch::meanfield_backward(const float* grad_Q, float* grad_U, double* grad_
     DCRF_LAUNCH_CHECK();
     if (nt) DCRF_CUDA(cudaMemcpyAsync(grad_w, dw, sizeof(double) * nt, cudaMemcpyDeviceToHost, stream));
     DCRF_CUDA(cudaStreamSynchronize(stream));
+    if (recompute_lattice)
+        for (auto& t : terms) t->lat.reset();
 }
 
 }  // namespace dcrf

@@ -38,10 +38,14 @@ struct Batch {
     const float* warm_out = nullptr;
     int warm_max_iter = -1;
 
-    // mean-field checkpoints Q_0 .. Q_mf_T, [mf_T + 1][Ntot][L]
-    DevBuf<float> mf_ck, mf_g0, mf_g1, mf_ga, mf_m;
+    // mean-field checkpoints: Q_t for t % ck_every == 0 and Q_T, [slots][Ntot][L];
+    // the other iterates are recomputed segment by segment in the backward
+    // pass into mf_seg ([ck_every - 1][Ntot][L]).
+    DevBuf<float> mf_ck, mf_seg, mf_g0, mf_g1, mf_ga, mf_m, mf_x0, mf_x1;
     DevBuf<double> mf_dw;
     int mf_T = -1;
+    int ck_every = 1;              // keep every ck_every-th iterate (1 = all)
+    bool recompute_lattice = false;  // release the lattices between the passes, rebuild them
 
 
     Batch(int n, const int* widths, const int* heights, int L_);
@@ -65,9 +69,20 @@ struct Batch {
     // dL/dU and dL/dw_k (summed over all images, FP64) out.
     void meanfield_backward(const float* grad_Q, float* grad_U, double* grad_w);
     void set_weight(int k, float w);
+    void set_checkpointing(int every, bool recompute_lat);
+    // Builds every term's concatenated lattice that is not there (released
+    // by the recompute_lattice mode), from the term's features.
+    void ensure_lattices();
+    // Device bytes the mean-field checkpoints and recompute buffers take for
+    // T iterations under the current checkpointing.
+    size_t meanfield_state_bytes(int T) const;
 
   private:
     void ensure_image_models();
+    void build_lattice(Term& t);
+    int ck_slot(int t) const { return t == mf_T && t % ck_every ? mf_T / ck_every + 1 : t / ck_every; }
+    bool ck_stored(int t) const { return t % ck_every == 0 || t == mf_T; }
+    void mf_iteration(const float* q, float* qn, const float* negU, float* logits);
 };
 
 constexpr int kQpThreads = 8;  // host threads of a batch QP

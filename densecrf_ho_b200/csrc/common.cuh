@@ -51,6 +51,11 @@ void dev_release(void* p, size_t bytes) noexcept;
 // Frees the cached blocks of the current device, or of every device
 // (dcrf_release_cached_memory).
 void dev_trim(bool all_devices) noexcept;
+// A budget on the bytes held by live DevBufs (0 = none): a request beyond it
+// fails with DCRF_E_NOMEM on the host, before any device call.
+void set_device_memory_limit(size_t bytes);
+// Bytes held by live DevBufs, bytes kept in the cache, cudaMalloc calls made.
+void device_memory_stats(size_t* live, size_t* cached, unsigned long long* mallocs);
 
 // Owning device allocation; grows, never shrinks.
 template <typename T>

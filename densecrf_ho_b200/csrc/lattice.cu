@@ -546,12 +546,19 @@ __global__ void count_long_kernel(int M, const int* __restrict__ counts, int thr
     if ((threadIdx.x & 31) == 0 && b) atomicAdd(n, __popc(b));
 }
 
-// Sort key that puts long splat lists first (stable radix sort ascending).
+// Sort key of the splat visiting order (stable radix sort ascending): the
+// long lists first, longest first, so that their chains start early; the
+// short lists after them in vertex-id order.  Ids follow the pixels' scan
+// order (first occurrence), so consecutive short lists gather rows of nearby
+// pixels and each input row is fetched from DRAM about once although d + 1
+// lists read it (sorting the short lists by length too scattered them over
+// the whole image).
 __global__ void order_key_kernel(int M, const int* __restrict__ counts, int* __restrict__ keys,
                                  int* __restrict__ vals) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= M) return;
-    keys[v] = kMaxOrderKey - min(counts[v], kMaxOrderKey);
+    const int c = counts[v];
+    keys[v] = c > kLongList ? kMaxOrderKey - min(c, kMaxOrderKey) : kMaxOrderKey;
     vals[v] = v;
 }
 

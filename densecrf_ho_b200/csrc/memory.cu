@@ -23,6 +23,9 @@ struct Block {
 };
 
 std::mutex g_mu;
+size_t g_live = 0;         // bytes handed out and not yet released (every device)
+size_t g_limit = 0;        // cap on g_live; 0 = none (dcrf_set_device_memory_limit)
+unsigned long long g_mallocs = 0;  // cudaMalloc calls that succeeded
 std::vector<Block>& cache() {
     static auto* c = new std::vector<Block>();  // never destroyed: the process exit frees the memory
     return *c;
@@ -58,6 +61,11 @@ void* dev_alloc(size_t bytes, size_t* got) {
     DCRF_CUDA(cudaGetDevice(&dev));
     {
         std::lock_guard<std::mutex> lk(g_mu);
+        // A caller-set budget: refused on the host, before any device call.
+        if (g_limit && g_live + b > g_limit)
+            throw Error(DCRF_E_NOMEM, "device memory limit of " + std::to_string(g_limit) + " bytes reached (" +
+                                          std::to_string(g_live) + " in use, " + std::to_string(b) + " requested)");
+        g_live += b;
         auto& c = cache();
         for (size_t i = c.size(); i-- > 0;)
             if (c[i].dev == dev && c[i].bytes == b) {
@@ -77,13 +85,37 @@ void* dev_alloc(size_t bytes, size_t* got) {
         dev_trim(false);
         e = cudaMalloc(&p, b);
     }
+    if (e != cudaSuccess) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_live -= b;
+    }
     DCRF_CUDA(e);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_mallocs++;
+    }
     *got = b;
     return p;
 }
 
+void set_device_memory_limit(size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_limit = bytes;
+}
+
+void device_memory_stats(size_t* live, size_t* cached, unsigned long long* mallocs) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    *live = g_live;
+    *cached = g_cached;
+    *mallocs = g_mallocs;
+}
+
 void dev_release(void* p, size_t bytes) noexcept {
     if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_live -= bytes;
+    }
     std::lock_guard<std::recursive_mutex> cap(capture_mutex());
     // the block's own device (the caller's current device may be another)
     int cur = 0, dev = 0;

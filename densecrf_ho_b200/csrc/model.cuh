@@ -62,6 +62,8 @@ struct SolverScalars {
     int done;             // batched QP: the image had stopped before this iteration
     int gamma_sum;        // LP: qp-gamma iterations of the whole solve
     int chunk;            // QP graph: iterations in the current launch
+    int numeric;          // bits: 1 a NaN / inf in a solver's input, 2 in a rescaled
+                          // iterate, 4 rescale's maxval < 0 (src/eigen_utils.cpp:138)
 };
 
 constexpr int kQpChunk = 64;  // QP iterations per graph launch at most

@@ -124,6 +124,12 @@ __global__ void dot_kernel(long n, const float* __restrict__ a, const float* __r
     block_sum_store<1>(v, partials);
 }
 
+// min / max that carry a NaN through (fminf / fmaxf drop it): equal to
+// fminf / fmaxf on numbers, NaN as soon as either side is NaN, so a NaN
+// anywhere in the data reaches the result.
+__device__ __forceinline__ float nan_min(float a, float b) { return a != a ? a : (b != b ? b : fminf(a, b)); }
+__device__ __forceinline__ float nan_max(float a, float b) { return a != a ? a : (b != b ? b : fmaxf(a, b)); }
+
 // min / max of x (exact, so order-free): per-block partials stored as
 // doubles, then minmax_finish_kernel combines them into sc->qmin / sc->qmax.
 __global__ void minmax_partial_kernel(long n, const float* __restrict__ x, double* __restrict__ partials) {
@@ -131,13 +137,13 @@ __global__ void minmax_partial_kernel(long n, const float* __restrict__ x, doubl
     float mn = INFINITY, mx = -INFINITY;
     for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
         const float v = x[t];
-        mn = fminf(mn, v);
-        mx = fmaxf(mx, v);
+        mn = nan_min(mn, v);
+        mx = nan_max(mx, v);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
-        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+        mn = nan_min(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = nan_max(mx, __shfl_down_sync(kFullMask, mx, o));
     }
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (lane == 0) {
@@ -147,26 +153,29 @@ __global__ void minmax_partial_kernel(long n, const float* __restrict__ x, doubl
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int i = 1; i < kRedThreads / 32; i++) {
-            mn = fminf(mn, smin[i]);
-            mx = fmaxf(mx, smax[i]);
+            mn = nan_min(mn, smin[i]);
+            mx = nan_max(mx, smax[i]);
         }
         partials[blockIdx.x] = mn;
         partials[gridDim.x + blockIdx.x] = mx;
     }
 }
 
-// Launched with one block of any multiple of 32 threads (<= 1024).
+// Launched with one block of any multiple of 32 threads (<= 1024).  Also
+// records in sc->numeric a NaN or infinity among the values (bit 2) and
+// rescale's "Maxval < 0" condition, max(x - min x) < 0 (bit 4,
+// src/eigen_utils.cpp:136-138).
 __global__ void minmax_finish_kernel(const double* __restrict__ partials, int nblk, SolverScalars* sc) {
     __shared__ float smn[32], smx[32];
     float mn = INFINITY, mx = -INFINITY;
     for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-        mn = fminf(mn, (float)partials[b]);
-        mx = fmaxf(mx, (float)partials[nblk + b]);
+        mn = nan_min(mn, (float)partials[b]);
+        mx = nan_max(mx, (float)partials[nblk + b]);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
-        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+        mn = nan_min(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = nan_max(mx, __shfl_down_sync(kFullMask, mx, o));
     }
     if ((threadIdx.x & 31) == 0) {
         smn[threadIdx.x >> 5] = mn;
@@ -175,12 +184,24 @@ __global__ void minmax_finish_kernel(const double* __restrict__ partials, int nb
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
-            mn = fminf(mn, smn[w]);
-            mx = fmaxf(mx, smx[w]);
+            mn = nan_min(mn, smn[w]);
+            mx = nan_max(mx, smx[w]);
         }
         sc->qmin = mn;
         sc->qmax = mx;
+        if (!(isfinite(mn) && isfinite(mx))) sc->numeric |= 2;
+        else if (fsub(mx, mn) < 0.0f) sc->numeric |= 4;
     }
+}
+
+// A NaN or infinity in a solver's inputs (the initial Q, the unaries):
+// sc->numeric |= 1, one atomicOr per block that saw one.
+__global__ void nonfinite_kernel(long n, const float* __restrict__ a, const float* __restrict__ b,
+                                 SolverScalars* sc) {
+    bool bad = false;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
+        bad |= !isfinite(a[t]) || !isfinite(b[t]);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&sc->numeric, 1);
 }
 
 // rescale (src/eigen_utils.cpp:120-141): out = (Q - min) / (max - min);
@@ -195,12 +216,44 @@ __global__ void rescale_kernel(long n, const float* __restrict__ Q, const Solver
     out[t] = v;
 }
 
-// expAndNormalize(-U) (src/densecrf.cpp:328-336).  expf is CUDA's; the
-// reference evaluates exp with Eigen's SSE packet polynomial, so results may
-// differ by an ulp.
+// Eigen 3.2's pexp<Packet4f> (Core/arch/SSE/MathFunctions.h:107-170) as
+// the reference's SSE2 build evaluates it, one lane: the Cephes
+// single-precision exp -- clamp to +-88.376, n = floor(x log2(e) + 1/2) by
+// truncation and correction, x - n C1 - n C2, the degree-5 polynomial by
+// Horner steps (pmadd is a separate multiply and add there, so each rounds),
+// times 2^n built in the exponent bits, then the max with the input.
+__device__ __forceinline__ float eigen_pexp(float x0) {
+    float x = x0 < 88.3762626647950f ? x0 : 88.3762626647950f;
+    x = x > -88.3762626647949f ? x : -88.3762626647949f;
+    float fx = fadd(fmul(x, 1.44269504088896341f), 0.5f);
+    float t = (float)(int)fx;
+    if (t > fx) t = fsub(t, 1.0f);
+    fx = t;
+    x = fsub(x, fmul(fx, 0.693359375f));
+    x = fsub(x, fmul(fx, -2.12194440e-4f));
+    const float z = fmul(x, x);
+    float y = 1.9875691500E-4f;
+    y = fadd(fmul(y, x), 1.3981999507E-3f);
+    y = fadd(fmul(y, x), 8.3334519073E-3f);
+    y = fadd(fmul(y, x), 4.1665795894E-2f);
+    y = fadd(fmul(y, x), 1.6666665459E-1f);
+    y = fadd(fmul(y, x), 5.0000001201E-1f);
+    y = fadd(fmul(y, z), x);
+    y = fadd(y, 1.0f);
+    const float r = fmul(y, __int_as_float(((int)fx + 0x7f) << 23));
+    return r > x0 ? r : x0;
+}
+
+// expAndNormalize(-U) (src/densecrf.cpp:321-336): Eigen evaluates
+// b.array().exp() with its packet exp over the aligned packets of four and
+// std::exp (libm expf, within 0.502 ulp) over the tail; the tail here is the
+// double-precision exp rounded once to float, which is the nearest float and
+// equals libm's except where the exact value lies within 0.002 ulp of a
+// rounding boundary.  The sum is Eigen's packet redux, then one division.
 template <int LC>
 __global__ void unary_init_kernel(int N, int Lrt, const float* __restrict__ U, float* __restrict__ Q) {
     const int L = LC ? LC : Lrt;
+    const int L4 = L & ~3;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
     float b[PixVec<LC>::S];
@@ -213,7 +266,10 @@ __global__ void unary_init_kernel(int N, int Lrt, const float* __restrict__ U, f
         if (k < L && b[k] > mx) mx = b[k];
 #pragma unroll
     for (int k = 0; k < PixVec<LC>::S; k++)
-        if (k < L) b[k] = expf(fsub(b[k], mx));
+        if (k < L) {
+            const float v = fsub(b[k], mx);
+            b[k] = k < L4 ? eigen_pexp(v) : (float)exp((double)v);
+        }
     const float s = vec_sum<LC>(b, L);
 #pragma unroll
     for (int k = 0; k < PixVec<LC>::S; k++)

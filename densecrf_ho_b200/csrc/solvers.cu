@@ -516,15 +516,15 @@ __global__ void lp_q_kernel(int N, int Lrt, float lambda, const float* __restric
                 const float x = fsub(fadd(fadd(fadd(alpha[e], beta), u[e]), gamma[e]), U[e]);
                 const float q = fadd(fmul(x, lambda), curQ[e]);
                 Q[e] = q;
-                mn = fminf(mn, q);
-                mx = fmaxf(mx, q);
+                mn = nan_min(mn, q);
+                mx = nan_max(mx, q);
             }
     }
     __shared__ float smn[32], smx[32];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
-        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+        mn = nan_min(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = nan_max(mx, __shfl_down_sync(kFullMask, mx, o));
     }
     if ((threadIdx.x & 31) == 0) {
         smn[threadIdx.x >> 5] = mn;
@@ -533,8 +533,8 @@ __global__ void lp_q_kernel(int N, int Lrt, float lambda, const float* __restric
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
-            mn = fminf(mn, smn[w]);
-            mx = fmaxf(mx, smx[w]);
+            mn = nan_min(mn, smn[w]);
+            mx = nan_max(mx, smx[w]);
         }
         partials[blockIdx.x] = mn;
         partials[gridDim.x + blockIdx.x] = mx;
@@ -641,8 +641,8 @@ __global__ void __launch_bounds__(32 * kTileWarps)
             const float q = fadd(fmul(t[k], lambda), rq[k]);
             rq[k] = q;
             if (act) {
-                mn = fminf(mn, q);
-                mx = fmaxf(mx, q);
+                mn = nan_min(mn, q);
+                mx = nan_max(mx, q);
             }
         }
         __syncwarp();
@@ -650,8 +650,8 @@ __global__ void __launch_bounds__(32 * kTileWarps)
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
-        mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
+        mn = nan_min(mn, __shfl_down_sync(kFullMask, mn, o));
+        mx = nan_max(mx, __shfl_down_sync(kFullMask, mx, o));
     }
     if (lane == 0) {
         smn[wib] = mn;
@@ -660,8 +660,8 @@ __global__ void __launch_bounds__(32 * kTileWarps)
     __syncthreads();
     if (threadIdx.x == 0) {
         for (int w = 1; w < kTileWarps; w++) {
-            mn = fminf(mn, smn[w]);
-            mx = fmaxf(mx, smx[w]);
+            mn = nan_min(mn, smn[w]);
+            mx = nan_max(mx, smx[w]);
         }
         partials[blockIdx.x] = mn;
         partials[gridDim.x + blockIdx.x] = mx;
@@ -1277,8 +1277,11 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
     launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, part);
     launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
     launch(qp_init_energy_kernel, 1, 1, 0, stream, sc, nt, max_iter);
+    launch(nonfinite_kernel, kRedBlocks, kRedThreads, 0, stream, NL, (const float*)Q, unary.get(), sc);
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
+    if (h_scal->numeric & 1)
+        throw Error(DCRF_E_NUMERIC, "qp: the initial Q or the unary energy holds a NaN or an infinity");
     // One Frank-Wolfe iteration (src/densecrf.cpp:389-436) and its stop test.
     auto qp_iter = [&]() {
         with_lc(L, [&](auto lc) {
@@ -1381,13 +1384,17 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
     const int tgrid = ceil_div(ceil_div(N, 32), kTileWarps);  // row-tiled kernels
 
     DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    DCRF_CUDA(cudaMemsetAsync(&sc->numeric, 0, sizeof(int), stream));
+    launch(nonfinite_kernel, kRedBlocks, kRedThreads, 0, stream, NL, (const float*)Q, unary.get(), sc);
     with_lc(L, [&](auto lc) {
         constexpr int LC = decltype(lc)::value;
         launch(renormalize_kernel<LC>, pg, kPix, 0, stream, N, L, Q);
     });
     DCRF_CUDA(cudaMemcpyAsync(bestQ, Q, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
     current_map(Q, lab);
-    double int_energy = energy_true(lab, true);
+    double int_energy = energy_true(lab, true);  // reads the scalars back
+    if (h_scal->numeric & 1)
+        throw Error(DCRF_E_NUMERIC, "lp: the initial Q or the unary energy holds a NaN or an infinity");
     double energy = energy_lp(Q);
     if (energy > int_energy) {
         with_lc(L, [&](auto lc) {
@@ -1630,7 +1637,12 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             launch(lp_project_kernel<LC>, pg, kPix, 0, stream, N, L, Q, lab);
         });
         const double prev_int_energy = int_energy;
-        int_energy = energy_true(lab, true);
+        int_energy = energy_true(lab, true);  // reads the scalars back
+        // rescale() of an iterate: the reference throws (src/eigen_utils.cpp:138)
+        // and the LP rethrows it (src/densecrf.cpp:698-703); a NaN or infinity,
+        // which the reference would carry on with, ends the solve too.
+        if (h_scal->numeric & 4) throw Error(DCRF_E_NUMERIC, "Maxval < 0, skipping");
+        if (h_scal->numeric & 2) throw Error(DCRF_E_NUMERIC, "lp: an iterate holds a NaN or an infinity");
         if (p.best_int) {
             if (std::abs(int_energy - prev_int_energy) < p.prox_energy_tol) ++count;
             else count = 0;

@@ -37,7 +37,8 @@ typedef enum {
     DCRF_E_RANGE = 3,   /* "Value out of bounds" (src/pairwise.cpp:218-219)      */
     DCRF_E_STATE = 4,   /* call order (e.g. solve before set_unary)              */
     DCRF_E_NOMEM = 5,   /* device allocation failed                              */
-    DCRF_E_NUMERIC = 6, /* "Maxval < 0, skipping" (src/eigen_utils.cpp:138)      */
+    DCRF_E_NUMERIC = 6, /* "Maxval < 0, skipping" (src/eigen_utils.cpp:138), or a
+                           NaN / infinity in a solver's input or iterate        */
     DCRF_E_TIMEOUT = 7  /* a bounded device loop hit its iteration cap           */
 } dcrf_status;
 
@@ -49,6 +50,14 @@ typedef struct dcrf_model_s* dcrf_model;
  * the environment); this hands every cached block back to the driver.  No
  * counterpart in the reference, which allocates on the host. */
 dcrf_status dcrf_release_cached_memory(void);
+/* A budget on the device memory the library holds for live models, lattices
+ * and batches (bytes; 0 = none, the default).  A request beyond it fails with
+ * DCRF_E_NOMEM before any device call.  No counterpart in the reference. */
+dcrf_status dcrf_set_device_memory_limit(uint64_t bytes);
+/* Bytes held by live models / lattices / batches, bytes kept in the cache,
+ * and the number of cudaMalloc calls the library has made (any may be NULL).
+ * No counterpart in the reference. */
+dcrf_status dcrf_device_memory_stats(uint64_t* in_use, uint64_t* cached, uint64_t* mallocs);
 
 const char* dcrf_last_error(void);
 /* Library version string. */
@@ -368,6 +377,15 @@ dcrf_status dcrf_batch_qp(dcrf_batch b, const float* init, float* out,
 dcrf_status dcrf_batch_qp_dev(dcrf_batch b, const float* d_init, float* d_out,
                               const dcrf_qp_params* params, dcrf_solve_stats* stats);
 dcrf_status dcrf_batch_stream(dcrf_batch b, void** stream);
+/* PairwisePotential::apply (src/pairwise.cpp:203-208) of pairwise term k on
+ * every image at once, over the term's concatenated lattice:
+ * out = -w_k n o K(n o in), device arrays [sum N_i][L] on the batch's stream.
+ * Each image's rows equal its single-image dcrf_model_pairwise_apply, bit for
+ * bit (no splat list, blur neighbour or slice crosses an image). */
+dcrf_status dcrf_batch_pairwise_apply(dcrf_batch b, int k, float* out, const float* in);
+dcrf_status dcrf_batch_pairwise_apply_dev(dcrf_batch b, int k, float* d_out, const float* d_in);
+/* Vertex count of term k's concatenated lattice (the sum of the images' M). */
+dcrf_status dcrf_batch_lattice_size(dcrf_batch b, int k, int64_t* M);
 
 /* ---- Differentiation: unrolled mean-field and its adjoint ----------------
  * No counterpart in the reference, whose solvers are not differentiable
@@ -391,6 +409,17 @@ dcrf_status dcrf_batch_meanfield_backward_dev(dcrf_batch b, const float* d_grad_
 /* Potts weight of pairwise term k (the PottsCompatibility parameter,
  * src/labelcompatibility.cpp:68-70), and the number of terms. */
 dcrf_status dcrf_batch_set_weight(dcrf_batch b, int k, float w_potts);
+/* Checkpointing of meanfield / meanfield_backward: the forward pass keeps
+ * Q_t for t a multiple of checkpoint_every and Q_T (1 = every iterate, the
+ * default); the backward pass recomputes the others segment by segment from
+ * the checkpoint before them.  recompute_lattice != 0: the terms' lattices
+ * are released at the end of each pass and rebuilt from the features by the
+ * next (the backward pass rebuilds them before its first filter).  Results
+ * do not depend on either setting: every recomputed value is computed by the
+ * same kernels from the same inputs. */
+dcrf_status dcrf_batch_set_checkpointing(dcrf_batch b, int checkpoint_every, int recompute_lattice);
+/* Device bytes the checkpoints and recompute buffers take for T iterations. */
+dcrf_status dcrf_batch_meanfield_state_bytes(dcrf_batch b, int T, uint64_t* bytes);
 dcrf_status dcrf_batch_terms(dcrf_batch b, int* n_terms);
 
 #ifdef __cplusplus

@@ -17,8 +17,8 @@
  *   - energies src/densecrf.cpp:844-957, 982-1037.
  * Eigen 3.2 reductions are restated with their SSE2 packet order
  * (Core/Redux.h LinearVectorizedTraversal, Packet4f / Packet2d) so results
- * are bit-identical to the reference, except unary_init, whose exp() the
- * reference evaluates with Eigen's packet exp (we call expf).
+ * are bit-identical to the reference, unary_init included (Eigen's packet
+ * exp restated, eigen_pexp).
  *
  * Compiled with -ffp-contract=off so no multiply-add is fused.
  */
@@ -604,9 +604,48 @@ void orc_model_set_cliques(orc_model* m, int R, const int* offsets, const int* i
 
 int orc_model_lattice_M(const orc_model* m, int k) { return m->terms[k].lat->M; }
 
-/* expAndNormalize(-U) (src/densecrf.cpp:321-336). */
+/* Eigen 3.2's pexp<Packet4f> (include/Eigen/src/Core/arch/SSE/MathFunctions.h:
+ * 107-170) as the reference's x86-64 SSE2 build evaluates it, one lane: the
+ * Cephes single-precision exp -- clamp to +-88.376, n = floor(x log2(e) +
+ * 1/2) by truncation and correction, x - n C1 - n C2, the degree-5
+ * polynomial by Horner steps, times 2^n assembled in the exponent bits, and
+ * the max with the input.  pmadd is a separate multiply and add on SSE2, so
+ * every product and sum rounds on its own (this file is compiled without
+ * contraction); _mm_min_ps / _mm_max_ps return their second operand when the
+ * comparison fails. */
+static float eigen_pexp(float x0) {
+    float x = x0 < 88.3762626647950f ? x0 : 88.3762626647950f;
+    x = x > -88.3762626647949f ? x : -88.3762626647949f;
+    float fx = x * 1.44269504088896341f;
+    fx = fx + 0.5f;
+    float t = (float)(int)fx;
+    if (t > fx) t = t - 1.0f;
+    fx = t;
+    const float a = fx * 0.693359375f, c = fx * -2.12194440e-4f;
+    x = x - a;
+    x = x - c;
+    const float z = x * x;
+    float y = 1.9875691500E-4f;
+    y = y * x + 1.3981999507E-3f;
+    y = y * x + 8.3334519073E-3f;
+    y = y * x + 4.1665795894E-2f;
+    y = y * x + 1.6666665459E-1f;
+    y = y * x + 5.0000001201E-1f;
+    y = y * z + x;
+    y = y + 1.0f;
+    const int bits = ((int)fx + 0x7f) << 23;
+    float p2;
+    memcpy(&p2, &bits, sizeof p2);
+    const float r = y * p2;
+    return r > x0 ? r : x0;
+}
+
+/* expAndNormalize(-U) (src/densecrf.cpp:321-336).  b.array().exp() on a
+ * VectorXf runs Eigen's packet exp over the aligned packets of four and
+ * std::exp (libm expf) over the remaining tail; the sum is Eigen's packet
+ * redux. */
 void orc_unary_init(const orc_model* m, float* Q) {
-    const int L = m->L;
+    const int L = m->L, L4 = L & ~3;
     float* b = (float*)malloc(sizeof(float) * L);
     for (int i = 0; i < m->N; i++) {
         float mx = -FLT_MAX;
@@ -614,7 +653,7 @@ void orc_unary_init(const orc_model* m, float* Q) {
             b[k] = -m->unary[(size_t)i * L + k];
             if (k == 0 || b[k] > mx) mx = b[k];
         }
-        for (int k = 0; k < L; k++) b[k] = expf(b[k] - mx);
+        for (int k = 0; k < L; k++) b[k] = k < L4 ? eigen_pexp(b[k] - mx) : expf(b[k] - mx);
         float s = eig_sum_f(b, L, 0);
         for (int k = 0; k < L; k++) Q[(size_t)i * L + k] = b[k] / s;
     }

@@ -104,3 +104,19 @@ def test_batch_single_image_and_errors():
     with pytest.raises(DCRFError) as e:
         nb.qp_inference_super_pixels_non_convex(np.zeros((80, 21), np.float32))
     assert e.value.code == 4
+
+
+def test_batch_pairwise_apply_equals_single_applies():
+    """PairwisePotential::apply over the concatenated lattice of each term:
+    every image's rows equal its own single-image apply, bit for bit."""
+    imgs = _images(SIZES, 40)
+    b = _batch(SIZES, imgs)
+    x = np.random.default_rng(4).random((b.N, 21)).astype(np.float32)
+    for k in range(2):
+        out = b.pairwise_apply(k, x)
+        Ms = 0
+        for i, ((w, h), im) in enumerate(zip(SIZES, imgs)):
+            m = _single(w, h, im)
+            assert np.array_equal(b.split(out)[i], m.pairwise_apply(k, b.split(x)[i])), (k, i)
+            Ms += m.lattice_size(k)
+        assert b.lattice_size(k) == Ms

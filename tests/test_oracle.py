@@ -1,10 +1,13 @@
 """The CPU oracle (our C restatement) pinned against the reference.
 
 Every check is bit-exact (``np.array_equal``): the restatement follows the
-reference's float operation order, including Eigen's SSE2 reduction order.
-Only ``unary_init`` differs (the reference evaluates exp with Eigen's packet
-polynomial): there the bound is 8 ulp.
+reference's float operation order, including Eigen's SSE2 reduction order and
+its packet exp in ``unary_init``.
 """
+import hashlib
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -47,8 +50,7 @@ def test_model_pinned_to_golden(name, oracle_mod):
     g = golden(name)
     m = _oracle_model(oracle_mod, g)
     Q = g["unary_init"]  # the reference's own initialisation
-    ulp = np.abs(m.unary_init().view(np.int32) - Q.view(np.int32)).max()
-    assert ulp <= 8  # expf vs Eigen's packet exp, then one division
+    assert _bits_equal(m.unary_init(), Q)
     rq = (Q - Q.min()) / (Q - Q.min()).max()
     for k in range(2):
         assert _bits_equal(m.apply(k, Q), g[f"apply{k}"])
@@ -193,3 +195,17 @@ def test_per_pixel_energies_pinned_to_golden(oracle_mod):
     assert _bits_equal(O.max_rounding(g["Q"]), g["maxround"])
     # compute_LR_QP_value(Q, diag_dom): double sums in Eigen's packet order
     assert O.lr_qp_value_diag(m, img["unary"], g["Q"], g["dd"]) == float(g["lrqp_dd"])
+
+
+@pytest.mark.parametrize("record,W,H,L", [("qp_320x240_seed1.json", 320, 240, 21),
+                                          ("lp_640x480_seed2.json", 640, 480, 21)])
+def test_unary_init_of_the_benchmark_images_pinned(record, W, H, L, oracle_mod):
+    """The restated expAndNormalize (Eigen's packet exp over the aligned
+    packets, libm expf over the tail, the packet-order sum) gives the very
+    bytes the reference started its recorded full-size solves from."""
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, record)) as f:
+        rec = json.load(f)
+    img = synth.make_image(W, H, L, rec["seed"])
+    Q = oracle_mod.build_model(oracle_mod.OracleModel, img).unary_init()
+    assert hashlib.sha256(Q.tobytes()).hexdigest() == rec["init_sha256"]

@@ -18,6 +18,17 @@ pytestmark = pytest.mark.gpu
 ENERGY_RTOL = 1e-4
 
 
+def unary_init_close(got, ref):
+    """The GPU's expAndNormalize against the reference's: Eigen's packet exp
+    is restated exactly, the tail label's libm expf is replaced by the
+    correctly rounded exp, which differs from libm's in about 0.06 % of
+    values, by one ulp; a pixel where that happens may then differ by an ulp
+    or two after the division by its sum.  Every other pixel is bit-exact."""
+    got, ref = np.asarray(got), np.asarray(ref)
+    d = np.abs(got.view(np.int32).astype(np.int64) - ref.view(np.int32))
+    return d.max() <= 2 and (d.max(axis=1) > 0).mean() <= 0.005
+
+
 def _eq(a, b):
     return np.array_equal(np.asarray(a), np.asarray(b))
 
@@ -38,7 +49,7 @@ def test_model_against_reference_golden(name):
     g = golden(name)
     m = gpu_model(g)
     Q = g["unary_init"]
-    assert np.abs(m.unary_init().view(np.int32) - Q.view(np.int32)).max() <= 8
+    assert unary_init_close(m.unary_init(), Q)
     rq = (Q - Q.min()) / (Q - Q.min()).max()
     for k in range(2):
         assert _eq(m.pairwise_apply(k, Q), g[f"apply{k}"])
@@ -108,8 +119,11 @@ def test_state_and_argument_errors():
 def test_lp_full_size_bit_exact_to_reference(oracle_mod):
     """The benchmark workload itself: 640x480, 21 labels, 50 proximal
     iterations (500 Frank-Wolfe steps).  The GPU solve must reproduce the
-    reference's output bit for bit (SHA-256 of Q recorded from the bit-exact
-    CPU restatement by tests/golden/make_full_size.py)."""
+    reference's output bit for bit: SHA-256 of Q, iteration count and integer
+    energy recorded from the stock reference (oracle/_ref, compiled from the
+    reference's sources) by tests/golden/make_config_goldens.py lp640.  The
+    initial Q is the oracle's restated unary_init, equal to the reference's
+    bytes (its hash is in the record too)."""
     import hashlib
     import json
     import os
@@ -126,6 +140,7 @@ def test_lp_full_size_bit_exact_to_reference(oracle_mod):
     out, st = m.lp_inference_prox_super_pixels(Q, stats=True, prox_max_iter=rec["prox_max_iter"],
                                                prox_energy_tol=rec["prox_energy_tol"])
     assert st.iterations == rec["prox_iters"]
+    assert unary_init_close(m.unary_init(), Q)
     assert hashlib.sha256(out.tobytes()).hexdigest() == rec["q_sha256"]
     assert m.assignment_energy_true(m.currentMap(out)) == pytest.approx(rec["energy_true"], rel=1e-12)
 
@@ -211,8 +226,8 @@ def test_label_compatibilities_vs_reference(name):
             return _eq(a, b)
         return np.abs(a - b).max() <= tol * np.abs(b).max()
 
-    Q = g["unary_init"]   # the reference's exp: unary_init itself agrees to a few ulp
-    assert np.abs(m.unary_init().view(np.int32) - Q.view(np.int32)).max() <= 8
+    Q = g["unary_init"]   # the reference's own initialisation
+    assert unary_init_close(m.unary_init(), Q)
     rq = (Q - Q.min()) / (Q - Q.min()).max()
     for k in range(2):
         assert close(m.pairwise_apply(k, Q), g[f"apply{k}"]), k
