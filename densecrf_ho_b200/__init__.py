@@ -384,6 +384,31 @@ class DenseCRF2D:
                                   C.byref(p), C.byref(st)))
         return (out, st) if stats else out
 
+    def addSuperPixel(self, rgb, spatial_radius, range_radius, min_region_count, constant, normaliser):
+        """``DenseCRF2D::addSuperPixel`` (src/densecrf.cpp:193-251): mean-shift
+        regions of ``rgb`` (EDISON's segmentation, the mode search on the GPU)
+        appended as cliques; returns the number of regions added."""
+        im = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1)
+        if im.size != 3 * self.N:
+            raise DCRFError(1, "rgb must hold 3 bytes per pixel")
+        n = C.c_int()
+        check(lib().dcrf_model_add_superpixel(self._h, im.ctypes.data_as(C.c_void_p), int(spatial_radius),
+                                              int(range_radius), int(min_region_count), C.c_float(constant),
+                                              C.c_float(normaliser), C.byref(n)))
+        return n.value
+
+    def getCliques(self):
+        """The cliques the model holds: ``(offsets, idx, exp_weight, constants)``."""
+        R, T = C.c_int(), C.c_int()
+        check(lib().dcrf_model_clique_info(self._h, C.byref(R), C.byref(T)))
+        off = np.zeros(R.value + 1, np.int32)
+        idx = np.zeros(max(T.value, 1), np.int32)
+        ew = np.zeros(max(R.value, 1), np.float32)
+        cs = np.zeros(max(R.value, 1), np.float32)
+        check(lib().dcrf_model_get_cliques(self._h, off.ctypes.data_as(C.c_void_p), idx.ctypes.data_as(C.c_void_p),
+                                           ew.ctypes.data_as(C.c_void_p), cs.ctypes.data_as(C.c_void_p)))
+        return off, idx[:T.value], ew[:R.value], cs[:R.value]
+
     def lp_inference_prox_super_pixels(self, init, params=None, stats=False, **kw):
         x = self._mat(init)
         out = self._new()
@@ -615,3 +640,33 @@ def device_memory_stats():
 
 
 __all__ += ["set_device_memory_limit", "device_memory_stats"]
+
+
+def meanshift_segment(rgb, W, H, spatial_radius, range_radius, min_region_count):
+    """EDISON's mean-shift segmentation (the step addSuperPixel runs):
+    ``(labels int32 [W*H], n_regions)``."""
+    im = np.ascontiguousarray(rgb, dtype=np.uint8).reshape(-1)
+    if im.size != 3 * W * H:
+        raise DCRFError(1, "rgb must hold 3 bytes per pixel")
+    lab = np.empty(W * H, np.int32)
+    n = C.c_int()
+    check(lib().dcrf_meanshift_segment(im.ctypes.data_as(C.c_void_p), int(W), int(H), int(spatial_radius),
+                                       C.c_float(range_radius), int(min_region_count),
+                                       lab.ctypes.data_as(C.c_void_p), C.byref(n)))
+    return lab, n.value
+
+
+def meanshift_regions(filtered, W, H, range_radius, min_region_count):
+    """The region steps alone (host, no GPU) from a filtered L*u*v* image
+    ``[W*H, 3]``: ``(labels, n_regions)``."""
+    f = np.ascontiguousarray(filtered, dtype=np.float32).reshape(-1)
+    if f.size != 3 * W * H:
+        raise DCRFError(1, "filtered must hold 3 floats per pixel")
+    lab = np.empty(W * H, np.int32)
+    n = C.c_int()
+    check(lib().dcrf_meanshift_regions(f.ctypes.data_as(C.c_void_p), int(W), int(H), C.c_float(range_radius),
+                                       int(min_region_count), lab.ctypes.data_as(C.c_void_p), C.byref(n)))
+    return lab, n.value
+
+
+__all__ += ["meanshift_segment", "meanshift_regions"]

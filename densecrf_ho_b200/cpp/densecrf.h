@@ -11,10 +11,10 @@
 //
 // Scope (the B200 path): Potts, Diagonal and Matrix compatibilities, every
 // KernelType and NormalizationType (and the NO_NORMALIZATION copy), constant unaries, the
-// qp / lp / qp_sp / lp_sp solvers.  Superpixel cliques are given as a
-// per-pixel region map (addSuperPixel's segmentation step, EDISON mean-shift,
-// stays with the caller); the clique weights are derived from the image
-// exactly as src/densecrf.cpp:212-247 does.
+// qp / lp / qp_sp / lp_sp solvers.  addSuperPixel keeps the reference's
+// signature: the engine runs EDISON's mean-shift segmentation itself (the
+// mode search on the GPU) and derives the clique weights as
+// src/densecrf.cpp:212-247 does; an overload also takes a caller's region map.
 //
 // Header-only; needs Eigen (the reference vendors 3.2.7) and include/dcrf.h.
 #pragma once
@@ -340,6 +340,19 @@ protected:
     std::vector<int> cl_off_{0}, cl_idx_;
     std::vector<float> cl_exp_, cl_const_;
     DenseCRF(DenseCRF&) = delete;
+    // The model's cliques back into the host copies (after the engine
+    // appended some).
+    void pull_cliques() {
+        int R = 0, total = 0;
+        dcrf_shim::check(dcrf_model_clique_info(m_, &R, &total));
+        cl_off_.assign(R + 1, 0);
+        cl_idx_.assign(total, 0);
+        cl_exp_.assign(R, 0.0f);
+        cl_const_.assign(R, 0.0f);
+        dcrf_shim::check(dcrf_model_get_cliques(m_, cl_off_.data(), cl_idx_.data(), cl_exp_.data(),
+                                                cl_const_.data()));
+        R_ = R;
+    }
     void push_cliques() {
         dcrf_shim::check(dcrf_model_set_cliques(m_, R_, cl_off_.data(), cl_idx_.empty() ? nullptr : cl_idx_.data(),
                                                 cl_exp_.data(), cl_const_.data()));
@@ -444,6 +457,15 @@ public:
         double e = 0;
         dcrf_shim::check(dcrf_model_lr_qp_value_diag(m_, Q.data(), diag_dom.size() ? diag_dom.data() : nullptr, &e));
         return e;
+    }
+    // addSuperPixel (include/densecrf.h:190, src/densecrf.cpp:193-251):
+    // mean-shift regions of img at the given radii, each appended as a clique.
+    void addSuperPixel(unsigned char* img, int spatial_radius, int range_radius, int min_region_count,
+                       float constant, float normaliser) {
+        int reg = 0;
+        dcrf_shim::check(dcrf_model_add_superpixel(m_, img, spatial_radius, range_radius, min_region_count,
+                                                   constant, normaliser, &reg));
+        pull_cliques();
     }
     // The clique state addSuperPixel leaves behind (src/densecrf.cpp:212-247),
     // from a segmentation computed by the caller: region_of_pixel[i] in

@@ -5,6 +5,7 @@
 #include <string>
 
 #include "batch.cuh"
+#include "meanshift.cuh"
 #include "model.cuh"
 
 using dcrf::DevBuf;
@@ -547,6 +548,100 @@ dcrf_status dcrf_model_set_cliques(dcrf_model h, int R, const int32_t* offsets, 
         }
         static const int zero = 0;
         m.set_cliques(R, R > 0 ? offsets : &zero, idx, exp_weight, constants);
+    });
+}
+
+dcrf_status dcrf_model_add_superpixel(dcrf_model h, const uint8_t* rgb, int spatial_radius, int range_radius,
+                                      int min_region_count, float constant, float normaliser, int* n_regions) {
+    return guard([&] {
+        auto& m = M(h);
+        need(rgb, "rgb");
+        std::vector<int> labels(m.N);
+        const int reg = dcrf::meanshift_segment(rgb, m.W, m.H, spatial_radius, (float)range_radius,
+                                                min_region_count, labels.data(), m.stream);
+        std::vector<int> off, idx;
+        std::vector<float> ew, cs;
+        dcrf::superpixel_cliques(rgb, labels.data(), m.N, reg, m.R, constant, normaliser, off, idx, ew, cs);
+        // appended after the cliques the model holds, as the reference's R_,
+        // super_pixel_container_ and weight vectors grow
+        std::vector<int> all_off(m.h_cl_off.empty() ? std::vector<int>{0} : m.h_cl_off);
+        std::vector<int> all_idx(m.h_cl_idx);
+        std::vector<float> all_ew(m.h_cl_exp), all_cs(m.h_cl_const);
+        const int base = all_off.back();
+        for (int r = 0; r < reg; r++) all_off.push_back(base + off[r + 1]);
+        all_idx.insert(all_idx.end(), idx.begin(), idx.end());
+        all_ew.insert(all_ew.end(), ew.begin(), ew.end());
+        all_cs.insert(all_cs.end(), cs.begin(), cs.end());
+        m.set_cliques(m.R + reg, all_off.data(), all_idx.data(), all_ew.data(), all_cs.data());
+        if (n_regions) *n_regions = reg;
+    });
+}
+
+dcrf_status dcrf_model_clique_info(dcrf_model h, int* R, int* total) {
+    return guard([&] {
+        auto& m = M(h);
+        if (R) *R = m.R;
+        if (total) *total = m.R ? m.h_cl_off[m.R] : 0;
+    });
+}
+
+dcrf_status dcrf_model_get_cliques(dcrf_model h, int32_t* offsets, int32_t* idx, float* exp_weight,
+                                   float* constants) {
+    return guard([&] {
+        auto& m = M(h);
+        if (offsets) {
+            if (m.R) std::memcpy(offsets, m.h_cl_off.data(), sizeof(int) * (m.R + 1));
+            else offsets[0] = 0;
+        }
+        if (m.R == 0) return;
+        if (idx) std::memcpy(idx, m.h_cl_idx.data(), sizeof(int) * m.h_cl_off[m.R]);
+        if (exp_weight) std::memcpy(exp_weight, m.h_cl_exp.data(), sizeof(float) * m.R);
+        if (constants) std::memcpy(constants, m.h_cl_const.data(), sizeof(float) * m.R);
+    });
+}
+
+namespace {
+// A stream for the model-less mean-shift calls, destroyed on every path.
+struct OwnStream {
+    cudaStream_t s = nullptr;
+    OwnStream() { DCRF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)); }
+    ~OwnStream() {
+        if (s) cudaStreamDestroy(s);
+    }
+};
+}  // namespace
+
+dcrf_status dcrf_meanshift_filter(const uint8_t* rgb, int W, int H, int spatial_radius, float range_radius,
+                                  float* filtered) {
+    return guard([&] {
+        need(rgb, "rgb");
+        need(filtered, "filtered");
+        check_device();
+        OwnStream st;
+        dcrf::meanshift_filter(rgb, W, H, spatial_radius, range_radius, filtered, st.s);
+    });
+}
+
+dcrf_status dcrf_meanshift_regions(const float* filtered, int W, int H, float range_radius, int min_region_count,
+                                   int32_t* labels, int* n_regions) {
+    return guard([&] {
+        need(filtered, "filtered");
+        need(labels, "labels");
+        const int reg = dcrf::meanshift_regions(filtered, W, H, range_radius, min_region_count, labels);
+        if (n_regions) *n_regions = reg;
+    });
+}
+
+dcrf_status dcrf_meanshift_segment(const uint8_t* rgb, int W, int H, int spatial_radius, float range_radius,
+                                   int min_region_count, int32_t* labels, int* n_regions) {
+    return guard([&] {
+        need(rgb, "rgb");
+        need(labels, "labels");
+        check_device();
+        OwnStream st;
+        const int reg = dcrf::meanshift_segment(rgb, W, H, spatial_radius, range_radius, min_region_count, labels,
+                                                st.s);
+        if (n_regions) *n_regions = reg;
     });
 }
 

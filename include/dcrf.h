@@ -236,6 +236,39 @@ dcrf_status dcrf_model_pairwise_set_kernel_parameters(dcrf_model m, int k, const
 #define DCRF_COMPAT_DIAGONAL 1
 #define DCRF_COMPAT_MATRIX 2
 dcrf_status dcrf_model_set_compat(dcrf_model m, int k, int kind, const float* params);
+/* DenseCRF2D::addSuperPixel(img, spatial_radius, range_radius,
+ * min_region_count, constant, normaliser) (include/densecrf.h:190,
+ * src/densecrf.cpp:193-251): mean-shift segmentation of the model's W x H
+ * image rgb (host, pixel-major RGB bytes) as EDISON's Segment(spatial_radius,
+ * range_radius, min_region_count, NO_SPEEDUP) computes it
+ * (src/mean-shift/msImageProcessor.cpp:714), then one clique per region with
+ * the reference's weight constant * exp(-sd / (normaliser * count)), appended
+ * after the cliques already set.  n_regions (may be NULL): the regions
+ * added. */
+dcrf_status dcrf_model_add_superpixel(dcrf_model m, const uint8_t* rgb, int spatial_radius, int range_radius,
+                                      int min_region_count, float constant, float normaliser, int* n_regions);
+/* The segmentation step alone (msImageProcessor::DefineImage(rgb, COLOR, H,
+ * W); Segment(...); GetRegions, src/mean-shift/msImageProcessor.cpp:158,
+ * 714, 1122): labels (host, W*H) receives every pixel's region, numbered from
+ * 0 in EDISON's order; n_regions the count. */
+dcrf_status dcrf_meanshift_segment(const uint8_t* rgb, int W, int H, int spatial_radius, float range_radius,
+                                   int min_region_count, int32_t* labels, int* n_regions);
+/* Its two halves: the mean-shift filtered L*u*v* colour of every pixel
+ * (filtered, host W*H*3 floats: EDISON's msRawData after Filter, :353; the
+ * mode search runs on the GPU), and the region steps on the host from such
+ * a filtered image (Connect, TransitiveClosure as Segment repeats it, Prune:
+ * :1166, :1600, :1985), which need no GPU. */
+dcrf_status dcrf_meanshift_filter(const uint8_t* rgb, int W, int H, int spatial_radius, float range_radius,
+                                  float* filtered);
+dcrf_status dcrf_meanshift_regions(const float* filtered, int W, int H, float range_radius,
+                                   int min_region_count, int32_t* labels, int* n_regions);
+/* The clique state the model holds (the reference's super_pixel_container_,
+ * exp_of_superpixels_ and constants_, include/densecrf.h:78-94): first the
+ * count R and total pixel entries, then the arrays (offsets R+1, idx total,
+ * exp_weight R, constants R; any may be NULL). */
+dcrf_status dcrf_model_clique_info(dcrf_model m, int* R, int* total);
+dcrf_status dcrf_model_get_cliques(dcrf_model m, int32_t* offsets, int32_t* idx, float* exp_weight,
+                                   float* constants);
 /* The clique state that addSuperPixel (src/densecrf.cpp:193-251) leaves in
  * super_pixel_container_, exp_of_superpixels_ and constants_, supplied
  * directly: R cliques, pixel ids idx[offsets[r] .. offsets[r+1]), their

@@ -170,6 +170,8 @@ def ref_lib():
             getattr(L, fn).argtypes = [vp, _f32p]
         L.refm_apply_bf.argtypes = [vp, C.c_int, C.c_int, _f32p, _f32p]
         L.refm_apply_sorted.argtypes = [vp, C.c_int, C.c_int, C.c_int, _f32p, _i32p, vp]
+        L.refms_filter.argtypes = [_u8p, C.c_int, C.c_int, C.c_int, C.c_float, _f32p]
+        L.refms_segment.argtypes = [_u8p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, _i32p]
         L.ref_last_error.restype = C.c_char_p
         _rlib = L
     return _rlib
@@ -545,6 +547,20 @@ class ReferenceModel(_Model):
         if rc != 0:
             raise RuntimeError(self._lib.ref_last_error().decode())
         return out, None
+
+
+def ref_meanshift_filter(rgb, W, H, spatial, rng):
+    """EDISON's filtered L*u*v* image (reference, Filter NO_SPEEDUP)."""
+    out = np.zeros((W * H, 3), np.float32)
+    ref_lib().refms_filter(_c(rgb, np.uint8).copy(), W, H, spatial, C.c_float(rng), out)
+    return out
+
+
+def ref_meanshift_segment(rgb, W, H, spatial, rng, min_region):
+    """EDISON's region labels (reference, Segment NO_SPEEDUP) and count."""
+    lab = np.zeros(W * H, np.int32)
+    n = ref_lib().refms_segment(_c(rgb, np.uint8).copy(), W, H, spatial, C.c_float(rng), min_region, lab)
+    return lab, n
 
 
 def build_model(cls, img, gaussian=(3.0, 3.0), bilateral=(50.0, 15.0, 5.0)):

@@ -19,6 +19,7 @@
 
 #include "densecrf.h"
 #include "probimage.h"
+#include "msImageProcessor.h"
 
 #include <cmath>
 #include <netinet/in.h>
@@ -510,6 +511,25 @@ int ref_load_unary(const char* path, float* out, int* W, int* H, int* D) {
                 for (int k = 0; k < t.depth(); k++)
                     out[((size_t)i * t.width() + j) * t.depth() + k] = -log(t(j, i, k));
     return 0;
+}
+
+// EDISON's mean shift as addSuperPixel drives it (src/densecrf.cpp:206-210):
+// the filtered L*u*v* image of Filter(spatial, range, NO_SPEEDUP), and the
+// region labels of Segment(spatial, range, min_region, NO_SPEEDUP).
+void refms_filter(unsigned char* rgb, int W, int H, int sr, float rr, float* out) {
+    msImageProcessor p;
+    p.DefineImage(rgb, COLOR, H, W);
+    p.Filter(sr, rr, NO_SPEEDUP);
+    p.GetRawData(out);
+}
+int refms_segment(unsigned char* rgb, int W, int H, int sr, float rr, int minreg, int* labels) {
+    msImageProcessor p;
+    p.DefineImage(rgb, COLOR, H, W);
+    p.Segment(sr, rr, minreg, NO_SPEEDUP);
+    std::vector<int> lab;
+    const int n = p.GetRegions(lab);
+    std::memcpy(labels, lab.data(), sizeof(int) * lab.size());
+    return n;
 }
 
 }  // extern "C"

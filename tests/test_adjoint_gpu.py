@@ -18,6 +18,12 @@ pytestmark = pytest.mark.gpu
 
 GAUSS = (3.0, 3.0)
 BILAT = (50.0, 15.0, 5.0)
+# Gradient bound against FP64 finite differences: relative per coordinate,
+# with coordinates whose finite difference is below ADJOINT_FLOOR of the
+# largest measured against that floor instead (an FP32 forward carries
+# absolute errors of a few 1e-8 of the largest gradient).
+ADJOINT_RTOL = 1e-4
+ADJOINT_FLOOR = 1e-2
 
 
 def _setup(sizes, L, seed):
@@ -139,6 +145,67 @@ def test_meanfield_gradient_vs_fp64_finite_differences(oracle_mod):
         wm[k] -= h
         fdw = (f(U64, wp) - f(U64, wm)) / (2 * h)
         assert abs(gw[k] - fdw) <= 1e-3 * abs(fdw) + 1e-6, (k, gw[k], fdw)
+
+
+def _fd_at(ref, U64, c, T, w0, flat, h):
+    """FP64 central differences of loss = sum(c o Q_T) at the flat unary
+    coordinates, each on the image it belongs to alone (the others do not
+    move), the two forwards subtracted element by element before the sum.
+    The oracle's filter runs outside the GIL, so threads share the work."""
+    import concurrent.futures as cf
+    import os
+    L = U64.shape[1]
+
+    def one(idx):
+        i = int(np.searchsorted(ref.off, idx // L, side="right") - 1)
+        a, b = ref.off[i], ref.off[i + 1]
+        sub = FP64MeanField.__new__(FP64MeanField)
+        sub.sizes, sub.terms, sub.off = ref.sizes[i:i + 1], ref.terms[i:i + 1], np.array([0, b - a])
+        Up, Um = U64[a:b].copy(), U64[a:b].copy()
+        Up.flat[idx - a * L] += h
+        Um.flat[idx - a * L] -= h
+        return float((c[a:b] * (sub.run(Up, w0, T) - sub.run(Um, w0, T))).sum()) / (2 * h)
+
+    with cf.ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        return np.array(list(ex.map(one, flat)))
+
+
+def test_meanfield_gradient_21_labels_128x128_vs_fp64_finite_differences(oracle_mod):
+    """The stated check at a realistic size: 21 labels, a 128x128 image and
+    a 26x19 one in the batch, 256 random unary coordinates, FP64 central
+    differences with step 1e-6 (forward in FP64 with the oracle's FP64
+    filter on the same lattices), and each Potts weight.  The GPU forward is
+    FP32; ADJOINT_RTOL / ADJOINT_FLOOR give the bound."""
+    import torch
+    sizes = [(128, 128), (26, 19)]
+    L, T = 21, 10
+    b, U, imgs = _setup(sizes, L, 3)
+    c = np.random.default_rng(0).standard_normal(U.shape)
+    Ut = torch.from_numpy(U).cuda().requires_grad_(True)
+    Q = _torch_meanfield().apply(Ut, b, T)
+    (torch.from_numpy(c).cuda() * Q.double()).sum().backward()
+    gU = Ut.grad.cpu().numpy().astype(np.float64)
+    gw = b.last_grad_w
+    ref = FP64MeanField(sizes, imgs, oracle_mod)
+    w0 = [GAUSS[1], BILAT[2]]
+    U64 = U.astype(np.float64)
+    flat = np.random.default_rng(1).choice(U.size, 256, replace=False)
+    fd = _fd_at(ref, U64, c, T, w0, flat, 1e-6)
+    g = gU.flat[flat]
+    scale = np.abs(fd).max()
+    rel = np.abs(g - fd) / np.maximum(np.abs(fd), ADJOINT_FLOOR * scale)
+    print("adjoint vs FD: max rel", rel.max(), "median", np.median(rel), "p99", np.percentile(rel, 99),
+          "plain rel max", (np.abs(g - fd) / np.abs(fd)).max(), "max|fd|", scale)
+    wrel = []
+    for k in range(2):
+        wp, wm = list(w0), list(w0)
+        wp[k] += 1e-6
+        wm[k] -= 1e-6
+        fdw = float((c * (ref.run(U64, wp, T) - ref.run(U64, wm, T))).sum()) / 2e-6
+        wrel.append(abs(gw[k] - fdw) / abs(fdw))
+    print("weights rel", wrel)
+    assert rel.max() <= ADJOINT_RTOL, (rel.max(), np.median(rel), scale)
+    assert max(wrel) <= ADJOINT_RTOL, wrel
 
 
 def test_meanfield_directional_derivative_larger_batch():
