@@ -67,6 +67,8 @@ def parse():
                     help="time only qp_sp / lp_sp, the 64-image batched QP and the 16-image mean-field adjoint")
     ap.add_argument("--only-batch-filter", action="store_true",
                     help="time only the batched lattice filter over the 64-image concatenated lattices")
+    ap.add_argument("--batch-images", type=int, default=64,
+                    help="images of the batched workloads (64 = the benchmark; fewer for profiling runs)")
     ap.add_argument("--prox-iters", type=int, default=50,
                     help="prox_max_iter of the solve (50 = the benchmark; smaller for profiling runs)")
     return ap.parse_args()
@@ -439,19 +441,42 @@ def measure_qp(reps=10, cpu=True):
 
 def measure_ho(W=640, H=480, seed=2, cpu=True):
     """Config 3: qp_sp and lp_sp (the QP / LP with sparse superpixel cliques)
-    at 640x480.  Cliques: three seeded superpixel scales (synth.superpixels,
-    the stand-in for the reference's mean-shift at spatial 8 / 16 / 32), each
-    clique 500-2000 pixels, with addSuperPixel's weights for the HO settings
-    (constant, normaliser) = (1.0, 0.5) and the CLI's (50, 1000).  GPU solves/s
-    (device-resident) and the energies; for the (50, 1000) setting also the
-    reference's own qp_sp on one CPU core and the relative energy gap."""
+    at 640x480.  Cliques: the reference's own addSuperPixel (EDISON mean
+    shift at spatial radii 8 / 16 / 32, range 8, min region 100) on the
+    benchmark image, recorded by tests/golden/make_config_goldens.py, with
+    the HO settings (constant, normaliser) = (1.0, 0.5) and the CLI's
+    (50, 1000).  GPU solves/s (device-resident) and the energies; for the
+    (50, 1000) setting the reference's own qp_sp on one CPU core and the
+    relative energy gap.  Also the engine's own addSuperPixel at the three
+    radii (the mean-shift mode search on the GPU) beside the reference's
+    recorded CPU seconds, and whether its cliques equal the reference's."""
     import torch
     from densecrf_ho_b200 import DenseCRF2D, LPParams, SolveStats, lib, check
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from make_config_goldens import load_cliques
     Ls = lib()
     img = synth.make_image(W, H, L, seed)
-    out = {"workload": f"qp_sp / lp_sp {W}x{H} L={L}, synthetic superpixel cliques at 3 scales (500-2000 px)"}
+    z = np.load(os.path.join(ROOT, "tests", "golden", "cliques_640x480_seed2.npz"))
+    out = {"workload": f"qp_sp / lp_sp {W}x{H} L={L}, the reference's mean-shift cliques at spatial radii "
+                       f"{[int(x) for x in z['scales']]}, range 8, min region 100"}
+    # the engine's addSuperPixel, three radii (warm: one run first)
+    seg = DenseCRF2D(W, H, L)
+    for s_ in z["scales"]:
+        seg.addSuperPixel(img["rgb"], int(s_), 8, 100, 50.0, 1000.0)
+    t0 = time.perf_counter()
+    seg = DenseCRF2D(W, H, L)
+    for s_ in z["scales"]:
+        seg.addSuperPixel(img["rgb"], int(s_), 8, 100, 50.0, 1000.0)
+    t_ms = time.perf_counter() - t0
+    so, si, se, sc = seg.getCliques()
+    ro, ri, re_, rc = load_cliques(50.0, 1000.0)
+    ref_ms_s = float(np.sum(z["meanshift_seconds"][:len(z["scales"])]))
+    out["add_superpixel_3_radii"] = {"seconds": t_ms, "cpu_reference_seconds": ref_ms_s, "cores": 1,
+                                     "speedup": ref_ms_s / t_ms,
+                                     "cliques_equal_reference": bool(np.array_equal(so, ro) and np.array_equal(si, ri)
+                                                                     and np.array_equal(se, re_))}
     for const, norm in ((1.0, 0.5), (50.0, 1000.0)):
-        off, idx, ew, cs = synth.cliques_three_scales(img, const, norm, seed)
+        off, idx, ew, cs = load_cliques(const, norm)
         crf = DenseCRF2D(W, H, L)
         crf.setUnaryEnergy(img["unary"])
         crf.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
@@ -890,7 +915,7 @@ def run_ours(args):
         print(json.dumps(measure_filters(W, H, img, reps=3)))
         return
     if args.only_batch_filter:
-        print(json.dumps(measure_batch_filter()))
+        print(json.dumps(measure_batch_filter(n=args.batch_images)))
         return
     if args.only_batch:
         print(json.dumps(measure_ho()))

@@ -9,11 +9,9 @@
 // DCRF_UNARY / DCRF_OUTPUT name others; the labelling is written as a PGM
 // (../data/seg.pgm by default).
 //
-// qp_sp / lp_sp need superpixels: the reference segments the image with
-// EDISON mean-shift (spatial radius 8, range 4, minimum region 100).  This
-// program uses a deterministic grid stand-in instead (seeds 3 x 8 pixels
-// apart, each pixel joined to the nearest of its 3 x 3 neighbouring seeds in
-// (x, y, rgb)); the clique weights then follow addSuperPixel exactly.
+// qp_sp / lp_sp add superpixel cliques as the reference does:
+// addSuperPixel(img, 8, 4, 100, const_1, norm_1), the engine's own EDISON
+// mean-shift segmentation (spatial radius 8, range 4, minimum region 100).
 //
 // Extra modes, no GPU needed: example_inference --dump-unary in.c_unary
 // out.f32 writes the decoded unaries [N][D] as raw float32, and
@@ -39,54 +37,6 @@ std::string env_or(const char* name, const char* dflt) {
     return v && *v ? std::string(v) : std::string(dflt);
 }
 
-// Grid superpixels standing in for the mean-shift segmentation.
-std::vector<int> grid_superpixels(const unsigned char* rgb, int W, int H, int spacing, int& n_regions) {
-    const int gx = (W + spacing - 1) / spacing, gy = (H + spacing - 1) / spacing;
-    std::vector<float> sx(gx * gy), sy(gx * gy), sc(3 * gx * gy);
-    for (int b = 0; b < gy; b++)
-        for (int a = 0; a < gx; a++) {
-            const int x = std::min(W - 1, a * spacing + spacing / 2), y = std::min(H - 1, b * spacing + spacing / 2);
-            const int s = b * gx + a;
-            sx[s] = (float)x;
-            sy[s] = (float)y;
-            for (int c = 0; c < 3; c++) sc[3 * s + c] = rgb[3 * ((size_t)y * W + x) + c];
-        }
-    const float cw = 20.0f;
-    std::vector<int> owner((size_t)W * H);
-    for (int y = 0; y < H; y++)
-        for (int x = 0; x < W; x++) {
-            const int cx = x / spacing, cy = y / spacing;
-            float best = 1e30f;
-            int bs = 0;
-            for (int oy = -1; oy <= 1; oy++)
-                for (int ox = -1; ox <= 1; ox++) {
-                    const int tx = cx + ox, ty = cy + oy;
-                    if (tx < 0 || tx >= gx || ty < 0 || ty >= gy) continue;
-                    const int s = ty * gx + tx;
-                    const float dx = (x - sx[s]) / spacing, dy = (y - sy[s]) / spacing;
-                    float dc = 0.0f;
-                    for (int c = 0; c < 3; c++) {
-                        const float e = (rgb[3 * ((size_t)y * W + x) + c] - sc[3 * s + c]) / cw;
-                        dc += e * e;
-                    }
-                    const float dd = dx * dx + dy * dy + dc;
-                    if (dd < best) {
-                        best = dd;
-                        bs = s;
-                    }
-                }
-            owner[(size_t)y * W + x] = bs;
-        }
-    // ids in first-pixel order
-    std::vector<int> id(gx * gy, -1), region((size_t)W * H);
-    n_regions = 0;
-    for (size_t i = 0; i < owner.size(); i++) {
-        if (id[owner[i]] < 0) id[owner[i]] = n_regions++;
-        region[i] = id[owner[i]];
-    }
-    return region;
-}
-
 void image_inference(const std::string& method, const std::string& path_to_results, const std::string& path_to_image,
                      const std::string& path_to_unaries, float spc_std, float spc_potts, float bil_spcstd,
                      float bil_colstd, float bil_potts, LP_inf_params& lp_params, sp_params params) {
@@ -103,11 +53,7 @@ void image_inference(const std::string& method, const std::string& path_to_resul
                              new PottsCompatibility(bil_potts));
     MatrixXf Q = crf.unary_init();
 
-    auto add_superpixels = [&]() {
-        int R = 0;
-        std::vector<int> region = grid_superpixels(img.data(), W, H, 3 * 8, R);
-        crf.addSuperPixel(region, R, img.data(), params.const_1, params.norm_1);
-    };
+    auto add_superpixels = [&]() { crf.addSuperPixel(img.data(), 8, 4, 100, params.const_1, params.norm_1); };
     if (method == "lp_sp") {
         std::cout << "---Running tests on proximal LP with higher order potentials\r\n";
         add_superpixels();

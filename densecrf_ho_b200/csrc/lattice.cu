@@ -399,7 +399,7 @@ template <bool PRE_NORM, int LC = 0>
 __global__ void __launch_bounds__(32 * kStageWarps)
     splat_kernel(int M, int Lrt, const int* __restrict__ order, const int* __restrict__ seg_start,
                  const int* __restrict__ seg_pix, const float* __restrict__ seg_w, const float* __restrict__ in,
-                 const float* __restrict__ norm, float* __restrict__ vals, Skip sk) {
+                 const float* __restrict__ norm, float* __restrict__ vals, Skip sk, int Lrow) {
     const int L = LC ? LC : Lrt;
     __shared__ float ring[kStageWarps][kStages][kChunk][32];
     __shared__ float mw[kStageWarps][kStages][kChunk];
@@ -423,8 +423,9 @@ __global__ void __launch_bounds__(32 * kStageWarps)
                                              acc = fadd(acc, fmul(mw[wib][slot][e], x));
                                          }
                                      });
-        if (act) vals[(long)(v + 1) * L + k] = acc;
+        if (act) vals[(long)(v + 1) * Lrow + k] = acc;
     }
+    for (int k = L + lane; k < Lrow; k += 32) vals[(long)(v + 1) * Lrow + k] = 0.0f;  // row padding
 }
 
 // The longest lists with L = 21: the cp.async ring of splat_kernel, kStages chunks
@@ -438,7 +439,7 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     splat_ring21_kernel(int M, const int* __restrict__ order, const int* __restrict__ seg_start,
                         const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
                         const float* __restrict__ in, const float* __restrict__ norm, float* __restrict__ vals,
-                        Skip sk) {
+                        Skip sk, int Lrow) {
     constexpr int L = 21;
     __shared__ __align__(16) float X[kStageWarps][kStages][L][kRS];
     __shared__ __align__(16) float Wr[kStageWarps][kStages][kChunk];
@@ -511,7 +512,8 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     }
     cp_async_wait<0>();
     __syncwarp();
-    if (lane < L) vals[(long)(v + 1) * L + lane] = acc;
+    if (lane < L) vals[(long)(v + 1) * Lrow + lane] = acc;
+    else if (lane < Lrow) vals[(long)(v + 1) * Lrow + lane] = 0.0f;  // row padding
 }
 
 // Short lists (at most kLongList entries; the tail of `order`): one thread
@@ -520,13 +522,17 @@ template <bool PRE_NORM, int LC = 0>
 __global__ void splat_short_kernel(int n_short, int Lrt, const int* __restrict__ order,
                                    const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
                                    const float* __restrict__ seg_w, const float* __restrict__ in,
-                                   const float* __restrict__ norm, float* __restrict__ vals, Skip sk) {
+                                   const float* __restrict__ norm, float* __restrict__ vals, Skip sk, int Lrow) {
     const int L = LC ? LC : Lrt;
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)n_short * L) return;
-    const int u = (int)(t / L), k = (int)(t - (long)u * L);
+    if (t >= (long)n_short * Lrow) return;
+    const int u = (int)(t / Lrow), k = (int)(t - (long)u * Lrow);
     const int v = order[u];
     if (skipped(sk, v)) return;
+    if (k >= L) {  // row padding
+        vals[(long)(v + 1) * Lrow + k] = 0.0f;
+        return;
+    }
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
     float acc = 0.0f;
 #pragma unroll 4
@@ -536,7 +542,7 @@ __global__ void splat_short_kernel(int n_short, int Lrt, const int* __restrict__
         if (PRE_NORM) x = fmul(x, norm[p]);
         acc = fadd(acc, fmul(seg_w[s], x));
     }
-    vals[(long)(v + 1) * L + k] = acc;
+    vals[(long)(v + 1) * Lrow + k] = acc;
 }
 
 __global__ void count_long_kernel(int M, const int* __restrict__ counts, int threshold, int* __restrict__ n) {
@@ -581,6 +587,31 @@ __global__ void blur_kernel(int M, int Lrt, const int2* __restrict__ nbr,
     dst[(long)(v + 1) * L + k] = r;
 }
 
+// The blur pass over rows padded to Lp = 4 Q floats (sseCompute, L > 2):
+// one thread per (vertex, four labels), float4 loads of the vertex's row and
+// of its two neighbours' rows.  The same operations per element as
+// blur_kernel; the padding lanes hold zeros and stay zero.
+template <int Q>
+__global__ void blur4_kernel(int M, int Qrt, const int2* __restrict__ nbr, const float* __restrict__ src,
+                             float* __restrict__ dst, Skip sk) {
+    const int Qn = Q ? Q : Qrt;
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long)M * Qn) return;
+    const int v = (int)(t / Qn), q = (int)(t - (long)v * Qn);
+    if (skipped(sk, v)) return;
+    const long lp = 4L * Qn;
+    const int2 nb = nbr[v];
+    const float4 a = *reinterpret_cast<const float4*>(src + (long)(v + 1) * lp + 4 * q);
+    const float4 x = *reinterpret_cast<const float4*>(src + (long)nb.x * lp + 4 * q);
+    const float4 y = *reinterpret_cast<const float4*>(src + (long)nb.y * lp + 4 * q);
+    float4 r;
+    r.x = fadd(a.x, fmul(0.5f, fadd(x.x, y.x)));
+    r.y = fadd(a.y, fmul(0.5f, fadd(x.y, y.y)));
+    r.z = fadd(a.z, fmul(0.5f, fadd(x.z, y.z)));
+    r.w = fadd(a.w, fmul(0.5f, fadd(x.w, y.w)));
+    *reinterpret_cast<float4*>(dst + (long)(v + 1) * lp + 4 * q) = r;
+}
+
 __device__ __forceinline__ float apply_epilogue(float v, long t, int i, int k, const SliceEpilogue& ep) {
     if (ep.potts) {
         if (ep.norm) v = fmul(v, ep.norm[i]);
@@ -613,6 +644,65 @@ __global__ void slice_kernel(int N, int Lrt, int drt, const int* __restrict__ of
         else acc = fadd(acc, fmul(fmul(w, alpha), v));
     }
     out[t] = apply_epilogue(acc, t, i, k, ep);
+}
+
+// Slice over rows padded to Lp = 4 Q floats (sseCompute, L > 2), a tile of
+// `tile` pixels per block (kSliceTile, fewer for very wide rows): the tile's offsets and (barycentric * alpha)
+// weights are staged once in shared memory (coalesced: they are contiguous),
+// every (pixel, four labels) item gathers the d+1 vertex rows with float4
+// loads, and the tile's L outputs per pixel -- contiguous in `out` -- leave
+// through shared memory with the epilogue, coalesced.  Per element the
+// arithmetic is slice_kernel's: acc = sum over j in order of
+// (bary_j * alpha) * value_j, from +0.
+constexpr int kSliceTile = 128;
+constexpr int kSliceThreads = 256;
+template <int DC, int Q>
+__global__ void __launch_bounds__(kSliceThreads)
+    slice4_kernel(int N, int L, int Qrt, int drt, int tile, const int* __restrict__ offset,
+                  const float* __restrict__ bary, const float* __restrict__ vals, float alpha, float* out,
+                  SliceEpilogue ep, Skip sk) {
+    extern __shared__ __align__(16) unsigned char slice_smem[];
+    const int d1 = (DC ? DC : drt) + 1, Qn = Q ? Q : Qrt;
+    const long lp = 4L * Qn;
+    int* s_off = reinterpret_cast<int*>(slice_smem);
+    float* s_wa = reinterpret_cast<float*>(s_off + tile * d1);
+    float* s_out = s_wa + tile * d1;
+    const long p0 = (long)blockIdx.x * tile;
+    const int np = (int)min((long)tile, (long)N - p0);
+    for (int e = threadIdx.x; e < np * d1; e += blockDim.x) {
+        s_off[e] = offset[p0 * d1 + e];
+        s_wa[e] = fmul(bary[p0 * d1 + e], alpha);
+    }
+    __syncthreads();
+    for (int it = threadIdx.x; it < np * Qn; it += blockDim.x) {
+        const int pl = it / Qn, q = it - pl * Qn;
+        if (skipped(sk, s_off[pl * d1])) continue;
+        float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int j = 0; j < (DC ? DC + 1 : 17); j++) {
+            if (!DC && j >= d1) break;
+            const int o = s_off[pl * d1 + j];
+            const float wa = s_wa[pl * d1 + j];
+            const float4 v = *reinterpret_cast<const float4*>(vals + (long)(o + 1) * lp + 4 * q);
+            acc.x = fadd(acc.x, fmul(wa, v.x));
+            acc.y = fadd(acc.y, fmul(wa, v.y));
+            acc.z = fadd(acc.z, fmul(wa, v.z));
+            acc.w = fadd(acc.w, fmul(wa, v.w));
+        }
+        float* so = s_out + pl * L + 4 * q;
+        const int rem = L - 4 * q;
+        so[0] = acc.x;  // 4 q < L always
+        if (rem > 1) so[1] = acc.y;
+        if (rem > 2) so[2] = acc.z;
+        if (rem > 3) so[3] = acc.w;
+    }
+    __syncthreads();
+    const long t0 = p0 * L;
+    for (int e = threadIdx.x; e < np * L; e += blockDim.x) {
+        const int pl = e / L, k = e - pl * L;
+        if (skipped(sk, s_off[pl * d1])) continue;
+        out[t0 + e] = apply_epilogue(s_out[e], t0 + e, (int)(p0 + pl), k, ep);
+    }
 }
 
 // addSplitArray / sliceSplitArray bins (:548-589): the lower pass rounds
@@ -1284,11 +1374,11 @@ void gradient_impl(Lattice& lat, float* df, const float* a, const float* b, int 
         if (lat.n_long)
             launch(splat_kernel<false>, ceil_div(lat.n_long, kStageWarps), 32 * kStageWarps, 0, st, lat.n_long, L,
                    lat.vorder.get(), lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in, nullptr, src,
-                   Skip{});
+                   Skip{}, L);
         if (n_short)
             launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L,
                    lat.vorder.get() + lat.n_long, lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in,
-                   nullptr, src, Skip{});
+                   nullptr, src, Skip{}, L);
         for (int jj = 0; jj <= d; jj++) {
             const int j = dir ? d - jj : jj;
             launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, lat.nbr.get() + (long)j * M, src, dst,
@@ -1510,10 +1600,10 @@ void Lattice::compute_noalloc(float* out, const float* in, int L, bool reverse) 
     const int n_short = M - n_long;
     if (n_long)
         launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{});
+               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{}, L);
     if (n_short)
         launch(splat_short_kernel<false>, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
-               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{});
+               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{}, L);
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
@@ -1540,14 +1630,20 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
     slice(out, L, ep);
 }
 
+// Row stride of the plain filter's value buffers: L padded to a multiple of
+// four (float4 rows) on the sseCompute path (L > 2); seqCompute (L <= 2)
+// keeps L.
+static int value_row(int L) { return L > 2 ? (L + 3) & ~3 : L; }
+
 void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_norm) {
     require(L >= 1, DCRF_E_ARG, "compute: L must be >= 1");
-    ensure_values((size_t)L);
+    const int Lp = value_row(L);
+    ensure_values((size_t)Lp);
     cudaStream_t st = stream;
-    const long ML = (long)M * L, NL = (long)N * L;
+    const long ML = (long)M * L;
     float *src = va.get(), *dst = vb.get();
     const int n_short = M - n_long;
-    const long SL = (long)n_short * L;
+    const long SL = (long)n_short * Lp;
     const Skip sk{vimg.get(), skip_done};
     // As in the ordered filter, the lists longer than kHugeList run on the
     // high-priority side stream while the others are splatted.
@@ -1567,21 +1663,21 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
         if (L == 21 && first < nh) {
             if (pre_norm)
                 launch(splat_ring21_kernel<true>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count,
-                       vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
+                       vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk, Lp);
             else
                 launch(splat_ring21_kernel<false>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count,
                        vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, (const float*)nullptr,
-                       src, sk);
+                       src, sk, Lp);
             return;
         }
         if (pre_norm)
             launch(L == 21 ? splat_kernel<true, 21> : splat_kernel<true>, ceil_div(count, kStageWarps),
                    32 * kStageWarps, 0, ls, count, L,
-                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
+                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk, Lp);
         else
             launch(L == 21 ? splat_kernel<false, 21> : splat_kernel<false>, ceil_div(count, kStageWarps),
                    32 * kStageWarps, 0, ls, count, L,
-                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
+                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk, Lp);
     };
     long_range(0, nh, forked ? aux : st);
     long_range(nh, n_long - nh, st);
@@ -1589,25 +1685,28 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
         if (pre_norm)
             launch(L == 21 ? splat_short_kernel<true, 21> : splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st,
                    n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk);
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk, Lp);
         else
             launch(L == 21 ? splat_short_kernel<false, 21> : splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st,
                    n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk);
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk, Lp);
     }
     if (forked) {
         DCRF_CUDA(cudaEventRecord(ev_join, aux));
         DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
     }
     const bool seq = L <= 2;
+    const int Q = Lp / 4;
+    const long MQ = (long)M * Q;
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
+        const int2* nb = nbr.get() + (long)j * M;
         if (seq)
-            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
-        else if (L == 21)
-            launch(blur_kernel<false, 21>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nb, src, dst, sk);
+        else if (Q == 6)
+            launch(blur4_kernel<6>, ceil_div(MQ, kTB), kTB, 0, st, M, Q, nb, src, dst, sk);
         else
-            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{vimg.get(), skip_done});
+            launch(blur4_kernel<0>, ceil_div(MQ, kTB), kTB, 0, st, M, Q, nb, src, dst, sk);
         std::swap(src, dst);
     }
     plain_vals = src;
@@ -1619,16 +1718,25 @@ void Lattice::slice(float* out, int L, const SliceEpilogue& ep) {
     cudaStream_t st = stream;
     const long NL = (long)N * L;
     const float* src = plain_vals;
-    const bool seq = L <= 2;
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     const Skip sks{vimg.get(), skip_done};
-    auto sl = [&](auto kern) {
-        launch(kern, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha, out, ep, sks);
-    };
-    if (seq) sl(slice_kernel<true, 0, 0>);
-    else if (L == 21 && d == 5) sl(slice_kernel<false, 5, 21>);
-    else if (L == 21 && d == 2) sl(slice_kernel<false, 2, 21>);
-    else sl(slice_kernel<false, 0, 0>);
+    if (L <= 2) {
+        launch(slice_kernel<true, 0, 0>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
+               alpha, out, ep, sks);
+    } else {
+        const int Q = value_row(L) / 4;
+        // pixels per tile: kSliceTile, fewer for very wide rows (40 KB of shared memory at most)
+        const int per_px = (d + 1) * 8 + L * 4;
+        const int tile = std::max(1, std::min(kSliceTile, (40 << 10) / per_px));
+        const size_t smem = (size_t)tile * per_px;
+        auto sl = [&](auto kern) {
+            launch(kern, ceil_div(N, tile), kSliceThreads, smem, st, N, L, Q, d, tile, offset.get(), bary.get(), src,
+                   alpha, out, ep, sks);
+        };
+        if (d == 5 && Q == 6) sl(slice4_kernel<5, 6>);
+        else if (d == 2 && Q == 6) sl(slice4_kernel<2, 6>);
+        else sl(slice4_kernel<0, 0>);
+    }
     DCRF_LAUNCH_CHECK();
 }
 

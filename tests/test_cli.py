@@ -103,12 +103,37 @@ def test_cli_matches_python_api(method, tmp_path):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("method", ["qp_sp", "lp_sp"])
-def test_cli_higher_order_methods_run(method, tmp_path):
+def test_cli_higher_order_methods_match_python_api(method, tmp_path):
+    """qp_sp / lp_sp: the program adds addSuperPixel(img, 8, 4, 100, 50, 1000)
+    cliques (the engine's mean-shift) as the reference's does; its labels and
+    reported energy equal the same solve through the Python API."""
     _need_cli()
+    from densecrf_ho_b200 import DenseCRF2D, LPParams
+    rec = json.load(open(FIX + ".json"))
+    W, H, D = rec["W"], rec["H"], rec["D"]
     env = {"DCRF_IMAGE": FIX + ".bmp", "DCRF_UNARY": FIX + ".c_unary", "DCRF_OUTPUT": str(tmp_path / "seg.pgm")}
     r = _run([method, "3", "5", "30", "5", "10"], env)
     assert r.returncode == 0, r.stderr
     assert "Running tests on" in r.stdout
     line = [l for l in r.stdout.splitlines() if l.startswith("# method: ")][-1]
-    assert np.isfinite(float(line.split("\t")[1]))
-    assert _pgm(tmp_path / "seg.pgm").size == 48 * 32
+    energy = float(line.split("\t")[1])
+    _run(["--dump-unary", FIX + ".c_unary", str(tmp_path / "u.f32")])
+    _run(["--dump-image", FIX + ".bmp", str(tmp_path / "i.u8")])
+    U = np.fromfile(tmp_path / "u.f32", np.float32).reshape(W * H, D)
+    rgb = np.fromfile(tmp_path / "i.u8", np.uint8)
+    m = DenseCRF2D(W, H, D)
+    m.setUnaryEnergy(U)
+    m.addPairwiseGaussian(3.0, 3.0, 5.0)
+    m.addPairwiseBilateral(30.0, 30.0, 5.0, 5.0, 5.0, rgb, 10.0)
+    Q = m.unary_init()
+    assert m.addSuperPixel(rgb, 8, 4, 100, 50.0, 1000.0) >= 1
+    if method == "qp_sp":
+        Q = m.qp_inference_super_pixels_non_convex(Q)
+    else:
+        prm = LPParams.default()
+        prm.prox_energy_tol = prm.dual_gap_tol
+        Q = m.lp_inference_prox_super_pixels(Q, prm)
+    lab = m.currentMap(Q)
+    assert np.array_equal(_pgm(tmp_path / "seg.pgm"), lab.astype(np.uint8))
+    ref = m.assignment_energy_higher_order(lab) if method == "qp_sp" else m.assignment_energy_true(lab)
+    assert energy == pytest.approx(ref, rel=1e-5)
