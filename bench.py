@@ -65,6 +65,8 @@ def parse():
                     help="skip the extra workloads (QP, qp_sp / lp_sp, batch, adjoint): a short command for ncu")
     ap.add_argument("--only-batch", action="store_true",
                     help="time only qp_sp / lp_sp, the 64-image batched QP and the 16-image mean-field adjoint")
+    ap.add_argument("--only-batch-qp", action="store_true",
+                    help="time only the batched QP, without the sequential comparison (a short command for ncu)")
     ap.add_argument("--only-batch-filter", action="store_true",
                     help="time only the batched lattice filter over the 64-image concatenated lattices")
     ap.add_argument("--batch-images", type=int, default=64,
@@ -535,7 +537,7 @@ def measure_ho(W=640, H=480, seed=2, cpu=True):
     return out
 
 
-def measure_batch(n=64, max_iter=100, reps=3):
+def measure_batch(n=64, max_iter=100, reps=3, sequential=True):
     """Config 4: the plain QP (as config 1, up to 100 Frank-Wolfe iterations)
     of n images of uneven sizes (H ~ U[240, 500], W ~ U[320, 500], seeded),
     solved as one batch (dcrf_batch_qp_dev: concatenated lattices, per-image
@@ -578,6 +580,9 @@ def measure_batch(n=64, max_iter=100, reps=3):
     batch_launches = (Ls.dcrf_kernel_launches() - l0) // reps
     batch_ms = e0.elapsed_time(e1) / reps
     steps = [s.iterations for s in st]
+    if not sequential:
+        return {"images": n, "pixels": int(b.N), "batch_ms": batch_ms, "fw_steps": steps,
+                "batch_launches_per_solve": int(batch_launches)}
 
     # Sequential: every image once after the other, as a caller with one
     # model per image would run them (each solve ends with its host read of
@@ -669,9 +674,14 @@ def measure_batch_filter(n=64, reps=10):
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1) / reps / 1e3
         fb = filter_bytes(N, M, d)
+        shp = (C.c_int * 4)()
+        check(Ls.dcrf_batch_filter_shape(b._h, k, shp))
         out[name] = {"M": M, "d": d, "ms": t * 1e3, "bytes": fb, "gbs": fb / t / 1e9, "frac": fb / t / 1e9 / peak,
                      "gpix_label_s": N * L / t / 1e9,
-                     "launches_per_call": int((Ls.dcrf_kernel_launches() - l0) // reps)}
+                     "launches_per_call": int((Ls.dcrf_kernel_launches() - l0) // reps),
+                     "tuned_shape": {"splat_form": ("staged", "warp_long", "warp_all")[shp[3]],
+                                     "splat_vertices_per_block": shp[0], "blur_threads": shp[1],
+                                     "slice_pixels_per_block": shp[2]}}
     return out
 
 
@@ -916,6 +926,9 @@ def run_ours(args):
         return
     if args.only_batch_filter:
         print(json.dumps(measure_batch_filter(n=args.batch_images)))
+        return
+    if args.only_batch_qp:
+        print(json.dumps(measure_batch(n=args.batch_images, reps=1, sequential=False)))
         return
     if args.only_batch:
         print(json.dumps(measure_ho()))

@@ -1291,6 +1291,20 @@ dcrf_status dcrf_batch_pairwise_apply(dcrf_batch h, int k, float* out, const flo
     });
 }
 
+dcrf_status dcrf_batch_filter_shape(dcrf_batch h, int k, int* shape) {
+    return guard([&] {
+        auto& b = BT(h);
+        need(shape, "shape");
+        dcrf::require(k >= 0 && k < (int)b.terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+        b.ensure_lattices();
+        const dcrf::FilterShape& f = b.terms[k]->lat->shape;
+        shape[0] = f.splat_warps;
+        shape[1] = f.blur_threads;
+        shape[2] = f.slice_tile;
+        shape[3] = f.splat_kind;
+    });
+}
+
 dcrf_status dcrf_batch_lattice_size(dcrf_batch h, int k, int64_t* M) {
     return guard([&] {
         auto& b = BT(h);

@@ -95,6 +95,301 @@ __global__ void accumulate_total_kernel(const double* __restrict__ partials, int
     if (lane == 0) *acc += s;
 }
 
+// ---- lockstep QP ---------------------------------------------------------
+// Every image's reductions use the block decomposition Model::qp gives a
+// single image of that size (kRedBlocks virtual blocks striding over the
+// image's elements, or its row tiles), and every image keeps its own
+// SolverScalars, so each image's trajectory, output and energy are those of
+// its own solve.  Images whose loop has ended (done[i]) are skipped by every
+// kernel, the filters included (Lattice::skip_done).
+constexpr int kBPart = 2 * kRedBlocks;  // partial slots per image (two values at most)
+
+struct BImages {
+    const long* pix_off;  // B + 1 pixel offsets
+    const int* done;      // per image: its loop has ended
+    int L;
+};
+
+// block_sum_store for virtual block vb of an image: partials[j kRedBlocks + vb].
+template <int NV>
+__device__ __forceinline__ void vblock_store(double (&v)[NV], double* partials, int vb) {
+    __shared__ double sm[NV][kRedThreads / 32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; j++)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_down_sync(kFullMask, v[j], o);
+    if (lane == 0)
+#pragma unroll
+        for (int j = 0; j < NV; j++) sm[j][w] = v[j];
+    __syncthreads();
+    if (threadIdx.x < NV) {
+        double t = 0.0;
+        for (int ww = 0; ww < kRedThreads / 32; ww++) t += sm[threadIdx.x][ww];
+        partials[(long)threadIdx.x * kRedBlocks + vb] = t;
+    }
+}
+
+// Virtual block (image, vb) of blockIdx.x; false when the image is done.
+__device__ __forceinline__ bool vblock(const BImages& bi, int& img, int& vb, long& base, long& n) {
+    img = blockIdx.x / kRedBlocks;
+    vb = blockIdx.x - img * kRedBlocks;
+    if (bi.done && bi.done[img]) return false;  // block-uniform
+    base = bi.pix_off[img] * bi.L;
+    n = (bi.pix_off[img + 1] - bi.pix_off[img]) * bi.L;
+    return true;
+}
+
+// dot_kernel per image: partials of a . b.
+__global__ void bdot_kernel(BImages bi, const float* __restrict__ a, const float* __restrict__ b,
+                            double* __restrict__ part) {
+    int img, vb;
+    long base, n;
+    if (!vblock(bi, img, vb, base, n)) return;
+    double v[1] = {0.0};
+    for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x)
+        v[0] += (double)a[base + t] * (double)b[base + t];
+    vblock_store<1>(v, part + (long)img * kBPart, vb);
+}
+
+// dots2_kernel per image: partials of a . c and b . c.
+__global__ void bdots2_kernel(BImages bi, const float* __restrict__ a, const float* __restrict__ b,
+                              const float* __restrict__ c, double* __restrict__ part) {
+    int img, vb;
+    long base, n;
+    if (!vblock(bi, img, vb, base, n)) return;
+    double v[2] = {0.0, 0.0};
+    for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x) {
+        const double cc = c[base + t];
+        v[0] += (double)a[base + t] * cc;
+        v[1] += (double)b[base + t] * cc;
+    }
+    vblock_store<2>(v, part + (long)img * kBPart, vb);
+}
+
+// qp_update_kernel per image.
+__global__ void bqp_update_kernel(BImages bi, const float* __restrict__ sx, const float* __restrict__ psi,
+                                  const float* __restrict__ U, float* __restrict__ Q, float* __restrict__ grad,
+                                  const SolverScalars* __restrict__ sc, double* __restrict__ part) {
+    int img, vb;
+    long base, n;
+    if (!vblock(bi, img, vb, base, n)) return;
+    if (sc[img].zero_step) return;
+    const float fs = sc[img].fstep, f2s = sc[img].f2step;
+    double v[1] = {0.0};
+    for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x) {
+        const long e = base + t;
+        const float q = fadd(Q[e], fmul(fs, sx[e]));
+        const float g = fadd(grad[e], fadd(fmul(f2s, psi[e]), fmul(fs, 0.0f)));
+        Q[e] = q;
+        grad[e] = g;
+        v[0] += (double)q * (double)fadd(g, U[e]);
+    }
+    vblock_store<1>(v, part + (long)img * kBPart, vb);
+}
+
+// qp_direction_kernel per image (run-time L): one-hot of the first arg-min
+// of grad minus Q, and partials of U . sx.
+__global__ void bqp_direction_kernel(BImages bi, const float* __restrict__ grad, const float* __restrict__ Q,
+                                     const float* __restrict__ U, float* __restrict__ sx, double* __restrict__ part) {
+    int img, vb;
+    long base, n;
+    if (!vblock(bi, img, vb, base, n)) return;
+    const int L = bi.L;
+    const long p0 = bi.pix_off[img], np = bi.pix_off[img + 1] - p0;
+    double v[1] = {0.0};
+    for (long i = (long)vb * blockDim.x + threadIdx.x; i < np; i += (long)kRedBlocks * blockDim.x) {
+        const float* g = grad + (p0 + i) * L;
+        float best = g[0];
+        int bk = 0;
+        for (int k = 1; k < L; k++)
+            if (g[k] < best) {
+                best = g[k];
+                bk = k;
+            }
+        for (int k = 0; k < L; k++) {
+            const long e = (p0 + i) * L + k;
+            const float s = fsub(k == bk ? 1.0f : 0.0f, Q[e]);
+            sx[e] = s;
+            v[0] += (double)U[e] * (double)s;
+        }
+    }
+    vblock_store<1>(v, part + (long)img * kBPart, vb);
+}
+
+// qp_direction_tiled per image (L = 21): the image's row tiles of 32 pixels,
+// blocks numbered image after image (tile_off), one partial per block.
+template <int LC>
+__global__ void __launch_bounds__(32 * kTileWarps)
+    bqp_direction_tiled(const int* __restrict__ tile_img, const int* __restrict__ tile_off, BImages bi,
+                        const float* __restrict__ grad, const float* __restrict__ Q, const float* __restrict__ U,
+                        float* __restrict__ sx, double* __restrict__ part) {
+    __shared__ float sm[kTileWarps][3][32 * LC];
+    __shared__ double s32[32];
+    const int img = tile_img[blockIdx.x];
+    if (bi.done[img]) return;  // block-uniform
+    const int lb = blockIdx.x - tile_off[img];
+    const long off = bi.pix_off[img], N = bi.pix_off[img + 1] - off;
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long pix0 = ((long)lb * kTileWarps + wib) * 32;
+    double acc = 0.0;
+    if (pix0 < N) {
+        const int npix = (int)min(32L, N - pix0);
+        float *Gt = sm[wib][0], *Qt = sm[wib][1], *Ut = sm[wib][2];
+        tile_in<LC>(Gt, grad, off + pix0, npix, lane);
+        tile_in<LC>(Qt, Q, off + pix0, npix, lane);
+        tile_in<LC>(Ut, U, off + pix0, npix, lane);
+        __syncwarp();
+        const float* rg = Gt + lane * LC;
+        float* rq = Qt + lane * LC;
+        const float* ru = Ut + lane * LC;
+        float best = rg[0];
+        int bk = 0;
+#pragma unroll
+        for (int k = 1; k < LC; k++)
+            if (rg[k] < best) {
+                best = rg[k];
+                bk = k;
+            }
+        const bool act = lane < npix;
+#pragma unroll
+        for (int k = 0; k < LC; k++) {
+            const float s = fsub(k == bk ? 1.0f : 0.0f, rq[k]);
+            rq[k] = s;
+            if (act) acc += (double)ru[k] * (double)s;
+        }
+        __syncwarp();
+        tile_out<LC>(Qt, sx, off + pix0, npix, lane);
+    }
+    const double tot = block_sum_any(acc, s32);
+    if (threadIdx.x == 0) part[tile_off[img] + lb] = tot;
+}
+
+// finalize_sums_kernel per image (one block per image, one warp per value).
+__global__ void bfinalize_sums_kernel(const double* __restrict__ part, int nv, int dst, const int* __restrict__ done,
+                                      SolverScalars* sc) {
+    const int img = blockIdx.x, j = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (done[img] || j >= nv) return;
+    const double* p = part + (long)img * kBPart + (long)j * kRedBlocks;
+    double s = 0.0;
+    int b = lane;
+    for (; b + 7 * 32 < kRedBlocks; b += 8 * 32) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = p[b + i * 32];
+#pragma unroll
+        for (int i = 0; i < 8; i++) s += x[i];
+    }
+    for (; b < kRedBlocks; b += 32) s += p[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(kFullMask, s, o);
+    if (lane == 0) sc[img].sums[dst + j] = s;
+}
+
+// finalize_large_kernel per image over its tile partials (1024 threads).
+__global__ void bfinalize_large_kernel(const double* __restrict__ part, const int* __restrict__ tile_off, int dst,
+                                       const int* __restrict__ done, SolverScalars* sc) {
+    __shared__ double s[32];
+    const int img = blockIdx.x;
+    if (done[img]) return;  // block-uniform
+    const double* p = part + tile_off[img];
+    const int nblk = tile_off[img + 1] - tile_off[img];
+    const int bd = blockDim.x;
+    double v = 0.0;
+    int b = threadIdx.x;
+    for (; b + 7 * bd < nblk; b += 8 * bd) {
+        double x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = p[b + i * bd];
+#pragma unroll
+        for (int i = 0; i < 8; i++) v += x[i];
+    }
+    for (; b < nblk; b += bd) v += p[b];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(kFullMask, v, o);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s[w];
+        sc[img].sums[dst] = t;
+    }
+}
+
+// The single-thread QP scalar steps, one thread per image.
+__global__ void bqp_init_energy_kernel(int B, SolverScalars* sc, int nterms, int max_iter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B) return;
+    SolverScalars* s = sc + i;
+    double e = 0.0;
+    e += s->sums[0];
+    e -= 0.0;
+    for (int k = 0; k < nterms; k++) e += s->sums[1 + k];
+    e += 0.0;
+    e += s->sums[8];
+    s->energy = e;
+    s->old_energy = DBL_MAX;
+    s->zero_step = 0;
+    s->steps = 0;
+    s->stop = max_iter > 0 ? 0 : !((s->old_energy - s->energy) > 100.0);
+}
+
+__global__ void bqp_step_kernel(int B, const int* __restrict__ done, SolverScalars* sc) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || done[i]) return;
+    SolverScalars* s = sc + i;
+    s->old_energy = s->energy;
+    const double num = s->sums[0] + 2 * s->sums[1] + s->sums[3] + s->sums[4] + s->sums[5];
+    const double denom = s->sums[2] + s->sums[6];
+    double step = -num / (2 * denom);
+    if (denom == 0 || num == 0) {
+        s->zero_step = 1;
+        s->stop = 1;
+        return;
+    }
+    if (denom < 0) step = 1;
+    s->fstep = (float)step;
+    s->f2step = (float)(2 * step);
+    s->steps++;
+}
+
+__global__ void bqp_energy_kernel(int B, const int* __restrict__ done, SolverScalars* sc, int max_iter) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= B || done[i]) return;
+    SolverScalars* s = sc + i;
+    if (s->zero_step) return;
+    const double e = s->sums[7] + s->sums[8];
+    s->energy = e;
+    if (max_iter > 0) s->stop = s->steps >= max_iter;
+    else s->stop = !((s->old_energy - e) > 100.0);
+}
+
+// End of an iteration: images whose stop rule fired are done from now on;
+// the loop goes on while any image runs, at most `cap` iterations per
+// launch (the count kept in *chunk).  With a graph handle it sets the
+// loop's condition, otherwise *running for the host.
+__global__ void bqp_cond_kernel(int B, const SolverScalars* __restrict__ sc, int* __restrict__ done, int* chunk,
+                                int cap, int* running, cudaGraphConditionalHandle h, int use_handle) {
+    int any = 0;
+    for (int i = threadIdx.x; i < B; i += blockDim.x) {
+        const int st = sc[i].stop;
+        done[i] = st;
+        any |= !st;
+    }
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) {
+        const int c = ++*chunk;
+        *running = any;
+        if (use_handle) cudaGraphSetConditional(h, (any && c < cap) ? 1u : 0u);
+    }
+}
+
+// a += coef * b over the whole batch (grad_y += 2 tmp, src/densecrf.cpp:380).
+__global__ void badd_scaled_kernel(long n, float* __restrict__ a, const float* __restrict__ b, float coef) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] = fadd(a[t], fmul(coef, b[t]));
+}
+
 }  // namespace
 
 Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_) {
@@ -119,6 +414,7 @@ Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_)
 
 Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
+    if (bqp_graph) cudaGraphExecDestroy(bqp_graph);
     img.clear();
     terms.clear();
     if (stream) cudaStreamDestroy(stream);
@@ -149,6 +445,7 @@ void Batch::ensure_lattices() {
 void Batch::add_term(const float* d_features, int d, float w) {
     img.clear();  // rebuilt with the new term at the next QP
     qp_warm = false;
+    weights_gen++;
     ensure_lattices();
     auto t = std::make_unique<Term>();
     DCRF_CUDA(cudaMemcpyAsync(t->feat.ensure((size_t)Ntot * d), d_features, sizeof(float) * Ntot * d,
@@ -212,7 +509,7 @@ void Batch::ensure_image_models() {
     img_unary_gen = ~0ull;
 }
 
-int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* energies) {
+int Batch::qp_threaded(const float* init, float* out, int max_iter, int* steps, double* energies) {
     require(has_unary, DCRF_E_STATE, "qp: no unary energy set");
     ensure_image_models();
     if (img_unary_gen != unary_gen) {  // each image's slice of the unaries
@@ -284,9 +581,201 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
     return most;
 }
 
+// Batched QP in lockstep: every Frank-Wolfe iteration of every image that
+// is still running, one launch per step over all images -- the filters over
+// the terms' concatenated lattices, the per-pixel and per-image scalar steps
+// over the concatenated arrays -- with the loop on the device: a CUDA graph
+// whose `while` node repeats the iteration until no image runs (or kQpChunk
+// iterations, after which the host relaunches it).  Each image's reductions
+// use its own single-image decomposition and scalars, so its output, step
+// count and energy are those of its own solve (src/densecrf.cpp:340-442).
+int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* energies) {
+    require(has_unary, DCRF_E_STATE, "qp: no unary energy set");
+    ensure_lattices();
+    const long NL = Ntot * L;
+    float* Q = out;  // iterated in place
+    float* grad = buf(0);
+    float* sx = buf(1);
+    float* psi = buf(2);
+    float* tmp = buf(3);
+    const int nt = (int)terms.size();
+    SolverScalars* sc = bsc.ensure(B);
+    int* done = bdone.ensure(B);
+    int* flags = bflags.ensure(2);  // [0] iterations of the current launch, [1] some image runs
+    double* part = bpart.ensure((size_t)B * kBPart);
+    const bool tiled = L == 21;
+    if (tiled && btiles == 0) {  // row-tile blocks of the direction kernel, image after image
+        std::vector<int> toff(B + 1, 0), timg;
+        for (int i = 0; i < B; i++) {
+            const int tg = ceil_div(ceil_div((int)(pix_off[i + 1] - pix_off[i]), 32), kTileWarps);
+            toff[i + 1] = toff[i] + tg;
+            timg.insert(timg.end(), tg, i);
+        }
+        btiles = toff[B];
+        DCRF_CUDA(cudaMemcpyAsync(btile_off.ensure(B + 1), toff.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice,
+                                  stream));
+        DCRF_CUDA(cudaMemcpyAsync(btile_img.ensure(btiles), timg.data(), sizeof(int) * btiles, cudaMemcpyHostToDevice,
+                                  stream));
+        DCRF_CUDA(cudaStreamSynchronize(stream));  // the host vectors are the copies' sources
+    }
+    double* part_dir = tiled ? bpart_dir.ensure(btiles) : nullptr;
+    const BImages all{d_pix_off.get(), nullptr, L};
+    const BImages live{d_pix_off.get(), done, L};
+    const int sb = ceil_div(B, 128);
+
+    if (Q != init) DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    DCRF_CUDA(cudaMemcpyAsync(grad, unary.get(), sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
+    DCRF_CUDA(cudaMemsetAsync(sc, 0, sizeof(SolverScalars) * B, stream));
+    DCRF_CUDA(cudaMemsetAsync(done, 0, sizeof(int) * B, stream));
+    // grad_y = unary + sum_k 2 A_k Q; the energy terms Q . A_k Q (the same applies)
+    for (int k = 0; k < nt; k++) {
+        apply(k, tmp, Q);
+        launch(badd_scaled_kernel, ceil_div(NL, 256), 256, 0, stream, NL, grad, tmp, 2.0f);
+        launch(bdot_kernel, B * kRedBlocks, kRedThreads, 0, stream, all, Q, tmp, part);
+        launch(bfinalize_sums_kernel, B, 32, 0, stream, part, 1, 1 + k, done, sc);
+    }
+    launch(bdot_kernel, B * kRedBlocks, kRedThreads, 0, stream, all, unary.get(), Q, part);
+    launch(bfinalize_sums_kernel, B, 32, 0, stream, part, 1, 0, done, sc);
+    launch(bqp_init_energy_kernel, sb, 128, 0, stream, B, sc, nt, max_iter);
+    // a NaN or infinity in Q or the unaries
+    DCRF_CUDA(cudaMemsetAsync(&sc[0].numeric, 0, sizeof(int), stream));
+    launch(nonfinite_kernel, kRedBlocks, kRedThreads, 0, stream, NL, (const float*)Q, (const float*)unary.get(), sc);
+    launch(bqp_cond_kernel, 1, 256, 0, stream, B, (const SolverScalars*)sc, done, flags, 1 << 30, flags + 1,
+           cudaGraphConditionalHandle{}, 0);
+    DCRF_LAUNCH_CHECK();
+    int hf[2] = {0, 0};
+    int numeric = 0;
+    DCRF_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, stream));
+    DCRF_CUDA(cudaMemcpyAsync(&numeric, &sc[0].numeric, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    DCRF_CUDA(cudaStreamSynchronize(stream));
+    if (numeric & 1) throw Error(DCRF_E_NUMERIC, "qp: the initial Q or the unary energy holds a NaN or an infinity");
+
+    // One Frank-Wolfe iteration of every running image (src/densecrf.cpp:389-436)
+    // and the loop test.
+    for (auto& t : terms) t->lat->skip_done = done;  // finished images: no filter work
+    auto iteration = [&](bool graph, cudaGraphConditionalHandle h) {
+        if (tiled) {
+            launch(bqp_direction_tiled<21>, btiles, 32 * kTileWarps, 0, stream, (const int*)btile_img.get(),
+                   (const int*)btile_off.get(), live, (const float*)grad, (const float*)Q,
+                   (const float*)unary.get(), sx, part_dir);
+            launch(bfinalize_large_kernel, B, 1024, 0, stream, (const double*)part_dir, (const int*)btile_off.get(), 0,
+                   (const int*)done, sc);
+        } else {
+            launch(bqp_direction_kernel, B * kRedBlocks, kRedThreads, 0, stream, live, (const float*)grad,
+                   (const float*)Q, (const float*)unary.get(), sx, part);
+            launch(bfinalize_sums_kernel, B, 32, 0, stream, (const double*)part, 1, 0, (const int*)done, sc);
+        }
+        for (int k = 0; k < nt; k++) apply(k, psi, sx, k == 0 ? nullptr : psi, 1.0f, k == 0);
+        if (nt == 0) DCRF_CUDA(cudaMemsetAsync(psi, 0, sizeof(float) * NL, stream));
+        launch(bdots2_kernel, B * kRedBlocks, kRedThreads, 0, stream, live, (const float*)Q, (const float*)sx,
+               (const float*)psi, part);
+        launch(bfinalize_sums_kernel, B, 64, 0, stream, (const double*)part, 2, 1, (const int*)done, sc);
+        launch(bqp_step_kernel, sb, 128, 0, stream, B, (const int*)done, sc);
+        launch(bqp_update_kernel, B * kRedBlocks, kRedThreads, 0, stream, live, (const float*)sx, (const float*)psi,
+               (const float*)unary.get(), Q, grad, (const SolverScalars*)sc, part);
+        launch(bfinalize_sums_kernel, B, 32, 0, stream, (const double*)part, 1, 7, (const int*)done, sc);
+        launch(bqp_energy_kernel, sb, 128, 0, stream, B, (const int*)done, sc, max_iter);
+        launch(bqp_cond_kernel, 1, 256, 0, stream, B, (const SolverScalars*)sc, done, flags, kQpChunk, flags + 1, h,
+               graph ? 1 : 0);
+    };
+    std::vector<const void*> key = {Q, grad, sx, psi, unary.get(), sc, done, part, part_dir,
+                                    (const void*)(uintptr_t)max_iter, (const void*)(uintptr_t)weights_gen};
+    for (auto& t : terms) {
+        key.push_back(t->lat->va.get());
+        key.push_back(t->lat->vb.get());
+        key.push_back(t->lat.get());
+    }
+    int guard = 0;
+    try {
+        while (hf[1]) {
+            require(++guard < (1 << 26), DCRF_E_TIMEOUT, "batch qp: iteration cap reached");
+            if (bqp_graph && key == bqp_key) {
+                DCRF_CUDA(cudaMemsetAsync(flags, 0, sizeof(int), stream));
+                DCRF_CUDA(cudaGraphLaunch(bqp_graph, stream));
+            } else {
+                iteration(false, cudaGraphConditionalHandle{});
+                DCRF_LAUNCH_CHECK();
+            }
+            DCRF_CUDA(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, stream));
+            DCRF_CUDA(cudaStreamSynchronize(stream));
+            if (hf[1] && !(bqp_graph && key == bqp_key) && !bqp_graph_failed && graphs_enabled()) {
+                try {
+                    build_bqp_graph(iteration, flags);
+                    bqp_key = key;
+                } catch (const Error&) {
+                    if (bqp_graph) cudaGraphExecDestroy(bqp_graph);
+                    bqp_graph = nullptr;
+                    bqp_graph_failed = true;  // this device or driver cannot run it: stay eager
+                }
+            }
+        }
+    } catch (...) {
+        for (auto& t : terms) t->lat->skip_done = nullptr;
+        throw;
+    }
+    for (auto& t : terms) t->lat->skip_done = nullptr;
+    std::vector<SolverScalars> hs(B);
+    DCRF_CUDA(cudaMemcpyAsync(hs.data(), sc, sizeof(SolverScalars) * B, cudaMemcpyDeviceToHost, stream));
+    DCRF_CUDA(cudaStreamSynchronize(stream));
+    int most = 0;
+    for (int i = 0; i < B; i++) {
+        if (steps) steps[i] = hs[i].steps;
+        if (energies) energies[i] = hs[i].energy;
+        most = std::max(most, hs[i].steps);
+    }
+    return most;
+}
+
+// The lockstep iteration as a graph: a `while` node whose body is one
+// iteration, its condition set by bqp_cond_kernel (some image runs and fewer
+// than kQpChunk iterations ran in this launch).  The body is checked to end
+// in that kernel, so the loop cannot run on without its test.
+template <typename F>
+void Batch::build_bqp_graph(F&& iteration, int* flags) {
+    std::lock_guard<std::recursive_mutex> cap(capture_mutex());
+    if (bqp_graph) cudaGraphExecDestroy(bqp_graph);
+    bqp_graph = nullptr;
+    cudaGraph_t g = nullptr;
+    DCRF_CUDA(cudaGraphCreate(&g, 0));
+    bool capturing = false;
+    try {
+        cudaGraphConditionalHandle h;
+        DCRF_CUDA(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        cudaGraphNode_t wn;
+        DCRF_CUDA(cudaGraphAddNode(&wn, g, nullptr, 0, &np));
+        const unsigned long long k0 = g_kernel_launches.load();
+        DCRF_CUDA(cudaStreamBeginCaptureToGraph(stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                cudaStreamCaptureModeRelaxed));
+        capturing = true;
+        iteration(true, h);
+        cudaGraph_t bo = nullptr;
+        capturing = false;
+        DCRF_CUDA(cudaStreamEndCapture(stream, &bo));
+        const unsigned long long captured = g_kernel_launches.load() - k0;
+        g_kernel_launches.fetch_sub(captured);
+        require(captured >= 2, DCRF_E_STATE, "batch qp: unexpected loop body");
+        bqp_graph_kernels = captured;
+        DCRF_CUDA(cudaGraphInstantiate(&bqp_graph, g, 0));
+        cudaGraphDestroy(g);
+    } catch (...) {
+        cudaGraph_t junk = nullptr;
+        if (capturing) cudaStreamEndCapture(stream, &junk);
+        cudaGraphDestroy(g);
+        cudaGetLastError();
+        throw;
+    }
+    (void)flags;
+}
+
 void Batch::set_weight(int k, float w) {
     require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
     terms[k]->w = w;
+    weights_gen++;
     for (auto& m : img) m->set_compat(k, kPotts, &w);  // the per-image models' QP graphs are rebuilt
     qp_warm = false;
 }

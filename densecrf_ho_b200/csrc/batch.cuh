@@ -60,6 +60,21 @@ struct Batch {
     // Returns the largest per-image step count; per-image counts / energies
     // go to steps / energies when given (host arrays of B).
     int qp(const float* init, float* out, int max_iter, int* steps, double* energies);
+    // The same solves from up to kQpThreads host threads, each image's own
+    // single-image solve (the earlier form, kept for comparison).
+    int qp_threaded(const float* init, float* out, int max_iter, int* steps, double* energies);
+
+    // Lockstep QP state: per-image scalars and loop flags, per-image partial
+    // sums, the row-tile table of the direction kernel, the loop as a graph.
+    DevBuf<SolverScalars> bsc;
+    DevBuf<int> bdone, bflags, btile_img, btile_off;
+    DevBuf<double> bpart, bpart_dir;
+    int btiles = 0;
+    cudaGraphExec_t bqp_graph = nullptr;
+    std::vector<const void*> bqp_key;
+    unsigned long long bqp_graph_kernels = 0;
+    bool bqp_graph_failed = false;
+    unsigned long long weights_gen = 0;  // bumped by set_weight and add_term (captured scales)
 
     // Mean-field iterations Q_0 = softmax(-U), Q_{t+1} = softmax(-U + sum_k
     // w_k K~_k Q_t) (K~ = the normalised Gaussian / bilateral filter), with
@@ -78,6 +93,8 @@ struct Batch {
     size_t meanfield_state_bytes(int T) const;
 
   private:
+    template <typename F>
+    void build_bqp_graph(F&& iteration, int* flags);
     void ensure_image_models();
     void build_lattice(Term& t);
     int ck_slot(int t) const { return t == mf_T && t % ck_every ? mf_T / ck_every + 1 : t / ck_every; }

@@ -326,10 +326,6 @@ __global__ void seg_fill_kernel(int E, int d1, const int* __restrict__ sorted_en
 // Images whose work a batched solve no longer needs: the filters skip the
 // vertices (and pixels, by their first vertex) of image vimg[v] when
 // done[vimg[v]] is set.  done == nullptr (single images) skips nothing.
-struct Skip {
-    const int* vimg = nullptr;
-    const int* done = nullptr;
-};
 __device__ __forceinline__ bool skipped(const Skip& sk, int v) { return sk.done && sk.done[sk.vimg[v]]; }
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
@@ -516,6 +512,64 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     else if (lane < Lrow) vals[(long)(v + 1) * Lrow + lane] = 0.0f;  // row padding
 }
 
+// Lists of at most kHugeList entries: one warp per vertex, lane = label (in
+// chunks of 32 labels).  The list streams in chunks of 32 entries: each
+// lane loads one entry's pixel, weight and normalisation factor (coalesced,
+// the next chunk's while the current one is summed) and stores them as one
+// 16-byte record in shared memory; then every entry costs one broadcast
+// record read and one coalesced read of the pixel's L input values.  The
+// sum is the same in-order chain per (vertex, label) as splat_kernel's.
+template <bool PRE_NORM, int LC, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS)
+    splat_warp_kernel(int n, int Lrt, const int* __restrict__ order, const int* __restrict__ seg_start,
+                      const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                      const float* __restrict__ in, const float* __restrict__ norm, float* __restrict__ vals,
+                      Skip sk, int Lrow) {
+    const int L = LC ? LC : Lrt;
+    __shared__ float4 rec[WARPS][32];
+    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int unit = blockIdx.x * WARPS + wib;
+    if (unit >= n) return;  // warp-uniform; no block-wide barrier below
+    const int v = order[unit];
+    if (skipped(sk, v)) return;
+    const int s0 = seg_start[v], s1 = seg_start[v + 1];
+    float4* r = rec[wib];
+    for (int kb = 0; kb < L; kb += 32) {
+        const int k = kb + lane;
+        const bool act = k < L;
+        float acc = 0.0f;
+        int p = 0;
+        float w = 0.0f, nn = 1.0f;
+        auto fetch = [&](int base) {
+            const int e = base + lane;
+            if (e < s1) {
+                p = seg_pix[e];
+                w = seg_w[e];
+                if (PRE_NORM) nn = norm[p];
+            }
+        };
+        fetch(s0);
+        for (int c0 = s0; c0 < s1; c0 += 32) {
+            r[lane] = make_float4(__int_as_float(p), w, nn, 0.0f);
+            fetch(c0 + 32);  // in flight while this chunk is summed
+            __syncwarp();
+            const int cnt = min(32, s1 - c0);
+            if (act) {
+#pragma unroll 8
+                for (int e = 0; e < cnt; e++) {
+                    const float4 q = r[e];
+                    float x = in[(long)__float_as_int(q.x) * L + k];
+                    if (PRE_NORM) x = fmul(x, q.z);
+                    acc = fadd(acc, fmul(q.y, x));
+                }
+            }
+            __syncwarp();  // the records are rewritten next chunk
+        }
+        if (act) vals[(long)(v + 1) * Lrow + k] = acc;
+    }
+    for (int k = L + lane; k < Lrow; k += 32) vals[(long)(v + 1) * Lrow + k] = 0.0f;  // row padding
+}
+
 // Short lists (at most kLongList entries; the tail of `order`): one thread
 // per (vertex, label), the same in-order sum without staging.
 template <bool PRE_NORM, int LC = 0>
@@ -647,61 +701,85 @@ __global__ void slice_kernel(int N, int Lrt, int drt, const int* __restrict__ of
 }
 
 // Slice over rows padded to Lp = 4 Q floats (sseCompute, L > 2), a tile of
-// `tile` pixels per block (kSliceTile, fewer for very wide rows): the tile's offsets and (barycentric * alpha)
-// weights are staged once in shared memory (coalesced: they are contiguous),
-// every (pixel, four labels) item gathers the d+1 vertex rows with float4
-// loads, and the tile's L outputs per pixel -- contiguous in `out` -- leave
-// through shared memory with the epilogue, coalesced.  Per element the
-// arithmetic is slice_kernel's: acc = sum over j in order of
-// (bary_j * alpha) * value_j, from +0.
+// `tile` pixels per block (kSliceTile, fewer for very wide rows): the
+// tile's offsets, (barycentric * alpha) weights and normalisation factors
+// are staged once in shared memory (coalesced: they are contiguous), every
+// (pixel, four labels) item gathers the d+1 vertex rows with float4 loads
+// and applies the per-pixel part of the epilogue (norm, compatibility
+// scale), and the tile's L outputs per pixel -- contiguous in `out` --
+// leave through shared memory, coalesced, with the accumulation part
+// (base + coef * v).  Per element the arithmetic is slice_kernel's and
+// apply_epilogue's: acc = sum over j in order of (bary_j * alpha) *
+// value_j, from +0.
 constexpr int kSliceTile = 128;
 constexpr int kSliceThreads = 256;
-template <int DC, int Q>
+template <int DC, int Q, int LC>
 __global__ void __launch_bounds__(kSliceThreads)
-    slice4_kernel(int N, int L, int Qrt, int drt, int tile, const int* __restrict__ offset,
+    slice4_kernel(int N, int Lrt, int Qrt, int drt, int tile, const int* __restrict__ offset,
                   const float* __restrict__ bary, const float* __restrict__ vals, float alpha, float* out,
                   SliceEpilogue ep, Skip sk) {
     extern __shared__ __align__(16) unsigned char slice_smem[];
-    const int d1 = (DC ? DC : drt) + 1, Qn = Q ? Q : Qrt;
+    const int d1 = (DC ? DC : drt) + 1, Qn = Q ? Q : Qrt, L = LC ? LC : Lrt;
     const long lp = 4L * Qn;
     int* s_off = reinterpret_cast<int*>(slice_smem);
     float* s_wa = reinterpret_cast<float*>(s_off + tile * d1);
-    float* s_out = s_wa + tile * d1;
+    float* s_nrm = s_wa + tile * d1;
+    float* s_out = s_nrm + tile;
     const long p0 = (long)blockIdx.x * tile;
     const int np = (int)min((long)tile, (long)N - p0);
     for (int e = threadIdx.x; e < np * d1; e += blockDim.x) {
         s_off[e] = offset[p0 * d1 + e];
         s_wa[e] = fmul(bary[p0 * d1 + e], alpha);
     }
+    const bool use_norm = ep.potts && ep.norm;
+    if (use_norm)
+        for (int e = threadIdx.x; e < np; e += blockDim.x) s_nrm[e] = ep.norm[p0 + e];
     __syncthreads();
     for (int it = threadIdx.x; it < np * Qn; it += blockDim.x) {
         const int pl = it / Qn, q = it - pl * Qn;
         if (skipped(sk, s_off[pl * d1])) continue;
-        float4 acc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
         for (int j = 0; j < (DC ? DC + 1 : 17); j++) {
             if (!DC && j >= d1) break;
             const int o = s_off[pl * d1 + j];
             const float wa = s_wa[pl * d1 + j];
             const float4 v = *reinterpret_cast<const float4*>(vals + (long)(o + 1) * lp + 4 * q);
-            acc.x = fadd(acc.x, fmul(wa, v.x));
-            acc.y = fadd(acc.y, fmul(wa, v.y));
-            acc.z = fadd(acc.z, fmul(wa, v.z));
-            acc.w = fadd(acc.w, fmul(wa, v.w));
+            a[0] = fadd(a[0], fmul(wa, v.x));
+            a[1] = fadd(a[1], fmul(wa, v.y));
+            a[2] = fadd(a[2], fmul(wa, v.z));
+            a[3] = fadd(a[3], fmul(wa, v.w));
         }
-        float* so = s_out + pl * L + 4 * q;
-        const int rem = L - 4 * q;
-        so[0] = acc.x;  // 4 q < L always
-        if (rem > 1) so[1] = acc.y;
-        if (rem > 2) so[2] = acc.z;
-        if (rem > 3) so[3] = acc.w;
+        const int k0 = 4 * q;
+        float* so = s_out + pl * L + k0;
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            if (k0 + c >= L) break;
+            float v = a[c];
+            if (ep.potts) {
+                if (use_norm) v = fmul(v, s_nrm[pl]);
+                v = ep.scale_vec ? fmul(ep.scale_vec[k0 + c], v) : fmul(ep.scale, v);
+            }
+            so[c] = v;
+        }
     }
     __syncthreads();
     const long t0 = p0 * L;
-    for (int e = threadIdx.x; e < np * L; e += blockDim.x) {
-        const int pl = e / L, k = e - pl * L;
-        if (skipped(sk, s_off[pl * d1])) continue;
-        out[t0 + e] = apply_epilogue(s_out[e], t0 + e, (int)(p0 + pl), k, ep);
+    const int ne = np * L;
+    if (sk.done) {  // batched solves: pixels of finished images keep their output
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            if (skipped(sk, s_off[(e / L) * d1])) continue;
+            float v = s_out[e];
+            if (ep.base) v = fadd(ep.base[t0 + e], fmul(ep.coef, v));
+            else if (ep.zero_base) v = fadd(0.0f, fmul(ep.coef, v));
+            out[t0 + e] = v;
+        }
+    } else if (ep.base) {
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = fadd(ep.base[t0 + e], fmul(ep.coef, s_out[e]));
+    } else if (ep.zero_base) {
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = fadd(0.0f, fmul(ep.coef, s_out[e]));
+    } else {
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = s_out[e];
     }
 }
 
@@ -850,7 +928,8 @@ constexpr int kOrdBlockMaxL = 160;      // larger L use ord_splat_kernel (shared
 constexpr int kGroupChoices[] = {1, 2, 3, 5, 10};
 
 // Bin split with the fewest warp instructions per list entry: warps x (three
-// instructions per bin slot + about two for the shared-memory loads).
+// instructions per bin slot -- two masks and one f32x2 FMA -- + about two
+// for the shared-memory loads).
 int ord_groups_cheapest(int L) {
     int best = 1;
     long best_cost = -1;
@@ -879,7 +958,7 @@ size_t ord_block_smem(int kb) {
 // staging threads are entry-major (t = g * nk + k) so one warp's copies read
 // consecutive labels of one pixel.
 template <int G>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(kOrdBlockMaxL * G < 1024 ? kOrdBlockMaxL * G : 1024)
     ord_splat_block_kernel(int L, int kb, int kblocks, const int* __restrict__ order,
                            const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
                            const float* __restrict__ seg_w, const float2* __restrict__ bins,
@@ -950,10 +1029,13 @@ __global__ void __launch_bounds__(1024)
         cp_async_commit();
     }
 
-    float lo[NB], up[NB], bf[NB];  // lower / upper sums of bin g*NB + i
+    // Bin g*NB + i's (lower, upper) sums as one packed pair: ord_step2 adds
+    // an entry to both with one f32x2 FMA (each half rounded as fma.rn.f32).
+    unsigned long long acc[NB];
+    float bf[NB];
 #pragma unroll
     for (int i = 0; i < NB; i++) {
-        lo[i] = up[i] = 0.0f;
+        acc[i] = 0ull;
         bf[i] = (float)(g * NB + i);
     }
     for (int c = 0; c < nch; c++) {
@@ -964,30 +1046,38 @@ __global__ void __launch_bounds__(1024)
         cp_async_commit();
         if (worker) {
             const float4* xs = reinterpret_cast<const float4*>(&xr[((size_t)(c % kOXS) * kb + k) * kORow]);
-            const float4* ws = reinterpret_cast<const float4*>(&wr[(c % kOPS) * kOE * 2]);
+            const ulonglong2* ws = reinterpret_cast<const ulonglong2*>(&wr[(c % kOPS) * kOE * 2]);
             const int n2 = (min(kOE, s1 - (s0 + c * kOE)) + 1) >> 1;
-            // Eight entries per batch: their loads are issued together, then
-            // summed.  A batch may run past n2 into the chunk's zero-weight
-            // tail (the ring rows hold kOE entries).
+            // Batches of eight entries, the next batch's loads issued before
+            // this batch is summed.  A batch may run past n2 into the chunk's
+            // zero-weight tail (the ring rows hold kOE entries).
+            float4 x[4];      // (c_lower, c_upper) of entries 2 j, 2 j + 1
+            ulonglong2 w[4];  // ((w, w), (w, w)) of the same entries
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                x[j] = xs[j];
+                w[j] = ws[j];
+            }
             for (int b0 = 0; b0 < n2; b0 += 4) {
-                float4 x[4], w[4];  // (c_lower, c_upper) and (w, w) of entries 2 j, 2 j + 1
+                float4 xn[4];
+                ulonglong2 wn[4];
+                const int nb0 = b0 + 4 < kOE / 2 ? b0 + 4 : b0;  // stays inside the ring row
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
-                    x[j] = xs[b0 + j];
-                    w[j] = ws[b0 + j];
+                    xn[j] = xs[nb0 + j];
+                    wn[j] = ws[nb0 + j];
                 }
 #pragma unroll
                 for (int j = 0; j < 4; j++) {
 #pragma unroll
-                    for (int i = 0; i < NB; i++) {
-                        lo[i] = __fmaf_rn(step_ge(x[j].x, bf[i]), w[j].x, lo[i]);
-                        up[i] = __fmaf_rn(step_ge(bf[i], x[j].y), w[j].y, up[i]);
-                    }
+                    for (int i = 0; i < NB; i++) ord_step2(acc[i], x[j].x, x[j].y, bf[i], w[j].x);
 #pragma unroll
-                    for (int i = 0; i < NB; i++) {
-                        lo[i] = __fmaf_rn(step_ge(x[j].z, bf[i]), w[j].z, lo[i]);
-                        up[i] = __fmaf_rn(step_ge(bf[i], x[j].w), w[j].w, up[i]);
-                    }
+                    for (int i = 0; i < NB; i++) ord_step2(acc[i], x[j].z, x[j].w, bf[i], w[j].y);
+                }
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    x[j] = xn[j];
+                    w[j] = wn[j];
                 }
             }
         }
@@ -998,8 +1088,9 @@ __global__ void __launch_bounds__(1024)
 #pragma unroll
         for (int i = 0; i < NB; i++) {
             if (g * NB + i >= kRes) break;
-            row[(long)(g * NB + i) * L] = lo[i];
-            row[(long)(kRes + g * NB + i) * L] = up[i];
+            const float2 r = unpack2(acc[i]);
+            row[(long)(g * NB + i) * L] = r.x;
+            row[(long)(kRes + g * NB + i) * L] = r.y;
         }
     }
 }
@@ -1166,6 +1257,101 @@ __global__ void __launch_bounds__(kTB, 8) ord_slice_pair_kernel(int N, int Lrt, 
         float s1 = a1;
         if (t1.ep.potts) {
             if (t1.ep.norm) s1 = fmul(s1, t1.ep.norm[i]);
+            s1 = t1.ep.scale_vec ? fmul(t1.ep.scale_vec[k], s1) : fmul(t1.ep.scale, s1);
+        }
+        const float v = fadd(v0, fmul(t1.ep.coef, s1));
+        out[t] = v;
+        if (GAP) {
+            const float tmp = fsub(fadd(gf.alpha[t], gf.u[t]), fadd(v, gf.su ? gf.su[t] : 0.0f));
+            g0 = (double)tmp * (double)gf.Q[t];
+            g1 = (double)tmp * (double)tmp;
+        }
+    }
+    if (GAP) {
+        __shared__ double s0[kTB / 32], s1[kTB / 32];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            g0 += __shfl_down_sync(0xffffffffu, g0, o);
+            g1 += __shfl_down_sync(0xffffffffu, g1, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            s0[threadIdx.x >> 5] = g0;
+            s1[threadIdx.x >> 5] = g1;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double a = 0.0, b = 0.0;
+            for (int w = 0; w < kTB / 32; w++) {
+                a += s0[w];
+                b += s1[w];
+            }
+            gf.partials[blockIdx.x] = a;
+            gf.partials[gridDim.x + blockIdx.x] = b;
+        }
+    }
+}
+
+// ord_slice_pair_kernel for the LP's common case (L = 21, a d = 2 and a
+// d = 5 term) with the per-pixel data staged: a block covers the same 256
+// elements (at most 14 pixels), and its pixels' offsets, alpha-scaled
+// barycentric weights and normalisation factors are loaded once, coalesced,
+// into shared memory instead of by each label's thread.  Element, block and
+// dual-gap partial sums are those of ord_slice_pair_kernel, so the values
+// are too: the lower pass's fmul(-w, alpha) is the exact negation of
+// fmul(w, alpha).
+template <bool GAP>
+__global__ void __launch_bounds__(kTB, 8) ord_slice_pair_staged(int N, OrdSliceTerm t0, OrdSliceTerm t1,
+                                                               const float2* __restrict__ bins, float* out,
+                                                               GapFusion gf) {
+    constexpr int L = 21, D0 = 3, D1 = 6, P = kTB / L + 2;  // pixels a block touches at most
+    __shared__ int so0[P * D0], so1[P * D1];
+    __shared__ float sw0[P * D0], sw1[P * D1], sn0[P], sn1[P];
+    const long NL = (long)N * L;
+    const long tb = (long)blockIdx.x * blockDim.x;
+    const long t = tb + threadIdx.x;
+    const int pf = (int)(tb / L);
+    const int np = (int)min((long)P, (long)N - pf);
+    for (int e = threadIdx.x; e < np * D0; e += blockDim.x) {
+        so0[e] = t0.offset[(long)pf * D0 + e];
+        sw0[e] = fmul(t0.bary[(long)pf * D0 + e], t0.alpha);
+    }
+    for (int e = threadIdx.x; e < np * D1; e += blockDim.x) {
+        so1[e] = t1.offset[(long)pf * D1 + e];
+        sw1[e] = fmul(t1.bary[(long)pf * D1 + e], t1.alpha);
+    }
+    if (threadIdx.x < np) {
+        if (t0.ep.norm) sn0[threadIdx.x] = t0.ep.norm[pf + threadIdx.x];
+        if (t1.ep.norm) sn1[threadIdx.x] = t1.ep.norm[pf + threadIdx.x];
+    }
+    __syncthreads();
+    double g0 = 0.0, g1 = 0.0;
+    if (t < NL) {
+        const int i = (int)(t / L), k = (int)(t - (long)i * L), li = i - pf;
+        const float2 bp = bins[t];
+        const int cl = ord_lower_of(bp), cu = ord_upper_of(bp);
+        float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll
+        for (int j = 0; j < D0; j++)
+            a0 = fadd(a0, fmul(t0.vals[((long)(so0[li * D0 + j] + 1) * kOrdW + cl) * L + k], -sw0[li * D0 + j]));
+#pragma unroll
+        for (int j = 0; j < D0; j++)
+            a0 = fadd(a0, fmul(t0.vals[((long)(so0[li * D0 + j] + 1) * kOrdW + kRes + cu) * L + k], sw0[li * D0 + j]));
+#pragma unroll
+        for (int j = 0; j < D1; j++)
+            a1 = fadd(a1, fmul(t1.vals[((long)(so1[li * D1 + j] + 1) * kOrdW + cl) * L + k], -sw1[li * D1 + j]));
+#pragma unroll
+        for (int j = 0; j < D1; j++)
+            a1 = fadd(a1, fmul(t1.vals[((long)(so1[li * D1 + j] + 1) * kOrdW + kRes + cu) * L + k], sw1[li * D1 + j]));
+        float v0 = a0;
+        if (t0.ep.potts) {
+            if (t0.ep.norm) v0 = fmul(v0, sn0[li]);
+            v0 = t0.ep.scale_vec ? fmul(t0.ep.scale_vec[k], v0) : fmul(t0.ep.scale, v0);
+        }
+        if (t0.ep.base) v0 = fadd(t0.ep.base[t], fmul(t0.ep.coef, v0));
+        else if (t0.ep.zero_base) v0 = fadd(0.0f, fmul(t0.ep.coef, v0));
+        float s1 = a1;
+        if (t1.ep.potts) {
+            if (t1.ep.norm) s1 = fmul(s1, sn1[li]);
             s1 = t1.ep.scale_vec ? fmul(t1.ep.scale_vec[k], s1) : fmul(t1.ep.scale, s1);
         }
         const float v = fadd(v0, fmul(t1.ep.coef, s1));
@@ -1635,62 +1821,193 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
 // keeps L.
 static int value_row(int L) { return L > 2 ? (L + 3) & ~3 : L; }
 
+// The warp splat (L = 21) over order[first, first + count) with `warps`
+// vertices per block.
+static void splat_warp_range(const Lattice& lat, int warps, int first, int count, int L, int Lp, const float* in,
+                             const float* pre_norm, float* vals, const Skip& sk, cudaStream_t st) {
+    if (count <= 0) return;
+    auto go = [&](auto kern, int w) {
+        launch(kern, ceil_div(count, w), 32 * w, 0, st, count, L, lat.vorder.get() + first, lat.seg_start.get(),
+               lat.seg_pix.get(), lat.seg_w.get(), in, pre_norm, vals, sk, Lp);
+    };
+    if (pre_norm) {
+        if (warps == 2) go(splat_warp_kernel<true, 21, 2>, 2);
+        else if (warps == 8) go(splat_warp_kernel<true, 21, 8>, 8);
+        else go(splat_warp_kernel<true, 21, 4>, 4);
+    } else {
+        if (warps == 2) go(splat_warp_kernel<false, 21, 2>, 2);
+        else if (warps == 8) go(splat_warp_kernel<false, 21, 8>, 8);
+        else go(splat_warp_kernel<false, 21, 4>, 4);
+    }
+}
+
+namespace {
+constexpr int kTuneMinPixels = 1 << 18;  // smaller lattices keep the default shapes
+std::mutex g_tune_mu;
+std::vector<std::pair<std::vector<long>, FilterShape>>& tune_cache() {
+    static auto* c = new std::vector<std::pair<std::vector<long>, FilterShape>>();  // never destroyed
+    return *c;
+}
+bool autotune_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("DCRF_AUTOTUNE");
+        return !(v && v[0] == '0');
+    }();
+    return on;
+}
+}  // namespace
+
+void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
+    shape_L = L;  // also when the defaults stay
+    if (N < kTuneMinPixels || !autotune_enabled()) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    DCRF_CUDA(cudaStreamIsCapturing(stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {  // no timing inside a capture: defaults, tuned next time
+        shape_L = 0;
+        return;
+    }
+    int dev = 0;
+    DCRF_CUDA(cudaGetDevice(&dev));
+    int lg = 0;
+    while ((1L << (lg + 1)) <= (long)N) lg++;
+    const std::vector<long> key = {dev, L, d, lg, M / std::max(N / 64, 1)};
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        for (const auto& e : tune_cache())
+            if (e.first == key) {
+                shape = e.second;
+                return;
+            }
+    }
+    const int Lp = value_row(L);
+    cudaStream_t st = stream;
+    cudaEvent_t e0, e1;
+    DCRF_CUDA(cudaEventCreate(&e0));
+    DCRF_CUDA(cudaEventCreate(&e1));
+    auto timed = [&](auto&& fn) {
+        fn();  // warm
+        DCRF_CUDA(cudaEventRecord(e0, st));
+        for (int r = 0; r < 2; r++) fn();
+        DCRF_CUDA(cudaEventRecord(e1, st));
+        DCRF_CUDA(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        DCRF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+        return ms;
+    };
+    FilterShape best;
+    float* src = va.get();
+    float* dst = vb.get();
+    const Skip none{};
+    float tbest = 1e30f;
+    for (int kind = 0; kind < 3; kind++) {
+        for (int w : {2, 4, 8}) {
+            if (kind == 0 && w != 4) continue;  // no warp splat in this form
+            FilterShape fs = best;
+            fs.splat_kind = kind;
+            fs.splat_warps = w;
+            const float t = timed([&] { splat_rest(fs, in, L, pre_norm, src, none, st); });
+            if (t < tbest) {
+                tbest = t;
+                best.splat_kind = kind;
+                best.splat_warps = w;
+            }
+        }
+    }
+    const int Q = Lp / 4;
+    const long MQ = (long)M * Q;
+    tbest = 1e30f;
+    for (int bt : {128, 256, 512}) {
+        const float t = timed([&] {
+            launch(blur4_kernel<6>, ceil_div(MQ, bt), bt, 0, st, M, Q, nbr.get(), (const float*)src, dst, none);
+        });
+        if (t < tbest) tbest = t, best.blur_threads = bt;
+    }
+    {
+        DevBuf<float> probe;  // the slice candidates write here, not to the caller's output
+        float* o = probe.ensure((size_t)N * L);
+        const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
+        const SliceEpilogue ep;
+        const int per_px = (d + 1) * 8 + 4 + L * 4;
+        tbest = 1e30f;
+        for (int tile : {64, 128, 256}) {
+            const int tl = std::max(1, std::min(tile, (40 << 10) / per_px));
+            const float t = timed([&] {
+                auto sl = [&](auto kern) {
+                    launch(kern, ceil_div(N, tl), kSliceThreads, (size_t)tl * per_px, st, N, L, Q, d, tl,
+                           offset.get(), bary.get(), (const float*)src, alpha, o, ep, none);
+                };
+                if (d == 5) sl(slice4_kernel<5, 6, 21>);
+                else if (d == 2) sl(slice4_kernel<2, 6, 21>);
+                else sl(slice4_kernel<0, 0, 0>);
+            });
+            if (t < tbest) tbest = t, best.slice_tile = tile;
+        }
+        DCRF_CUDA(cudaStreamSynchronize(st));  // before the probe buffer goes back
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    DCRF_LAUNCH_CHECK();
+    shape = best;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    tune_cache().push_back({key, best});
+}
+
+void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
+                         const Skip& sk, cudaStream_t st) {
+    const int Lp = value_row(L);
+    const int nh = n_huge, n_short = M - n_long;
+    const int kind = L == 21 ? fs.splat_kind : 0;
+    if (kind == 2) {
+        splat_warp_range(*this, fs.splat_warps, nh, M - nh, L, Lp, in, pre_norm, vals, sk, st);
+        return;
+    }
+    if (n_long > nh) {
+        if (kind == 1)
+            splat_warp_range(*this, fs.splat_warps, nh, n_long - nh, L, Lp, in, pre_norm, vals, sk, st);
+        else
+            launch(L == 21 ? (pre_norm ? splat_kernel<true, 21> : splat_kernel<false, 21>)
+                           : (pre_norm ? splat_kernel<true> : splat_kernel<false>),
+                   ceil_div(n_long - nh, kStageWarps), 32 * kStageWarps, 0, st, n_long - nh, L, vorder.get() + nh,
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals, sk, Lp);
+    }
+    if (n_short)
+        launch(L == 21 ? (pre_norm ? splat_short_kernel<true, 21> : splat_short_kernel<false, 21>)
+                       : (pre_norm ? splat_short_kernel<true> : splat_short_kernel<false>),
+               ceil_div((long)n_short * Lp, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long, seg_start.get(),
+               seg_pix.get(), seg_w.get(), in, pre_norm, vals, sk, Lp);
+}
+
 void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_norm) {
     require(L >= 1, DCRF_E_ARG, "compute: L must be >= 1");
     const int Lp = value_row(L);
     ensure_values((size_t)Lp);
+    if (L == 21 && shape_L != L) tune_shape(in, L, pre_norm);
     cudaStream_t st = stream;
     const long ML = (long)M * L;
     float *src = va.get(), *dst = vb.get();
-    const int n_short = M - n_long;
-    const long SL = (long)n_short * Lp;
     const Skip sk{vimg.get(), skip_done};
-    // As in the ordered filter, the lists longer than kHugeList run on the
-    // high-priority side stream while the others are splatted.
+    // As in the ordered filter, the lists longer than kHugeList (the first
+    // nh of the order) run on the high-priority side stream while the
+    // others are splatted: with L = 21 by the transposing ring (one warp's
+    // chain sets their time, and its three chunks of copies in flight hide
+    // the load latency a lone warp cannot hide otherwise), else by
+    // splat_kernel.
     const int nh = n_huge;
     const bool forked = nh > 0;
     if (forked) {
         ensure_aux();
         DCRF_CUDA(cudaEventRecord(ev_fork, st));
         DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
-    }
-    auto long_range = [&](int first, int count, cudaStream_t ls) {
-        if (count <= 0) return;
-        // The lists longer than kHugeList (the first nh of the order) use the
-        // transposing ring: one warp's chain sets their time, and it issues
-        // about half the instructions per entry.  On the shorter long lists,
-        // where many warps share the SMs, splat_kernel measured faster.
-        if (L == 21 && first < nh) {
-            if (pre_norm)
-                launch(splat_ring21_kernel<true>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count,
-                       vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk, Lp);
-            else
-                launch(splat_ring21_kernel<false>, ceil_div(count, kStageWarps), 32 * kStageWarps, 0, ls, count,
-                       vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, (const float*)nullptr,
-                       src, sk, Lp);
-            return;
-        }
-        if (pre_norm)
-            launch(L == 21 ? splat_kernel<true, 21> : splat_kernel<true>, ceil_div(count, kStageWarps),
-                   32 * kStageWarps, 0, ls, count, L,
-                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk, Lp);
+        if (L == 21)
+            launch(pre_norm ? splat_ring21_kernel<true> : splat_ring21_kernel<false>, ceil_div(nh, kStageWarps),
+                   32 * kStageWarps, 0, aux, nh, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in,
+                   pre_norm, src, sk, Lp);
         else
-            launch(L == 21 ? splat_kernel<false, 21> : splat_kernel<false>, ceil_div(count, kStageWarps),
-                   32 * kStageWarps, 0, ls, count, L,
-                   vorder.get() + first, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk, Lp);
-    };
-    long_range(0, nh, forked ? aux : st);
-    long_range(nh, n_long - nh, st);
-    if (n_short) {
-        if (pre_norm)
-            launch(L == 21 ? splat_short_kernel<true, 21> : splat_short_kernel<true>, ceil_div(SL, kTB), kTB, 0, st,
-                   n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, sk, Lp);
-        else
-            launch(L == 21 ? splat_short_kernel<false, 21> : splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st,
-                   n_short, L, vorder.get() + n_long,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, sk, Lp);
+            launch(pre_norm ? splat_kernel<true> : splat_kernel<false>, ceil_div(nh, kStageWarps),
+                   32 * kStageWarps, 0, aux, nh, L, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in,
+                   pre_norm, src, sk, Lp);
     }
+    splat_rest(shape, in, L, pre_norm, src, sk, st);
     if (forked) {
         DCRF_CUDA(cudaEventRecord(ev_join, aux));
         DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
@@ -1704,7 +2021,8 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
         if (seq)
             launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nb, src, dst, sk);
         else if (Q == 6)
-            launch(blur4_kernel<6>, ceil_div(MQ, kTB), kTB, 0, st, M, Q, nb, src, dst, sk);
+            launch(blur4_kernel<6>, ceil_div(MQ, shape.blur_threads), shape.blur_threads, 0, st, M, Q, nb, src, dst,
+                   sk);
         else
             launch(blur4_kernel<0>, ceil_div(MQ, kTB), kTB, 0, st, M, Q, nb, src, dst, sk);
         std::swap(src, dst);
@@ -1726,16 +2044,16 @@ void Lattice::slice(float* out, int L, const SliceEpilogue& ep) {
     } else {
         const int Q = value_row(L) / 4;
         // pixels per tile: kSliceTile, fewer for very wide rows (40 KB of shared memory at most)
-        const int per_px = (d + 1) * 8 + L * 4;
-        const int tile = std::max(1, std::min(kSliceTile, (40 << 10) / per_px));
+        const int per_px = (d + 1) * 8 + 4 + L * 4;
+        const int tile = std::max(1, std::min(L == 21 ? shape.slice_tile : kSliceTile, (40 << 10) / per_px));
         const size_t smem = (size_t)tile * per_px;
         auto sl = [&](auto kern) {
             launch(kern, ceil_div(N, tile), kSliceThreads, smem, st, N, L, Q, d, tile, offset.get(), bary.get(), src,
                    alpha, out, ep, sks);
         };
-        if (d == 5 && Q == 6) sl(slice4_kernel<5, 6>);
-        else if (d == 2 && Q == 6) sl(slice4_kernel<2, 6>);
-        else sl(slice4_kernel<0, 0>);
+        if (d == 5 && L == 21) sl(slice4_kernel<5, 6, 21>);
+        else if (d == 2 && L == 21) sl(slice4_kernel<2, 6, 21>);
+        else sl(slice4_kernel<0, 0, 0>);
     }
     DCRF_LAUNCH_CHECK();
 }
@@ -1831,9 +2149,14 @@ void Lattice::ord_slice_pair(float* out, const float2* bins, int L, const Lattic
     auto sl = [&](auto kern) {
         launch(kern, ceil_div(NL, kTB), kTB, 0, a.stream, a.N, L, t0, t1, bins, out, gf);
     };
-    const bool common = L == 21 && a.d == 2 && b.d == 5;
-    if (gap) sl(common ? ord_slice_pair_kernel<true, 2, 5, 21> : ord_slice_pair_kernel<true, 0, 0, 0>);
-    else sl(common ? ord_slice_pair_kernel<false, 2, 5, 21> : ord_slice_pair_kernel<false, 0, 0, 0>);
+    if (L == 21 && a.d == 2 && b.d == 5) {
+        launch(gap ? ord_slice_pair_staged<true> : ord_slice_pair_staged<false>, ceil_div(NL, kTB), kTB, 0,
+               a.stream, a.N, t0, t1, bins, out, gf);
+    } else if (gap) {
+        sl(ord_slice_pair_kernel<true, 0, 0, 0>);
+    } else {
+        sl(ord_slice_pair_kernel<false, 0, 0, 0>);
+    }
     DCRF_LAUNCH_CHECK();
 }
 

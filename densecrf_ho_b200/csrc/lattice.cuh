@@ -48,8 +48,33 @@ int slice_grid(long n);
 // Capacity, in floats, of the fixed scratch array of compute_noalloc.
 size_t noalloc_scratch_floats();
 
+// Per-vertex skip flags of a concatenated lattice: vertex v is skipped when
+// done[vimg[v]] is set (no flags: nothing is skipped).
+struct Skip {
+    const int* vimg = nullptr;
+    const int* done = nullptr;
+};
+
+// Launch shapes of the plain filter for L = 21 (Lattice::splat_blur /
+// slice).  Every shape computes the same arithmetic; only the speed
+// differs.  Lattice::tune_shape picks them by timing, once per device and
+// problem class (L, d, size), and caches the choice for the process.
+struct FilterShape {
+    // Splat of the lists up to the huge-list threshold (L = 21):
+    // 0 = staged splat_kernel for the long lists, one thread per (vertex,
+    //     label) for the short ones;
+    // 1 = warp splat for the long lists, the thread form for the short ones;
+    // 2 = warp splat for every list.
+    int splat_kind = 0;
+    int splat_warps = 4;     // vertices (warps) per block of the warp splat: 2, 4 or 8
+    int blur_threads = 256;  // threads per block of the float4 blur: 128, 256 or 512
+    int slice_tile = 128;    // pixels per block of the tiled slice: 64, 128 or 256
+};
+
 struct Lattice {
     int N = 0, d = 0, M = 0;
+    FilterShape shape;      // launch shapes in use
+    int shape_L = 0;        // the label count they were tuned for (0: defaults)
     int n_long = 0;  // vertices whose splat list exceeds the staging threshold
     int n_huge = 0;  // ... and the (leading) ones whose list is very long
     cudaStream_t stream = nullptr;  // borrowed
@@ -127,6 +152,14 @@ struct Lattice {
 
     void ensure_values(size_t row_width);
     void ensure_aux();
+    // Times the candidate shapes on this lattice with the input `in` (the
+    // first large call) unless the process has tuned this problem class
+    // already; outputs are not touched.
+    void tune_shape(const float* in, int L, const float* pre_norm);
+    // Splat of every list after the first n_huge (whose splat runs on the
+    // side stream) into vals, in the form `fs` names.
+    void splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
+                    const Skip& sk, cudaStream_t st);
 
     Lattice() = default;
     Lattice(const Lattice&) = delete;

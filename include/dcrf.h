@@ -417,6 +417,13 @@ dcrf_status dcrf_batch_stream(dcrf_batch b, void** stream);
  * bit (no splat list, blur neighbour or slice crosses an image). */
 dcrf_status dcrf_batch_pairwise_apply(dcrf_batch b, int k, float* out, const float* in);
 dcrf_status dcrf_batch_pairwise_apply_dev(dcrf_batch b, int k, float* d_out, const float* d_in);
+/* The launch shapes the filter of term k uses, as the autotuner chose them
+ * (shape[0] warp-splat vertices per block, [1] blur threads per block, [2]
+ * slice pixels per block, [3] splat form: 0 staged long lists + thread-per-
+ * label short lists, 1 warp splat for the long lists, 2 warp splat for
+ * every list); the defaults until a filter call of 2^18 pixels or more has
+ * tuned them.  shape holds 4 ints.  No counterpart in the reference. */
+dcrf_status dcrf_batch_filter_shape(dcrf_batch b, int k, int* shape);
 /* Vertex count of term k's concatenated lattice (the sum of the images' M). */
 dcrf_status dcrf_batch_lattice_size(dcrf_batch b, int k, int64_t* M);
 
