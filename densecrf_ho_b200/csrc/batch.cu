@@ -10,10 +10,7 @@
 
 #include "batch.cuh"
 
-#include <atomic>
-#include <exception>
 #include <mutex>
-#include <thread>
 #include "model_kernels.cuh"
 
 namespace dcrf {
@@ -100,15 +97,32 @@ __global__ void accumulate_total_kernel(const double* __restrict__ partials, int
 // single image of that size (kRedBlocks virtual blocks striding over the
 // image's elements, or its row tiles), and every image keeps its own
 // SolverScalars, so each image's trajectory, output and energy are those of
-// its own solve.  Images whose loop has ended (done[i]) are skipped by every
-// kernel, the filters included (Lattice::skip_done).
+// its own solve.  Each iteration starts by compacting the images still
+// running (live_build_kernel); every kernel of the iteration, the filters
+// included (Lattice::live_n), then loops over the live images' work only,
+// with grids sized for the device rather than for the batch.
 constexpr int kBPart = 2 * kRedBlocks;  // partial slots per image (two values at most)
 
 struct BImages {
-    const long* pix_off;  // B + 1 pixel offsets
-    const int* done;      // per image: its loop has ended
+    const long* pix_off;            // B + 1 pixel offsets
+    const int* live_n = nullptr;    // live images (device), or nullptr: every image
+    const int* live_img = nullptr;
+    int B;
     int L;
 };
+
+// Virtual blocks (image, vb) of every image or of the live images, numbered
+// image after image; the kernels loop over them block-uniformly.
+__device__ __forceinline__ long vblocks_total(const BImages& bi) {
+    return (long)(bi.live_n ? *bi.live_n : bi.B) * kRedBlocks;
+}
+__device__ __forceinline__ void vblock_at(const BImages& bi, long u, int& img, int& vb, long& base, long& n) {
+    const int r = (int)(u / kRedBlocks);
+    vb = (int)(u - (long)r * kRedBlocks);
+    img = bi.live_n ? bi.live_img[r] : r;
+    base = bi.pix_off[img] * bi.L;
+    n = (bi.pix_off[img + 1] - bi.pix_off[img]) * bi.L;
+}
 
 // block_sum_store for virtual block vb of an image: partials[j kRedBlocks + vb].
 template <int NV>
@@ -130,139 +144,145 @@ __device__ __forceinline__ void vblock_store(double (&v)[NV], double* partials, 
     }
 }
 
-// Virtual block (image, vb) of blockIdx.x; false when the image is done.
-__device__ __forceinline__ bool vblock(const BImages& bi, int& img, int& vb, long& base, long& n) {
-    img = blockIdx.x / kRedBlocks;
-    vb = blockIdx.x - img * kRedBlocks;
-    if (bi.done && bi.done[img]) return false;  // block-uniform
-    base = bi.pix_off[img] * bi.L;
-    n = (bi.pix_off[img + 1] - bi.pix_off[img]) * bi.L;
-    return true;
-}
-
 // dot_kernel per image: partials of a . b.
 __global__ void bdot_kernel(BImages bi, const float* __restrict__ a, const float* __restrict__ b,
                             double* __restrict__ part) {
-    int img, vb;
-    long base, n;
-    if (!vblock(bi, img, vb, base, n)) return;
-    double v[1] = {0.0};
-    for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x)
-        v[0] += (double)a[base + t] * (double)b[base + t];
-    vblock_store<1>(v, part + (long)img * kBPart, vb);
+    for (long u = blockIdx.x; u < vblocks_total(bi); u += gridDim.x) {
+        int img, vb;
+        long base, n;
+        vblock_at(bi, u, img, vb, base, n);
+        double v[1] = {0.0};
+        for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x)
+            v[0] += (double)a[base + t] * (double)b[base + t];
+        vblock_store<1>(v, part + (long)img * kBPart, vb);
+        __syncthreads();  // vblock_store's shared sums are rewritten next
+    }
 }
 
 // dots2_kernel per image: partials of a . c and b . c.
 __global__ void bdots2_kernel(BImages bi, const float* __restrict__ a, const float* __restrict__ b,
                               const float* __restrict__ c, double* __restrict__ part) {
-    int img, vb;
-    long base, n;
-    if (!vblock(bi, img, vb, base, n)) return;
-    double v[2] = {0.0, 0.0};
-    for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x) {
-        const double cc = c[base + t];
-        v[0] += (double)a[base + t] * cc;
-        v[1] += (double)b[base + t] * cc;
+    for (long u = blockIdx.x; u < vblocks_total(bi); u += gridDim.x) {
+        int img, vb;
+        long base, n;
+        vblock_at(bi, u, img, vb, base, n);
+        double v[2] = {0.0, 0.0};
+        for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x) {
+            const double cc = c[base + t];
+            v[0] += (double)a[base + t] * cc;
+            v[1] += (double)b[base + t] * cc;
+        }
+        vblock_store<2>(v, part + (long)img * kBPart, vb);
+        __syncthreads();
     }
-    vblock_store<2>(v, part + (long)img * kBPart, vb);
 }
 
 // qp_update_kernel per image.
 __global__ void bqp_update_kernel(BImages bi, const float* __restrict__ sx, const float* __restrict__ psi,
                                   const float* __restrict__ U, float* __restrict__ Q, float* __restrict__ grad,
                                   const SolverScalars* __restrict__ sc, double* __restrict__ part) {
-    int img, vb;
-    long base, n;
-    if (!vblock(bi, img, vb, base, n)) return;
-    if (sc[img].zero_step) return;
-    const float fs = sc[img].fstep, f2s = sc[img].f2step;
-    double v[1] = {0.0};
-    for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x) {
-        const long e = base + t;
-        const float q = fadd(Q[e], fmul(fs, sx[e]));
-        const float g = fadd(grad[e], fadd(fmul(f2s, psi[e]), fmul(fs, 0.0f)));
-        Q[e] = q;
-        grad[e] = g;
-        v[0] += (double)q * (double)fadd(g, U[e]);
+    for (long u = blockIdx.x; u < vblocks_total(bi); u += gridDim.x) {
+        int img, vb;
+        long base, n;
+        vblock_at(bi, u, img, vb, base, n);
+        if (sc[img].zero_step) continue;  // block-uniform
+        const float fs = sc[img].fstep, f2s = sc[img].f2step;
+        double v[1] = {0.0};
+        for (long t = (long)vb * blockDim.x + threadIdx.x; t < n; t += (long)kRedBlocks * blockDim.x) {
+            const long e = base + t;
+            const float q = fadd(Q[e], fmul(fs, sx[e]));
+            const float g = fadd(grad[e], fadd(fmul(f2s, psi[e]), fmul(fs, 0.0f)));
+            Q[e] = q;
+            grad[e] = g;
+            v[0] += (double)q * (double)fadd(g, U[e]);
+        }
+        vblock_store<1>(v, part + (long)img * kBPart, vb);
+        __syncthreads();
     }
-    vblock_store<1>(v, part + (long)img * kBPart, vb);
 }
 
 // qp_direction_kernel per image (run-time L): one-hot of the first arg-min
 // of grad minus Q, and partials of U . sx.
 __global__ void bqp_direction_kernel(BImages bi, const float* __restrict__ grad, const float* __restrict__ Q,
                                      const float* __restrict__ U, float* __restrict__ sx, double* __restrict__ part) {
-    int img, vb;
-    long base, n;
-    if (!vblock(bi, img, vb, base, n)) return;
     const int L = bi.L;
-    const long p0 = bi.pix_off[img], np = bi.pix_off[img + 1] - p0;
-    double v[1] = {0.0};
-    for (long i = (long)vb * blockDim.x + threadIdx.x; i < np; i += (long)kRedBlocks * blockDim.x) {
-        const float* g = grad + (p0 + i) * L;
-        float best = g[0];
-        int bk = 0;
-        for (int k = 1; k < L; k++)
-            if (g[k] < best) {
-                best = g[k];
-                bk = k;
+    for (long u = blockIdx.x; u < vblocks_total(bi); u += gridDim.x) {
+        int img, vb;
+        long base, n;
+        vblock_at(bi, u, img, vb, base, n);
+        const long p0 = bi.pix_off[img], np = bi.pix_off[img + 1] - p0;
+        double v[1] = {0.0};
+        for (long i = (long)vb * blockDim.x + threadIdx.x; i < np; i += (long)kRedBlocks * blockDim.x) {
+            const float* g = grad + (p0 + i) * L;
+            float best = g[0];
+            int bk = 0;
+            for (int k = 1; k < L; k++)
+                if (g[k] < best) {
+                    best = g[k];
+                    bk = k;
+                }
+            for (int k = 0; k < L; k++) {
+                const long e = (p0 + i) * L + k;
+                const float s = fsub(k == bk ? 1.0f : 0.0f, Q[e]);
+                sx[e] = s;
+                v[0] += (double)U[e] * (double)s;
             }
-        for (int k = 0; k < L; k++) {
-            const long e = (p0 + i) * L + k;
-            const float s = fsub(k == bk ? 1.0f : 0.0f, Q[e]);
-            sx[e] = s;
-            v[0] += (double)U[e] * (double)s;
         }
+        vblock_store<1>(v, part + (long)img * kBPart, vb);
+        __syncthreads();
     }
-    vblock_store<1>(v, part + (long)img * kBPart, vb);
 }
 
-// qp_direction_tiled per image (L = 21): the image's row tiles of 32 pixels,
-// blocks numbered image after image (tile_off), one partial per block.
+// qp_direction_tiled per image (L = 21): the image's row tiles of 32 pixels
+// per warp, its blocks numbered image after image (the domain lt: tile_off
+// as the base), one partial per block; the kernel loops over the live
+// images' blocks.
 template <int LC>
 __global__ void __launch_bounds__(32 * kTileWarps)
-    bqp_direction_tiled(const int* __restrict__ tile_img, const int* __restrict__ tile_off, BImages bi,
-                        const float* __restrict__ grad, const float* __restrict__ Q, const float* __restrict__ U,
-                        float* __restrict__ sx, double* __restrict__ part) {
+    bqp_direction_tiled(Live lt, BImages bi, const float* __restrict__ grad, const float* __restrict__ Q,
+                        const float* __restrict__ U, float* __restrict__ sx, double* __restrict__ part) {
     __shared__ float sm[kTileWarps][3][32 * LC];
     __shared__ double s32[32];
-    const int img = tile_img[blockIdx.x];
-    if (bi.done[img]) return;  // block-uniform
-    const int lb = blockIdx.x - tile_off[img];
-    const long off = bi.pix_off[img], N = bi.pix_off[img + 1] - off;
-    const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long pix0 = ((long)lb * kTileWarps + wib) * 32;
-    double acc = 0.0;
-    if (pix0 < N) {
-        const int npix = (int)min(32L, N - pix0);
-        float *Gt = sm[wib][0], *Qt = sm[wib][1], *Ut = sm[wib][2];
-        tile_in<LC>(Gt, grad, off + pix0, npix, lane);
-        tile_in<LC>(Qt, Q, off + pix0, npix, lane);
-        tile_in<LC>(Ut, U, off + pix0, npix, lane);
-        __syncwarp();
-        const float* rg = Gt + lane * LC;
-        float* rq = Qt + lane * LC;
-        const float* ru = Ut + lane * LC;
-        float best = rg[0];
-        int bk = 0;
+    const long total = live_total(lt, 0);
+    for (long u = blockIdx.x; u < total; u += gridDim.x) {  // block-uniform
+        long lb;
+        const int img = live_locate(lt, u, lb);
+        const long off = bi.pix_off[img], N = bi.pix_off[img + 1] - off;
+        const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const long pix0 = (lb * kTileWarps + wib) * 32;
+        double acc = 0.0;
+        if (pix0 < N) {
+            const int npix = (int)min(32L, N - pix0);
+            float *Gt = sm[wib][0], *Qt = sm[wib][1], *Ut = sm[wib][2];
+            tile_in<LC>(Gt, grad, off + pix0, npix, lane);
+            tile_in<LC>(Qt, Q, off + pix0, npix, lane);
+            tile_in<LC>(Ut, U, off + pix0, npix, lane);
+            __syncwarp();
+            const float* rg = Gt + lane * LC;
+            float* rq = Qt + lane * LC;
+            const float* ru = Ut + lane * LC;
+            float best = rg[0];
+            int bk = 0;
 #pragma unroll
-        for (int k = 1; k < LC; k++)
-            if (rg[k] < best) {
-                best = rg[k];
-                bk = k;
+            for (int k = 1; k < LC; k++)
+                if (rg[k] < best) {
+                    best = rg[k];
+                    bk = k;
+                }
+            const bool act = lane < npix;
+#pragma unroll
+            for (int k = 0; k < LC; k++) {
+                const float s = fsub(k == bk ? 1.0f : 0.0f, rq[k]);
+                rq[k] = s;
+                if (act) acc += (double)ru[k] * (double)s;
             }
-        const bool act = lane < npix;
-#pragma unroll
-        for (int k = 0; k < LC; k++) {
-            const float s = fsub(k == bk ? 1.0f : 0.0f, rq[k]);
-            rq[k] = s;
-            if (act) acc += (double)ru[k] * (double)s;
+            __syncwarp();
+            tile_out<LC>(Qt, sx, off + pix0, npix, lane);
         }
-        __syncwarp();
-        tile_out<LC>(Qt, sx, off + pix0, npix, lane);
+        const double tot = block_sum_any(acc, s32);
+        if (threadIdx.x == 0) part[lt.base[img] + lb] = tot;
+        __syncthreads();  // the tiles and s32 are rewritten next
     }
-    const double tot = block_sum_any(acc, s32);
-    if (threadIdx.x == 0) part[tile_off[img] + lb] = tot;
 }
 
 // finalize_sums_kernel per image (one block per image, one warp per value).
@@ -390,6 +410,79 @@ __global__ void badd_scaled_kernel(long n, float* __restrict__ a, const float* _
     if (t < n) a[t] = fadd(a[t], fmul(coef, b[t]));
 }
 
+// The per-image work domains whose live prefixes an iteration needs.
+constexpr int kMaxLiveDoms = 64;
+struct LiveDoms {
+    const long* base[kMaxLiveDoms];  // B + 1 unit offsets per image
+    long* pre[kMaxLiveDoms];         // out: live prefix, live count + 1 entries
+    int n;
+};
+
+// Exclusive block-wide scan of one long per thread (blockDim.x a multiple of
+// 32, at most 1024); returns the thread's prefix, *total the block's sum.
+__device__ __forceinline__ long block_excl_scan(long x, long* s32, long& total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    long v = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const long y = __shfl_up_sync(kFullMask, v, o);
+        if (lane >= o) v += y;
+    }
+    if (lane == 31) s32[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        long t = lane < nw ? s32[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const long y = __shfl_up_sync(kFullMask, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < nw) s32[lane] = t;  // inclusive warp totals
+    }
+    __syncthreads();
+    total = s32[nw - 1];
+    const long r = v - x + (w > 0 ? s32[w - 1] : 0);
+    __syncthreads();  // s32 is reused by the next scan
+    return r;
+}
+
+// Start of a lockstep iteration, one block: the images still running, in
+// ascending order (live_img, *live_n), and each domain's live prefix.
+__global__ void live_build_kernel(int B, const int* __restrict__ done, int* __restrict__ live_n,
+                                  int* __restrict__ live_img, LiveDoms doms) {
+    __shared__ long s32[32];
+    long carry = 0;
+    for (int c0 = 0; c0 < B; c0 += blockDim.x) {
+        const int i = c0 + threadIdx.x;
+        const long f = (i < B && !done[i]) ? 1 : 0;
+        long tot;
+        const long pos = carry + block_excl_scan(f, s32, tot);
+        if (f) live_img[pos] = i;
+        carry += tot;
+    }
+    const int n = (int)carry;
+    if (threadIdx.x == 0) *live_n = n;
+    __syncthreads();  // live_img complete
+    for (int d = 0; d < doms.n; d++) {
+        const long* base = doms.base[d];
+        long* pre = doms.pre[d];
+        long acc = 0;
+        for (int r0 = 0; r0 < n; r0 += blockDim.x) {
+            const int r = r0 + threadIdx.x;
+            long cnt = 0;
+            if (r < n) {
+                const int img = live_img[r];
+                cnt = base[img + 1] - base[img];
+            }
+            long tot;
+            const long p = acc + block_excl_scan(cnt, s32, tot);
+            if (r < n) pre[r] = p;
+            acc += tot;
+        }
+        if (threadIdx.x == 0) pre[n] = acc;
+    }
+}
+
 }  // namespace
 
 Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_) {
@@ -415,7 +508,6 @@ Batch::Batch(int n, const int* widths, const int* heights, int L_) : B(n), L(L_)
 Batch::~Batch() {
     if (stream) cudaStreamSynchronize(stream);
     if (bqp_graph) cudaGraphExecDestroy(bqp_graph);
-    img.clear();
     terms.clear();
     if (stream) cudaStreamDestroy(stream);
 }
@@ -443,8 +535,6 @@ void Batch::ensure_lattices() {
 }
 
 void Batch::add_term(const float* d_features, int d, float w) {
-    img.clear();  // rebuilt with the new term at the next QP
-    qp_warm = false;
     weights_gen++;
     ensure_lattices();
     auto t = std::make_unique<Term>();
@@ -484,103 +574,6 @@ void Batch::unary_init(float* Q) {
     DCRF_LAUNCH_CHECK();
 }
 
-// One Frank-Wolfe iteration for every image that has not stopped, then the
-// count of images still running, copied to pinned host memory.
-// Batch QP: every image's own single-image solve (Model::qp, whose
-// Frank-Wolfe loop is a device-side graph loop), from up to kQpThreads host
-// threads so that the images' solves overlap on their own streams; a solve
-// of one image alone leaves SMs idle (one-block reductions and step kernels,
-// the longest splat lists' chains), which the other images' kernels fill.
-// Each image's output, step count and energy are those of its single-image
-// solve, bit for bit.  The per-image models are built at the first solve
-// from the features each term was added with, and kept.
-void Batch::ensure_image_models() {
-    if ((int)img.size() == B) return;
-    img.clear();
-    DCRF_CUDA(cudaStreamSynchronize(stream));  // the terms' features were copied on this stream
-    for (int i = 0; i < B; i++) {
-        auto m = std::make_unique<Model>(W[i], H[i], L);
-        for (const auto& t : terms) {
-            m->add_term(t->feat.get() + pix_off[i] * t->d, t->d, t->w);
-            m->sync();
-        }
-        img.push_back(std::move(m));
-    }
-    img_unary_gen = ~0ull;
-}
-
-int Batch::qp_threaded(const float* init, float* out, int max_iter, int* steps, double* energies) {
-    require(has_unary, DCRF_E_STATE, "qp: no unary energy set");
-    ensure_image_models();
-    if (img_unary_gen != unary_gen) {  // each image's slice of the unaries
-        for (int i = 0; i < B; i++) {
-            Model& m = *img[i];
-            const size_t n = (size_t)(pix_off[i + 1] - pix_off[i]) * L;
-            DCRF_CUDA(cudaMemcpyAsync(m.unary.ensure(n), unary.get() + pix_off[i] * L, sizeof(float) * n,
-                                      cudaMemcpyDeviceToDevice, stream));
-            m.has_unary = true;
-            m.logit_F = 0;
-            m.gen++;
-        }
-        img_unary_gen = unary_gen;
-        qp_warm = false;  // the models changed: their graphs are captured again
-    }
-    // the images' streams start after the batch stream's work (the unaries, init)
-    DCRF_CUDA(cudaStreamSynchronize(stream));
-    std::vector<int> st(B, 0);
-    std::vector<double> en(B, 0.0);
-    // A solve that sizes buffers or captures its graph (the first one for an
-    // output buffer, max_iter and model state) runs on this thread, image
-    // after image: allocation and capture stay out of the concurrent phase.
-    if (!(qp_warm && out == warm_out && max_iter == warm_max_iter)) {
-        for (int i = 0; i < B; i++)
-            st[i] = img[i]->qp(init + pix_off[i] * L, out + pix_off[i] * L, max_iter, &en[i]);
-        qp_warm = true;
-        warm_out = out;
-        warm_max_iter = max_iter;
-        int most = 0;
-        for (int i = 0; i < B; i++) {
-            if (steps) steps[i] = st[i];
-            if (energies) energies[i] = en[i];
-            most = std::max(most, st[i]);
-        }
-        return most;
-    }
-    std::atomic<int> next{0};
-    std::exception_ptr err = nullptr;
-    std::mutex emu;
-    auto worker = [&]() {
-        cudaSetDevice(device);
-        for (;;) {
-            const int i = next.fetch_add(1);
-            if (i >= B) break;
-            try {
-                st[i] = img[i]->qp(init + pix_off[i] * L, out + pix_off[i] * L, max_iter, &en[i]);
-            } catch (...) {
-                std::lock_guard<std::mutex> lk(emu);
-                if (!err) err = std::current_exception();
-                next.store(B);
-            }
-        }
-    };
-    const int nth = std::min(B, kQpThreads);
-    std::vector<std::thread> pool;
-    try {
-        for (int t = 1; t < nth; t++) pool.emplace_back(worker);
-    } catch (...) {  // fewer threads than asked for: the ones running finish the images
-    }
-    worker();
-    for (auto& th : pool) th.join();
-    if (err) std::rethrow_exception(err);
-    int most = 0;
-    for (int i = 0; i < B; i++) {
-        if (steps) steps[i] = st[i];
-        if (energies) energies[i] = en[i];
-        most = std::max(most, st[i]);
-    }
-    return most;
-}
-
 // Batched QP in lockstep: every Frank-Wolfe iteration of every image that
 // is still running, one launch per step over all images -- the filters over
 // the terms' concatenated lattices, the per-pixel and per-image scalar steps
@@ -605,22 +598,50 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
     double* part = bpart.ensure((size_t)B * kBPart);
     const bool tiled = L == 21;
     if (tiled && btiles == 0) {  // row-tile blocks of the direction kernel, image after image
-        std::vector<int> toff(B + 1, 0), timg;
+        std::vector<int> toff(B + 1, 0);
+        std::vector<long> tbase(B + 1, 0);
         for (int i = 0; i < B; i++) {
             const int tg = ceil_div(ceil_div((int)(pix_off[i + 1] - pix_off[i]), 32), kTileWarps);
             toff[i + 1] = toff[i] + tg;
-            timg.insert(timg.end(), tg, i);
+            tbase[i + 1] = toff[i + 1];
         }
         btiles = toff[B];
         DCRF_CUDA(cudaMemcpyAsync(btile_off.ensure(B + 1), toff.data(), sizeof(int) * (B + 1), cudaMemcpyHostToDevice,
                                   stream));
-        DCRF_CUDA(cudaMemcpyAsync(btile_img.ensure(btiles), timg.data(), sizeof(int) * btiles, cudaMemcpyHostToDevice,
-                                  stream));
+        DCRF_CUDA(cudaMemcpyAsync(btile_base.ensure(B + 1), tbase.data(), sizeof(long) * (B + 1),
+                                  cudaMemcpyHostToDevice, stream));
         DCRF_CUDA(cudaStreamSynchronize(stream));  // the host vectors are the copies' sources
     }
     double* part_dir = tiled ? bpart_dir.ensure(btiles) : nullptr;
-    const BImages all{d_pix_off.get(), nullptr, L};
-    const BImages live{d_pix_off.get(), done, L};
+    // The live images and each domain's live prefix, rebuilt at the start of
+    // every iteration: kDomains domains per term (its lattice's lists,
+    // vertices, slice tiles and pixels), then the direction kernel's tiles.
+    const int nt_l = (int)terms.size();
+    require(nt_l * Lattice::kDomains + 1 <= kMaxLiveDoms, DCRF_E_ARG, "batch qp: too many pairwise terms");
+    int* live_buf = blive.ensure(B + 1);
+    const int* live_n = live_buf;
+    const int* live_img = live_buf + 1;
+    long* lpre = blive_pre.ensure((size_t)(nt_l * Lattice::kDomains + 1) * (B + 1));
+    LiveDoms doms{};
+    for (int k = 0; k < nt_l; k++) {
+        Lattice& lat = *terms[k]->lat;
+        lat.prepare_live(L);
+        for (int dm = 0; dm < Lattice::kDomains; dm++) {
+            doms.base[doms.n] = lat.dom_base.get() + (long)dm * (B + 1);
+            doms.pre[doms.n++] = lpre + (long)(k * Lattice::kDomains + dm) * (B + 1);
+        }
+    }
+    long* tile_pre = lpre + (long)nt_l * Lattice::kDomains * (B + 1);
+    if (tiled) {
+        doms.base[doms.n] = btile_base.get();
+        doms.pre[doms.n++] = tile_pre;
+    }
+    const BImages all{d_pix_off.get(), nullptr, nullptr, B, L};
+    const BImages live{d_pix_off.get(), live_n, live_img, B, L};
+    const Live ltiles{live_n, live_img, tiled ? btile_base.get() : nullptr, tile_pre};
+    // Grids of the live loops: a few waves of the device, not the batch.
+    const int vgrid = std::min(B, 16) * kRedBlocks;
+    const int tgrid = std::max(1, std::min(btiles, sm_count() * 2 * (2048 / (32 * kTileWarps))));
     const int sb = ceil_div(B, 128);
 
     if (Q != init) DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
@@ -639,7 +660,7 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
     launch(bqp_init_energy_kernel, sb, 128, 0, stream, B, sc, nt, max_iter);
     // a NaN or infinity in Q or the unaries
     DCRF_CUDA(cudaMemsetAsync(&sc[0].numeric, 0, sizeof(int), stream));
-    launch(nonfinite_kernel, kRedBlocks, kRedThreads, 0, stream, NL, (const float*)Q, (const float*)unary.get(), sc);
+    launch(nonfinite_kernel, nonfinite_grid(NL), 256, 0, stream, NL, (const float*)Q, (const float*)unary.get(), sc);
     launch(bqp_cond_kernel, 1, 256, 0, stream, B, (const SolverScalars*)sc, done, flags, 1 << 30, flags + 1,
            cudaGraphConditionalHandle{}, 0);
     DCRF_LAUNCH_CHECK();
@@ -652,26 +673,31 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
 
     // One Frank-Wolfe iteration of every running image (src/densecrf.cpp:389-436)
     // and the loop test.
-    for (auto& t : terms) t->lat->skip_done = done;  // finished images: no filter work
+    for (auto& t : terms) {  // finished images: no filter work
+        Lattice& lat = *t->lat;
+        lat.live_n = live_n;
+        lat.live_img = live_img;
+    }
+    for (int k = 0; k < nt_l; k++) terms[k]->lat->live_pre = lpre + (long)k * Lattice::kDomains * (B + 1);
     auto iteration = [&](bool graph, cudaGraphConditionalHandle h) {
+        launch(live_build_kernel, 1, 256, 0, stream, B, (const int*)done, live_buf, live_buf + 1, doms);
         if (tiled) {
-            launch(bqp_direction_tiled<21>, btiles, 32 * kTileWarps, 0, stream, (const int*)btile_img.get(),
-                   (const int*)btile_off.get(), live, (const float*)grad, (const float*)Q,
-                   (const float*)unary.get(), sx, part_dir);
+            launch(bqp_direction_tiled<21>, tgrid, 32 * kTileWarps, 0, stream, ltiles, live, (const float*)grad,
+                   (const float*)Q, (const float*)unary.get(), sx, part_dir);
             launch(bfinalize_large_kernel, B, 1024, 0, stream, (const double*)part_dir, (const int*)btile_off.get(), 0,
                    (const int*)done, sc);
         } else {
-            launch(bqp_direction_kernel, B * kRedBlocks, kRedThreads, 0, stream, live, (const float*)grad,
+            launch(bqp_direction_kernel, vgrid, kRedThreads, 0, stream, live, (const float*)grad,
                    (const float*)Q, (const float*)unary.get(), sx, part);
             launch(bfinalize_sums_kernel, B, 32, 0, stream, (const double*)part, 1, 0, (const int*)done, sc);
         }
         for (int k = 0; k < nt; k++) apply(k, psi, sx, k == 0 ? nullptr : psi, 1.0f, k == 0);
         if (nt == 0) DCRF_CUDA(cudaMemsetAsync(psi, 0, sizeof(float) * NL, stream));
-        launch(bdots2_kernel, B * kRedBlocks, kRedThreads, 0, stream, live, (const float*)Q, (const float*)sx,
+        launch(bdots2_kernel, vgrid, kRedThreads, 0, stream, live, (const float*)Q, (const float*)sx,
                (const float*)psi, part);
         launch(bfinalize_sums_kernel, B, 64, 0, stream, (const double*)part, 2, 1, (const int*)done, sc);
         launch(bqp_step_kernel, sb, 128, 0, stream, B, (const int*)done, sc);
-        launch(bqp_update_kernel, B * kRedBlocks, kRedThreads, 0, stream, live, (const float*)sx, (const float*)psi,
+        launch(bqp_update_kernel, vgrid, kRedThreads, 0, stream, live, (const float*)sx, (const float*)psi,
                (const float*)unary.get(), Q, grad, (const SolverScalars*)sc, part);
         launch(bfinalize_sums_kernel, B, 32, 0, stream, (const double*)part, 1, 7, (const int*)done, sc);
         launch(bqp_energy_kernel, sb, 128, 0, stream, B, (const int*)done, sc, max_iter);
@@ -680,11 +706,21 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
     };
     std::vector<const void*> key = {Q, grad, sx, psi, unary.get(), sc, done, part, part_dir,
                                     (const void*)(uintptr_t)max_iter, (const void*)(uintptr_t)weights_gen};
+    key.push_back(live_buf);
+    key.push_back(lpre);
     for (auto& t : terms) {
         key.push_back(t->lat->va.get());
         key.push_back(t->lat->vb.get());
         key.push_back(t->lat.get());
+        key.push_back((const void*)(uintptr_t)t->lat->dom_tile);
     }
+    auto detach = [&] {
+        for (auto& t : terms) {
+            t->lat->live_n = nullptr;
+            t->lat->live_img = nullptr;
+            t->lat->live_pre = nullptr;
+        }
+    };
     int guard = 0;
     try {
         while (hf[1]) {
@@ -710,10 +746,10 @@ int Batch::qp(const float* init, float* out, int max_iter, int* steps, double* e
             }
         }
     } catch (...) {
-        for (auto& t : terms) t->lat->skip_done = nullptr;
+        detach();
         throw;
     }
-    for (auto& t : terms) t->lat->skip_done = nullptr;
+    detach();
     std::vector<SolverScalars> hs(B);
     DCRF_CUDA(cudaMemcpyAsync(hs.data(), sc, sizeof(SolverScalars) * B, cudaMemcpyDeviceToHost, stream));
     DCRF_CUDA(cudaStreamSynchronize(stream));
@@ -776,8 +812,6 @@ void Batch::set_weight(int k, float w) {
     require(k >= 0 && k < (int)terms.size(), DCRF_E_ARG, "pairwise term index out of range");
     terms[k]->w = w;
     weights_gen++;
-    for (auto& m : img) m->set_compat(k, kPotts, &w);  // the per-image models' QP graphs are rebuilt
-    qp_warm = false;
 }
 
 // out = base + scale * n o K(n o in), K transposed (blur axes reversed) when

@@ -1,10 +1,10 @@
 // Many images of different sizes behind one handle: their pixels are
-// concatenated ([sum N_i][L]).  The mean-field iterations and their adjoint
-// run over all images at once on each Potts term's concatenated lattice
-// (Lattice::concat).  The Frank-Wolfe QP runs every image's own model
-// (Model::qp, its loop a device-side graph loop) from several host threads,
-// so the images' solves overlap; each image's result is that of its own
-// single-image solve, bit for bit.
+// concatenated ([sum N_i][L]) and each Potts term's lattices are
+// concatenated too (Lattice::concat).  The mean-field iterations and their
+// adjoint, and the Frank-Wolfe QP, run over all images at once: the QP in
+// lockstep, one launch per step for every image still running (its loop a
+// device-side graph loop), each image's result that of its own single-image
+// solve, bit for bit.
 #pragma once
 #include <memory>
 #include <vector>
@@ -28,16 +28,6 @@ struct Batch {
     DevBuf<double> partials;
     unsigned long long unary_gen = 0;  // bumped by every unary change
 
-    // The QP runs each image's own model (built at the first solve from the
-    // terms' features, kept until a term is added).
-    std::vector<std::unique_ptr<Model>> img;
-    unsigned long long img_unary_gen = ~0ull;
-    // The last QP ran (or captured) every image's graph for this output
-    // buffer and max_iter: the next such QP may run the images concurrently.
-    bool qp_warm = false;
-    const float* warm_out = nullptr;
-    int warm_max_iter = -1;
-
     // mean-field checkpoints: Q_t for t % ck_every == 0 and Q_T, [slots][Ntot][L];
     // the other iterates are recomputed segment by segment in the backward
     // pass into mf_seg ([ck_every - 1][Ntot][L]).
@@ -60,14 +50,14 @@ struct Batch {
     // Returns the largest per-image step count; per-image counts / energies
     // go to steps / energies when given (host arrays of B).
     int qp(const float* init, float* out, int max_iter, int* steps, double* energies);
-    // The same solves from up to kQpThreads host threads, each image's own
-    // single-image solve (the earlier form, kept for comparison).
-    int qp_threaded(const float* init, float* out, int max_iter, int* steps, double* energies);
 
     // Lockstep QP state: per-image scalars and loop flags, per-image partial
     // sums, the row-tile table of the direction kernel, the loop as a graph.
     DevBuf<SolverScalars> bsc;
-    DevBuf<int> bdone, bflags, btile_img, btile_off;
+    DevBuf<int> bdone, bflags, btile_off;
+    DevBuf<long> btile_base;  // btile_off as the direction kernel's domain
+    DevBuf<int> blive;        // [0] live image count, [1 .. B] their ids
+    DevBuf<long> blive_pre;   // live prefixes: kDomains per term, then the direction tiles
     DevBuf<double> bpart, bpart_dir;
     int btiles = 0;
     cudaGraphExec_t bqp_graph = nullptr;
@@ -95,13 +85,11 @@ struct Batch {
   private:
     template <typename F>
     void build_bqp_graph(F&& iteration, int* flags);
-    void ensure_image_models();
     void build_lattice(Term& t);
     int ck_slot(int t) const { return t == mf_T && t % ck_every ? mf_T / ck_every + 1 : t / ck_every; }
     bool ck_stored(int t) const { return t % ck_every == 0 || t == mf_T; }
     void mf_iteration(const float* q, float* qn, const float* negU, float* logits);
 };
 
-constexpr int kQpThreads = 8;  // host threads of a batch QP
 
 }  // namespace dcrf

@@ -323,10 +323,10 @@ __global__ void seg_fill_kernel(int E, int d1, const int* __restrict__ sorted_en
 // and normalisation factors) are in flight, so a single long list is not
 // serialised on L2 latency.  Vertices are visited longest list first
 // (`order`) so the few very long lists of a coarse lattice start early.
-// Images whose work a batched solve no longer needs: the filters skip the
-// vertices (and pixels, by their first vertex) of image vimg[v] when
-// done[vimg[v]] is set.  done == nullptr (single images) skips nothing.
-__device__ __forceinline__ bool skipped(const Skip& sk, int v) { return sk.done && sk.done[sk.vimg[v]]; }
+// The filter kernels loop over their units (list positions, vertices,
+// pixels or tiles) with a grid-stride loop: one pass with a full grid, or,
+// in a batched solve, the units of the images still running (Live) with a
+// grid sized for the device.
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -395,33 +395,34 @@ template <bool PRE_NORM, int LC = 0>
 __global__ void __launch_bounds__(32 * kStageWarps)
     splat_kernel(int M, int Lrt, const int* __restrict__ order, const int* __restrict__ seg_start,
                  const int* __restrict__ seg_pix, const float* __restrict__ seg_w, const float* __restrict__ in,
-                 const float* __restrict__ norm, float* __restrict__ vals, Skip sk, int Lrow) {
+                 const float* __restrict__ norm, float* __restrict__ vals, Live lv, int Lrow) {
     const int L = LC ? LC : Lrt;
     __shared__ float ring[kStageWarps][kStages][kChunk][32];
     __shared__ float mw[kStageWarps][kStages][kChunk];
     __shared__ float mn[kStageWarps][kStages][kChunk];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int unit = blockIdx.x * kStageWarps + wib;
-    if (unit >= M) return;  // warp-uniform; the kernel has no block-wide barrier
-    const int v = order[unit];
-    if (skipped(sk, v)) return;
-    const int s0 = seg_start[v], s1 = seg_start[v + 1];
-    for (int kb = 0; kb < L; kb += 32) {
-        const int k = kb + lane;
-        const bool act = k < L;
-        float acc = 0.0f;
-        stream_list<float, PRE_NORM>(s0, s1, L, k, act, lane, seg_pix, seg_w, in, norm, ring[wib], mw[wib],
-                                     mn[wib], [&](int slot, int n) {
+    const long total = live_total(lv, M);
+    // warp-uniform loop; the kernel has no block-wide barrier
+    for (long unit = (long)blockIdx.x * kStageWarps + wib; unit < total; unit += (long)gridDim.x * kStageWarps) {
+        const int v = order[live_unit(lv, unit)];
+        const int s0 = seg_start[v], s1 = seg_start[v + 1];
+        for (int kb = 0; kb < L; kb += 32) {
+            const int k = kb + lane;
+            const bool act = k < L;
+            float acc = 0.0f;
+            stream_list<float, PRE_NORM>(s0, s1, L, k, act, lane, seg_pix, seg_w, in, norm, ring[wib], mw[wib],
+                                         mn[wib], [&](int slot, int n) {
 #pragma unroll 4
-                                         for (int e = 0; e < n; e++) {
-                                             float x = ring[wib][slot][e][lane];
-                                             if (PRE_NORM) x = fmul(x, mn[wib][slot][e]);
-                                             acc = fadd(acc, fmul(mw[wib][slot][e], x));
-                                         }
-                                     });
-        if (act) vals[(long)(v + 1) * Lrow + k] = acc;
+                                             for (int e = 0; e < n; e++) {
+                                                 float x = ring[wib][slot][e][lane];
+                                                 if (PRE_NORM) x = fmul(x, mn[wib][slot][e]);
+                                                 acc = fadd(acc, fmul(mw[wib][slot][e], x));
+                                             }
+                                         });
+            if (act) vals[(long)(v + 1) * Lrow + k] = acc;
+        }
+        for (int k = L + lane; k < Lrow; k += 32) vals[(long)(v + 1) * Lrow + k] = 0.0f;  // row padding
     }
-    for (int k = L + lane; k < Lrow; k += 32) vals[(long)(v + 1) * Lrow + k] = 0.0f;  // row padding
 }
 
 // The longest lists with L = 21: the cp.async ring of splat_kernel, kStages chunks
@@ -435,81 +436,82 @@ __global__ void __launch_bounds__(32 * kStageWarps)
     splat_ring21_kernel(int M, const int* __restrict__ order, const int* __restrict__ seg_start,
                         const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
                         const float* __restrict__ in, const float* __restrict__ norm, float* __restrict__ vals,
-                        Skip sk, int Lrow) {
+                        Live lv, int Lrow) {
     constexpr int L = 21;
     __shared__ __align__(16) float X[kStageWarps][kStages][L][kRS];
     __shared__ __align__(16) float Wr[kStageWarps][kStages][kChunk];
     __shared__ __align__(16) float Nr[kStageWarps][kStages][kChunk];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int unit = blockIdx.x * kStageWarps + wib;
-    if (unit >= M) return;  // warp-uniform; the kernel has no block-wide barrier
-    const int v = order[unit];
-    if (skipped(sk, v)) return;
-    const int s0 = seg_start[v], s1 = seg_start[v + 1];
-    const int nch = (s1 - s0 + kChunk - 1) / kChunk;
-    auto pix_of = [&](int c) {
-        const int e = s0 + c * kChunk + lane;
-        return (c < nch && e < s1) ? seg_pix[e] : -1;
-    };
-    auto issue = [&](int c, int p) {
-        if (p < 0) return;  // past the end of the list: never summed
-        const int slot = c % kStages, e = s0 + c * kChunk + lane;
-        const float* row = in + (long)p * L;
+    const long total = live_total(lv, M);
+    // warp-uniform loop; no block-wide barrier inside
+    for (long unit = (long)blockIdx.x * kStageWarps + wib; unit < total; unit += (long)gridDim.x * kStageWarps) {
+        const int v = order[live_unit(lv, unit)];
+        const int s0 = seg_start[v], s1 = seg_start[v + 1];
+        const int nch = (s1 - s0 + kChunk - 1) / kChunk;
+        auto pix_of = [&](int c) {
+            const int e = s0 + c * kChunk + lane;
+            return (c < nch && e < s1) ? seg_pix[e] : -1;
+        };
+        auto issue = [&](int c, int p) {
+            if (p < 0) return;  // past the end of the list: never summed
+            const int slot = c % kStages, e = s0 + c * kChunk + lane;
+            const float* row = in + (long)p * L;
 #pragma unroll
-        for (int k = 0; k < L; k++) cp_async4(&X[wib][slot][k][lane], row + k);
-        cp_async4(&Wr[wib][slot][lane], seg_w + e);
-        if (PRE_NORM) cp_async4(&Nr[wib][slot][lane], norm + p);
-    };
-    float acc = 0.0f;
-    int pcur = pix_of(0);
+            for (int k = 0; k < L; k++) cp_async4(&X[wib][slot][k][lane], row + k);
+            cp_async4(&Wr[wib][slot][lane], seg_w + e);
+            if (PRE_NORM) cp_async4(&Nr[wib][slot][lane], norm + p);
+        };
+        float acc = 0.0f;
+        int pcur = pix_of(0);
 #pragma unroll
-    for (int c = 0; c < kStages - 1; c++) {
-        const int pn = pix_of(c + 1);
-        issue(c, pcur);
-        cp_async_commit();
-        pcur = pn;
-    }
-    for (int c = 0; c < nch; c++) {
-        const int ci = c + kStages - 1;
-        const int pn = pix_of(ci + 1);
-        issue(ci, pcur);
-        cp_async_commit();
-        pcur = pn;
-        cp_async_wait<kStages - 1>();  // chunk c has landed (this lane's copies)
-        __syncwarp();                  // ... and every other lane's
-        const int slot = c % kStages, n = min(kChunk, s1 - (s0 + c * kChunk));
-        if (lane < L) {
-            const float4* xs = reinterpret_cast<const float4*>(&X[wib][slot][lane][0]);
-            const float4* ws = reinterpret_cast<const float4*>(&Wr[wib][slot][0]);
-            const float4* ns = reinterpret_cast<const float4*>(&Nr[wib][slot][0]);
-            const int n4 = n >> 2;
-            for (int q = 0; q < n4; q++) {
-                float4 x = xs[q];
-                const float4 w = ws[q];
-                if (PRE_NORM) {
-                    const float4 nv = ns[q];
-                    x.x = fmul(x.x, nv.x);
-                    x.y = fmul(x.y, nv.y);
-                    x.z = fmul(x.z, nv.z);
-                    x.w = fmul(x.w, nv.w);
-                }
-                acc = fadd(acc, fmul(w.x, x.x));
-                acc = fadd(acc, fmul(w.y, x.y));
-                acc = fadd(acc, fmul(w.z, x.z));
-                acc = fadd(acc, fmul(w.w, x.w));
-            }
-            for (int e = n4 << 2; e < n; e++) {
-                float x = X[wib][slot][lane][e];
-                if (PRE_NORM) x = fmul(x, Nr[wib][slot][e]);
-                acc = fadd(acc, fmul(Wr[wib][slot][e], x));
-            }
+        for (int c = 0; c < kStages - 1; c++) {
+            const int pn = pix_of(c + 1);
+            issue(c, pcur);
+            cp_async_commit();
+            pcur = pn;
         }
-        __syncwarp();  // the slot is refilled kStages-1 chunks later
+        for (int c = 0; c < nch; c++) {
+            const int ci = c + kStages - 1;
+            const int pn = pix_of(ci + 1);
+            issue(ci, pcur);
+            cp_async_commit();
+            pcur = pn;
+            cp_async_wait<kStages - 1>();  // chunk c has landed (this lane's copies)
+            __syncwarp();                  // ... and every other lane's
+            const int slot = c % kStages, n = min(kChunk, s1 - (s0 + c * kChunk));
+            if (lane < L) {
+                const float4* xs = reinterpret_cast<const float4*>(&X[wib][slot][lane][0]);
+                const float4* ws = reinterpret_cast<const float4*>(&Wr[wib][slot][0]);
+                const float4* ns = reinterpret_cast<const float4*>(&Nr[wib][slot][0]);
+                const int n4 = n >> 2;
+                for (int q = 0; q < n4; q++) {
+                    float4 x = xs[q];
+                    const float4 w = ws[q];
+                    if (PRE_NORM) {
+                        const float4 nv = ns[q];
+                        x.x = fmul(x.x, nv.x);
+                        x.y = fmul(x.y, nv.y);
+                        x.z = fmul(x.z, nv.z);
+                        x.w = fmul(x.w, nv.w);
+                    }
+                    acc = fadd(acc, fmul(w.x, x.x));
+                    acc = fadd(acc, fmul(w.y, x.y));
+                    acc = fadd(acc, fmul(w.z, x.z));
+                    acc = fadd(acc, fmul(w.w, x.w));
+                }
+                for (int e = n4 << 2; e < n; e++) {
+                    float x = X[wib][slot][lane][e];
+                    if (PRE_NORM) x = fmul(x, Nr[wib][slot][e]);
+                    acc = fadd(acc, fmul(Wr[wib][slot][e], x));
+                }
+            }
+            __syncwarp();  // the slot is refilled kStages-1 chunks later
+        }
+        cp_async_wait<0>();
+        __syncwarp();
+        if (lane < L) vals[(long)(v + 1) * Lrow + lane] = acc;
+        else if (lane < Lrow) vals[(long)(v + 1) * Lrow + lane] = 0.0f;  // row padding
     }
-    cp_async_wait<0>();
-    __syncwarp();
-    if (lane < L) vals[(long)(v + 1) * Lrow + lane] = acc;
-    else if (lane < Lrow) vals[(long)(v + 1) * Lrow + lane] = 0.0f;  // row padding
 }
 
 // Lists of at most kHugeList entries: one warp per vertex, lane = label (in
@@ -524,50 +526,51 @@ __global__ void __launch_bounds__(32 * WARPS)
     splat_warp_kernel(int n, int Lrt, const int* __restrict__ order, const int* __restrict__ seg_start,
                       const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
                       const float* __restrict__ in, const float* __restrict__ norm, float* __restrict__ vals,
-                      Skip sk, int Lrow) {
+                      Live lv, int Lrow) {
     const int L = LC ? LC : Lrt;
     __shared__ float4 rec[WARPS][32];
     const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int unit = blockIdx.x * WARPS + wib;
-    if (unit >= n) return;  // warp-uniform; no block-wide barrier below
-    const int v = order[unit];
-    if (skipped(sk, v)) return;
-    const int s0 = seg_start[v], s1 = seg_start[v + 1];
-    float4* r = rec[wib];
-    for (int kb = 0; kb < L; kb += 32) {
-        const int k = kb + lane;
-        const bool act = k < L;
-        float acc = 0.0f;
-        int p = 0;
-        float w = 0.0f, nn = 1.0f;
-        auto fetch = [&](int base) {
-            const int e = base + lane;
-            if (e < s1) {
-                p = seg_pix[e];
-                w = seg_w[e];
-                if (PRE_NORM) nn = norm[p];
-            }
-        };
-        fetch(s0);
-        for (int c0 = s0; c0 < s1; c0 += 32) {
-            r[lane] = make_float4(__int_as_float(p), w, nn, 0.0f);
-            fetch(c0 + 32);  // in flight while this chunk is summed
-            __syncwarp();
-            const int cnt = min(32, s1 - c0);
-            if (act) {
-#pragma unroll 8
-                for (int e = 0; e < cnt; e++) {
-                    const float4 q = r[e];
-                    float x = in[(long)__float_as_int(q.x) * L + k];
-                    if (PRE_NORM) x = fmul(x, q.z);
-                    acc = fadd(acc, fmul(q.y, x));
+    const long total = live_total(lv, n);
+    // warp-uniform loop; no block-wide barrier inside
+    for (long unit = (long)blockIdx.x * WARPS + wib; unit < total; unit += (long)gridDim.x * WARPS) {
+        const int v = order[live_unit(lv, unit)];
+        const int s0 = seg_start[v], s1 = seg_start[v + 1];
+        float4* r = rec[wib];
+        for (int kb = 0; kb < L; kb += 32) {
+            const int k = kb + lane;
+            const bool act = k < L;
+            float acc = 0.0f;
+            int p = 0;
+            float w = 0.0f, nn = 1.0f;
+            auto fetch = [&](int base) {
+                const int e = base + lane;
+                if (e < s1) {
+                    p = seg_pix[e];
+                    w = seg_w[e];
+                    if (PRE_NORM) nn = norm[p];
                 }
+            };
+            fetch(s0);
+            for (int c0 = s0; c0 < s1; c0 += 32) {
+                r[lane] = make_float4(__int_as_float(p), w, nn, 0.0f);
+                fetch(c0 + 32);  // in flight while this chunk is summed
+                __syncwarp();
+                const int cnt = min(32, s1 - c0);
+                if (act) {
+#pragma unroll 8
+                    for (int e = 0; e < cnt; e++) {
+                        const float4 q = r[e];
+                        float x = in[(long)__float_as_int(q.x) * L + k];
+                        if (PRE_NORM) x = fmul(x, q.z);
+                        acc = fadd(acc, fmul(q.y, x));
+                    }
+                }
+                __syncwarp();  // the records are rewritten next chunk
             }
-            __syncwarp();  // the records are rewritten next chunk
+            if (act) vals[(long)(v + 1) * Lrow + k] = acc;
         }
-        if (act) vals[(long)(v + 1) * Lrow + k] = acc;
+        for (int k = L + lane; k < Lrow; k += 32) vals[(long)(v + 1) * Lrow + k] = 0.0f;  // row padding
     }
-    for (int k = L + lane; k < Lrow; k += 32) vals[(long)(v + 1) * Lrow + k] = 0.0f;  // row padding
 }
 
 // Short lists (at most kLongList entries; the tail of `order`): one thread
@@ -576,27 +579,28 @@ template <bool PRE_NORM, int LC = 0>
 __global__ void splat_short_kernel(int n_short, int Lrt, const int* __restrict__ order,
                                    const int* __restrict__ seg_start, const int* __restrict__ seg_pix,
                                    const float* __restrict__ seg_w, const float* __restrict__ in,
-                                   const float* __restrict__ norm, float* __restrict__ vals, Skip sk, int Lrow) {
+                                   const float* __restrict__ norm, float* __restrict__ vals, Live lv, int Lrow) {
     const int L = LC ? LC : Lrt;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)n_short * Lrow) return;
-    const int u = (int)(t / Lrow), k = (int)(t - (long)u * Lrow);
-    const int v = order[u];
-    if (skipped(sk, v)) return;
-    if (k >= L) {  // row padding
-        vals[(long)(v + 1) * Lrow + k] = 0.0f;
-        return;
-    }
-    const int s0 = seg_start[v], s1 = seg_start[v + 1];
-    float acc = 0.0f;
+    const long total = live_total(lv, n_short) * Lrow;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const long u = t / Lrow;
+        const int k = (int)(t - u * Lrow);
+        const int v = order[live_unit(lv, u)];
+        if (k >= L) {  // row padding
+            vals[(long)(v + 1) * Lrow + k] = 0.0f;
+            continue;
+        }
+        const int s0 = seg_start[v], s1 = seg_start[v + 1];
+        float acc = 0.0f;
 #pragma unroll 4
-    for (int s = s0; s < s1; s++) {
-        const int p = seg_pix[s];
-        float x = in[(long)p * L + k];
-        if (PRE_NORM) x = fmul(x, norm[p]);
-        acc = fadd(acc, fmul(seg_w[s], x));
+        for (int s = s0; s < s1; s++) {
+            const int p = seg_pix[s];
+            float x = in[(long)p * L + k];
+            if (PRE_NORM) x = fmul(x, norm[p]);
+            acc = fadd(acc, fmul(seg_w[s], x));
+        }
+        vals[(long)(v + 1) * Lrow + k] = acc;
     }
-    vals[(long)(v + 1) * Lrow + k] = acc;
 }
 
 __global__ void count_long_kernel(int M, const int* __restrict__ counts, int threshold, int* __restrict__ n) {
@@ -604,6 +608,24 @@ __global__ void count_long_kernel(int M, const int* __restrict__ counts, int thr
     const bool is_long = v < M && counts[v] > threshold;
     const unsigned b = __ballot_sync(0xffffffffu, is_long);
     if ((threadIdx.x & 31) == 0 && b) atomicAdd(n, __popc(b));
+}
+
+// Class of a splat list by its length: 0 huge, 1 long, 2 short.
+__device__ __forceinline__ int list_class(int c) { return c > kHugeList ? 0 : c > kLongList ? 1 : 2; }
+
+// Concatenated lattices: the key (class, image) of each position of the
+// length-sorted visiting order, for a second stable sort that groups each
+// class's lists by image (longest first within an image), and the number of
+// lists per (class, image).
+__global__ void class_image_key_kernel(int M, const int* __restrict__ order, const int* __restrict__ counts,
+                                       const int* __restrict__ vimg, int images, int* __restrict__ keys,
+                                       int* __restrict__ per_class_image) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const int v = order[p];
+    const int key = list_class(counts[v]) * images + vimg[v];
+    keys[p] = key;
+    atomicAdd(&per_class_image[key], 1);
 }
 
 // Sort key of the splat visiting order (stable radix sort ascending): the
@@ -626,19 +648,21 @@ __global__ void order_key_kernel(int M, const int* __restrict__ counts, int* __r
 // evaluates it in double (0.5 is a double literal there, :518).
 template <bool SEQ, int LC = 0>
 __global__ void blur_kernel(int M, int Lrt, const int2* __restrict__ nbr,
-                            const float* __restrict__ src, float* __restrict__ dst, Skip sk) {
+                            const float* __restrict__ src, float* __restrict__ dst, Live lv) {
     const int L = LC ? LC : Lrt;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)M * L) return;
-    const int v = (int)(t / L), k = (int)(t - (long)v * L);
-    if (skipped(sk, v)) return;
-    const int2 nb = nbr[v];
-    const float a = src[(long)(v + 1) * L + k];
-    const float s = fadd(src[(long)nb.x * L + k], src[(long)nb.y * L + k]);
-    float r;
-    if (SEQ) r = (float)dadd((double)a, dmul(0.5, (double)s));
-    else r = fadd(a, fmul(0.5f, s));
-    dst[(long)(v + 1) * L + k] = r;
+    const long total = live_total(lv, M) * L;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const long u = t / L;
+        const int k = (int)(t - u * L);
+        const int v = (int)live_unit(lv, u);
+        const int2 nb = nbr[v];
+        const float a = src[(long)(v + 1) * L + k];
+        const float s = fadd(src[(long)nb.x * L + k], src[(long)nb.y * L + k]);
+        float r;
+        if (SEQ) r = (float)dadd((double)a, dmul(0.5, (double)s));
+        else r = fadd(a, fmul(0.5f, s));
+        dst[(long)(v + 1) * L + k] = r;
+    }
 }
 
 // The blur pass over rows padded to Lp = 4 Q floats (sseCompute, L > 2):
@@ -647,23 +671,25 @@ __global__ void blur_kernel(int M, int Lrt, const int2* __restrict__ nbr,
 // blur_kernel; the padding lanes hold zeros and stay zero.
 template <int Q>
 __global__ void blur4_kernel(int M, int Qrt, const int2* __restrict__ nbr, const float* __restrict__ src,
-                             float* __restrict__ dst, Skip sk) {
+                             float* __restrict__ dst, Live lv) {
     const int Qn = Q ? Q : Qrt;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)M * Qn) return;
-    const int v = (int)(t / Qn), q = (int)(t - (long)v * Qn);
-    if (skipped(sk, v)) return;
     const long lp = 4L * Qn;
-    const int2 nb = nbr[v];
-    const float4 a = *reinterpret_cast<const float4*>(src + (long)(v + 1) * lp + 4 * q);
-    const float4 x = *reinterpret_cast<const float4*>(src + (long)nb.x * lp + 4 * q);
-    const float4 y = *reinterpret_cast<const float4*>(src + (long)nb.y * lp + 4 * q);
-    float4 r;
-    r.x = fadd(a.x, fmul(0.5f, fadd(x.x, y.x)));
-    r.y = fadd(a.y, fmul(0.5f, fadd(x.y, y.y)));
-    r.z = fadd(a.z, fmul(0.5f, fadd(x.z, y.z)));
-    r.w = fadd(a.w, fmul(0.5f, fadd(x.w, y.w)));
-    *reinterpret_cast<float4*>(dst + (long)(v + 1) * lp + 4 * q) = r;
+    const long total = live_total(lv, M) * Qn;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+        const long u = t / Qn;
+        const int q = (int)(t - u * Qn);
+        const int v = (int)live_unit(lv, u);
+        const int2 nb = nbr[v];
+        const float4 a = *reinterpret_cast<const float4*>(src + (long)(v + 1) * lp + 4 * q);
+        const float4 x = *reinterpret_cast<const float4*>(src + (long)nb.x * lp + 4 * q);
+        const float4 y = *reinterpret_cast<const float4*>(src + (long)nb.y * lp + 4 * q);
+        float4 r;
+        r.x = fadd(a.x, fmul(0.5f, fadd(x.x, y.x)));
+        r.y = fadd(a.y, fmul(0.5f, fadd(x.y, y.y)));
+        r.z = fadd(a.z, fmul(0.5f, fadd(x.z, y.z)));
+        r.w = fadd(a.w, fmul(0.5f, fadd(x.w, y.w)));
+        *reinterpret_cast<float4*>(dst + (long)(v + 1) * lp + 4 * q) = r;
+    }
 }
 
 __device__ __forceinline__ float apply_epilogue(float v, long t, int i, int k, const SliceEpilogue& ep) {
@@ -681,23 +707,26 @@ __device__ __forceinline__ float apply_epilogue(float v, long t, int i, int k, c
 template <bool SEQ, int DC, int LC>
 __global__ void slice_kernel(int N, int Lrt, int drt, const int* __restrict__ offset,
                              const float* __restrict__ bary, const float* __restrict__ vals,
-                             float alpha, float* out, SliceEpilogue ep, Skip sk) {
+                             float alpha, float* out, SliceEpilogue ep, Live lv) {
     const int L = LC ? LC : Lrt, d = DC ? DC : drt;
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long)N * L) return;
-    const int i = (int)(t / L), k = (int)(t - (long)i * L);
     const int d1 = d + 1;
-    if (skipped(sk, offset[(long)i * d1])) return;
-    float acc = 0.0f;
+    const long total = live_total(lv, N) * L;
+    for (long tl = (long)blockIdx.x * blockDim.x + threadIdx.x; tl < total; tl += (long)gridDim.x * blockDim.x) {
+        const long u = tl / L;
+        const int k = (int)(tl - u * L);
+        const int i = (int)live_unit(lv, u);  // the pixel
+        const long t = (long)i * L + k;
+        float acc = 0.0f;
 #pragma unroll
-    for (int j = 0; j <= d; j++) {
-        const int o = offset[(long)i * d1 + j];
-        const float w = bary[(long)i * d1 + j];
-        const float v = vals[(long)(o + 1) * L + k];
-        if (SEQ) acc = fadd(acc, fmul(fmul(w, v), alpha));
-        else acc = fadd(acc, fmul(fmul(w, alpha), v));
+        for (int j = 0; j <= d; j++) {
+            const int o = offset[(long)i * d1 + j];
+            const float w = bary[(long)i * d1 + j];
+            const float v = vals[(long)(o + 1) * L + k];
+            if (SEQ) acc = fadd(acc, fmul(fmul(w, v), alpha));
+            else acc = fadd(acc, fmul(fmul(w, alpha), v));
+        }
+        out[t] = apply_epilogue(acc, t, i, k, ep);
     }
-    out[t] = apply_epilogue(acc, t, i, k, ep);
 }
 
 // Slice over rows padded to Lp = 4 Q floats (sseCompute, L > 2), a tile of
@@ -717,7 +746,7 @@ template <int DC, int Q, int LC>
 __global__ void __launch_bounds__(kSliceThreads)
     slice4_kernel(int N, int Lrt, int Qrt, int drt, int tile, const int* __restrict__ offset,
                   const float* __restrict__ bary, const float* __restrict__ vals, float alpha, float* out,
-                  SliceEpilogue ep, Skip sk) {
+                  SliceEpilogue ep, Live lv, const long* __restrict__ pix_base) {
     extern __shared__ __align__(16) unsigned char slice_smem[];
     const int d1 = (DC ? DC : drt) + 1, Qn = Q ? Q : Qrt, L = LC ? LC : Lrt;
     const long lp = 4L * Qn;
@@ -725,61 +754,67 @@ __global__ void __launch_bounds__(kSliceThreads)
     float* s_wa = reinterpret_cast<float*>(s_off + tile * d1);
     float* s_nrm = s_wa + tile * d1;
     float* s_out = s_nrm + tile;
-    const long p0 = (long)blockIdx.x * tile;
-    const int np = (int)min((long)tile, (long)N - p0);
-    for (int e = threadIdx.x; e < np * d1; e += blockDim.x) {
-        s_off[e] = offset[p0 * d1 + e];
-        s_wa[e] = fmul(bary[p0 * d1 + e], alpha);
-    }
     const bool use_norm = ep.potts && ep.norm;
-    if (use_norm)
-        for (int e = threadIdx.x; e < np; e += blockDim.x) s_nrm[e] = ep.norm[p0 + e];
-    __syncthreads();
-    for (int it = threadIdx.x; it < np * Qn; it += blockDim.x) {
-        const int pl = it / Qn, q = it - pl * Qn;
-        if (skipped(sk, s_off[pl * d1])) continue;
-        float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int j = 0; j < (DC ? DC + 1 : 17); j++) {
-            if (!DC && j >= d1) break;
-            const int o = s_off[pl * d1 + j];
-            const float wa = s_wa[pl * d1 + j];
-            const float4 v = *reinterpret_cast<const float4*>(vals + (long)(o + 1) * lp + 4 * q);
-            a[0] = fadd(a[0], fmul(wa, v.x));
-            a[1] = fadd(a[1], fmul(wa, v.y));
-            a[2] = fadd(a[2], fmul(wa, v.z));
-            a[3] = fadd(a[3], fmul(wa, v.w));
+    // Tiles: of the whole pixel range, or (live images) of each live image's
+    // pixels, image by image (pix_base: its pixel offsets).
+    const long total = live_total(lv, ((long)N + tile - 1) / tile);
+    for (long u = blockIdx.x; u < total; u += gridDim.x) {  // block-uniform
+        long p0, pend = N;
+        if (lv.n) {
+            long local;
+            const int img = live_locate(lv, u, local);
+            p0 = pix_base[img] + local * tile;
+            pend = pix_base[img + 1];
+        } else {
+            p0 = u * tile;
         }
-        const int k0 = 4 * q;
-        float* so = s_out + pl * L + k0;
+        const int np = (int)min((long)tile, pend - p0);
+        for (int e = threadIdx.x; e < np * d1; e += blockDim.x) {
+            s_off[e] = offset[p0 * d1 + e];
+            s_wa[e] = fmul(bary[p0 * d1 + e], alpha);
+        }
+        if (use_norm)
+            for (int e = threadIdx.x; e < np; e += blockDim.x) s_nrm[e] = ep.norm[p0 + e];
+        __syncthreads();
+        for (int it = threadIdx.x; it < np * Qn; it += blockDim.x) {
+            const int pl = it / Qn, q = it - pl * Qn;
+            float a[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-        for (int c = 0; c < 4; c++) {
-            if (k0 + c >= L) break;
-            float v = a[c];
-            if (ep.potts) {
-                if (use_norm) v = fmul(v, s_nrm[pl]);
-                v = ep.scale_vec ? fmul(ep.scale_vec[k0 + c], v) : fmul(ep.scale, v);
+            for (int j = 0; j < (DC ? DC + 1 : 17); j++) {
+                if (!DC && j >= d1) break;
+                const int o = s_off[pl * d1 + j];
+                const float wa = s_wa[pl * d1 + j];
+                const float4 v = *reinterpret_cast<const float4*>(vals + (long)(o + 1) * lp + 4 * q);
+                a[0] = fadd(a[0], fmul(wa, v.x));
+                a[1] = fadd(a[1], fmul(wa, v.y));
+                a[2] = fadd(a[2], fmul(wa, v.z));
+                a[3] = fadd(a[3], fmul(wa, v.w));
             }
-            so[c] = v;
+            const int k0 = 4 * q;
+            float* so = s_out + pl * L + k0;
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                if (k0 + c >= L) break;
+                float v = a[c];
+                if (ep.potts) {
+                    if (use_norm) v = fmul(v, s_nrm[pl]);
+                    v = ep.scale_vec ? fmul(ep.scale_vec[k0 + c], v) : fmul(ep.scale, v);
+                }
+                so[c] = v;
+            }
         }
-    }
-    __syncthreads();
-    const long t0 = p0 * L;
-    const int ne = np * L;
-    if (sk.done) {  // batched solves: pixels of finished images keep their output
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            if (skipped(sk, s_off[(e / L) * d1])) continue;
-            float v = s_out[e];
-            if (ep.base) v = fadd(ep.base[t0 + e], fmul(ep.coef, v));
-            else if (ep.zero_base) v = fadd(0.0f, fmul(ep.coef, v));
-            out[t0 + e] = v;
+        __syncthreads();
+        const long t0 = p0 * L;
+        const int ne = np * L;
+        if (ep.base) {
+            for (int e = threadIdx.x; e < ne; e += blockDim.x)
+                out[t0 + e] = fadd(ep.base[t0 + e], fmul(ep.coef, s_out[e]));
+        } else if (ep.zero_base) {
+            for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = fadd(0.0f, fmul(ep.coef, s_out[e]));
+        } else {
+            for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = s_out[e];
         }
-    } else if (ep.base) {
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = fadd(ep.base[t0 + e], fmul(ep.coef, s_out[e]));
-    } else if (ep.zero_base) {
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = fadd(0.0f, fmul(ep.coef, s_out[e]));
-    } else {
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) out[t0 + e] = s_out[e];
+        __syncthreads();  // the next tile restages the shared arrays
     }
 }
 
@@ -830,16 +865,31 @@ __device__ __forceinline__ float step_ge(float a, float b) {  // a >= b ? 1 : 0
 
 // One entry into the bin-b pair (lower, upper) of packed accumulators:
 // acc = fma({[cl >= b], [b >= cu]}, w2, acc) with one f32x2 FMA, which rounds
-// each half exactly as fma.rn.f32 does.  w2 holds (w, w).
+// each half exactly as fma.rn.f32 does.  w2 holds (w, w).  The bins are
+// small integers, so the masks are saturated sums: cl + (1 - b) and
+// (b + 1) - cu are exact integers, clamped to [0, 1] they are exactly the
+// comparisons (and a NaN would clamp to +0).  One `add.sat` per mask.
 __device__ __forceinline__ void ord_step2(unsigned long long& acc, float cl, float cu, float b,
                                           unsigned long long w2) {
+    const float lo_c = 1.0f - b, up_c = b + 1.0f;  // exact; hoisted out of the entry loops
     asm("{\n\t.reg .f32 ml, mu;\n\t.reg .b64 m;\n\t"
-        "set.ge.f32.f32 ml, %1, %3;\n\t"
-        "set.ge.f32.f32 mu, %3, %2;\n\t"
+        "add.rn.sat.f32 ml, %1, %3;\n\t"
+        "sub.rn.sat.f32 mu, %4, %2;\n\t"
         "mov.b64 m, {ml, mu};\n\t"
-        "fma.rn.f32x2 %0, m, %4, %0;\n\t}"
+        "fma.rn.f32x2 %0, m, %5, %0;\n\t}"
         : "+l"(acc)
-        : "f"(cl), "f"(cu), "f"(b), "l"(w2));
+        : "f"(cl), "f"(cu), "f"(lo_c), "f"(up_c), "l"(w2));
+}
+// The single masks of ord_step2: [cl >= b] and [b >= cu] as 0.0 / 1.0.
+__device__ __forceinline__ float ord_mask_lower(float cl, int b) {
+    float m;
+    asm("add.rn.sat.f32 %0, %1, %2;" : "=f"(m) : "f"(cl), "f"(1.0f - (float)b));
+    return m;
+}
+__device__ __forceinline__ float ord_mask_upper(float cu, int b) {
+    float m;
+    asm("sub.rn.sat.f32 %0, %1, %2;" : "=f"(m) : "f"((float)b + 1.0f), "f"(cu));
+    return m;
 }
 __device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
     unsigned long long r;
@@ -1108,23 +1158,29 @@ __global__ void ord_splat_short_kernel(int n_short, int Lrt, const int* __restri
     const int u = (int)(t / L), k = (int)(t - (long)u * L);
     const int v = order[u];
     const int s0 = seg_start[v], s1 = seg_start[v + 1];
-    unsigned long long acc[kRes];  // (lower, upper) sums of bin b
+    // Scalar chains: every entry reaches lower bin 0 (c_lower >= 0) and upper
+    // bin 9 (c_upper <= 9), plain adds there; the other 18 bins take a
+    // saturated-sum mask (exactly 0 or 1) and an FMA, fma(1, w, acc) being
+    // acc + w rounded once.
+    float lo[kRes], up[kRes];
 #pragma unroll
-    for (int b = 0; b < kRes; b++) acc[b] = 0ull;
+    for (int b = 0; b < kRes; b++) lo[b] = up[b] = 0.0f;
 #pragma unroll 2
     for (int s = s0; s < s1; s++) {
         const float2 x = bins[(long)seg_pix[s] * L + k];
         const float w = seg_w[s];
-        const unsigned long long w2 = pack2(w, w);
+        lo[0] = fadd(lo[0], w);
 #pragma unroll
-        for (int b = 0; b < kRes; b++) ord_step2(acc[b], x.x, x.y, (float)b, w2);
+        for (int b = 1; b < kRes; b++) lo[b] = __fmaf_rn(ord_mask_lower(x.x, b), w, lo[b]);
+#pragma unroll
+        for (int b = 0; b < kRes - 1; b++) up[b] = __fmaf_rn(ord_mask_upper(x.y, b), w, up[b]);
+        up[kRes - 1] = fadd(up[kRes - 1], w);
     }
     float* row = vals + (long)(v + 1) * kOrdW * L + k;
 #pragma unroll
     for (int b = 0; b < kRes; b++) {
-        const float2 r = unpack2(acc[b]);
-        row[(long)b * L] = r.x;
-        row[(long)(kRes + b) * L] = r.y;
+        row[(long)b * L] = lo[b];
+        row[(long)(kRes + b) * L] = up[b];
     }
 }
 
@@ -1560,15 +1616,15 @@ void gradient_impl(Lattice& lat, float* df, const float* a, const float* b, int 
         if (lat.n_long)
             launch(splat_kernel<false>, ceil_div(lat.n_long, kStageWarps), 32 * kStageWarps, 0, st, lat.n_long, L,
                    lat.vorder.get(), lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in, nullptr, src,
-                   Skip{}, L);
+                   Live{}, L);
         if (n_short)
             launch(splat_short_kernel<false>, ceil_div(SL, kTB), kTB, 0, st, n_short, L,
                    lat.vorder.get() + lat.n_long, lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in,
-                   nullptr, src, Skip{}, L);
+                   nullptr, src, Live{}, L);
         for (int jj = 0; jj <= d; jj++) {
             const int j = dir ? d - jj : jj;
             launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, lat.nbr.get() + (long)j * M, src, dst,
-                   Skip{});
+                   Live{});
             std::swap(src, dst);
         }
         launch(grad_slice_kernel<DM>, ceil_div(N, 128), 128, 0, st, N, L, d, lat.offset.get(), lat.rank.get(), src,
@@ -1674,18 +1730,69 @@ void Lattice::concat(const std::vector<const Lattice*>& parts) {
     int* ok = vorder_keys.ensure(M);
     launch(order_key_kernel, ceil_div(M, kTB), kTB, 0, st, M, cnt, ok, vo);
     radix_sort_pairs(ok, vo, M, 24, sort, st);
+    // Then, stably, by (class, image): each class (huge, long, short lists)
+    // holds its lists image by image, longest first within an image, so
+    // that an image's lists of a class are one contiguous range of the order
+    // (the live-image domains of a batched solve).
+    const int B = (int)parts.size();
+    DevBuf<int> pci;
+    int* per_ci = pci.ensure((size_t)3 * B);
+    DCRF_CUDA(cudaMemsetAsync(per_ci, 0, sizeof(int) * 3 * B, st));
+    launch(class_image_key_kernel, ceil_div(M, kTB), kTB, 0, st, M, (const int*)vo, (const int*)cnt,
+           (const int*)vi, B, ok, per_ci);
+    int kbits = 1;
+    while ((1L << kbits) < 3L * B) kbits++;
+    radix_sort_pairs(ok, vo, M, kbits, sort, st);
     int* dl = total.ensure(2);
     DCRF_CUDA(cudaMemsetAsync(dl, 0, 2 * sizeof(int), st));
     launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, cnt, kLongList, dl);
     launch(count_long_kernel, ceil_div(M, kTB), kTB, 0, st, M, cnt, kHugeList, dl + 1);
     DCRF_LAUNCH_CHECK();
     int nl[2];
+    std::vector<int> hci((size_t)3 * B);
     DCRF_CUDA(cudaMemcpyAsync(nl, dl, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    DCRF_CUDA(cudaMemcpyAsync(hci.data(), per_ci, sizeof(int) * 3 * B, cudaMemcpyDeviceToHost, st));
     DCRF_CUDA(cudaStreamSynchronize(st));  // also keeps &Ei alive until its copy ran
     n_long = nl[0];
     n_huge = nl[1];
+    // Per-image domains: list positions per class, vertex ids, pixels.
+    images = B;
+    img_pixels.assign(B, 0);
+    std::vector<long> hb((size_t)kDomains * (B + 1), 0);
+    auto row = [&](int dom) { return hb.data() + (long)dom * (B + 1); };
+    long pos = 0;
+    for (int c = 0; c < 3; c++) {
+        long* r = row(kDomHuge + c);
+        for (int i = 0; i < B; i++) {
+            r[i] = pos;
+            pos += hci[(size_t)c * B + i];
+        }
+        r[B] = pos;
+    }
+    for (int i = 0; i < B; i++) {
+        img_pixels[i] = parts[i]->N;
+        row(kDomVert)[i + 1] = row(kDomVert)[i] + parts[i]->M;
+        row(kDomPix)[i + 1] = row(kDomPix)[i] + parts[i]->N;
+    }
+    long* db = dom_base.ensure(hb.size());
+    DCRF_CUDA(cudaMemcpyAsync(db, hb.data(), sizeof(long) * hb.size(), cudaMemcpyHostToDevice, st));
+    DCRF_CUDA(cudaStreamSynchronize(st));  // hb is the copy's source
+    dom_tile = 0;
     va_floats = 0;
     concatenated = true;
+}
+
+void Lattice::prepare_live(int L) {
+    require(concatenated && images > 0, DCRF_E_STATE, "live images: not a concatenated lattice");
+    if (L <= 2) return;  // the element-wise slice needs no tile domain
+    const int tile = slice_tile_for(L);
+    if (tile == dom_tile) return;
+    std::vector<long> r(images + 1, 0);
+    for (int i = 0; i < images; i++) r[i + 1] = r[i] + (img_pixels[i] + tile - 1) / tile;
+    DCRF_CUDA(cudaMemcpyAsync(dom_base.get() + (long)kDomTile * (images + 1), r.data(), sizeof(long) * r.size(),
+                              cudaMemcpyHostToDevice, stream));
+    DCRF_CUDA(cudaStreamSynchronize(stream));  // r is the copy's source
+    dom_tile = tile;
 }
 
 void Lattice::build(const float* d_features, int d_, int N_) {
@@ -1786,27 +1893,27 @@ void Lattice::compute_noalloc(float* out, const float* in, int L, bool reverse) 
     const int n_short = M - n_long;
     if (n_long)
         launch(splat_kernel<false>, ceil_div(n_long, kStageWarps), 32 * kStageWarps, 0, st, n_long, L,
-               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{}, L);
+               vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Live{}, L);
     if (n_short)
         launch(splat_short_kernel<false>, ceil_div((long)n_short * L, kTB), kTB, 0, st, n_short, L,
-               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Skip{}, L);
+               vorder.get() + n_long, seg_start.get(), seg_pix.get(), seg_w.get(), in, nullptr, src, Live{}, L);
     const bool seq = L <= 2;
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
         if (seq)
-            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{});
+            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Live{});
         else
-            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Skip{});
+            launch(blur_kernel<false>, ceil_div(ML, kTB), kTB, 0, st, M, L, nbr.get() + (long)j * M, src, dst, Live{});
         std::swap(src, dst);
     }
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
     const SliceEpilogue ep;
     if (seq)
         launch(slice_kernel<true, 0, 0>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
-               out, ep, Skip{});
+               out, ep, Live{});
     else
         launch(slice_kernel<false, 0, 0>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src, alpha,
-               out, ep, Skip{});
+               out, ep, Live{});
     DCRF_LAUNCH_CHECK();
 }
 
@@ -1821,14 +1928,25 @@ void Lattice::compute(float* out, const float* in, int L, bool reverse, const Sl
 // keeps L.
 static int value_row(int L) { return L > 2 ? (L + 3) & ~3 : L; }
 
+// Blocks of a launch over `units` work items, `per_block` per block of
+// `threads` threads: all of them at once, or -- with live images, whose
+// units are counted on the device -- twice as many blocks as the SMs hold
+// at full occupancy, looping over them.
+static int unit_grid(long units, int per_block, bool live, int threads) {
+    const long g = std::max(1L, (units + per_block - 1) / per_block);
+    return live ? (int)std::min(g, (long)sm_count() * 2 * (2048 / threads)) : (int)g;
+}
+
 // The warp splat (L = 21) over order[first, first + count) with `warps`
-// vertices per block.
-static void splat_warp_range(const Lattice& lat, int warps, int first, int count, int L, int Lp, const float* in,
-                             const float* pre_norm, float* vals, const Skip& sk, cudaStream_t st) {
+// vertices per block; with live images, over domain `dom`'s live lists.
+static void splat_warp_range(const Lattice& lat, int warps, int dom, int first, int count, int L, int Lp,
+                             const float* in, const float* pre_norm, float* vals, cudaStream_t st) {
     if (count <= 0) return;
+    const Live lv = lat.live_of(dom);
+    const int* order = lat.vorder.get() + (lv.n ? 0 : first);
     auto go = [&](auto kern, int w) {
-        launch(kern, ceil_div(count, w), 32 * w, 0, st, count, L, lat.vorder.get() + first, lat.seg_start.get(),
-               lat.seg_pix.get(), lat.seg_w.get(), in, pre_norm, vals, sk, Lp);
+        launch(kern, unit_grid(count, w, lv.n != nullptr, 32 * w), 32 * w, 0, st, count, L, order, lat.seg_start.get(),
+               lat.seg_pix.get(), lat.seg_w.get(), in, pre_norm, vals, lv, Lp);
     };
     if (pre_norm) {
         if (warps == 2) go(splat_warp_kernel<true, 21, 2>, 2);
@@ -1897,7 +2015,6 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
     FilterShape best;
     float* src = va.get();
     float* dst = vb.get();
-    const Skip none{};
     float tbest = 1e30f;
     for (int kind = 0; kind < 3; kind++) {
         for (int w : {2, 4, 8}) {
@@ -1905,7 +2022,7 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
             FilterShape fs = best;
             fs.splat_kind = kind;
             fs.splat_warps = w;
-            const float t = timed([&] { splat_rest(fs, in, L, pre_norm, src, none, st); });
+            const float t = timed([&] { splat_rest(fs, in, L, pre_norm, src, false, st); });
             if (t < tbest) {
                 tbest = t;
                 best.splat_kind = kind;
@@ -1918,7 +2035,7 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
     tbest = 1e30f;
     for (int bt : {128, 256, 512}) {
         const float t = timed([&] {
-            launch(blur4_kernel<6>, ceil_div(MQ, bt), bt, 0, st, M, Q, nbr.get(), (const float*)src, dst, none);
+            launch(blur4_kernel<6>, ceil_div(MQ, bt), bt, 0, st, M, Q, nbr.get(), (const float*)src, dst, Live{});
         });
         if (t < tbest) tbest = t, best.blur_threads = bt;
     }
@@ -1934,7 +2051,8 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
             const float t = timed([&] {
                 auto sl = [&](auto kern) {
                     launch(kern, ceil_div(N, tl), kSliceThreads, (size_t)tl * per_px, st, N, L, Q, d, tl,
-                           offset.get(), bary.get(), (const float*)src, alpha, o, ep, none);
+                           offset.get(), bary.get(), (const float*)src, alpha, o, ep, Live{},
+                           (const long*)nullptr);
                 };
                 if (d == 5) sl(slice4_kernel<5, 6, 21>);
                 else if (d == 2) sl(slice4_kernel<2, 6, 21>);
@@ -1953,28 +2071,37 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
 }
 
 void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
-                         const Skip& sk, cudaStream_t st) {
+                         bool live, cudaStream_t st) {
     const int Lp = value_row(L);
     const int nh = n_huge, n_short = M - n_long;
     const int kind = L == 21 ? fs.splat_kind : 0;
-    if (kind == 2) {
-        splat_warp_range(*this, fs.splat_warps, nh, M - nh, L, Lp, in, pre_norm, vals, sk, st);
+    if (kind == 2 && !live) {
+        splat_warp_range(*this, fs.splat_warps, kDomLong, nh, M - nh, L, Lp, in, pre_norm, vals, st);
         return;
     }
     if (n_long > nh) {
-        if (kind == 1)
-            splat_warp_range(*this, fs.splat_warps, nh, n_long - nh, L, Lp, in, pre_norm, vals, sk, st);
-        else
+        if (kind >= 1) {
+            splat_warp_range(*this, fs.splat_warps, kDomLong, nh, n_long - nh, L, Lp, in, pre_norm, vals, st);
+        } else {
+            const Live lv = live ? live_of(kDomLong) : Live{};
             launch(L == 21 ? (pre_norm ? splat_kernel<true, 21> : splat_kernel<false, 21>)
                            : (pre_norm ? splat_kernel<true> : splat_kernel<false>),
-                   ceil_div(n_long - nh, kStageWarps), 32 * kStageWarps, 0, st, n_long - nh, L, vorder.get() + nh,
-                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals, sk, Lp);
+                   unit_grid(n_long - nh, kStageWarps, live, 32 * kStageWarps), 32 * kStageWarps, 0, st, n_long - nh, L,
+                   vorder.get() + (live ? 0 : nh), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals,
+                   lv, Lp);
+        }
     }
-    if (n_short)
-        launch(L == 21 ? (pre_norm ? splat_short_kernel<true, 21> : splat_short_kernel<false, 21>)
-                       : (pre_norm ? splat_short_kernel<true> : splat_short_kernel<false>),
-               ceil_div((long)n_short * Lp, kTB), kTB, 0, st, n_short, L, vorder.get() + n_long, seg_start.get(),
-               seg_pix.get(), seg_w.get(), in, pre_norm, vals, sk, Lp);
+    if (n_short) {
+        if (kind == 2) {  // live: the short lists are their own domain
+            splat_warp_range(*this, fs.splat_warps, kDomShort, n_long, n_short, L, Lp, in, pre_norm, vals, st);
+        } else {
+            const Live lv = live ? live_of(kDomShort) : Live{};
+            launch(L == 21 ? (pre_norm ? splat_short_kernel<true, 21> : splat_short_kernel<false, 21>)
+                           : (pre_norm ? splat_short_kernel<true> : splat_short_kernel<false>),
+                   unit_grid((long)n_short * Lp, kTB, live, kTB), kTB, 0, st, n_short, L, vorder.get() + (live ? 0 : n_long),
+                   seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals, lv, Lp);
+        }
+    }
 }
 
 void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_norm) {
@@ -1985,7 +2112,8 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
     cudaStream_t st = stream;
     const long ML = (long)M * L;
     float *src = va.get(), *dst = vb.get();
-    const Skip sk{vimg.get(), skip_done};
+    // A batched solve's live images: only their lists, vertices and pixels.
+    const bool live = live_n != nullptr;
     // As in the ordered filter, the lists longer than kHugeList (the first
     // nh of the order) run on the high-priority side stream while the
     // others are splatted: with L = 21 by the transposing ring (one warp's
@@ -1998,16 +2126,16 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
         ensure_aux();
         DCRF_CUDA(cudaEventRecord(ev_fork, st));
         DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
+        const Live lv = live_of(kDomHuge);
+        const int g = unit_grid(nh, kStageWarps, live, 32 * kStageWarps);
         if (L == 21)
-            launch(pre_norm ? splat_ring21_kernel<true> : splat_ring21_kernel<false>, ceil_div(nh, kStageWarps),
-                   32 * kStageWarps, 0, aux, nh, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in,
-                   pre_norm, src, sk, Lp);
+            launch(pre_norm ? splat_ring21_kernel<true> : splat_ring21_kernel<false>, g, 32 * kStageWarps, 0, aux,
+                   nh, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, lv, Lp);
         else
-            launch(pre_norm ? splat_kernel<true> : splat_kernel<false>, ceil_div(nh, kStageWarps),
-                   32 * kStageWarps, 0, aux, nh, L, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in,
-                   pre_norm, src, sk, Lp);
+            launch(pre_norm ? splat_kernel<true> : splat_kernel<false>, g, 32 * kStageWarps, 0, aux, nh, L,
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, lv, Lp);
     }
-    splat_rest(shape, in, L, pre_norm, src, sk, st);
+    splat_rest(shape, in, L, pre_norm, src, live, st);
     if (forked) {
         DCRF_CUDA(cudaEventRecord(ev_join, aux));
         DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
@@ -2015,20 +2143,29 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
     const bool seq = L <= 2;
     const int Q = Lp / 4;
     const long MQ = (long)M * Q;
+    const Live lvv = live_of(kDomVert);
     for (int jj = 0; jj <= d; jj++) {
         const int j = reverse ? d - jj : jj;
         const int2* nb = nbr.get() + (long)j * M;
-        if (seq)
-            launch(blur_kernel<true>, ceil_div(ML, kTB), kTB, 0, st, M, L, nb, src, dst, sk);
-        else if (Q == 6)
-            launch(blur4_kernel<6>, ceil_div(MQ, shape.blur_threads), shape.blur_threads, 0, st, M, Q, nb, src, dst,
-                   sk);
-        else
-            launch(blur4_kernel<0>, ceil_div(MQ, kTB), kTB, 0, st, M, Q, nb, src, dst, sk);
+        if (seq) {
+            launch(blur_kernel<true>, unit_grid(ML, kTB, live, kTB), kTB, 0, st, M, L, nb, src, dst, lvv);
+        } else if (Q == 6) {
+            const int bt = shape.blur_threads;
+            launch(blur4_kernel<6>, unit_grid(MQ, bt, live, bt), bt, 0, st, M, Q, nb, src, dst, lvv);
+        } else {
+            launch(blur4_kernel<0>, unit_grid(MQ, kTB, live, kTB), kTB, 0, st, M, Q, nb, src, dst, lvv);
+        }
         std::swap(src, dst);
     }
     plain_vals = src;
     plain_L = L;
+}
+
+int Lattice::slice_tile_for(int L) const {
+    // pixels per tile: kSliceTile (the tuned size for L = 21), fewer for very
+    // wide rows (40 KB of shared memory at most)
+    const int per_px = (d + 1) * 8 + 4 + L * 4;
+    return std::max(1, std::min(L == 21 ? shape.slice_tile : kSliceTile, (40 << 10) / per_px));
 }
 
 void Lattice::slice(float* out, int L, const SliceEpilogue& ep) {
@@ -2037,19 +2174,21 @@ void Lattice::slice(float* out, int L, const SliceEpilogue& ep) {
     const long NL = (long)N * L;
     const float* src = plain_vals;
     const float alpha = 1.0f / (1.0f + std::pow(2.0f, (float)-d));
-    const Skip sks{vimg.get(), skip_done};
+    const bool live = live_n != nullptr;
     if (L <= 2) {
-        launch(slice_kernel<true, 0, 0>, ceil_div(NL, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(), src,
-               alpha, out, ep, sks);
+        launch(slice_kernel<true, 0, 0>, unit_grid(NL, kTB, live, kTB), kTB, 0, st, N, L, d, offset.get(), bary.get(),
+               src, alpha, out, ep, live_of(kDomPix));
     } else {
         const int Q = value_row(L) / 4;
-        // pixels per tile: kSliceTile, fewer for very wide rows (40 KB of shared memory at most)
         const int per_px = (d + 1) * 8 + 4 + L * 4;
-        const int tile = std::max(1, std::min(L == 21 ? shape.slice_tile : kSliceTile, (40 << 10) / per_px));
+        // live images: tiles of each image's pixels, the size prepare_live fixed
+        const int tile = live ? dom_tile : slice_tile_for(L);
+        require(tile > 0, DCRF_E_STATE, "slice: live images without prepare_live");
         const size_t smem = (size_t)tile * per_px;
+        const long* pix_base = live ? dom_base.get() + (long)kDomPix * (images + 1) : nullptr;
         auto sl = [&](auto kern) {
-            launch(kern, ceil_div(N, tile), kSliceThreads, smem, st, N, L, Q, d, tile, offset.get(), bary.get(), src,
-                   alpha, out, ep, sks);
+            launch(kern, unit_grid(N, tile, live, kSliceThreads), kSliceThreads, smem, st, N, L, Q, d, tile, offset.get(),
+                   bary.get(), src, alpha, out, ep, live_of(kDomTile), pix_base);
         };
         if (d == 5 && L == 21) sl(slice4_kernel<5, 6, 21>);
         else if (d == 2 && L == 21) sl(slice4_kernel<2, 6, 21>);

@@ -48,12 +48,44 @@ int slice_grid(long n);
 // Capacity, in floats, of the fixed scratch array of compute_noalloc.
 size_t noalloc_scratch_floats();
 
-// Per-vertex skip flags of a concatenated lattice: vertex v is skipped when
-// done[vimg[v]] is set (no flags: nothing is skipped).
-struct Skip {
-    const int* vimg = nullptr;
-    const int* done = nullptr;
+// The units a filter launch covers.  Without `n`, every unit of the
+// launch's range.  With it (a batched solve), only the units of the images
+// still running: image i owns units [base[i], base[i+1]) of the launch's
+// domain (list positions, vertex ids or slice tiles), and the live images'
+// units are numbered consecutively, pre[r] being the number of units of the
+// live images before the r-th (n + 1 entries, written on the device each
+// iteration).  Work for finished images is then never launched, and the
+// kernels loop over the live units with grids sized for the device, not for
+// the batch.
+struct Live {
+    const int* n = nullptr;     // number of live images (device), or nullptr
+    const int* img = nullptr;   // their ids, ascending (device)
+    const long* base = nullptr; // the domain: B + 1 ascending unit offsets
+    const long* pre = nullptr;  // live prefix: n + 1 entries
 };
+
+#ifdef __CUDACC__
+// Units of a launch over `count` units, or over its live images' units.
+__device__ __forceinline__ long live_total(const Live& lv, long count) { return lv.n ? lv.pre[*lv.n] : count; }
+// Live unit u -> its image and its unit within that image.
+__device__ __forceinline__ int live_locate(const Live& lv, long u, long& local) {
+    int lo = 0, hi = *lv.n;  // pre[lo] <= u < pre[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (lv.pre[mid] <= u) lo = mid;
+        else hi = mid;
+    }
+    local = u - lv.pre[lo];
+    return lv.img[lo];
+}
+// Live unit u -> its unit in the domain (the identity without live images).
+__device__ __forceinline__ long live_unit(const Live& lv, long u) {
+    if (!lv.n) return u;
+    long local;
+    const int img = live_locate(lv, u, local);
+    return lv.base[img] + local;
+}
+#endif
 
 // Launch shapes of the plain filter for L = 21 (Lattice::splat_blur /
 // slice).  Every shape computes the same arithmetic; only the speed
@@ -100,7 +132,30 @@ struct Lattice {
 
     bool concatenated = false;  // built by concat(): no vertex keys
     DevBuf<int> vimg;           // concat(): image of each vertex
-    const int* skip_done = nullptr;  // concat(): per-image flags; compute() skips flagged images
+    // concat(): per-image work domains, kDomains rows of (images + 1) longs:
+    // the positions in vorder of each image's huge, long and short lists,
+    // its vertex ids, its slice tiles (tiles of dom_tile pixels, none
+    // crossing an image) and its pixels.
+    enum { kDomHuge, kDomLong, kDomShort, kDomVert, kDomTile, kDomPix, kDomains };
+    int images = 0;
+    std::vector<long> img_pixels;  // host: pixels of each image
+    DevBuf<long> dom_base;
+    int dom_tile = 0;
+    // A batched solve's live images (set around its loop, null otherwise) and
+    // this lattice's live prefixes: kDomains rows of (images + 1) longs.
+    const int* live_n = nullptr;
+    const int* live_img = nullptr;
+    const long* live_pre = nullptr;
+    // The Live of domain `dom` (no compaction when no live set is attached).
+    Live live_of(int dom) const {
+        if (!live_n) return Live{};
+        return Live{live_n, live_img, dom_base.get() + (long)dom * (images + 1),
+                    live_pre + (long)dom * (images + 1)};
+    }
+    // Tile size of the L = 21 / L > 2 plain slice for label count L.
+    int slice_tile_for(int L) const;
+    // Sets the slice-tile domain for label count L (host work, a small copy).
+    void prepare_live(int L);
 
     // features: device [N][d]
     void build(const float* d_features, int d_, int N_);
@@ -159,7 +214,7 @@ struct Lattice {
     // Splat of every list after the first n_huge (whose splat runs on the
     // side stream) into vals, in the form `fs` names.
     void splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
-                    const Skip& sk, cudaStream_t st);
+                    bool live, cudaStream_t st);
 
     Lattice() = default;
     Lattice(const Lattice&) = delete;

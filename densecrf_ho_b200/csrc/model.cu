@@ -28,26 +28,6 @@ int sm_count() {
 
 namespace {
 
-__global__ void gaussian_features_kernel(int W, int H, float sx, float sy, float* f) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= W * H) return;
-    const int j = p / W, i = p - j * W;
-    f[2 * (long)p] = (float)i / sx;
-    f[2 * (long)p + 1] = (float)j / sy;
-}
-
-__global__ void bilateral_features_kernel(int W, int H, float sx, float sy, float sr, float sg,
-                                          float sb, const uint8_t* __restrict__ im, float* f) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= W * H) return;
-    const int j = p / W, i = p - j * W;
-    f[5 * (long)p] = (float)i / sx;
-    f[5 * (long)p + 1] = (float)j / sy;
-    f[5 * (long)p + 2] = (float)im[3 * (long)p] / sr;
-    f[5 * (long)p + 3] = (float)im[3 * (long)p + 1] / sg;
-    f[5 * (long)p + 4] = (float)im[3 * (long)p + 2] / sb;
-}
-
 __global__ void fill_kernel(long n, float v, float* x) {
     const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t < n) x[t] = v;

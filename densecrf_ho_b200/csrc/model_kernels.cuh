@@ -195,13 +195,31 @@ __global__ void minmax_finish_kernel(const double* __restrict__ partials, int nb
 }
 
 // A NaN or infinity in a solver's inputs (the initial Q, the unaries):
-// sc->numeric |= 1, one atomicOr per block that saw one.
+// sc->numeric |= 1, one atomicOr per block that saw one.  float4 loads when
+// both arrays are 16-byte aligned (the tail and unaligned arrays by floats);
+// nonfinite_grid(n) blocks of 256 threads keep enough loads in flight for
+// HBM rate.
+__device__ __forceinline__ bool nonfinite4(float4 v) {
+    return !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w);
+}
 __global__ void nonfinite_kernel(long n, const float* __restrict__ a, const float* __restrict__ b,
                                  SolverScalars* sc) {
     bool bad = false;
-    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x)
-        bad |= !isfinite(a[t]) || !isfinite(b[t]);
+    const long t0 = (long)blockIdx.x * blockDim.x + threadIdx.x, stride = (long)gridDim.x * blockDim.x;
+    long head = 0;
+    if (((reinterpret_cast<unsigned long long>(a) | reinterpret_cast<unsigned long long>(b)) & 15) == 0) {
+        const long n4 = n / 4;
+        const float4* a4 = reinterpret_cast<const float4*>(a);
+        const float4* b4 = reinterpret_cast<const float4*>(b);
+        for (long t = t0; t < n4; t += stride) bad |= nonfinite4(a4[t]) || nonfinite4(b4[t]);
+        head = n4 * 4;
+    }
+    for (long t = head + t0; t < n; t += stride) bad |= !isfinite(a[t]) || !isfinite(b[t]);
     if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&sc->numeric, 1);
+}
+inline int nonfinite_grid(long n) {
+    const long g = (n / 4 + 255) / 256;
+    return (int)(g < 1 ? 1 : (g > 148 * 16 ? 148 * 16 : g));
 }
 
 // rescale (src/eigen_utils.cpp:120-141): out = (Q - min) / (max - min);

@@ -780,18 +780,6 @@ __global__ void lp_delta_kernel(SolverScalars* sc, float lambda) {
     sc->delta = delta;
 }
 
-// alpha += delta (sa - alpha); u += delta (su - u) (:737-738).
-__global__ void lp_alpha_kernel(long n, const float* __restrict__ sa, const float* __restrict__ su,
-                                float* __restrict__ alpha, float* __restrict__ u,
-                                const SolverScalars* __restrict__ sc) {
-    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const float d = sc->delta;
-    alpha[t] = fadd(alpha[t], fmul(d, fsub(sa[t], alpha[t])));
-    const float s = su ? su[t] : 0.0f;
-    u[t] = fadd(u[t], fmul(d, fsub(s, u[t])));
-}
-
 template <int LC>
 __device__ __forceinline__ void sort_desc(float* s, int L) {
     // insertion sort (values only: ties cannot change feasible_Q's result)
@@ -1277,7 +1265,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
     launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, part);
     launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 0, sc);
     launch(qp_init_energy_kernel, 1, 1, 0, stream, sc, nt, max_iter);
-    launch(nonfinite_kernel, kRedBlocks, kRedThreads, 0, stream, NL, (const float*)Q, unary.get(), sc);
+    launch(nonfinite_kernel, nonfinite_grid(NL), 256, 0, stream, NL, (const float*)Q, unary.get(), sc);
     DCRF_LAUNCH_CHECK();
     fetch_scalars();
     if (h_scal->numeric & 1)
@@ -1385,7 +1373,7 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
 
     DCRF_CUDA(cudaMemcpyAsync(Q, init, sizeof(float) * NL, cudaMemcpyDeviceToDevice, stream));
     DCRF_CUDA(cudaMemsetAsync(&sc->numeric, 0, sizeof(int), stream));
-    launch(nonfinite_kernel, kRedBlocks, kRedThreads, 0, stream, NL, (const float*)Q, unary.get(), sc);
+    launch(nonfinite_kernel, nonfinite_grid(NL), 256, 0, stream, NL, (const float*)Q, unary.get(), sc);
     with_lc(L, [&](auto lc) {
         constexpr int LC = decltype(lc)::value;
         launch(renormalize_kernel<LC>, pg, kPix, 0, stream, N, L, Q);
