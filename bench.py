@@ -679,7 +679,8 @@ def measure_batch_filter(n=64, reps=10):
         out[name] = {"M": M, "d": d, "ms": t * 1e3, "bytes": fb, "gbs": fb / t / 1e9, "frac": fb / t / 1e9 / peak,
                      "gpix_label_s": N * L / t / 1e9,
                      "launches_per_call": int((Ls.dcrf_kernel_launches() - l0) // reps),
-                     "tuned_shape": {"splat_form": ("staged", "warp_long", "warp_all")[shp[3]],
+                     "tuned_shape": {"splat_form": ("staged", "warp_long", "warp_all", "tiled_all",
+                                                    "staged_long_tiled_short")[shp[3]],
                                      "splat_vertices_per_block": shp[0], "blur_threads": shp[1],
                                      "slice_pixels_per_block": shp[2]}}
     return out

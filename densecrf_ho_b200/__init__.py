@@ -71,6 +71,19 @@ class Permutohedral:
                                          x.ctypes.data_as(C.c_void_p), x.shape[1], int(reverse)))
         return out
 
+    def filter_shape(self):
+        """Launch shapes of the 21-label plain filter: (splat warps per block,
+        blur threads, slice pixels per tile, splat form)."""
+        shp = (C.c_int * 4)()
+        check(lib().dcrf_lattice_filter_shape(self._h, shp))
+        return tuple(shp)
+
+    def set_filter_shape(self, shape):
+        """Pins the launch shapes (no autotuning for this lattice)."""
+        shp = (C.c_int * 4)(*[int(x) for x in shape])
+        check(lib().dcrf_lattice_set_filter_shape(self._h, shp))
+        return self
+
     def compute_upper_minus_lower_ord(self, Q):
         x = _f32(Q)
         out = np.empty_like(x)
@@ -529,6 +542,17 @@ class DenseCRF2DBatch:
         check(lib().dcrf_batch_pairwise_apply(self._h, int(k), out.ctypes.data_as(C.c_void_p),
                                               xx.ctypes.data_as(C.c_void_p)))
         return out
+
+    def filter_shape(self, k):
+        """Term k's launch shapes (see Permutohedral.filter_shape)."""
+        shp = (C.c_int * 4)()
+        check(lib().dcrf_batch_filter_shape(self._h, int(k), shp))
+        return tuple(shp)
+
+    def set_filter_shape(self, k, shape):
+        """Pins term k's launch shapes (no autotuning for its lattice)."""
+        shp = (C.c_int * 4)(*[int(x) for x in shape])
+        check(lib().dcrf_batch_set_filter_shape(self._h, int(k), shp))
 
     def lattice_size(self, k):
         """Vertex count of term k's concatenated lattice."""

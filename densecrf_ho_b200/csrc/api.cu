@@ -321,6 +321,47 @@ dcrf_status dcrf_lattice_export(dcrf_lattice h, int32_t* offset, int32_t* rank, 
     });
 }
 
+namespace {
+// shape[4] = {splat warps per block, blur threads, slice pixels per tile,
+// splat form} (FilterShape), validated against the tuner's candidates.
+dcrf::FilterShape shape_from(const int* shape) {
+    need(shape, "shape");
+    const int w = shape[0], bt = shape[1], tile = shape[2], kind = shape[3];
+    dcrf::require((w == 2 || w == 4 || w == 8) && (bt == 128 || bt == 256 || bt == 512) &&
+                      (tile == 64 || tile == 128 || tile == 256) && kind >= 0 && kind <= 4,
+                  DCRF_E_ARG, "filter shape: warps in {2,4,8}, blur threads in {128,256,512}, "
+                              "slice tile in {64,128,256}, splat form in 0..4");
+    dcrf::FilterShape f;
+    f.splat_warps = w;
+    f.blur_threads = bt;
+    f.slice_tile = tile;
+    f.splat_kind = kind;
+    return f;
+}
+void shape_to(const dcrf::FilterShape& f, int* shape) {
+    need(shape, "shape");
+    shape[0] = f.splat_warps;
+    shape[1] = f.blur_threads;
+    shape[2] = f.slice_tile;
+    shape[3] = f.splat_kind;
+}
+}  // namespace
+
+dcrf_status dcrf_lattice_filter_shape(dcrf_lattice h, int* shape) {
+    return guard([&] {
+        need(h, "lattice");
+        shape_to(h->lat.shape, shape);
+    });
+}
+
+dcrf_status dcrf_lattice_set_filter_shape(dcrf_lattice h, const int* shape) {
+    return guard([&] {
+        need(h, "lattice");
+        h->lat.shape = shape_from(shape);
+        h->lat.shape_L = 21;  // pinned: no tuning for this lattice
+    });
+}
+
 dcrf_status dcrf_lattice_stream(dcrf_lattice h, void** stream) {
     return guard([&] {
         need(h, "lattice");
@@ -1297,11 +1338,18 @@ dcrf_status dcrf_batch_filter_shape(dcrf_batch h, int k, int* shape) {
         need(shape, "shape");
         dcrf::require(k >= 0 && k < (int)b.terms.size(), DCRF_E_ARG, "pairwise term index out of range");
         b.ensure_lattices();
-        const dcrf::FilterShape& f = b.terms[k]->lat->shape;
-        shape[0] = f.splat_warps;
-        shape[1] = f.blur_threads;
-        shape[2] = f.slice_tile;
-        shape[3] = f.splat_kind;
+        shape_to(b.terms[k]->lat->shape, shape);
+    });
+}
+
+dcrf_status dcrf_batch_set_filter_shape(dcrf_batch h, int k, const int* shape) {
+    return guard([&] {
+        auto& b = BT(h);
+        dcrf::require(k >= 0 && k < (int)b.terms.size(), DCRF_E_ARG, "pairwise term index out of range");
+        const dcrf::FilterShape f = shape_from(shape);
+        b.ensure_lattices();
+        b.terms[k]->lat->shape = f;
+        b.terms[k]->lat->shape_L = 21;  // pinned: no tuning for this lattice
     });
 }
 

@@ -603,6 +603,152 @@ __global__ void splat_short_kernel(int n_short, int Lrt, const int* __restrict__
     }
 }
 
+// Block-tiled splat for L = 21.  A block takes kTV consecutive lists of the
+// visiting order at a time (a tile) and stages their entries through shared
+// memory in slabs of kSL entries per list, so that hundreds of input rows
+// are in flight per block instead of a few per warp:
+//   1. the slab's (pixel, weight) pairs of the kTV lists (coalesced) and the
+//      next tile's list ranges are loaded one step ahead into registers and
+//      published to shared memory at the start of the step;
+//   2. thread (list g, label k) copies label k of every entry of list g with
+//      cp.async into a [list][entry][label] buffer: the 21 threads of a list
+//      read one entry's 84 contiguous bytes, and the list stride (693
+//      floats, 21 mod 32) makes one warp's writes and reads conflict-free;
+//      the record owners copy the entries' norms beside them;
+//   3. thread (g, k) adds the slab to its running sum in entry order.
+// The per-(vertex, label) chain is the same sequence of float operations as
+// in every other splat form, so the values are bit-identical.  Lists longer
+// than one slab take several slabs with the sum carried in a register; the
+// visiting order puts lists of similar length next to each other.
+constexpr int kTV = 12;           // lists per tile (12 x 21 = 252 worker threads)
+constexpr int kSL = 32;           // entries per list per slab
+constexpr int kTE = kTV * kSL;    // entry slots per slab
+constexpr int kXV = kSL * 21 + 21;  // floats per list in the row buffer (21 mod 32)
+constexpr int kRV = kSL + 1;      // per-list stride of the weight / norm arrays
+constexpr int kTileThreads = 256;
+constexpr int kTileBlocksPerSM = 5;
+template <bool PRE_NORM>
+__global__ void __launch_bounds__(kTileThreads)
+    splat_tile21_kernel(int count, const int* __restrict__ order, const int* __restrict__ seg_start,
+                        const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                        const float* __restrict__ in, const float* __restrict__ norm, float* __restrict__ vals,
+                        Live lv, int Lrow) {
+    constexpr int L = 21;
+    __shared__ __align__(16) float X[kTV * kXV];
+    __shared__ float Ws[kTV * kRV], Ns[kTV * kRV];
+    __shared__ int Ps[kTV * kRV];
+    __shared__ int tv[2][kTV], ts0[2][kTV], tn[2][kTV];
+    const int t = threadIdx.x;
+    const int g = t / L, k = t - g * L;  // worker role (t < kTV * L)
+    const bool worker = t < kTV * L;
+    const long total = live_total(lv, count);
+    const long ntiles = (total + kTV - 1) / kTV;
+    // list range (v, s0, n) of slot t < kTV of a tile
+    auto load_meta = [&](long tile, int& v, int& s0, int& n) {
+        v = -1;
+        s0 = n = 0;
+        const long u = tile * kTV + t;
+        if (tile < ntiles && u < total) {
+            v = order[live_unit(lv, u)];
+            s0 = seg_start[v];
+            n = seg_start[v + 1] - s0;
+        }
+    };
+    // (pixel, weight) of this thread's record slots j = t, t + 256 of slab s
+    // of the tile whose ranges are in buffer b
+    int rp[2] = {0, 0};
+    float rw[2] = {0.0f, 0.0f};
+    auto fetch = [&](int b, int s) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int j = t + h * kTileThreads;
+            rp[h] = -1;
+            if (j < kTE) {
+                const int li = j / kSL, e = s * kSL + (j - li * kSL);
+                if (e < tn[b][li]) {
+                    rp[h] = seg_pix[ts0[b][li] + e];
+                    rw[h] = seg_w[ts0[b][li] + e];
+                }
+            }
+        }
+    };
+    long tile = blockIdx.x;
+    if (tile >= ntiles) return;  // block-uniform
+    int mv = -1, ms0 = 0, mn = 0;
+    if (t < kTV) {
+        load_meta(tile, mv, ms0, mn);
+        tv[0][t] = mv;
+        ts0[0][t] = ms0;
+        tn[0][t] = mn;
+        load_meta(tile + gridDim.x, mv, ms0, mn);  // in flight during the first tile
+    }
+    __syncthreads();
+    fetch(0, 0);
+    for (int it = 0; tile < ntiles; it++, tile += gridDim.x) {  // block-uniform
+        const int b = it & 1;
+        int nmax = 0;
+#pragma unroll
+        for (int i = 0; i < kTV; i++) nmax = max(nmax, tn[b][i]);
+        const int nslab = (nmax + kSL - 1) / kSL;
+        float acc = 0.0f;
+        for (int s = 0; s < nslab; s++) {
+            const bool last = s + 1 == nslab;
+            __syncthreads();  // the previous step's readers of Ps / Ws / Ns / X are done
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int j = t + h * kTileThreads;
+                if (j < kTE && rp[h] >= 0) {
+                    const int li = j / kSL, r = li * kRV + (j - li * kSL);
+                    Ps[r] = rp[h];
+                    Ws[r] = rw[h];
+                    if (PRE_NORM) cp_async4(&Ns[r], norm + rp[h]);
+                }
+            }
+            if (last && t < kTV) {  // the next tile's ranges, loaded during this one
+                tv[b ^ 1][t] = mv;
+                ts0[b ^ 1][t] = ms0;
+                tn[b ^ 1][t] = mn;
+            }
+            __syncthreads();
+            const int n = worker ? min(kSL, tn[b][g] - s * kSL) : 0;
+            if (n > 0) {
+                const float* src = in + k;
+                float* dst = &X[g * kXV + k];
+                const int* pp = &Ps[g * kRV];
+#pragma unroll 4
+                for (int e = 0; e < n; e++) cp_async4(dst + e * L, src + (long)pp[e] * L);
+            }
+            cp_async_commit();
+            // next step's records (and, after this tile, the following tile's
+            // ranges) in flight while this slab lands and is summed
+            if (!last) {
+                fetch(b, s + 1);
+            } else {
+                fetch(b ^ 1, 0);
+                if (t < kTV) load_meta(tile + 2L * gridDim.x, mv, ms0, mn);
+            }
+            cp_async_wait<0>();
+            __syncthreads();
+            if (n > 0) {
+                const float* xs = &X[g * kXV + k];
+                const float* ws = &Ws[g * kRV];
+                const float* ns = &Ns[g * kRV];
+#pragma unroll 4
+                for (int e = 0; e < n; e++) {
+                    float x = xs[e * L];
+                    if (PRE_NORM) x = fmul(x, ns[e]);
+                    acc = fadd(acc, fmul(ws[e], x));
+                }
+            }
+        }
+        if (worker && tv[b][g] >= 0) vals[(long)(tv[b][g] + 1) * Lrow + k] = acc;
+        for (int q = t; q < kTV * (Lrow - L); q += kTileThreads) {  // row padding
+            const int li = q / (Lrow - L);
+            if (tv[b][li] >= 0) vals[(long)(tv[b][li] + 1) * Lrow + L + (q - li * (Lrow - L))] = 0.0f;
+        }
+    }
+}
+
 __global__ void count_long_kernel(int M, const int* __restrict__ counts, int threshold, int* __restrict__ n) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const bool is_long = v < M && counts[v] > threshold;
@@ -1959,6 +2105,32 @@ static void splat_warp_range(const Lattice& lat, int warps, int dom, int first, 
     }
 }
 
+// The tiled splat (L = 21) over order[first, first + count); with live
+// images, over domain `dom`'s live lists.
+static void splat_tile_range(const Lattice& lat, int dom, int first, int count, const float* in,
+                             const float* pre_norm, float* vals, int Lp, cudaStream_t st) {
+    if (count <= 0) return;
+    // 38 KB of static shared memory per block: ask for the largest carveout
+    // so that kTileBlocksPerSM blocks fit on an SM.
+    static const bool carveout = [] {
+        DCRF_CUDA(cudaFuncSetAttribute(splat_tile21_kernel<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+        DCRF_CUDA(cudaFuncSetAttribute(splat_tile21_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+        return true;
+    }();
+    (void)carveout;
+    const Live lv = lat.live_of(dom);
+    const bool live = lv.n != nullptr;
+    const int* order = lat.vorder.get() + (live ? 0 : first);
+    // persistent blocks: each walks its tiles with the next tile's ranges and
+    // records prefetched
+    const int grid = (int)std::min<long>((count + kTV - 1) / kTV, (long)sm_count() * kTileBlocksPerSM);
+    launch(pre_norm ? splat_tile21_kernel<true> : splat_tile21_kernel<false>,
+           grid, kTileThreads, 0, st, count, order, lat.seg_start.get(),
+           lat.seg_pix.get(), lat.seg_w.get(), in, pre_norm, vals, lv, Lp);
+}
+
 namespace {
 constexpr int kTuneMinPixels = 1 << 18;  // smaller lattices keep the default shapes
 std::mutex g_tune_mu;
@@ -2016,9 +2188,9 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
     float* src = va.get();
     float* dst = vb.get();
     float tbest = 1e30f;
-    for (int kind = 0; kind < 3; kind++) {
+    for (int kind = 0; kind < 5; kind++) {
         for (int w : {2, 4, 8}) {
-            if (kind == 0 && w != 4) continue;  // no warp splat in this form
+            if ((kind == 0 || kind >= 3) && w != 4) continue;  // no warp splat in these forms
             FilterShape fs = best;
             fs.splat_kind = kind;
             fs.splat_warps = w;
@@ -2077,6 +2249,26 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
     const int kind = L == 21 ? fs.splat_kind : 0;
     if (kind == 2 && !live) {
         splat_warp_range(*this, fs.splat_warps, kDomLong, nh, M - nh, L, Lp, in, pre_norm, vals, st);
+        return;
+    }
+    if (kind == 3) {  // the tiled splat for every list up to the huge ones
+        if (!live) {
+            splat_tile_range(*this, kDomLong, nh, M - nh, in, pre_norm, vals, Lp, st);
+        } else {
+            splat_tile_range(*this, kDomLong, nh, n_long - nh, in, pre_norm, vals, Lp, st);
+            splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
+        }
+        return;
+    }
+    if (kind == 4) {  // the staged warp splat for the long lists, the tiled splat for the short ones
+        if (n_long > nh) {
+            const Live lv = live ? live_of(kDomLong) : Live{};
+            launch(pre_norm ? splat_kernel<true, 21> : splat_kernel<false, 21>,
+                   unit_grid(n_long - nh, kStageWarps, live, 32 * kStageWarps), 32 * kStageWarps, 0, st, n_long - nh,
+                   L, vorder.get() + (live ? 0 : nh), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals,
+                   lv, Lp);
+        }
+        splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
         return;
     }
     if (n_long > nh) {

@@ -96,7 +96,10 @@ struct FilterShape {
     // 0 = staged splat_kernel for the long lists, one thread per (vertex,
     //     label) for the short ones;
     // 1 = warp splat for the long lists, the thread form for the short ones;
-    // 2 = warp splat for every list.
+    // 2 = warp splat for every list;
+    // 3 = tiled splat (splat_tile21_kernel) for every list;
+    // 4 = staged splat_kernel for the long lists, the tiled splat for the
+    //     short ones.
     int splat_kind = 0;
     int splat_warps = 4;     // vertices (warps) per block of the warp splat: 2, 4 or 8
     int blur_threads = 256;  // threads per block of the float4 blur: 128, 256 or 512

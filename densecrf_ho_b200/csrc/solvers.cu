@@ -157,45 +157,103 @@ struct CliqueView {
 };
 
 // The clique-local prefix chains below walk q = 0 .. max_size-1 with one
-// thread per label; the rows Q[q][*] they read are staged through shared
-// memory kHoChunk at a time by the whole block.
-constexpr int kHoChunk = 128;
+// thread per label; the rows p[q][*] they read are staged through shared
+// memory kHoChunk at a time by the whole block, the next chunk's copies in
+// flight while the current one is summed.
+constexpr int kHoChunk = 64;  // two staging buffers of 64 rows x kLMax labels: 32 KB
 constexpr int kHoThreads = 256;
+
+__device__ __forceinline__ void cp_async4_ca(void* sdst, const void* gsrc) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(sdst)),
+                 "l"(gsrc)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // The clique-local prefix chains of multiplySuperPixels: pre(lab, s) =
 // sum_{q < s} p(lab, q) with p = Q - 1 (or p as given), one sequential chain
-// per label -- in float (FP32 = 1) as the reference sums it, or in FP64 --
-// recorded at every clique size: out[ptr * L + lab] = pre(lab, size of the
-// ptr-th clique in size order).  Rows of p are staged through shared memory
-// kHoChunk at a time; the bucket starts of the chunk too.
-template <bool FP32>
+// per label -- in float as the reference sums it (OUT32) and / or in FP64
+// (OUT64), both from the same staged rows -- recorded at every clique size:
+// out[ptr * L + lab] = pre(lab, size of the ptr-th clique in size order).
+// The chain thread only adds and compares: the next record point is the
+// size of the next clique in size order, so the loads of the staged rows
+// run ahead of the dependent adds.
+template <bool OUT32, bool OUT64>
 __global__ void __launch_bounds__(kHoThreads)
-    ho_prefix_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one,
-                     typename std::conditional<FP32, float, double>::type* __restrict__ out,
-                     const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
-    using T = typename std::conditional<FP32, float, double>::type;
+    ho_prefix_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one, float* __restrict__ out32,
+                     double* __restrict__ out64, const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
     if (sc && skip_on_zero_step && sc->zero_step) return;
-    __shared__ float rows[kHoChunk * kLMax];
-    __shared__ int bs[kHoChunk + 1];
+    __shared__ __align__(16) float rows[2][kHoChunk * kLMax];
     const int lab = threadIdx.x;
-    if (lab < L)
-        for (int ptr = 0; ptr < cv.bstart[1]; ptr++) out[(long)ptr * L + lab] = T(0);  // empty cliques
-    T s = T(0);
-    for (int c0 = 0; c0 < cv.max_size; c0 += kHoChunk) {
-        const int nq = min(kHoChunk, cv.max_size - c0);
-        __syncthreads();
-        for (int e = threadIdx.x; e < nq * L; e += blockDim.x) rows[e] = p[(long)c0 * L + e];
-        for (int e = threadIdx.x; e <= nq; e += blockDim.x) bs[e] = cv.bstart[c0 + 1 + e];
-        __syncthreads();
-        if (lab < L)
-            for (int qq = 0; qq < nq; qq++) {
-                float x = rows[qq * L + lab];
+    const bool chain = lab < L;
+    int ptr = cv.bstart[1];  // cliques of size 0 come first in size order
+    if (chain)
+        for (int r = 0; r < ptr; r++) {
+            if (OUT32) out32[(long)r * L + lab] = 0.0f;
+            if (OUT64) out64[(long)r * L + lab] = 0.0;
+        }
+    int next = ptr < cv.R ? cv.sizes[ptr] : INT_MAX;
+    const int nchunks = (cv.max_size + kHoChunk - 1) / kHoChunk;
+    auto stage = [&](int c) {
+        const int q0 = c * kHoChunk, n = min(kHoChunk, cv.max_size - q0) * L;
+        float* dst = rows[c & 1];
+        const float* src = p + (long)q0 * L;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) cp_async4_ca(dst + e, src + e);
+    };
+    stage(0);
+    cp_async_commit_group();
+    float s32 = 0.0f;
+    double s64 = 0.0;
+    for (int c = 0; c < nchunks; c++) {
+        if (c + 1 < nchunks) stage(c + 1);
+        cp_async_commit_group();
+        cp_async_wait_group<1>();  // chunk c has landed (this thread's copies)
+        __syncthreads();           // ... and everyone's
+        if (chain) {
+            const float* r = rows[c & 1] + lab;
+            const int q0 = c * kHoChunk, nq = min(kHoChunk, cv.max_size - q0);
+            // one element: add, then record at every clique whose size is
+            // the prefix length reached
+            auto step = [&](float x, int len) {
                 if (minus_one) x = fsub(x, 1.0f);
-                if constexpr (FP32) s = fadd(s, x);
-                else s += (double)x;
-                for (int ptr = bs[qq]; ptr < bs[qq + 1]; ptr++) out[(long)ptr * L + lab] = s;
+                if (OUT32) s32 = fadd(s32, x);
+                if (OUT64) s64 += (double)x;
+                while (len == next) {
+                    if (OUT32) out32[(long)ptr * L + lab] = s32;
+                    if (OUT64) out64[(long)ptr * L + lab] = s64;
+                    ptr++;
+                    next = ptr < cv.R ? cv.sizes[ptr] : INT_MAX;
+                }
+            };
+            int qq = 0;
+            // batches of eight: the eight loads first, then the chain; no
+            // record check inside a batch that ends before the next record
+            for (; qq + 8 <= nq; qq += 8) {
+                float x[8];
+#pragma unroll
+                for (int i = 0; i < 8; i++) x[i] = r[(qq + i) * L];
+                if (q0 + qq + 8 < next) {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) {
+                        float xi = x[i];
+                        if (minus_one) xi = fsub(xi, 1.0f);
+                        if (OUT32) s32 = fadd(s32, xi);
+                        if (OUT64) s64 += (double)xi;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; i++) step(x[i], q0 + qq + i + 1);
+                }
             }
+            for (; qq < nq; qq++) step(r[qq * L], q0 + qq + 1);
+        }
+        __syncthreads();  // rows[c & 1] is restaged for chunk c + 2
     }
+    cp_async_wait_group<0>();
 }
 
 // multiplySuperPixels(p [L x N]) with p = Q - 1 (src/densecrf.cpp:81-88): the
@@ -237,7 +295,7 @@ __global__ void ho_direction_kernel(CliqueView cv, int L, const float* __restric
 // sum_r sum_{q < size_r} sum_lab p1(lab, r) p2(lab, q), clique-local q again.
 // Evaluated in FP64 as sum_lab sum_r p1(lab, r) * prefix_lab(size_r), the r
 // in size order, then rounded to float; the FP64 prefixes come from
-// ho_prefix_kernel<false>.  One thread per label; its loads do not depend on
+// ho_prefix_kernel<.., true>.  One thread per label; its loads do not depend on
 // its sum, so they run ahead of it.
 __global__ void ho_scalar_kernel(CliqueView cv, int L, const float* __restrict__ p1, const double* __restrict__ pre,
                                  int slot, SolverScalars* sc, int add_to_slot) {
@@ -1108,7 +1166,8 @@ double Model::energy_qp_ho(const float* Q) {
         launch(clear_step_flags_kernel, 1, 1, 0, stream, sc);
         launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, (const float*)z_last.get(), zc, omz, sc);
         launch(eig_sum_kernel, 1, kHoThreads, 0, stream, (const float*)zc, LR, 8, sc, 2);
-        launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, preQ, nullptr, 0);
+        launch(ho_prefix_kernel<false, true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, (float*)nullptr, preQ,
+               (const SolverScalars*)nullptr, 0);
         launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, (const float*)omz, (const double*)preQ, 8, sc, 1);
     }
     launch(ho_energy_finish_kernel, 1, 1, 0, stream, nt, sc, (int)(R > 0));
@@ -1244,7 +1303,9 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(fill_float_kernel, ceil_div(LR, 256), 256, 0, stream, LR, 1.0f, z);
         ho = buf(4);
         DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
-        launch(ho_prefix_kernel<true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, nullptr, 0);
+        // the float and the FP64 prefixes of Q - 1 in one pass
+        launch(ho_prefix_kernel<true, true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, preQ,
+               (const SolverScalars*)nullptr, 0);
         launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 0, nullptr);
     }
     // grad_y = unary + sum_k 2 A_k Q; energy terms Q . A_k Q (same applies).
@@ -1259,7 +1320,6 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(add_inplace_kernel, ceil_div(NL, 256), 256, 0, stream, NL, grad, ho);
         launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
         launch(eig_sum_kernel, 1, kHoThreads, 0, stream, zc, LR, 8, sc, 2);
-        launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, preQ, nullptr, 0);
         launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, preQ, 8, sc, 1);
     }
     launch(dot_kernel, kRedBlocks, kRedThreads, 0, stream, NL, unary.get(), Q, part);
@@ -1286,7 +1346,8 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         if (R > 0) {
             launch(ho_direction_kernel, 1, 256, 0, stream, cv, L, gz, z, sxz, t1, t2, cz, sc);
             launch(eig_sum_kernel, 1, kHoThreads, 0, stream, sxz, LR, 5, sc, 0);
-            launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, sx, 0, preS, sc, 0);
+            launch(ho_prefix_kernel<false, true>, 1, kHoThreads, 0, stream, cv, L, sx, 0, (float*)nullptr, preS,
+                   (const SolverScalars*)sc, 0);
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preQ, 3, sc, 0);    // a
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t2, preS, 4, sc, 0);   // b
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preS, 6, sc, 0);   // denom term
@@ -1302,11 +1363,13 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(qp_update_kernel, kRedBlocks, kRedThreads, 0, stream, NL, sx, psi, ho, unary.get(), Q, grad, sc, part);
         launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 7, sc);
         if (R > 0) {
-            launch(ho_prefix_kernel<true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, sc, 1);
+            // both prefixes of the updated Q - 1 in one pass (after a zero
+            // step Q is unchanged, so recomputing the float one is exact)
+            launch(ho_prefix_kernel<true, true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, preQ,
+                   (const SolverScalars*)nullptr, 0);
             launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 1, sc);
             launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
             launch(eig_sum_kernel, 1, kHoThreads, 0, stream, zc, LR, 8, sc, 2);
-            launch(ho_prefix_kernel<false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, preQ, nullptr, 0);
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, omz, preQ, 8, sc, 1);
         }
         launch(qp_energy_kernel, 1, 1, 0, stream, sc, max_iter);

@@ -131,6 +131,15 @@ dcrf_status dcrf_lattice_export(dcrf_lattice lat, int32_t* offset, int32_t* rank
                                 int16_t* keys, int32_t* nbr);
 /* The stream the lattice's work is queued on (a cudaStream_t). */
 dcrf_status dcrf_lattice_stream(dcrf_lattice lat, void** stream);
+/* Launch shapes of the 21-label plain filter (shape[4]: splat warps per
+ * block in {2,4,8}, blur threads per block in {128,256,512}, slice pixels
+ * per tile in {64,128,256}, splat form 0..4 as dcrf_batch_filter_shape
+ * lists them).  The autotuner sets them on the first 21-label filter call of
+ * a lattice of 2^18 pixels or more; set_filter_shape pins a shape instead
+ * (that lattice is then never tuned).  Every shape computes bit-identical
+ * values.  No counterpart in the reference. */
+dcrf_status dcrf_lattice_filter_shape(dcrf_lattice lat, int* shape);
+dcrf_status dcrf_lattice_set_filter_shape(dcrf_lattice lat, const int* shape);
 
 /* ------------------------------------------------------------------------
  * Dense CRF model -- class DenseCRF / DenseCRF2D (include/densecrf.h:73-194)
@@ -421,9 +430,12 @@ dcrf_status dcrf_batch_pairwise_apply_dev(dcrf_batch b, int k, float* d_out, con
  * (shape[0] warp-splat vertices per block, [1] blur threads per block, [2]
  * slice pixels per block, [3] splat form: 0 staged long lists + thread-per-
  * label short lists, 1 warp splat for the long lists, 2 warp splat for
- * every list); the defaults until a filter call of 2^18 pixels or more has
+ * every list, 3 tiled splat for every list, 4 staged long lists + tiled
+ * short lists); the defaults until a filter call of 2^18 pixels or more has
  * tuned them.  shape holds 4 ints.  No counterpart in the reference. */
 dcrf_status dcrf_batch_filter_shape(dcrf_batch b, int k, int* shape);
+/* Pins term k's launch shapes (as dcrf_lattice_set_filter_shape). */
+dcrf_status dcrf_batch_set_filter_shape(dcrf_batch b, int k, const int* shape);
 /* Vertex count of term k's concatenated lattice (the sum of the images' M). */
 dcrf_status dcrf_batch_lattice_size(dcrf_batch b, int k, int64_t* M);
 

@@ -120,3 +120,26 @@ def test_batch_pairwise_apply_equals_single_applies():
             assert np.array_equal(b.split(out)[i], m.pairwise_apply(k, b.split(x)[i])), (k, i)
             Ms += m.lattice_size(k)
         assert b.lattice_size(k) == Ms
+
+
+@pytest.mark.parametrize("kind", [0, 2, 3, 4])
+def test_batch_splat_forms_equal_single_solves(kind):
+    """The batched QP (live-image compaction) and the batched apply with each
+    splat form pinned on both terms' concatenated lattices: outputs, steps
+    and energies equal the single-image solves and applies, bit for bit."""
+    imgs = _images(SIZES, 60)
+    b = _batch(SIZES, imgs)
+    for k in range(2):
+        b.set_filter_shape(k, (4, 256, 128, kind))
+    q0 = b.unary_init()
+    out, st = b.qp_inference_super_pixels_non_convex(q0, max_iter=9, stats=True)
+    x = np.random.default_rng(9).random((b.N, 21)).astype(np.float32)
+    applied = [b.pairwise_apply(k, x) for k in range(2)]
+    for i, ((w, h), im) in enumerate(zip(SIZES, imgs)):
+        m = _single(w, h, im)
+        o, s = m.qp_inference_super_pixels_non_convex(b.split(q0)[i], max_iter=9, stats=True)
+        assert np.array_equal(b.split(out)[i], o), i
+        assert st[i].iterations == s.iterations and st[i].energy == s.energy
+        for k in range(2):
+            assert np.array_equal(b.split(applied[k])[i], m.pairwise_apply(k, b.split(x)[i])), (k, i)
+    assert b.filter_shape(0) == (4, 256, 128, kind)

@@ -109,6 +109,29 @@ def test_ordered_filter_huge_lists(L, oracle_mod):
     assert _eq(lat.compute(x), orc.compute(x))
 
 
+# Every launch shape the autotuner can choose for the 21-label plain filter:
+# (splat warps per block, blur threads, slice pixels per tile, splat form).
+FILTER_SHAPES = [(4, 256, 128, 0), (2, 128, 64, 1), (8, 512, 256, 1), (2, 256, 128, 2), (8, 128, 64, 2),
+                 (4, 512, 256, 3), (4, 128, 128, 4)]
+
+
+@pytest.mark.parametrize("shape", FILTER_SHAPES)
+def test_filter_every_launch_shape_bit_exact(shape, oracle_mod):
+    """Each pinned shape on lattices with short (<= 64 entries), long and
+    huge (> 1024) splat lists, both blur orders: bit-equal to the oracle."""
+    W, H = 160, 120
+    img = synth.make_image(W, H, 21, 5)
+    feats = (synth.gaussian_features(W, H, 3, 3),
+             synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"]),
+             synth.bilateral_features(W, H, 300, 300, 60, 60, 60, img["rgb"]))
+    x = np.random.default_rng(17).standard_normal((W * H, 21)).astype(np.float32)
+    for f in feats:
+        lat, orc = Permutohedral().init(f).set_filter_shape(shape), oracle_mod.OracleLattice(f)
+        assert lat.filter_shape() == tuple(shape)
+        assert _eq(lat.compute(x), orc.compute(x))
+        assert _eq(lat.compute(x, reverse=True), orc.compute(x, True))
+
+
 def test_filter_error_vs_fp64_oracle(oracle_mod):
     """Relative error of the FP32 filter against the FP64 lattice oracle."""
     W, H = 160, 120
