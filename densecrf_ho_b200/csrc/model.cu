@@ -563,6 +563,23 @@ void Model::set_cliques(int R_, const int* off, const int* idx, const float* exp
     int* didx = cl_idx.ensure(std::max(clique_total, 1));
     if (clique_total)
         DCRF_CUDA(cudaMemcpyAsync(didx, idx, sizeof(int) * clique_total, cudaMemcpyHostToDevice, stream));
+    // the chunked clique kernels' units: chunks of kCliqueChunk pixels per clique, L units each
+    {
+        std::vector<int2> ch;
+        std::vector<int> ub((size_t)R + 1, 0);
+        for (int r = 0; r < R; r++) {
+            const int nch = (off[r + 1] - off[r] + kCliqueChunk - 1) / kCliqueChunk;
+            for (int c = 0; c < nch; c++) ch.push_back(make_int2(r, c));
+            ub[r + 1] = ub[r] + L * nch;
+        }
+        uc_nchunks = (int)ch.size();
+        uc_units = ub[R];
+        int2* dch = uc_chunks.ensure(std::max<size_t>(ch.size(), 1));
+        if (!ch.empty())
+            DCRF_CUDA(cudaMemcpyAsync(dch, ch.data(), sizeof(int2) * ch.size(), cudaMemcpyHostToDevice, stream));
+        int* dub = uc_base.ensure(ub.size());
+        DCRF_CUDA(cudaMemcpyAsync(dub, ub.data(), sizeof(int) * ub.size(), cudaMemcpyHostToDevice, stream));
+    }
     float* de = cl_exp.ensure(std::max(R, 1));
     float* dc = cl_const.ensure(std::max(R, 1));
     if (R) {
@@ -867,7 +884,12 @@ double Model::energy_lp(const float* Q) {
     }
     if (R > 0) {
         float* diffs = b[13].ensure(std::max(R, 1));
-        launch(clique_maxdiff_kernel, R, 256, 0, stream, cl_off.get(), cl_idx.get(), L, Q, diffs);
+        float2* part = reinterpret_cast<float2*>(uc_scan.ensure(std::max<size_t>(3 * (size_t)uc_units, 1)));
+        if (uc_nchunks > 0)
+            launch(clique_maxdiff_chunk_kernel, uc_nchunks, 256, 0, stream, uc_chunks.get(), cl_off.get(),
+                   cl_idx.get(), uc_base.get(), L, Q, part);
+        launch(clique_maxdiff_finish_kernel, R, 64, 0, stream, cl_off.get(), uc_base.get(), L, (const float2*)part,
+               diffs);
     }
     launch(energy_lp_finish_kernel, 1, 1, 0, stream, (int)terms.size(), R, b[13].get(), cl_exp.get(), scal.get());
     DCRF_LAUNCH_CHECK();

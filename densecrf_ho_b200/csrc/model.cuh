@@ -69,6 +69,10 @@ struct SolverScalars {
 constexpr int kQpChunk = 64;  // QP iterations per graph launch at most
 constexpr int kSplitMaxPixels = 1 << 17;  // apply_sum runs the terms' filters concurrently up to this size
 
+// Pixels per chunk of the chunked clique kernels (computeUCondGrad, the LP
+// clique energy): a clique of n pixels has ceil(n / kCliqueChunk) chunks.
+constexpr int kCliqueChunk = 128;
+
 struct Model {
     int W = 0, H = 0, N = 0, L = 0, device = 0;
     cudaStream_t stream = nullptr;
@@ -117,6 +121,13 @@ struct Model {
     // the last QP (DCRF_E_STATE with cliques and no QP since they were set).
     double energy_qp_ho(const float* Q);
     DevBuf<int> lp_win;  // lp_sp: per element, the latest clique write claiming it (-1 between calls)
+    // lp_sp: computeUCondGrad's units (clique r, label, chunk c of kCliqueChunk pixels):
+    // the (r, c) of every chunk, each clique's first unit, and per unit the
+    // (min, max) partials, carries and selected positions
+    DevBuf<int2> uc_chunks;
+    DevBuf<int> uc_base;
+    DevBuf<int2> uc_scan;  // [3][uc_units]
+    int uc_nchunks = 0, uc_units = 0;
     SolverScalars* h_scal = nullptr;  // pinned mirror
 
     Model(int W_, int H_, int L_);

@@ -376,41 +376,62 @@ __global__ void energy_ho_finish_kernel(int R, const int* __restrict__ flags, co
 }
 
 // Per clique: max over labels of (max - min of Q over the clique's pixels)
-// (src/densecrf.cpp:1020-1034).
-__global__ void clique_maxdiff_kernel(const int* __restrict__ off, const int* __restrict__ idx, int L,
-                                      const float* __restrict__ Q, float* __restrict__ diffs) {
-    const int r = blockIdx.x;
-    const int s0 = off[r], s1 = off[r + 1];
-    __shared__ float smx[32], smn[32];
-    float best = 0.0f;
-    for (int lab = 0; lab < L; lab++) {
-        float mx = -INFINITY, mn = INFINITY;
-        for (int p = s0 + threadIdx.x; p < s1; p += blockDim.x) {
-            const float q = Q[(long)idx[p] * L + lab];
+// (src/densecrf.cpp:1020-1034).  The per-label max / min do not depend on
+// the order of the pixels, so they are taken per chunk of kCliqueChunk
+// pixels (one block per chunk, coalesced reads of the pixels' rows, all SMs
+// busy however uneven the clique sizes) and then over each clique's chunks;
+// the max over labels runs in label order as Eigen's maxCoeff does.
+__global__ void __launch_bounds__(256)
+    clique_maxdiff_chunk_kernel(const int2* __restrict__ chunks, const int* __restrict__ off,
+                                const int* __restrict__ idx, const int* __restrict__ ubase, int L,
+                                const float* __restrict__ Q, float2* __restrict__ part) {
+    __shared__ float smx[256], smn[256];
+    const int2 rc = chunks[blockIdx.x];
+    const int r = rc.x, c = rc.y, t = threadIdx.x;
+    const int s0 = off[r], sz = off[r + 1] - s0, nch = (sz + kCliqueChunk - 1) / kCliqueChunk;
+    const int j0 = c * kCliqueChunk, n = min(kCliqueChunk, sz - j0);
+    const int G = blockDim.x / L;  // pixel groups; thread (g, lab) keeps one label
+    const int g = t / L, lab = t - g * L;
+    float mx = -INFINITY, mn = INFINITY;
+    if (g < G)
+        for (int j = g; j < n; j += G) {
+            const float q = Q[(long)idx[s0 + j0 + j] * L + lab];
             mx = fmaxf(mx, q);
             mn = fminf(mn, q);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            mx = fmaxf(mx, __shfl_down_sync(kFullMask, mx, o));
-            mn = fminf(mn, __shfl_down_sync(kFullMask, mn, o));
+    smx[t] = mx;
+    smn[t] = mn;
+    __syncthreads();
+    if (t < L) {
+        for (int gg = 1; gg < G; gg++) {
+            mx = fmaxf(mx, smx[gg * L + t]);
+            mn = fminf(mn, smn[gg * L + t]);
         }
-        if ((threadIdx.x & 31) == 0) {
-            smx[threadIdx.x >> 5] = mx;
-            smn[threadIdx.x >> 5] = mn;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 1; w < (int)(blockDim.x >> 5); w++) {
-                mx = fmaxf(mx, smx[w]);
-                mn = fminf(mn, smn[w]);
-            }
-            const float diff = fsub(mx, mn);
-            if (lab == 0 || diff > best) best = diff;
-        }
-        __syncthreads();
+        part[ubase[r] + t * nch + c] = make_float2(mx, mn);
     }
-    if (threadIdx.x == 0) diffs[r] = best;
+}
+
+__global__ void clique_maxdiff_finish_kernel(const int* __restrict__ off, const int* __restrict__ ubase, int L,
+                                             const float2* __restrict__ part, float* __restrict__ diffs) {
+    __shared__ float sd[kLMax];
+    const int r = blockIdx.x, t = threadIdx.x;
+    const int sz = off[r + 1] - off[r], nch = (sz + kCliqueChunk - 1) / kCliqueChunk;
+    if (t < L) {
+        float mx = -INFINITY, mn = INFINITY;
+        for (int c = 0; c < nch; c++) {
+            const float2 v = part[ubase[r] + t * nch + c];
+            mx = fmaxf(mx, v.x);
+            mn = fminf(mn, v.y);
+        }
+        sd[t] = fsub(mx, mn);
+    }
+    __syncthreads();
+    if (t == 0) {
+        float best = 0.0f;
+        for (int lab = 0; lab < L; lab++)
+            if (lab == 0 || sd[lab] > best) best = sd[lab];
+        diffs[r] = best;
+    }
 }
 
 __global__ void energy_lp_finish_kernel(int nterms, int R, const float* __restrict__ diffs,

@@ -964,90 +964,192 @@ __device__ __forceinline__ int trunc_x86(float q) {
     return fabsf(q) < 2147483648.0f ? (int)q : INT_MIN;
 }
 
-// computeUCondGrad (src/densecrf.cpp:803-830) for clique r = blockIdx.x.
+// computeUCondGrad (src/densecrf.cpp:803-830): the positions it selects.
 // The reference keeps its running min / max in an int, so position p (in
 // label-major, clique order: p = lab * size + j) updates the min iff
 // Q_p < (float)s, where s is the running min of trunc(Q) over the positions
 // before p (it starts at INT_MAX); the LAST such p is selected.  Same for the
-// max.  Each thread takes a contiguous run of positions: pass 1 finds its
-// run's min / max of trunc(Q), one block-wide exclusive scan gives every run
-// its carry-in, and pass 2 replays the run from that carry exactly as the
-// reference's loop does.
-constexpr int kUcondThreads = 1024;
+// max.  A min / max over the positions before p does not depend on their
+// order, so the scan splits into units (clique r, label lab, chunk c of
+// kUcChunk pixels), ordered by (lab, c) within a clique:
+//   ucond_minmax_kernel   per (r, c): the min / max of trunc(Q) of each
+//                         label's unit (coalesced reads of the pixels' rows);
+//   ucond_carry_kernel    per clique: exclusive scan of the units -> carry-in;
+//   ucond_select_kernel   per (r, c), a warp per label: its lanes replay runs
+//                         of the unit from the carry (a warp scan gives each
+//                         run its own) exactly as the reference's loop, and
+//                         the unit's last selected positions are kept;
+//   ucond_pos_kernel      per clique: the last over its units.
+// Work is spread over all SMs however uneven the clique sizes are.
+constexpr int kUcChunk = kCliqueChunk;  // pixels per unit (4 per lane of a warp)
 
-__global__ void __launch_bounds__(kUcondThreads)
-    ucond_kernel(const int* __restrict__ off, const int* __restrict__ idx, int L, const float* __restrict__ Q,
-                 int* __restrict__ pos) {
-    __shared__ int smin[kUcondThreads / 32], smax[kUcondThreads / 32];
-    const int r = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const int s0 = off[r], sz = off[r + 1] - s0;
-    const long n = (long)L * sz;
-    const long per = (n + kUcondThreads - 1) / kUcondThreads;
-    const long p0 = min((long)t * per, n), p1 = min(p0 + per, n);
-    auto q_at = [&](long p) {
-        const int lab = (int)(p / sz), j = (int)(p - (long)lab * sz);
-        return Q[(long)idx[s0 + j] * L + lab];
-    };
-    int tmin = INT_MAX, tmax = INT_MIN;
-    for (long p = p0; p < p1; p++) {
-        const int v = trunc_x86(q_at(p));
-        tmin = min(tmin, v);
-        tmax = max(tmax, v);
+__global__ void __launch_bounds__(256)
+    ucond_minmax_kernel(const int2* __restrict__ chunks, const int* __restrict__ off, const int* __restrict__ idx,
+                        const int* __restrict__ ubase, int L, const float* __restrict__ Q, int2* __restrict__ part) {
+    __shared__ int smn[kLMax], smx[kLMax];
+    const int2 rc = chunks[blockIdx.x];
+    const int r = rc.x, c = rc.y, t = threadIdx.x;
+    const int s0 = off[r], sz = off[r + 1] - s0, nch = (sz + kUcChunk - 1) / kUcChunk;
+    const int j0 = c * kUcChunk, n = min(kUcChunk, sz - j0);
+    if (t < L) {
+        smn[t] = INT_MAX;
+        smx[t] = INT_MIN;
     }
-    // exclusive scan of (min, max) over the threads' runs, in thread order
-    int xmin = tmin, xmax = tmax;
+    __syncthreads();
+    const int G = blockDim.x / L;  // pixel groups; thread (g, lab) keeps one label
+    const int g = t / L, lab = t - g * L;
+    if (g < G) {
+        int mn = INT_MAX, mx = INT_MIN;
+        for (int j = g; j < n; j += G) {
+            const int v = trunc_x86(Q[(long)idx[s0 + j0 + j] * L + lab]);
+            mn = min(mn, v);
+            mx = max(mx, v);
+        }
+        atomicMin(&smn[lab], mn);
+        atomicMax(&smx[lab], mx);
+    }
+    __syncthreads();
+    if (t < L) part[ubase[r] + t * nch + c] = make_int2(smn[t], smx[t]);
+}
+
+__global__ void __launch_bounds__(1024)
+    ucond_carry_kernel(const int* __restrict__ off, const int* __restrict__ ubase, int L,
+                       const int2* __restrict__ part, int2* __restrict__ carry) {
+    __shared__ int wmn[32], wmx[32];
+    __shared__ int tmn, tmx;
+    const int r = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int sz = off[r + 1] - off[r], units = L * ((sz + kUcChunk - 1) / kUcChunk), base = ubase[r];
+    if (t == 0) {
+        tmn = INT_MAX;
+        tmx = INT_MIN;
+    }
+    for (int u0 = 0; u0 < units; u0 += blockDim.x) {  // block-uniform
+        __syncthreads();
+        const int u = u0 + t;
+        const int2 v = u < units ? part[base + u] : make_int2(INT_MAX, INT_MIN);
+        int xmn = v.x, xmx = v.y;  // inclusive warp scan
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int ymin = __shfl_up_sync(kFullMask, xmin, o), ymax = __shfl_up_sync(kFullMask, xmax, o);
-        if (lane >= o) {
-            xmin = min(xmin, ymin);
-            xmax = max(xmax, ymax);
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ymn = __shfl_up_sync(kFullMask, xmn, o), ymx = __shfl_up_sync(kFullMask, xmx, o);
+            if (lane >= o) {
+                xmn = min(xmn, ymn);
+                xmx = max(xmx, ymx);
+            }
+        }
+        if (lane == 31) {
+            wmn[w] = xmn;
+            wmx[w] = xmx;
+        }
+        __syncthreads();
+        int emn = tmn, emx = tmx;  // carry of the tiles before, then of the warps before
+        for (int ww = 0; ww < w; ww++) {
+            emn = min(emn, wmn[ww]);
+            emx = max(emx, wmx[ww]);
+        }
+        int pmn = __shfl_up_sync(kFullMask, xmn, 1), pmx = __shfl_up_sync(kFullMask, xmx, 1);
+        if (lane > 0) {
+            emn = min(emn, pmn);
+            emx = max(emx, pmx);
+        }
+        if (u < units) carry[base + u] = make_int2(emn, emx);
+        __syncthreads();
+        if (t == blockDim.x - 1) {  // the tile's total joins the running carry
+            tmn = min(emn, xmn);
+            tmx = max(emx, xmx);
         }
     }
-    int emin = __shfl_up_sync(kFullMask, xmin, 1), emax = __shfl_up_sync(kFullMask, xmax, 1);
-    if (lane == 0) {
-        emin = INT_MAX;
-        emax = INT_MIN;
+}
+
+__global__ void __launch_bounds__(256)
+    ucond_select_kernel(const int2* __restrict__ chunks, const int* __restrict__ off, const int* __restrict__ idx,
+                        const int* __restrict__ ubase, int L, const float* __restrict__ Q,
+                        const int2* __restrict__ carry, int2* __restrict__ cand) {
+    constexpr int kRun = kUcChunk / 32;
+    const int2 rc = chunks[blockIdx.x];
+    const int r = rc.x, c = rc.y, lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int s0 = off[r], sz = off[r + 1] - s0, nch = (sz + kUcChunk - 1) / kUcChunk;
+    const int j0 = c * kUcChunk, n = min(kUcChunk, sz - j0);
+    const int a = min(lane * kRun, n), b = min(a + kRun, n);  // this lane's run of the unit
+    for (int lab = w; lab < L; lab += nw) {  // warp-uniform
+        float q[kRun];
+        int mn = INT_MAX, mx = INT_MIN;
+#pragma unroll
+        for (int i = 0; i < kRun; i++) {
+            q[i] = a + i < b ? Q[(long)idx[s0 + j0 + a + i] * L + lab] : 0.0f;
+            if (a + i < b) {
+                const int v = trunc_x86(q[i]);
+                mn = min(mn, v);
+                mx = max(mx, v);
+            }
+        }
+        int xmn = mn, xmx = mx;  // inclusive warp scan of the runs
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int ymn = __shfl_up_sync(kFullMask, xmn, o), ymx = __shfl_up_sync(kFullMask, xmx, o);
+            if (lane >= o) {
+                xmn = min(xmn, ymn);
+                xmx = max(xmx, ymx);
+            }
+        }
+        const int2 cin = carry[ubase[r] + lab * nch + c];
+        int emn = cin.x, emx = cin.y;
+        const int pmn = __shfl_up_sync(kFullMask, xmn, 1), pmx = __shfl_up_sync(kFullMask, xmx, 1);
+        if (lane > 0) {
+            emn = min(emn, pmn);
+            emx = max(emx, pmx);
+        }
+        int cmn = -1, cmx = -1;
+#pragma unroll
+        for (int i = 0; i < kRun; i++) {
+            if (a + i < b) {
+                const int p = lab * sz + j0 + a + i;
+                if (q[i] < (float)emn) cmn = p;
+                if (q[i] > (float)emx) cmx = p;
+                const int v = trunc_x86(q[i]);
+                emn = min(emn, v);
+                emx = max(emx, v);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            cmn = max(cmn, __shfl_down_sync(kFullMask, cmn, o));
+            cmx = max(cmx, __shfl_down_sync(kFullMask, cmx, o));
+        }
+        if (lane == 0) cand[ubase[r] + lab * nch + c] = make_int2(cmn, cmx);
     }
-    if (lane == 31) {
-        smin[w] = xmin;
-        smax[w] = xmax;
+}
+
+__global__ void __launch_bounds__(256)
+    ucond_pos_kernel(const int* __restrict__ off, const int* __restrict__ idx, const int* __restrict__ ubase, int L,
+                     const int2* __restrict__ cand, int* __restrict__ pos) {
+    __shared__ int smn[8], smx[8];
+    const int r = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int s0 = off[r], sz = off[r + 1] - s0, units = L * ((sz + kUcChunk - 1) / kUcChunk), base = ubase[r];
+    int cmn = -1, cmx = -1;
+    for (int u = t; u < units; u += blockDim.x) {
+        const int2 v = cand[base + u];
+        cmn = max(cmn, v.x);
+        cmx = max(cmx, v.y);
     }
-    __syncthreads();
-    for (int ww = 0; ww < w; ww++) {
-        emin = min(emin, smin[ww]);
-        emax = max(emax, smax[ww]);
-    }
-    int cmin = -1, cmax = -1;
-    for (long p = p0; p < p1; p++) {
-        const float q = q_at(p);
-        if (q < (float)emin) cmin = (int)p;
-        if (q > (float)emax) cmax = (int)p;
-        const int v = trunc_x86(q);
-        emin = min(emin, v);
-        emax = max(emax, v);
-    }
-    // the last selected position: block max
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
-        cmin = max(cmin, __shfl_down_sync(kFullMask, cmin, o));
-        cmax = max(cmax, __shfl_down_sync(kFullMask, cmax, o));
+        cmn = max(cmn, __shfl_down_sync(kFullMask, cmn, o));
+        cmx = max(cmx, __shfl_down_sync(kFullMask, cmx, o));
     }
-    __syncthreads();
     if (lane == 0) {
-        smin[w] = cmin;
-        smax[w] = cmax;
+        smn[w] = cmn;
+        smx[w] = cmx;
     }
     __syncthreads();
     if (t == 0) {
-        int lmin = -1, lmax = -1;
-        for (int ww = 0; ww < kUcondThreads / 32; ww++) {
-            lmin = max(lmin, smin[ww]);
-            lmax = max(lmax, smax[ww]);
+        int lmn = -1, lmx = -1;
+        for (int ww = 0; ww < (int)(blockDim.x >> 5); ww++) {
+            lmn = max(lmn, smn[ww]);
+            lmx = max(lmx, smx[ww]);
         }
         // element index pixel*L + label, or -1 when nothing was selected
-        pos[2 * r] = lmin < 0 ? -1 : idx[s0 + lmin % sz] * L + lmin / sz;
-        pos[2 * r + 1] = lmax < 0 ? -1 : idx[s0 + lmax % sz] * L + lmax / sz;
+        pos[2 * r] = lmn < 0 ? -1 : idx[s0 + lmn % sz] * L + lmn / sz;
+        pos[2 * r + 1] = lmx < 0 ? -1 : idx[s0 + lmx % sz] * L + lmx / sz;
     }
 }
 
@@ -1537,7 +1639,17 @@ int Model::lp(const float* init, float* out, const dcrf_lp_params& p, dcrf_solve
             const int nw = 2 * R;
             int* tgt = upos + 2 * R;
             DCRF_CUDA(cudaMemsetAsync(su, 0, sizeof(float) * NL, stream));
-            launch(ucond_kernel, R, kUcondThreads, 0, stream, cl_off.get(), cl_idx.get(), L, Q, upos);
+            int2* ucp = uc_scan.ensure(std::max<size_t>(3 * (size_t)uc_units, 1));
+            if (uc_nchunks > 0) {
+                launch(ucond_minmax_kernel, uc_nchunks, 256, 0, stream, uc_chunks.get(), cl_off.get(), cl_idx.get(),
+                       uc_base.get(), L, Q, ucp);
+                launch(ucond_carry_kernel, R, 1024, 0, stream, cl_off.get(), uc_base.get(), L, (const int2*)ucp,
+                       ucp + uc_units);
+                launch(ucond_select_kernel, uc_nchunks, 256, 0, stream, uc_chunks.get(), cl_off.get(), cl_idx.get(),
+                       uc_base.get(), L, Q, (const int2*)(ucp + uc_units), ucp + 2 * (size_t)uc_units);
+            }
+            launch(ucond_pos_kernel, R, 256, 0, stream, cl_off.get(), cl_idx.get(), uc_base.get(), L,
+                   (const int2*)(ucp + 2 * (size_t)uc_units), upos);
             launch(ucond_targets_kernel, 1, 1024, 0, stream, R, upos, tgt);
             launch(ucond_claim_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, lp_win.get());
             launch(ucond_write_kernel, ceil_div(nw, 256), 256, 0, stream, nw, tgt, cl_const.get(), cl_exp.get(),
