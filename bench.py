@@ -680,7 +680,7 @@ def measure_batch_filter(n=64, reps=10):
                      "gpix_label_s": N * L / t / 1e9,
                      "launches_per_call": int((Ls.dcrf_kernel_launches() - l0) // reps),
                      "tuned_shape": {"splat_form": ("staged", "warp_long", "warp_all", "tiled_all",
-                                                    "staged_long_tiled_short")[shp[3]],
+                                                    "staged_long_tiled_short", "bulk_all")[shp[3]],
                                      "splat_vertices_per_block": shp[0], "blur_threads": shp[1],
                                      "slice_pixels_per_block": shp[2]}}
     return out

@@ -328,9 +328,9 @@ dcrf::FilterShape shape_from(const int* shape) {
     need(shape, "shape");
     const int w = shape[0], bt = shape[1], tile = shape[2], kind = shape[3];
     dcrf::require((w == 2 || w == 4 || w == 8) && (bt == 128 || bt == 256 || bt == 512) &&
-                      (tile == 64 || tile == 128 || tile == 256) && kind >= 0 && kind <= 4,
+                      (tile == 64 || tile == 128 || tile == 256) && kind >= 0 && kind <= 5,
                   DCRF_E_ARG, "filter shape: warps in {2,4,8}, blur threads in {128,256,512}, "
-                              "slice tile in {64,128,256}, splat form in 0..4");
+                              "slice tile in {64,128,256}, splat form in 0..5");
     dcrf::FilterShape f;
     f.splat_warps = w;
     f.blur_threads = bt;
@@ -346,6 +346,13 @@ void shape_to(const dcrf::FilterShape& f, int* shape) {
     shape[3] = f.splat_kind;
 }
 }  // namespace
+
+dcrf_status dcrf_device_wait_timeouts(unsigned long long* count) {
+    return guard([&] {
+        need(count, "count");
+        *count = dcrf::bulk_wait_timeouts();
+    });
+}
 
 dcrf_status dcrf_lattice_filter_shape(dcrf_lattice h, int* shape) {
     return guard([&] {

@@ -749,6 +749,232 @@ __global__ void __launch_bounds__(kTileThreads)
     }
 }
 
+// ------------------------------------------------- bulk-copy (TMA) splat --
+// 1-D bulk copies (cp.async.bulk, the TMA engine; this GPU's own memory, no
+// multicast) complete on a shared-memory mbarrier.  Waits are bounded: a
+// wait that runs out counts itself in g_bulk_wait_timeouts and the filter's
+// output rows of that tile are written as NaN, so a result never silently
+// uses unfinished copies.
+__device__ unsigned long long g_bulk_wait_timeouts = 0;
+constexpr long kBulkWaitLimit = 1L << 24;  // try_wait polls (each suspends briefly): seconds
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase with the given parity; false if the wait ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (long it = 0; it < kBulkWaitLimit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void* sdst, const void* gsrc, unsigned bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+            smem_addr(sdst)),
+        "l"(gsrc), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// Splat for L = 21 whose input rows arrive by bulk copy.  The structure is
+// splat_tile21_kernel's (tiles of kTV lists, slabs of kSL entries, the next
+// tile's ranges and records prefetched), but the rows of a slab are fetched
+// per run of consecutive pixels in a list: one cp.async.bulk of the run's
+// 16-byte-aligned byte span (at most 96 bytes per entry) into a packed
+// shared-memory buffer, issued by the run's first entry.  The rows then
+// never pass through the L1 load pipeline, which bounds the other forms.
+// Each entry records where its row starts in the buffer.  A run whose
+// aligned span would end past the input (the last pixel, when 84 N is not a
+// multiple of 16) is copied with plain loads instead.  `in` must be 16-byte
+// aligned (the host checks it and uses another form otherwise).
+constexpr int kBulkFloats = kTE * 24;  // 96 bytes per entry slot at most
+constexpr int kBulkBlocksPerSM = 4;
+template <bool PRE_NORM>
+__global__ void __launch_bounds__(kTileThreads, kBulkBlocksPerSM)
+    splat_bulk21_kernel(int count, const int* __restrict__ order, const int* __restrict__ seg_start,
+                        const int* __restrict__ seg_pix, const float* __restrict__ seg_w,
+                        const float* __restrict__ in, int N, const float* __restrict__ norm,
+                        float* __restrict__ vals, Live lv, int Lrow) {
+    constexpr int L = 21;
+    __shared__ __align__(128) float X[kBulkFloats];
+    __shared__ float Ws[kTV * kRV], Ns[kTV * kRV];
+    __shared__ int Ps[kTV * kRV], Os[kTV * kRV];
+    __shared__ int tv[2][kTV], ts0[2][kTV], tn[2][kTV];
+    __shared__ unsigned s_space, s_tx;
+    __shared__ int s_timeout;
+    __shared__ __align__(8) unsigned long long bar;
+    const int t = threadIdx.x;
+    const int g = t / L, k = t - g * L;  // worker role (t < kTV * L)
+    const bool worker = t < kTV * L;
+    const long total = live_total(lv, count);
+    const long ntiles = (total + kTV - 1) / kTV;
+    const char* in_b = reinterpret_cast<const char*>(in);
+    const char* in_end = in_b + (size_t)N * L * sizeof(float);
+    auto load_meta = [&](long tile, int& v, int& s0, int& n) {
+        v = -1;
+        s0 = n = 0;
+        const long u = tile * kTV + t;
+        if (tile < ntiles && u < total) {
+            v = order[live_unit(lv, u)];
+            s0 = seg_start[v];
+            n = seg_start[v + 1] - s0;
+        }
+    };
+    int rp[2] = {0, 0};
+    float rw[2] = {0.0f, 0.0f};
+    auto fetch = [&](int b, int s) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const int j = t + h * kTileThreads;
+            rp[h] = -1;
+            if (j < kTE) {
+                const int li = j / kSL, e = s * kSL + (j - li * kSL);
+                if (e < tn[b][li]) {
+                    rp[h] = seg_pix[ts0[b][li] + e];
+                    rw[h] = seg_w[ts0[b][li] + e];
+                }
+            }
+        }
+    };
+    long tile = blockIdx.x;
+    if (tile >= ntiles) return;  // block-uniform
+    if (t == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    int mv = -1, ms0 = 0, mn = 0;
+    if (t < kTV) {
+        load_meta(tile, mv, ms0, mn);
+        tv[0][t] = mv;
+        ts0[0][t] = ms0;
+        tn[0][t] = mn;
+        load_meta(tile + gridDim.x, mv, ms0, mn);
+    }
+    __syncthreads();
+    fetch(0, 0);
+    unsigned phase = 0;
+    for (int it = 0; tile < ntiles; it++, tile += gridDim.x) {  // block-uniform
+        const int b = it & 1;
+        int nmax = 0;
+#pragma unroll
+        for (int i = 0; i < kTV; i++) nmax = max(nmax, tn[b][i]);
+        const int nslab = (nmax + kSL - 1) / kSL;
+        float acc = 0.0f;
+        bool bad = false;
+        for (int s = 0; s < nslab; s++) {
+            const bool last = s + 1 == nslab;
+            __syncthreads();  // the previous step's readers of the shared arrays are done
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int j = t + h * kTileThreads;
+                if (j < kTE && rp[h] >= 0) {
+                    const int li = j / kSL, r = li * kRV + (j - li * kSL);
+                    Ps[r] = rp[h];
+                    Ws[r] = rw[h];
+                    if (PRE_NORM) cp_async4(&Ns[r], norm + rp[h]);
+                }
+            }
+            if (last && t < kTV) {
+                tv[b ^ 1][t] = mv;
+                ts0[b ^ 1][t] = ms0;
+                tn[b ^ 1][t] = mn;
+            }
+            if (t == 0) {
+                s_space = 0;
+                s_tx = 0;
+                s_timeout = 0;
+            }
+            __syncthreads();
+            // runs of consecutive pixels: the first entry of each places the
+            // run in the buffer and records every entry's row start
+            const char* rsrc[2] = {nullptr, nullptr};
+            unsigned rdst[2] = {0, 0}, rbytes[2] = {0, 0};
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int j = t + h * kTileThreads;
+                if (j >= kTE || rp[h] < 0) continue;
+                const int li = j / kSL, el = j - li * kSL, base = li * kRV;
+                const int n = min(kSL, tn[b][li] - s * kSL);
+                const int p = Ps[base + el];
+                if (el > 0 && Ps[base + el - 1] == p - 1) continue;  // not a run start
+                int len = 1;
+                while (el + len < n && Ps[base + el + len] == p + len) len++;
+                const char* b0 = in_b + (size_t)p * (L * sizeof(float));
+                const char* b1 = b0 + (size_t)len * (L * sizeof(float));
+                const char* a0 = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(b0) & ~(uintptr_t)15);
+                const char* a1 =
+                    reinterpret_cast<const char*>((reinterpret_cast<uintptr_t>(b1) + 15) & ~(uintptr_t)15);
+                const unsigned bytes = (unsigned)(a1 - a0);
+                const unsigned off = atomicAdd(&s_space, bytes);  // bytes and offsets: multiples of 16
+                const int row0 = (int)((off + (unsigned)(b0 - a0)) / sizeof(float));
+                for (int i = 0; i < len; i++) Os[base + el + i] = row0 + i * L;
+                if (a1 <= in_end) {
+                    atomicAdd(&s_tx, bytes);
+                    rsrc[h] = a0;
+                    rdst[h] = off;
+                    rbytes[h] = bytes;
+                } else {  // the span would pass the end of the input: plain loads
+                    for (int i = 0; i < len * L; i++) X[row0 + i] = in[(size_t)p * L + i];
+                }
+            }
+            fence_proxy_async_smem();  // this thread's generic writes of X before any async copy
+            __syncthreads();
+            // the phase's byte count before any copy can complete against it
+            if (t == 0) mbar_expect_tx(&bar, s_tx);
+            __syncthreads();
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+                if (rbytes[h]) bulk_g2s(reinterpret_cast<char*>(X) + rdst[h], rsrc[h], rbytes[h], &bar);
+            cp_async_commit();
+            if (!last) {
+                fetch(b, s + 1);
+            } else {
+                fetch(b ^ 1, 0);
+                if (t < kTV) load_meta(tile + 2L * gridDim.x, mv, ms0, mn);
+            }
+            cp_async_wait<0>();
+            if (!mbar_wait_bounded(&bar, phase)) s_timeout = 1;
+            phase ^= 1;
+            __syncthreads();
+            if (s_timeout) bad = true;
+            const int n = worker ? min(kSL, tn[b][g] - s * kSL) : 0;
+            if (n > 0) {
+                const int* os = &Os[g * kRV];
+                const float* ws = &Ws[g * kRV];
+                const float* ns = &Ns[g * kRV];
+#pragma unroll 4
+                for (int e = 0; e < n; e++) {
+                    float x = X[os[e] + k];
+                    if (PRE_NORM) x = fmul(x, ns[e]);
+                    acc = fadd(acc, fmul(ws[e], x));
+                }
+            }
+        }
+        if (bad && t == 0) atomicAdd(&g_bulk_wait_timeouts, 1ull);
+        if (worker && tv[b][g] >= 0) vals[(long)(tv[b][g] + 1) * Lrow + k] = bad ? __int_as_float(0x7fc00000) : acc;
+        for (int q = t; q < kTV * (Lrow - L); q += kTileThreads) {  // row padding
+            const int li = q / (Lrow - L);
+            if (tv[b][li] >= 0) vals[(long)(tv[b][li] + 1) * Lrow + L + (q - li * (Lrow - L))] = 0.0f;
+        }
+    }
+}
+
 __global__ void count_long_kernel(int M, const int* __restrict__ counts, int threshold, int* __restrict__ n) {
     const int v = blockIdx.x * blockDim.x + threadIdx.x;
     const bool is_long = v < M && counts[v] > threshold;
@@ -2131,6 +2357,40 @@ static void splat_tile_range(const Lattice& lat, int dom, int first, int count, 
            lat.seg_pix.get(), lat.seg_w.get(), in, pre_norm, vals, lv, Lp);
 }
 
+// Bounded waits of the bulk-copy splat that ran out, since the library
+// loaded (read from the current device).
+unsigned long long bulk_wait_timeouts() {
+    unsigned long long v = 0;
+    DCRF_CUDA(cudaMemcpyFromSymbol(&v, g_bulk_wait_timeouts, sizeof(v)));
+    return v;
+}
+
+// The bulk-copy splat (L = 21) over order[first, first + count) (or domain
+// `dom`'s live lists); inputs that are not 16-byte aligned take the tiled
+// splat, which computes the same values.
+static void splat_bulk_range(const Lattice& lat, int dom, int first, int count, const float* in,
+                             const float* pre_norm, float* vals, int Lp, cudaStream_t st) {
+    if (count <= 0) return;
+    if (reinterpret_cast<uintptr_t>(in) % 16 != 0) {
+        splat_tile_range(lat, dom, first, count, in, pre_norm, vals, Lp, st);
+        return;
+    }
+    static const bool carveout = [] {
+        DCRF_CUDA(cudaFuncSetAttribute(splat_bulk21_kernel<true>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+        DCRF_CUDA(cudaFuncSetAttribute(splat_bulk21_kernel<false>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                       (int)cudaSharedmemCarveoutMaxShared));
+        return true;
+    }();
+    (void)carveout;
+    const Live lv = lat.live_of(dom);
+    const bool live = lv.n != nullptr;
+    const int* order = lat.vorder.get() + (live ? 0 : first);
+    const int grid = (int)std::min<long>((count + kTV - 1) / kTV, (long)sm_count() * kBulkBlocksPerSM);
+    launch(pre_norm ? splat_bulk21_kernel<true> : splat_bulk21_kernel<false>, grid, kTileThreads, 0, st, count,
+           order, lat.seg_start.get(), lat.seg_pix.get(), lat.seg_w.get(), in, lat.N, pre_norm, vals, lv, Lp);
+}
+
 namespace {
 constexpr int kTuneMinPixels = 1 << 18;  // smaller lattices keep the default shapes
 std::mutex g_tune_mu;
@@ -2188,7 +2448,7 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
     float* src = va.get();
     float* dst = vb.get();
     float tbest = 1e30f;
-    for (int kind = 0; kind < 5; kind++) {
+    for (int kind = 0; kind < 6; kind++) {
         for (int w : {2, 4, 8}) {
             if ((kind == 0 || kind >= 3) && w != 4) continue;  // no warp splat in these forms
             FilterShape fs = best;
@@ -2257,6 +2517,15 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
         } else {
             splat_tile_range(*this, kDomLong, nh, n_long - nh, in, pre_norm, vals, Lp, st);
             splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
+        }
+        return;
+    }
+    if (kind == 5) {  // the bulk-copy splat for every list up to the huge ones
+        if (!live) {
+            splat_bulk_range(*this, kDomLong, nh, M - nh, in, pre_norm, vals, Lp, st);
+        } else {
+            splat_bulk_range(*this, kDomLong, nh, n_long - nh, in, pre_norm, vals, Lp, st);
+            splat_bulk_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
         }
         return;
     }

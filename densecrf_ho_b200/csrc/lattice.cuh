@@ -47,6 +47,8 @@ void rescaled_bins(float2* bins, const float* Q, long n, const float* qminmax, c
 int slice_grid(long n);
 // Capacity, in floats, of the fixed scratch array of compute_noalloc.
 size_t noalloc_scratch_floats();
+// Bounded device waits (bulk-copy splat) that ran out on the current device.
+unsigned long long bulk_wait_timeouts();
 
 // The units a filter launch covers.  Without `n`, every unit of the
 // launch's range.  With it (a batched solve), only the units of the images
@@ -99,7 +101,8 @@ struct FilterShape {
     // 2 = warp splat for every list;
     // 3 = tiled splat (splat_tile21_kernel) for every list;
     // 4 = staged splat_kernel for the long lists, the tiled splat for the
-    //     short ones.
+    //     short ones;
+    // 5 = bulk-copy splat (splat_bulk21_kernel) for every list.
     int splat_kind = 0;
     int splat_warps = 4;     // vertices (warps) per block of the warp splat: 2, 4 or 8
     int blur_threads = 256;  // threads per block of the float4 blur: 128, 256 or 512

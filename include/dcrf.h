@@ -133,12 +133,17 @@ dcrf_status dcrf_lattice_export(dcrf_lattice lat, int32_t* offset, int32_t* rank
 dcrf_status dcrf_lattice_stream(dcrf_lattice lat, void** stream);
 /* Launch shapes of the 21-label plain filter (shape[4]: splat warps per
  * block in {2,4,8}, blur threads per block in {128,256,512}, slice pixels
- * per tile in {64,128,256}, splat form 0..4 as dcrf_batch_filter_shape
+ * per tile in {64,128,256}, splat form 0..5 as dcrf_batch_filter_shape
  * lists them).  The autotuner sets them on the first 21-label filter call of
  * a lattice of 2^18 pixels or more; set_filter_shape pins a shape instead
  * (that lattice is then never tuned).  Every shape computes bit-identical
  * values.  No counterpart in the reference. */
 dcrf_status dcrf_lattice_filter_shape(dcrf_lattice lat, int* shape);
+/* Number of bounded device waits that ran out on the current device since
+ * the library was loaded (the bulk-copy splat waits for its copies with a
+ * poll limit; a tile whose wait ran out writes NaN rows and counts here).
+ * 0 in normal operation.  No counterpart in the reference. */
+dcrf_status dcrf_device_wait_timeouts(unsigned long long* count);
 dcrf_status dcrf_lattice_set_filter_shape(dcrf_lattice lat, const int* shape);
 
 /* ------------------------------------------------------------------------
@@ -431,7 +436,8 @@ dcrf_status dcrf_batch_pairwise_apply_dev(dcrf_batch b, int k, float* d_out, con
  * slice pixels per block, [3] splat form: 0 staged long lists + thread-per-
  * label short lists, 1 warp splat for the long lists, 2 warp splat for
  * every list, 3 tiled splat for every list, 4 staged long lists + tiled
- * short lists); the defaults until a filter call of 2^18 pixels or more has
+ * short lists, 5 bulk-copy splat for every list); the defaults until a
+ * filter call of 2^18 pixels or more has
  * tuned them.  shape holds 4 ints.  No counterpart in the reference. */
 dcrf_status dcrf_batch_filter_shape(dcrf_batch b, int k, int* shape);
 /* Pins term k's launch shapes (as dcrf_lattice_set_filter_shape). */

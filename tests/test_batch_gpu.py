@@ -122,7 +122,7 @@ def test_batch_pairwise_apply_equals_single_applies():
         assert b.lattice_size(k) == Ms
 
 
-@pytest.mark.parametrize("kind", [0, 2, 3, 4])
+@pytest.mark.parametrize("kind", [0, 2, 3, 4, 5])
 def test_batch_splat_forms_equal_single_solves(kind):
     """The batched QP (live-image compaction) and the batched apply with each
     splat form pinned on both terms' concatenated lattices: outputs, steps

@@ -5,11 +5,13 @@ neighbours) and filter outputs are required to be BIT-EXACT: the CUDA path
 reproduces the reference's float operation order and the splat gathers in
 the order the reference's scatter accumulates.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
 from conftest import golden, golden_names
-from densecrf_ho_b200 import Permutohedral, synth
+from densecrf_ho_b200 import Permutohedral, check, lib, synth
 
 pytestmark = pytest.mark.gpu
 
@@ -112,7 +114,7 @@ def test_ordered_filter_huge_lists(L, oracle_mod):
 # Every launch shape the autotuner can choose for the 21-label plain filter:
 # (splat warps per block, blur threads, slice pixels per tile, splat form).
 FILTER_SHAPES = [(4, 256, 128, 0), (2, 128, 64, 1), (8, 512, 256, 1), (2, 256, 128, 2), (8, 128, 64, 2),
-                 (4, 512, 256, 3), (4, 128, 128, 4)]
+                 (4, 512, 256, 3), (4, 128, 128, 4), (4, 256, 128, 5)]
 
 
 @pytest.mark.parametrize("shape", FILTER_SHAPES)
@@ -130,6 +132,9 @@ def test_filter_every_launch_shape_bit_exact(shape, oracle_mod):
         assert lat.filter_shape() == tuple(shape)
         assert _eq(lat.compute(x), orc.compute(x))
         assert _eq(lat.compute(x, reverse=True), orc.compute(x, True))
+    n = C.c_ulonglong(99)
+    check(lib().dcrf_device_wait_timeouts(C.byref(n)))
+    assert n.value == 0
 
 
 def test_filter_error_vs_fp64_oracle(oracle_mod):
