@@ -2454,7 +2454,7 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
             FilterShape fs = best;
             fs.splat_kind = kind;
             fs.splat_warps = w;
-            const float t = timed([&] { splat_rest(fs, in, L, pre_norm, src, false, st); });
+            const float t = timed([&] { splat_rest(fs, in, L, pre_norm, src, false, st, nullptr); });
             if (t < tbest) {
                 tbest = t;
                 best.splat_kind = kind;
@@ -2503,8 +2503,11 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
 }
 
 void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
-                         bool live, cudaStream_t st) {
+                         bool live, cudaStream_t st, cudaStream_t st_short) {
     const int Lp = value_row(L);
+    // live images: the short lists are their own domain, splatted on
+    // st_short (concurrent with the long lists) when the caller gives one
+    cudaStream_t sts = live && st_short ? st_short : st;
     const int nh = n_huge, n_short = M - n_long;
     const int kind = L == 21 ? fs.splat_kind : 0;
     if (kind == 2 && !live) {
@@ -2516,7 +2519,7 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
             splat_tile_range(*this, kDomLong, nh, M - nh, in, pre_norm, vals, Lp, st);
         } else {
             splat_tile_range(*this, kDomLong, nh, n_long - nh, in, pre_norm, vals, Lp, st);
-            splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
+            splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, sts);
         }
         return;
     }
@@ -2525,7 +2528,7 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
             splat_bulk_range(*this, kDomLong, nh, M - nh, in, pre_norm, vals, Lp, st);
         } else {
             splat_bulk_range(*this, kDomLong, nh, n_long - nh, in, pre_norm, vals, Lp, st);
-            splat_bulk_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
+            splat_bulk_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, sts);
         }
         return;
     }
@@ -2537,7 +2540,7 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
                    L, vorder.get() + (live ? 0 : nh), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals,
                    lv, Lp);
         }
-        splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, st);
+        splat_tile_range(*this, kDomShort, n_long, n_short, in, pre_norm, vals, Lp, sts);
         return;
     }
     if (n_long > nh) {
@@ -2554,12 +2557,12 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
     }
     if (n_short) {
         if (kind == 2) {  // live: the short lists are their own domain
-            splat_warp_range(*this, fs.splat_warps, kDomShort, n_long, n_short, L, Lp, in, pre_norm, vals, st);
+            splat_warp_range(*this, fs.splat_warps, kDomShort, n_long, n_short, L, Lp, in, pre_norm, vals, sts);
         } else {
             const Live lv = live ? live_of(kDomShort) : Live{};
             launch(L == 21 ? (pre_norm ? splat_short_kernel<true, 21> : splat_short_kernel<false, 21>)
                            : (pre_norm ? splat_short_kernel<true> : splat_short_kernel<false>),
-                   unit_grid((long)n_short * Lp, kTB, live, kTB), kTB, 0, st, n_short, L, vorder.get() + (live ? 0 : n_long),
+                   unit_grid((long)n_short * Lp, kTB, live, kTB), kTB, 0, sts, n_short, L, vorder.get() + (live ? 0 : n_long),
                    seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals, lv, Lp);
         }
     }
@@ -2581,12 +2584,17 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
     // chain sets their time, and its three chunks of copies in flight hide
     // the load latency a lone warp cannot hide otherwise), else by
     // splat_kernel.
+    // With live images the short lists are a separate launch: it runs on the
+    // side stream too (after the very long lists), beside the long lists'.
     const int nh = n_huge;
-    const bool forked = nh > 0;
+    const bool fork_short = live && M - n_long > 0 && n_long > nh;
+    const bool forked = nh > 0 || fork_short;
     if (forked) {
         ensure_aux();
         DCRF_CUDA(cudaEventRecord(ev_fork, st));
         DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
+    }
+    if (nh > 0) {
         const Live lv = live_of(kDomHuge);
         const int g = unit_grid(nh, kStageWarps, live, 32 * kStageWarps);
         if (L == 21)
@@ -2596,7 +2604,7 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
             launch(pre_norm ? splat_kernel<true> : splat_kernel<false>, g, 32 * kStageWarps, 0, aux, nh, L,
                    vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, lv, Lp);
     }
-    splat_rest(shape, in, L, pre_norm, src, live, st);
+    splat_rest(shape, in, L, pre_norm, src, live, st, fork_short ? aux : nullptr);
     if (forked) {
         DCRF_CUDA(cudaEventRecord(ev_join, aux));
         DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));

@@ -218,9 +218,10 @@ struct Lattice {
     // already; outputs are not touched.
     void tune_shape(const float* in, int L, const float* pre_norm);
     // Splat of every list after the first n_huge (whose splat runs on the
-    // side stream) into vals, in the form `fs` names.
+    // side stream) into vals, in the form `fs` names; with live images the
+    // short lists' launch goes on st_short when one is given.
     void splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
-                    bool live, cudaStream_t st);
+                    bool live, cudaStream_t st, cudaStream_t st_short);
 
     Lattice() = default;
     Lattice(const Lattice&) = delete;
