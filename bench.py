@@ -69,6 +69,13 @@ def parse():
                     help="time only the batched QP, without the sequential comparison (a short command for ncu)")
     ap.add_argument("--only-batch-filter", action="store_true",
                     help="time only the batched lattice filter over the 64-image concatenated lattices")
+    ap.add_argument("--splat-form", type=int, default=None,
+                    help="pin the 21-label plain filter's splat form (0-5, dcrf_batch_set_filter_shape) in the "
+                         "batched filter and batched QP legs instead of autotuning it")
+    ap.add_argument("--all-splat-forms", action="store_true",
+                    help="with --only-batch-filter: time the batched filter with every splat form pinned")
+    ap.add_argument("--only-ho", action="store_true",
+                    help="time only qp_sp / lp_sp at 640x480 (no CPU reference)")
     ap.add_argument("--batch-images", type=int, default=64,
                     help="images of the batched workloads (64 = the benchmark; fewer for profiling runs)")
     ap.add_argument("--prox-iters", type=int, default=50,
@@ -334,10 +341,13 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ ours --
-def measure_filters(W, H, img, reps=20):
+def measure_filters(W, H, img, reps=20, lp_q=None):
     """Times the ordered filter (the LP's dominant operation) and the plain
     splat/blur/slice filter on the bilateral and Gaussian lattices of the
-    workload image, with CUDA events on each lattice's own stream."""
+    workload image, with CUDA events on each lattice's own stream.  The
+    ordered filter's input is uniform random Q (its bins spread over all ten
+    bins: the slice's least local case); with lp_q (device [N][L]) it is also
+    timed on that Q, the LP's own iterate."""
     import torch
     from densecrf_ho_b200 import Permutohedral, lib, check
     Ls = lib()
@@ -367,6 +377,19 @@ def measure_filters(W, H, img, reps=20):
         t = e0.elapsed_time(e1) / reps / 1e3
         ab = ord_filter_bytes(N, lat.M, lat.d)
         roof[name] = dict(M=lat.M, d=lat.d, seconds=t, bytes=ab, gbs=ab / t / 1e9)
+        if lp_q is not None:
+            runq = lambda: check(Ls.dcrf_lattice_compute_ord_dev(lat._h, C.c_void_p(ro.data_ptr()),
+                                                                 C.c_void_p(lp_q.data_ptr()), L))
+            for _ in range(3):
+                runq()
+            torch.cuda.synchronize()
+            e0.record(ls)
+            for _ in range(reps):
+                runq()
+            e1.record(ls)
+            torch.cuda.synchronize()
+            tq = e0.elapsed_time(e1) / reps / 1e3
+            roof[name]["lp_q"] = dict(seconds=tq, gbs=ab / tq / 1e9)
         # plain splat/blur/slice filter: the lattice-filter metric
         x = torch.rand((N, L), device="cuda")
         y = torch.empty_like(x)
@@ -537,7 +560,17 @@ def measure_ho(W=640, H=480, seed=2, cpu=True):
     return out
 
 
-def measure_batch(n=64, max_iter=100, reps=3, sequential=True):
+def pin_splat_form(b, form):
+    """Pins both terms' launch shapes of a batch: the default blur / slice
+    shapes with splat form `form` (no autotuning)."""
+    for k in range(b.n_terms()):
+        b.set_filter_shape(k, (4, 256, 128, int(form)))
+
+
+SPLAT_FORMS = ("staged", "warp_long", "warp_all", "tiled_all", "staged_long_tiled_short", "bulk_all")
+
+
+def measure_batch(n=64, max_iter=100, reps=3, sequential=True, splat_form=None):
     """Config 4: the plain QP (as config 1, up to 100 Frank-Wolfe iterations)
     of n images of uneven sizes (H ~ U[240, 500], W ~ U[320, 500], seeded),
     solved as one batch (dcrf_batch_qp_dev: concatenated lattices, per-image
@@ -558,6 +591,8 @@ def measure_batch(n=64, max_iter=100, reps=3, sequential=True):
     b.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
                            np.concatenate([im["rgb"] for im in imgs]), BILAT[2])
     setup_ms = (time.perf_counter() - t0) * 1e3
+    if splat_form is not None:
+        pin_splat_form(b, splat_form)
     q0 = b.unary_init()
     init = torch.from_numpy(q0).cuda()
     out = torch.empty_like(init)
@@ -630,7 +665,7 @@ def measure_batch(n=64, max_iter=100, reps=3, sequential=True):
             "outputs_match_sequential": same}
 
 
-def measure_batch_filter(n=64, reps=10):
+def measure_batch_filter(n=64, reps=10, splat_form=None, all_forms=False):
     """The batched lattice filter: PairwisePotential::apply of each pairwise
     term (normalised Potts filter, pre- and post-scaled by the norm) over the
     term's concatenated lattice of the config-4 batch (n images, H ~ U[240,
@@ -649,12 +684,35 @@ def measure_batch_filter(n=64, reps=10):
     b.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1],
                            np.concatenate([im["rgb"] for im in imgs]), BILAT[2])
     N = int(b.N)
+    if splat_form is not None:
+        pin_splat_form(b, splat_form)
     x = torch.rand((N, L), device="cuda", generator=torch.Generator("cuda").manual_seed(1))
     y = torch.empty_like(x)
     sptr = C.c_void_p()
     check(Ls.dcrf_batch_stream(b._h, C.byref(sptr)))
     bs = torch.cuda.ExternalStream(sptr.value)
     peak, peak_kind = measured_peaks()
+    if all_forms:  # every splat form pinned in turn; outputs must not change
+        forms = {}
+        for k, name in enumerate(("gaussian", "bilateral")):
+            ref = None
+            for f, fname in enumerate(SPLAT_FORMS):
+                b.set_filter_shape(k, (4, 256, 128, f))
+                run = lambda: check(Ls.dcrf_batch_pairwise_apply_dev(b._h, k, C.c_void_p(y.data_ptr()),
+                                                                     C.c_void_p(x.data_ptr())))
+                for _ in range(3):
+                    run()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(bs)
+                for _ in range(reps):
+                    run()
+                e1.record(bs)
+                torch.cuda.synchronize()
+                if ref is None:
+                    ref = y.clone()
+                forms[f"{name}_{fname}"] = {"ms": e0.elapsed_time(e1) / reps, "same_output": bool(torch.equal(ref, y))}
+        return {"images": n, "pixels": N, "forms": forms}
     out = {"workload": f"PairwisePotential::apply over the concatenated lattice of {n} images "
                        f"H~U[240,500] W~U[320,500] (seeded), L={L}, device-resident",
            "images": n, "pixels": N, "peak_gbs": peak, "peak_kind": peak_kind}
@@ -679,8 +737,7 @@ def measure_batch_filter(n=64, reps=10):
         out[name] = {"M": M, "d": d, "ms": t * 1e3, "bytes": fb, "gbs": fb / t / 1e9, "frac": fb / t / 1e9 / peak,
                      "gpix_label_s": N * L / t / 1e9,
                      "launches_per_call": int((Ls.dcrf_kernel_launches() - l0) // reps),
-                     "tuned_shape": {"splat_form": ("staged", "warp_long", "warp_all", "tiled_all",
-                                                    "staged_long_tiled_short", "bulk_all")[shp[3]],
+                     "tuned_shape": {"splat_form": SPLAT_FORMS[shp[3]],
                                      "splat_vertices_per_block": shp[0], "blur_threads": shp[1],
                                      "slice_pixels_per_block": shp[2]}}
     return out
@@ -901,11 +958,94 @@ def measure_adjoint(n=16, size=512, T=10, reps=3):
     pred = float((gU.double() * torch.from_numpy(V).cuda().double()).sum())
     dd = (loss(U + eps * V) - loss(U - eps * V)) / (2 * eps)
     b.setUnaryEnergy(U)
+    full_bytes = b.meanfield_state_bytes(T)
+    # checkpointing: every 5th iterate kept, the rest recomputed in the
+    # backward pass, the lattices released after the forward and rebuilt
+    b.set_checkpointing(5, True)
+    fwd()
+    bwd()
+    torch.cuda.synchronize()
+    tfr = tbr = 0.0
+    for _ in range(reps):
+        ev[0].record(st)
+        fwd()
+        ev[1].record(st)
+        bwd()
+        ev[2].record(st)
+        torch.cuda.synchronize()
+        tfr += ev[0].elapsed_time(ev[1])
+        tbr += ev[1].elapsed_time(ev[2])
+    tfr, tbr = tfr / reps, tbr / reps
+    ck_bytes = b.meanfield_state_bytes(T)
+    b.set_checkpointing(1, False)
     return {"workload": f"unrolled mean-field, {n} images {size}x{size}, L={L}, {T} iterations, forward + adjoint "
                         f"(dL/dU and dL/dw for the Gaussian and bilateral Potts weights)",
             "forward_ms": tf, "backward_ms": tb, "images_per_s": n / ((tf + tb) / 1e3),
+            "state_bytes": full_bytes,
+            "checkpoint_every_5_lattice_recompute": {"forward_ms": tfr, "backward_ms": tbr,
+                                                      "images_per_s": n / ((tfr + tbr) / 1e3),
+                                                      "state_bytes": ck_bytes},
             "pixels": n * size * size, "directional_check_rel_err": abs(dd - pred) / abs(pred),
+            "fd64_check": adjoint_fd64_check(T=T),
             "grad_w": [float(x) for x in gw]}
+
+
+def adjoint_fd64_check(T=10, W=48, H=40, coords=16, h=1e-6):
+    """The adjoint against FP64 central finite differences on a small image
+    (21 labels, `coords` random unary coordinates and both Potts weights):
+    the finite differences run an FP64 mean-field on the host with the
+    oracle's FP64 lattice filter on the same lattices (the checker only).
+    Returns the largest relative error, each coordinate's error measured
+    against max(|fd|, 1e-2 max|fd|)."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    from densecrf_ho_b200 import DenseCRF2DBatch
+    img = synth.make_image(W, H, L, 3)
+    U = img["unary"].astype(np.float32)
+    b = DenseCRF2DBatch([(W, H)], L)
+    b.setUnaryEnergy(U)
+    b.addPairwiseGaussian(GAUSS[0], GAUSS[0], GAUSS[1])
+    b.addPairwiseBilateral(BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"], BILAT[2])
+    c = np.random.default_rng(0).standard_normal(U.shape)
+    b.meanfield(T)
+    gU, gw = b.meanfield_backward(c.astype(np.float32))
+    lats = []
+    for f in (synth.gaussian_features(W, H, GAUSS[0], GAUSS[0]),
+              synth.bilateral_features(W, H, BILAT[0], BILAT[0], BILAT[1], BILAT[1], BILAT[1], img["rgb"])):
+        lat = O.OracleLattice(f)
+        lats.append((lat, 1.0 / np.sqrt(lat.compute_f64(np.ones((W * H, 1)))[:, 0] + 1e-20)))
+
+    def softmax(a):
+        e = np.exp(a - a.max(1, keepdims=True))
+        return e / e.sum(1, keepdims=True)
+
+    def run(UU, ws):
+        q = softmax(-UU)
+        for _ in range(T):
+            a = -UU.copy()
+            for (lat, nrm), w in zip(lats, ws):
+                a += w * nrm[:, None] * lat.compute_f64(nrm[:, None] * q)
+            q = softmax(a)
+        return float((c * q).sum())
+
+    U64, w0 = U.astype(np.float64), [GAUSS[1], BILAT[2]]
+    flat = np.random.default_rng(1).choice(U.size, coords, replace=False)
+    fd = np.empty(coords)
+    for j, idx in enumerate(flat):
+        Up, Um = U64.copy(), U64.copy()
+        Up.flat[idx] += h
+        Um.flat[idx] -= h
+        fd[j] = (run(Up, w0) - run(Um, w0)) / (2 * h)
+    rel = np.abs(gU.flat[flat].astype(np.float64) - fd) / np.maximum(np.abs(fd), 1e-2 * np.abs(fd).max())
+    wrel = []
+    for k in range(2):
+        wp, wm = list(w0), list(w0)
+        wp[k] += h
+        wm[k] -= h
+        fdw = (run(U64, wp) - run(U64, wm)) / (2 * h)
+        wrel.append(abs(gw[k] - fdw) / abs(fdw))
+    return {"image": f"{W}x{H}", "labels": L, "iterations": T, "coordinates": coords, "step": h,
+            "unary_max_rel_err": float(rel.max()), "weight_max_rel_err": float(max(wrel))}
 
 
 def run_ours(args):
@@ -926,10 +1066,14 @@ def run_ours(args):
         print(json.dumps(measure_filters(W, H, img, reps=3)))
         return
     if args.only_batch_filter:
-        print(json.dumps(measure_batch_filter(n=args.batch_images)))
+        print(json.dumps(measure_batch_filter(n=args.batch_images, splat_form=args.splat_form,
+                                              all_forms=args.all_splat_forms)))
+        return
+    if args.only_ho:
+        print(json.dumps(measure_ho(cpu=False)))
         return
     if args.only_batch_qp:
-        print(json.dumps(measure_batch(n=args.batch_images, reps=1, sequential=False)))
+        print(json.dumps(measure_batch(n=args.batch_images, reps=1, sequential=False, splat_form=args.splat_form)))
         return
     if args.only_batch:
         print(json.dumps(measure_ho()))
@@ -999,7 +1143,7 @@ def run_ours(args):
     e2e_value = world * args.steps / (ms_e2e / 1e3)
     same = bool(torch.equal(out_h, out_d.cpu()))
 
-    roof = measure_filters(W, H, img, reps=20)
+    roof = measure_filters(W, H, img, reps=20, lp_q=out_d)
     peak, peak_kind = measured_peaks()
     dom = roof["bilateral"]
     traffic = None
@@ -1012,7 +1156,10 @@ def run_ours(args):
                 "kernel": f"ordered lattice filter, bilateral d=5 lattice (M={dom['M']}), {W}x{H}, L={L}",
                 "peak_kind": peak_kind,
                 "gaussian_d2": {"M": roof["gaussian"]["M"], "gbs": roof["gaussian"]["gbs"],
-                                "frac": roof["gaussian"]["gbs"] / peak}}
+                                "frac": roof["gaussian"]["gbs"] / peak},
+                "on_lp_solution": {"input": "the LP's final Q (bins concentrated at 0 and 9) instead of uniform Q",
+                                   "ms": dom["lp_q"]["seconds"] * 1e3, "gbs": dom["lp_q"]["gbs"],
+                                   "frac": dom["lp_q"]["gbs"] / peak}}
 
     line = {"metric": "LP solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
