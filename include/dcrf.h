@@ -46,8 +46,9 @@ typedef struct dcrf_lattice_s* dcrf_lattice;
 typedef struct dcrf_model_s* dcrf_model;
 
 /* Device memory freed by a destroyed model, lattice or batch stays cached in
- * the process for the next one (up to DCRF_CACHE_MB MiB, default 2048, in
- * the environment); this hands every cached block back to the driver.  No
+ * the process for the next one (up to DCRF_CACHE_MB MiB from the
+ * environment; by default a quarter of the device's memory, at least 2048
+ * MiB); this hands every cached block back to the driver.  No
  * counterpart in the reference, which allocates on the host. */
 dcrf_status dcrf_release_cached_memory(void);
 /* A budget on the device memory the library holds for live models, lattices
