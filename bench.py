@@ -234,6 +234,48 @@ def _ref_worker(args):
     return dict(times=times, kind="reference" if use_ref else "port")
 
 
+def _ref_batch_worker(args):
+    """The stock reference's QP (qp_inference_super_pixels_non_convex, its
+    own stop rule) on a share of the batch's images, one core: the models are
+    built first, then (after the barrier) the solves are timed together."""
+    idx, n, barrier = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    sizes = synth.batch_sizes(n, 4)
+    models = []
+    for i in idx:
+        w, h = sizes[i]
+        img = synth.make_image(w, h, L, 1000 + i)
+        m = O.build_model(O.ReferenceModel, img, gaussian=GAUSS, bilateral=BILAT)
+        models.append((m, m.unary_init()))
+    if barrier is not None:
+        barrier.wait()
+    t0 = time.perf_counter()
+    for m, q0 in models:
+        m.qp(q0)
+    return time.perf_counter() - t0
+
+
+def cpu_batch_reference(n=64):
+    """The batch's images solved by the stock reference as independent
+    single-threaded processes over the usable host cores (round robin); the
+    wall time of the slowest worker."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    if not O.reference_available():
+        return None
+    workers = min(usable_cores(), n)
+    shares = [list(range(w, n, workers)) for w in range(workers)]
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Manager().Barrier(workers)
+    with ctx.Pool(workers) as pool:
+        times = pool.map(_ref_batch_worker, [(sh, n, barrier) for sh in shares])
+    wall = max(times)
+    return {"images": n, "cores": workers, "kind": "reference", "seconds": wall, "solves_per_s": n / wall,
+            "sample": f"all {n} images, the stock reference's QP (its stop rule), {workers} single-threaded "
+                      f"processes, round robin; models built before the timed solves"}
+
+
 def cpu_reference(W, H, seed, workers, fw, reps):
     """Per step: the wall time of `workers` concurrent samples (the slowest
     worker's), so that steps x time is time actually spent."""
@@ -1194,6 +1236,11 @@ def run_ours(args):
         line["extra"]["ho_640x480"] = measure_ho(cpu=not args.no_cpu_baseline)
         line["extra"]["batch_filter_64"] = measure_batch_filter()
         line["extra"]["batch_qp_64"] = measure_batch()
+        if not args.no_cpu_baseline:
+            cb = cpu_batch_reference()
+            if cb is not None:
+                cb["gpu_batch_vs_cpu"] = line["extra"]["batch_qp_64"]["batch_solves_per_s"] / cb["solves_per_s"]
+                line["extra"]["batch_qp_64"]["cpu_reference_all_cores"] = cb
         line["extra"]["adjoint_16x512x512"] = measure_adjoint()
         line["extra"]["next_rows_640x480"] = measure_next_rows(cpu=not args.no_cpu_baseline)
 
