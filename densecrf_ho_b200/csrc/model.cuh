@@ -115,6 +115,7 @@ struct Model {
     DevBuf<float2> lp_bins;  // ordered-filter bins of rescale(Q), shared by all terms
     DevBuf<int> ipart;
     DevBuf<double> ho_pre;  // qp_sp: FP64 clique prefixes [2][R][L]
+    DevBuf<double> ho_seg;  // qp_sp: FP64 per-segment totals of a clique prefix chain
     DevBuf<float> z_last;   // the clique variables z [R][L] at the end of the last QP (z_labels_)
     bool has_z_last = false;
     // compute_energy_higher_order(Q) (src/densecrf.cpp:960-980), with the z of

@@ -256,6 +256,88 @@ __global__ void __launch_bounds__(kHoThreads)
     cp_async_wait_group<0>();
 }
 
+// The FP64 prefix chains in segments of kHoSeg rows, so that they run in
+// parallel instead of one thread per label over every row.  The FP64 chains
+// are this engine's own choice (the reference sums in float; see
+// ho_scalar_kernel), so their order is free: segment 0 is summed from 0.0
+// exactly as the sequential chain (every clique of at most kHoSeg pixels gets
+// the sequential chain's value), a later segment starts from the sum of the
+// segments before it.  ho_seg_total_kernel: per (segment, label) the FP64
+// sum of the segment's rows; ho_seg_prefix_kernel: per (segment, label) the
+// carry-in from the totals, then the segment's prefix with the records of
+// the cliques whose size ends in it.
+constexpr int kHoSeg = 256;
+
+__global__ void ho_seg_total_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one,
+                                    double* __restrict__ tot, const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
+    if (sc && skip_on_zero_step && sc->zero_step) return;
+    const int seg = blockIdx.x, lab = threadIdx.x;
+    if (lab >= L) return;
+    const int q0 = seg * kHoSeg, q1 = min(cv.max_size, q0 + kHoSeg);
+    double s = 0.0;
+    int q = q0;
+    for (; q + 8 <= q1; q += 8) {
+        float x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = p[(long)(q + i) * L + lab];
+#pragma unroll
+        for (int i = 0; i < 8; i++) s += (double)(minus_one ? fsub(x[i], 1.0f) : x[i]);
+    }
+    for (; q < q1; q++) {
+        const float x = p[(long)q * L + lab];
+        s += (double)(minus_one ? fsub(x, 1.0f) : x);
+    }
+    tot[(long)seg * L + lab] = s;
+}
+
+__global__ void ho_seg_prefix_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one,
+                                     const double* __restrict__ tot, double* __restrict__ out64,
+                                     const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
+    if (sc && skip_on_zero_step && sc->zero_step) return;
+    const int seg = blockIdx.x, lab = threadIdx.x;
+    if (lab >= L) return;
+    const int q0 = seg * kHoSeg, q1 = min(cv.max_size, q0 + kHoSeg);
+    if (seg == 0)
+        for (int r = 0; r < cv.bstart[1]; r++) out64[(long)r * L + lab] = 0.0;  // empty cliques
+    double s = 0.0;
+    for (int g = 0; g < seg; g++) s += tot[(long)g * L + lab];
+    int ptr = cv.bstart[q0 + 1];  // the first clique of size > q0
+    int next = ptr < cv.R ? cv.sizes[ptr] : INT_MAX;
+    auto step = [&](float x, int len) {
+        s += (double)(minus_one ? fsub(x, 1.0f) : x);
+        while (len == next) {
+            out64[(long)ptr * L + lab] = s;
+            ptr++;
+            next = ptr < cv.R ? cv.sizes[ptr] : INT_MAX;
+        }
+    };
+    int q = q0;
+    for (; q + 8 <= q1; q += 8) {  // eight loads ahead of the eight dependent adds
+        float x[8];
+#pragma unroll
+        for (int i = 0; i < 8; i++) x[i] = p[(long)(q + i) * L + lab];
+#pragma unroll
+        for (int i = 0; i < 8; i++) step(x[i], q + i + 1);
+    }
+    for (; q < q1; q++) step(p[(long)q * L + lab], q + 1);
+}
+
+// FP64 clique prefixes of p (minus one when asked) into out64 [R][L]:
+// segment totals, then the segments' prefixes with their carries.
+static void ho_prefix64(cudaStream_t stream, DevBuf<double>& seg_buf, int clique_max, int L, const CliqueView& cv,
+                        const float* p, int minus_one, double* out64, const SolverScalars* sc, int skip_on_zero_step) {
+    const int nseg = (clique_max + kHoSeg - 1) / kHoSeg;
+    if (nseg == 0) {  // only empty cliques: their zeros
+        launch(ho_seg_prefix_kernel, 1, 64, 0, stream, cv, L, p, minus_one, (const double*)nullptr, out64, sc,
+               skip_on_zero_step);
+        return;
+    }
+    double* tot = seg_buf.ensure((size_t)nseg * L);
+    launch(ho_seg_total_kernel, nseg, 64, 0, stream, cv, L, p, minus_one, tot, sc, skip_on_zero_step);
+    launch(ho_seg_prefix_kernel, nseg, 64, 0, stream, cv, L, p, minus_one, (const double*)tot, out64, sc,
+           skip_on_zero_step);
+}
+
 // multiplySuperPixels(p [L x N]) with p = Q - 1 (src/densecrf.cpp:81-88): the
 // reference sums p(lab, 0..size_r-1) -- the clique-LOCAL index -- so every
 // clique's value is a prefix of one chain per label (ho_prefix_kernel).  Then
@@ -1268,8 +1350,7 @@ double Model::energy_qp_ho(const float* Q) {
         launch(clear_step_flags_kernel, 1, 1, 0, stream, sc);
         launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, (const float*)z_last.get(), zc, omz, sc);
         launch(eig_sum_kernel, 1, kHoThreads, 0, stream, (const float*)zc, LR, 8, sc, 2);
-        launch(ho_prefix_kernel<false, true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, (float*)nullptr, preQ,
-               (const SolverScalars*)nullptr, 0);
+        ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
         launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, (const float*)omz, (const double*)preQ, 8, sc, 1);
     }
     launch(ho_energy_finish_kernel, 1, 1, 0, stream, nt, sc, (int)(R > 0));
@@ -1405,9 +1486,10 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(fill_float_kernel, ceil_div(LR, 256), 256, 0, stream, LR, 1.0f, z);
         ho = buf(4);
         DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
-        // the float and the FP64 prefixes of Q - 1 in one pass
-        launch(ho_prefix_kernel<true, true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, preQ,
+        // the float chain of Q - 1 (sequential, as the reference sums it) and its FP64 prefixes
+        launch(ho_prefix_kernel<true, false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (double*)nullptr,
                (const SolverScalars*)nullptr, 0);
+        ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
         launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 0, nullptr);
     }
     // grad_y = unary + sum_k 2 A_k Q; energy terms Q . A_k Q (same applies).
@@ -1448,8 +1530,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         if (R > 0) {
             launch(ho_direction_kernel, 1, 256, 0, stream, cv, L, gz, z, sxz, t1, t2, cz, sc);
             launch(eig_sum_kernel, 1, kHoThreads, 0, stream, sxz, LR, 5, sc, 0);
-            launch(ho_prefix_kernel<false, true>, 1, kHoThreads, 0, stream, cv, L, sx, 0, (float*)nullptr, preS,
-                   (const SolverScalars*)sc, 0);
+            ho_prefix64(stream, ho_seg, clique_max, L, cv, sx, 0, preS, sc, 0);
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preQ, 3, sc, 0);    // a
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t2, preS, 4, sc, 0);   // b
             launch(ho_scalar_kernel, 1, kLMax, 0, stream, cv, L, t1, preS, 6, sc, 0);   // denom term
@@ -1465,10 +1546,11 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         launch(qp_update_kernel, kRedBlocks, kRedThreads, 0, stream, NL, sx, psi, ho, unary.get(), Q, grad, sc, part);
         launch(finalize_sums_kernel, 1, 32, 0, stream, part, kRedBlocks, 1, 7, sc);
         if (R > 0) {
-            // both prefixes of the updated Q - 1 in one pass (after a zero
-            // step Q is unchanged, so recomputing the float one is exact)
-            launch(ho_prefix_kernel<true, true>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, preQ,
-                   (const SolverScalars*)nullptr, 0);
+            // the prefixes of the updated Q - 1 (after a zero step Q is
+            // unchanged, and so is the float chain)
+            launch(ho_prefix_kernel<true, false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (double*)nullptr,
+                   (const SolverScalars*)sc, 1);
+            ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
             launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 1, sc);
             launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
             launch(eig_sum_kernel, 1, kHoThreads, 0, stream, zc, LR, 8, sc, 2);
