@@ -1222,6 +1222,17 @@ __global__ void ord_bins_kernel(long n, const float* __restrict__ Q, float2* __r
     bins[t] = ord_bin_pair(Q[t]);
 }
 
+// The same, four elements per thread with 16-byte loads and stores (Q and
+// bins 16-byte aligned; n4 = n / 4 quads, the tail by ord_bins_kernel).
+__global__ void ord_bins4_kernel(long n4, const float4* __restrict__ Q, float4* __restrict__ bins) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n4) return;
+    const float4 q = Q[t];
+    const float2 a = ord_bin_pair(q.x), b = ord_bin_pair(q.y), c = ord_bin_pair(q.z), d = ord_bin_pair(q.w);
+    bins[2 * t] = make_float4(a.x, a.y, b.x, b.y);
+    bins[2 * t + 1] = make_float4(c.x, c.y, d.x, d.y);
+}
+
 // Each of the 10 bins accumulates, in entry order, the weights of the entries
 // that reach it: bins 0..c (lower pass) or c..9 (upper pass), addSplitArray
 // (:548-569).  Branch-free and bit-identical: the mask m = [c_lower >= b]
@@ -1824,6 +1835,36 @@ __global__ void rescaled_bins_kernel(long n, const float* __restrict__ Q, const 
     float rq = fsub(Q[t], mn);
     if (range > 0.0f) rq = rq / range;
     bins[t] = ord_bin_pair(rq);
+}
+
+// The same, four elements per thread (as ord_bins4_kernel).
+__global__ void rescaled_bins4_kernel(long n4, const float4* __restrict__ Q, const float* __restrict__ qmm,
+                                      float4* __restrict__ bins) {
+    const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n4) return;
+    const float mn = qmm[0], range = fsub(qmm[1], qmm[0]);
+    const float4 q = Q[t];
+    float r[4] = {fsub(q.x, mn), fsub(q.y, mn), fsub(q.z, mn), fsub(q.w, mn)};
+    if (range > 0.0f)
+#pragma unroll
+        for (int i = 0; i < 4; i++) r[i] = r[i] / range;
+    const float2 a = ord_bin_pair(r[0]), b = ord_bin_pair(r[1]), c = ord_bin_pair(r[2]), d = ord_bin_pair(r[3]);
+    bins[2 * t] = make_float4(a.x, a.y, b.x, b.y);
+    bins[2 * t + 1] = make_float4(c.x, c.y, d.x, d.y);
+}
+
+bool aligned16(const void* p) { return reinterpret_cast<uintptr_t>(p) % 16 == 0; }
+
+// Ordered-filter bins of Q [n]: four per thread where the pointers allow.
+void ord_bins(float2* bins, const float* Q, long n, cudaStream_t st) {
+    if (aligned16(Q) && aligned16(bins)) {
+        const long n4 = n / 4;
+        if (n4) launch(ord_bins4_kernel, ceil_div(n4, kTB), kTB, 0, st, n4, reinterpret_cast<const float4*>(Q),
+                       reinterpret_cast<float4*>(bins));
+        if (n > 4 * n4) launch(ord_bins_kernel, 1, kTB, 0, st, n - 4 * n4, Q + 4 * n4, bins + 4 * n4);
+    } else {
+        launch(ord_bins_kernel, ceil_div(n, kTB), kTB, 0, st, n, Q, bins);
+    }
 }
 
 int bits_for(int n) {  // bits needed to hold values 0..n-1
@@ -2670,12 +2711,20 @@ void Lattice::compute_ord(float* out, const float* Q, int L, const SliceEpilogue
     require(L >= 1, DCRF_E_ARG, "compute_ord: L must be >= 1");
     const long NL = (long)N * L;
     float2* bins = obins.ensure((size_t)NL);
-    launch(ord_bins_kernel, ceil_div(NL, kTB), kTB, 0, stream, NL, Q, bins);
+    ord_bins(bins, Q, NL, stream);
     compute_ord_bins(out, bins, L, ep, nullptr);
 }
 
 void rescaled_bins(float2* bins, const float* Q, long n, const float* qminmax, cudaStream_t st) {
-    launch(rescaled_bins_kernel, ceil_div(n, kTB), kTB, 0, st, n, Q, qminmax, bins);
+    if (aligned16(Q) && aligned16(bins)) {
+        const long n4 = n / 4;
+        if (n4) launch(rescaled_bins4_kernel, ceil_div(n4, kTB), kTB, 0, st, n4, reinterpret_cast<const float4*>(Q),
+                       qminmax, reinterpret_cast<float4*>(bins));
+        if (n > 4 * n4)
+            launch(rescaled_bins_kernel, 1, kTB, 0, st, n - 4 * n4, Q + 4 * n4, qminmax, bins + 4 * n4);
+    } else {
+        launch(rescaled_bins_kernel, ceil_div(n, kTB), kTB, 0, st, n, Q, qminmax, bins);
+    }
     DCRF_LAUNCH_CHECK();
 }
 
@@ -2927,12 +2976,12 @@ void Lattice::compute_ord_restricted(float* rout, const float* rQ, const int* pI
     launch(fill_int_kernel, ceil_div(N, kTB), kTB, 0, st, (long)N, -1, pos);
     if (nP) {
         launch(scatter_pos_kernel, ceil_div(nP, kTB), kTB, 0, st, nP, pI, pos);
-        launch(ord_bins_kernel, ceil_div((long)nP * L, kTB), kTB, 0, st, (long)nP * L, rQ, rb);
+        ord_bins(rb, rQ, (long)nP * L, st);
     }
     const float2* eb = nullptr;
     if (store) {
         float2* e = r_ebins.ensure((size_t)N * L);
-        launch(ord_bins_kernel, ceil_div((long)N * L, kTB), kTB, 0, st, (long)N * L, Q, e);
+        ord_bins(e, Q, (long)N * L, st);
         eb = e;
         r_L = 0;  // until this call has stored its splat
     }
