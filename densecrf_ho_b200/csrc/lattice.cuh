@@ -64,6 +64,7 @@ struct Live {
     const int* img = nullptr;   // their ids, ascending (device)
     const long* base = nullptr; // the domain: B + 1 ascending unit offsets
     const long* pre = nullptr;  // live prefix: n + 1 entries
+    int images = 0;             // images of the domain (B), when known: all live -> no search
 };
 
 #ifdef __CUDACC__
@@ -81,8 +82,11 @@ __device__ __forceinline__ int live_locate(const Live& lv, long u, long& local) 
     return lv.img[lo];
 }
 // Live unit u -> its unit in the domain (the identity without live images).
+// With every image live the live units are the domain's units in order, so
+// no search is needed.
 __device__ __forceinline__ long live_unit(const Live& lv, long u) {
     if (!lv.n) return u;
+    if (*lv.n == lv.images) return lv.base[0] + u;
     long local;
     const int img = live_locate(lv, u, local);
     return lv.base[img] + local;
@@ -156,7 +160,7 @@ struct Lattice {
     Live live_of(int dom) const {
         if (!live_n) return Live{};
         return Live{live_n, live_img, dom_base.get() + (long)dom * (images + 1),
-                    live_pre + (long)dom * (images + 1)};
+                    live_pre + (long)dom * (images + 1), images};
     }
     // Tile size of the L = 21 / L > 2 plain slice for label count L.
     int slice_tile_for(int L) const;
