@@ -2478,7 +2478,7 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
     auto timed = [&](auto&& fn) {
         fn();  // warm
         DCRF_CUDA(cudaEventRecord(e0, st));
-        for (int r = 0; r < 2; r++) fn();
+        for (int r = 0; r < 3; r++) fn();
         DCRF_CUDA(cudaEventRecord(e1, st));
         DCRF_CUDA(cudaEventSynchronize(e1));
         float ms = 0.0f;
@@ -2495,7 +2495,15 @@ void Lattice::tune_shape(const float* in, int L, const float* pre_norm) {
             FilterShape fs = best;
             fs.splat_kind = kind;
             fs.splat_warps = w;
-            const float t = timed([&] { splat_rest(fs, in, L, pre_norm, src, false, st, nullptr); });
+            // as splat_blur runs it: beside the very long lists' splat on the side stream
+            const float t = timed([&] {
+                const bool fork = splat_huge_fork(in, L, pre_norm, src, false);
+                splat_rest(fs, in, L, pre_norm, src, false, st, nullptr);
+                if (fork) {
+                    DCRF_CUDA(cudaEventRecord(ev_join, aux));
+                    DCRF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+                }
+            });
             if (t < tbest) {
                 tbest = t;
                 best.splat_kind = kind;
@@ -2609,6 +2617,33 @@ void Lattice::splat_rest(const FilterShape& fs, const float* in, int L, const fl
     }
 }
 
+// The lists longer than kHugeList (the first n_huge of the order) run on the
+// high-priority side stream while the others are splatted: with L = 21 by
+// the transposing ring (one warp's chain sets their time, and its three
+// chunks of copies in flight hide the load latency a lone warp cannot hide
+// otherwise), else by splat_kernel.  Forks the side stream from `stream`
+// when there are such lists or `fork_anyway`; the caller joins it.
+bool Lattice::splat_huge_fork(const float* in, int L, const float* pre_norm, float* vals, bool fork_anyway) {
+    const int nh = n_huge;
+    if (nh == 0 && !fork_anyway) return false;
+    const int Lp = value_row(L);
+    const bool live = live_n != nullptr;
+    ensure_aux();
+    DCRF_CUDA(cudaEventRecord(ev_fork, stream));
+    DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
+    if (nh > 0) {
+        const Live lv = live_of(kDomHuge);
+        const int g = unit_grid(nh, kStageWarps, live, 32 * kStageWarps);
+        if (L == 21)
+            launch(pre_norm ? splat_ring21_kernel<true> : splat_ring21_kernel<false>, g, 32 * kStageWarps, 0, aux,
+                   nh, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals, lv, Lp);
+        else
+            launch(pre_norm ? splat_kernel<true> : splat_kernel<false>, g, 32 * kStageWarps, 0, aux, nh, L,
+                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, vals, lv, Lp);
+    }
+    return true;
+}
+
 void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_norm) {
     require(L >= 1, DCRF_E_ARG, "compute: L must be >= 1");
     const int Lp = value_row(L);
@@ -2619,32 +2654,11 @@ void Lattice::splat_blur(const float* in, int L, bool reverse, const float* pre_
     float *src = va.get(), *dst = vb.get();
     // A batched solve's live images: only their lists, vertices and pixels.
     const bool live = live_n != nullptr;
-    // As in the ordered filter, the lists longer than kHugeList (the first
-    // nh of the order) run on the high-priority side stream while the
-    // others are splatted: with L = 21 by the transposing ring (one warp's
-    // chain sets their time, and its three chunks of copies in flight hide
-    // the load latency a lone warp cannot hide otherwise), else by
-    // splat_kernel.
-    // With live images the short lists are a separate launch: it runs on the
+    // As in the ordered filter, the very long lists run on the side stream
+    // (splat_huge_fork).  With live images the short lists are a separate launch: it runs on the
     // side stream too (after the very long lists), beside the long lists'.
-    const int nh = n_huge;
-    const bool fork_short = live && M - n_long > 0 && n_long > nh;
-    const bool forked = nh > 0 || fork_short;
-    if (forked) {
-        ensure_aux();
-        DCRF_CUDA(cudaEventRecord(ev_fork, st));
-        DCRF_CUDA(cudaStreamWaitEvent(aux, ev_fork, 0));
-    }
-    if (nh > 0) {
-        const Live lv = live_of(kDomHuge);
-        const int g = unit_grid(nh, kStageWarps, live, 32 * kStageWarps);
-        if (L == 21)
-            launch(pre_norm ? splat_ring21_kernel<true> : splat_ring21_kernel<false>, g, 32 * kStageWarps, 0, aux,
-                   nh, vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, lv, Lp);
-        else
-            launch(pre_norm ? splat_kernel<true> : splat_kernel<false>, g, 32 * kStageWarps, 0, aux, nh, L,
-                   vorder.get(), seg_start.get(), seg_pix.get(), seg_w.get(), in, pre_norm, src, lv, Lp);
-    }
+    const bool fork_short = live && M - n_long > 0 && n_long > n_huge;
+    const bool forked = splat_huge_fork(in, L, pre_norm, src, fork_short);
     splat_rest(shape, in, L, pre_norm, src, live, st, fork_short ? aux : nullptr);
     if (forked) {
         DCRF_CUDA(cudaEventRecord(ev_join, aux));

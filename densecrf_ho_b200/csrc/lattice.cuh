@@ -226,6 +226,9 @@ struct Lattice {
     // short lists' launch goes on st_short when one is given.
     void splat_rest(const FilterShape& fs, const float* in, int L, const float* pre_norm, float* vals,
                     bool live, cudaStream_t st, cudaStream_t st_short);
+    // Forks the side stream and splats the very long lists there (see
+    // lattice.cu); true when it forked (the caller joins ev_join).
+    bool splat_huge_fork(const float* in, int L, const float* pre_norm, float* vals, bool fork_anyway);
 
     Lattice() = default;
     Lattice(const Lattice&) = delete;
