@@ -137,6 +137,29 @@ def test_filter_every_launch_shape_bit_exact(shape, oracle_mod):
     assert n.value == 0
 
 
+@pytest.mark.parametrize("form", [3, 5])
+def test_staged_splat_ragged_end_and_unaligned_input(form, oracle_mod):
+    """The staged splat forms at an odd pixel count (84 N not a multiple of
+    16: the bulk copy of the last pixel's run would pass the end of the input
+    and takes plain loads instead) and with an input pointer that is not
+    16-byte aligned (the bulk-copy form falls back to the tiled one)."""
+    import torch
+    W, H = 161, 119
+    img = synth.make_image(W, H, 21, 8)
+    f = synth.bilateral_features(W, H, 50, 50, 15, 15, 15, img["rgb"])
+    lat, orc = Permutohedral().init(f).set_filter_shape((4, 256, 128, form)), oracle_mod.OracleLattice(f)
+    x = np.random.default_rng(23).standard_normal((W * H, 21)).astype(np.float32)
+    ref = orc.compute(x)
+    assert _eq(lat.compute(x), ref)
+    buf = torch.empty(W * H * 21 + 1, device="cuda")
+    buf[1:] = torch.from_numpy(x.ravel()).cuda()  # 4 bytes past a 16-byte boundary
+    out = torch.empty(W * H * 21, device="cuda")
+    check(lib().dcrf_lattice_compute_dev(lat._h, C.c_void_p(out.data_ptr()), C.c_void_p(buf[1:].data_ptr()),
+                                         21, 0))
+    torch.cuda.synchronize()
+    assert _eq(out.cpu().numpy().reshape(W * H, 21), ref)
+
+
 def test_filter_error_vs_fp64_oracle(oracle_mod):
     """Relative error of the FP32 filter against the FP64 lattice oracle."""
     W, H = 160, 120
