@@ -177,6 +177,41 @@ def test_many_cliques_vs_oracle(oracle_mod):
     assert abs(ea - eb) <= ENERGY_RTOL * abs(eb)
 
 
+def test_large_cliques_across_chunks_vs_oracle(oracle_mod):
+    """Cliques whose sizes straddle the chunked clique kernels' boundaries
+    (128-pixel chunks of computeUCondGrad and of the LP clique energy,
+    256-row segments of the FP64 prefix chains) up to nearly the whole image,
+    overlapping, with heavy weights: the LP clique energy of a given Q equals
+    the oracle's, lp_sp and qp_sp agree with it."""
+    W, H = 64, 48
+    N = W * H
+    img = synth.make_image(W, H, 21, 12)
+    rng = np.random.default_rng(31)
+    sizes = np.array([1, 2, 127, 128, 129, 255, 256, 257, 300, 513, 1000, 2900])
+    idx = np.concatenate([np.sort(rng.choice(N, s, replace=False)) for s in sizes]).astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    ew = rng.uniform(2.0, 20.0, len(sizes)).astype(np.float32)
+    cs = np.full(len(sizes), 50.0, np.float32)
+    orc = oracle_mod.build_model(oracle_mod.OracleModel, img)
+    orc.set_cliques(off, idx, ew, cs)
+    m = DenseCRF2D(W, H, 21)
+    m.setUnaryEnergy(img["unary"])
+    m.addPairwiseGaussian(3.0, 3.0, 3.0)
+    m.addPairwiseBilateral(50.0, 50.0, 15.0, 15.0, 15.0, img["rgb"], 5.0)
+    m.setCliques(off, idx, ew, cs)
+    Q = orc.unary_init()
+    rq = rng.random(Q.shape).astype(np.float32)
+    assert m.compute_energy_LP_higher_order(rq) == pytest.approx(orc.energy_lp(rq), rel=1e-9)
+    a = m.lp_inference_prox_super_pixels(Q, prox_max_iter=3, fw_max_iter=5)
+    b, _ = orc.lp(Q, prox_max_iter=3, fw_max_iter=5)
+    assert (m.currentMap(a) == orc.current_map(b)).mean() >= 0.999
+    assert np.abs(a - b).max() < 1e-3
+    a, st = m.qp_inference_super_pixels_non_convex(Q, max_iter=20, stats=True)
+    b, it, en = orc.qp(Q, 20)
+    assert (m.currentMap(a) == orc.current_map(b)).mean() >= 0.999
+    assert st.energy == pytest.approx(float(en[-1]), rel=1e-6)
+
+
 def test_kernel_and_weight_gradients_vs_reference():
     """pairwise_[k]->kernelGradient(b, Q) (feature-scale gradient of the
     diagonal kernel, symmetric normalisation) and ->gradient(b, Q) (Potts
