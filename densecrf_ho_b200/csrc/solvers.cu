@@ -230,6 +230,21 @@ __global__ void __launch_bounds__(kHoThreads)
                 }
             };
             int qq = 0;
+            if (nq == kHoChunk && q0 + kHoChunk < next) {
+                // a whole chunk before the next record: all its loads first,
+                // then one straight chain of adds
+                float x[kHoChunk];
+#pragma unroll
+                for (int i = 0; i < kHoChunk; i++) x[i] = r[i * L];
+#pragma unroll
+                for (int i = 0; i < kHoChunk; i++) {
+                    float xi = x[i];
+                    if (minus_one) xi = fsub(xi, 1.0f);
+                    if (OUT32) s32 = fadd(s32, xi);
+                    if (OUT64) s64 += (double)xi;
+                }
+                qq = kHoChunk;
+            }
             // batches of eight: the eight loads first, then the chain; no
             // record check inside a batch that ends before the next record
             for (; qq + 8 <= nq; qq += 8) {
