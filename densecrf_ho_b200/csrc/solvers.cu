@@ -176,16 +176,16 @@ __device__ __forceinline__ void cp_async_wait_group() {
 
 // The clique-local prefix chains of multiplySuperPixels: pre(lab, s) =
 // sum_{q < s} p(lab, q) with p = Q - 1 (or p as given), one sequential chain
-// per label -- in float as the reference sums it (OUT32) and / or in FP64
-// (OUT64), both from the same staged rows -- recorded at every clique size:
-// out[ptr * L + lab] = pre(lab, size of the ptr-th clique in size order).
+// per label in float, as the reference sums it, recorded at every clique
+// size: out32[ptr * L + lab] = pre(lab, size of the ptr-th clique in size
+// order).  (The FP64 prefixes the clique products use come from
+// ho_prefix64's parallel segments.)
 // The chain thread only adds and compares: the next record point is the
 // size of the next clique in size order, so the loads of the staged rows
 // run ahead of the dependent adds.
-template <bool OUT32, bool OUT64>
 __global__ void __launch_bounds__(kHoThreads)
     ho_prefix_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one, float* __restrict__ out32,
-                     double* __restrict__ out64, const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
+                     const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
     if (sc && skip_on_zero_step && sc->zero_step) return;
     __shared__ __align__(16) float rows[2][kHoChunk * kLMax];
     const int lab = threadIdx.x;
@@ -193,8 +193,7 @@ __global__ void __launch_bounds__(kHoThreads)
     int ptr = cv.bstart[1];  // cliques of size 0 come first in size order
     if (chain)
         for (int r = 0; r < ptr; r++) {
-            if (OUT32) out32[(long)r * L + lab] = 0.0f;
-            if (OUT64) out64[(long)r * L + lab] = 0.0;
+            out32[(long)r * L + lab] = 0.0f;
         }
     int next = ptr < cv.R ? cv.sizes[ptr] : INT_MAX;
     const int nchunks = (cv.max_size + kHoChunk - 1) / kHoChunk;
@@ -207,7 +206,6 @@ __global__ void __launch_bounds__(kHoThreads)
     stage(0);
     cp_async_commit_group();
     float s32 = 0.0f;
-    double s64 = 0.0;
     for (int c = 0; c < nchunks; c++) {
         if (c + 1 < nchunks) stage(c + 1);
         cp_async_commit_group();
@@ -220,11 +218,9 @@ __global__ void __launch_bounds__(kHoThreads)
             // the prefix length reached
             auto step = [&](float x, int len) {
                 if (minus_one) x = fsub(x, 1.0f);
-                if (OUT32) s32 = fadd(s32, x);
-                if (OUT64) s64 += (double)x;
+                s32 = fadd(s32, x);
                 while (len == next) {
-                    if (OUT32) out32[(long)ptr * L + lab] = s32;
-                    if (OUT64) out64[(long)ptr * L + lab] = s64;
+                    out32[(long)ptr * L + lab] = s32;
                     ptr++;
                     next = ptr < cv.R ? cv.sizes[ptr] : INT_MAX;
                 }
@@ -240,8 +236,7 @@ __global__ void __launch_bounds__(kHoThreads)
                 for (int i = 0; i < kHoChunk; i++) {
                     float xi = x[i];
                     if (minus_one) xi = fsub(xi, 1.0f);
-                    if (OUT32) s32 = fadd(s32, xi);
-                    if (OUT64) s64 += (double)xi;
+                    s32 = fadd(s32, xi);
                 }
                 qq = kHoChunk;
             }
@@ -256,8 +251,7 @@ __global__ void __launch_bounds__(kHoThreads)
                     for (int i = 0; i < 8; i++) {
                         float xi = x[i];
                         if (minus_one) xi = fsub(xi, 1.0f);
-                        if (OUT32) s32 = fadd(s32, xi);
-                        if (OUT64) s64 += (double)xi;
+                        s32 = fadd(s32, xi);
                     }
                 } else {
 #pragma unroll
@@ -392,7 +386,7 @@ __global__ void ho_direction_kernel(CliqueView cv, int L, const float* __restric
 // sum_r sum_{q < size_r} sum_lab p1(lab, r) p2(lab, q), clique-local q again.
 // Evaluated in FP64 as sum_lab sum_r p1(lab, r) * prefix_lab(size_r), the r
 // in size order, then rounded to float; the FP64 prefixes come from
-// ho_prefix_kernel<.., true>.  One thread per label; its loads do not depend on
+// ho_prefix64.  One thread per label; its loads do not depend on
 // its sum, so they run ahead of it.
 __global__ void ho_scalar_kernel(CliqueView cv, int L, const float* __restrict__ p1, const double* __restrict__ pre,
                                  int slot, SolverScalars* sc, int add_to_slot) {
@@ -1502,8 +1496,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         ho = buf(4);
         DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
         // the float chain of Q - 1 (sequential, as the reference sums it) and its FP64 prefixes
-        launch(ho_prefix_kernel<true, false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (double*)nullptr,
-               (const SolverScalars*)nullptr, 0);
+        launch(ho_prefix_kernel, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (const SolverScalars*)nullptr, 0);
         ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
         launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 0, nullptr);
     }
@@ -1563,8 +1556,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         if (R > 0) {
             // the prefixes of the updated Q - 1 (after a zero step Q is
             // unchanged, and so is the float chain)
-            launch(ho_prefix_kernel<true, false>, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (double*)nullptr,
-                   (const SolverScalars*)sc, 1);
+            launch(ho_prefix_kernel, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (const SolverScalars*)sc, 1);
             ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
             launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 1, sc);
             launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
