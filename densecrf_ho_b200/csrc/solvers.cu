@@ -160,7 +160,7 @@ struct CliqueView {
 // thread per label; the rows p[q][*] they read are staged through shared
 // memory kHoChunk at a time by the whole block, the next chunk's copies in
 // flight while the current one is summed.
-constexpr int kHoChunk = 64;  // two staging buffers of 64 rows x kLMax labels: 32 KB
+constexpr int kHoChunk = 128;  // rows per staged chunk (two buffers of kHoChunk x L floats, dynamic)
 constexpr int kHoThreads = 256;
 
 __device__ __forceinline__ void cp_async4_ca(void* sdst, const void* gsrc) {
@@ -187,7 +187,7 @@ __global__ void __launch_bounds__(kHoThreads)
     ho_prefix_kernel(CliqueView cv, int L, const float* __restrict__ p, int minus_one, float* __restrict__ out32,
                      const SolverScalars* __restrict__ sc, int skip_on_zero_step) {
     if (sc && skip_on_zero_step && sc->zero_step) return;
-    __shared__ __align__(16) float rows[2][kHoChunk * kLMax];
+    extern __shared__ __align__(16) float ho_rows[];  // [2][kHoChunk][L]
     const int lab = threadIdx.x;
     const bool chain = lab < L;
     int ptr = cv.bstart[1];  // cliques of size 0 come first in size order
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kHoThreads)
     const int nchunks = (cv.max_size + kHoChunk - 1) / kHoChunk;
     auto stage = [&](int c) {
         const int q0 = c * kHoChunk, n = min(kHoChunk, cv.max_size - q0) * L;
-        float* dst = rows[c & 1];
+        float* dst = ho_rows + (size_t)(c & 1) * kHoChunk * L;
         const float* src = p + (long)q0 * L;
         for (int e = threadIdx.x; e < n; e += blockDim.x) cp_async4_ca(dst + e, src + e);
     };
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(kHoThreads)
         cp_async_wait_group<1>();  // chunk c has landed (this thread's copies)
         __syncthreads();           // ... and everyone's
         if (chain) {
-            const float* r = rows[c & 1] + lab;
+            const float* r = ho_rows + (size_t)(c & 1) * kHoChunk * L + lab;
             const int q0 = c * kHoChunk, nq = min(kHoChunk, cv.max_size - q0);
             // one element: add, then record at every clique whose size is
             // the prefix length reached
@@ -329,6 +329,19 @@ __global__ void ho_seg_prefix_kernel(CliqueView cv, int L, const float* __restri
         for (int i = 0; i < 8; i++) step(x[i], q + i + 1);
     }
     for (; q < q1; q++) step(p[(long)q * L + lab], q + 1);
+}
+
+// The float clique prefix chain of p (minus one when asked) into out32.
+static void ho_prefix32(cudaStream_t stream, int L, const CliqueView& cv, const float* p, int minus_one, float* out32,
+                        const SolverScalars* sc, int skip_on_zero_step) {
+    static const bool attr = [] {  // two 128-row buffers: up to 64 KB for L = 64
+        DCRF_CUDA(cudaFuncSetAttribute(ho_prefix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(sizeof(float) * 2 * kHoChunk * kLMax)));
+        return true;
+    }();
+    (void)attr;
+    launch(ho_prefix_kernel, 1, kHoThreads, sizeof(float) * 2 * kHoChunk * L, stream, cv, L, p, minus_one, out32, sc,
+           skip_on_zero_step);
 }
 
 // FP64 clique prefixes of p (minus one when asked) into out64 [R][L]:
@@ -1496,7 +1509,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         ho = buf(4);
         DCRF_CUDA(cudaMemsetAsync(ho, 0, sizeof(float) * NL, stream));
         // the float chain of Q - 1 (sequential, as the reference sums it) and its FP64 prefixes
-        launch(ho_prefix_kernel, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (const SolverScalars*)nullptr, 0);
+        ho_prefix32(stream, L, cv, Q, 1, pre32, nullptr, 0);
         ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
         launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 0, nullptr);
     }
@@ -1556,7 +1569,7 @@ int Model::qp(const float* init, float* out, int max_iter, double* energy_out) {
         if (R > 0) {
             // the prefixes of the updated Q - 1 (after a zero step Q is
             // unchanged, and so is the float chain)
-            launch(ho_prefix_kernel, 1, kHoThreads, 0, stream, cv, L, Q, 1, pre32, (const SolverScalars*)sc, 1);
+            ho_prefix32(stream, L, cv, Q, 1, pre32, sc, 1);
             ho_prefix64(stream, ho_seg, clique_max, L, cv, Q, 1, preQ, nullptr, 0);
             launch(ho_regions_kernel, ceil_div(LR, 256), 256, 0, stream, cv, L, pre32, gz, 1, sc);
             launch(ho_zterm_prep_kernel, 1, 256, 0, stream, cv, L, z, zc, omz, sc);
